@@ -1,0 +1,158 @@
+"""Seeded synthetic inputs for the cross-power path.
+
+Host-side numpy generator of detector data (not part of the GPU path and
+never timed).  It restates the reference's injection helpers:
+
+* ``gaussian_white_noise``      -- inject.c:48-56
+* ``inject_transform_point_source`` -- inject.c:119-152 (FFT fractional
+  delay by r.s / dt, periodic)
+* ``inject_into``               -- inject.c:187-203
+* ``tseries_to_fseries``        -- correlator.c:224-231 (r2c FFT, then the
+  negative frequencies filled with conjugates)
+
+plus the coloured-noise / chirp / whitening recipe of the demo front end
+(sphradiometer_demo.c:456-460) used by the benchmark workloads.  Random
+numbers come from numpy's Philox generator; a segment's seed is the
+workload seed xor the segment index.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+C_LIGHT = 299792458.0
+R_EARTH = 6.371e6
+R_EARTH_S = R_EARTH / C_LIGHT
+
+
+def rng_for(seed: int, index: int = 0) -> np.random.Generator:
+    return np.random.Generator(np.random.Philox(int(seed) ^ int(index)))
+
+
+def vector_r_dot_s(v, theta, phi):
+    """instrument.c:77-80."""
+    return (v[0] * np.cos(phi) + v[1] * np.sin(phi)) * np.sin(theta) + v[2] * np.cos(theta)
+
+
+def gaussian_white_noise(n: int, variance: float, rng: np.random.Generator) -> np.ndarray:
+    return rng.normal(0.0, np.sqrt(variance), n)
+
+
+def inject_transform_point_source(position, x, dt: float, theta: float, phi: float) -> np.ndarray:
+    n = len(x)
+    r_dot_s = vector_r_dot_s(position, theta, phi)
+    ft = np.fft.rfft(x)
+    k = np.arange(n // 2 + 1)
+    ft *= np.exp(1j * 2 * np.pi * r_dot_s * k / (dt * n))
+    return np.fft.irfft(ft, n)
+
+
+def inject_into(position, series, injection, dt: float, ra: float, dec: float, gmst: float):
+    gha = gmst - ra
+    series += inject_transform_point_source(position, injection, dt, np.pi / 2 - dec, -gha)
+    return series
+
+
+def tseries_to_fseries(x) -> np.ndarray:
+    n = len(x)
+    F = np.zeros(n, np.complex128)
+    h = np.fft.rfft(x)
+    F[: n // 2 + 1] = h
+    for i in range(1, (n + 1) // 2):
+        F[n - i] = np.conj(F[i])
+    return F
+
+
+def random_positions(n_det: int, radius: float, rng: np.random.Generator) -> np.ndarray:
+    """Detectors at isotropic random points on a sphere of the given radius
+    (seconds)."""
+    v = rng.normal(size=(n_det, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    return v * radius
+
+
+def pair_positions(separation_s: float, rng: np.random.Generator) -> np.ndarray:
+    """Two Earth-surface points whose chord is ``separation_s`` seconds."""
+    half = np.arcsin(min(1.0, separation_s / (2 * R_EARTH_S)))
+    u = rng.normal(size=3)
+    u /= np.linalg.norm(u)
+    w = rng.normal(size=3)
+    w -= u * (w @ u)
+    w /= np.linalg.norm(w)
+    p0 = R_EARTH_S * (np.cos(half) * u + np.sin(half) * w)
+    p1 = R_EARTH_S * (np.cos(half) * u - np.sin(half) * w)
+    return np.stack([p0, p1])
+
+
+def isotropic_direction(rng: np.random.Generator):
+    """(theta, phi) uniform on the sphere."""
+    return float(np.arccos(rng.uniform(-1, 1))), float(rng.uniform(0, 2 * np.pi))
+
+
+def psd(f) -> np.ndarray:
+    """S(f) = 1e-46 [(f/100)^-4 + 2 + (f/100)^2] on 20-1000 Hz, 0 outside."""
+    f = np.asarray(f, np.float64)
+    out = np.zeros_like(f)
+    band = (f >= 20.0) & (f <= 1000.0)
+    x = f[band] / 100.0
+    out[band] = 1e-46 * (x ** -4 + 2.0 + x ** 2)
+    return out
+
+
+def chirp(n: int, dt: float, f0: float = 60.0, f1: float = 400.0, duration: float = 0.25) -> np.ndarray:
+    """A Tukey-windowed linear chirp f0 -> f1, centred in the segment."""
+    t = np.arange(n) * dt
+    t0 = 0.5 * n * dt - 0.5 * duration
+    tau = t - t0
+    on = (tau >= 0) & (tau < duration)
+    h = np.zeros(n)
+    ph = 2 * np.pi * (f0 * tau[on] + 0.5 * (f1 - f0) * tau[on] ** 2 / duration)
+    w = np.sin(np.pi * tau[on] / duration) ** 2
+    h[on] = w * np.sin(ph)
+    return h
+
+
+def whitened_segment(positions, n: int, dt: float, theta: float, phi: float, snr: float,
+                     rng: np.random.Generator, hermitian: bool = True) -> np.ndarray:
+    """One segment for every detector: coloured noise plus a chirp from
+    (theta, phi) (Earth-fixed), delayed per detector with the FFT
+    fractional delay, then whitened by 1/sqrt(S) in the 20-1000 Hz band.
+    Returns n_det x (n/2+1) (hermitian=True) or n_det x n spectra."""
+    nd = len(positions)
+    k = np.arange(n // 2 + 1)
+    f = k / (n * dt)
+    S = psd(f)
+    inband = S > 0
+    wh = np.zeros_like(S)
+    wh[inband] = 1.0 / np.sqrt(S[inband])
+    # noise with one-sided PSD S: E|X_k|^2 = n S / (2 dt)
+    sigma = np.sqrt(S * n / (2 * dt) / 2.0)
+    h = chirp(n, dt)
+    Hf = np.fft.rfft(h)
+    rho2 = 4.0 * np.sum(np.abs(Hf[inband] * dt) ** 2 / S[inband]) / (n * dt)
+    h *= snr / np.sqrt(rho2) if rho2 > 0 else 0.0
+    out = np.zeros((nd, n // 2 + 1), np.complex128)
+    for d in range(nd):
+        nz = sigma * (rng.normal(size=k.size) + 1j * rng.normal(size=k.size))
+        nz[0] = nz[0].real
+        if n % 2 == 0:
+            nz[-1] = nz[-1].real
+        x = np.fft.irfft(nz, n)
+        x += inject_transform_point_source(positions[d], h, dt, theta, phi)
+        out[d] = np.fft.rfft(x) * wh
+    if hermitian:
+        return out
+    full = np.zeros((nd, n), np.complex128)
+    full[:, : n // 2 + 1] = out
+    for i in range(1, (n + 1) // 2):
+        full[:, n - i] = np.conj(out[:, i])
+    return full
+
+
+def full_from_half(half, n: int) -> np.ndarray:
+    """Hermitian completion of n/2+1 bins to n bins (last axis)."""
+    half = np.asarray(half)
+    full = np.zeros(half.shape[:-1] + (n,), np.complex128)
+    full[..., : n // 2 + 1] = half
+    idx = np.arange(1, (n + 1) // 2)
+    full[..., n - idx] = np.conj(half[..., idx])
+    return full
