@@ -1,0 +1,408 @@
+"""Benchmark: sky maps/s of the batched split-precision cross-power path.
+
+Workload (the configuration the headline metric is quoted on): a 3-detector
+network at seeded points on an Earth-radius sphere (3 baselines), 1 s
+segments at 4096 Hz (n = 4096, 2049 unique bins), power l_max = 32
+((l_max+1)^2 = 1089 a_lm per sky), synthetic whitened Gaussian noise plus a
+chirp injection per segment (seeded), per-segment GMST rotation.  A step
+integrates one batch of ``--segments`` segments (default 4096) into that
+many Earth-frame skies.  Inputs are a ring of distinct batches whose total
+size exceeds the 126 MB L2, so every step streams its spectra from HBM.
+
+Printed: one JSON line (rank 0).  ``value`` is whole-job maps/s with
+spectra resident in HBM; ``e2e`` the same through the C-ABI host-buffer
+entry point (pinned host memory, copies inside the timed region);
+``roofline`` the contraction kernel's achieved HBM bandwidth against the
+measured copy peak; ``cpu_baseline`` the CPU oracle (FP64 C restatement of
+the reference's path) on the host cores.  ``--impl reference`` times only
+that CPU oracle and prints its own line.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "sky maps/sec @ l_max=32, 3 baselines: split-prec batched vs FP64 plain"
+N_SAMPLES, DT, L_MAX, N_DET = 4096, 1.0 / 4096, 32, 3
+WORKLOAD = ("c1: 3-detector network on an Earth-radius sphere (3 baselines), 1 s segments at 4096 Hz "
+            "(n=4096, 2049 unique bins), l_max=32 (1089 a_lm), per-segment GMST rotation")
+L2_BYTES = 126 * 2 ** 20
+
+
+def env_rank():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def positions(seed=2):
+    from sphradiometer_b200 import workload as W
+    return W.random_positions(N_DET, W.R_EARTH_S, W.rng_for(seed))
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(segments: int):
+    """DRAM bytes per contraction launch from the committed ncu summary,
+    scaled to ``segments`` (traffic grows with the segments streamed)."""
+    p = os.path.join(ROOT, "profiles", "k_tc_contract_c1.md")
+    if not os.path.exists(p):
+        return None
+    txt = open(p).read()
+    m = re.search(r"dram_bytes_per_segment:\s*([0-9.eE+]+)", txt)
+    return float(m.group(1)) * segments if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = "clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 6:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[2:6]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_oracle_rate(net_tables, F_half, gmst, budget_s: float, threads: int):
+    """Maps/s of the CPU oracle (C, FP64) integrating segments exactly as
+    correlator_network_integrate_power_fd + sh_series_rotate_z do, on
+    ``threads`` host threads (ctypes releases the GIL)."""
+    from oracle import oracle as O
+    from sphradiometer_b200 import workload as W
+    lib = O.lib()
+    n = N_SAMPLES
+    pairs = [(1, 0), (2, 0), (2, 1)]
+    D = [np.ascontiguousarray(t[0]) for t in net_tables]
+    R = [np.ascontiguousarray(t[1]) for t in net_tables]
+    n_seg = F_half.shape[1]
+    full = [W.full_from_half(F_half[:, s, :], n) for s in range(min(n_seg, 64))]
+    done = [0] * threads
+    stop = time.perf_counter() + budget_s
+
+    def work(tid):
+        out = np.zeros((L_MAX + 1) ** 2, np.complex128)
+        tmp = np.zeros_like(out)
+        k = tid
+        while time.perf_counter() < stop:
+            F = full[k % len(full)]
+            out[:] = 0
+            for b, (i, j) in enumerate(pairs):
+                lib.orc_baseline_integrate_power_fd(F[i], F[j], n, D[b].ravel(), L_MAX, R[b], tmp)
+                out += tmp / 3
+            lib.orc_rotate_z(out, L_MAX, 0, float(gmst[k % len(gmst)]))
+            done[tid] += 1
+            k += threads
+
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=work, args=(t,)) for t in range(threads)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    el = time.perf_counter() - t0
+    return sum(done) / el, sum(done), el
+
+
+def run_reference(args):
+    """--impl reference: the CPU oracle (FP64 restatement of the reference's
+    own CPU path) on all host cores."""
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    from sphradiometer_b200 import workload as W
+    pos = positions()
+    tables = []
+    for i in range(1, N_DET):
+        for j in range(i):
+            d = pos[i] - pos[j]
+            th, ph = O.vector_direction(d)
+            tables.append((O.delay_product(float(np.linalg.norm(d)), DT, N_SAMPLES, L_MAX),
+                           O.rotation_plan(L_MAX, O.rot_matrix(th, ph))))
+    batch = W.make_batch(pos, N_SAMPLES, DT, 64, seed=1234)
+    threads = os.cpu_count() or 1
+    rates = []
+    per_step = max(2.0, min(10.0, 60.0 / max(1, args.steps + args.warmup)))
+    for it in range(args.warmup + args.steps):
+        r, cnt, el = cpu_oracle_rate(tables, batch["F"], batch["gmst"], per_step, threads)
+        if it >= args.warmup:
+            rates.append(r)
+    value = statistics.median(rates)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "maps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded whitened noise + chirp injections)",
+        "config": {"workload": WORKLOAD, "segments_per_sample": 64},
+        "cpu_baseline": {"value": value, "unit": "maps/s", "cores": threads, "kind": "port",
+                         "sample": f"each step: {per_step:.0f} s of segments integrated by the C oracle on {threads} threads"},
+        "e2e": {"value": value, "unit": "maps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run(args):
+    import torch
+    import torch.distributed as dist
+    import sphradiometer_b200 as S
+    from sphradiometer_b200 import workload as W
+
+    rank, world, local = env_rank()
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    n_seg = args.segments
+    K = N_SAMPLES // 2 + 1
+    pos = positions()
+    net = S.Network(pos, N_SAMPLES, DT, l_max=L_MAX)
+    prec = args.precision
+    bp = S.BatchPlan(net, prec)
+
+    # ring of distinct batches whose total exceeds L2
+    batch_bytes = N_DET * n_seg * K * 16
+    n_ring = max(1, -(-2 * L2_BYTES // batch_bytes))
+    n_ring = min(n_ring, 64)
+    base = W.make_batch(pos, N_SAMPLES, DT, min(n_seg, 1024), seed=1000 + rank)
+    ring, gm = [], []
+    for r in range(n_ring):
+        idx = (np.arange(n_seg) + r * 7) % base["F"].shape[1]
+        Fr = np.ascontiguousarray(base["F"][:, idx, :])
+        ring.append(torch.from_numpy(Fr).to(dev))
+        gm.append(torch.from_numpy(base["gmst"][idx].copy() + 0.01 * r).to(dev))
+    out = torch.empty((n_seg, (L_MAX + 1) ** 2), dtype=torch.complex128, device=dev)
+    split = bp.autotune(ring[0]) if args.autotune else bp.split(n_seg)
+    st = torch.cuda.current_stream()
+
+    # warm-up
+    for w in range(args.warmup):
+        bp.integrate(ring[w % n_ring], gm[w % n_ring], out=out)
+    torch.cuda.synchronize()
+
+    # per-step events around the contraction kernel (recorded by the library)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_begin, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index) as clk:
+        t_begin.record(st)
+        for s in range(args.steps):
+            S.load().sphrad_batch_set_timing_events(bp._p, C.c_void_p(ev[s][0].cuda_event), C.c_void_p(ev[s][1].cuda_event))
+            bp.integrate(ring[s % n_ring], gm[s % n_ring], out=out)
+        t_end.record(st)
+        torch.cuda.synchronize()
+    S.load().sphrad_batch_set_timing_events(bp._p, None, None)
+    elapsed_ms = t_begin.elapsed_time(t_end)
+    kern_ms = [a.elapsed_time(b) for a, b in ev]
+    if world > 1:
+        t = torch.tensor([elapsed_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+        dist.barrier()
+    status = bp.status()
+    value = world * n_seg * args.steps / (elapsed_ms / 1e3)
+    kernels = bp.kernels_per_call()
+
+    # roofline of the contraction kernel: algorithmic bytes per launch =
+    # spectra (n_det x bins x 16 B per segment) + the delay-table operand
+    # (read once per launch) + FP32 partial sums (B x accstride x 4 B per
+    # segment per split)
+    mean_k = statistics.mean(kern_ms) / 1e3
+    accstride = ((L_MAX + 1) + 3) & ~3
+    if prec == "bf16x3":
+        npad = ((L_MAX + 1) + 15) & ~15
+        d_bytes = -(-K // 8) * 3 * 2 * npad * 16 * 2
+        acc_el = 4
+    else:
+        d_bytes = K * 3 * (L_MAX + 1) * (16 if prec == "fp64" else 8)
+        acc_el = 8 if prec == "fp64" else 4
+    alg_bytes = N_DET * n_seg * K * 16 + d_bytes + split * n_seg * 3 * accstride * acc_el
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / mean_k / 1e9
+
+    extra = {}
+    e2e = None
+    cpu = None
+    if rank == 0:
+        # e2e through the C-ABI host-buffer entry point (pinned memory)
+        Fh = torch.empty((N_DET, n_seg, K), dtype=torch.complex128, pin_memory=True)
+        Fh.copy_(ring[0].cpu())
+        Fh_np = Fh.numpy()
+        gh = gm[0].cpu().numpy().copy()
+        sky_h = torch.empty((n_seg, (L_MAX + 1) ** 2), dtype=torch.complex128, pin_memory=True).numpy()
+        for _ in range(2):
+            bp.integrate_host(Fh_np, gh, out=sky_h)
+        e2e_steps = max(3, min(20, args.steps))
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            bp.integrate_host(Fh_np, gh, out=sky_h)
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+        e2e = {"value": n_seg / e2e_s, "unit": "maps/s", "h2d_bytes_per_step": int(N_DET * n_seg * K * 16 + n_seg * 8),
+               "d2h_bytes_per_step": int(n_seg * (L_MAX + 1) ** 2 * 16)}
+
+        # plain FP64 GPU path: the drop-in correlator_network_integrate_power_fd
+        # (one segment per call, host buffers, FP64 kernels) + rotate_z
+        nfull = min(64, n_seg)
+        full = [W.full_from_half(base["F"][:, s, :], N_SAMPLES) for s in range(nfull)]
+        L = S.load()
+        sky = L.sh_series_new_zero(L_MAX, 0)
+        ptr_sets = []
+        for F in full:
+            arrs = [np.ascontiguousarray(F[d]) for d in range(N_DET)]
+            ptr_sets.append((arrs, (C.c_void_p * N_DET)(*[a.ctypes.data for a in arrs])))
+        for arrs, ptrs in ptr_sets[:4]:
+            L.correlator_network_integrate_power_fd(sky, ptrs, net.plan)
+        t0 = time.perf_counter()
+        cnt = 0
+        while time.perf_counter() - t0 < 3.0:
+            arrs, ptrs = ptr_sets[cnt % len(ptr_sets)]
+            L.correlator_network_integrate_power_fd(sky, ptrs, net.plan)
+            L.sh_series_rotate_z(sky, sky, 0.1)
+            cnt += 1
+        plain = cnt / (time.perf_counter() - t0)
+        L.sh_series_free(sky)
+        extra["fp64_plain_maps_per_s"] = plain
+        extra["split_vs_fp64_plain"] = value / world / plain
+
+        # other precisions of the batched path, same workload and timing
+        for other in ("fp64", "fp32"):
+            if other == prec:
+                continue
+            op = S.BatchPlan(net, other)
+            for w in range(3):
+                op.integrate(ring[w % n_ring], gm[w % n_ring], out=out)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            reps = max(5, args.steps // 10)
+            a.record(st)
+            for s in range(reps):
+                op.integrate(ring[s % n_ring], gm[s % n_ring], out=out)
+            b.record(st)
+            torch.cuda.synchronize()
+            extra[f"{other}_batched_maps_per_s"] = n_seg * reps / (a.elapsed_time(b) / 1e3)
+            op.close()
+        # exactly the c1 batch size (64 segments per launch)
+        if n_seg != 64:
+            bp64 = S.BatchPlan(net, prec)
+            F64 = ring[0][:, :64, :].contiguous()
+            g64 = gm[0][:64].contiguous()
+            o64 = torch.empty((64, (L_MAX + 1) ** 2), dtype=torch.complex128, device=dev)
+            bp64.autotune(F64)
+            for _ in range(5):
+                bp64.integrate(F64, g64, out=o64)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            for _ in range(200):
+                bp64.integrate(F64, g64, out=o64)
+            b.record(st)
+            torch.cuda.synchronize()
+            extra["c1_64_segments_per_launch_maps_per_s"] = 64 * 200 / (a.elapsed_time(b) / 1e3)
+            bp64.close()
+
+        # CPU baseline: the oracle on the host cores, bounded sample
+        tables = [(net.delay_table(k), net.rotation_flat(k)) for k in range(3)]
+        threads = os.cpu_count() or 1
+        rate, nmaps, el = cpu_oracle_rate(tables, base["F"], base["gmst"], args.cpu_seconds, threads)
+        cpu = {"value": rate, "unit": "maps/s", "cores": threads, "kind": "port",
+               "sample": f"{nmaps} skies of this workload in {el:.1f} s (C oracle, FP64, {threads} threads)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "maps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16x3 (fp32 accumulate)" if prec == "bf16x3" else prec, "data": "synthetic (seeded whitened noise + chirp injections)",
+            "config": {"workload": WORKLOAD, "segments_per_step": n_seg, "precision": prec, "split_k": split,
+                       "l2": f"inputs larger than L2: ring of {n_ring} distinct batches, {n_ring * batch_bytes / 2**20:.0f} MiB",
+                       "parallelism": f"replicas x{world} (segments sharded, no collective)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": profiled_traffic(n_seg), "kernel": "k_tc_contract" if prec == "bf16x3" else "k_cc_contract",
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
+                         "algorithmic_bytes_per_launch": alg_bytes, "mean_launch_ms": mean_k * 1e3},
+            "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kernels * args.steps, "clocks": clk.summary(), "device_status": status,
+        }
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--segments", type=int, default=4096)
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp32", "fp64"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

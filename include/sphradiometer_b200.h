@@ -1,0 +1,92 @@
+/*
+ * sphradiometer_b200.h -- batched, device-resident extension API of
+ * libsphradiometer_b200 (no counterpart in the reference, which integrates
+ * one segment per call: correlator_network_integrate_power_fd,
+ * correlator.c:993-1010, followed by the caller's sh_series_rotate_z).
+ *
+ * One call integrates the cross power of n_seg segments of one detector
+ * network and returns one Earth-frame sky (a_lm up to l_max, the
+ * reference's m-major order, FP64 complex) per segment, each optionally
+ * rotated about z by the segment's GMST.  All pointers are device
+ * pointers; the call is asynchronous on the given CUDA stream.
+ *
+ * Input spectra are the n/2 + 1 unique bins of real time series (what an
+ * r2c FFT produces; bins n/2+1 .. n-1 of the reference's conjugate-filled
+ * spectra are not read), laid out as double complex [n_det][n_seg][ld]
+ * with ld >= n/2 + 1, 16-byte aligned.
+ */
+#ifndef SPHRADIOMETER_B200_BATCH_H
+#define SPHRADIOMETER_B200_BATCH_H
+
+#include <stddef.h>
+
+#include <sphradiometer/correlator.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Arithmetic of the contraction sum_k X(k) D_l(k):
+ *   SPHRAD_PREC_FP64   FP64 on CUDA cores
+ *   SPHRAD_PREC_FP32   FP32 on CUDA cores
+ *   SPHRAD_PREC_BF16X3 tcgen05 tensor cores, bf16 hi/lo split operands
+ *                      (hi*hi + hi*lo + lo*hi), FP32 accumulation; up to 3
+ *                      detectors.
+ * Cross spectra are formed in FP64 in every mode; normalisation, rotation
+ * and the z rotation run in FP32 (FP64 for SPHRAD_PREC_FP64). */
+enum {
+	SPHRAD_PREC_FP64 = 0,
+	SPHRAD_PREC_FP32 = 1,
+	SPHRAD_PREC_BF16X3 = 2
+};
+
+typedef struct sphrad_batch_plan sphrad_batch_plan;
+
+/* Device tables for every baseline of a network plan (all baselines must
+ * share the DFT length n; the output l_max is the largest baseline
+ * l_max).  NULL on failure. */
+sphrad_batch_plan *sphrad_batch_plan_new(const struct correlator_network_plan_fd *plan, int precision);
+void sphrad_batch_plan_free(sphrad_batch_plan *plan);
+unsigned sphrad_batch_plan_l_max(const sphrad_batch_plan *plan);
+int sphrad_batch_plan_bins(const sphrad_batch_plan *plan);
+
+/* Workspace for split-K partial sums.  It must be zero-filled before its
+ * first use; every call leaves it zero-filled again.  Calls that share a
+ * workspace must not overlap on the GPU. */
+size_t sphrad_batch_workspace_size(const sphrad_batch_plan *plan, int n_seg);
+
+/* fseries: device [n_det][n_seg][ld] double complex; gmst: device [n_seg]
+ * doubles or NULL; sky: device [n_seg][(l_max+1)^2] double complex.
+ * Returns 0, or -1 with sphrad_b200_last_error() set. */
+int sphrad_batch_integrate(sphrad_batch_plan *plan, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky, void *workspace,
+			   size_t workspace_bytes, void *cuda_stream);
+
+/* The same with host buffers: copies in, integrates, copies out and
+ * synchronises (library-owned device buffers).  Use pinned host memory for
+ * full copy bandwidth. */
+int sphrad_batch_integrate_host(sphrad_batch_plan *plan, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky);
+
+/* Split-K factor used for n_seg segments: the value stored by
+ * sphrad_batch_set_split / sphrad_batch_autotune, else a heuristic. */
+int sphrad_batch_get_split(const sphrad_batch_plan *plan, int n_seg);
+int sphrad_batch_set_split(sphrad_batch_plan *plan, int n_seg, int split);
+/* Times the candidate split factors on the given device data (timed with
+ * CUDA events on the stream) and stores the fastest for n_seg.  Returns
+ * the chosen split or -1. */
+int sphrad_batch_autotune(sphrad_batch_plan *plan, const void *fseries, int n_seg, long long ld, void *sky, void *workspace, size_t workspace_bytes,
+			  void *cuda_stream);
+/* Kernels launched by the last integrate call. */
+int sphrad_batch_kernels_per_call(const sphrad_batch_plan *plan);
+/* Profiling hook: when set (cudaEvent_t handles, or NULL to clear), every
+ * integrate call records ev_begin just before and ev_end just after the
+ * contraction kernel on the call's stream. */
+int sphrad_batch_set_timing_events(sphrad_batch_plan *plan, void *ev_begin, void *ev_end);
+/* 0 when no device-side wait has timed out, else the code of the wait that
+ * gave up (synchronises with the device). */
+int sphrad_batch_status(sphrad_batch_plan *plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,220 @@
+"""sphradiometer_b200: B200-native (sm_100a) full-sky cross-power path.
+
+The product is ``libsphradiometer_b200.so`` (``csrc/``), a drop-in for the
+reference's C ABI (``include/sphradiometer/*.h``) plus a batched,
+device-resident API (``include/sphradiometer_b200.h``).  This module is the
+Python host side over that C ABI, used by the tests and the benchmark; it
+holds no numerics of its own, and it raises if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _abi
+from ._abi import last_error, load, series_length, series_to_numpy, numpy_to_series, array_to_numpy, rotation_plan_flat
+
+PREC_FP64 = 0
+PREC_FP32 = 1
+PREC_BF16X3 = 2
+PRECISIONS = {"fp64": PREC_FP64, "fp32": PREC_FP32, "bf16x3": PREC_BF16X3}
+
+
+class SphradError(RuntimeError):
+    pass
+
+
+def _check(ptr, what: str):
+    if not ptr:
+        raise SphradError(f"{what} failed: {last_error()}")
+    return ptr
+
+
+class Network:
+    """A detector network with its frequency-domain correlation plan.
+
+    ``positions``: n_det x 3 phase centres in light-seconds.  ``l_max``:
+    power l_max of every baseline (the plan is built directly at
+    min(l_max, native) with ``correlator_network_plan_fd_new_l``); ``None``
+    builds at each baseline's native l_max as ``correlator_network_plan_fd_new``
+    does.
+    """
+
+    def __init__(self, positions, n: int, delta_t: float, l_max: int | None = None):
+        L = load()
+        self.positions = np.asarray(positions, np.float64)
+        self.n, self.delta_t = int(n), float(delta_t)
+        self._inst = _check(L.instrument_array_new(0), "instrument_array_new")
+        for p in self.positions:
+            _check(L.instrument_array_append(self._inst, _check(L.instrument_new(p[0], p[1], p[2], None), "instrument_new")),
+                   "instrument_array_append")
+        self._bl = _check(L.correlator_network_baselines_new(self._inst), "correlator_network_baselines_new")
+        if l_max is None:
+            self._plan = _check(L.correlator_network_plan_fd_new(self._bl, self.n, self.delta_t), "correlator_network_plan_fd_new")
+        else:
+            self._plan = _check(L.correlator_network_plan_fd_new_l(self._bl, self.n, self.delta_t, int(l_max)),
+                                "correlator_network_plan_fd_new_l")
+        self.n_det = len(self.positions)
+        self.n_baselines = self._bl.contents.n_baselines
+
+    @property
+    def plan(self):
+        return self._plan
+
+    def baseline(self, k: int):
+        return self._bl.contents.baselines[k].contents
+
+    def plan_fd(self, k: int):
+        return self._plan.contents.plans[k]
+
+    def baseline_l_max(self, k: int) -> int:
+        return self.plan_fd(k).contents.power_1d.contents.l_max
+
+    @property
+    def l_max(self) -> int:
+        return max(self.baseline_l_max(k) for k in range(self.n_baselines))
+
+    def delay_table(self, k: int) -> np.ndarray:
+        return array_to_numpy(self.plan_fd(k).contents.delay_product)
+
+    def rotation_flat(self, k: int) -> np.ndarray:
+        return rotation_plan_flat(self.plan_fd(k).contents.rotation_plan)
+
+    def set_l(self, l_max: int):
+        _check(load().correlator_network_plan_fd_set_l(self._plan, int(l_max)), "correlator_network_plan_fd_set_l")
+
+    def integrate(self, fseries, sky_l_max: int | None = None) -> np.ndarray:
+        """correlator_network_integrate_power_fd on one segment: fseries is
+        n_det x n (full conjugate-filled spectra).  Returns the sky a_lm."""
+        L = load()
+        F = [np.ascontiguousarray(f, np.complex128) for f in fseries]
+        ptrs = (C.c_void_p * len(F))(*[f.ctypes.data for f in F])
+        lm = self.l_max if sky_l_max is None else sky_l_max
+        sky = _check(L.sh_series_new_zero(lm, 0), "sh_series_new_zero")
+        try:
+            _check(L.correlator_network_integrate_power_fd(sky, ptrs, self._plan), "correlator_network_integrate_power_fd")
+            return series_to_numpy(sky)
+        finally:
+            L.sh_series_free(sky)
+
+    def integrate_baseline(self, k: int, a, b) -> np.ndarray:
+        L = load()
+        a = np.ascontiguousarray(a, np.complex128)
+        b = np.ascontiguousarray(b, np.complex128)
+        out = _check(L.correlator_baseline_integrate_power_fd(a.ctypes.data, b.ctypes.data, self.plan_fd(k)),
+                     "correlator_baseline_integrate_power_fd")
+        try:
+            return series_to_numpy(out)
+        finally:
+            L.sh_series_free(out)
+
+    def close(self):
+        L = load()
+        if getattr(self, "_plan", None):
+            L.correlator_network_plan_fd_free(self._plan)
+            self._plan = None
+        if getattr(self, "_bl", None):
+            L.correlator_network_baselines_free(self._bl)
+            self._bl = None
+        if getattr(self, "_inst", None):
+            L.instrument_array_free(self._inst)
+            self._inst = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class BatchPlan:
+    """Batched device-resident integrator over a Network (sphrad_batch_*).
+
+    ``integrate(F, gmst)``: F is a torch complex128 CUDA tensor
+    [n_det][n_seg][ld] holding the n/2+1 unique bins of each segment's
+    spectrum; gmst an optional float64 CUDA tensor [n_seg].  Returns a
+    complex128 CUDA tensor [n_seg][(l_max+1)^2].
+    """
+
+    def __init__(self, net: Network, precision: str | int = "bf16x3"):
+        self.precision = PRECISIONS.get(precision, precision) if isinstance(precision, str) else int(precision)
+        self.net = net
+        self._p = _check(load().sphrad_batch_plan_new(net.plan, self.precision), "sphrad_batch_plan_new")
+        self.l_max = load().sphrad_batch_plan_l_max(self._p)
+        self.bins = load().sphrad_batch_plan_bins(self._p)
+        self._ws = None
+        self._ws_bytes = 0
+
+    def workspace(self, n_seg: int):
+        import torch
+        need = load().sphrad_batch_workspace_size(self._p, n_seg)
+        if self._ws is None or self._ws_bytes < need:
+            self._ws = torch.zeros(max(need, 16), dtype=torch.uint8, device="cuda")
+            self._ws_bytes = need
+        return self._ws
+
+    def integrate(self, F, gmst=None, out=None, stream=None):
+        import torch
+        assert F.is_cuda and F.dtype == torch.complex128 and F.dim() == 3 and F.stride(2) == 1
+        n_det, n_seg, ld = F.shape
+        assert F.stride(1) == ld and F.stride(0) == n_seg * ld, "spectra must be contiguous [n_det][n_seg][ld]"
+        nq = (self.l_max + 1) ** 2
+        if out is None:
+            out = torch.empty((n_seg, nq), dtype=torch.complex128, device=F.device)
+        ws = self.workspace(n_seg)
+        st = stream if stream is not None else torch.cuda.current_stream()
+        rc = load().sphrad_batch_integrate(self._p, F.data_ptr(), n_seg, ld, gmst.data_ptr() if gmst is not None else None,
+                                           out.data_ptr(), ws.data_ptr(), self._ws_bytes, st.cuda_stream)
+        if rc:
+            raise SphradError("sphrad_batch_integrate: " + last_error())
+        return out
+
+    def integrate_host(self, F_host: np.ndarray, gmst_host: np.ndarray | None = None, out: np.ndarray | None = None):
+        n_det, n_seg, ld = F_host.shape
+        assert F_host.flags.c_contiguous and F_host.dtype == np.complex128
+        nq = (self.l_max + 1) ** 2
+        if out is None:
+            out = np.empty((n_seg, nq), np.complex128)
+        g = None
+        if gmst_host is not None:
+            gmst_host = np.ascontiguousarray(gmst_host, np.float64)
+            g = gmst_host.ctypes.data
+        rc = load().sphrad_batch_integrate_host(self._p, F_host.ctypes.data, n_seg, ld, g, out.ctypes.data)
+        if rc:
+            raise SphradError("sphrad_batch_integrate_host: " + last_error())
+        return out
+
+    def autotune(self, F):
+        import torch
+        n_det, n_seg, ld = F.shape
+        ws = self.workspace(n_seg)
+        out = torch.empty((n_seg, (self.l_max + 1) ** 2), dtype=torch.complex128, device=F.device)
+        k = load().sphrad_batch_autotune(self._p, F.data_ptr(), n_seg, ld, out.data_ptr(), ws.data_ptr(), self._ws_bytes,
+                                         torch.cuda.current_stream().cuda_stream)
+        if k < 0:
+            raise SphradError("sphrad_batch_autotune: " + last_error())
+        return k
+
+    def split(self, n_seg: int) -> int:
+        return load().sphrad_batch_get_split(self._p, n_seg)
+
+    def set_split(self, n_seg: int, split: int):
+        load().sphrad_batch_set_split(self._p, n_seg, split)
+
+    def kernels_per_call(self) -> int:
+        return load().sphrad_batch_kernels_per_call(self._p)
+
+    def status(self) -> int:
+        return load().sphrad_batch_status(self._p)
+
+    def close(self):
+        if getattr(self, "_p", None):
+            load().sphrad_batch_plan_free(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

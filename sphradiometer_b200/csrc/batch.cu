@@ -1,0 +1,1079 @@
+// batch.cu -- batched, device-resident frequency-domain cross-power
+// integration for many segments of one detector network.
+//
+// Per segment s and baseline b = (i, j) the reference computes
+// (correlator.c:681-711, 993-1010)
+//     X_b[k]   = F_j[k] conj(F_i[k])                    (cross spectrum)
+//     P_b[l]   = (1/n) sum_k X_b[k] D_b[k][l]           (sh_series_array_dotc)
+//     sky[lm'] += (1/B) D_b^l_{0m'} P_b[l]              (polar rotation)
+// and callers then rotate the sky about z by the segment's GMST
+// (sh_series_rotate_z).  For spectra of real series X[n-k] = conj(X[k]) and
+// D[n-k] = conj(D[k]), so P_b[l] = sum_{k<=n/2} w_k Re(X_b[k] D_b[k][l]) with
+// w_0 = w_{n/2} = 1 and w_k = 2 otherwise: a real GEMM over the n/2 + 1
+// unique bins, M = segments, K = 2 (n/2 + 1) (re, im interleaved), N = l.
+//
+// Kernels:
+//   k_tc_contract   tcgen05 GEMM with bf16 hi/lo split operands (three
+//                   MMAs: hi*hi + hi*lo + lo*hi, FP32 accumulation in TMEM).
+//                   Raw FP64 spectra arrive by TMA (3-D box: 8 bins x 128
+//                   segments x all detectors, 128B swizzle); converter
+//                   warps form X_b for every baseline in registers and write
+//                   the split operands straight into the UMMA layout; the
+//                   delay-table operand is pre-laid-out in HBM and fetched
+//                   by bulk copy.  Split-K partial sums go to an FP32
+//                   workspace by vector atomics.
+//   k_cc_contract   the same contraction on CUDA cores in FP32 or FP64.
+//   k_epilogue      1/n normalisation, polar rotation of every baseline,
+//                   1/B network sum and the per-segment z rotation, fused;
+//                   writes FP64 complex a_lm and re-zeroes the workspace.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cudaTypedefs.h>
+
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "runtime.h"
+
+namespace sphrad {
+
+#define CKB(call)                                                                \
+	do {                                                                     \
+		cudaError_t e_ = (call);                                         \
+		if(e_ != cudaSuccess) {                                          \
+			set_error("%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+			return -1;                                               \
+		}                                                                \
+	} while(0)
+
+namespace {
+constexpr int TM = 128;                  // segments per tile = MMA M
+constexpr int KB = 8;                    // bins per pipeline stage
+constexpr int KE = 16;                   // real K per stage = MMA K (bf16)
+constexpr int NF = 3;                    // depth of the spectrum ring
+constexpr int NAB = 2;                   // depth of the operand ring
+constexpr int TC_THREADS = 192;          // 6 warps: TMA, MMA, 4 converter/epilogue
+constexpr int TC_MAXB = 8;
+constexpr int TC_MAXDET = 3;
+constexpr int A_TILE = TM * KE * 2;      // bytes of one bf16 A tile (4096)
+constexpr int CC_TS = 16;                // segments per CUDA-core block
+constexpr int CC_KC = 16;                // bins per CUDA-core stage
+constexpr unsigned long long kWaitCycles = 4000000000ull;  // ~2 s bound on every wait
+}  // namespace
+
+// ------------------------------------------------------------------------
+// PTX wrappers (sm_100a)
+// ------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t) __cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_tx(uint32_t bar, uint32_t bytes)
+{
+	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity)
+{
+	uint32_t ok;
+	asm volatile(
+		"{\n\t.reg .pred P;\n\t"
+		"mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+		"selp.u32 %0, 1, 0, P;\n\t}"
+		: "=r"(ok)
+		: "r"(bar), "r"(parity)
+		: "memory");
+	return ok != 0;
+}
+
+// bounded wait: false on timeout (sets the abort flag and the error word)
+// or when another role has aborted
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag, unsigned *err, unsigned code)
+{
+	const unsigned long long t0 = clock64();
+	while(true) {
+		if(mbar_try(bar, parity))
+			return true;
+		if(*abort_flag)
+			return false;
+		if(clock64() - t0 > kWaitCycles) {
+			*abort_flag = 1;
+			atomicExch(err, code);
+			return false;
+		}
+	}
+}
+
+// bounded wait that ignores the abort flag (draining copies in flight)
+__device__ __forceinline__ void mbar_drain(uint32_t bar, uint32_t parity)
+{
+	const unsigned long long t0 = clock64();
+	while(!mbar_try(bar, parity) && clock64() - t0 < kWaitCycles) {
+	}
+}
+
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int x, int y, int z)
+{
+	asm volatile(
+		"cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
+		"l"((uint64_t) map), "r"(bar), "r"(x), "r"(y), "r"(z)
+		: "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
+		     : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// UMMA shared-memory descriptor, K-major, no swizzle: core matrices of
+// 8 rows x 16 bytes; LBO = byte step between core matrices along K, SBO =
+// byte step between 8-row groups; version field 1 (sm100).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
+{
+	uint64_t d = 0;
+	d |= (uint64_t) ((saddr >> 4) & 0x3FFF);
+	d |= (uint64_t) ((lbo >> 4) & 0x3FFF) << 16;
+	d |= (uint64_t) ((sbo >> 4) & 0x3FFF) << 32;
+	d |= (uint64_t) 1 << 46;
+	return d;
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate)
+{
+	asm volatile(
+		"{\n\t.reg .pred p;\n\t"
+		"setp.ne.b32 p, %4, 0;\n\t"
+		"tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
+		"l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar)
+{
+	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t *v)
+{
+	asm volatile(
+		"tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+		: "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]),
+		  "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+		: "r"(taddr));
+	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo_elem, float hi_elem)
+{
+	const __nv_bfloat16 a = __float2bfloat16_rn(lo_elem);
+	const __nv_bfloat16 b = __float2bfloat16_rn(hi_elem);
+	return (uint32_t) __bfloat16_as_ushort(a) | ((uint32_t) __bfloat16_as_ushort(b) << 16);
+}
+
+// ------------------------------------------------------------------------
+// tcgen05 contraction
+// ------------------------------------------------------------------------
+struct TcArgs {
+	int S, n_det, B, Kst, ks, npad, tmem_cols, accstride;
+	int bi[TC_MAXB], bj[TC_MAXB];
+	const uint8_t *bops;   // [Kst][B][2][npad * KE bf16], UMMA layout
+	float *acc;            // [S][B][accstride]
+	unsigned *err;
+};
+
+__global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_constant__ CUtensorMap tmF, const __grid_constant__ TcArgs a)
+{
+	extern __shared__ uint8_t smem_raw[];
+	uint8_t *smem = (uint8_t *) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
+	const int f_slab = TM * 128;
+	const int f_stage = a.n_det * f_slab;
+	const int btile = a.npad * KE * 2;
+	const int ab_bytes = a.B * 2 * btile;
+	uint8_t *sF = smem;
+	uint8_t *sA = sF + NF * f_stage;
+	uint8_t *sB = sA + NAB * a.B * 2 * A_TILE;
+	uint64_t *bars = (uint64_t *) (sB + NAB * ab_bytes);
+	uint64_t *f_full = bars;
+	uint64_t *f_empty = bars + NF;
+	uint64_t *ab_full = bars + 2 * NF;
+	uint64_t *b_full = ab_full + NAB;
+	uint64_t *ab_empty = b_full + NAB;
+	uint64_t *acc_full = ab_empty + NAB;
+	uint32_t *tslot = (uint32_t *) (acc_full + 1);
+	volatile int *abort_flag = (volatile int *) (tslot + 1);
+
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const int tile = blockIdx.x / a.ks, split = blockIdx.x % a.ks;
+	const int k_begin = (int) ((long long) a.Kst * split / a.ks);
+	const int k_end = (int) ((long long) a.Kst * (split + 1) / a.ks);
+	const int nst = k_end - k_begin;
+
+	if(threadIdx.x == 0) {
+		for(int i = 0; i < NF; i++) {
+			mbar_init(smem_u32(&f_full[i]), 1);
+			mbar_init(smem_u32(&f_empty[i]), 4);
+		}
+		for(int i = 0; i < NAB; i++) {
+			mbar_init(smem_u32(&ab_full[i]), 4);
+			mbar_init(smem_u32(&b_full[i]), 1);
+			mbar_init(smem_u32(&ab_empty[i]), 1);
+		}
+		mbar_init(smem_u32(acc_full), 1);
+		*abort_flag = 0;
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	if(warp == 1) {
+		asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)), "r"(a.tmem_cols));
+		asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+	}
+	tc_fence_before();
+	__syncthreads();
+	tc_fence_after();
+	const uint32_t tmem = *tslot;
+
+	if(warp == 0) {
+		// ---------------- producer ----------------
+		if(lane == 0) {
+			int issued = 0;
+			for(int it = 0; it < nst; it++) {
+				const int st = k_begin + it;
+				const int fs = it % NF;
+				const uint32_t fph = (it / NF) & 1;
+				if(!mbar_wait(smem_u32(&f_empty[fs]), fph ^ 1, abort_flag, a.err, 1))
+					break;
+				mbar_arrive_tx(smem_u32(&f_full[fs]), f_stage);
+				tma_load_3d(smem_u32(sF + fs * f_stage), &tmF, smem_u32(&f_full[fs]), st * 2 * KB, tile * TM, 0);
+				const int as = it % NAB;
+				const uint32_t aph = (it / NAB) & 1;
+				if(!mbar_wait(smem_u32(&ab_empty[as]), aph ^ 1, abort_flag, a.err, 2)) {
+					issued = -(it + 1);  // F load of this stage is in flight, B load is not
+					break;
+				}
+				mbar_arrive_tx(smem_u32(&b_full[as]), ab_bytes);
+				bulk_g2s(smem_u32(sB + as * ab_bytes), a.bops + (size_t) st * ab_bytes, ab_bytes, smem_u32(&b_full[as]));
+				issued = it + 1;
+			}
+			// drain the copies that may still be in flight
+			const int nf = issued < 0 ? -issued : issued;
+			const int nb = issued < 0 ? -issued - 1 : issued;
+			for(int it = (nf > NF ? nf - NF : 0); it < nf; it++)
+				mbar_drain(smem_u32(&f_full[it % NF]), (it / NF) & 1);
+			for(int it = (nb > NAB ? nb - NAB : 0); it < nb; it++)
+				mbar_drain(smem_u32(&b_full[it % NAB]), (it / NAB) & 1);
+		}
+	} else if(warp == 1) {
+		// ---------------- MMA issuer ----------------
+		if(lane == 0) {
+			// kind::f16, D = F32, A = B = BF16, both K-major, N = npad, M = 128
+			const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (a.npad >> 3) << 17) | ((uint32_t) (TM >> 4) << 24);
+			for(int it = 0; it < nst; it++) {
+				const int as = it % NAB;
+				const uint32_t aph = (it / NAB) & 1;
+				if(!mbar_wait(smem_u32(&ab_full[as]), aph, abort_flag, a.err, 3))
+					break;
+				if(!mbar_wait(smem_u32(&b_full[as]), aph, abort_flag, a.err, 4))
+					break;
+				tc_fence_after();
+				for(int b = 0; b < a.B; b++) {
+					const uint32_t d = tmem + (uint32_t) (b * a.npad);
+					const uint32_t ahi = smem_u32(sA + ((as * a.B + b) * 2 + 0) * A_TILE);
+					const uint32_t alo = ahi + A_TILE;
+					const uint32_t bhi = smem_u32(sB + as * ab_bytes + (b * 2 + 0) * btile);
+					const uint32_t blo = bhi + btile;
+					umma_bf16(d, umma_desc(ahi, 128, 256), umma_desc(bhi, 128, 256), idesc, it > 0 ? 1u : 0u);
+					umma_bf16(d, umma_desc(ahi, 128, 256), umma_desc(blo, 128, 256), idesc, 1u);
+					umma_bf16(d, umma_desc(alo, 128, 256), umma_desc(bhi, 128, 256), idesc, 1u);
+				}
+				umma_commit(smem_u32(&ab_empty[as]));
+			}
+			umma_commit(smem_u32(acc_full));
+		}
+	} else {
+		// ---------------- converters, then epilogue ----------------
+		const int r = threadIdx.x - 64;  // tile row 0..127
+		const int roff = (r >> 3) * 256 + (r & 7) * 16;
+		for(int it = 0; it < nst; it++) {
+			const int fs = it % NF;
+			const uint32_t fph = (it / NF) & 1;
+			const bool okf = mbar_wait(smem_u32(&f_full[fs]), fph, abort_flag, a.err, 5);
+			if(!__all_sync(0xffffffffu, okf))
+				break;
+			double2 f0[KB], f1[KB], f2[KB];
+			{
+				const uint8_t *base = sF + fs * f_stage + r * 128;
+#pragma unroll
+				for(int c = 0; c < KB; c++) {
+					f0[c] = *(const double2 *) (base + ((c ^ (r & 7)) << 4));
+					f1[c] = a.n_det > 1 ? *(const double2 *) (base + f_slab + ((c ^ (r & 7)) << 4)) : make_double2(0, 0);
+					f2[c] = a.n_det > 2 ? *(const double2 *) (base + 2 * f_slab + ((c ^ (r & 7)) << 4)) : make_double2(0, 0);
+				}
+			}
+			__syncwarp();
+			if(lane == 0)
+				mbar_arrive(smem_u32(&f_empty[fs]));
+			const int as = it % NAB;
+			const uint32_t aph = (it / NAB) & 1;
+			const bool oke = mbar_wait(smem_u32(&ab_empty[as]), aph ^ 1, abort_flag, a.err, 6);
+			if(!__all_sync(0xffffffffu, oke))
+				break;
+			for(int b = 0; b < a.B; b++) {
+				uint32_t hi[KB], lo[KB];
+#pragma unroll
+				for(int c = 0; c < KB; c++) {
+					const int da = a.bi[b], db = a.bj[b];
+					const double2 fa = da == 0 ? f0[c] : (da == 1 ? f1[c] : f2[c]);
+					const double2 fb = db == 0 ? f0[c] : (db == 1 ? f1[c] : f2[c]);
+					// X = fb * conj(fa)
+					const float xr = (float) (fb.x * fa.x + fb.y * fa.y);
+					const float xi = (float) (fb.y * fa.x - fb.x * fa.y);
+					const float hr = __bfloat162float(__float2bfloat16_rn(xr));
+					const float hm = __bfloat162float(__float2bfloat16_rn(xi));
+					hi[c] = pack_bf16(xr, xi);
+					lo[c] = pack_bf16(xr - hr, xi - hm);
+				}
+				uint8_t *th = sA + ((as * a.B + b) * 2 + 0) * A_TILE + roff;
+				uint8_t *tl = th + A_TILE;
+				*(uint4 *) (th) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+				*(uint4 *) (th + 128) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
+				*(uint4 *) (tl) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+				*(uint4 *) (tl + 128) = make_uint4(lo[4], lo[5], lo[6], lo[7]);
+			}
+			fence_proxy_async();
+			__syncwarp();
+			if(lane == 0)
+				mbar_arrive(smem_u32(&ab_full[as]));
+		}
+		// epilogue: TMEM -> registers -> FP32 atomics into the workspace
+		const bool got = mbar_wait(smem_u32(acc_full), 0, abort_flag, a.err, 7);
+		tc_fence_after();
+		const bool ok = __all_sync(0xffffffffu, got && !*abort_flag && nst > 0);
+		if(ok) {
+			const int q = warp & 3;
+			const int row = q * 32 + lane;
+			const int s = tile * TM + row;
+			for(int b = 0; b < a.B; b++) {
+				for(int c0 = 0; c0 < a.accstride; c0 += 16) {
+					uint32_t v[16];
+					tmem_ld16(tmem + ((uint32_t) (q * 32) << 16) + (uint32_t) (b * a.npad + c0), v);
+					if(s < a.S) {
+						float *dst = a.acc + ((size_t) s * a.B + b) * a.accstride + c0;
+#pragma unroll
+						for(int j = 0; j < 4; j++)
+							if(c0 + 4 * j < a.accstride)
+								atomicAdd((float4 *) (dst + 4 * j),
+									  make_float4(__uint_as_float(v[4 * j]), __uint_as_float(v[4 * j + 1]), __uint_as_float(v[4 * j + 2]),
+										      __uint_as_float(v[4 * j + 3])));
+					}
+				}
+			}
+		}
+	}
+	tc_fence_before();
+	__syncthreads();
+	if(warp == 1) {
+		tc_fence_after();
+		asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(a.tmem_cols));
+	}
+}
+
+// operand table for the tcgen05 path: stage st, baseline b, part p (hi/lo),
+// row n (l), k element kk (bin st*KB + kk/2, re/im = kk%2) in the no-swizzle
+// K-major core-matrix layout (LBO 128 B, SBO 256 B)
+__global__ void k_build_bops(int Kst, int B, int npad, int Lp1, int Ku, const double2 *Dt, uint8_t *bops)
+{
+	const long long total = (long long) Kst * B * npad * KE;
+	const int btile = npad * KE * 2;
+	for(long long idx = blockIdx.x * (long long) blockDim.x + threadIdx.x; idx < total; idx += (long long) gridDim.x * blockDim.x) {
+		const int kk = idx % KE;
+		const int n = (idx / KE) % npad;
+		const int b = (idx / ((long long) KE * npad)) % B;
+		const int st = idx / ((long long) KE * npad * B);
+		const int bin = st * KB + kk / 2;
+		double v = 0.0;
+		if(n < Lp1 && bin < Ku) {
+			const double2 d = Dt[((size_t) bin * B + b) * Lp1 + n];
+			v = (kk & 1) ? -d.y : d.x;
+		}
+		const __nv_bfloat16 h = __float2bfloat16_rn((float) v);
+		const __nv_bfloat16 l = __float2bfloat16_rn((float) (v - (double) __bfloat162float(h)));
+		const size_t off = (size_t) (n >> 3) * 256 + (kk >> 3) * 128 + (n & 7) * 16 + (kk & 7) * 2;
+		uint8_t *t = bops + ((size_t) st * B + b) * 2 * btile;
+		*(__nv_bfloat16 *) (t + off) = h;
+		*(__nv_bfloat16 *) (t + btile + off) = l;
+	}
+}
+
+// ------------------------------------------------------------------------
+// CUDA-core contraction (FP32 or FP64)
+// ------------------------------------------------------------------------
+template <class T> struct V2;
+template <> struct V2<float> { using type = float2; };
+template <> struct V2<double> { using type = double2; };
+
+struct CcArgs {
+	int S, n_det, B, Lp1, Ku, ks, accstride;
+	long long ld;
+	int bi[kMaxBaselines], bj[kMaxBaselines];
+	const double2 *F;    // [n_det][S][ld]
+	const void *Dt;      // [Ku][B][Lp1] complex T, hermitian weights folded in
+	void *acc;           // [S][B][accstride] T
+};
+
+template <class T>
+__global__ void k_cc_contract(const __grid_constant__ CcArgs c)
+{
+	using T2 = typename V2<T>::type;
+	extern __shared__ __align__(16) uint8_t cc_smem[];
+	double2 *sF = (double2 *) cc_smem;                                    // [n_det][TS][KC]
+	T2 *sX = (T2 *) (sF + (size_t) c.n_det * CC_TS * CC_KC);               // [B][TS][KC]
+	T2 *sD = sX + (size_t) c.B * CC_TS * CC_KC;                            // [KC][B*Lp1]
+	const int np = c.B * c.Lp1;
+	const int p = threadIdx.x;
+	const bool active = p < np;
+	const int b = active ? p / c.Lp1 : 0;
+	const int s0 = blockIdx.x * CC_TS;
+	const int nch = (c.Ku + CC_KC - 1) / CC_KC;
+	const int ch0 = (int) ((long long) nch * blockIdx.y / c.ks);
+	const int ch1 = (int) ((long long) nch * (blockIdx.y + 1) / c.ks);
+	const T2 *Dt = (const T2 *) c.Dt;
+	T acc[CC_TS];
+#pragma unroll
+	for(int s = 0; s < CC_TS; s++)
+		acc[s] = 0;
+	for(int ch = ch0; ch < ch1; ch++) {
+		const int k0 = ch * CC_KC;
+		for(int idx = threadIdx.x; idx < c.n_det * CC_TS * CC_KC; idx += blockDim.x) {
+			const int k = idx % CC_KC, s = (idx / CC_KC) % CC_TS, d = idx / (CC_KC * CC_TS);
+			double2 v = make_double2(0, 0);
+			if(s0 + s < c.S && k0 + k < c.Ku)
+				v = c.F[((size_t) d * c.S + s0 + s) * c.ld + k0 + k];
+			sF[idx] = v;
+		}
+		for(int idx = threadIdx.x; idx < CC_KC * np; idx += blockDim.x) {
+			const int k = idx / np;
+			T2 v;
+			v.x = 0;
+			v.y = 0;
+			if(k0 + k < c.Ku)
+				v = Dt[(size_t) (k0 + k) * np + idx % np];
+			sD[idx] = v;
+		}
+		__syncthreads();
+		for(int idx = threadIdx.x; idx < c.B * CC_TS * CC_KC; idx += blockDim.x) {
+			const int k = idx % CC_KC, s = (idx / CC_KC) % CC_TS, bb = idx / (CC_KC * CC_TS);
+			const double2 fa = sF[((size_t) c.bi[bb] * CC_TS + s) * CC_KC + k];
+			const double2 fb = sF[((size_t) c.bj[bb] * CC_TS + s) * CC_KC + k];
+			T2 x;
+			x.x = (T) (fb.x * fa.x + fb.y * fa.y);
+			x.y = (T) (fb.y * fa.x - fb.x * fa.y);
+			sX[idx] = x;
+		}
+		__syncthreads();
+		if(active) {
+			for(int k = 0; k < CC_KC; k++) {
+				const T2 d = sD[k * np + p];
+#pragma unroll
+				for(int s = 0; s < CC_TS; s++) {
+					const T2 x = sX[((size_t) b * CC_TS + s) * CC_KC + k];
+					acc[s] += x.x * d.x - x.y * d.y;
+				}
+			}
+		}
+		__syncthreads();
+	}
+	if(active) {
+		const int l = p % c.Lp1;
+		T *out = (T *) c.acc;
+		for(int s = 0; s < CC_TS; s++)
+			if(s0 + s < c.S)
+				atomicAdd(&out[((size_t) (s0 + s) * c.B + b) * c.accstride + l], acc[s]);
+	}
+}
+
+// ------------------------------------------------------------------------
+// epilogue: normalisation, rotation, network sum, z rotation
+// ------------------------------------------------------------------------
+struct EpArgs {
+	int S, B, Lp1, L, accstride, nq;
+	const short *lq;        // l of output index q
+	const short *mq;        // m of output index q
+	const void *W;          // [B][nq] complex T: weight / n * D_b^l_{0 m}
+	const double *gmst;     // [S] or NULL
+	double2 *sky;           // [S][nq]
+};
+
+template <class T>
+__global__ void k_epilogue(const __grid_constant__ EpArgs e, T *acc)
+{
+	using T2 = typename V2<T>::type;
+	extern __shared__ __align__(16) uint8_t ep_smem[];
+	double2 *sPh = (double2 *) ep_smem;                             // [2L+1]
+	T *sP = (T *) (sPh + 2 * e.L + 1);                              // [B][Lp1]
+	const int s = blockIdx.x;
+	T *row = acc + (size_t) s * e.B * e.accstride;
+	for(int i = threadIdx.x; i < e.B * e.Lp1; i += blockDim.x)
+		sP[i] = row[(i / e.Lp1) * e.accstride + i % e.Lp1];
+	for(int m = (int) threadIdx.x - e.L; m <= e.L; m += blockDim.x) {
+		double sn = 0.0, cs = 1.0;
+		if(e.gmst)
+			sincos(-m * e.gmst[s], &sn, &cs);
+		sPh[m + e.L] = make_double2(cs, sn);
+	}
+	__syncthreads();
+	// leave the workspace zeroed for the next launch
+	for(int i = threadIdx.x; i < e.B * e.accstride; i += blockDim.x)
+		row[i] = 0;
+	const T2 *W = (const T2 *) e.W;
+	for(int q = threadIdx.x; q < e.nq; q += blockDim.x) {
+		const int l = e.lq[q];
+		T re = 0, im = 0;
+		for(int b = 0; b < e.B; b++) {
+			const T2 w = W[(size_t) b * e.nq + q];
+			const T pv = sP[b * e.Lp1 + l];
+			re += w.x * pv;
+			im += w.y * pv;
+		}
+		const double2 ph = sPh[e.mq[q] + e.L];
+		e.sky[(size_t) s * e.nq + q] = make_double2((double) re * ph.x - (double) im * ph.y, (double) re * ph.y + (double) im * ph.x);
+	}
+}
+
+// ------------------------------------------------------------------------
+// plan
+// ------------------------------------------------------------------------
+struct BatchPlan {
+	int precision = 0;
+	int n_det = 0, B = 0, n = 0, Ku = 0, Lp1 = 0, nq = 0, accstride = 0;
+	unsigned L = 0;
+	int bi[kMaxBaselines], bj[kMaxBaselines];
+	// device tables
+	void *Dt = nullptr;        // [Ku][B][Lp1] complex (T of the CUDA-core path)
+	uint8_t *bops = nullptr;   // tcgen05 operand table
+	int Kst = 0, npad = 0, tmem_cols = 0;
+	void *W = nullptr;         // [B][nq] complex T
+	short *lq = nullptr, *mq = nullptr;
+	unsigned *err = nullptr;
+	// tuned split per S
+	std::map<int, int> split;
+	// optional CUDA events recorded around the contraction kernel
+	cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+	int last_kernels = 0;
+	// host-buffer path scratch
+	void *hF = nullptr, *hG = nullptr, *hSky = nullptr, *hWs = nullptr;
+	size_t hF_bytes = 0, hG_bytes = 0, hSky_bytes = 0, hWs_bytes = 0;
+	// tensor map cache
+	const void *tm_ptr = nullptr;
+	int tm_S = -1;
+	long long tm_ld = -1;
+	CUtensorMap tm;
+};
+
+static PFN_cuTensorMapEncodeTiled_v12000 get_encode()
+{
+	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+	static std::once_flag once;
+	std::call_once(once, [] {
+		void *p = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+			fn = (PFN_cuTensorMapEncodeTiled_v12000) p;
+	});
+	return fn;
+}
+
+static size_t tc_smem_bytes(const BatchPlan &P)
+{
+	const size_t f = (size_t) NF * P.n_det * TM * 128;
+	const size_t aa = (size_t) NAB * P.B * 2 * A_TILE;
+	const size_t bb = (size_t) NAB * P.B * 2 * P.npad * KE * 2;
+	const size_t bars = 8 * (2 * NF + 3 * NAB + 1) + 16;
+	// 1 KB for aligning the base, 4 KB of slack past the last tile
+	return 1024 + f + aa + bb + bars + 4096;
+}
+
+void batch_plan_destroy(void *pp)
+{
+	BatchPlan *P = (BatchPlan *) pp;
+	if(!P)
+		return;
+	dfree(P->Dt);
+	dfree(P->bops);
+	dfree(P->W);
+	dfree(P->lq);
+	dfree(P->mq);
+	dfree(P->err);
+	dfree(P->hF);
+	dfree(P->hG);
+	dfree(P->hSky);
+	dfree(P->hWs);
+	delete P;
+}
+
+unsigned batch_plan_l_max(const void *p) { return ((const BatchPlan *) p)->L; }
+int batch_plan_bins(const void *p) { return ((const BatchPlan *) p)->Ku; }
+int batch_last_kernel_count(const void *p) { return ((const BatchPlan *) p)->last_kernels; }
+
+static size_t lmoff(unsigned L, int l, int m)
+{
+	const long long LL = (long long) L + 1;
+	const long long x = (long long) m * (m - 1);
+	const long long mo = (m >= 0) ? LL * m - x / 2 : LL * (LL + m) + x / 2;
+	return (size_t) (mo + l - (m < 0 ? -m : m));
+}
+
+void *batch_plan_create(const BatchPlanDesc &d, int precision)
+{
+	if(ensure_device())
+		return nullptr;
+	if(d.n_baselines <= 0 || d.n_baselines > kMaxBaselines || d.n_det <= 1 || d.n <= 1) {
+		set_error("batch plan: bad network (detectors %d, baselines %d, n %d)", d.n_det, d.n_baselines, d.n);
+		return nullptr;
+	}
+	if(!d.hermitian) {
+		set_error("batch plan: only spectra of real series (n/2+1 unique bins) are supported");
+		return nullptr;
+	}
+	if(precision == kPrecBF16x3) {
+		int dev = 0, major = 0;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+		if(major != 10) {
+			set_error("batch plan: the bf16x3 tcgen05 path needs an sm_100 device");
+			return nullptr;
+		}
+		if(d.n_det > TC_MAXDET || d.n_baselines > TC_MAXB) {
+			set_error("batch plan: the bf16x3 path supports up to %d detectors", TC_MAXDET);
+			return nullptr;
+		}
+		if(!get_encode()) {
+			set_error("batch plan: cuTensorMapEncodeTiled unavailable");
+			return nullptr;
+		}
+	}
+	BatchPlan *P = new BatchPlan();
+	P->precision = precision;
+	P->n_det = d.n_det;
+	P->B = d.n_baselines;
+	P->n = d.n;
+	P->Ku = d.n / 2 + 1;
+	unsigned L = 0;
+	for(int b = 0; b < P->B; b++) {
+		P->bi[b] = d.bi[b];
+		P->bj[b] = d.bj[b];
+		L = d.lb[b] > L ? d.lb[b] : L;
+		if(d.bi[b] < 0 || d.bi[b] >= d.n_det || d.bj[b] < 0 || d.bj[b] >= d.n_det) {
+			set_error("batch plan: baseline %d names a missing detector", b);
+			batch_plan_destroy(P);
+			return nullptr;
+		}
+	}
+	P->L = L;
+	P->Lp1 = L + 1;
+	P->nq = (L + 1) * (L + 1);
+	P->accstride = (P->Lp1 + 3) & ~3;
+	const bool dbl = precision == kPrecFP64;
+	const int Ku = P->Ku, B = P->B, Lp1 = P->Lp1;
+	// hermitian-weighted delay table [Ku][B][Lp1]
+	std::vector<double> Dt((size_t) Ku * B * Lp1 * 2, 0.0);
+	for(int k = 0; k < Ku; k++) {
+		const double wk = (k == 0 || 2 * k == d.n) ? 1.0 : 2.0;
+		for(int b = 0; b < B; b++) {
+			const int lp = d.lb[b] + 1;
+			const double *row = d.D[b] + 2 * (size_t) k * lp;
+			for(int l = 0; l < lp; l++) {
+				Dt[2 * (((size_t) k * B + b) * Lp1 + l)] = wk * row[2 * l];
+				Dt[2 * (((size_t) k * B + b) * Lp1 + l) + 1] = wk * row[2 * l + 1];
+			}
+		}
+	}
+	// rotation weights W[b][q] = weight / n * D_b^l_{0 m}, q = (l, m)
+	std::vector<double> W((size_t) B * P->nq * 2, 0.0);
+	std::vector<short> lq(P->nq), mq(P->nq);
+	for(int m = -(int) L; m <= (int) L; m++)
+		for(int l = m < 0 ? -m : m; l <= (int) L; l++) {
+			const size_t q = lmoff(L, l, m);
+			lq[q] = (short) l;
+			mq[q] = (short) m;
+			for(int b = 0; b < B; b++) {
+				if(l > (int) d.lb[b])
+					continue;
+				double re = 1.0, im = 0.0;
+				if(l > 0) {
+					const size_t e = rot_offset(l) + (size_t) (2 * l + 1) * (m + l) + (0 + l);
+					re = d.rot[b][2 * e];
+					im = d.rot[b][2 * e + 1];
+				} else if(m != 0)
+					continue;
+				const double s = d.weight / d.n;
+				W[2 * ((size_t) b * P->nq + q)] = s * re;
+				W[2 * ((size_t) b * P->nq + q) + 1] = s * im;
+			}
+		}
+	bool fail = false;
+	auto up = [&](void **dst, const void *src, size_t bytes) {
+		*dst = dmalloc(bytes);
+		if(!*dst || h2d(*dst, src, bytes))
+			fail = true;
+	};
+	if(dbl) {
+		up(&P->Dt, Dt.data(), Dt.size() * sizeof(double));
+		up(&P->W, W.data(), W.size() * sizeof(double));
+	} else {
+		std::vector<float> Dtf(Dt.begin(), Dt.end()), Wf(W.begin(), W.end());
+		up(&P->Dt, Dtf.data(), Dtf.size() * sizeof(float));
+		up(&P->W, Wf.data(), Wf.size() * sizeof(float));
+		if(!fail)
+			fail = stream_sync() != 0;
+	}
+	up((void **) &P->lq, lq.data(), lq.size() * sizeof(short));
+	up((void **) &P->mq, mq.data(), mq.size() * sizeof(short));
+	P->err = (unsigned *) dmalloc(sizeof(unsigned));
+	if(!P->err || dmemset(P->err, 0, sizeof(unsigned)))
+		fail = true;
+	if(!fail && precision == kPrecBF16x3) {
+		P->Kst = (Ku + KB - 1) / KB;
+		P->npad = (Lp1 + 15) & ~15;
+		int cols = 32;
+		while(cols < B * P->npad)
+			cols <<= 1;
+		P->tmem_cols = cols;
+		if(P->npad > 256 || cols > 512) {
+			set_error("batch plan: l_max %u too large for the bf16x3 path", L);
+			fail = true;
+		} else {
+			// a double-precision copy of Dt for the operand builder
+			void *Dt64 = nullptr;
+			up(&Dt64, Dt.data(), Dt.size() * sizeof(double));
+			const size_t bbytes = (size_t) P->Kst * B * 2 * P->npad * KE * 2;
+			P->bops = (uint8_t *) dmalloc(bbytes);
+			if(!fail && P->bops) {
+				k_build_bops<<<512, 256, 0, (cudaStream_t) lib_stream()>>>(P->Kst, B, P->npad, Lp1, Ku, (const double2 *) Dt64, P->bops);
+				if(cudaGetLastError() != cudaSuccess)
+					fail = true;
+			} else
+				fail = true;
+			if(stream_sync())
+				fail = true;
+			dfree(Dt64);
+			if(!fail && tc_smem_bytes(*P) > 227 * 1024) {
+				set_error("batch plan: shared-memory budget exceeded");
+				fail = true;
+			}
+			if(!fail && cudaFuncSetAttribute(k_tc_contract, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess) {
+				set_error("batch plan: cannot reserve %zu bytes of shared memory", tc_smem_bytes(*P));
+				fail = true;
+			}
+		}
+	}
+	if(!fail && stream_sync())
+		fail = true;
+	if(fail) {
+		batch_plan_destroy(P);
+		return nullptr;
+	}
+	return P;
+}
+
+size_t batch_workspace_bytes(const void *pp, int S)
+{
+	const BatchPlan *P = (const BatchPlan *) pp;
+	const size_t el = P->precision == kPrecFP64 ? sizeof(double) : sizeof(float);
+	return (size_t) (S > 0 ? S : 0) * P->B * P->accstride * el;
+}
+
+int batch_pick_split(const void *pp, int S)
+{
+	const BatchPlan *P = (const BatchPlan *) pp;
+	auto it = P->split.find(S);
+	if(it != P->split.end())
+		return it->second;
+	int sms = 148;
+	int dev = 0;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	if(P->precision == kPrecBF16x3) {
+		const int tiles = (S + TM - 1) / TM;
+		int ks = sms / tiles;
+		if(ks < 1)
+			ks = 1;
+		if(ks > P->Kst / 4)
+			ks = P->Kst / 4 > 0 ? P->Kst / 4 : 1;
+		return ks;
+	}
+	const int blocks = (S + CC_TS - 1) / CC_TS;
+	const int nch = (P->Ku + CC_KC - 1) / CC_KC;
+	int ks = (2 * sms + blocks - 1) / blocks;
+	if(ks < 1)
+		ks = 1;
+	if(ks > nch)
+		ks = nch;
+	return ks;
+}
+
+int batch_set_split(void *pp, int S, int ks)
+{
+	BatchPlan *P = (BatchPlan *) pp;
+	if(ks <= 0)
+		P->split.erase(S);
+	else
+		P->split[S] = ks;
+	return 0;
+}
+
+int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream_v, int split)
+{
+	BatchPlan *P = (BatchPlan *) pp;
+	cudaStream_t st = (cudaStream_t) stream_v;
+	if(S <= 0)
+		return 0;
+	if(ld < P->Ku) {
+		set_error("batch_run: row stride %lld below the %d bins read", ld, P->Ku);
+		return -1;
+	}
+	if(ws_bytes < batch_workspace_bytes(P, S) || !ws) {
+		set_error("batch_run: workspace of %zu bytes needed", batch_workspace_bytes(P, S));
+		return -1;
+	}
+	const int ks = split > 0 ? split : batch_pick_split(P, S);
+	int launches = 0;
+	if(P->precision == kPrecBF16x3) {
+		if(((uintptr_t) F & 15) || ((ld * 16) & 15)) {
+			set_error("batch_run: spectra must be 16-byte aligned");
+			return -1;
+		}
+		if(ks > P->Kst) {
+			set_error("batch_run: split %d above %d stages", ks, P->Kst);
+			return -1;
+		}
+		if(P->tm_ptr != F || P->tm_S != S || P->tm_ld != ld) {
+			cuuint64_t gdim[3] = {(cuuint64_t) 2 * P->Ku, (cuuint64_t) S, (cuuint64_t) P->n_det};
+			cuuint64_t gstr[2] = {(cuuint64_t) ld * 16, (cuuint64_t) S * ld * 16};
+			cuuint32_t box[3] = {2 * KB, TM, (cuuint32_t) P->n_det};
+			cuuint32_t estr[3] = {1, 1, 1};
+			CUresult r = get_encode()(&P->tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void *>(F), gdim, gstr, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+						  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+			if(r != CUDA_SUCCESS) {
+				set_error("batch_run: cuTensorMapEncodeTiled failed (%d)", (int) r);
+				P->tm_ptr = nullptr;
+				return -1;
+			}
+			P->tm_ptr = F;
+			P->tm_S = S;
+			P->tm_ld = ld;
+		}
+		TcArgs a;
+		memset(&a, 0, sizeof(a));
+		a.S = S;
+		a.n_det = P->n_det;
+		a.B = P->B;
+		a.Kst = P->Kst;
+		a.ks = ks;
+		a.npad = P->npad;
+		a.tmem_cols = P->tmem_cols;
+		a.accstride = P->accstride;
+		for(int b = 0; b < P->B; b++) {
+			a.bi[b] = P->bi[b];
+			a.bj[b] = P->bj[b];
+		}
+		a.bops = P->bops;
+		a.acc = (float *) ws;
+		a.err = P->err;
+		const int tiles = (S + TM - 1) / TM;
+		if(P->ev_begin)
+			cudaEventRecord(P->ev_begin, st);
+		k_tc_contract<<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+		if(P->ev_end)
+			cudaEventRecord(P->ev_end, st);
+		launches++;
+	} else {
+		CcArgs c;
+		memset(&c, 0, sizeof(c));
+		c.S = S;
+		c.n_det = P->n_det;
+		c.B = P->B;
+		c.Lp1 = P->Lp1;
+		c.Ku = P->Ku;
+		c.ks = ks;
+		c.accstride = P->accstride;
+		c.ld = ld;
+		for(int b = 0; b < P->B; b++) {
+			c.bi[b] = P->bi[b];
+			c.bj[b] = P->bj[b];
+		}
+		c.F = (const double2 *) F;
+		c.Dt = P->Dt;
+		c.acc = ws;
+		const int np = P->B * P->Lp1;
+		const int threads = ((np + 31) / 32) * 32;
+		if(threads > 1024) {
+			set_error("batch_run: %d (baseline, l) pairs exceed one block", np);
+			return -1;
+		}
+		const size_t el2 = P->precision == kPrecFP64 ? sizeof(double2) : sizeof(float2);
+		const size_t smem = (size_t) P->n_det * CC_TS * CC_KC * sizeof(double2) + (size_t) P->B * CC_TS * CC_KC * el2 + (size_t) CC_KC * np * el2;
+		dim3 grid((S + CC_TS - 1) / CC_TS, ks);
+		if(P->ev_begin)
+			cudaEventRecord(P->ev_begin, st);
+		if(P->precision == kPrecFP64) {
+			if(smem > 48 * 1024)
+				cudaFuncSetAttribute(k_cc_contract<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+			k_cc_contract<double><<<grid, threads, smem, st>>>(c);
+		} else {
+			if(smem > 48 * 1024)
+				cudaFuncSetAttribute(k_cc_contract<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+			k_cc_contract<float><<<grid, threads, smem, st>>>(c);
+		}
+		if(P->ev_end)
+			cudaEventRecord(P->ev_end, st);
+		launches++;
+	}
+	EpArgs e;
+	e.S = S;
+	e.B = P->B;
+	e.Lp1 = P->Lp1;
+	e.L = P->L;
+	e.accstride = P->accstride;
+	e.nq = P->nq;
+	e.lq = P->lq;
+	e.mq = P->mq;
+	e.W = P->W;
+	e.gmst = gmst;
+	e.sky = (double2 *) sky;
+	const size_t el = P->precision == kPrecFP64 ? sizeof(double) : sizeof(float);
+	const size_t esmem = (size_t) P->B * P->Lp1 * el + (2 * P->L + 1) * sizeof(double2);
+	if(P->precision == kPrecFP64)
+		k_epilogue<double><<<S, 128, esmem, st>>>(e, (double *) ws);
+	else
+		k_epilogue<float><<<S, 128, esmem, st>>>(e, (float *) ws);
+	launches++;
+	P->last_kernels = launches;
+	CKB(cudaGetLastError());
+	return 0;
+}
+
+// Times every candidate split-K factor (3 launches each, CUDA events on the
+// caller's stream, after one warm-up) and keeps the fastest for S.
+int batch_autotune(void *pp, const void *F, int S, long long ld, void *sky, void *ws, size_t ws_bytes, void *stream_v)
+{
+	BatchPlan *P = (BatchPlan *) pp;
+	cudaStream_t st = (cudaStream_t) stream_v;
+	int sms = 148, dev = 0;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	std::vector<int> cand;
+	if(P->precision == kPrecBF16x3) {
+		const int tiles = (S + TM - 1) / TM;
+		for(int ks = 1; ks <= P->Kst / 2 && tiles * ks <= 4 * sms; ks++)
+			if(ks <= 8 || tiles * ks <= 2 * sms)
+				cand.push_back(ks);
+	} else {
+		const int nch = (P->Ku + CC_KC - 1) / CC_KC;
+		for(int ks = 1; ks <= nch && ks <= 64; ks *= 2)
+			cand.push_back(ks);
+	}
+	if(cand.empty())
+		cand.push_back(1);
+	cudaEvent_t e0, e1;
+	CKB(cudaEventCreate(&e0));
+	CKB(cudaEventCreate(&e1));
+	int best = cand[0];
+	float best_ms = 1e30f;
+	for(int ks : cand) {
+		if(batch_run(P, F, S, ld, nullptr, sky, ws, ws_bytes, st, ks))
+			return -1;
+		CKB(cudaEventRecord(e0, st));
+		for(int r = 0; r < 3; r++)
+			if(batch_run(P, F, S, ld, nullptr, sky, ws, ws_bytes, st, ks))
+				return -1;
+		CKB(cudaEventRecord(e1, st));
+		CKB(cudaEventSynchronize(e1));
+		float ms = 0;
+		CKB(cudaEventElapsedTime(&ms, e0, e1));
+		if(ms < best_ms) {
+			best_ms = ms;
+			best = ks;
+		}
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	P->split[S] = best;
+	return best;
+}
+
+int batch_set_timing_events(void *pp, void *ev_begin, void *ev_end)
+{
+	BatchPlan *P = (BatchPlan *) pp;
+	P->ev_begin = (cudaEvent_t) ev_begin;
+	P->ev_end = (cudaEvent_t) ev_end;
+	return 0;
+}
+
+int batch_check_error(void *pp, unsigned *code)
+{
+	BatchPlan *P = (BatchPlan *) pp;
+	unsigned h = 0;
+	CKB(cudaMemcpy(&h, P->err, sizeof(h), cudaMemcpyDeviceToHost));
+	*code = h;
+	return 0;
+}
+
+static int grow(void **p, size_t *have, size_t need)
+{
+	if(*have >= need && *p)
+		return 0;
+	dfree(*p);
+	*p = dmalloc(need);
+	*have = *p ? need : 0;
+	return *p ? 0 : -1;
+}
+
+int batch_run_host(void *pp, const void *F_host, int S, long long ld, const double *gmst_host, void *sky_host)
+{
+	BatchPlan *P = (BatchPlan *) pp;
+	if(S <= 0)
+		return 0;
+	cudaStream_t st = (cudaStream_t) lib_stream();
+	const size_t fbytes = (size_t) P->n_det * S * ld * 16;
+	const size_t sbytes = (size_t) S * P->nq * 16;
+	const size_t wbytes = batch_workspace_bytes(P, S);
+	if(grow(&P->hF, &P->hF_bytes, fbytes) || grow(&P->hSky, &P->hSky_bytes, sbytes) || grow(&P->hG, &P->hG_bytes, (size_t) S * 8))
+		return -1;
+	if(P->hWs_bytes < wbytes) {
+		if(grow(&P->hWs, &P->hWs_bytes, wbytes))
+			return -1;
+		CKB(cudaMemsetAsync(P->hWs, 0, wbytes, st));
+	}
+	CKB(cudaMemcpyAsync(P->hF, F_host, fbytes, cudaMemcpyHostToDevice, st));
+	if(gmst_host)
+		CKB(cudaMemcpyAsync(P->hG, gmst_host, (size_t) S * 8, cudaMemcpyHostToDevice, st));
+	if(batch_run(P, P->hF, S, ld, gmst_host ? (const double *) P->hG : nullptr, P->hSky, P->hWs, P->hWs_bytes, st, 0))
+		return -1;
+	CKB(cudaMemcpyAsync(sky_host, P->hSky, sbytes, cudaMemcpyDeviceToHost, st));
+	CKB(cudaStreamSynchronize(st));
+	unsigned code = 0;
+	if(batch_check_error(P, &code))
+		return -1;
+	if(code) {
+		set_error("batch_run_host: device pipeline timed out (code %u)", code);
+		return -1;
+	}
+	return 0;
+}
+
+}  // namespace sphrad

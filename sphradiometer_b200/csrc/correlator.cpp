@@ -1,0 +1,744 @@
+// correlator.cpp -- C-ABI implementation of instruments, baselines,
+// frequency-domain correlation plans, the FD integrators, and the batched
+// device-resident extension API (host C++).
+//
+// Reference: instrument.c, correlator.c (cannon-zz/sphradiometer).  Plan
+// construction and integration run on the GPU (runtime.cu, batch.cu);
+// these functions manage the host structs and their device mirrors.
+#include <sphradiometer/correlator.h>
+#include <sphradiometer_b200.h>
+
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "abi_common.h"
+
+using namespace sphrad;
+
+namespace sphrad {
+const double *rotation_plan_flat_for(const struct sh_series_rotation_plan *plan, std::vector<dcplx> &scratch);
+int batch_set_split(void *plan, int S, int ks);
+int batch_check_error(void *plan, unsigned *code);
+int batch_set_timing_events(void *plan, void *ev_begin, void *ev_end);
+int batch_autotune(void *plan, const void *F, int S, long long ld, void *sky, void *ws, size_t ws_bytes, void *stream);
+}  // namespace sphrad
+
+// ------------------------------------------------------------------------
+// gsl_vector-compatible allocation (layout of GSL's gsl_vector/gsl_block)
+// ------------------------------------------------------------------------
+static gsl_vector *vec3_alloc()
+{
+	gsl_vector *v = (gsl_vector *) malloc(sizeof(*v));
+	gsl_block *b = (gsl_block *) malloc(sizeof(*b));
+	double *d = (double *) calloc(3, sizeof(double));
+	if(!v || !b || !d) {
+		free(v);
+		free(b);
+		free(d);
+		return NULL;
+	}
+	b->size = 3;
+	b->data = d;
+	v->size = 3;
+	v->stride = 1;
+	v->data = d;
+	v->block = b;
+	v->owner = 1;
+	return v;
+}
+
+static void vec3_free(gsl_vector *v)
+{
+	if(!v)
+		return;
+	if(v->owner && v->block) {
+		free(v->block->data);
+		free(v->block);
+	}
+	free(v);
+}
+
+static inline double vget(const gsl_vector *v, int i) { return v->data[(size_t) i * v->stride]; }
+static inline void vset(gsl_vector *v, int i, double x) { v->data[(size_t) i * v->stride] = x; }
+
+// ------------------------------------------------------------------------
+// vectors and instruments (instrument.c:60-336)
+// ------------------------------------------------------------------------
+extern "C" double vector_magnitude(const gsl_vector *v)
+{
+	const double x = vget(v, 0), y = vget(v, 1), z = vget(v, 2);
+	return sqrt(x * x + y * y + z * z);
+}
+
+extern "C" double vector_r_dot_s(const gsl_vector *v, double theta, double phi)
+{
+	return (vget(v, 0) * cos(phi) + vget(v, 1) * sin(phi)) * sin(theta) + vget(v, 2) * cos(theta);
+}
+
+extern "C" void vector_direction(const gsl_vector *v, double *theta, double *phi)
+{
+	const double x = vget(v, 0), y = vget(v, 1), z = vget(v, 2);
+	*theta = atan2(sqrt(x * x + y * y), z);
+	*phi = atan2(y, x);
+	if(*phi < 0)
+		*phi += 2. * M_PI;
+}
+
+extern "C" struct instrument *instrument_new(double x, double y, double z, void *data)
+{
+	struct instrument *n = (struct instrument *) malloc(sizeof(*n));
+	gsl_vector *pc = vec3_alloc();
+	if(!n || !pc) {
+		free(n);
+		vec3_free(pc);
+		return NULL;
+	}
+	vset(pc, 0, x);
+	vset(pc, 1, y);
+	vset(pc, 2, z);
+	n->phase_centre = pc;
+	n->data = data;
+	return n;
+}
+
+extern "C" void instrument_free(struct instrument *i)
+{
+	if(i)
+		vec3_free(i->phase_centre);
+	free(i);
+}
+
+extern "C" struct instrument *instrument_copy(const struct instrument *i)
+{
+	return instrument_new(vget(i->phase_centre, 0), vget(i->phase_centre, 1), vget(i->phase_centre, 2), i->data);
+}
+
+extern "C" struct instrument *instrument_new_from_r_theta_phi(double r, double theta, double phi, void *data)
+{
+	return instrument_new(r * sin(theta) * cos(phi), r * sin(theta) * sin(phi), r * cos(theta), data);
+}
+
+extern "C" double instrument_r(const struct instrument *i) { return vector_magnitude(i->phase_centre); }
+
+// a - b (instrument.c:210-218)
+extern "C" gsl_vector *instrument_baseline(const struct instrument *a, const struct instrument *b)
+{
+	gsl_vector *v = vec3_alloc();
+	if(!v)
+		return NULL;
+	for(int k = 0; k < 3; k++)
+		vset(v, k, vget(a->phase_centre, k) - vget(b->phase_centre, k));
+	return v;
+}
+
+extern "C" struct instrument_array *instrument_array_new(int n)
+{
+	struct instrument_array *a = (struct instrument_array *) malloc(sizeof(*a));
+	struct instrument **v = (struct instrument **) calloc(n > 0 ? n : 1, sizeof(*v));
+	if(!a || !v) {
+		free(a);
+		free(v);
+		return NULL;
+	}
+	a->instruments = v;
+	a->n = n;
+	return a;
+}
+
+extern "C" int instrument_array_len(const struct instrument_array *a) { return a->n; }
+
+extern "C" struct instrument *instrument_array_get(const struct instrument_array *a, int k)
+{
+	return (0 <= k && k < a->n) ? a->instruments[k] : NULL;
+}
+
+// takes ownership of the instrument; frees it on failure
+extern "C" struct instrument *instrument_array_set(struct instrument_array *a, int k, struct instrument *i)
+{
+	if(k < 0 || k >= a->n) {
+		instrument_free(i);
+		return NULL;
+	}
+	instrument_free(a->instruments[k]);
+	a->instruments[k] = i;
+	return i;
+}
+
+extern "C" struct instrument *instrument_array_append(struct instrument_array *a, struct instrument *i)
+{
+	struct instrument **v = (struct instrument **) realloc(a->instruments, (a->n + 1) * sizeof(*v));
+	if(!v) {
+		instrument_free(i);
+		return NULL;
+	}
+	a->instruments = v;
+	a->instruments[a->n++] = i;
+	return i;
+}
+
+extern "C" void instrument_array_free(struct instrument_array *a)
+{
+	if(a) {
+		for(int i = 0; i < a->n; i++)
+			instrument_free(a->instruments[i]);
+		free(a->instruments);
+	}
+	free(a);
+}
+
+extern "C" struct instrument_array *instrument_array_copy(const struct instrument_array *a)
+{
+	struct instrument_array *n = instrument_array_new(a->n);
+	if(!n)
+		return NULL;
+	for(int i = 0; i < a->n; i++)
+		n->instruments[i] = a->instruments[i] ? instrument_copy(a->instruments[i]) : NULL;
+	return n;
+}
+
+// ------------------------------------------------------------------------
+// sizing utilities (correlator.c:55-111, projection.c:56-87)
+// ------------------------------------------------------------------------
+extern "C" unsigned int correlator_baseline_power_l_max_naive(double D, double delta_t)
+{
+	return (unsigned) floor(M_PI / (2. * asin(delta_t / (2. * D))) + 1.);
+}
+
+extern "C" unsigned int correlator_baseline_power_l_max(const struct correlator_baseline *baseline, double delta_t)
+{
+	const double D = vector_magnitude(baseline->d);
+	if(delta_t <= 0. || D <= 0.)
+		return (unsigned) -1;
+	return correlator_baseline_power_l_max_naive(D, delta_t);
+}
+
+extern "C" double correlator_dump_interval(unsigned int power_l_max, unsigned int dumps_per_lobe)
+{
+	const double seconds_per_day = 86164.0;
+	const double radians_per_second = 2 * M_PI / seconds_per_day;
+	const double radians_per_lobe = 2 * M_PI / power_l_max;
+	return radians_per_lobe / radians_per_second / dumps_per_lobe;
+}
+
+extern "C" int correlator_transient(const struct sh_series_array *a, const struct sh_series_array *b)
+{
+	return ((a->n > b->n ? a->n : b->n) - 1) / 2;
+}
+
+extern "C" int projection_matrix_n_elements(double r, double delta_t) { return 2 * (int) (60 + r / delta_t + 1) + 1; }
+
+extern "C" unsigned int projection_matrix_l_max(double r, double delta_t)
+{
+	const int l = M_PI * r / delta_t + 1;
+	return l;
+}
+
+extern "C" double *correlator_square_window_new(const int n, const int zero_samples, const double amplitude)
+{
+	if(2 * zero_samples > n || zero_samples < 0)
+		return NULL;
+	double *w = (double *) malloc((n > 0 ? n : 1) * sizeof(double));
+	if(!w)
+		return NULL;
+	for(int i = 0; i < n; i++)
+		w[i] = (i < zero_samples || i >= n - zero_samples) ? 0.0 : amplitude;
+	return w;
+}
+
+extern "C" double *correlator_tukey_window_new(const int n, const int zero_samples, const int taper_samples, const double amplitude)
+{
+	if(2 * (zero_samples + taper_samples) > n || zero_samples < 0)
+		return NULL;
+	double *w = (double *) malloc((n > 0 ? n : 1) * sizeof(double));
+	if(!w)
+		return NULL;
+	const double dtheta = M_PI_2 / taper_samples;
+	for(int i = 0; i < n; i++)
+		w[i] = 0.0;
+	for(int i = 0; i < taper_samples; i++) {
+		const double s = sin(dtheta * i);
+		w[zero_samples + i] = w[n - 1 - zero_samples - i] = amplitude * s * s;
+	}
+	for(int i = zero_samples + taper_samples; i < n - zero_samples - taper_samples; i++)
+		w[i] = amplitude;
+	return w;
+}
+
+// ------------------------------------------------------------------------
+// baselines (correlator.c:262-322, 720-818)
+// ------------------------------------------------------------------------
+extern "C" struct correlator_baseline *correlator_baseline_new(const struct instrument_array *instruments, int index_a, int index_b)
+{
+	const struct instrument *a = instrument_array_get(instruments, index_a);
+	const struct instrument *b = instrument_array_get(instruments, index_b);
+	if(!a || !b)
+		return NULL;
+	struct correlator_baseline *n = (struct correlator_baseline *) malloc(sizeof(*n));
+	gsl_vector *d = instrument_baseline(a, b);
+	if(!n || !d) {
+		vec3_free(d);
+		free(n);
+		return NULL;
+	}
+	n->instruments = instruments;
+	n->index_a = index_a;
+	n->index_b = index_b;
+	n->d = d;
+	vector_direction(d, &n->theta, &n->phi);
+	return n;
+}
+
+extern "C" void correlator_baseline_free(struct correlator_baseline *b)
+{
+	if(b)
+		vec3_free(b->d);
+	free(b);
+}
+
+extern "C" struct correlator_baseline *correlator_baseline_copy(const struct correlator_baseline *b)
+{
+	struct correlator_baseline *n = (struct correlator_baseline *) malloc(sizeof(*n));
+	if(!n)
+		return NULL;
+	*n = *b;
+	n->d = vec3_alloc();
+	if(!n->d) {
+		free(n);
+		return NULL;
+	}
+	for(int k = 0; k < 3; k++)
+		vset(n->d, k, vget(b->d, k));
+	return n;
+}
+
+extern "C" struct correlator_network_baselines *correlator_network_baselines_new(const struct instrument_array *instruments)
+{
+	const int nd = instrument_array_len(instruments);
+	const int nb = nd * (nd - 1) / 2;
+	struct correlator_network_baselines *n = (struct correlator_network_baselines *) malloc(sizeof(*n));
+	struct correlator_baseline **v = (struct correlator_baseline **) calloc(nb > 0 ? nb : 1, sizeof(*v));
+	if(!n || !v) {
+		free(n);
+		free(v);
+		return NULL;
+	}
+	int k = 0;
+	for(int i = 1; i < nd; i++)
+		for(int j = 0; j < i; j++, k++) {
+			v[k] = correlator_baseline_new(instruments, i, j);
+			if(!v[k]) {
+				while(--k >= 0)
+					correlator_baseline_free(v[k]);
+				free(v);
+				free(n);
+				return NULL;
+			}
+		}
+	n->baselines = v;
+	n->n_baselines = nb;
+	return n;
+}
+
+extern "C" void correlator_network_baselines_free(struct correlator_network_baselines *n)
+{
+	if(n) {
+		for(int i = 0; i < n->n_baselines; i++)
+			correlator_baseline_free(n->baselines[i]);
+		free(n->baselines);
+	}
+	free(n);
+}
+
+extern "C" struct correlator_network_baselines *correlator_network_baselines_copy(const struct correlator_network_baselines *n)
+{
+	struct correlator_network_baselines *c = (struct correlator_network_baselines *) malloc(sizeof(*c));
+	if(!c)
+		return NULL;
+	*c = *n;
+	c->baselines = (struct correlator_baseline **) calloc(n->n_baselines > 0 ? n->n_baselines : 1, sizeof(*c->baselines));
+	if(!c->baselines) {
+		free(c);
+		return NULL;
+	}
+	for(int i = 0; i < n->n_baselines; i++) {
+		c->baselines[i] = correlator_baseline_copy(n->baselines[i]);
+		if(!c->baselines[i]) {
+			correlator_network_baselines_free(c);
+			return NULL;
+		}
+	}
+	return c;
+}
+
+extern "C" unsigned int correlator_network_l_max(struct correlator_network_baselines *n, double delta_t)
+{
+	unsigned l_max = 0;
+	for(int i = 0; i < n->n_baselines; i++) {
+		const unsigned l = correlator_baseline_power_l_max(n->baselines[i], delta_t);
+		if(l > l_max)
+			l_max = l;
+	}
+	return l_max;
+}
+
+// ------------------------------------------------------------------------
+// FD plans (correlator.c:325-591)
+// ------------------------------------------------------------------------
+static void plan_register(struct correlator_plan_fd *p)
+{
+	const struct sh_series_array *a = p->delay_product;
+	register_buffer(a->coeff, (size_t) a->n * a->stride * sizeof(dcplx), p);
+	bump_owner(p);
+}
+
+static struct correlator_plan_fd *plan_fd_build(const struct correlator_baseline *baseline, int n, double delta_t, unsigned l_req)
+{
+	const double d_len = vector_magnitude(baseline->d);
+	if(!(delta_t > 0) || !(d_len > 0) || n <= 0) {
+		set_error("correlator_plan_fd_new: bad baseline, sample interval or length");
+		return NULL;
+	}
+	const double r = d_len / 2;
+	const unsigned a_l = projection_matrix_l_max(r, delta_t);
+	unsigned L = correlator_baseline_power_l_max(baseline, delta_t);
+	if(L > 2 * a_l)
+		L = 2 * a_l;
+	if(l_req < L)
+		L = l_req;
+	const int n_el = projection_matrix_n_elements(r, delta_t);
+	struct correlator_plan_fd *p = (struct correlator_plan_fd *) calloc(1, sizeof(*p));
+	dcplx *fsp = (dcplx *) calloc(n, sizeof(dcplx));
+	struct sh_series_array *dp = sh_series_array_new(n, L, 1);
+	struct sh_series *p1 = sh_series_new_zero(L, 1);
+	double *R = sh_series_rot_matrix(baseline->theta, baseline->phi);
+	struct sh_series_rotation_plan *rp = NULL;
+	if(!p || !fsp || !dp || !p1 || !R)
+		goto fail;
+	if(build_delay_table(d_len, delta_t, n, L, (double *) dp->coeff, NULL))
+		goto fail;
+	rp = sh_series_rotation_plan_new(p1, R);
+	if(!rp)
+		goto fail;
+	free(R);
+	p->baseline = baseline;
+	p->delta_t = delta_t;
+	p->transient = (n_el - 1) / 2;  // correlator_transient of the two projections
+	p->delay_product = dp;
+	p->fseries_product = fsp;
+	p->power_1d = p1;
+	p->rotation_plan = rp;
+	plan_register(p);
+	return p;
+fail:
+	free(R);
+	sh_series_free(p1);
+	sh_series_array_free(dp);
+	free(fsp);
+	free(p);
+	return NULL;
+}
+
+extern "C" struct correlator_plan_fd *correlator_plan_fd_new(const struct correlator_baseline *baseline, int n, double delta_t)
+{
+	return plan_fd_build(baseline, n, delta_t, ~0u);
+}
+
+extern "C" struct correlator_plan_fd *correlator_plan_fd_new_l(const struct correlator_baseline *baseline, int n, double delta_t, unsigned l_max)
+{
+	return plan_fd_build(baseline, n, delta_t, l_max);
+}
+
+extern "C" void correlator_plan_fd_free(struct correlator_plan_fd *p)
+{
+	if(p) {
+		forget_mirror(p);
+		unregister_owner(p);
+		free(p->fseries_product);
+		sh_series_array_free(p->delay_product);
+		sh_series_free(p->power_1d);
+		sh_series_rotation_plan_free(p->rotation_plan);
+	}
+	free(p);
+}
+
+extern "C" struct correlator_plan_fd *correlator_plan_fd_copy(const struct correlator_plan_fd *plan)
+{
+	struct correlator_plan_fd *n = (struct correlator_plan_fd *) malloc(sizeof(*n));
+	if(!n)
+		return NULL;
+	*n = *plan;
+	n->fseries_product = (dcplx *) malloc((size_t) plan->delay_product->n * sizeof(dcplx));
+	n->delay_product = sh_series_array_copy(plan->delay_product);
+	n->power_1d = sh_series_copy(plan->power_1d);
+	n->rotation_plan = sh_series_rotation_plan_copy(plan->rotation_plan);
+	if(!n->fseries_product || !n->delay_product || !n->power_1d || !n->rotation_plan) {
+		free(n->fseries_product);
+		sh_series_array_free(n->delay_product);
+		sh_series_free(n->power_1d);
+		sh_series_rotation_plan_free(n->rotation_plan);
+		free(n);
+		return NULL;
+	}
+	memcpy(n->fseries_product, plan->fseries_product, (size_t) plan->delay_product->n * sizeof(dcplx));
+	plan_register(n);
+	return n;
+}
+
+extern "C" struct correlator_plan_fd *correlator_plan_fd_set_l(struct correlator_plan_fd *plan, unsigned l_max)
+{
+	if(plan->delay_product->l_max != plan->power_1d->l_max || plan->rotation_plan->l_max != plan->power_1d->l_max)
+		return NULL;
+	if(l_max > plan->power_1d->l_max)
+		return NULL;
+	if(l_max == plan->power_1d->l_max)
+		return plan;
+	if(!sh_series_array_set_l(plan->delay_product, l_max) || !sh_series_resize(plan->power_1d, l_max) || !sh_series_rotation_plan_set_l(plan->rotation_plan, l_max))
+		return NULL;
+	plan_register(plan);
+	return plan;
+}
+
+extern "C" void sphrad_b200_plan_fd_touch(struct correlator_plan_fd *plan)
+{
+	if(plan)
+		bump_owner(plan);
+}
+
+extern "C" struct correlator_network_plan_fd *correlator_network_plan_fd_new_l(struct correlator_network_baselines *baselines, int n, double delta_t, unsigned l_max)
+{
+	struct correlator_network_plan_fd *np = (struct correlator_network_plan_fd *) malloc(sizeof(*np));
+	struct correlator_plan_fd **plans = (struct correlator_plan_fd **) calloc(baselines->n_baselines > 0 ? baselines->n_baselines : 1, sizeof(*plans));
+	if(!np || !plans) {
+		free(np);
+		free(plans);
+		return NULL;
+	}
+	for(int i = 0; i < baselines->n_baselines; i++) {
+		plans[i] = plan_fd_build(baselines->baselines[i], n, delta_t, l_max);
+		if(!plans[i]) {
+			while(--i >= 0)
+				correlator_plan_fd_free(plans[i]);
+			free(plans);
+			free(np);
+			return NULL;
+		}
+	}
+	np->baselines = baselines;
+	np->plans = plans;
+	return np;
+}
+
+extern "C" struct correlator_network_plan_fd *correlator_network_plan_fd_new(struct correlator_network_baselines *baselines, int n, double delta_t)
+{
+	return correlator_network_plan_fd_new_l(baselines, n, delta_t, ~0u);
+}
+
+extern "C" void correlator_network_plan_fd_free(struct correlator_network_plan_fd *p)
+{
+	if(p) {
+		for(int i = 0; i < p->baselines->n_baselines; i++)
+			correlator_plan_fd_free(p->plans[i]);
+		free(p->plans);
+	}
+	free(p);
+}
+
+extern "C" struct correlator_network_plan_fd *correlator_network_plan_fd_copy(const struct correlator_network_plan_fd *p)
+{
+	struct correlator_network_plan_fd *n = (struct correlator_network_plan_fd *) malloc(sizeof(*n));
+	if(!n)
+		return NULL;
+	*n = *p;
+	n->plans = (struct correlator_plan_fd **) calloc(p->baselines->n_baselines > 0 ? p->baselines->n_baselines : 1, sizeof(*n->plans));
+	if(!n->plans) {
+		free(n);
+		return NULL;
+	}
+	for(int i = 0; i < p->baselines->n_baselines; i++) {
+		n->plans[i] = correlator_plan_fd_copy(p->plans[i]);
+		if(!n->plans[i]) {
+			correlator_network_plan_fd_free(n);
+			return NULL;
+		}
+	}
+	return n;
+}
+
+extern "C" struct correlator_network_plan_fd *correlator_network_plan_fd_set_l(struct correlator_network_plan_fd *p, unsigned l_max)
+{
+	for(int i = 0; i < p->baselines->n_baselines; i++) {
+		if(p->plans[i]->power_1d->l_max <= l_max)
+			continue;
+		if(!correlator_plan_fd_set_l(p->plans[i], l_max))
+			return NULL;
+	}
+	return p;
+}
+
+// ------------------------------------------------------------------------
+// integrators (correlator.c:681-711, 993-1010)
+// ------------------------------------------------------------------------
+static int make_job(struct correlator_plan_fd *plan, const dcplx *a, const dcplx *b, double weight, std::vector<dcplx> &rot_scratch, BaselineJob &j)
+{
+	const struct sh_series_array *dp = plan->delay_product;
+	if(dp->l_max != plan->power_1d->l_max || dp->polar != plan->power_1d->polar || plan->rotation_plan->l_max < plan->power_1d->l_max) {
+		set_error("correlator: plan's delay_product, power_1d and rotation_plan disagree");
+		return -1;
+	}
+	// keep the write-tracking registration on the current table
+	register_buffer(dp->coeff, (size_t) dp->n * dp->stride * sizeof(dcplx), plan);
+	j.a = (const double *) a;
+	j.b = (const double *) b;
+	j.key = plan;
+	j.gen = (owner_generation(plan) << 24) ^ owner_generation(plan->rotation_plan);
+	j.n = dp->n;
+	j.stride = dp->stride;
+	j.l_max = dp->l_max;
+	j.polar = dp->polar;
+	j.D = (const double *) dp->coeff;
+	j.rot = rotation_plan_flat_for(plan->rotation_plan, rot_scratch);
+	if(!rot_scratch.empty())
+		j.gen = next_generation();
+	j.weight = weight;
+	j.power_1d = (double *) plan->power_1d->coeff;
+	j.fseries_product = (double *) plan->fseries_product;
+	return 0;
+}
+
+extern "C" struct sh_series *correlator_baseline_integrate_power_fd(const dcplx *a, const dcplx *b, struct correlator_plan_fd *plan)
+{
+	std::vector<dcplx> scratch;
+	BaselineJob j;
+	if(make_job(plan, a, b, 1.0, scratch, j))
+		return NULL;
+	struct sh_series *out = sh_series_new(plan->power_1d->l_max, 0);
+	if(!out)
+		return NULL;
+	if(integrate_fd(&j, 1, out->l_max, (double *) out->coeff)) {
+		sh_series_free(out);
+		return NULL;
+	}
+	return out;
+}
+
+extern "C" struct sh_series *correlator_network_integrate_power_fd(struct sh_series *sky, dcplx **fseries, struct correlator_network_plan_fd *plan)
+{
+	const int nb = plan->baselines->n_baselines;
+	if(nb <= 0 || sky->polar) {
+		set_error("correlator_network_integrate_power_fd: empty network or polar sky");
+		return NULL;
+	}
+	const int nd = instrument_array_len(plan->baselines->baselines[0]->instruments);
+	std::vector<BaselineJob> jobs(nb);
+	std::vector<std::vector<dcplx>> scratch(nb);
+	int k = 0;
+	for(int i = 1; i < nd && k < nb; i++)
+		for(int j = 0; j < i && k < nb; j++, k++) {
+			if(plan->plans[k]->power_1d->l_max > sky->l_max) {
+				set_error("correlator_network_integrate_power_fd: sky l_max below a baseline's");
+				return NULL;
+			}
+			if(make_job(plan->plans[k], fseries[i], fseries[j], 1.0 / nb, scratch[k], jobs[k]))
+				return NULL;
+		}
+	if(k != nb) {
+		set_error("correlator_network_integrate_power_fd: network and instrument count disagree");
+		return NULL;
+	}
+	if(integrate_fd(jobs.data(), nb, sky->l_max, (double *) sky->coeff))
+		return NULL;
+	note_write(sky->coeff);
+	return sky;
+}
+
+// ------------------------------------------------------------------------
+// batched extension API
+// ------------------------------------------------------------------------
+struct sphrad_batch_plan {
+	void *impl;
+};
+
+extern "C" sphrad_batch_plan *sphrad_batch_plan_new(const struct correlator_network_plan_fd *plan, int precision)
+{
+	const int nb = plan->baselines->n_baselines;
+	if(nb <= 0 || nb > kMaxBaselines) {
+		set_error("sphrad_batch_plan_new: %d baselines (1..%d supported)", nb, kMaxBaselines);
+		return NULL;
+	}
+	BatchPlanDesc d;
+	d.n_det = instrument_array_len(plan->baselines->baselines[0]->instruments);
+	d.n_baselines = nb;
+	d.n = plan->plans[0]->delay_product->n;
+	d.hermitian = 1;
+	d.weight = 1.0 / nb;
+	std::vector<std::vector<dcplx>> scratch(nb);
+	for(int b = 0; b < nb; b++) {
+		const struct correlator_plan_fd *p = plan->plans[b];
+		if(p->delay_product->n != d.n || !p->delay_product->polar || p->rotation_plan->l_max < p->power_1d->l_max) {
+			set_error("sphrad_batch_plan_new: baselines need polar delay tables of equal length");
+			return NULL;
+		}
+		d.bi[b] = plan->baselines->baselines[b]->index_a;
+		d.bj[b] = plan->baselines->baselines[b]->index_b;
+		d.D[b] = (const double *) p->delay_product->coeff;
+		d.lb[b] = p->delay_product->l_max;
+		d.rot[b] = rotation_plan_flat_for(p->rotation_plan, scratch[b]);
+	}
+	void *impl = batch_plan_create(d, precision);
+	if(!impl)
+		return NULL;
+	sphrad_batch_plan *bp = (sphrad_batch_plan *) malloc(sizeof(*bp));
+	if(!bp) {
+		batch_plan_destroy(impl);
+		return NULL;
+	}
+	bp->impl = impl;
+	return bp;
+}
+
+extern "C" void sphrad_batch_plan_free(sphrad_batch_plan *p)
+{
+	if(p)
+		batch_plan_destroy(p->impl);
+	free(p);
+}
+
+extern "C" unsigned sphrad_batch_plan_l_max(const sphrad_batch_plan *p) { return batch_plan_l_max(p->impl); }
+extern "C" int sphrad_batch_plan_bins(const sphrad_batch_plan *p) { return batch_plan_bins(p->impl); }
+extern "C" size_t sphrad_batch_workspace_size(const sphrad_batch_plan *p, int n_seg) { return batch_workspace_bytes(p->impl, n_seg); }
+
+extern "C" int sphrad_batch_integrate(sphrad_batch_plan *p, const void *fseries_dev, int n_seg, long long ld, const double *gmst_dev, void *sky_dev, void *workspace,
+				      size_t workspace_bytes, void *stream)
+{
+	return batch_run(p->impl, fseries_dev, n_seg, ld, gmst_dev, sky_dev, workspace, workspace_bytes, stream, 0);
+}
+
+extern "C" int sphrad_batch_integrate_host(sphrad_batch_plan *p, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky)
+{
+	return batch_run_host(p->impl, fseries, n_seg, ld, gmst, sky);
+}
+
+extern "C" int sphrad_batch_set_split(sphrad_batch_plan *p, int n_seg, int split) { return batch_set_split(p->impl, n_seg, split); }
+extern "C" int sphrad_batch_get_split(const sphrad_batch_plan *p, int n_seg) { return batch_pick_split(p->impl, n_seg); }
+extern "C" int sphrad_batch_kernels_per_call(const sphrad_batch_plan *p) { return batch_last_kernel_count(p->impl); }
+
+extern "C" int sphrad_batch_autotune(sphrad_batch_plan *p, const void *fseries_dev, int n_seg, long long ld, void *sky_dev, void *workspace, size_t workspace_bytes,
+				     void *stream)
+{
+	return batch_autotune(p->impl, fseries_dev, n_seg, ld, sky_dev, workspace, workspace_bytes, stream);
+}
+
+extern "C" int sphrad_batch_set_timing_events(sphrad_batch_plan *p, void *ev_begin, void *ev_end)
+{
+	return batch_set_timing_events(p->impl, ev_begin, ev_end);
+}
+
+extern "C" int sphrad_batch_status(sphrad_batch_plan *p)
+{
+	unsigned code = 0;
+	if(batch_check_error(p->impl, &code))
+		return -1;
+	return (int) code;
+}

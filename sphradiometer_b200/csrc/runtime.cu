@@ -1,0 +1,927 @@
+// runtime.cu -- device context and the FP64 kernels of the drop-in path:
+// delay-table (D_l(k)) construction, Wigner-D rotation plans, rotation,
+// and the per-call frequency-domain integrator.
+//
+// Reference algorithms (cannon-zz/sphradiometer):
+//   delay table      correlator.c:424-519, projection.c:99-131,
+//                    sh_series_trans.c:663-734, sh_series_product.c:269-329
+//   rotation plan    sh_series_rotation.c:279-422 (Choi, Ivanic, Gordon &
+//                    Ruedenberg recursion)
+//   rotation         sh_series_rotation.c:546-589
+//   integration      correlator.c:681-711 and 993-1010
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "runtime.h"
+
+namespace sphrad {
+
+// ------------------------------------------------------------------------
+// errors
+// ------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+void set_error(const char *fmt, ...)
+{
+	char buf[512];
+	va_list ap;
+	va_start(ap, fmt);
+	vsnprintf(buf, sizeof(buf), fmt, ap);
+	va_end(ap);
+	g_err = buf;
+}
+
+const char *last_error() { return g_err.c_str(); }
+
+#define CK(call)                                                                 \
+	do {                                                                     \
+		cudaError_t e_ = (call);                                         \
+		if(e_ != cudaSuccess) {                                          \
+			set_error("%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+			return -1;                                               \
+		}                                                                \
+	} while(0)
+
+// ------------------------------------------------------------------------
+// device context: one non-blocking stream per device
+// ------------------------------------------------------------------------
+static std::mutex g_ctx_mu;
+static std::unordered_map<int, cudaStream_t> g_streams;
+
+int ensure_device()
+{
+	int n = 0;
+	cudaError_t e = cudaGetDeviceCount(&n);
+	if(e != cudaSuccess || n == 0) {
+		set_error("no usable CUDA device (%s)", e == cudaSuccess ? "count 0" : cudaGetErrorString(e));
+		return -1;
+	}
+	int dev = 0;
+	CK(cudaGetDevice(&dev));
+	std::lock_guard<std::mutex> lk(g_ctx_mu);
+	if(!g_streams.count(dev)) {
+		cudaStream_t s;
+		CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+		g_streams[dev] = s;
+	}
+	return 0;
+}
+
+void *lib_stream()
+{
+	int dev = 0;
+	cudaGetDevice(&dev);
+	std::lock_guard<std::mutex> lk(g_ctx_mu);
+	auto it = g_streams.find(dev);
+	return it == g_streams.end() ? nullptr : (void *) it->second;
+}
+
+static cudaStream_t S() { return (cudaStream_t) lib_stream(); }
+
+int stream_sync()
+{
+	CK(cudaStreamSynchronize(S()));
+	CK(cudaGetLastError());
+	return 0;
+}
+
+void *dmalloc(size_t bytes)
+{
+	void *p = nullptr;
+	cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+	if(e != cudaSuccess) {
+		set_error("cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+		return nullptr;
+	}
+	return p;
+}
+
+void dfree(void *p)
+{
+	if(p)
+		cudaFree(p);
+}
+
+int h2d(void *dst, const void *src, size_t bytes)
+{
+	CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, S()));
+	return 0;
+}
+
+int d2h(void *dst, const void *src, size_t bytes)
+{
+	CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, S()));
+	return 0;
+}
+
+int dmemset(void *dst, int value, size_t bytes)
+{
+	CK(cudaMemsetAsync(dst, value, bytes, S()));
+	return 0;
+}
+
+// RAII device buffer
+struct DBuf {
+	void *p = nullptr;
+	DBuf() = default;
+	explicit DBuf(size_t bytes) { p = dmalloc(bytes); }
+	~DBuf() { dfree(p); }
+	DBuf(const DBuf &) = delete;
+	DBuf &operator=(const DBuf &) = delete;
+	template <class T> T *as() const { return (T *) p; }
+};
+
+// ------------------------------------------------------------------------
+// small device helpers
+// ------------------------------------------------------------------------
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double2 cmulc(double2 a, double2 b) { return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y); }  // a * conj(b)
+
+// sizing of the projection matrices: projection.c:56-87, correlator.c:55-65
+static int n_elements(double r, double dt) { return 2 * (int) (60 + r / dt + 1) + 1; }
+static unsigned proj_l_max(double r, double dt) { return (int) (M_PI * r / dt + 1); }
+static unsigned power_l_max_naive(double d, double dt) { return (unsigned) floor(M_PI / (2. * asin(dt / (2. * d))) + 1.); }
+
+// ------------------------------------------------------------------------
+// Gauss-Legendre nodes (Newton on P_n), decreasing x  (the mesh ordering of
+// sh_series_trans.c:149-196)
+// ------------------------------------------------------------------------
+__device__ static void legendre_pn(int n, double z, double *pn, double *pn1)
+{
+	double p0 = 1.0, p1 = z;
+	for(int k = 2; k <= n; k++) {
+		const double p2 = ((2.0 * k - 1.0) * z * p1 - (k - 1.0) * p0) / k;
+		p0 = p1;
+		p1 = p2;
+	}
+	*pn = p1;
+	*pn1 = p0;
+}
+
+__global__ void k_gl_nodes(int n, double *x, double *w)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if(i >= (n + 1) / 2)
+		return;
+	double z = cos(M_PI * (i + 0.75) / (n + 0.5));
+	double pn, pn1, pp = 1.0;
+	for(int it = 0; it < 100; it++) {
+		legendre_pn(n, z, &pn, &pn1);
+		pp = n * (z * pn - pn1) / (z * z - 1.0);
+		const double dz = pn / pp;
+		z -= dz;
+		if(fabs(dz) < 1e-16)
+			break;
+	}
+	legendre_pn(n, z, &pn, &pn1);
+	pp = n * (z * pn - pn1) / (z * z - 1.0);
+	x[i] = z;
+	x[n - 1 - i] = -z;
+	const double wi = 2.0 / ((1.0 - z * z) * pp * pp);
+	w[i] = wi;
+	w[n - 1 - i] = wi;
+	if((n & 1) && i == n / 2)
+		x[i] = 0.0;
+}
+
+// normalised m = 0 Legendre table P~_l(x_i), l < LP, in both layouts
+__global__ void k_plm0_table(int nt, const double *x, int LP, double *P, double *PT)
+{
+	const int i = blockIdx.x * blockDim.x + threadIdx.x;
+	if(i >= nt)
+		return;
+	const double xi = x[i];
+	double p0 = sqrt(1.0 / (4.0 * M_PI));
+	double p1 = xi * sqrt(3.0) * p0;
+	for(int l = 0; l < LP; l++) {
+		double p;
+		if(l == 0)
+			p = p0;
+		else if(l == 1)
+			p = p1;
+		else {
+			const double a = sqrt((2.0 * l + 1.0) * (2.0 * l - 1.0)) / l;
+			const double b = sqrt((2.0 * l + 1.0) / (2.0 * l - 3.0)) * (l - 1.0) / l;
+			p = a * xi * p1 - b * p0;
+			p0 = p1;
+			p1 = p;
+		}
+		P[(size_t) i * LP + l] = p;
+		PT[(size_t) l * nt + i] = p;
+	}
+}
+
+// polar projection of the sinc delay taps (projection.c:99-131): for a phase
+// centre at r z-hat the mesh samples do not depend on phi, so the m = 0 bin
+// of the reference's phi transform is nphi times the ring value and the tap
+// is 2 pi sum_i w_i sinc(pi(-k - r x_i / dt)) P~_l(x_i).
+__global__ void k_taps(double r, double dt, int n_el, int A, int nt, const double *x, const double *w, const double *P, int LP, double *taps)
+{
+	extern __shared__ double s_f[];
+	const int t = blockIdx.x;
+	const int k = t - (n_el - 1) / 2;
+	for(int i = threadIdx.x; i < nt; i += blockDim.x) {
+		const double pi_x = M_PI * (0 - k - r * x[i] / dt);
+		const double s = (pi_x == 0.0) ? 1.0 : sin(pi_x) / pi_x;
+		s_f[i] = 2.0 * M_PI * w[i] * s;
+	}
+	__syncthreads();
+	for(int l = threadIdx.x; l < A; l += blockDim.x) {
+		double acc = 0.0;
+		for(int i = 0; i < nt; i++)
+			acc += s_f[i] * P[(size_t) i * LP + l];
+		taps[(size_t) t * A + l] = acc;
+	}
+}
+
+// zero-padded DFT of the taps along the tap axis (correlator.c:446-451):
+// Ahat[f][l] = sum_t taps[t][l] exp(-2 pi i f t / n), twiddles indexed
+// exactly by (f t) mod n.
+__global__ void k_tap_dft(int n, int n_el, int A, const double *taps, double2 *Ahat)
+{
+	extern __shared__ double2 s_tw[];
+	const int f = blockIdx.x;
+	const int n_tap = n_el < n ? n_el : n;
+	for(int t = threadIdx.x; t < n_tap; t += blockDim.x) {
+		const long long idx = ((long long) f * t) % n;
+		double s, c;
+		sincospi(-2.0 * (double) idx / n, &s, &c);
+		s_tw[t] = make_double2(c, s);
+	}
+	__syncthreads();
+	for(int l = threadIdx.x; l < A; l += blockDim.x) {
+		double2 acc = make_double2(0, 0);
+		for(int t = 0; t < n_tap; t++) {
+			const double v = taps[(size_t) t * A + l];
+			acc.x += v * s_tw[t].x;
+			acc.y += v * s_tw[t].y;
+		}
+		Ahat[(size_t) f * A + l] = acc;
+	}
+}
+
+// per-bin delay product conj(A_f) B_f truncated to l < Ld, stored at bin
+// (n - f) mod n with one 1/n applied (correlator.c:482-492).  The product is
+// the Gauss-Legendre quadrature of the reference's pixel-domain product
+// (exact: the integrand has degree 2 a_l_max + l_max < 2 nt).  The b-side
+// taps are the a-side ones mirrored in cos(theta), B_l = (-1)^l A_l, so
+// sum_l B_l P~_l(x_i) = Q_f(x_{nt-1-i}) with Q_f(x) = sum_l A_l P~_l(x).
+__global__ void k_delay_product(int n, int A, int nt, const double2 *Ahat, const double *PT, const double *P, int LP, const double *w, int Ld, double2 *D)
+{
+	extern __shared__ double2 s_mem[];
+	double2 *s_a = s_mem;          // A
+	double2 *s_q = s_a + A;        // nt
+	double2 *s_h = s_q + nt;       // nt
+	const int f = blockIdx.x;
+	for(int l = threadIdx.x; l < A; l += blockDim.x)
+		s_a[l] = Ahat[(size_t) f * A + l];
+	__syncthreads();
+	for(int i = threadIdx.x; i < nt; i += blockDim.x) {
+		double2 q = make_double2(0, 0);
+		for(int l = 0; l < A; l++) {
+			const double p = PT[(size_t) l * nt + i];
+			q.x += s_a[l].x * p;
+			q.y += s_a[l].y * p;
+		}
+		s_q[i] = q;
+	}
+	__syncthreads();
+	const double scale = 2.0 * M_PI / n;
+	for(int i = threadIdx.x; i < nt; i += blockDim.x) {
+		const double2 u = s_q[i];
+		const double2 v = s_q[nt - 1 - i];
+		// conj(u) * v
+		const double2 h = make_double2(u.x * v.x + u.y * v.y, u.x * v.y - u.y * v.x);
+		s_h[i] = make_double2(scale * w[i] * h.x, scale * w[i] * h.y);
+	}
+	__syncthreads();
+	const size_t row = (size_t) ((n - f) % n) * Ld;
+	for(int l = threadIdx.x; l < Ld; l += blockDim.x) {
+		double2 acc = make_double2(0, 0);
+		for(int i = 0; i < nt; i++) {
+			const double p = P[(size_t) i * LP + l];
+			acc.x += s_h[i].x * p;
+			acc.y += s_h[i].y * p;
+		}
+		D[row + l] = acc;
+	}
+}
+
+int build_delay_table(double d_len, double delta_t, int n, unsigned l_max, double *D_host, double **dev_out)
+{
+	if(ensure_device())
+		return -1;
+	if(!(d_len > 0) || !(delta_t > 0) || n <= 0) {
+		set_error("build_delay_table: bad arguments (d=%g dt=%g n=%d)", d_len, delta_t, n);
+		return -1;
+	}
+	const double r = d_len / 2;
+	const int a_l = proj_l_max(r, delta_t);
+	const int n_el = n_elements(r, delta_t);
+	unsigned p_l = power_l_max_naive(d_len, delta_t);
+	if(p_l > 2u * a_l)
+		p_l = 2 * a_l;
+	if(l_max > p_l) {
+		set_error("build_delay_table: l_max %u above the baseline's power l_max %u", l_max, p_l);
+		return -1;
+	}
+	const int A = a_l + 1;
+	const int nt = 2 * A;
+	const int Ld = l_max + 1;
+	const int LP = A > Ld ? A : Ld;
+	const size_t smem_dp = (size_t) (A + 2 * nt) * sizeof(double2);
+	if(smem_dp > 200 * 1024 || (size_t) nt * sizeof(double) > 200 * 1024) {
+		set_error("build_delay_table: baseline too long for this sample rate (a_l_max %d)", a_l);
+		return -1;
+	}
+	DBuf x(nt * sizeof(double)), w(nt * sizeof(double));
+	DBuf P((size_t) nt * LP * sizeof(double)), PT((size_t) nt * LP * sizeof(double));
+	DBuf taps((size_t) n_el * A * sizeof(double));
+	DBuf Ahat((size_t) n * A * sizeof(double2));
+	double2 *D = (double2 *) dmalloc((size_t) n * Ld * sizeof(double2));
+	if(!x.p || !w.p || !P.p || !PT.p || !taps.p || !Ahat.p || !D) {
+		dfree(D);
+		return -1;
+	}
+	cudaStream_t s = S();
+	k_gl_nodes<<<(nt / 2 + 127) / 128, 128, 0, s>>>(nt, x.as<double>(), w.as<double>());
+	k_plm0_table<<<(nt + 127) / 128, 128, 0, s>>>(nt, x.as<double>(), LP, P.as<double>(), PT.as<double>());
+	k_taps<<<n_el, 256, nt * sizeof(double), s>>>(r, delta_t, n_el, A, nt, x.as<double>(), w.as<double>(), P.as<double>(), LP, taps.as<double>());
+	const int n_tap = n_el < n ? n_el : n;
+	k_tap_dft<<<n, 256, n_tap * sizeof(double2), s>>>(n, n_el, A, taps.as<double>(), Ahat.as<double2>());
+	if(smem_dp > 48 * 1024)
+		cudaFuncSetAttribute(k_delay_product, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem_dp);
+	k_delay_product<<<n, 256, smem_dp, s>>>(n, A, nt, Ahat.as<double2>(), PT.as<double>(), P.as<double>(), LP, w.as<double>(), Ld, D);
+	cudaError_t e = cudaGetLastError();
+	if(e != cudaSuccess) {
+		set_error("build_delay_table: launch failed: %s", cudaGetErrorString(e));
+		dfree(D);
+		return -1;
+	}
+	if(D_host && d2h(D_host, D, (size_t) n * Ld * sizeof(double2))) {
+		dfree(D);
+		return -1;
+	}
+	if(stream_sync()) {
+		dfree(D);
+		return -1;
+	}
+	if(dev_out)
+		*dev_out = (double *) D;
+	else
+		dfree(D);
+	return 0;
+}
+
+// ------------------------------------------------------------------------
+// Wigner-D rotation plan (sh_series_rotation.c:279-422)
+// ------------------------------------------------------------------------
+size_t rot_offset(unsigned l)
+{
+	// sum_{k=1}^{l-1} (2k+1)^2 = (4 l^3 - l - 3) / 3 for l >= 1
+	if(l <= 1)
+		return 0;
+	const size_t L = l;
+	return (4 * L * L * L - L - 3) / 3;
+}
+
+__device__ __forceinline__ size_t d_rot_offset(int l)
+{
+	if(l <= 1)
+		return 0;
+	const size_t L = l;
+	return (4 * L * L * L - L - 3) / 3;
+}
+
+#define DEL(Dp, l, m, mp) (Dp)[(size_t) (2 * (l) + 1) * ((mp) + (l)) + ((m) + (l))]
+
+__device__ __forceinline__ double rc_a(int l, int m, int mp) { return sqrt((double) (l + m) * (l - m) / ((double) (l + mp) * (l - mp))); }
+__device__ __forceinline__ double rc_b(int l, int m, int mp) { return sqrt((double) (l + m) * (l + m - 1) / (2.0 * (l + mp) * (l - mp))); }
+__device__ __forceinline__ double rc_c(int l, int m, int mp) { return sqrt(2.0 * (l + m) * (l - m) / ((double) (l + mp) * (l + mp - 1))); }
+__device__ __forceinline__ double rc_d(int l, int m, int mp) { return sqrt((double) (l + m) * (l + m - 1) / ((double) (l + mp) * (l + mp - 1))); }
+
+// One block per plan.  The l = 1 matrix (equations 5.3-5.5 of Choi et al.)
+// is built from R; level l is then computed from level l - 1 and level 1,
+// one element per thread, with a block barrier between levels.
+__global__ void k_rotation_plan(int l_max, const double *R_all, double2 *D_all, size_t plan_stride)
+{
+	__shared__ double2 d1[9];
+	const double *R = R_all + 9 * blockIdx.x;
+	double2 *Dall = D_all + plan_stride * blockIdx.x;
+	if(threadIdx.x == 0) {
+		enum { x = 0, y = 1, z = 2 };
+		const double s2 = sqrt(2.0);
+		// index (m, m') -> (m'+1)*3 + (m+1)
+		d1[0 * 3 + 0] = make_double2((R[3 * y + y] + R[3 * x + x]) / 2, -(R[3 * x + y] - R[3 * y + x]) / 2);  // (-1,-1)
+		d1[1 * 3 + 0] = make_double2(R[3 * z + x] / s2, -R[3 * z + y] / s2);                                    // (-1, 0)
+		d1[2 * 3 + 0] = make_double2((R[3 * y + y] - R[3 * x + x]) / 2, (R[3 * x + y] + R[3 * y + x]) / 2);   // (-1,+1)
+		d1[0 * 3 + 1] = make_double2(R[3 * x + z] / s2, R[3 * y + z] / s2);                                     // ( 0,-1)
+		d1[1 * 3 + 1] = make_double2(R[3 * z + z], 0.0);                                                        // ( 0, 0)
+		d1[2 * 3 + 1] = make_double2(-R[3 * x + z] / s2, R[3 * y + z] / s2);                                    // ( 0,+1)
+		d1[0 * 3 + 2] = make_double2((R[3 * y + y] - R[3 * x + x]) / 2, -(R[3 * x + y] + R[3 * y + x]) / 2);  // (+1,-1)
+		d1[1 * 3 + 2] = make_double2(-R[3 * z + x] / s2, -R[3 * z + y] / s2);                                   // (+1, 0)
+		d1[2 * 3 + 2] = make_double2((R[3 * y + y] + R[3 * x + x]) / 2, -(R[3 * y + x] - R[3 * x + y]) / 2);  // (+1,+1)
+		for(int k = 0; k < 9; k++)
+			Dall[k] = d1[k];
+	}
+	__syncthreads();
+	auto D1 = [&](int m, int mp) { return d1[(mp + 1) * 3 + (m + 1)]; };
+	for(int l = 2; l <= l_max; l++) {
+		const double2 *Dp = Dall + d_rot_offset(l - 1);
+		double2 *D = Dall + d_rot_offset(l);
+		const int w = 2 * l + 1;
+		const int lp = l - 1;
+		for(int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
+			const int m = idx % w - l;
+			const int mp = idx / w - l;
+			double2 v = make_double2(0, 0);
+			if(mp > -l && mp < l) {
+				// (6.1), (6.4), (6.5)
+				if(abs(m) != l) {
+					const double2 t = cmul(D1(0, 0), DEL(Dp, lp, m, mp));
+					const double c = rc_a(l, m, mp);
+					v.x += c * t.x;
+					v.y += c * t.y;
+				}
+				if(m > -l + 1) {
+					const double2 t = cmul(D1(1, 0), DEL(Dp, lp, m - 1, mp));
+					const double c = rc_b(l, m, mp);
+					v.x += c * t.x;
+					v.y += c * t.y;
+				}
+				if(-m > -l + 1) {
+					const double2 t = cmul(D1(-1, 0), DEL(Dp, lp, m + 1, mp));
+					const double c = rc_b(l, -m, mp);
+					v.x += c * t.x;
+					v.y += c * t.y;
+				}
+			} else if(mp == -l) {
+				// (6.9), (6.12), (6.13)
+				if(abs(m) != l) {
+					const double2 t = cmul(D1(0, -1), DEL(Dp, lp, m, mp + 1));
+					const double c = rc_c(l, m, -mp);
+					v.x += c * t.x;
+					v.y += c * t.y;
+				}
+				if(m > -l + 1) {
+					const double2 t = cmul(D1(1, -1), DEL(Dp, lp, m - 1, mp + 1));
+					const double c = rc_d(l, m, -mp);
+					v.x += c * t.x;
+					v.y += c * t.y;
+				}
+				if(-m > -l + 1) {
+					const double2 t = cmul(D1(-1, -1), DEL(Dp, lp, m + 1, mp + 1));
+					const double c = rc_d(l, -m, -mp);
+					v.x += c * t.x;
+					v.y += c * t.y;
+				}
+			} else {
+				// mp == l: (6.14), (6.12), (6.13)
+				if(abs(m) != l) {
+					const double2 t = cmul(D1(0, 1), DEL(Dp, lp, m, mp - 1));
+					const double c = rc_c(l, m, mp);
+					v.x += c * t.x;
+					v.y += c * t.y;
+				}
+				if(m > -l + 1) {
+					const double2 t = cmul(D1(1, 1), DEL(Dp, lp, m - 1, mp - 1));
+					const double c = rc_d(l, m, mp);
+					v.x += c * t.x;
+					v.y += c * t.y;
+				}
+				if(-m > -l + 1) {
+					const double2 t = cmul(D1(-1, 1), DEL(Dp, lp, m + 1, mp - 1));
+					const double c = rc_d(l, -m, mp);
+					v.x += c * t.x;
+					v.y += c * t.y;
+				}
+			}
+			D[idx] = v;
+		}
+		__syncthreads();
+	}
+}
+
+int build_rotation_plan(unsigned l_max, const double *R, double *D_host)
+{
+	if(l_max == 0)
+		return 0;
+	if(ensure_device())
+		return -1;
+	const size_t len = rot_offset(l_max + 1);
+	DBuf dR(9 * sizeof(double));
+	DBuf dD(len * sizeof(double2));
+	if(!dR.p || !dD.p)
+		return -1;
+	if(h2d(dR.p, R, 9 * sizeof(double)))
+		return -1;
+	k_rotation_plan<<<1, 1024, 0, S()>>>((int) l_max, dR.as<double>(), dD.as<double2>(), len);
+	CK(cudaGetLastError());
+	if(d2h(D_host, dD.p, len * sizeof(double2)))
+		return -1;
+	return stream_sync();
+}
+
+// ------------------------------------------------------------------------
+// rotation of one series (sh_series_rotation.c:546-589)
+// ------------------------------------------------------------------------
+// grid over m' + l_max, threads over l >= |m'|.  Polar input: c'_{l m'} =
+// D^l_{0 m'} c_l.  Otherwise c'_{l m'} = sum_m D^l_{m m'} c_{l m}.
+__device__ __forceinline__ size_t d_lmoffset(int L, int l, int m)
+{
+	const long long LL = L + 1;
+	const long long x = (long long) m * (m - 1);
+	const long long mo = (m >= 0) ? LL * m - x / 2 : LL * (LL + m) + x / 2;
+	return (size_t) (mo + l - abs(m));
+}
+
+__global__ void k_rotate(int L, int polar, const double2 *Dall, const double2 *in, double2 *out)
+{
+	const int mp = (int) blockIdx.x - L;
+	for(int l = abs(mp) + threadIdx.x; l <= L; l += blockDim.x) {
+		double2 c;
+		if(l == 0)
+			c = in[0];
+		else {
+			const double2 *D = Dall + d_rot_offset(l);
+			if(polar)
+				c = cmul(DEL(D, l, 0, mp), in[l]);
+			else {
+				c = make_double2(0, 0);
+				for(int m = -l; m <= l; m++) {
+					const double2 t = cmul(DEL(D, l, m, mp), in[d_lmoffset(L, l, m)]);
+					c.x += t.x;
+					c.y += t.y;
+				}
+			}
+		}
+		out[d_lmoffset(L, l, mp)] = c;
+	}
+}
+
+struct RotMirror {
+	uint64_t gen = 0;
+	unsigned l_max = 0;
+	double2 *D = nullptr;
+};
+static std::mutex g_rot_mu;
+static std::unordered_map<const void *, RotMirror> g_rot_cache;
+
+void forget_rot_mirror(const void *key)
+{
+	std::lock_guard<std::mutex> lk(g_rot_mu);
+	auto it = g_rot_cache.find(key);
+	if(it != g_rot_cache.end()) {
+		dfree(it->second.D);
+		g_rot_cache.erase(it);
+	}
+}
+
+int rotate_series(unsigned l_max, int polar, const double *series, const double *Dflat, const void *cache_key, uint64_t gen, double *result)
+{
+	if(ensure_device())
+		return -1;
+	const size_t len = rot_offset(l_max + 1);
+	double2 *dD = nullptr;
+	{
+		std::lock_guard<std::mutex> lk(g_rot_mu);
+		RotMirror &m = g_rot_cache[cache_key];
+		if(!m.D || m.gen != gen || m.l_max != l_max) {
+			dfree(m.D);
+			m.D = (double2 *) dmalloc((len ? len : 1) * sizeof(double2));
+			if(!m.D)
+				return -1;
+			if(len && h2d(m.D, Dflat, len * sizeof(double2)))
+				return -1;
+			m.gen = gen;
+			m.l_max = l_max;
+		}
+		dD = m.D;
+	}
+	const size_t in_len = polar ? l_max + 1 : (size_t) (l_max + 1) * (l_max + 1);
+	const size_t out_len = (size_t) (l_max + 1) * (l_max + 1);
+	DBuf din(in_len * sizeof(double2)), dout(out_len * sizeof(double2));
+	if(!din.p || !dout.p)
+		return -1;
+	if(h2d(din.p, series, in_len * sizeof(double2)))
+		return -1;
+	k_rotate<<<2 * l_max + 1, 64, 0, S()>>>((int) l_max, polar, dD, din.as<double2>(), dout.as<double2>());
+	CK(cudaGetLastError());
+	if(d2h(result, dout.p, out_len * sizeof(double2)))
+		return -1;
+	return stream_sync();
+}
+
+// ------------------------------------------------------------------------
+// FP64 frequency-domain integration (correlator.c:681-711, 993-1010)
+// ------------------------------------------------------------------------
+struct DevJob {
+	const double2 *a, *b;   // spectra
+	const double2 *D;       // n x stride delay table
+	const double2 *rot;     // polar: rows D^l_{0 m'} at offset l^2; else full flat plan
+	double2 *X;             // cross spectrum out (n)
+	double2 *P;             // sum_k X D (stride), zeroed before the launch
+	int n, stride, l_max, polar;
+	double weight;
+};
+
+constexpr int XS_CHUNK = 64;
+
+// cross-spectrum X[k] = b[k] conj(a[k]) and P[j] += sum_k X[k] D[k][j] over
+// a chunk of bins (sh_series_array.c:437-456 inner loop order transposed)
+__global__ void k_xspec_dot(const DevJob *jobs)
+{
+	const DevJob J = jobs[blockIdx.y];
+	const int k0 = blockIdx.x * XS_CHUNK;
+	if(k0 >= J.n)
+		return;
+	__shared__ double2 s_x[XS_CHUNK];
+	const int kc = min(XS_CHUNK, J.n - k0);
+	for(int k = threadIdx.x; k < kc; k += blockDim.x) {
+		const double2 v = cmulc(J.b[k0 + k], J.a[k0 + k]);
+		s_x[k] = v;
+		if(J.X)
+			J.X[k0 + k] = v;
+	}
+	__syncthreads();
+	for(int j = threadIdx.x; j < J.stride; j += blockDim.x) {
+		double2 acc = make_double2(0, 0);
+		const double2 *d = J.D + (size_t) k0 * J.stride + j;
+		for(int k = 0; k < kc; k++) {
+			const double2 t = cmul(d[(size_t) k * J.stride], s_x[k]);
+			acc.x += t.x;
+			acc.y += t.y;
+		}
+		atomicAdd(&J.P[j].x, acc.x);
+		atomicAdd(&J.P[j].y, acc.y);
+	}
+}
+
+// sky_{l m'} = sum_b weight_b / n_b * (rotated P_b)_{l m'}; also rescales
+// P_b to power_1d = P_b / n_b (grid: m' + L, threads over l)
+__global__ void k_rotate_sum(const DevJob *jobs, int n_jobs, int L, double2 *sky)
+{
+	const int mp = (int) blockIdx.x - L;
+	for(int l = abs(mp) + threadIdx.x; l <= L; l += blockDim.x) {
+		double2 acc = make_double2(0, 0);
+		for(int b = 0; b < n_jobs; b++) {
+			const DevJob &J = jobs[b];
+			if(l > J.l_max)
+				continue;
+			const double s = J.weight / J.n;
+			double2 c;
+			if(l == 0)
+				c = J.P[0];
+			else if(J.polar)
+				c = cmul(J.rot[(size_t) l * l + (mp + l)], J.P[l]);
+			else {
+				c = make_double2(0, 0);
+				const double2 *D = J.rot + d_rot_offset(l);
+				for(int m = -l; m <= l; m++) {
+					const double2 t = cmul(DEL(D, l, m, mp), J.P[d_lmoffset(J.l_max, l, m)]);
+					c.x += t.x;
+					c.y += t.y;
+				}
+			}
+			acc.x += s * c.x;
+			acc.y += s * c.y;
+		}
+		sky[d_lmoffset(L, l, mp)] = acc;
+	}
+}
+
+__global__ void k_scale_power(const DevJob *jobs, double2 *out, int out_stride)
+{
+	const DevJob J = jobs[blockIdx.x];
+	for(int j = threadIdx.x; j < J.stride; j += blockDim.x) {
+		const double2 p = J.P[j];
+		out[(size_t) blockIdx.x * out_stride + j] = make_double2(p.x / J.n, p.y / J.n);
+	}
+}
+
+// device mirror of a plan: delay table and rotation data
+struct PlanMirror {
+	uint64_t gen = ~0ull;
+	const double *D_host = nullptr;
+	const double *rot_host = nullptr;
+	int n = 0, stride = 0, polar = -1;
+	unsigned l_max = 0;
+	double2 *D = nullptr;
+	double2 *rot = nullptr;
+};
+static std::mutex g_mir_mu;
+static std::unordered_map<const void *, PlanMirror> g_mirrors;
+
+void forget_mirror(const void *key)
+{
+	std::lock_guard<std::mutex> lk(g_mir_mu);
+	auto it = g_mirrors.find(key);
+	if(it != g_mirrors.end()) {
+		dfree(it->second.D);
+		dfree(it->second.rot);
+		g_mirrors.erase(it);
+	}
+}
+
+static int refresh_mirror(const BaselineJob &j, PlanMirror &m)
+{
+	if(m.D && m.gen == j.gen && m.D_host == j.D && m.rot_host == j.rot && m.n == j.n && m.stride == j.stride && m.l_max == j.l_max && m.polar == j.polar)
+		return 0;
+	dfree(m.D);
+	dfree(m.rot);
+	m.D = m.rot = nullptr;
+	m.D = (double2 *) dmalloc((size_t) j.n * j.stride * sizeof(double2));
+	if(!m.D)
+		return -1;
+	if(h2d(m.D, j.D, (size_t) j.n * j.stride * sizeof(double2)))
+		return -1;
+	if(j.polar) {
+		// rows D^l_{0 m'} at offset l^2, l = 0 row is 1
+		const size_t rl = (size_t) (j.l_max + 1) * (j.l_max + 1);
+		std::vector<double> rows(2 * rl, 0.0);
+		rows[0] = 1.0;
+		for(unsigned l = 1; l <= j.l_max; l++) {
+			const double *Dl = j.rot + 2 * rot_offset(l);
+			for(int mp = -(int) l; mp <= (int) l; mp++) {
+				const size_t e = (size_t) (2 * l + 1) * (mp + l) + (0 + l);
+				rows[2 * ((size_t) l * l + mp + l)] = Dl[2 * e];
+				rows[2 * ((size_t) l * l + mp + l) + 1] = Dl[2 * e + 1];
+			}
+		}
+		m.rot = (double2 *) dmalloc(rl * sizeof(double2));
+		if(!m.rot || h2d(m.rot, rows.data(), rl * sizeof(double2)) || stream_sync())
+			return -1;
+	} else {
+		const size_t len = rot_offset(j.l_max + 1);
+		m.rot = (double2 *) dmalloc((len ? len : 1) * sizeof(double2));
+		if(!m.rot || (len && h2d(m.rot, j.rot, len * sizeof(double2))))
+			return -1;
+	}
+	m.gen = j.gen;
+	m.D_host = j.D;
+	m.rot_host = j.rot;
+	m.n = j.n;
+	m.stride = j.stride;
+	m.l_max = j.l_max;
+	m.polar = j.polar;
+	return 0;
+}
+
+int integrate_fd(const BaselineJob *jobs, int n_jobs, unsigned sky_l_max, double *sky)
+{
+	if(ensure_device())
+		return -1;
+	if(n_jobs <= 0) {
+		set_error("integrate_fd: no baselines");
+		return -1;
+	}
+	std::vector<DevJob> dj(n_jobs);
+	// unique input spectra (the network shares detectors between baselines)
+	std::vector<const double *> uniq;
+	std::vector<int> uniq_n;
+	auto find_or_add = [&](const double *p, int n) {
+		for(size_t i = 0; i < uniq.size(); i++)
+			if(uniq[i] == p && uniq_n[i] == n)
+				return (int) i;
+		uniq.push_back(p);
+		uniq_n.push_back(n);
+		return (int) uniq.size() - 1;
+	};
+	std::vector<int> ia(n_jobs), ib(n_jobs);
+	size_t spec_total = 0, x_total = 0, p_total = 0;
+	int max_n = 0, max_stride = 0;
+	for(int i = 0; i < n_jobs; i++) {
+		const BaselineJob &J = jobs[i];
+		if(J.n <= 0 || J.stride <= 0 || J.l_max > sky_l_max) {
+			set_error("integrate_fd: bad baseline job %d", i);
+			return -1;
+		}
+		ia[i] = find_or_add(J.a, J.n);
+		ib[i] = find_or_add(J.b, J.n);
+		x_total += J.n;
+		p_total += J.stride;
+		max_n = J.n > max_n ? J.n : max_n;
+		max_stride = J.stride > max_stride ? J.stride : max_stride;
+	}
+	for(size_t i = 0; i < uniq.size(); i++)
+		spec_total += uniq_n[i];
+	const size_t sky_len = (size_t) (sky_l_max + 1) * (sky_l_max + 1);
+	DBuf spec(spec_total * sizeof(double2)), X(x_total * sizeof(double2)), P(p_total * sizeof(double2));
+	DBuf pw((size_t) n_jobs * max_stride * sizeof(double2)), dsky(sky_len * sizeof(double2)), djobs(n_jobs * sizeof(DevJob));
+	if(!spec.p || !X.p || !P.p || !pw.p || !dsky.p || !djobs.p)
+		return -1;
+	std::vector<size_t> uoff(uniq.size());
+	{
+		size_t o = 0;
+		for(size_t i = 0; i < uniq.size(); i++) {
+			uoff[i] = o;
+			if(h2d(spec.as<double2>() + o, uniq[i], uniq_n[i] * sizeof(double2)))
+				return -1;
+			o += uniq_n[i];
+		}
+	}
+	size_t xo = 0, po = 0;
+	{
+		std::lock_guard<std::mutex> lk(g_mir_mu);
+		for(int i = 0; i < n_jobs; i++) {
+			const BaselineJob &J = jobs[i];
+			PlanMirror &m = g_mirrors[J.key];
+			if(refresh_mirror(J, m))
+				return -1;
+			DevJob &d = dj[i];
+			d.a = spec.as<double2>() + uoff[ia[i]];
+			d.b = spec.as<double2>() + uoff[ib[i]];
+			d.D = m.D;
+			d.rot = m.rot;
+			d.X = X.as<double2>() + xo;
+			d.P = P.as<double2>() + po;
+			d.n = J.n;
+			d.stride = J.stride;
+			d.l_max = (int) J.l_max;
+			d.polar = J.polar;
+			d.weight = J.weight;
+			xo += J.n;
+			po += J.stride;
+		}
+	}
+	if(h2d(djobs.p, dj.data(), n_jobs * sizeof(DevJob)) || dmemset(P.p, 0, p_total * sizeof(double2)))
+		return -1;
+	dim3 g1((max_n + XS_CHUNK - 1) / XS_CHUNK, n_jobs);
+	k_xspec_dot<<<g1, 128, 0, S()>>>(djobs.as<DevJob>());
+	k_rotate_sum<<<2 * sky_l_max + 1, 64, 0, S()>>>(djobs.as<DevJob>(), n_jobs, (int) sky_l_max, dsky.as<double2>());
+	k_scale_power<<<n_jobs, 128, 0, S()>>>(djobs.as<DevJob>(), pw.as<double2>(), max_stride);
+	CK(cudaGetLastError());
+	if(d2h(sky, dsky.p, sky_len * sizeof(double2)))
+		return -1;
+	xo = 0;
+	for(int i = 0; i < n_jobs; i++) {
+		const BaselineJob &J = jobs[i];
+		if(J.power_1d && d2h(J.power_1d, pw.as<double2>() + (size_t) i * max_stride, J.stride * sizeof(double2)))
+			return -1;
+		if(J.fseries_product && d2h(J.fseries_product, X.as<double2>() + xo, J.n * sizeof(double2)))
+			return -1;
+		xo += J.n;
+	}
+	return stream_sync();
+}
+
+// ------------------------------------------------------------------------
+// array contraction (sh_series_array.c:404-456)
+// ------------------------------------------------------------------------
+__global__ void k_array_dot(int n, int stride, const double2 *coeff, const double2 *vec, double2 *out)
+{
+	const int k0 = blockIdx.x * XS_CHUNK;
+	const int kc = min(XS_CHUNK, n - k0);
+	__shared__ double2 s_v[XS_CHUNK];
+	for(int k = threadIdx.x; k < kc; k += blockDim.x)
+		s_v[k] = vec[k0 + k];
+	__syncthreads();
+	for(int j = threadIdx.x; j < stride; j += blockDim.x) {
+		double2 acc = make_double2(0, 0);
+		for(int k = 0; k < kc; k++) {
+			const double2 t = cmul(coeff[(size_t) (k0 + k) * stride + j], s_v[k]);
+			acc.x += t.x;
+			acc.y += t.y;
+		}
+		atomicAdd(&out[j].x, acc.x);
+		atomicAdd(&out[j].y, acc.y);
+	}
+}
+
+int array_dotc(int n, int stride, const double *coeff, const double *vec, int vec_is_complex, double *result)
+{
+	if(ensure_device())
+		return -1;
+	if(n <= 0) {
+		memset(result, 0, stride * sizeof(double2));
+		return 0;
+	}
+	DBuf dc((size_t) n * stride * sizeof(double2)), dv((size_t) n * sizeof(double2)), dout(stride * sizeof(double2));
+	if(!dc.p || !dv.p || !dout.p)
+		return -1;
+	std::vector<double> v2;
+	const double *vp = vec;
+	if(!vec_is_complex) {
+		v2.assign(2 * (size_t) n, 0.0);
+		for(int k = 0; k < n; k++)
+			v2[2 * k] = vec[k];
+		vp = v2.data();
+	}
+	if(h2d(dc.p, coeff, (size_t) n * stride * sizeof(double2)) || h2d(dv.p, vp, n * sizeof(double2)) || dmemset(dout.p, 0, stride * sizeof(double2)))
+		return -1;
+	k_array_dot<<<(n + XS_CHUNK - 1) / XS_CHUNK, 128, 0, S()>>>(n, stride, dc.as<double2>(), dv.as<double2>(), dout.as<double2>());
+	CK(cudaGetLastError());
+	if(d2h(result, dout.p, stride * sizeof(double2)))
+		return -1;
+	return stream_sync();
+}
+
+}  // namespace sphrad

@@ -148,6 +148,51 @@ def whitened_segment(positions, n: int, dt: float, theta: float, phi: float, snr
     return full
 
 
+def make_batch(positions, n: int, dt: float, n_seg: int, seed: int, snr_range=(6.0, 30.0)):
+    """A batch of whitened segments, vectorised over segments.
+
+    Per segment: an isotropic source direction (Earth-fixed theta, phi), an
+    SNR uniform in ``snr_range`` and a GMST uniform in [0, 2 pi).  Each
+    detector sees coloured Gaussian noise of PSD S(f) plus the chirp
+    delayed by r_det . s (the periodic FFT delay of inject.c:119-152,
+    applied as a phase ramp on the chirp's spectrum), whitened by
+    1/sqrt(S) in the 20-1000 Hz band.  Returns a dict with ``F``
+    (n_det x n_seg x (n/2+1) complex128), ``theta``, ``phi``, ``snr`` and
+    ``gmst`` (n_seg each)."""
+    rng = rng_for(seed)
+    pos = np.asarray(positions, np.float64)
+    nd = len(pos)
+    K = n // 2 + 1
+    k = np.arange(K)
+    f = k / (n * dt)
+    S = psd(f)
+    inband = S > 0
+    wh = np.zeros_like(S)
+    wh[inband] = 1.0 / np.sqrt(S[inband])
+    sigma = np.sqrt(S * n / (2 * dt) / 2.0)
+    h = chirp(n, dt)
+    Hf = np.fft.rfft(h)
+    rho1 = np.sqrt(4.0 * np.sum(np.abs(Hf[inband] * dt) ** 2 / S[inband]) / (n * dt))
+    theta = np.arccos(rng.uniform(-1, 1, n_seg))
+    phi = rng.uniform(0, 2 * np.pi, n_seg)
+    snr = rng.uniform(snr_range[0], snr_range[1], n_seg)
+    gmst = rng.uniform(0, 2 * np.pi, n_seg)
+    s_hat = np.stack([np.sin(theta) * np.cos(phi), np.sin(theta) * np.sin(phi), np.cos(theta)], axis=1)
+    tau = s_hat @ pos.T                                   # n_seg x n_det, r . s
+    F = np.empty((nd, n_seg, K), np.complex128)
+    amp = snr / rho1
+    for d in range(nd):
+        nz = sigma[None, :] * (rng.normal(size=(n_seg, K)) + 1j * rng.normal(size=(n_seg, K)))
+        nz[:, 0] = nz[:, 0].real
+        if n % 2 == 0:
+            nz[:, -1] = nz[:, -1].real
+        sig = (amp[:, None] * Hf[None, :]) * np.exp(1j * 2 * np.pi * np.outer(tau[:, d], k) / (dt * n))
+        if n % 2 == 0:
+            sig[:, -1] = sig[:, -1].real   # c2r drops the Nyquist imaginary part
+        F[d] = (nz + sig) * wh[None, :]
+    return dict(F=F, theta=theta, phi=phi, snr=snr, gmst=gmst)
+
+
 def full_from_half(half, n: int) -> np.ndarray:
     """Hermitian completion of n/2+1 bins to n bins (last axis)."""
     half = np.asarray(half)

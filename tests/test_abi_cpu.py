@@ -1,0 +1,119 @@
+"""CPU-side checks of libsphradiometer_b200 (no GPU needed).
+
+* the library loads and exports every function that include/*.h declares;
+* host bookkeeping functions (assign, resize, add, conj, real/imag,
+  rotate_z, eval, impulse, Y) agree with the oracle;
+* GPU-backed entry points fail loudly (NULL plus an error message) when no
+  CUDA device is present, rather than falling back to host code.
+"""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def S():
+    import sphradiometer_b200 as S
+    from sphradiometer_b200 import build
+    build.build()
+    S.load()
+    return S
+
+
+def declared_functions():
+    names = set()
+    for dp, _, fs in os.walk(os.path.join(ROOT, "include")):
+        for f in fs:
+            if not f.endswith(".h"):
+                continue
+            src = open(os.path.join(dp, f)).read()
+            src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+            src = re.sub(r"static inline[^{]*\{.*?\n\}", "", src, flags=re.S)
+            for m in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b([a-z_][a-z0-9_]*)\s*\([^;{]*\)\s*;", src, flags=re.M):
+                names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_function(S):
+    lib = S.load()
+    names = declared_functions()
+    assert len(names) > 80
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def _rand(rng, l_max, polar):
+    n = O.length(l_max, polar)
+    return rng.normal(size=n) + 1j * rng.normal(size=n)
+
+
+def test_host_bookkeeping_matches_oracle(S):
+    L = S.load()
+    rng = np.random.default_rng(1)
+    for polar in (0, 1):
+        a = _rand(rng, 9, polar)
+        s = S.numpy_to_series(a, 9, polar)
+        # resize up and down (sh_series.c:200-233)
+        L.sh_series_resize(s, 13)
+        assert np.allclose(S.series_to_numpy(s), O.assign(a, 9, polar, 13, polar), atol=0, rtol=0)
+        L.sh_series_resize(s, 5)
+        assert np.array_equal(S.series_to_numpy(s), O.assign(a, 9, polar, 5, polar))
+        L.sh_series_free(s)
+    a = _rand(rng, 11, 0)
+    for fn, ref in (("sh_series_conj", lambda x: O.conj(x, 11, False)),):
+        s = S.numpy_to_series(a, 11, 0)
+        getattr(L, fn)(s)
+        assert np.allclose(S.series_to_numpy(s), ref(a), rtol=0, atol=1e-15)
+        L.sh_series_free(s)
+    # real + i imag reproduces the function (sh_series.c:487-600)
+    s1, s2 = S.numpy_to_series(a, 11, 0), S.numpy_to_series(a, 11, 0)
+    L.sh_series_real(s1)
+    L.sh_series_imag(s2)
+    r, i = S.series_to_numpy(s1), S.series_to_numpy(s2)
+    assert np.allclose(r + 1j * i, a, atol=1e-14)
+    for t, p in ((0.3, 1.2), (2.9, 5.0)):
+        assert abs(np.imag(O.eval_at(r, 11, False, t, p))) < 1e-12
+    L.sh_series_free(s1)
+    L.sh_series_free(s2)
+    # rotate_z, eval, impulse, Y
+    s = S.numpy_to_series(a, 11, 0)
+    L.sh_series_rotate_z(s, s, 0.7)
+    assert np.allclose(S.series_to_numpy(s), O.rotate_z(a, 11, False, 0.7), atol=1e-14)
+    v = L.sh_series_eval(s, 1.0, 2.0)
+    ref = O.eval_at(O.rotate_z(a, 11, False, 0.7), 11, False, 1.0, 2.0)
+    assert abs(complex(v.re, v.im) - ref) < 1e-12
+    L.sh_series_free(s)
+    imp = L.sh_series_impulse(10, 0.4, 1.9)
+    assert np.allclose(S.series_to_numpy(imp), O.impulse(10, 0.4, 1.9), atol=1e-14)
+    L.sh_series_free(imp)
+    y = L.sh_series_Y(7, -3, 0.8, 0.2)
+    assert abs(complex(y.re, y.im) - O.Y(7, -3, 0.8, 0.2)) < 1e-14
+
+
+def test_add_checks_shapes(S):
+    L = S.load()
+    a = L.sh_series_new_zero(4, 1)
+    b = L.sh_series_new_zero(6, 0)
+    assert not L.sh_series_add(a, S._abi.cplx(1.0), b)  # lossy: refused
+    assert L.sh_series_add(b, S._abi.cplx(1.0), a)
+    L.sh_series_free(a)
+    L.sh_series_free(b)
+
+
+@pytest.mark.skipif(__import__("torch").cuda.is_available(), reason="checks the no-GPU behaviour")
+def test_gpu_entry_points_fail_loudly_without_a_device(S):
+    L = S.load()
+    s = L.sh_series_new_zero(4, 0)
+    R = L.euler_rotation_matrix(0.1, 0.2, 0.3)
+    assert not L.sh_series_rotation_plan_new(s, R)
+    assert "CUDA" in S.last_error() or "device" in S.last_error()
+    L.sh_series_free(s)
+    with pytest.raises(S.SphradError):
+        S.Network(np.array([[0, 0, 0.001], [0.001, 0, 0]]), 64, 1.0 / 256, l_max=2)

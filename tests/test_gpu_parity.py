@@ -1,0 +1,246 @@
+"""GPU parity of libsphradiometer_b200 against the CPU oracle.
+
+Every test calls the library through its C ABI (ctypes) and compares with
+the FP64 oracle on the same seeded inputs.  Tolerances:
+* FP64 paths (plans, rotation, the drop-in integrator, the FP64 batch):
+  relative L2 <= 1e-10 (rounding differs only in summation order);
+* FP32 batch: relative L2 <= 1e-5;
+* bf16x3 (tcgen05) batch: relative L2 <= 1e-5 per sky, the accuracy target
+  of the split-precision path.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from sphradiometer_b200 import workload as W
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    import torch
+    assert torch.cuda.is_available()
+    import sphradiometer_b200 as S
+    S.load()
+    return S
+
+
+def c0_positions(seed=1):
+    return W.pair_positions(3.0e6 / W.C_LIGHT, W.rng_for(seed))
+
+
+def c1_positions(seed=2):
+    return W.random_positions(3, W.R_EARTH_S, W.rng_for(seed))
+
+
+# ---------------------------------------------------------------- plans --
+
+def test_rotation_plan_matches_oracle(lib):
+    L = lib.load()
+    rng = np.random.default_rng(3)
+    for l_max in (1, 7, 20, 48):
+        g, b, a = rng.uniform(0, 2 * np.pi), np.arccos(rng.uniform(-1, 1)), rng.uniform(0, 2 * np.pi)
+        s = L.sh_series_new_zero(l_max, 0)
+        R = L.euler_rotation_matrix(g, b, a)
+        p = L.sh_series_rotation_plan_new(s, R)
+        assert p, lib.last_error()
+        got = lib.rotation_plan_flat(p)
+        ref = O.rotation_plan(l_max, O.euler_rotation_matrix(g, b, a))
+        assert rel_l2(got, ref) < 1e-12
+        L.sh_series_rotation_plan_free(p)
+        L.sh_series_free(s)
+
+
+def test_delay_table_matches_oracle(lib):
+    pos = c0_positions()
+    dt = 1.0 / 2048
+    net = lib.Network(pos, 2048, dt, l_max=25)
+    d = pos[1] - pos[0]
+    ref = O.delay_product(float(np.linalg.norm(d)), dt, 2048, 25)
+    got = net.delay_table(0)
+    assert got.shape == ref.shape
+    assert rel_l2(got, ref) < 1e-10
+    net.close()
+
+
+def test_native_plan_then_set_l_equals_direct_plan(lib):
+    """correlator_plan_fd_new + set_l (the reference's route) equals the
+    direct correlator_plan_fd_new_l build."""
+    pos = W.pair_positions(0.002, W.rng_for(5))
+    dt = 1.0 / 1024
+    a = lib.Network(pos, 256, dt)            # native l_max
+    a.set_l(6)
+    b = lib.Network(pos, 256, dt, l_max=6)
+    assert a.baseline_l_max(0) == 6 and b.baseline_l_max(0) == 6
+    assert np.max(np.abs(a.delay_table(0) - b.delay_table(0))) < 1e-13 * np.max(np.abs(b.delay_table(0)))
+    assert np.max(np.abs(a.rotation_flat(0) - b.rotation_flat(0))) < 1e-14
+    a.close()
+    b.close()
+
+
+# ------------------------------------------------------------- rotation --
+
+@pytest.mark.parametrize("polar", [True, False])
+def test_rotate_matches_oracle(lib, polar):
+    L = lib.load()
+    rng = np.random.default_rng(11)
+    l_max = 20
+    n = lib.series_length(l_max, polar)
+    a = rng.normal(size=n) + 1j * rng.normal(size=n)
+    s = lib.numpy_to_series(a, l_max, polar)
+    res = L.sh_series_new(l_max, 0)
+    R = L.euler_rotation_matrix(0.3, 1.1, 2.0)
+    p = L.sh_series_rotation_plan_new(res, R)
+    assert L.sh_series_rotate(res, s, p), lib.last_error()
+    ref = O.rotate(a, l_max, polar, O.rotation_plan(l_max, O.euler_rotation_matrix(0.3, 1.1, 2.0)))
+    assert rel_l2(lib.series_to_numpy(res), ref) < 1e-12
+    # result == series is refused, as in the reference
+    assert not L.sh_series_rotate(res, res, p)
+    for x in (s, res):
+        L.sh_series_free(x)
+    L.sh_series_rotation_plan_free(p)
+
+
+# ------------------------------------------------------ drop-in integrator --
+
+def test_network_integrate_c0_matches_oracle(lib):
+    """c0: two detectors 3000 km apart, 1 s at 2048 Hz, l_max = 25."""
+    pos = c0_positions()
+    n, dt, L = 2048, 1.0 / 2048, 25
+    net = lib.Network(pos, n, dt, l_max=L)
+    batch = W.make_batch(pos, n, dt, 1, seed=21)
+    F = W.full_from_half(batch["F"][:, 0, :], n)
+    got = net.integrate(F)
+    b = dict(D=net.delay_table(0), Rot=net.rotation_flat(0))
+    ref = O.baseline_integrate_power_fd(F[1], F[0], b["D"], L, b["Rot"])
+    assert rel_l2(got, ref) < 1e-10
+    # and the oracle's own plan gives the same sky
+    ref2 = O.NetworkPlan(pos, n, dt, L).integrate(F)
+    assert rel_l2(got, ref2) < 1e-9
+    net.close()
+
+
+def test_baseline_integrate_side_effects(lib):
+    """power_1d holds the normalised polar power and fseries_product the
+    cross spectrum after the call (correlator.c:681-711)."""
+    pos = c0_positions()
+    n, dt, L = 512, 1.0 / 512, 8
+    net = lib.Network(pos, n, dt, l_max=L)
+    rng = np.random.default_rng(4)
+    a = rng.normal(size=n) + 1j * rng.normal(size=n)
+    b = rng.normal(size=n) + 1j * rng.normal(size=n)
+    sky = net.integrate_baseline(0, a, b)
+    D = net.delay_table(0)
+    p1 = (b * np.conj(a)) @ D / n
+    plan = net.plan_fd(0).contents
+    assert rel_l2(lib.series_to_numpy(plan.power_1d), p1) < 1e-12
+    fsp = np.frombuffer((np.ctypeslib.as_array((__import__("ctypes").c_double * (2 * n)).from_address(plan.fseries_product))),
+                        dtype=np.complex128)
+    assert rel_l2(fsp, b * np.conj(a)) < 1e-15
+    ref = O.rotate(p1, L, True, net.rotation_flat(0))
+    assert rel_l2(sky, ref) < 1e-12
+    net.close()
+
+
+def test_mirror_refresh_after_in_place_edit(lib):
+    """Writing into delay_product through the library is seen by the next
+    integration (fastX.c:485-487 edits plans in place)."""
+    L = lib.load()
+    pos = c0_positions()
+    n, dt = 256, 1.0 / 256
+    net = lib.Network(pos, n, dt, l_max=4)
+    rng = np.random.default_rng(8)
+    F = rng.normal(size=(2, n)) + 1j * rng.normal(size=(2, n))
+    first = net.integrate(F)
+    dp = net.plan_fd(0).contents.delay_product
+    L.sh_series_scale(__import__("ctypes").byref(dp.contents.series[3]), lib._abi.cplx(5.0))
+    second = net.integrate(F)
+    D = net.delay_table(0)
+    ref = O.baseline_integrate_power_fd(F[1], F[0], D, 4, net.rotation_flat(0))
+    assert rel_l2(second, ref) < 1e-12
+    assert rel_l2(second, first) > 1e-6
+    net.close()
+
+
+# -------------------------------------------------------- batched path --
+
+@pytest.fixture(scope="module")
+def c1(lib):
+    """c1: 3 detectors on the Earth sphere, 64 x 1 s segments at 4096 Hz,
+    l_max = 32."""
+    pos = c1_positions()
+    n, dt, L = 4096, 1.0 / 4096, 32
+    net = lib.Network(pos, n, dt, l_max=L)
+    batch = W.make_batch(pos, n, dt, 64, seed=77)
+    # oracle skies on the library's delay tables (the tables themselves are
+    # checked against the oracle above)
+    tabs = [(net.delay_table(k), net.rotation_flat(k)) for k in range(3)]
+    pairs = [(1, 0), (2, 0), (2, 1)]
+    ref = np.zeros((64, (L + 1) ** 2), np.complex128)
+    for s in range(64):
+        F = W.full_from_half(batch["F"][:, s, :], n)
+        for k, (i, j) in enumerate(pairs):
+            ref[s] += O.baseline_integrate_power_fd(F[i], F[j], tabs[k][0], L, tabs[k][1]) / 3
+        ref[s] = O.rotate_z(ref[s], L, False, batch["gmst"][s])
+    return dict(net=net, batch=batch, ref=ref, n=n, L=L)
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-10), ("fp32", 1e-5), ("bf16x3", 1e-5)])
+def test_batched_matches_oracle(lib, c1, prec, tol):
+    import torch
+    bp = lib.BatchPlan(c1["net"], prec)
+    F = torch.from_numpy(np.ascontiguousarray(c1["batch"]["F"])).cuda()
+    g = torch.from_numpy(c1["batch"]["gmst"]).cuda()
+    sky = bp.integrate(F, g).cpu().numpy()
+    assert bp.status() == 0
+    errs = [rel_l2(sky[s], c1["ref"][s]) for s in range(64)]
+    assert max(errs) < tol, (prec, max(errs))
+    # a second call on the re-zeroed workspace gives the same answer
+    sky2 = bp.integrate(F, g).cpu().numpy()
+    assert rel_l2(sky2, sky) < (1e-12 if prec == "fp64" else 1e-6)
+    bp.close()
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16x3"])
+def test_batched_ragged_sizes_and_splits(lib, c1, prec):
+    """Segment counts that do not fill a tile, padded rows, every split."""
+    import torch
+    bp = lib.BatchPlan(c1["net"], prec)
+    K = c1["n"] // 2 + 1
+    for S in (1, 5, 64):
+        Fh = np.zeros((3, S, K + 7), np.complex128)
+        Fh[:, :, :K] = c1["batch"]["F"][:, :S, :]
+        F = torch.from_numpy(Fh).cuda()
+        g = torch.from_numpy(c1["batch"]["gmst"][:S].copy()).cuda()
+        for split in (1, 3, 17):
+            bp.set_split(S, split)
+            sky = bp.integrate(F, g).cpu().numpy()
+            assert max(rel_l2(sky[s], c1["ref"][s]) for s in range(S)) < 1e-5, (S, split)
+    assert bp.status() == 0
+    bp.close()
+
+
+def test_batched_host_entry_point(lib, c1):
+    bp = lib.BatchPlan(c1["net"], "bf16x3")
+    Fh = np.ascontiguousarray(c1["batch"]["F"])
+    sky = bp.integrate_host(Fh, c1["batch"]["gmst"])
+    assert max(rel_l2(sky[s], c1["ref"][s]) for s in range(64)) < 1e-5
+    bp.close()
+
+
+def test_batched_autotune_keeps_results(lib, c1):
+    import torch
+    bp = lib.BatchPlan(c1["net"], "bf16x3")
+    F = torch.from_numpy(np.ascontiguousarray(c1["batch"]["F"])).cuda()
+    k = bp.autotune(F)
+    assert k >= 1 and bp.split(64) == k
+    g = torch.from_numpy(c1["batch"]["gmst"]).cuda()
+    sky = bp.integrate(F, g).cpu().numpy()
+    assert max(rel_l2(sky[s], c1["ref"][s]) for s in range(64)) < 1e-5
+    bp.close()
