@@ -239,6 +239,9 @@ def run(args):
 
     # per-step events around the contraction kernel (recorded by the library)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for a_, b_ in ev:  # torch creates the CUDA event on first record
+        a_.record(st)
+        b_.record(st)
     t_begin, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if world > 1:
         dist.barrier()

@@ -31,13 +31,18 @@ extern "C" {
  *   SPHRAD_PREC_FP32   FP32 on CUDA cores
  *   SPHRAD_PREC_BF16X3 tcgen05 tensor cores, bf16 hi/lo split operands
  *                      (hi*hi + hi*lo + lo*hi), FP32 accumulation; up to 3
- *                      detectors.
- * Cross spectra are formed in FP64 in every mode; normalisation, rotation
- * and the z rotation run in FP32 (FP64 for SPHRAD_PREC_FP64). */
+ *                      detectors.  About 2^-16 relative error per product.
+ *   SPHRAD_PREC_BF16X6 tcgen05 tensor cores, bf16 hi/mid/lo split operands
+ *                      (the six products down to 2^-24 of hi*hi), FP32
+ *                      accumulation; up to 3 detectors.
+ * Cross spectra are formed in FP64 in every mode and rounded once to FP32
+ * before splitting; normalisation, rotation and the z rotation run in FP32
+ * (FP64 for SPHRAD_PREC_FP64). */
 enum {
 	SPHRAD_PREC_FP64 = 0,
 	SPHRAD_PREC_FP32 = 1,
-	SPHRAD_PREC_BF16X3 = 2
+	SPHRAD_PREC_BF16X3 = 2,
+	SPHRAD_PREC_BF16X6 = 3
 };
 
 typedef struct sphrad_batch_plan sphrad_batch_plan;

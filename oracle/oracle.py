@@ -305,10 +305,12 @@ class NetworkPlan:
     """Oracle-side equivalent of a correlator_network_plan_fd at l_max."""
 
     def __init__(self, positions, n: int, dt: float, l_max: int):
+        """Each baseline's power l_max is min(l_max, its native value), as
+        correlator_network_plan_fd_set_l leaves it (correlator.c:949-959);
+        skies come out at the largest of them."""
         self.positions = np.asarray(positions, np.float64)
         self.n = n
         self.dt = dt
-        self.l_max = l_max
         self.baselines = []
         nd = len(self.positions)
         for i in range(1, nd):
@@ -316,17 +318,19 @@ class NetworkPlan:
                 d = self.positions[i] - self.positions[j]
                 th, ph = vector_direction(d)
                 d_len = float(np.sqrt(d @ d))
-                D = delay_product(d_len, dt, n, l_max)
-                Rot = rotation_plan(l_max, rot_matrix(th, ph))
-                self.baselines.append(dict(i=i, j=j, d=d, d_len=d_len, theta=th, phi=ph, D=D, Rot=Rot))
+                lb = min(l_max, native_power_l_max(d_len, dt))
+                D = delay_product(d_len, dt, n, lb)
+                Rot = rotation_plan(lb, rot_matrix(th, ph))
+                self.baselines.append(dict(i=i, j=j, d=d, d_len=d_len, theta=th, phi=ph, l=lb, D=D, Rot=Rot))
+        self.l_max = max(b["l"] for b in self.baselines)
 
     def integrate(self, fseries) -> np.ndarray:
         """correlator.c:993-1010 for one segment; fseries is n_det x n."""
         sky = np.zeros(length(self.l_max, False), np.complex128)
         nb = len(self.baselines)
         for b in self.baselines:
-            p = baseline_integrate_power_fd(fseries[b["i"]], fseries[b["j"]], b["D"], self.l_max, b["Rot"])
-            sky += (1.0 / nb) * p
+            p = baseline_integrate_power_fd(fseries[b["i"]], fseries[b["j"]], b["D"], b["l"], b["Rot"])
+            sky += (1.0 / nb) * assign(p, b["l"], False, self.l_max, False)
         return sky
 
 

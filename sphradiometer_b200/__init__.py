@@ -18,7 +18,8 @@ from ._abi import last_error, load, series_length, series_to_numpy, numpy_to_ser
 PREC_FP64 = 0
 PREC_FP32 = 1
 PREC_BF16X3 = 2
-PRECISIONS = {"fp64": PREC_FP64, "fp32": PREC_FP32, "bf16x3": PREC_BF16X3}
+PREC_BF16X6 = 3
+PRECISIONS = {"fp64": PREC_FP64, "fp32": PREC_FP32, "bf16x3": PREC_BF16X3, "bf16x6": PREC_BF16X6}
 
 
 class SphradError(RuntimeError):

@@ -13,8 +13,10 @@
 // unique bins, M = segments, K = 2 (n/2 + 1) (re, im interleaved), N = l.
 //
 // Kernels:
-//   k_tc_contract   tcgen05 GEMM with bf16 hi/lo split operands (three
-//                   MMAs: hi*hi + hi*lo + lo*hi, FP32 accumulation in TMEM).
+//   k_tc_contract   tcgen05 GEMM with bf16 split operands, FP32
+//                   accumulation in TMEM: hi+lo parts and three MMAs
+//                   (hi*hi + hi*lo + lo*hi), or hi+mid+lo parts and six MMAs
+//                   (all products down to 2^-24 of hi*hi).
 //                   Raw FP64 spectra arrive by TMA (3-D box: 8 bins x 128
 //                   segments x all detectors, 128B swizzle); converter
 //                   warps form X_b for every baseline in registers and write
@@ -63,6 +65,7 @@ constexpr int A_TILE = TM * KE * 2;      // bytes of one bf16 A tile (4096)
 constexpr int CC_TS = 16;                // segments per CUDA-core block
 constexpr int CC_KC = 16;                // bins per CUDA-core stage
 constexpr unsigned long long kWaitCycles = 4000000000ull;  // ~2 s bound on every wait
+constexpr int kMaxChain = 64;            // most pipeline stages one tcgen05 CTA accumulates
 }  // namespace
 
 // ------------------------------------------------------------------------
@@ -192,11 +195,38 @@ __device__ __forceinline__ uint32_t pack_bf16(float lo_elem, float hi_elem)
 struct TcArgs {
 	int S, n_det, B, Kst, ks, npad, tmem_cols, accstride;
 	int bi[TC_MAXB], bj[TC_MAXB];
-	const uint8_t *bops;   // [Kst][B][2][npad * KE bf16], UMMA layout
+	const uint8_t *bops;   // [Kst][B][NPART][npad * KE bf16], UMMA layout
 	float *acc;            // [S][B][accstride]
 	unsigned *err;
 };
 
+// split x into NPART bf16 parts: x = p0 + p1 (+ p2) to 8 (16, 24) bits
+template <int NPART>
+__device__ __forceinline__ void split_bf16(float x, float *p)
+{
+	p[0] = __bfloat162float(__float2bfloat16_rn(x));
+	float r = x - p[0];
+	if(NPART >= 2)
+		p[1] = __bfloat162float(__float2bfloat16_rn(r));
+	if(NPART >= 3)
+		p[2] = r - p[1];
+}
+
+// The products kept for NPART parts (part a of X, part b of D): every pair
+// whose weight is at least 2^-16 (NPART = 2) or 2^-24 (NPART = 3) of hi*hi.
+template <int NPART> struct Prods;
+template <> struct Prods<2> {
+	static constexpr int n = 3;
+	__device__ static int a(int i) { return i == 2 ? 1 : 0; }
+	__device__ static int b(int i) { return i == 1 ? 1 : 0; }
+};
+template <> struct Prods<3> {
+	static constexpr int n = 6;
+	__device__ static int a(int i) { const int t[6] = {0, 0, 1, 0, 2, 1}; return t[i]; }
+	__device__ static int b(int i) { const int t[6] = {0, 1, 0, 2, 0, 1}; return t[i]; }
+};
+
+template <int NPART, int NFS>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_constant__ CUtensorMap tmF, const __grid_constant__ TcArgs a)
 {
 	extern __shared__ uint8_t smem_raw[];
@@ -204,14 +234,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	const int f_slab = TM * 128;
 	const int f_stage = a.n_det * f_slab;
 	const int btile = a.npad * KE * 2;
-	const int ab_bytes = a.B * 2 * btile;
+	const int ab_bytes = a.B * NPART * btile;
 	uint8_t *sF = smem;
-	uint8_t *sA = sF + NF * f_stage;
-	uint8_t *sB = sA + NAB * a.B * 2 * A_TILE;
+	uint8_t *sA = sF + NFS * f_stage;
+	uint8_t *sB = sA + NAB * a.B * NPART * A_TILE;
 	uint64_t *bars = (uint64_t *) (sB + NAB * ab_bytes);
 	uint64_t *f_full = bars;
-	uint64_t *f_empty = bars + NF;
-	uint64_t *ab_full = bars + 2 * NF;
+	uint64_t *f_empty = bars + NFS;
+	uint64_t *ab_full = bars + 2 * NFS;
 	uint64_t *b_full = ab_full + NAB;
 	uint64_t *ab_empty = b_full + NAB;
 	uint64_t *acc_full = ab_empty + NAB;
@@ -225,7 +255,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	const int nst = k_end - k_begin;
 
 	if(threadIdx.x == 0) {
-		for(int i = 0; i < NF; i++) {
+		for(int i = 0; i < NFS; i++) {
 			mbar_init(smem_u32(&f_full[i]), 1);
 			mbar_init(smem_u32(&f_empty[i]), 4);
 		}
@@ -253,8 +283,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			int issued = 0;
 			for(int it = 0; it < nst; it++) {
 				const int st = k_begin + it;
-				const int fs = it % NF;
-				const uint32_t fph = (it / NF) & 1;
+				const int fs = it % NFS;
+				const uint32_t fph = (it / NFS) & 1;
 				if(!mbar_wait(smem_u32(&f_empty[fs]), fph ^ 1, abort_flag, a.err, 1))
 					break;
 				mbar_arrive_tx(smem_u32(&f_full[fs]), f_stage);
@@ -272,8 +302,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			// drain the copies that may still be in flight
 			const int nf = issued < 0 ? -issued : issued;
 			const int nb = issued < 0 ? -issued - 1 : issued;
-			for(int it = (nf > NF ? nf - NF : 0); it < nf; it++)
-				mbar_drain(smem_u32(&f_full[it % NF]), (it / NF) & 1);
+			for(int it = (nf > NFS ? nf - NFS : 0); it < nf; it++)
+				mbar_drain(smem_u32(&f_full[it % NFS]), (it / NFS) & 1);
 			for(int it = (nb > NAB ? nb - NAB : 0); it < nb; it++)
 				mbar_drain(smem_u32(&b_full[it % NAB]), (it / NAB) & 1);
 		}
@@ -291,14 +321,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 					break;
 				tc_fence_after();
 				for(int b = 0; b < a.B; b++) {
-					const uint32_t d = tmem + (uint32_t) (b * a.npad);
-					const uint32_t ahi = smem_u32(sA + ((as * a.B + b) * 2 + 0) * A_TILE);
-					const uint32_t alo = ahi + A_TILE;
-					const uint32_t bhi = smem_u32(sB + as * ab_bytes + (b * 2 + 0) * btile);
-					const uint32_t blo = bhi + btile;
-					umma_bf16(d, umma_desc(ahi, 128, 256), umma_desc(bhi, 128, 256), idesc, it > 0 ? 1u : 0u);
-					umma_bf16(d, umma_desc(ahi, 128, 256), umma_desc(blo, 128, 256), idesc, 1u);
-					umma_bf16(d, umma_desc(alo, 128, 256), umma_desc(bhi, 128, 256), idesc, 1u);
+					// hi*hi accumulates in the main bank; the correction
+					// products, 2^8 smaller, in a second bank, so the large
+					// accumulator takes one rounding per stage
+					const uint32_t dm = tmem + (uint32_t) (b * a.npad);
+					const uint32_t dc = dm + (uint32_t) (a.B * a.npad);
+					const uint32_t a0 = smem_u32(sA + (as * a.B + b) * NPART * A_TILE);
+					const uint32_t b0 = smem_u32(sB + as * ab_bytes + b * NPART * btile);
+#pragma unroll
+					for(int i = 0; i < Prods<NPART>::n; i++)
+						umma_bf16(i == 0 ? dm : dc, umma_desc(a0 + Prods<NPART>::a(i) * A_TILE, 128, 256),
+							  umma_desc(b0 + Prods<NPART>::b(i) * btile, 128, 256), idesc, (it > 0 || i > 1) ? 1u : 0u);
 				}
 				umma_commit(smem_u32(&ab_empty[as]));
 			}
@@ -309,8 +342,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 		const int r = threadIdx.x - 64;  // tile row 0..127
 		const int roff = (r >> 3) * 256 + (r & 7) * 16;
 		for(int it = 0; it < nst; it++) {
-			const int fs = it % NF;
-			const uint32_t fph = (it / NF) & 1;
+			const int fs = it % NFS;
+			const uint32_t fph = (it / NFS) & 1;
 			const bool okf = mbar_wait(smem_u32(&f_full[fs]), fph, abort_flag, a.err, 5);
 			if(!__all_sync(0xffffffffu, okf))
 				break;
@@ -333,26 +366,26 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			if(!__all_sync(0xffffffffu, oke))
 				break;
 			for(int b = 0; b < a.B; b++) {
-				uint32_t hi[KB], lo[KB];
+				uint32_t part[NPART][KB];
 #pragma unroll
 				for(int c = 0; c < KB; c++) {
 					const int da = a.bi[b], db = a.bj[b];
 					const double2 fa = da == 0 ? f0[c] : (da == 1 ? f1[c] : f2[c]);
 					const double2 fb = db == 0 ? f0[c] : (db == 1 ? f1[c] : f2[c]);
-					// X = fb * conj(fa)
-					const float xr = (float) (fb.x * fa.x + fb.y * fa.y);
-					const float xi = (float) (fb.y * fa.x - fb.x * fa.y);
-					const float hr = __bfloat162float(__float2bfloat16_rn(xr));
-					const float hm = __bfloat162float(__float2bfloat16_rn(xi));
-					hi[c] = pack_bf16(xr, xi);
-					lo[c] = pack_bf16(xr - hr, xi - hm);
+					// X = fb * conj(fa), formed in FP64 and rounded once to FP32
+					float pr[3], pi[3];
+					split_bf16<NPART>((float) (fb.x * fa.x + fb.y * fa.y), pr);
+					split_bf16<NPART>((float) (fb.y * fa.x - fb.x * fa.y), pi);
+#pragma unroll
+					for(int q = 0; q < NPART; q++)
+						part[q][c] = pack_bf16(pr[q], pi[q]);
 				}
-				uint8_t *th = sA + ((as * a.B + b) * 2 + 0) * A_TILE + roff;
-				uint8_t *tl = th + A_TILE;
-				*(uint4 *) (th) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-				*(uint4 *) (th + 128) = make_uint4(hi[4], hi[5], hi[6], hi[7]);
-				*(uint4 *) (tl) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-				*(uint4 *) (tl + 128) = make_uint4(lo[4], lo[5], lo[6], lo[7]);
+				uint8_t *t0 = sA + (as * a.B + b) * NPART * A_TILE + roff;
+#pragma unroll
+				for(int q = 0; q < NPART; q++) {
+					*(uint4 *) (t0 + q * A_TILE) = make_uint4(part[q][0], part[q][1], part[q][2], part[q][3]);
+					*(uint4 *) (t0 + q * A_TILE + 128) = make_uint4(part[q][4], part[q][5], part[q][6], part[q][7]);
+				}
 			}
 			fence_proxy_async();
 			__syncwarp();
@@ -369,8 +402,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			const int s = tile * TM + row;
 			for(int b = 0; b < a.B; b++) {
 				for(int c0 = 0; c0 < a.accstride; c0 += 16) {
-					uint32_t v[16];
-					tmem_ld16(tmem + ((uint32_t) (q * 32) << 16) + (uint32_t) (b * a.npad + c0), v);
+					uint32_t v[16], w[16];
+					const uint32_t ta = tmem + ((uint32_t) (q * 32) << 16) + (uint32_t) (b * a.npad + c0);
+					tmem_ld16(ta, v);
+					tmem_ld16(ta + (uint32_t) (a.B * a.npad), w);
+#pragma unroll
+					for(int j = 0; j < 16; j++)
+						v[j] = __float_as_uint(__uint_as_float(v[j]) + __uint_as_float(w[j]));
 					if(s < a.S) {
 						float *dst = a.acc + ((size_t) s * a.B + b) * a.accstride + c0;
 #pragma unroll
@@ -392,10 +430,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	}
 }
 
-// operand table for the tcgen05 path: stage st, baseline b, part p (hi/lo),
-// row n (l), k element kk (bin st*KB + kk/2, re/im = kk%2) in the no-swizzle
-// K-major core-matrix layout (LBO 128 B, SBO 256 B)
-__global__ void k_build_bops(int Kst, int B, int npad, int Lp1, int Ku, const double2 *Dt, uint8_t *bops)
+// operand table for the tcgen05 path: stage st, baseline b, part p, row n
+// (l), k element kk (bin st*KB + kk/2, re/im = kk%2) in the no-swizzle
+// K-major core-matrix layout (LBO 128 B, SBO 256 B).  Parts split the FP64
+// value into bf16 pieces of 8 significant bits each.
+__global__ void k_build_bops(int Kst, int B, int npart, int npad, int Lp1, int Ku, const double2 *Dt, uint8_t *bops)
 {
 	const long long total = (long long) Kst * B * npad * KE;
 	const int btile = npad * KE * 2;
@@ -410,12 +449,13 @@ __global__ void k_build_bops(int Kst, int B, int npad, int Lp1, int Ku, const do
 			const double2 d = Dt[((size_t) bin * B + b) * Lp1 + n];
 			v = (kk & 1) ? -d.y : d.x;
 		}
-		const __nv_bfloat16 h = __float2bfloat16_rn((float) v);
-		const __nv_bfloat16 l = __float2bfloat16_rn((float) (v - (double) __bfloat162float(h)));
 		const size_t off = (size_t) (n >> 3) * 256 + (kk >> 3) * 128 + (n & 7) * 16 + (kk & 7) * 2;
-		uint8_t *t = bops + ((size_t) st * B + b) * 2 * btile;
-		*(__nv_bfloat16 *) (t + off) = h;
-		*(__nv_bfloat16 *) (t + btile + off) = l;
+		uint8_t *t = bops + ((size_t) st * B + b) * npart * btile;
+		for(int p = 0; p < npart; p++) {
+			const __nv_bfloat16 h = __float2bfloat16_rn((float) v);
+			*(__nv_bfloat16 *) (t + p * btile + off) = h;
+			v -= (double) __bfloat162float(h);
+		}
 	}
 }
 
@@ -566,6 +606,7 @@ struct BatchPlan {
 	void *Dt = nullptr;        // [Ku][B][Lp1] complex (T of the CUDA-core path)
 	uint8_t *bops = nullptr;   // tcgen05 operand table
 	int Kst = 0, npad = 0, tmem_cols = 0;
+	int npart = 2, nf = NF;    // bf16 parts per operand, spectrum-ring depth
 	void *W = nullptr;         // [B][nq] complex T
 	short *lq = nullptr, *mq = nullptr;
 	unsigned *err = nullptr;
@@ -597,12 +638,14 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode()
 	return fn;
 }
 
+static bool is_tc(int precision) { return precision == kPrecBF16x3 || precision == kPrecBF16x6; }
+
 static size_t tc_smem_bytes(const BatchPlan &P)
 {
-	const size_t f = (size_t) NF * P.n_det * TM * 128;
-	const size_t aa = (size_t) NAB * P.B * 2 * A_TILE;
-	const size_t bb = (size_t) NAB * P.B * 2 * P.npad * KE * 2;
-	const size_t bars = 8 * (2 * NF + 3 * NAB + 1) + 16;
+	const size_t f = (size_t) P.nf * P.n_det * TM * 128;
+	const size_t aa = (size_t) NAB * P.B * P.npart * A_TILE;
+	const size_t bb = (size_t) NAB * P.B * P.npart * P.npad * KE * 2;
+	const size_t bars = 8 * (2 * P.nf + 3 * NAB + 1) + 16;
 	// 1 KB for aligning the base, 4 KB of slack past the last tile
 	return 1024 + f + aa + bb + bars + 4096;
 }
@@ -649,7 +692,7 @@ void *batch_plan_create(const BatchPlanDesc &d, int precision)
 		set_error("batch plan: only spectra of real series (n/2+1 unique bins) are supported");
 		return nullptr;
 	}
-	if(precision == kPrecBF16x3) {
+	if(is_tc(precision)) {
 		int dev = 0, major = 0;
 		cudaGetDevice(&dev);
 		cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
@@ -746,11 +789,13 @@ void *batch_plan_create(const BatchPlanDesc &d, int precision)
 	P->err = (unsigned *) dmalloc(sizeof(unsigned));
 	if(!P->err || dmemset(P->err, 0, sizeof(unsigned)))
 		fail = true;
-	if(!fail && precision == kPrecBF16x3) {
+	if(!fail && is_tc(precision)) {
 		P->Kst = (Ku + KB - 1) / KB;
 		P->npad = (Lp1 + 15) & ~15;
+		P->npart = precision == kPrecBF16x6 ? 3 : 2;
+		P->nf = precision == kPrecBF16x6 ? 2 : 3;
 		int cols = 32;
-		while(cols < B * P->npad)
+		while(cols < 2 * B * P->npad)  // main and correction accumulators
 			cols <<= 1;
 		P->tmem_cols = cols;
 		if(P->npad > 256 || cols > 512) {
@@ -760,10 +805,10 @@ void *batch_plan_create(const BatchPlanDesc &d, int precision)
 			// a double-precision copy of Dt for the operand builder
 			void *Dt64 = nullptr;
 			up(&Dt64, Dt.data(), Dt.size() * sizeof(double));
-			const size_t bbytes = (size_t) P->Kst * B * 2 * P->npad * KE * 2;
+			const size_t bbytes = (size_t) P->Kst * B * P->npart * P->npad * KE * 2;
 			P->bops = (uint8_t *) dmalloc(bbytes);
 			if(!fail && P->bops) {
-				k_build_bops<<<512, 256, 0, (cudaStream_t) lib_stream()>>>(P->Kst, B, P->npad, Lp1, Ku, (const double2 *) Dt64, P->bops);
+				k_build_bops<<<512, 256, 0, (cudaStream_t) lib_stream()>>>(P->Kst, B, P->npart, P->npad, Lp1, Ku, (const double2 *) Dt64, P->bops);
 				if(cudaGetLastError() != cudaSuccess)
 					fail = true;
 			} else
@@ -775,7 +820,8 @@ void *batch_plan_create(const BatchPlanDesc &d, int precision)
 				set_error("batch plan: shared-memory budget exceeded");
 				fail = true;
 			}
-			if(!fail && cudaFuncSetAttribute(k_tc_contract, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess) {
+			if(!fail && (cudaFuncSetAttribute(k_tc_contract<2, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
+				     cudaFuncSetAttribute(k_tc_contract<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess)) {
 				set_error("batch plan: cannot reserve %zu bytes of shared memory", tc_smem_bytes(*P));
 				fail = true;
 			}
@@ -807,7 +853,7 @@ int batch_pick_split(const void *pp, int S)
 	int dev = 0;
 	cudaGetDevice(&dev);
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-	if(P->precision == kPrecBF16x3) {
+	if(is_tc(P->precision)) {
 		const int tiles = (S + TM - 1) / TM;
 		int ks = sms / tiles;
 		if(ks < 1)
@@ -850,9 +896,14 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 		set_error("batch_run: workspace of %zu bytes needed", batch_workspace_bytes(P, S));
 		return -1;
 	}
-	const int ks = split > 0 ? split : batch_pick_split(P, S);
+	int ks = split > 0 ? split : batch_pick_split(P, S);
+	if(is_tc(P->precision)) {
+		// keep each CTA's TMEM accumulation chain short (FP32 rounding)
+		const int min_ks = (P->Kst + kMaxChain - 1) / kMaxChain;
+		ks = ks < min_ks ? min_ks : ks;
+	}
 	int launches = 0;
-	if(P->precision == kPrecBF16x3) {
+	if(is_tc(P->precision)) {
 		if(((uintptr_t) F & 15) || ((ld * 16) & 15)) {
 			set_error("batch_run: spectra must be 16-byte aligned");
 			return -1;
@@ -897,7 +948,10 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 		const int tiles = (S + TM - 1) / TM;
 		if(P->ev_begin)
 			cudaEventRecord(P->ev_begin, st);
-		k_tc_contract<<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+		if(P->npart == 3)
+			k_tc_contract<3, 2><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+		else
+			k_tc_contract<2, NF><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		if(P->ev_end)
 			cudaEventRecord(P->ev_end, st);
 		launches++;
@@ -977,10 +1031,11 @@ int batch_autotune(void *pp, const void *F, int S, long long ld, void *sky, void
 	cudaGetDevice(&dev);
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 	std::vector<int> cand;
-	if(P->precision == kPrecBF16x3) {
+	if(is_tc(P->precision)) {
 		const int tiles = (S + TM - 1) / TM;
-		for(int ks = 1; ks <= P->Kst / 2 && tiles * ks <= 4 * sms; ks++)
-			if(ks <= 8 || tiles * ks <= 2 * sms)
+		const int min_ks = (P->Kst + kMaxChain - 1) / kMaxChain;
+		for(int ks = min_ks; ks <= P->Kst / 2 && (tiles * ks <= 4 * sms || ks == min_ks); ks++)
+			if(ks <= min_ks + 8 || tiles * ks <= 2 * sms)
 				cand.push_back(ks);
 	} else {
 		const int nch = (P->Ku + CC_KC - 1) / CC_KC;

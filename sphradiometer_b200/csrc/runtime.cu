@@ -411,7 +411,9 @@ __device__ __forceinline__ double rc_d(int l, int m, int mp) { return sqrt((doub
 // One block per plan.  The l = 1 matrix (equations 5.3-5.5 of Choi et al.)
 // is built from R; level l is then computed from level l - 1 and level 1,
 // one element per thread, with a block barrier between levels.
-__global__ void k_rotation_plan(int l_max, const double *R_all, double2 *D_all, size_t plan_stride)
+constexpr int ROT_THREADS = 512;
+
+__global__ void __launch_bounds__(ROT_THREADS) k_rotation_plan(int l_max, const double *R_all, double2 *D_all, size_t plan_stride)
 {
 	__shared__ double2 d1[9];
 	const double *R = R_all + 9 * blockIdx.x;
@@ -523,7 +525,7 @@ int build_rotation_plan(unsigned l_max, const double *R, double *D_host)
 		return -1;
 	if(h2d(dR.p, R, 9 * sizeof(double)))
 		return -1;
-	k_rotation_plan<<<1, 1024, 0, S()>>>((int) l_max, dR.as<double>(), dD.as<double2>(), len);
+	k_rotation_plan<<<1, ROT_THREADS, 0, S()>>>((int) l_max, dR.as<double>(), dD.as<double2>(), len);
 	CK(cudaGetLastError());
 	if(d2h(D_host, dD.p, len * sizeof(double2)))
 		return -1;

@@ -82,7 +82,7 @@ struct BatchPlanDesc {
 	const double *rot[kMaxBaselines];  // host flat rotation plans (>= lb)
 	double weight = 1.0;         // 1 / n_baselines (correlator.c:1004)
 };
-enum BatchPrecision { kPrecFP64 = 0, kPrecFP32 = 1, kPrecBF16x3 = 2 };
+enum BatchPrecision { kPrecFP64 = 0, kPrecFP32 = 1, kPrecBF16x3 = 2, kPrecBF16x6 = 3 };
 void *batch_plan_create(const BatchPlanDesc &desc, int precision);
 void batch_plan_destroy(void *plan);
 unsigned batch_plan_l_max(const void *plan);
