@@ -14,9 +14,10 @@
 //
 // Kernels:
 //   k_tc_contract   tcgen05 GEMM with bf16 split operands, FP32
-//                   accumulation in TMEM: hi+lo parts and three MMAs
-//                   (hi*hi + hi*lo + lo*hi), or hi+mid+lo parts and six MMAs
-//                   (all products down to 2^-24 of hi*hi).
+//                   accumulation in TMEM: hi+lo parts and the three products
+//                   hi*hi + hi*lo + lo*hi (two MMAs per baseline and stage),
+//                   or hi+mid+lo parts and the six products down to 2^-24
+//                   of hi*hi (three MMAs).
 //                   Raw FP64 spectra arrive by TMA (3-D box: 8 bins x 128
 //                   segments x all detectors, 128B swizzle); converter
 //                   warps form X_b for every baseline in registers and write
@@ -56,9 +57,10 @@ namespace {
 constexpr int TM = 128;                  // segments per tile = MMA M
 constexpr int KB = 8;                    // bins per pipeline stage
 constexpr int KE = 16;                   // real K per stage = MMA K (bf16)
-constexpr int NF = 3;                    // depth of the spectrum ring
-constexpr int NAB = 2;                   // depth of the operand ring
-constexpr int TC_THREADS = 192;          // 6 warps: TMA, MMA, 4 converter/epilogue
+constexpr int NF = 2;                    // depth of the spectrum ring (2 x 48 KB in flight sustains HBM rate)
+constexpr int CONV_WARPS = 16;           // converter/epilogue warps (four per SM sub-partition)
+constexpr int TC_THREADS = 32 * (3 + CONV_WARPS);  // + spectra TMA, MMA, operand copies
+constexpr int TC_MAXB3 = 3;              // baselines handled by the tcgen05 path (3 detectors)
 constexpr int TC_MAXB = 8;
 constexpr int TC_MAXDET = 3;
 constexpr int A_TILE = TM * KE * 2;      // bytes of one bf16 A tile (4096)
@@ -200,33 +202,38 @@ struct TcArgs {
 	unsigned *err;
 };
 
-// split x into NPART bf16 parts: x = p0 + p1 (+ p2) to 8 (16, 24) bits
+// Split the complex value (re, im) into NPART packed bf16x2 words (re in the
+// low half): part q is the round-to-nearest bf16 of what parts 0..q-1 left,
+// so re = sum of the parts to 8, 16 or 24 significant bits.
 template <int NPART>
-__device__ __forceinline__ void split_bf16(float x, float *p)
+__device__ __forceinline__ void split_pair(float re, float im, uint32_t *w)
 {
-	p[0] = __bfloat162float(__float2bfloat16_rn(x));
-	float r = x - p[0];
-	if(NPART >= 2)
-		p[1] = __bfloat162float(__float2bfloat16_rn(r));
-	if(NPART >= 3)
-		p[2] = r - p[1];
+#pragma unroll
+	for(int q = 0; q < NPART; q++) {
+		const __nv_bfloat162 h = __floats2bfloat162_rn(re, im);
+		w[q] = *reinterpret_cast<const uint32_t *>(&h);
+		if(q + 1 < NPART) {
+			const float2 hf = __bfloat1622float2(h);
+			re -= hf.x;
+			im -= hf.y;
+		}
+	}
 }
 
 // The products kept for NPART parts (part a of X, part b of D): every pair
 // whose weight is at least 2^-16 (NPART = 2) or 2^-24 (NPART = 3) of hi*hi.
-template <int NPART> struct Prods;
-template <> struct Prods<2> {
-	static constexpr int n = 3;
-	__device__ static int a(int i) { return i == 2 ? 1 : 0; }
-	__device__ static int b(int i) { return i == 1 ? 1 : 0; }
-};
-template <> struct Prods<3> {
-	static constexpr int n = 6;
-	__device__ static int a(int i) { const int t[6] = {0, 0, 1, 0, 2, 1}; return t[i]; }
-	__device__ static int b(int i) { const int t[6] = {0, 1, 0, 2, 0, 1}; return t[i]; }
-};
+//
+// Products that share a part of X go into one MMA whose N spans the D parts
+// side by side (the D parts of a baseline are adjacent N-row blocks of the
+// operand tile), writing adjacent TMEM column blocks.  Each baseline owns
+// NPART blocks of npad columns: block 0 gets hi*hi alone (the large
+// accumulator, one rounding per stage), blocks 1.. the correction products
+// (2^8 and more smaller), summed with block 0 in the epilogue.  MMA i uses
+// X part i, D parts 0 .. NPART-1-i, and writes blocks i .. NPART-1:
+//   NPART = 2: hi x [hi|lo] -> [0|1], lo x hi -> 1
+//   NPART = 3: hi x [hi|mid|lo] -> [0|1|2], mid x [hi|mid] -> [1|2], lo x hi -> 2
 
-template <int NPART, int NFS>
+template <int NPART, int NFS, int NABS, int NBS>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_constant__ CUtensorMap tmF, const __grid_constant__ TcArgs a)
 {
 	extern __shared__ uint8_t smem_raw[];
@@ -237,14 +244,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	const int ab_bytes = a.B * NPART * btile;
 	uint8_t *sF = smem;
 	uint8_t *sA = sF + NFS * f_stage;
-	uint8_t *sB = sA + NAB * a.B * NPART * A_TILE;
-	uint64_t *bars = (uint64_t *) (sB + NAB * ab_bytes);
-	uint64_t *f_full = bars;
-	uint64_t *f_empty = bars + NFS;
-	uint64_t *ab_full = bars + 2 * NFS;
-	uint64_t *b_full = ab_full + NAB;
-	uint64_t *ab_empty = b_full + NAB;
-	uint64_t *acc_full = ab_empty + NAB;
+	uint8_t *sB = sA + NABS * a.B * NPART * A_TILE;
+	uint64_t *bars = (uint64_t *) (sB + NBS * ab_bytes);
+	uint64_t *f_full = bars;                // spectra landed (TMA)
+	uint64_t *f_empty = f_full + NFS;       // spectra read by the converters
+	uint64_t *ab_full = f_empty + NFS;      // X operand written by the converters
+	uint64_t *ab_empty = ab_full + NABS;     // X operand consumed by the MMAs
+	uint64_t *b_full = ab_empty + NABS;      // delay-table operand landed (bulk copy)
+	uint64_t *b_empty = b_full + NBS;       // delay-table operand consumed by the MMAs
+	uint64_t *acc_full = b_empty + NBS;
 	uint32_t *tslot = (uint32_t *) (acc_full + 1);
 	volatile int *abort_flag = (volatile int *) (tslot + 1);
 
@@ -257,12 +265,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	if(threadIdx.x == 0) {
 		for(int i = 0; i < NFS; i++) {
 			mbar_init(smem_u32(&f_full[i]), 1);
-			mbar_init(smem_u32(&f_empty[i]), 4);
+			mbar_init(smem_u32(&f_empty[i]), CONV_WARPS);
 		}
-		for(int i = 0; i < NAB; i++) {
-			mbar_init(smem_u32(&ab_full[i]), 4);
-			mbar_init(smem_u32(&b_full[i]), 1);
+		for(int i = 0; i < NABS; i++) {
+			mbar_init(smem_u32(&ab_full[i]), CONV_WARPS);
 			mbar_init(smem_u32(&ab_empty[i]), 1);
+		}
+		for(int i = 0; i < NBS; i++) {
+			mbar_init(smem_u32(&b_full[i]), 1);
+			mbar_init(smem_u32(&b_empty[i]), 1);
 		}
 		mbar_init(smem_u32(acc_full), 1);
 		*abort_flag = 0;
@@ -278,7 +289,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	const uint32_t tmem = *tslot;
 
 	if(warp == 0) {
-		// ---------------- producer ----------------
+		// ---------------- producer: spectra only ----------------
+		// Runs NFS stages ahead of the converters, gated only by their
+		// release of the ring slot.
 		if(lane == 0) {
 			int issued = 0;
 			for(int it = 0; it < nst; it++) {
@@ -289,110 +302,126 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 					break;
 				mbar_arrive_tx(smem_u32(&f_full[fs]), f_stage);
 				tma_load_3d(smem_u32(sF + fs * f_stage), &tmF, smem_u32(&f_full[fs]), st * 2 * KB, tile * TM, 0);
-				const int as = it % NAB;
-				const uint32_t aph = (it / NAB) & 1;
-				if(!mbar_wait(smem_u32(&ab_empty[as]), aph ^ 1, abort_flag, a.err, 2)) {
-					issued = -(it + 1);  // F load of this stage is in flight, B load is not
-					break;
-				}
-				mbar_arrive_tx(smem_u32(&b_full[as]), ab_bytes);
-				bulk_g2s(smem_u32(sB + as * ab_bytes), a.bops + (size_t) st * ab_bytes, ab_bytes, smem_u32(&b_full[as]));
 				issued = it + 1;
 			}
-			// drain the copies that may still be in flight
-			const int nf = issued < 0 ? -issued : issued;
-			const int nb = issued < 0 ? -issued - 1 : issued;
-			for(int it = (nf > NFS ? nf - NFS : 0); it < nf; it++)
+			// drain the loads that may still be in flight
+			for(int it = (issued > NFS ? issued - NFS : 0); it < issued; it++)
 				mbar_drain(smem_u32(&f_full[it % NFS]), (it / NFS) & 1);
-			for(int it = (nb > NAB ? nb - NAB : 0); it < nb; it++)
-				mbar_drain(smem_u32(&b_full[it % NAB]), (it / NAB) & 1);
 		}
 	} else if(warp == 1) {
 		// ---------------- MMA issuer ----------------
 		if(lane == 0) {
 			// kind::f16, D = F32, A = B = BF16, both K-major, N = npad, M = 128
-			const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (a.npad >> 3) << 17) | ((uint32_t) (TM >> 4) << 24);
+			// MMA i spans N = (NPART - i) * npad columns
+			uint32_t idesc[NPART];
+#pragma unroll
+			for(int i = 0; i < NPART; i++)
+				idesc[i] = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (((NPART - i) * a.npad) >> 3) << 17) | ((uint32_t) (TM >> 4) << 24);
 			for(int it = 0; it < nst; it++) {
-				const int as = it % NAB;
-				const uint32_t aph = (it / NAB) & 1;
+				const int as = it % NABS;
+				const uint32_t aph = (it / NABS) & 1;
+				const int bs = it % NBS;
+				const uint32_t bph = (it / NBS) & 1;
 				if(!mbar_wait(smem_u32(&ab_full[as]), aph, abort_flag, a.err, 3))
 					break;
-				if(!mbar_wait(smem_u32(&b_full[as]), aph, abort_flag, a.err, 4))
+				if(!mbar_wait(smem_u32(&b_full[bs]), bph, abort_flag, a.err, 4))
 					break;
 				tc_fence_after();
 				for(int b = 0; b < a.B; b++) {
-					// hi*hi accumulates in the main bank; the correction
-					// products, 2^8 smaller, in a second bank, so the large
-					// accumulator takes one rounding per stage
-					const uint32_t dm = tmem + (uint32_t) (b * a.npad);
-					const uint32_t dc = dm + (uint32_t) (a.B * a.npad);
+					const uint32_t d0 = tmem + (uint32_t) (b * NPART * a.npad);
 					const uint32_t a0 = smem_u32(sA + (as * a.B + b) * NPART * A_TILE);
-					const uint32_t b0 = smem_u32(sB + as * ab_bytes + b * NPART * btile);
+					const uint32_t b0 = smem_u32(sB + bs * ab_bytes + b * NPART * btile);
 #pragma unroll
-					for(int i = 0; i < Prods<NPART>::n; i++)
-						umma_bf16(i == 0 ? dm : dc, umma_desc(a0 + Prods<NPART>::a(i) * A_TILE, 128, 256),
-							  umma_desc(b0 + Prods<NPART>::b(i) * btile, 128, 256), idesc, (it > 0 || i > 1) ? 1u : 0u);
+					for(int i = 0; i < NPART; i++)
+						umma_bf16(d0 + (uint32_t) (i * a.npad), umma_desc(a0 + i * A_TILE, 128, 256), umma_desc(b0, 128, 256), idesc[i],
+							  (it > 0 || i > 0) ? 1u : 0u);
 				}
 				umma_commit(smem_u32(&ab_empty[as]));
+				umma_commit(smem_u32(&b_empty[bs]));
 			}
 			umma_commit(smem_u32(acc_full));
 		}
+	} else if(warp == TC_THREADS / 32 - 1) {
+		// ---------------- producer: delay-table operand ----------------
+		// L2-resident; prefetched NBS stages ahead of the MMAs
+		if(lane == 0) {
+			int issued = 0;
+			for(int it = 0; it < nst; it++) {
+				const int bs = it % NBS;
+				if(!mbar_wait(smem_u32(&b_empty[bs]), ((it / NBS) & 1) ^ 1, abort_flag, a.err, 2))
+					break;
+				mbar_arrive_tx(smem_u32(&b_full[bs]), ab_bytes);
+				bulk_g2s(smem_u32(sB + bs * ab_bytes), a.bops + (size_t) (k_begin + it) * ab_bytes, ab_bytes, smem_u32(&b_full[bs]));
+				issued = it + 1;
+			}
+			for(int it = (issued > NBS ? issued - NBS : 0); it < issued; it++)
+				mbar_drain(smem_u32(&b_full[it % NBS]), (it / NBS) & 1);
+		}
 	} else {
 		// ---------------- converters, then epilogue ----------------
-		const int r = threadIdx.x - 64;  // tile row 0..127
-		const int roff = (r >> 3) * 256 + (r & 7) * 16;
+		// CONV_WARPS warps, four per SM sub-partition: thread t handles tile
+		// row r = t % 128 and bin pair g = t / 128 (bins 2g, 2g+1 of the
+		// stage: half g % 2 of k-core-matrix g / 2 of the UMMA tile)
+		constexpr int BPT = KB / (CONV_WARPS / 4);  // bins per thread
+		const int t = threadIdx.x - 64;
+		const int r = t & (TM - 1);
+		const int g = t >> 7;
+		const int roff = (r >> 3) * 256 + (r & 7) * 16 + (g >> 1) * 128 + (g & 1) * 8;
 		for(int it = 0; it < nst; it++) {
 			const int fs = it % NFS;
 			const uint32_t fph = (it / NFS) & 1;
 			const bool okf = mbar_wait(smem_u32(&f_full[fs]), fph, abort_flag, a.err, 5);
 			if(!__all_sync(0xffffffffu, okf))
 				break;
-			double2 f0[KB], f1[KB], f2[KB];
+			// this thread's bins of every detector, rounded to FP32
+			float2 f[TC_MAXDET][BPT];
 			{
 				const uint8_t *base = sF + fs * f_stage + r * 128;
 #pragma unroll
-				for(int c = 0; c < KB; c++) {
-					f0[c] = *(const double2 *) (base + ((c ^ (r & 7)) << 4));
-					f1[c] = a.n_det > 1 ? *(const double2 *) (base + f_slab + ((c ^ (r & 7)) << 4)) : make_double2(0, 0);
-					f2[c] = a.n_det > 2 ? *(const double2 *) (base + 2 * f_slab + ((c ^ (r & 7)) << 4)) : make_double2(0, 0);
-				}
+				for(int d = 0; d < TC_MAXDET; d++)
+#pragma unroll
+					for(int c = 0; c < BPT; c++) {
+						const int cc = g * BPT + c;
+						double2 v = make_double2(0, 0);
+						if(d < a.n_det)
+							v = *(const double2 *) (base + d * f_slab + ((cc ^ (r & 7)) << 4));
+						f[d][c] = make_float2((float) v.x, (float) v.y);
+					}
 			}
 			__syncwarp();
 			if(lane == 0)
 				mbar_arrive(smem_u32(&f_empty[fs]));
-			const int as = it % NAB;
-			const uint32_t aph = (it / NAB) & 1;
+			const int as = it % NABS;
+			const uint32_t aph = (it / NABS) & 1;
 			const bool oke = mbar_wait(smem_u32(&ab_empty[as]), aph ^ 1, abort_flag, a.err, 6);
 			if(!__all_sync(0xffffffffu, oke))
 				break;
-			for(int b = 0; b < a.B; b++) {
-				uint32_t part[NPART][KB];
 #pragma unroll
-				for(int c = 0; c < KB; c++) {
-					const int da = a.bi[b], db = a.bj[b];
-					const double2 fa = da == 0 ? f0[c] : (da == 1 ? f1[c] : f2[c]);
-					const double2 fb = db == 0 ? f0[c] : (db == 1 ? f1[c] : f2[c]);
-					// X = fb * conj(fa), formed in FP64 and rounded once to FP32
-					float pr[3], pi[3];
-					split_bf16<NPART>((float) (fb.x * fa.x + fb.y * fa.y), pr);
-					split_bf16<NPART>((float) (fb.y * fa.x - fb.x * fa.y), pi);
+			for(int b = 0; b < TC_MAXB3; b++) {
+				if(b >= a.B)
+					break;
+				const int da = a.bi[b], db = a.bj[b];
+				uint32_t part[BPT][NPART];
 #pragma unroll
-					for(int q = 0; q < NPART; q++)
-						part[q][c] = pack_bf16(pr[q], pi[q]);
+				for(int c = 0; c < BPT; c++) {
+					const float2 fa = da == 0 ? f[0][c] : (da == 1 ? f[1][c] : f[2][c]);
+					const float2 fb = db == 0 ? f[0][c] : (db == 1 ? f[1][c] : f[2][c]);
+					// X = fb * conj(fa)
+					split_pair<NPART>(fmaf(fb.x, fa.x, fb.y * fa.y), fmaf(fb.y, fa.x, -fb.x * fa.y), part[c]);
 				}
 				uint8_t *t0 = sA + (as * a.B + b) * NPART * A_TILE + roff;
 #pragma unroll
-				for(int q = 0; q < NPART; q++) {
-					*(uint4 *) (t0 + q * A_TILE) = make_uint4(part[q][0], part[q][1], part[q][2], part[q][3]);
-					*(uint4 *) (t0 + q * A_TILE + 128) = make_uint4(part[q][4], part[q][5], part[q][6], part[q][7]);
-				}
+				for(int q = 0; q < NPART; q++)
+					*(uint2 *) (t0 + q * A_TILE) = make_uint2(part[0][q], part[1][q]);
 			}
 			fence_proxy_async();
 			__syncwarp();
 			if(lane == 0)
 				mbar_arrive(smem_u32(&ab_full[as]));
 		}
-		// epilogue: TMEM -> registers -> FP32 atomics into the workspace
+		// epilogue: TMEM -> registers -> FP32 atomics into the workspace.
+		// Warps w and w + 4 share TMEM lane quarter w % 4 and split the
+		// baselines between them.
 		const bool got = mbar_wait(smem_u32(acc_full), 0, abort_flag, a.err, 7);
 		tc_fence_after();
 		const bool ok = __all_sync(0xffffffffu, got && !*abort_flag && nst > 0);
@@ -400,15 +429,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			const int q = warp & 3;
 			const int row = q * 32 + lane;
 			const int s = tile * TM + row;
-			for(int b = 0; b < a.B; b++) {
+			for(int b = (warp - 2) >> 2; b < a.B; b += CONV_WARPS / 4) {
 				for(int c0 = 0; c0 < a.accstride; c0 += 16) {
 					uint32_t v[16], w[16];
-					const uint32_t ta = tmem + ((uint32_t) (q * 32) << 16) + (uint32_t) (b * a.npad + c0);
+					const uint32_t ta = tmem + ((uint32_t) (q * 32) << 16) + (uint32_t) (b * NPART * a.npad + c0);
 					tmem_ld16(ta, v);
-					tmem_ld16(ta + (uint32_t) (a.B * a.npad), w);
 #pragma unroll
-					for(int j = 0; j < 16; j++)
-						v[j] = __float_as_uint(__uint_as_float(v[j]) + __uint_as_float(w[j]));
+					for(int p = 1; p < NPART; p++) {
+						tmem_ld16(ta + (uint32_t) (p * a.npad), w);
+#pragma unroll
+						for(int j = 0; j < 16; j++)
+							v[j] = __float_as_uint(__uint_as_float(v[j]) + __uint_as_float(w[j]));
+					}
 					if(s < a.S) {
 						float *dst = a.acc + ((size_t) s * a.B + b) * a.accstride + c0;
 #pragma unroll
@@ -606,7 +638,7 @@ struct BatchPlan {
 	void *Dt = nullptr;        // [Ku][B][Lp1] complex (T of the CUDA-core path)
 	uint8_t *bops = nullptr;   // tcgen05 operand table
 	int Kst = 0, npad = 0, tmem_cols = 0;
-	int npart = 2, nf = NF;    // bf16 parts per operand, spectrum-ring depth
+	int npart = 2, nf = NF, nab = 3, nb = 5;  // bf16 parts per operand; spectrum, X-operand and D-operand ring depths
 	void *W = nullptr;         // [B][nq] complex T
 	short *lq = nullptr, *mq = nullptr;
 	unsigned *err = nullptr;
@@ -643,9 +675,9 @@ static bool is_tc(int precision) { return precision == kPrecBF16x3 || precision 
 static size_t tc_smem_bytes(const BatchPlan &P)
 {
 	const size_t f = (size_t) P.nf * P.n_det * TM * 128;
-	const size_t aa = (size_t) NAB * P.B * P.npart * A_TILE;
-	const size_t bb = (size_t) NAB * P.B * P.npart * P.npad * KE * 2;
-	const size_t bars = 8 * (2 * P.nf + 3 * NAB + 1) + 16;
+	const size_t aa = (size_t) P.nab * P.B * P.npart * A_TILE;
+	const size_t bb = (size_t) P.nb * P.B * P.npart * P.npad * KE * 2;
+	const size_t bars = 8 * (2 * P.nf + 2 * P.nab + 2 * P.nb + 1) + 16;
 	// 1 KB for aligning the base, 4 KB of slack past the last tile
 	return 1024 + f + aa + bb + bars + 4096;
 }
@@ -793,9 +825,11 @@ void *batch_plan_create(const BatchPlanDesc &d, int precision)
 		P->Kst = (Ku + KB - 1) / KB;
 		P->npad = (Lp1 + 15) & ~15;
 		P->npart = precision == kPrecBF16x6 ? 3 : 2;
-		P->nf = precision == kPrecBF16x6 ? 2 : 3;
+		P->nf = NF;
+		P->nab = precision == kPrecBF16x6 ? 2 : 4;
+		P->nb = 3;
 		int cols = 32;
-		while(cols < 2 * B * P->npad)  // main and correction accumulators
+		while(cols < P->npart * B * P->npad)  // hi*hi and correction column blocks
 			cols <<= 1;
 		P->tmem_cols = cols;
 		if(P->npad > 256 || cols > 512) {
@@ -820,8 +854,8 @@ void *batch_plan_create(const BatchPlanDesc &d, int precision)
 				set_error("batch plan: shared-memory budget exceeded");
 				fail = true;
 			}
-			if(!fail && (cudaFuncSetAttribute(k_tc_contract<2, NF>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
-				     cudaFuncSetAttribute(k_tc_contract<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess)) {
+			if(!fail && (cudaFuncSetAttribute(k_tc_contract<2, NF, 4, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
+				     cudaFuncSetAttribute(k_tc_contract<3, NF, 2, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess)) {
 				set_error("batch plan: cannot reserve %zu bytes of shared memory", tc_smem_bytes(*P));
 				fail = true;
 			}
@@ -949,9 +983,9 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 		if(P->ev_begin)
 			cudaEventRecord(P->ev_begin, st);
 		if(P->npart == 3)
-			k_tc_contract<3, 2><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			k_tc_contract<3, NF, 2, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		else
-			k_tc_contract<2, NF><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			k_tc_contract<2, NF, 4, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		if(P->ev_end)
 			cudaEventRecord(P->ev_end, st);
 		launches++;
