@@ -66,6 +66,27 @@ size_t sphrad_batch_workspace_size(const sphrad_batch_plan *plan, int n_seg);
 int sphrad_batch_integrate(sphrad_batch_plan *plan, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky, void *workspace,
 			   size_t workspace_bytes, void *cuda_stream);
 
+/* sphrad_batch_integrate without a caller-supplied workspace, for callers
+ * that must not allocate device memory while they run: real-time pipelines
+ * that cannot afford the device-wide synchronisation cudaMalloc/cudaFree may
+ * cause, hosts that own all device memory through their own allocator or a
+ * fixed memory budget, and plug-ins whose host forbids allocation calls.
+ * This entry point calls no cudaMalloc, cudaFree or other allocating
+ * routine.  No counterpart in the reference.
+ *
+ * Its split-K scratch is a static 8 MiB array inside the library, held by
+ * every GPU that loads the library until the process exits; a call needing
+ * more (n_seg above 8 MiB / (n_baselines * round_up(l_max + 1, 4) * 4 B),
+ * about 19,000 segments for 3 baselines at l_max = 32, half that for
+ * SPHRAD_PREC_FP64) is refused with -1 and a message.  Each call zero-fills
+ * the part it uses before launching.  All calls share the array, so calls
+ * that overlap on the GPU (other streams, other threads) race and must be
+ * serialised by the caller.  The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  Arguments are those of
+ * sphrad_batch_integrate. */
+int sphrad_batch_integrate_noalloc(sphrad_batch_plan *plan, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky, void *cuda_stream);
+
 /* The same with host buffers: copies in, integrates, copies out and
  * synchronises (library-owned device buffers).  Use pinned host memory for
  * full copy bandwidth. */

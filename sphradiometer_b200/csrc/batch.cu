@@ -1113,6 +1113,65 @@ int batch_set_timing_events(void *pp, void *ev_begin, void *ev_end)
 	return 0;
 }
 
+// ------------------------------------------------------------------------
+// allocation-free variant
+// ------------------------------------------------------------------------
+// Split-K scratch for batch_run_noalloc: a fixed array in the module's own
+// device memory, so that entry point never asks the CUDA runtime for memory.
+// Every device that loads this library holds these bytes until the process
+// exits.  All calls share it, so calls that overlap on a GPU race.
+constexpr size_t kNoAllocScratchBytes = (size_t) 8 << 20;  // 8 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static void *g_noalloc_ptr[kMaxDevices];
+
+// Device address of the scratch array on the current device.  Host code
+// cannot name the array's device address directly; it is looked up once per
+// device with that device current.
+static int noalloc_scratch(void **out)
+{
+	int dev = 0;
+	CKB(cudaGetDevice(&dev));
+	if(dev < 0 || dev >= kMaxDevices) {
+		set_error("allocation-free integrate: device ordinal %d above %d", dev, kMaxDevices - 1);
+		return -1;
+	}
+	std::lock_guard<std::mutex> lk(g_noalloc_mu);
+	if(!g_noalloc_ptr[dev]) {
+		void *p = nullptr;
+		const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+		if(e != cudaSuccess || !p) {
+			set_error("allocation-free integrate: cudaGetSymbolAddress failed (%s)", cudaGetErrorString(e));
+			return -1;
+		}
+		g_noalloc_ptr[dev] = p;
+	}
+	*out = g_noalloc_ptr[dev];
+	return 0;
+}
+
+size_t batch_noalloc_capacity() { return kNoAllocScratchBytes; }
+
+int batch_run_noalloc(void *pp, const void *F, int S, long long ld, const double *gmst, void *sky, void *stream_v)
+{
+	BatchPlan *P = (BatchPlan *) pp;
+	const size_t need = batch_workspace_bytes(P, S);
+	if(need > kNoAllocScratchBytes) {
+		const size_t per_seg = batch_workspace_bytes(P, 1);
+		set_error("allocation-free integrate: %d segments need %zu bytes of scratch, above the %zu-byte static array (at most %zu segments for this plan)", S,
+			  need, kNoAllocScratchBytes, per_seg ? kNoAllocScratchBytes / per_seg : (size_t) 0);
+		return -1;
+	}
+	void *ws = nullptr;
+	if(noalloc_scratch(&ws))
+		return -1;
+	// the array keeps whatever the previous call left: zero the part used
+	CKB(cudaMemsetAsync(ws, 0, need ? need : 16, (cudaStream_t) stream_v));
+	return batch_run(P, F, S, ld, gmst, sky, ws, kNoAllocScratchBytes, stream_v, 0);
+}
+
 int batch_check_error(void *pp, unsigned *code)
 {
 	BatchPlan *P = (BatchPlan *) pp;

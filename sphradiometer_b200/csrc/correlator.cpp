@@ -22,6 +22,7 @@ const double *rotation_plan_flat_for(const struct sh_series_rotation_plan *plan,
 int batch_set_split(void *plan, int S, int ks);
 int batch_check_error(void *plan, unsigned *code);
 int batch_set_timing_events(void *plan, void *ev_begin, void *ev_end);
+int batch_run_noalloc(void *plan, const void *F, int S, long long ld, const double *gmst, void *sky, void *stream);
 int batch_autotune(void *plan, const void *F, int S, long long ld, void *sky, void *ws, size_t ws_bytes, void *stream);
 }  // namespace sphrad
 
@@ -728,6 +729,11 @@ extern "C" int sphrad_batch_autotune(sphrad_batch_plan *p, const void *fseries_d
 				     void *stream)
 {
 	return batch_autotune(p->impl, fseries_dev, n_seg, ld, sky_dev, workspace, workspace_bytes, stream);
+}
+
+extern "C" int sphrad_batch_integrate_noalloc(sphrad_batch_plan *p, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky, void *stream)
+{
+	return batch_run_noalloc(p->impl, fseries, n_seg, ld, gmst, sky, stream);
 }
 
 extern "C" int sphrad_batch_set_timing_events(sphrad_batch_plan *p, void *ev_begin, void *ev_end)
