@@ -161,6 +161,32 @@ def cpu_oracle_rate(net_tables, F_half, gmst, budget_s: float, threads: int):
     return sum(done) / el, sum(done), el
 
 
+def accuracy_report(S, net, base, n_check: int):
+    """Relative L2 error of the batched skies of every precision against the
+    FP64 oracle (correlator_network_integrate_power_fd + rotate_z restated)."""
+    import torch
+    from oracle import oracle as O
+    from sphradiometer_b200 import workload as W
+    pairs = [(1, 0), (2, 0), (2, 1)]
+    tabs = [(net.delay_table(k), net.rotation_flat(k)) for k in range(3)]
+    ref = np.zeros((n_check, (L_MAX + 1) ** 2), np.complex128)
+    for s in range(n_check):
+        F = W.full_from_half(base["F"][:, s, :], N_SAMPLES)
+        for k, (i, j) in enumerate(pairs):
+            ref[s] += O.baseline_integrate_power_fd(F[i], F[j], tabs[k][0], L_MAX, tabs[k][1]) / 3
+        ref[s] = O.rotate_z(ref[s], L_MAX, False, base["gmst"][s])
+    Fd = torch.from_numpy(np.ascontiguousarray(base["F"][:, :n_check, :])).cuda()
+    gd = torch.from_numpy(base["gmst"][:n_check].copy()).cuda()
+    out = {"segments": n_check, "metric": "relative L2 of the a_lm vs the FP64 oracle (whole sample; worst sky)"}
+    for prec in ("fp64", "fp32", "bf16x3", "bf16x6"):
+        bp = S.BatchPlan(net, prec)
+        sky = bp.integrate(Fd, gd).cpu().numpy()
+        bp.close()
+        worst = max(np.linalg.norm(sky[s] - ref[s]) / np.linalg.norm(ref[s]) for s in range(n_check))
+        out[prec] = [float(np.linalg.norm(sky - ref) / np.linalg.norm(ref)), float(worst)]
+    return out
+
+
 def run_reference(args):
     """--impl reference: the CPU oracle (FP64 restatement of the reference's
     own CPU path) on all host cores."""
@@ -327,7 +353,7 @@ def run(args):
         extra["split_vs_fp64_plain"] = value / world / plain
 
         # other precisions of the batched path, same workload and timing
-        for other in ("fp64", "fp32"):
+        for other in ("fp64", "fp32", "bf16x3", "bf16x6"):
             if other == prec:
                 continue
             op = S.BatchPlan(net, other)
@@ -359,6 +385,11 @@ def run(args):
             torch.cuda.synchronize()
             extra["c1_64_segments_per_launch_maps_per_s"] = 64 * 200 / (a.elapsed_time(b) / 1e3)
             bp64.close()
+
+        # accuracy of every precision against the FP64 oracle on a sample of
+        # segments (the oracle integrates the same delay tables, which the
+        # tests check against the oracle's own tables)
+        extra["accuracy"] = accuracy_report(S, net, base, min(32, base["F"].shape[1]))
 
         # CPU baseline: the oracle on the host cores, bounded sample
         tables = [(net.delay_table(k), net.rotation_flat(k)) for k in range(3)]
@@ -392,7 +423,7 @@ def run(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--segments", type=int, default=4096)
