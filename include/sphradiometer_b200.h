@@ -111,6 +111,53 @@ int sphrad_batch_set_timing_events(sphrad_batch_plan *plan, void *ev_begin, void
  * gave up (synchronises with the device). */
 int sphrad_batch_status(sphrad_batch_plan *plan);
 
+/* ---- sky grids and peak localisation (batched) -------------------------
+ *
+ * Inverse spherical-harmonic transforms of batches of skies onto an
+ * ntheta x nphi grid, and localisation of each sky's maximum of Re f.  No
+ * counterpart in the reference, which evaluates one series at a time
+ * (sh_series_to_mesh, sh_series_trans.c:796-871; sh_series_eval,
+ * sh_series_trans.c:257-291; sh_series_real_minimum,
+ * sh_series_extremize.c:273-360).
+ *
+ * Skies are device arrays [n_sky][(sky_l_max+1)^2] of double complex in
+ * the reference's m-major order (what sphrad_batch_integrate writes). */
+enum {
+	SPHRAD_GRID_GL = 0,   /* Gauss-Legendre rows of the reference's meshes
+			       * (sh_series_trans.c:149-196), increasing theta */
+	SPHRAD_GRID_CELL = 1  /* theta_i = pi (i + 1/2) / ntheta */
+};
+typedef struct sphrad_sky_grid sphrad_sky_grid;
+
+/* Tables for l <= l_max on the grid; columns are phi_j = 2 pi j / nphi.
+ * fp32 = 1 transforms in FP32, 0 in FP64.  NULL on failure. */
+sphrad_sky_grid *sphrad_sky_grid_new(unsigned l_max, int kind, int ntheta, int nphi, int fp32);
+void sphrad_sky_grid_free(sphrad_sky_grid *grid);
+/* Number of rows; their co-latitudes into theta (host, may be NULL). */
+int sphrad_sky_grid_rows(const sphrad_sky_grid *grid, double *theta);
+/* Device scratch for n_sky skies (render and arg max). */
+size_t sphrad_sky_grid_scratch_size(const sphrad_sky_grid *grid, int n_sky);
+/* out: device float [n_sky][ntheta][nphi] = Re f of each sky truncated at
+ * min(sky_l_max, the grid's l_max). */
+int sphrad_sky_render(sphrad_sky_grid *grid, const void *sky, int n_sky, unsigned sky_l_max, float *out, void *scratch, size_t scratch_bytes,
+		      void *cuda_stream);
+/* Grid pixel of the largest Re f of each sky truncated at l_use: device
+ * theta[n_sky], phi[n_sky] (ties go to the first pixel in row-major
+ * order, as the reference's scan, sh_series_extremize.c:214-229). */
+int sphrad_sky_grid_argmax(sphrad_sky_grid *grid, const void *sky, int n_sky, unsigned sky_l_max, unsigned l_use, double *theta, double *phi,
+			   void *scratch, size_t scratch_bytes, void *cuda_stream);
+/* Local maximum of Re f near (theta0, phi0), FP64 trust-region Newton
+ * iterations on analytic derivatives.  out: device [n_sky][4] = theta,
+ * phi, Re f there, angle moved from the start (rad); status: device
+ * [n_sky], bit 0 set when converged, iteration count in the bits above. */
+int sphrad_sky_refine_peaks(const void *sky, int n_sky, unsigned sky_l_max, const double *theta0, const double *phi0, double *out, int *status,
+			    void *cuda_stream);
+/* The reference's localisation applied to every sky (its extremizer on
+ * -Re f): brute-force search of the l <= 6 low-passed sky on its 14 x 14
+ * mesh, then refinement.  Arguments as sphrad_sky_refine_peaks; allocates
+ * its own scratch and returns when the work on the stream has finished. */
+int sphrad_sky_peaks(const void *sky, int n_sky, unsigned sky_l_max, double *out, int *status, void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -219,3 +219,178 @@ class BatchPlan:
             self.close()
         except Exception:
             pass
+
+
+GRID_GL = 0
+GRID_CELL = 1
+
+
+class SkyGrid:
+    """Batched inverse SHT onto a theta x phi grid (sphrad_sky_grid_*).
+
+    ``kind``: "gl" (the reference's Gauss-Legendre mesh rows) or "cell"
+    (theta_i = pi (i + 1/2) / ntheta); columns phi_j = 2 pi j / nphi.
+    ``render(sky)``: sky a complex128 CUDA tensor [n_sky][(L+1)^2] -> float32
+    [n_sky][ntheta][nphi] = Re f.  ``argmax(sky, l_use)`` -> (theta, phi)
+    float64 CUDA tensors of each sky's best pixel.
+    """
+
+    def __init__(self, l_max: int, ntheta: int, nphi: int, kind: str = "cell", fp32: bool = True):
+        self.l_max, self.ntheta, self.nphi = int(l_max), int(ntheta), int(nphi)
+        k = GRID_GL if kind == "gl" else GRID_CELL
+        self._g = _check(load().sphrad_sky_grid_new(self.l_max, k, self.ntheta, self.nphi, 1 if fp32 else 0), "sphrad_sky_grid_new")
+        self._scratch = None
+
+    def rows(self) -> np.ndarray:
+        th = np.empty(self.ntheta, np.float64)
+        load().sphrad_sky_grid_rows(self._g, th.ctypes.data)
+        return th
+
+    def _scr(self, n_sky: int):
+        import torch
+        need = load().sphrad_sky_grid_scratch_size(self._g, n_sky)
+        if self._scratch is None or self._scratch.numel() < need:
+            self._scratch = torch.empty(max(need, 16), dtype=torch.uint8, device="cuda")
+        return self._scratch
+
+    @staticmethod
+    def _sky_l(sky) -> int:
+        L = int(round(sky.shape[1] ** 0.5)) - 1
+        assert (L + 1) ** 2 == sky.shape[1], "sky rows must hold (l_max+1)^2 coefficients"
+        return L
+
+    def render(self, sky, out=None):
+        import torch
+        assert sky.is_cuda and sky.dtype == torch.complex128 and sky.is_contiguous()
+        n = sky.shape[0]
+        if out is None:
+            out = torch.empty((n, self.ntheta, self.nphi), dtype=torch.float32, device=sky.device)
+        scr = self._scr(n)
+        rc = load().sphrad_sky_render(self._g, sky.data_ptr(), n, self._sky_l(sky), out.data_ptr(), scr.data_ptr(), scr.numel(),
+                                      torch.cuda.current_stream().cuda_stream)
+        if rc:
+            raise SphradError("sphrad_sky_render: " + last_error())
+        return out
+
+    def argmax(self, sky, l_use: int | None = None):
+        import torch
+        assert sky.is_cuda and sky.dtype == torch.complex128 and sky.is_contiguous()
+        n = sky.shape[0]
+        L = self._sky_l(sky)
+        th = torch.empty(n, dtype=torch.float64, device=sky.device)
+        ph = torch.empty(n, dtype=torch.float64, device=sky.device)
+        scr = self._scr(n)
+        rc = load().sphrad_sky_grid_argmax(self._g, sky.data_ptr(), n, L, L if l_use is None else int(l_use), th.data_ptr(), ph.data_ptr(),
+                                           scr.data_ptr(), scr.numel(), torch.cuda.current_stream().cuda_stream)
+        if rc:
+            raise SphradError("sphrad_sky_grid_argmax: " + last_error())
+        return th, ph
+
+    def close(self):
+        if getattr(self, "_g", None):
+            load().sphrad_sky_grid_free(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def refine_peaks(sky, theta0, phi0):
+    """Local maxima of Re f from (theta0, phi0) (sphrad_sky_refine_peaks).
+    Returns (out [n][4] = theta, phi, Re f, angle moved; status [n])."""
+    import torch
+    n = sky.shape[0]
+    L = SkyGrid._sky_l(sky)
+    out = torch.empty((n, 4), dtype=torch.float64, device=sky.device)
+    st = torch.empty(n, dtype=torch.int32, device=sky.device)
+    rc = load().sphrad_sky_refine_peaks(sky.data_ptr(), n, L, theta0.contiguous().data_ptr(), phi0.contiguous().data_ptr(), out.data_ptr(),
+                                        st.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    if rc:
+        raise SphradError("sphrad_sky_refine_peaks: " + last_error())
+    return out, st
+
+
+def sky_peaks(sky):
+    """The reference's localisation (l <= 6 mesh search + refinement) of the
+    maximum of Re f of every sky (sphrad_sky_peaks)."""
+    import torch
+    n = sky.shape[0]
+    L = SkyGrid._sky_l(sky)
+    out = torch.empty((n, 4), dtype=torch.float64, device=sky.device)
+    st = torch.empty(n, dtype=torch.int32, device=sky.device)
+    rc = load().sphrad_sky_peaks(sky.data_ptr(), n, L, out.data_ptr(), st.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    if rc:
+        raise SphradError("sphrad_sky_peaks: " + last_error())
+    return out, st
+
+
+# ---- drop-in sh_series helpers over numpy coefficient vectors -------------
+
+def _with_series(coeff: np.ndarray, l_max: int, polar: bool):
+    return numpy_to_series(coeff, l_max, polar)
+
+
+def to_mesh(coeff: np.ndarray, l_max: int, polar: bool = False):
+    """sh_series_to_mesh: returns (mesh [nt][nphi] complex, cos theta rows)."""
+    L = load()
+    s = _with_series(coeff, l_max, polar)
+    try:
+        nt, npx = C.c_int(), C.c_int()
+        x = C.POINTER(C.c_double)()
+        m = L.sh_series_to_mesh(s, C.byref(nt), C.byref(npx), C.byref(x))
+        if not m:
+            raise SphradError("sh_series_to_mesh: " + last_error())
+        mesh = np.ctypeslib.as_array((C.c_double * (2 * nt.value * npx.value)).from_address(m)).view(np.complex128).reshape(nt.value, npx.value).copy()
+        cx = np.ctypeslib.as_array(x, shape=(nt.value,)).copy()
+        libc = C.CDLL(None)
+        libc.free(C.c_void_p(m))
+        libc.free(C.cast(x, C.c_void_p))
+        return mesh, cx
+    finally:
+        L.sh_series_free(s)
+
+
+def from_mesh(mesh: np.ndarray, l_max: int, polar: bool = False) -> np.ndarray:
+    """sh_series_from_mesh on a [2(l_max+1)]^2 complex mesh."""
+    L = load()
+    s = _check(L.sh_series_new(l_max, 1 if polar else 0), "sh_series_new")
+    try:
+        mesh = np.ascontiguousarray(mesh, np.complex128)
+        if not L.sh_series_from_mesh(s, mesh.ctypes.data):
+            raise SphradError("sh_series_from_mesh: " + last_error())
+        return series_to_numpy(s)
+    finally:
+        L.sh_series_free(s)
+
+
+def product(a: np.ndarray, la: int, pa: bool, b: np.ndarray, lb: int, pb: bool, ld: int, pd: bool) -> np.ndarray:
+    """sh_series_product through a product plan."""
+    L = load()
+    sa, sb = _with_series(a, la, pa), _with_series(b, lb, pb)
+    sd = _check(L.sh_series_new_zero(ld, 1 if pd else 0), "sh_series_new_zero")
+    plan = _check(L.sh_series_product_plan_new(sd, sa, sb), "sh_series_product_plan_new")
+    try:
+        if not L.sh_series_product(sd, sa, sb, plan):
+            raise SphradError("sh_series_product: " + last_error())
+        return series_to_numpy(sd)
+    finally:
+        L.sh_series_product_plan_free(plan)
+        for s in (sa, sb, sd):
+            L.sh_series_free(s)
+
+
+def real_minimum(coeff: np.ndarray, l_max: int, polar: bool = False):
+    """sh_series_real_minimum: (value, theta, phi)."""
+    L = load()
+    s = _with_series(coeff, l_max, polar)
+    try:
+        t, p = C.c_double(), C.c_double()
+        v = L.sh_series_real_minimum(s, C.byref(t), C.byref(p))
+        if v != v:
+            raise SphradError("sh_series_real_minimum: " + last_error())
+        return v, t.value, p.value
+    finally:
+        L.sh_series_free(s)

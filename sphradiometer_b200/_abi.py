@@ -157,6 +157,14 @@ SIGNATURES = {
     "sphrad_batch_status": (_i, [_vp]),
     "sphrad_batch_set_timing_events": (_i, [_vp, _vp, _vp]),
     "sphrad_batch_integrate_noalloc": (_i, [_vp, _vp, _i, _ll, _vp, _vp, _vp]),
+    "sphrad_sky_grid_new": (_vp, [_u, _i, _i, _i, _i]),
+    "sphrad_sky_grid_free": (None, [_vp]),
+    "sphrad_sky_grid_rows": (_i, [_vp, _vp]),
+    "sphrad_sky_grid_scratch_size": (_sz, [_vp, _i]),
+    "sphrad_sky_render": (_i, [_vp, _vp, _i, _u, _vp, _vp, _sz, _vp]),
+    "sphrad_sky_grid_argmax": (_i, [_vp, _vp, _i, _u, _u, _vp, _vp, _vp, _sz, _vp]),
+    "sphrad_sky_refine_peaks": (_i, [_vp, _i, _u, _vp, _vp, _vp, _vp, _vp]),
+    "sphrad_sky_peaks": (_i, [_vp, _i, _u, _vp, _vp, _vp]),
 }
 
 _lib = None

@@ -75,6 +75,13 @@ int ensure_device()
 	return 0;
 }
 
+int current_device()
+{
+	int dev = 0;
+	cudaGetDevice(&dev);
+	return dev;
+}
+
 void *lib_stream()
 {
 	int dev = 0;
@@ -85,6 +92,13 @@ void *lib_stream()
 }
 
 static cudaStream_t S() { return (cudaStream_t) lib_stream(); }
+
+int sync_stream(void *stream)
+{
+	CK(cudaStreamSynchronize(stream ? (cudaStream_t) stream : S()));
+	CK(cudaGetLastError());
+	return 0;
+}
 
 int stream_sync()
 {

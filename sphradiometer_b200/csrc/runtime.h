@@ -16,8 +16,10 @@ const char *last_error();
 // 0 when a CUDA device is current and usable, -1 (with the error set)
 // otherwise.  All library work goes to one non-blocking stream per device.
 int ensure_device();
+int current_device();
 void *lib_stream();  // cudaStream_t of the current device
 int stream_sync();
+int sync_stream(void *stream);  // a caller's cudaStream_t, NULL = library stream
 
 void *dmalloc(size_t bytes);  // NULL + error on failure
 void dfree(void *p);
@@ -92,5 +94,47 @@ int batch_run(void *plan, const void *F, int S, long long ld, const double *gmst
 int batch_run_host(void *plan, const void *F_host, int S, long long ld, const double *gmst_host, void *sky_host);
 int batch_pick_split(const void *plan, int S);
 int batch_last_kernel_count(const void *plan);
+
+// ---- spherical-harmonic transforms on theta x phi grids (sht.cu) -------
+// Gauss-Legendre nodes (decreasing x) and weights on [-1, 1] (host)
+void gl_nodes(int n, double *x, double *w);
+enum GridKind { kGridGL = 0, kGridEquiangular = 1 };
+enum PixOut { kPixComplex = 0, kPixReal = 1, kPixArgmax = 2 };
+// Tables for l <= L on an nt x nphi grid: GL rows (the reference's mesh
+// rows, increasing theta) or cell-centre rows theta_i = pi (i + 1/2) / nt;
+// columns phi_j = 2 pi j / nphi.  fp32 selects the transform arithmetic.
+void *sht_plan_create(unsigned L, int kind, int nt, int nphi, int fp32);
+void sht_plan_destroy(void *plan);
+int sht_plan_rows(const void *plan, double *theta);  // returns nt
+size_t sht_scratch_bytes(const void *plan, int S, int M);
+// coeff: device double2 [S][cstride] (layout L_in/polar), truncated at
+// Luse.  out: kPixComplex -> double2 (fp64 plan) or float2 (fp32 plan)
+// [S][nt][nphi]; kPixReal -> float [S][nt][nphi]; kPixArgmax -> per-row
+// best of sign * Re, sht_rowbest_bytes(plan, S) bytes, reduced by
+// sht_rows_argmax.  scratch: sht_scratch_bytes(plan, S, Luse or 0).
+int sht_synthesis(void *plan, const void *coeff, int S, long long cstride, unsigned L_in, int polar, unsigned Luse, int out_kind, void *out, void *scratch,
+		  void *stream, double sign);
+size_t sht_rowbest_bytes(const void *plan, int S);
+int sht_rows_argmax(void *plan, int S, const void *rowbest, double *theta, double *phi, double *value, void *stream);
+// mesh: device double2 [S][nt][nphi] -> coefficients (double2, layout
+// L_out/polar_out, stride ostride).  GL plans only (quadrature weights).
+int sht_analysis(void *plan, const void *mesh, int S, unsigned L_out, int polar_out, void *out, long long ostride, void *scratch, void *stream);
+// pixel-domain products of S pairs; the plan's grid must integrate degree
+// La + Lb + Ld exactly (GL rows >= (La+Lb+Ld+1)/2, columns > La+Lb+Ld)
+size_t sht_product_scratch_bytes(const void *plan, int S, unsigned La, int pa, unsigned Lb, int pb, unsigned Ld, int pd);
+int sht_product(void *plan, int S, const void *a, long long astride, unsigned La, int pa, const void *b, long long bstride, unsigned Lb, int pb, void *dest,
+		long long dstride, unsigned Ld, int pd, void *scratch, void *stream);
+// trust-region Newton refinement of the maximum of sign * Re f from
+// (theta0, phi0) per series; out [S][4] = theta, phi, Re f, angular
+// distance moved; status = converged | iterations << 1
+// in-place unnormalised DFT along the array index of n x stride host
+// complex values, e^{sign 2 pi i jk/n}
+int array_dft(int n, int stride, double *data, int sign);
+// the reference's extremization (l <= 6 mesh search, then refinement) of
+// the maximum of sign * Re f for S device series; returns after the work
+// on stream (NULL = library stream) has finished (host C++, sh_algebra.cpp)
+int extremum(const double *coeff_dev, long long cstride, int S, unsigned L, int polar, double sign, double *out_dev, int *status_dev, void *stream);
+int peak_refine(int S, unsigned L, int polar, const void *coeff, long long cstride, const double *theta0, const double *phi0, double sign, int max_iter,
+		double tol, double *out, int *status, void *stream);
 
 }  // namespace sphrad

@@ -1,0 +1,939 @@
+// sht.cu -- spherical-harmonic transforms between a_lm and theta x phi
+// grids, pixel-domain products, and the peak (extremum) finder.
+//
+// Reference algorithms (cannon-zz/sphradiometer):
+//   mesh layout      sh_series_trans.c:149-196 (2(l_max+1) Gauss-Legendre
+//                    rows ordered by increasing theta, 2(l_max+1) columns at
+//                    phi_j = 2 pi j / nphi)
+//   synthesis        sh_series_trans.c:796-871 (sh_series_to_mesh)
+//   analysis         sh_series_trans.c:575-659 (sh_series_from_mesh)
+//   product          sh_series_product.c:269-329 (pixel_domain_product)
+//   extremum         sh_series_extremize.c:168-360 (coarse mesh search of the
+//                    l <= 6 low-passed series, then local refinement)
+//
+// A transform is split into two stages over a per-series work array
+// F[s][i][m + M] (theta row i, azimuthal order m in [-M, M]):
+//   Legendre   F_m(theta_i) = sum_l a_lm lambda_l^|m|(cos theta_i)
+//              (times (-1)^m for m < 0: Y_{l,-m} = (-1)^m conj(Y_lm))
+//   azimuth    f(theta_i, phi_j) = sum_m F_m(theta_i) e^{i m phi_j}
+// and the reverse for analysis.  The azimuthal sums run directly over the
+// 2M+1 non-zero orders with an exact integer twiddle index (m j) mod nphi,
+// which also folds orders above the grid's Nyquist limit exactly as
+// evaluating e^{i m phi_j} would.  Legendre tables are built in FP64 by the
+// standard normalised three-term recurrence (GSL's sphPlm convention,
+// Condon-Shortley phase) and stored in the transform's arithmetic type.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "runtime.h"
+
+namespace sphrad {
+
+#define CK(call)                                                                 \
+	do {                                                                     \
+		cudaError_t e_ = (call);                                         \
+		if(e_ != cudaSuccess) {                                          \
+			set_error("%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+			return -1;                                               \
+		}                                                                \
+	} while(0)
+
+static cudaStream_t lstream() { return (cudaStream_t) lib_stream(); }
+
+namespace {
+
+template <class T> struct V2;
+template <> struct V2<float> { typedef float2 t; };
+template <> struct V2<double> { typedef double2 t; };
+
+__device__ __forceinline__ float2 mk2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double2 mk2(double a, double b) { return make_double2(a, b); }
+
+template <class T2> __device__ __forceinline__ T2 cmul2(T2 a, T2 b) { return mk2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+
+__device__ __forceinline__ long long lmoff(int L, int l, int m)
+{
+	const long long LL = L + 1;
+	const long long x = (long long) m * (m - 1);
+	const long long mo = (m >= 0) ? LL * m - x / 2 : LL * (LL + m) + x / 2;
+	return mo + l - (m < 0 ? -m : m);
+}
+
+// offset of order m's block in a Legendre table [m][l - m][i] of nt rows
+__host__ __device__ __forceinline__ long long tab_off(int L, int nt, int m) { return (long long) nt * ((long long) m * (L + 1) - (long long) m * (m - 1) / 2); }
+
+// log of the normalisation of lambda_m^m without the sin^m factor:
+// 0.5 log((2m+1)/(4 pi)) + sum_{k=1}^{m} 0.5 log((2k-1)/(2k))
+__device__ double lnpre_mm(int m)
+{
+	double v = 0.5 * log((2.0 * m + 1.0) / (4.0 * M_PI));
+	for(int k = 1; k <= m; k++)
+		v += 0.5 * log((2.0 * k - 1.0) / (2.0 * k));
+	return v;
+}
+
+// ---------------------------------------------------------------------------
+// Legendre table: tab[tab_off(m) + (l - m) nt + i] = lambda_l^m(x_i)
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_sht_table(int L, int nt, const double *x, T *tab)
+{
+	const int m = blockIdx.x;
+	const double lp = lnpre_mm(m);
+	T *base = tab + tab_off(L, nt, m);
+	for(int i = threadIdx.x; i < nt; i += blockDim.x) {
+		const double xi = x[i];
+		double pmm = (m > 0) ? exp(lp + 0.5 * m * log1p(-xi * xi)) : exp(lp);
+		if(m & 1)
+			pmm = -pmm;
+		base[i] = (T) pmm;
+		if(m == L)
+			continue;
+		double p0 = pmm, p1 = xi * sqrt(2.0 * m + 3.0) * pmm;
+		base[(long long) nt + i] = (T) p1;
+		for(int l = m + 2; l <= L; l++) {
+			const double a = sqrt((2.0 * l + 1.0) * (2.0 * l - 1.0) / ((double) (l - m) * (l + m)));
+			const double b = sqrt((2.0 * l + 1.0) * (l + m - 1.0) * (l - m - 1.0) / ((2.0 * l - 3.0) * (l - m) * (l + m)));
+			const double p = a * xi * p1 - b * p0;
+			base[(long long) (l - m) * nt + i] = (T) p;
+			p0 = p1;
+			p1 = p;
+		}
+	}
+}
+
+// twiddles tw[k] = e^{2 pi i k / nphi}, k < nphi
+template <class T>
+__global__ void k_twiddles(int nphi, typename V2<T>::t *tw)
+{
+	for(int k = blockIdx.x * blockDim.x + threadIdx.x; k < nphi; k += gridDim.x * blockDim.x) {
+		double s, c;
+		sincospi(2.0 * k / nphi, &s, &c);
+		tw[k] = mk2((T) c, (T) s);
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Legendre synthesis: F[s][i][m + M] = sum_{l = |m|}^{Luse} a_{s,lm} lambda
+// a_s in the reference layout (l_max L_in, polar flag) at coeff + s cstride.
+// One thread per (m, i); consecutive threads take consecutive rows so the
+// table reads coalesce.
+// ---------------------------------------------------------------------------
+template <class Tin2, class T>
+__global__ void k_sht_F(int L_in, int polar, const Tin2 *coeff, long long cstride, int Luse, int M, int Ltab, int nt, const T *tab,
+			typename V2<T>::t *F)
+{
+	const int W = 2 * M + 1;
+	const int tiles = (W * nt + blockDim.x - 1) / blockDim.x;
+	const int s = blockIdx.x / tiles;
+	const int idx = (blockIdx.x % tiles) * blockDim.x + threadIdx.x;
+	if(idx >= W * nt)
+		return;
+	const int i = idx % nt;
+	const int mi = idx / nt;
+	const int m = mi - M;
+	const int am = m < 0 ? -m : m;
+	const Tin2 *c = coeff + (long long) s * cstride;
+	T ar = 0, ai = 0;
+	if(!(polar && m != 0)) {
+		const T *t = tab + tab_off(Ltab, nt, am) + i;
+		for(int l = am; l <= Luse; l++) {
+			const Tin2 v = c[polar ? l : lmoff(L_in, l, m)];
+			const T p = t[(long long) (l - am) * nt];
+			ar += (T) v.x * p;
+			ai += (T) v.y * p;
+		}
+		if(m < 0 && (am & 1)) {
+			ar = -ar;
+			ai = -ai;
+		}
+	}
+	F[((long long) s * nt + i) * W + mi] = mk2(ar, ai);
+}
+
+// ---------------------------------------------------------------------------
+// azimuthal synthesis, one block per (row i, series s):
+//   v_j = sum_m F_m e^{2 pi i (m j mod nphi) / nphi}
+// MODE 0: complex mesh out (OutT2 = T2 or double2)
+// MODE 1: real part out as float
+// MODE 2: per-row arg max of sign * Re v (value, column) into rowbest
+// MODE 3: complex product of two series' rows (F and F2) out
+// ---------------------------------------------------------------------------
+struct RowBest {
+	double v;
+	int j;
+	int pad;
+};
+
+template <class T, int MODE, class OutT>
+__global__ void k_sht_pix(int nt, int nphi, int M, const typename V2<T>::t *F, const typename V2<T>::t *F2, const typename V2<T>::t *tw, OutT *out,
+			  double sign)
+{
+	typedef typename V2<T>::t T2;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int W = 2 * M + 1;
+	T2 *tws = (T2 *) smem_raw;
+	T2 *Fs = tws + nphi;
+	T2 *F2s = Fs + W;
+	const long long row = blockIdx.x;  // series * nt + theta row
+	for(int k = threadIdx.x; k < nphi; k += blockDim.x)
+		tws[k] = tw[k];
+	for(int k = threadIdx.x; k < W; k += blockDim.x) {
+		Fs[k] = F[row * W + k];
+		if(MODE == 3)
+			F2s[k] = F2[row * W + k];
+	}
+	__syncthreads();
+	double best = -INFINITY;
+	int bestj = 0;
+	const int mstart = ((-M) % nphi + nphi) % nphi;
+	for(int j = threadIdx.x; j < nphi; j += blockDim.x) {
+		int idx = (int) (((long long) mstart * j) % nphi);
+		T vr = 0, vi = 0, wr = 0, wi = 0;
+		for(int k = 0; k < W; k++) {
+			const T2 e = tws[idx];
+			const T2 f = Fs[k];
+			vr += f.x * e.x - f.y * e.y;
+			vi += f.x * e.y + f.y * e.x;
+			if(MODE == 3) {
+				const T2 g = F2s[k];
+				wr += g.x * e.x - g.y * e.y;
+				wi += g.x * e.y + g.y * e.x;
+			}
+			idx += j;
+			if(idx >= nphi)
+				idx -= nphi;
+		}
+		if(MODE == 0)
+			out[row * nphi + j] = OutT{vr, vi};
+		else if(MODE == 1)
+			((float *) out)[row * nphi + j] = (float) vr;
+		else if(MODE == 3)
+			out[row * nphi + j] = OutT{vr * wr - vi * wi, vr * wi + vi * wr};
+		else {
+			const double v = sign * (double) vr;
+			if(v > best) {
+				best = v;
+				bestj = j;
+			}
+		}
+	}
+	if(MODE == 2) {
+		// block arg max; ties go to the smallest column, as a sequential
+		// scan that keeps the first strict improvement would
+		for(int o = 16; o; o >>= 1) {
+			const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+			const int oj = __shfl_xor_sync(0xffffffffu, bestj, o);
+			if(ob > best || (ob == best && oj < bestj)) {
+				best = ob;
+				bestj = oj;
+			}
+		}
+		__shared__ double wb[32];
+		__shared__ int wj[32];
+		const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+		if(lane == 0) {
+			wb[warp] = best;
+			wj[warp] = bestj;
+		}
+		__syncthreads();
+		if(threadIdx.x == 0) {
+			for(int w = 1; w < (int) (blockDim.x >> 5); w++)
+				if(wb[w] > best || (wb[w] == best && wj[w] < bestj)) {
+					best = wb[w];
+					bestj = wj[w];
+				}
+			RowBest rb;
+			rb.v = best;
+			rb.j = bestj;
+			rb.pad = 0;
+			((RowBest *) out)[row] = rb;
+		}
+	}
+}
+
+// per-series arg max over rows -> start direction (theta, phi); rows in
+// increasing theta, ties to the first row (sequential scan order)
+__global__ void k_rows_argmax(int S, int nt, int nphi, const RowBest *rb, const double *theta_rows, double *theta, double *phi, double *value)
+{
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if(s >= S)
+		return;
+	double best = -INFINITY;
+	int bi = -1, bj = 0;
+	for(int i = 0; i < nt; i++) {
+		const RowBest r = rb[(long long) s * nt + i];
+		if(r.v > best) {
+			best = r.v;
+			bi = i;
+			bj = r.j;
+		}
+	}
+	if(bi < 0) {
+		theta[s] = phi[s] = NAN;
+		if(value)
+			value[s] = NAN;
+		return;
+	}
+	theta[s] = theta_rows[bi];
+	phi[s] = 2.0 * M_PI * bj / (double) nphi;
+	if(value)
+		value[s] = best;
+}
+
+// ---------------------------------------------------------------------------
+// azimuthal analysis, one block per (row i, series s), thread per order:
+//   H_m(theta_i) = (2 pi / nphi) w_i sum_j mesh_j e^{-2 pi i (m j mod nphi)/nphi}
+// ---------------------------------------------------------------------------
+template <class Tin2, class T>
+__global__ void k_sht_H(int nt, int nphi, int M, const Tin2 *mesh, const double *w, const typename V2<T>::t *tw, typename V2<T>::t *H)
+{
+	typedef typename V2<T>::t T2;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	T2 *tws = (T2 *) smem_raw;
+	T2 *row_s = tws + nphi;
+	const long long row = blockIdx.x;  // series * nt + theta row
+	const int i = (int) (row % nt);
+	const int W = 2 * M + 1;
+	for(int k = threadIdx.x; k < nphi; k += blockDim.x) {
+		tws[k] = tw[k];
+		const Tin2 v = mesh[row * nphi + k];
+		row_s[k] = mk2((T) v.x, (T) v.y);
+	}
+	__syncthreads();
+	const T scale = (T) (2.0 * M_PI / nphi * w[i]);
+	for(int mi = threadIdx.x; mi < W; mi += blockDim.x) {
+		const int m = mi - M;
+		const int step = ((m % nphi) + nphi) % nphi;
+		int idx = 0;
+		T hr = 0, hi = 0;
+		for(int j = 0; j < nphi; j++) {
+			const T2 e = tws[idx];
+			const T2 v = row_s[j];
+			// v * conj(e)
+			hr += v.x * e.x + v.y * e.y;
+			hi += v.y * e.x - v.x * e.y;
+			idx += step;
+			if(idx >= nphi)
+				idx -= nphi;
+		}
+		H[row * W + mi] = mk2(hr * scale, hi * scale);
+	}
+}
+
+// ---------------------------------------------------------------------------
+// Legendre analysis: a_lm = (-1)^m [m<0] sum_i H_m(theta_i) lambda_l^|m|(x_i)
+// One block per (order, series); warps over l, lanes over rows.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_sht_A(int L_out, int polar_out, int M, int Ltab, int nt, const typename V2<T>::t *H, const T *tab, double2 *out, long long ostride)
+{
+	typedef typename V2<T>::t T2;
+	const int W = 2 * M + 1;
+	const int mi = blockIdx.x % W, s = blockIdx.x / W;
+	const int m = mi - M;
+	const int am = m < 0 ? -m : m;
+	if(am > L_out || (polar_out && m != 0))
+		return;
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+	const T2 *h = H + (long long) s * nt * W + mi;
+	const T *t0 = tab + tab_off(Ltab, nt, am);
+	const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
+	for(int l = am + warp; l <= L_out; l += nw) {
+		const T *t = t0 + (long long) (l - am) * nt;
+		T ar = 0, ai = 0;
+		for(int i = lane; i < nt; i += 32) {
+			const T2 v = h[(long long) i * W];
+			const T p = t[i];
+			ar += v.x * p;
+			ai += v.y * p;
+		}
+		for(int o = 16; o; o >>= 1) {
+			ar += __shfl_xor_sync(0xffffffffu, ar, o);
+			ai += __shfl_xor_sync(0xffffffffu, ai, o);
+		}
+		if(lane == 0)
+			out[(long long) s * ostride + (polar_out ? l : lmoff(L_out, l, m))] = make_double2(sg * (double) ar, sg * (double) ai);
+	}
+}
+
+// zero-fill helper for outputs whose orders lie beyond what the analysis
+// writes (orders |m| > M of a non-polar destination)
+template <class Tout2>
+__global__ void k_zero2(long long n, Tout2 *p, long long stride, int S)
+{
+	for(long long k = blockIdx.x * (long long) blockDim.x + threadIdx.x; k < n * S; k += (long long) gridDim.x * blockDim.x) {
+		const long long s = k / n, e = k % n;
+		p[s * stride + e] = Tout2{0, 0};
+	}
+}
+
+// ---------------------------------------------------------------------------
+// peak refinement: one warp per series, FP64.  Maximises g = sign * Re f on
+// the sphere by trust-region Newton steps in the local orthonormal frame
+// (d theta, sin theta d phi) with the covariant Hessian; value, gradient and
+// Hessian come from one pass of the Legendre recurrences per step:
+//   d lambda_l/d theta = (l x lambda_l - c_l lambda_{l-1}) / sin theta,
+//     c_l = sqrt((2l+1)(l^2 - m^2)/(2l-1))
+//   d2 lambda/d theta2 = -(x / sin theta) d lambda/d theta
+//                        - (l(l+1) - m^2 / sin^2 theta) lambda
+// The first trust radius is pi/24, the reference's initial step
+// (sh_series_extremize.c:323).
+// ---------------------------------------------------------------------------
+struct PeakEval {
+	double f, ft, fp, ftt, ftp, fpp;
+};
+
+__device__ void peak_eval_order(int L, int polar, const double2 *c, int m, double x, double st, double phi, PeakEval &acc)
+{
+	const double lp = lnpre_mm(m);
+	double lam = exp(lp + m * log(st));
+	if(m & 1)
+		lam = -lam;
+	double lam_prev = 0;
+	double Ar = 0, Ai = 0, A1r = 0, A1i = 0, A2r = 0, A2i = 0;
+	double Br = 0, Bi = 0, B1r = 0, B1i = 0, B2r = 0, B2i = 0;
+	const double inv_s = 1.0 / st, cot = x / st, m2s = (double) m * m * inv_s * inv_s;
+	for(int l = m; l <= L; l++) {
+		if(l == m + 1) {
+			lam_prev = lam;
+			lam = x * sqrt(2.0 * m + 3.0) * lam;
+		} else if(l > m + 1) {
+			const double a = sqrt((2.0 * l + 1.0) * (2.0 * l - 1.0) / ((double) (l - m) * (l + m)));
+			const double b = sqrt((2.0 * l + 1.0) * (l + m - 1.0) * (l - m - 1.0) / ((2.0 * l - 3.0) * (l - m) * (l + m)));
+			const double p = a * x * lam - b * lam_prev;
+			lam_prev = lam;
+			lam = p;
+		}
+		const double cl = (l > m) ? sqrt((2.0 * l + 1.0) * ((double) l * l - (double) m * m) / (2.0 * l - 1.0)) : 0.0;
+		const double d1 = (l * x * lam - cl * lam_prev) * inv_s;
+		const double d2 = -cot * d1 - ((double) l * (l + 1) - m2s) * lam;
+		const double2 cp = c[polar ? l : lmoff(L, l, m)];
+		Ar += cp.x * lam;
+		Ai += cp.y * lam;
+		A1r += cp.x * d1;
+		A1i += cp.y * d1;
+		A2r += cp.x * d2;
+		A2i += cp.y * d2;
+		if(m > 0) {
+			const double2 cn = c[lmoff(L, l, -m)];
+			Br += cn.x * lam;
+			Bi += cn.y * lam;
+			B1r += cn.x * d1;
+			B1i += cn.y * d1;
+			B2r += cn.x * d2;
+			B2i += cn.y * d2;
+		}
+	}
+	if(m & 1) {
+		Br = -Br;
+		Bi = -Bi;
+		B1r = -B1r;
+		B1i = -B1i;
+		B2r = -B2r;
+		B2i = -B2i;
+	}
+	double sn, cs;
+	sincos(m * phi, &sn, &cs);
+	// A e^{i m phi} + B e^{-i m phi}
+	const double Re0 = Ar * cs - Ai * sn + Br * cs + Bi * sn;
+	const double ImA = Ar * sn + Ai * cs, ImB = Bi * cs - Br * sn;
+	const double Re1 = A1r * cs - A1i * sn + B1r * cs + B1i * sn;
+	const double ImA1 = A1r * sn + A1i * cs, ImB1 = B1i * cs - B1r * sn;
+	const double Re2 = A2r * cs - A2i * sn + B2r * cs + B2i * sn;
+	acc.f += Re0;
+	acc.ft += Re1;
+	acc.ftt += Re2;
+	// d/dphi: i m A e - i m B conj(e) -> Re = -m Im(A e) + m Im(B conj e)
+	acc.fp += -m * ImA + m * ImB;
+	acc.fpp += -(double) m * m * Re0;
+	acc.ftp += -m * ImA1 + m * ImB1;
+}
+
+__device__ PeakEval peak_eval(int L, int polar, const double2 *c, double theta, double phi)
+{
+	PeakEval e = {0, 0, 0, 0, 0, 0};
+	double st, x;
+	sincos(theta, &st, &x);
+	if(st < 1e-9)
+		st = 1e-9;
+	const int lane = threadIdx.x & 31;
+	const int M = polar ? 0 : L;
+	// pair order k with M - k so lanes carry equal recurrence lengths
+	for(int k = lane; k <= M / 2; k += 32) {
+		peak_eval_order(L, polar, c, k, x, st, phi, e);
+		if(M - k != k)
+			peak_eval_order(L, polar, c, M - k, x, st, phi, e);
+	}
+	for(int o = 16; o; o >>= 1) {
+		e.f += __shfl_xor_sync(0xffffffffu, e.f, o);
+		e.ft += __shfl_xor_sync(0xffffffffu, e.ft, o);
+		e.fp += __shfl_xor_sync(0xffffffffu, e.fp, o);
+		e.ftt += __shfl_xor_sync(0xffffffffu, e.ftt, o);
+		e.ftp += __shfl_xor_sync(0xffffffffu, e.ftp, o);
+		e.fpp += __shfl_xor_sync(0xffffffffu, e.fpp, o);
+	}
+	return e;
+}
+
+__device__ void condition_tp(double &t, double &p)
+{
+	t = fmod(t, 2 * M_PI);
+	if(t < 0)
+		t += 2 * M_PI;
+	if(t > M_PI) {
+		t = 2 * M_PI - t;
+		p += M_PI;
+	}
+	p = fmod(p, 2 * M_PI);
+	if(p < 0)
+		p += 2 * M_PI;
+}
+
+__device__ double ang_dist(double t1, double p1, double t2, double p2)
+{
+	const double x1 = sin(t1) * cos(p1), y1 = sin(t1) * sin(p1), z1 = cos(t1);
+	const double x2 = sin(t2) * cos(p2), y2 = sin(t2) * sin(p2), z2 = cos(t2);
+	const double cx = y1 * z2 - z1 * y2, cy = z1 * x2 - x1 * z2, cz = x1 * y2 - y1 * x2;
+	return atan2(sqrt(cx * cx + cy * cy + cz * cz), x1 * x2 + y1 * y2 + z1 * z2);
+}
+
+__global__ void k_peak_refine(int S, int L, int polar, const double2 *coeff, long long cstride, const double *theta0, const double *phi0, double sign,
+			      int max_iter, double tol, double *out /* [S][4] */, int *status)
+{
+	const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+	if(s >= S)
+		return;
+	const double2 *c = coeff + (long long) s * cstride;
+	double t = theta0[s], p = phi0[s];
+	if(!(t == t) || !(p == p)) {
+		if((threadIdx.x & 31) == 0) {
+			out[4 * s + 0] = out[4 * s + 1] = out[4 * s + 2] = out[4 * s + 3] = NAN;
+			status[s] = 0;
+		}
+		return;
+	}
+	condition_tp(t, p);
+	const double ts = t, ps = p;
+	double radius = M_PI / 24;
+	PeakEval e = peak_eval(L, polar, c, t, p);
+	double g = sign * e.f;
+	int it = 0, converged = 0;
+	for(; it < max_iter; it++) {
+		const double st = fmax(sin(t), 1e-9), ct = cos(t);
+		// gradient and covariant Hessian of g in the (u, v) frame
+		const double gu = sign * e.ft, gv = sign * e.fp / st;
+		const double huu = sign * e.ftt;
+		const double huv = sign * (e.ftp - ct / st * e.fp) / st;
+		const double hvv = sign * (e.fpp / (st * st) + ct / st * e.ft);
+		double du, dv;
+		const double det = huu * hvv - huv * huv;
+		if(huu < 0 && det > 0) {
+			du = -(hvv * gu - huv * gv) / det;
+			dv = -(-huv * gu + huu * gv) / det;
+		} else {
+			const double gn = sqrt(gu * gu + gv * gv);
+			du = gn > 0 ? radius * gu / gn : 0;
+			dv = gn > 0 ? radius * gv / gn : 0;
+		}
+		double len = sqrt(du * du + dv * dv);
+		if(len > radius) {
+			du *= radius / len;
+			dv *= radius / len;
+			len = radius;
+		}
+		if(len < tol) {
+			converged = 1;
+			break;
+		}
+		double tn = t + du, pn = p + dv / st;
+		condition_tp(tn, pn);
+		const PeakEval en = peak_eval(L, polar, c, tn, pn);
+		const double gn = sign * en.f;
+		if(gn >= g) {
+			t = tn;
+			p = pn;
+			e = en;
+			g = gn;
+			radius = fmin(2 * radius, M_PI / 24);
+		} else {
+			radius = 0.25 * len;
+			if(radius < tol) {
+				converged = 1;
+				break;
+			}
+		}
+	}
+	if((threadIdx.x & 31) == 0) {
+		out[4 * s + 0] = t;
+		out[4 * s + 1] = p;
+		out[4 * s + 2] = e.f;
+		out[4 * s + 3] = ang_dist(ts, ps, t, p);
+		status[s] = converged | (it << 1);
+	}
+}
+
+// ---------------------------------------------------------------------------
+// unnormalised DFT along the array index of every coefficient column
+// (sh_series_array.c:528-558):
+//   out[k][c] = sum_j in[j][c] e^{sign 2 pi i (j k mod n) / n}
+// one thread per (k, c); consecutive threads take consecutive columns
+// ---------------------------------------------------------------------------
+__global__ void k_array_dft(int n, int stride, const double2 *in, const double2 *tw, double sign, double2 *out)
+{
+	const int c = blockIdx.y * blockDim.x + threadIdx.x;
+	const int k = blockIdx.x;
+	if(c >= stride)
+		return;
+	double ar = 0, ai = 0;
+	int idx = 0;
+	for(int j = 0; j < n; j++) {
+		const double2 e = tw[idx];
+		const double2 v = in[(long long) j * stride + c];
+		const double es = sign * e.y;
+		ar += v.x * e.x - v.y * es;
+		ai += v.x * es + v.y * e.x;
+		idx += k;
+		if(idx >= n)
+			idx -= n;
+	}
+	out[(long long) k * stride + c] = make_double2(ar, ai);
+}
+
+}  // namespace
+
+// ===========================================================================
+// host side
+// ===========================================================================
+struct DevBuf {
+	void *p = nullptr;
+	DevBuf() = default;
+	explicit DevBuf(size_t bytes) { p = dmalloc(bytes); }
+	~DevBuf() { dfree(p); }
+	DevBuf(const DevBuf &) = delete;
+	DevBuf &operator=(const DevBuf &) = delete;
+	template <class T> T *as() const { return (T *) p; }
+};
+
+struct ShtPlan {
+	unsigned L = 0;       // table l_max
+	int kind = 0;         // kGridGL or kGridEquiangular
+	int nt = 0, nphi = 0;
+	int fp32 = 0;
+	std::vector<double> theta;  // row co-latitudes (increasing)
+	double *d_x = nullptr;      // cos theta_i
+	double *d_w = nullptr;      // quadrature weights (GL) or NULL
+	double *d_theta = nullptr;  // theta_i
+	void *d_tab = nullptr;      // Legendre table, double or float
+	void *d_tw = nullptr;       // twiddles, double2 or float2
+	~ShtPlan()
+	{
+		dfree(d_x);
+		dfree(d_w);
+		dfree(d_theta);
+		dfree(d_tab);
+		dfree(d_tw);
+	}
+};
+
+static size_t tab_len(unsigned L, int nt) { return (size_t) tab_off((int) L, nt, (int) L + 1); }
+
+void *sht_plan_create(unsigned L, int kind, int nt, int nphi, int fp32)
+{
+	if(ensure_device())
+		return nullptr;
+	if(nt < 1 || nphi < 1 || nt > 8192 || nphi > 8192 || L > 2048) {
+		set_error("sht plan: bad grid %d x %d or l_max %u", nt, nphi, L);
+		return nullptr;
+	}
+	ShtPlan *p = new ShtPlan;
+	p->L = L;
+	p->kind = kind;
+	p->nt = nt;
+	p->nphi = nphi;
+	p->fp32 = fp32 ? 1 : 0;
+	std::vector<double> x(nt), w(nt, 0.0);
+	p->theta.resize(nt);
+	if(kind == kGridGL) {
+		gl_nodes(nt, x.data(), w.data());  // decreasing x = increasing theta
+		for(int i = 0; i < nt; i++)
+			p->theta[i] = acos(x[i]);
+	} else {
+		for(int i = 0; i < nt; i++) {
+			p->theta[i] = M_PI * (i + 0.5) / nt;
+			x[i] = cos(p->theta[i]);
+		}
+	}
+	const size_t esz = fp32 ? sizeof(float) : sizeof(double);
+	p->d_x = (double *) dmalloc(nt * sizeof(double));
+	p->d_w = (double *) dmalloc(nt * sizeof(double));
+	p->d_theta = (double *) dmalloc(nt * sizeof(double));
+	p->d_tab = dmalloc(tab_len(L, nt) * esz);
+	p->d_tw = dmalloc((size_t) nphi * 2 * esz);
+	if(!p->d_x || !p->d_w || !p->d_theta || !p->d_tab || !p->d_tw || h2d(p->d_x, x.data(), nt * sizeof(double)) ||
+	   h2d(p->d_w, w.data(), nt * sizeof(double)) || h2d(p->d_theta, p->theta.data(), nt * sizeof(double))) {
+		delete p;
+		return nullptr;
+	}
+	const int tb = nt < 256 ? ((nt + 31) / 32) * 32 : 256;
+	if(fp32) {
+		k_sht_table<float><<<L + 1, tb, 0, lstream()>>>((int) L, nt, p->d_x, (float *) p->d_tab);
+		k_twiddles<float><<<(nphi + 255) / 256, 256, 0, lstream()>>>(nphi, (float2 *) p->d_tw);
+	} else {
+		k_sht_table<double><<<L + 1, tb, 0, lstream()>>>((int) L, nt, p->d_x, (double *) p->d_tab);
+		k_twiddles<double><<<(nphi + 255) / 256, 256, 0, lstream()>>>(nphi, (double2 *) p->d_tw);
+	}
+	if(cudaGetLastError() != cudaSuccess || stream_sync()) {
+		set_error("sht plan: table construction failed");
+		delete p;
+		return nullptr;
+	}
+	return p;
+}
+
+void sht_plan_destroy(void *plan) { delete (ShtPlan *) plan; }
+
+int sht_plan_rows(const void *plan, double *theta)
+{
+	const ShtPlan *p = (const ShtPlan *) plan;
+	if(theta)
+		memcpy(theta, p->theta.data(), p->nt * sizeof(double));
+	return p->nt;
+}
+
+// bytes of the per-series F array of a transform at order limit M
+static size_t f_bytes(const ShtPlan *p, int M) { return (size_t) p->nt * (2 * M + 1) * (p->fp32 ? sizeof(float2) : sizeof(double2)); }
+
+size_t sht_scratch_bytes(const void *plan, int S, int M) { return f_bytes((const ShtPlan *) plan, M) * (size_t) S; }
+
+template <class T>
+static int launch_F(const ShtPlan *p, const double2 *coeff, long long cstride, unsigned L_in, int polar, unsigned Luse, int M, int S, void *F,
+		    cudaStream_t st)
+{
+	const int W = 2 * M + 1;
+	const unsigned grid = (unsigned) ((W * p->nt + 127) / 128) * (unsigned) S;
+	k_sht_F<double2, T><<<grid, 128, 0, st>>>((int) L_in, polar, coeff, cstride, (int) Luse, M, (int) p->L, p->nt, (const T *) p->d_tab,
+						  (typename V2<T>::t *) F);
+	CK(cudaGetLastError());
+	return 0;
+}
+
+constexpr size_t kMaxDynSmem = 48 * 1024;
+static size_t align_up(size_t b) { return (b + 255) & ~(size_t) 255; }
+
+static int pix_threads(int nphi) { return nphi >= 256 ? 256 : ((nphi + 31) / 32) * 32; }
+
+int sht_synthesis(void *plan, const void *coeff, int S, long long cstride, unsigned L_in, int polar, unsigned Luse, int out_kind, void *out, void *scratch,
+		  void *stream, double sign)
+{
+	ShtPlan *p = (ShtPlan *) plan;
+	cudaStream_t st = stream ? (cudaStream_t) stream : lstream();
+	if(Luse > L_in)
+		Luse = L_in;
+	if(Luse > p->L) {
+		set_error("sht synthesis: l_max %u above the plan's %u", Luse, p->L);
+		return -1;
+	}
+	if(S <= 0)
+		return 0;
+	const int M = polar ? 0 : (int) Luse;
+	const int W = 2 * M + 1;
+	const int thr = pix_threads(p->nphi);
+	const unsigned grid = (unsigned) p->nt * (unsigned) S;
+	if((size_t) (p->nphi + W) * (p->fp32 ? sizeof(float2) : sizeof(double2)) > kMaxDynSmem) {
+		set_error("sht synthesis: grid of %d columns too wide", p->nphi);
+		return -1;
+	}
+	if(p->fp32) {
+		if(launch_F<float>(p, (const double2 *) coeff, cstride, L_in, polar, Luse, M, S, scratch, st))
+			return -1;
+		const size_t sm = (size_t) (p->nphi + W) * sizeof(float2);
+		const float2 *F = (const float2 *) scratch, *tw = (const float2 *) p->d_tw;
+		if(out_kind == kPixComplex)
+			k_sht_pix<float, 0, float2><<<grid, thr, sm, st>>>(p->nt, p->nphi, M, F, nullptr, tw, (float2 *) out, sign);
+		else if(out_kind == kPixReal)
+			k_sht_pix<float, 1, float2><<<grid, thr, sm, st>>>(p->nt, p->nphi, M, F, nullptr, tw, (float2 *) out, sign);
+		else
+			k_sht_pix<float, 2, float2><<<grid, thr, sm, st>>>(p->nt, p->nphi, M, F, nullptr, tw, (float2 *) out, sign);
+	} else {
+		if(launch_F<double>(p, (const double2 *) coeff, cstride, L_in, polar, Luse, M, S, scratch, st))
+			return -1;
+		const size_t sm = (size_t) (p->nphi + W) * sizeof(double2);
+		const double2 *F = (const double2 *) scratch, *tw = (const double2 *) p->d_tw;
+		if(out_kind == kPixComplex)
+			k_sht_pix<double, 0, double2><<<grid, thr, sm, st>>>(p->nt, p->nphi, M, F, nullptr, tw, (double2 *) out, sign);
+		else if(out_kind == kPixReal)
+			k_sht_pix<double, 1, double2><<<grid, thr, sm, st>>>(p->nt, p->nphi, M, F, nullptr, tw, (double2 *) out, sign);
+		else
+			k_sht_pix<double, 2, double2><<<grid, thr, sm, st>>>(p->nt, p->nphi, M, F, nullptr, tw, (double2 *) out, sign);
+	}
+	CK(cudaGetLastError());
+	return 0;
+}
+
+int sht_rows_argmax(void *plan, int S, const void *rowbest, double *theta, double *phi, double *value, void *stream)
+{
+	ShtPlan *p = (ShtPlan *) plan;
+	cudaStream_t st = stream ? (cudaStream_t) stream : lstream();
+	if(S <= 0)
+		return 0;
+	k_rows_argmax<<<(S + 127) / 128, 128, 0, st>>>(S, p->nt, p->nphi, (const RowBest *) rowbest, p->d_theta, theta, phi, value);
+	CK(cudaGetLastError());
+	return 0;
+}
+
+size_t sht_rowbest_bytes(const void *plan, int S) { return (size_t) ((const ShtPlan *) plan)->nt * S * sizeof(RowBest); }
+
+// analysis of complex meshes [S][nt][nphi] (double2) into coefficients
+// (double2, layout L_out/polar_out, stride ostride); orders above the
+// analysis limit are zero-filled
+int sht_analysis(void *plan, const void *mesh, int S, unsigned L_out, int polar_out, void *out, long long ostride, void *scratch, void *stream)
+{
+	ShtPlan *p = (ShtPlan *) plan;
+	cudaStream_t st = stream ? (cudaStream_t) stream : lstream();
+	if(L_out > p->L) {
+		set_error("sht analysis: l_max %u above the plan's %u", L_out, p->L);
+		return -1;
+	}
+	if(S <= 0)
+		return 0;
+	const int M = polar_out ? 0 : (int) L_out;
+	const int W = 2 * M + 1;
+	const int thr = pix_threads(p->nphi < W ? W : p->nphi);
+	if((size_t) 2 * p->nphi * (p->fp32 ? sizeof(float2) : sizeof(double2)) > kMaxDynSmem) {
+		set_error("sht analysis: grid of %d columns too wide", p->nphi);
+		return -1;
+	}
+	const unsigned grid = (unsigned) p->nt * (unsigned) S, agrid = (unsigned) W * (unsigned) S;
+	if(p->fp32) {
+		k_sht_H<double2, float><<<grid, thr, (size_t) 2 * p->nphi * sizeof(float2), st>>>(p->nt, p->nphi, M, (const double2 *) mesh, p->d_w,
+												    (const float2 *) p->d_tw, (float2 *) scratch);
+		k_sht_A<float><<<agrid, 256, 0, st>>>((int) L_out, polar_out, M, (int) p->L, p->nt, (const float2 *) scratch, (const float *) p->d_tab,
+								(double2 *) out, ostride);
+	} else {
+		k_sht_H<double2, double><<<grid, thr, (size_t) 2 * p->nphi * sizeof(double2), st>>>(p->nt, p->nphi, M, (const double2 *) mesh, p->d_w,
+												      (const double2 *) p->d_tw, (double2 *) scratch);
+		k_sht_A<double><<<agrid, 256, 0, st>>>((int) L_out, polar_out, M, (int) p->L, p->nt, (const double2 *) scratch,
+								 (const double *) p->d_tab, (double2 *) out, ostride);
+	}
+	CK(cudaGetLastError());
+	return 0;
+}
+
+// pixel-domain product (sh_series_product.c:269-329) of S pairs on one
+// plan whose grid integrates degree La + Lb + Ld exactly:
+//   dest = projection onto l <= Ld of (a b)
+// a, b, dest: double2 series arrays with the given layouts and strides.
+// scratch: 3 F arrays at order limit max(Ma, Mb, Md) + S complex meshes.
+// scratch of sht_product: F arrays of both factors at the product's order
+// limit, the S product meshes, and the analysis array at the destination's
+static void product_layout(const ShtPlan *p, int S, unsigned La, int pa, unsigned Lb, int pb, unsigned Ld, int pd, size_t *fb, size_t *mb, size_t *hb)
+{
+	const int M = (pa && pb) ? 0 : (int) (La > Lb ? La : Lb);
+	const int Md = (pd || (pa && pb)) ? 0 : (int) Ld;
+	*fb = align_up(f_bytes(p, M) * (size_t) S);
+	*mb = align_up((size_t) S * p->nt * p->nphi * sizeof(double2));
+	*hb = align_up(f_bytes(p, Md) * (size_t) S);
+}
+
+size_t sht_product_scratch_bytes(const void *plan, int S, unsigned La, int pa, unsigned Lb, int pb, unsigned Ld, int pd)
+{
+	size_t fb, mb, hb;
+	product_layout((const ShtPlan *) plan, S, La, pa, Lb, pb, Ld, pd, &fb, &mb, &hb);
+	return 2 * fb + mb + hb;
+}
+
+int sht_product(void *plan, int S, const void *a, long long astride, unsigned La, int pa, const void *b, long long bstride, unsigned Lb, int pb, void *dest,
+		long long dstride, unsigned Ld, int pd, void *scratch, void *stream)
+{
+	ShtPlan *p = (ShtPlan *) plan;
+	cudaStream_t st = stream ? (cudaStream_t) stream : lstream();
+	if(S <= 0)
+		return 0;
+	if(La > p->L || Lb > p->L || Ld > p->L) {
+		set_error("sht product: l_max above the plan's %u", p->L);
+		return -1;
+	}
+	const int M = (pa && pb) ? 0 : (int) (La > Lb ? La : Lb);
+	const int W = 2 * M + 1;
+	const size_t esz = p->fp32 ? sizeof(float2) : sizeof(double2);
+	const size_t sm = (size_t) (p->nphi + 2 * W) * esz;
+	if(sm > kMaxDynSmem) {
+		set_error("sht product: grid of %d columns too wide", p->nphi);
+		return -1;
+	}
+	size_t fb, mb, hb;
+	product_layout(p, S, La, pa, Lb, pb, Ld, pd, &fb, &mb, &hb);
+	char *Fa = (char *) scratch, *Fb = Fa + fb, *mesh = Fb + fb, *H = mesh + mb;
+	const int thr = pix_threads(p->nphi);
+	const unsigned grid = (unsigned) p->nt * (unsigned) S;
+	// F arrays at the common order limit M (a factor with fewer orders
+	// contributes zeros there)
+	auto fill = [&](const void *c, long long cs, unsigned Lc, int pc, char *F) -> int {
+		const unsigned g = (unsigned) ((W * p->nt + 127) / 128) * (unsigned) S;
+		if(p->fp32)
+			k_sht_F<double2, float><<<g, 128, 0, st>>>((int) Lc, pc, (const double2 *) c, cs, (int) Lc, M, (int) p->L, p->nt, (const float *) p->d_tab,
+								    (float2 *) F);
+		else
+			k_sht_F<double2, double><<<g, 128, 0, st>>>((int) Lc, pc, (const double2 *) c, cs, (int) Lc, M, (int) p->L, p->nt,
+								     (const double *) p->d_tab, (double2 *) F);
+		CK(cudaGetLastError());
+		return 0;
+	};
+	if(fill(a, astride, La, pa, Fa) || fill(b, bstride, Lb, pb, Fb))
+		return -1;
+	if(p->fp32)
+		k_sht_pix<float, 3, double2><<<grid, thr, sm, st>>>(p->nt, p->nphi, M, (const float2 *) Fa, (const float2 *) Fb, (const float2 *) p->d_tw,
+								    (double2 *) mesh, 1.0);
+	else
+		k_sht_pix<double, 3, double2><<<grid, thr, sm, st>>>(p->nt, p->nphi, M, (const double2 *) Fa, (const double2 *) Fb, (const double2 *) p->d_tw,
+								     (double2 *) mesh, 1.0);
+	CK(cudaGetLastError());
+	const int pd_eff = pd || (pa && pb);
+	if(pd_eff != pd) {
+		// polar product into a non-polar destination: zero the rest first
+		k_zero2<double2><<<256, 256, 0, st>>>((long long) (Ld + 1) * (Ld + 1), (double2 *) dest, dstride, S);
+		CK(cudaGetLastError());
+	}
+	return sht_analysis(plan, mesh, S, Ld, pd_eff, dest, dstride, H, stream);
+}
+
+int peak_refine(int S, unsigned L, int polar, const void *coeff, long long cstride, const double *theta0, const double *phi0, double sign, int max_iter,
+		double tol, double *out, int *status, void *stream)
+{
+	cudaStream_t st = stream ? (cudaStream_t) stream : lstream();
+	if(S <= 0)
+		return 0;
+	const int wpb = 4;
+	k_peak_refine<<<(S + wpb - 1) / wpb, 32 * wpb, 0, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out,
+								 status);
+	CK(cudaGetLastError());
+	return 0;
+}
+
+int array_dft(int n, int stride, double *data, int sign)
+{
+	if(ensure_device())
+		return -1;
+	if(n <= 0 || stride <= 0)
+		return 0;
+	const size_t bytes = (size_t) n * stride * sizeof(double2);
+	DevBuf din(bytes), dout(bytes), dtw((size_t) n * sizeof(double2));
+	if(!din.p || !dout.p || !dtw.p || h2d(din.p, data, bytes))
+		return -1;
+	k_twiddles<double><<<(n + 255) / 256, 256, 0, lstream()>>>(n, dtw.as<double2>());
+	const int thr = stride >= 128 ? 128 : ((stride + 31) / 32) * 32;
+	dim3 grid(n, (stride + thr - 1) / thr);
+	k_array_dft<<<grid, thr, 0, lstream()>>>(n, stride, din.as<double2>(), dtw.as<double2>(), sign < 0 ? -1.0 : 1.0, dout.as<double2>());
+	CK(cudaGetLastError());
+	if(d2h(data, dout.p, bytes))
+		return -1;
+	return stream_sync();
+}
+
+}  // namespace sphrad

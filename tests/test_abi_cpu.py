@@ -117,3 +117,27 @@ def test_gpu_entry_points_fail_loudly_without_a_device(S):
     L.sh_series_free(s)
     with pytest.raises(S.SphradError):
         S.Network(np.array([[0, 0, 0.001], [0.001, 0, 0]]), 64, 1.0 / 256, l_max=2)
+
+
+def test_library_wigner_3j_against_exact_values(S):
+    """sh_series_wigner_3j (host recursion in the library) against sympy's
+    exact 3-j symbols and the oracle, including the j1min = 0 and
+    single-term cases and large j."""
+    from sympy.physics.wigner import wigner_3j as exact
+    from oracle import oracle as O
+    L = S.load()
+    rng = np.random.default_rng(5)
+    cases = [(0, 0, 0, 0, 0, 0), (1, 1, 0, 0, 0, 0), (2, 1, 1, 0, 0, 0), (3, 2, 1, 1, -1, 0), (4, 2, 2, 0, 1, -1), (7, 3, 4, -2, 1, 1),
+             (10, 10, 0, 3, -3, 0), (5, 5, 10, 5, 5, -10), (2, 3, 4, 1, 1, -2), (3, 3, 3, 0, 0, 0), (1, 2, 5, 0, 0, 0)]
+    for _ in range(60):
+        j2, j3 = int(rng.integers(0, 25)), int(rng.integers(0, 25))
+        j1 = int(rng.integers(abs(j2 - j3), j2 + j3 + 1))
+        m2, m3 = int(rng.integers(-j2, j2 + 1)), int(rng.integers(-j3, j3 + 1))
+        cases.append((j1, j2, j3, -m2 - m3, m2, m3))
+    for args in cases:
+        ref = float(exact(*args).evalf(30))
+        got = L.sh_series_wigner_3j(*args)
+        assert abs(got - ref) <= 1e-13 * max(abs(ref), 1e-3), (args, got, ref)
+        assert abs(got - O.wigner_3j(*args)) <= 1e-13 * max(abs(ref), 1e-3)
+    for args in [(80, 60, 50, 3, -7, 4), (96, 48, 48, 0, 12, -12), (59, 59, 30, 20, -25, 5)]:
+        assert abs(L.sh_series_wigner_3j(*args) - O.wigner_3j(*args)) <= 1e-12 * max(abs(O.wigner_3j(*args)), 1e-6)
