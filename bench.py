@@ -161,9 +161,44 @@ def cpu_oracle_rate(net_tables, F_half, gmst, budget_s: float, threads: int):
     return sum(done) / el, sum(done), el
 
 
-def accuracy_report(S, net, base, n_check: int):
+def ang_deg(t1, p1, t2, p2):
+    u = np.array([np.sin(t1) * np.cos(p1), np.sin(t1) * np.sin(p1), np.cos(t1)])
+    w = np.array([np.sin(t2) * np.cos(p2), np.sin(t2) * np.sin(p2), np.cos(t2)])
+    return float(np.degrees(np.arctan2(np.linalg.norm(np.cross(u, w)), np.dot(u, w))))
+
+
+def mirror_partner(sky_ref, peak, positions, gmst):
+    """The other global maximum of a 3-detector sky: the power depends on
+    the source direction only through r_ij . s, so the Earth-frame map is
+    symmetric under reflection through the plane of the baselines; in the
+    output frame that plane is turned by the segment's z rotation.  Returns
+    the mirror image of ``peak`` (theta, phi) whose oracle value matches."""
+    from oracle import oracle as O
+    d1, d2 = positions[1] - positions[0], positions[2] - positions[0]
+    nrm = np.cross(d1, d2)
+    nrm /= np.linalg.norm(nrm)
+    t, p = peak
+    u = np.array([np.sin(t) * np.cos(p), np.sin(t) * np.sin(p), np.cos(t)])
+    f0 = O.eval_at(sky_ref, L_MAX, False, t, p).real
+    best = None
+    for sgn in (1.0, -1.0):
+        c, s_ = np.cos(sgn * gmst), np.sin(sgn * gmst)
+        nr = np.array([c * nrm[0] - s_ * nrm[1], s_ * nrm[0] + c * nrm[1], nrm[2]])
+        v = u - 2 * np.dot(u, nr) * nr
+        tv, pv = np.arccos(np.clip(v[2], -1, 1)), np.arctan2(v[1], v[0]) % (2 * np.pi)
+        dv = abs(O.eval_at(sky_ref, L_MAX, False, tv, pv).real - f0)
+        if best is None or dv < best[0]:
+            best = (dv, tv, pv)
+    return best[1], best[2]
+
+
+def accuracy_report(S, net, base, n_check: int, positions):
     """Relative L2 error of the batched skies of every precision against the
-    FP64 oracle (correlator_network_integrate_power_fd + rotate_z restated)."""
+    FP64 oracle (correlator_network_integrate_power_fd + rotate_z restated),
+    and the error of each sky's peak direction: the library's localisation
+    (sphrad_sky_peaks) of the GPU sky against the oracle's extremizer on the
+    oracle's sky, counted to the nearer of the oracle's peak and its mirror
+    image (the equal maximum every 3-detector sky has)."""
     import torch
     from oracle import oracle as O
     from sphradiometer_b200 import workload as W
@@ -175,16 +210,85 @@ def accuracy_report(S, net, base, n_check: int):
         for k, (i, j) in enumerate(pairs):
             ref[s] += O.baseline_integrate_power_fd(F[i], F[j], tabs[k][0], L_MAX, tabs[k][1]) / 3
         ref[s] = O.rotate_z(ref[s], L_MAX, False, base["gmst"][s])
+    ref_peaks = [O.real_maximum(ref[s], L_MAX, False) for s in range(n_check)]
+    mirrors = [mirror_partner(ref[s], ref_peaks[s][1:], positions, base["gmst"][s]) for s in range(n_check)]
     Fd = torch.from_numpy(np.ascontiguousarray(base["F"][:, :n_check, :])).cuda()
     gd = torch.from_numpy(base["gmst"][:n_check].copy()).cuda()
-    out = {"segments": n_check, "metric": "relative L2 of the a_lm vs the FP64 oracle (whole sample; worst sky)"}
+    out = {"segments": n_check,
+           "metric": "[relative L2 of the a_lm vs the FP64 oracle over the sample, worst sky, worst peak-direction error in degrees "
+                     "(to the nearer of the oracle's peak and its mirror image), skies whose peak is the mirror image]"}
     for prec in ("fp64", "fp32", "bf16x3", "bf16x6"):
         bp = S.BatchPlan(net, prec)
-        sky = bp.integrate(Fd, gd).cpu().numpy()
+        sky_d = bp.integrate(Fd, gd)
+        pk, _ = S.sky_peaks(sky_d)
+        sky, pk = sky_d.cpu().numpy(), pk.cpu().numpy()
         bp.close()
         worst = max(np.linalg.norm(sky[s] - ref[s]) / np.linalg.norm(ref[s]) for s in range(n_check))
-        out[prec] = [float(np.linalg.norm(sky - ref) / np.linalg.norm(ref)), float(worst)]
+        errs, n_mirror = [], 0
+        for s in range(n_check):
+            e0 = ang_deg(pk[s, 0], pk[s, 1], ref_peaks[s][1], ref_peaks[s][2])
+            e1 = ang_deg(pk[s, 0], pk[s, 1], mirrors[s][0], mirrors[s][1])
+            n_mirror += int(e1 < e0)
+            errs.append(min(e0, e1))
+        out[prec] = [float(np.linalg.norm(sky - ref) / np.linalg.norm(ref)), float(worst), float(max(errs)), n_mirror]
     return out
+
+
+def c0_report(S):
+    """The reference's single-baseline CPU case: one 1 s segment at 2048 Hz
+    from two detectors 3000 km apart, l_max 25, through the drop-in
+    correlator_network_integrate_power_fd (FP64 kernels), rendered to a
+    64 x 128 theta/phi grid and localised; each against the oracle."""
+    import torch
+    from oracle import oracle as O
+    from sphradiometer_b200 import workload as W
+    n, dt, L = 2048, 1.0 / 2048, 25
+    pos = W.pair_positions(3.0e6 / W.C_LIGHT, W.rng_for(1))
+    b = W.make_batch(pos, n, dt, 1, seed=77, snr_range=(12.0, 12.0))
+    F = W.full_from_half(b["F"][:, 0, :], n)
+    net = S.Network(pos, n, dt, l_max=L)
+    sky = net.integrate(F)
+    ref = O.NetworkPlan(pos, n, dt, L).integrate(F)
+    g = S.SkyGrid(L, 64, 128, kind="cell", fp32=True)
+    sd = torch.from_numpy(sky[None, :].copy()).cuda()
+    grid = g.render(sd).cpu().numpy()[0]
+    gref = O.render_grid(ref, L, False, 64, 128)
+    pk, _ = S.sky_peaks(sd)
+    pk = pk.cpu().numpy()[0]
+    rv, rt, rp = O.real_maximum(ref, L, False)
+    g.close()
+    net.close()
+    return {"alm_rel_l2": float(np.linalg.norm(sky - ref) / np.linalg.norm(ref)),
+            "grid_64x128_max_rel_err": float(np.max(np.abs(grid - gref)) / np.max(np.abs(gref))),
+            "peak_err_deg": ang_deg(pk[0], pk[1], rt, rp)}
+
+
+def sky_stage_rates(S, sky, reps: int = 5):
+    """Maps/s of the batched 64 x 128 render (FP32) and of the reference
+    localisation (l <= 6 mesh search + FP64 refinement) on device skies."""
+    import torch
+    n = sky.shape[0]
+    g = S.SkyGrid(L_MAX, 64, 128, kind="cell", fp32=True)
+    grid = torch.empty((n, 64, 128), dtype=torch.float32, device=sky.device)
+    g.render(sky, out=grid)
+    S.sky_peaks(sky)
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(reps):
+        g.render(sky, out=grid)
+    b.record(st)
+    torch.cuda.synchronize()
+    render = n * reps / (a.elapsed_time(b) / 1e3)
+    a.record(st)
+    for _ in range(reps):
+        S.sky_peaks(sky)
+    b.record(st)
+    torch.cuda.synchronize()
+    peaks = n * reps / (a.elapsed_time(b) / 1e3)
+    g.close()
+    return {"render_64x128_fp32_maps_per_s": render, "localise_maps_per_s": peaks}
 
 
 def run_reference(args):
@@ -389,7 +493,9 @@ def run(args):
         # accuracy of every precision against the FP64 oracle on a sample of
         # segments (the oracle integrates the same delay tables, which the
         # tests check against the oracle's own tables)
-        extra["accuracy"] = accuracy_report(S, net, base, min(32, base["F"].shape[1]))
+        extra["accuracy"] = accuracy_report(S, net, base, min(32, base["F"].shape[1]), pos)
+        extra["c0"] = c0_report(S)
+        extra.update(sky_stage_rates(S, out))
 
         # CPU baseline: the oracle on the host cores, bounded sample
         tables = [(net.delay_table(k), net.rotation_flat(k)) for k in range(3)]

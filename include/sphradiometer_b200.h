@@ -158,6 +158,34 @@ int sphrad_sky_refine_peaks(const void *sky, int n_sky, unsigned sky_l_max, cons
  * its own scratch and returns when the work on the stream has finished. */
 int sphrad_sky_peaks(const void *sky, int n_sky, unsigned sky_l_max, double *out, int *status, void *cuda_stream);
 
+/* ---- batched spherical-harmonic algebra -------------------------------
+ *
+ * Rotation: out[s] = sh_series_rotate(in[s], plan of R[s]) for n series
+ * (sh_series_rotation.c:287-422, 546-589), without materialising the
+ * plans: each series' Wigner-D matrices are built by the reference's FP64
+ * recursion from its 3x3 rotation matrix and applied at once, in FP32
+ * (fp32_apply = 1) or FP64.  in: device [n][len] double complex (len =
+ * l_max + 1 when polar, else (l_max+1)^2); R: device [n][9] doubles,
+ * row-major as euler_rotation_matrix returns them; out: device
+ * [n][(l_max+1)^2] double complex (non-polar). */
+size_t sphrad_sh_rotate_batch_scratch_size(unsigned l_max, int n);
+int sphrad_sh_rotate_batch(const void *in, int n, unsigned l_max, int polar, const double *R, void *out, int fp32_apply, void *scratch,
+			   size_t scratch_bytes, void *cuda_stream);
+
+/* Products: dest[s] = sh_series_product(a[s], b[s]) truncated at
+ * dest_l_max, for n pairs of non-polar series (sh_series_product.c:269-349),
+ * in the pixel domain on a Gauss-Legendre grid that integrates
+ * a b conj(Y_lm) exactly; transforms in FP32 (fp32 = 1) or FP64.
+ * a: device [n][(a_l_max+1)^2], b: [n][(b_l_max+1)^2], dest:
+ * [n][(dest_l_max+1)^2] double complex; dest coefficients above
+ * a_l_max + b_l_max are zero. */
+typedef struct sphrad_sh_product_grid sphrad_sh_product_grid;
+sphrad_sh_product_grid *sphrad_sh_product_grid_new(unsigned a_l_max, unsigned b_l_max, unsigned dest_l_max, int fp32);
+void sphrad_sh_product_grid_free(sphrad_sh_product_grid *grid);
+size_t sphrad_sh_product_scratch_size(const sphrad_sh_product_grid *grid, int n);
+int sphrad_sh_product_batch(sphrad_sh_product_grid *grid, const void *a, const void *b, int n, void *dest, void *scratch, size_t scratch_bytes,
+			    void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -394,3 +394,58 @@ def real_minimum(coeff: np.ndarray, l_max: int, polar: bool = False):
         return v, t.value, p.value
     finally:
         L.sh_series_free(s)
+
+
+# ---- batched spherical-harmonic algebra ------------------------------------
+
+def rotate_batch(series, R, l_max: int, polar: bool = False, fp32: bool = True, out=None):
+    """sphrad_sh_rotate_batch: series complex128 CUDA [n][len], R float64
+    CUDA [n][3][3] (or [n][9]) -> complex128 [n][(l_max+1)^2]."""
+    import torch
+    n = series.shape[0]
+    assert series.is_cuda and series.dtype == torch.complex128 and series.is_contiguous()
+    R = R.reshape(n, 9).contiguous()
+    if out is None:
+        out = torch.empty((n, (l_max + 1) ** 2), dtype=torch.complex128, device=series.device)
+    need = load().sphrad_sh_rotate_batch_scratch_size(l_max, n)
+    scr = torch.empty(max(need, 16), dtype=torch.uint8, device=series.device)
+    rc = load().sphrad_sh_rotate_batch(series.data_ptr(), n, l_max, int(polar), R.data_ptr(), out.data_ptr(), int(fp32), scr.data_ptr(), need,
+                                       torch.cuda.current_stream().cuda_stream)
+    if rc:
+        raise SphradError("sphrad_sh_rotate_batch: " + last_error())
+    return out
+
+
+class ProductGrid:
+    """Batched pixel-domain products (sphrad_sh_product_*):
+    ``multiply(a, b)`` for complex128 CUDA [n][(la+1)^2], [n][(lb+1)^2]."""
+
+    def __init__(self, a_l_max: int, b_l_max: int, dest_l_max: int, fp32: bool = True):
+        self.la, self.lb, self.ld = int(a_l_max), int(b_l_max), int(dest_l_max)
+        self._g = _check(load().sphrad_sh_product_grid_new(self.la, self.lb, self.ld, int(fp32)), "sphrad_sh_product_grid_new")
+        self._scr = None
+
+    def multiply(self, a, b, out=None):
+        import torch
+        n = a.shape[0]
+        if out is None:
+            out = torch.empty((n, (self.ld + 1) ** 2), dtype=torch.complex128, device=a.device)
+        need = load().sphrad_sh_product_scratch_size(self._g, n)
+        if self._scr is None or self._scr.numel() < need:
+            self._scr = torch.empty(max(need, 16), dtype=torch.uint8, device=a.device)
+        rc = load().sphrad_sh_product_batch(self._g, a.contiguous().data_ptr(), b.contiguous().data_ptr(), n, out.data_ptr(), self._scr.data_ptr(),
+                                            self._scr.numel(), torch.cuda.current_stream().cuda_stream)
+        if rc:
+            raise SphradError("sphrad_sh_product_batch: " + last_error())
+        return out
+
+    def close(self):
+        if getattr(self, "_g", None):
+            load().sphrad_sh_product_grid_free(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -165,6 +165,12 @@ SIGNATURES = {
     "sphrad_sky_grid_argmax": (_i, [_vp, _vp, _i, _u, _u, _vp, _vp, _vp, _sz, _vp]),
     "sphrad_sky_refine_peaks": (_i, [_vp, _i, _u, _vp, _vp, _vp, _vp, _vp]),
     "sphrad_sky_peaks": (_i, [_vp, _i, _u, _vp, _vp, _vp]),
+    "sphrad_sh_rotate_batch_scratch_size": (_sz, [_u, _i]),
+    "sphrad_sh_rotate_batch": (_i, [_vp, _i, _u, _i, _vp, _vp, _i, _vp, _sz, _vp]),
+    "sphrad_sh_product_grid_new": (_vp, [_u, _u, _u, _i]),
+    "sphrad_sh_product_grid_free": (None, [_vp]),
+    "sphrad_sh_product_scratch_size": (_sz, [_vp, _i]),
+    "sphrad_sh_product_batch": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _sz, _vp]),
 }
 
 _lib = None

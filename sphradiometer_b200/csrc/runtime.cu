@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "runtime.h"
+#include "wigner.cuh"
 
 namespace sphrad {
 
@@ -133,6 +134,12 @@ int h2d(void *dst, const void *src, size_t bytes)
 int d2h(void *dst, const void *src, size_t bytes)
 {
 	CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, S()));
+	return 0;
+}
+
+int dmemset_async(void *dst, int value, size_t bytes, void *stream)
+{
+	CK(cudaMemsetAsync(dst, value, bytes, stream ? (cudaStream_t) stream : S()));
 	return 0;
 }
 
@@ -407,21 +414,6 @@ size_t rot_offset(unsigned l)
 	return (4 * L * L * L - L - 3) / 3;
 }
 
-__device__ __forceinline__ size_t d_rot_offset(int l)
-{
-	if(l <= 1)
-		return 0;
-	const size_t L = l;
-	return (4 * L * L * L - L - 3) / 3;
-}
-
-#define DEL(Dp, l, m, mp) (Dp)[(size_t) (2 * (l) + 1) * ((mp) + (l)) + ((m) + (l))]
-
-__device__ __forceinline__ double rc_a(int l, int m, int mp) { return sqrt((double) (l + m) * (l - m) / ((double) (l + mp) * (l - mp))); }
-__device__ __forceinline__ double rc_b(int l, int m, int mp) { return sqrt((double) (l + m) * (l + m - 1) / (2.0 * (l + mp) * (l - mp))); }
-__device__ __forceinline__ double rc_c(int l, int m, int mp) { return sqrt(2.0 * (l + m) * (l - m) / ((double) (l + mp) * (l + mp - 1))); }
-__device__ __forceinline__ double rc_d(int l, int m, int mp) { return sqrt((double) (l + m) * (l + m - 1) / ((double) (l + mp) * (l + mp - 1))); }
-
 // One block per plan.  The l = 1 matrix (equations 5.3-5.5 of Choi et al.)
 // is built from R; level l is then computed from level l - 1 and level 1,
 // one element per thread, with a block barrier between levels.
@@ -433,26 +425,15 @@ __global__ void __launch_bounds__(ROT_THREADS) k_rotation_plan(int l_max, const 
 	const double *R = R_all + 9 * blockIdx.x;
 	double2 *Dall = D_all + plan_stride * blockIdx.x;
 	if(threadIdx.x == 0) {
-		enum { x = 0, y = 1, z = 2 };
-		const double s2 = sqrt(2.0);
-		// index (m, m') -> (m'+1)*3 + (m+1)
-		d1[0 * 3 + 0] = make_double2((R[3 * y + y] + R[3 * x + x]) / 2, -(R[3 * x + y] - R[3 * y + x]) / 2);  // (-1,-1)
-		d1[1 * 3 + 0] = make_double2(R[3 * z + x] / s2, -R[3 * z + y] / s2);                                    // (-1, 0)
-		d1[2 * 3 + 0] = make_double2((R[3 * y + y] - R[3 * x + x]) / 2, (R[3 * x + y] + R[3 * y + x]) / 2);   // (-1,+1)
-		d1[0 * 3 + 1] = make_double2(R[3 * x + z] / s2, R[3 * y + z] / s2);                                     // ( 0,-1)
-		d1[1 * 3 + 1] = make_double2(R[3 * z + z], 0.0);                                                        // ( 0, 0)
-		d1[2 * 3 + 1] = make_double2(-R[3 * x + z] / s2, R[3 * y + z] / s2);                                    // ( 0,+1)
-		d1[0 * 3 + 2] = make_double2((R[3 * y + y] - R[3 * x + x]) / 2, -(R[3 * x + y] + R[3 * y + x]) / 2);  // (+1,-1)
-		d1[1 * 3 + 2] = make_double2(-R[3 * z + x] / s2, -R[3 * z + y] / s2);                                   // (+1, 0)
-		d1[2 * 3 + 2] = make_double2((R[3 * y + y] + R[3 * x + x]) / 2, -(R[3 * y + x] - R[3 * x + y]) / 2);  // (+1,+1)
+		wig_d1(R, d1);
 		for(int k = 0; k < 9; k++)
 			Dall[k] = d1[k];
 	}
 	__syncthreads();
 	auto D1 = [&](int m, int mp) { return d1[(mp + 1) * 3 + (m + 1)]; };
 	for(int l = 2; l <= l_max; l++) {
-		const double2 *Dp = Dall + d_rot_offset(l - 1);
-		double2 *D = Dall + d_rot_offset(l);
+		const double2 *Dp = Dall + wig_offset(l - 1);
+		double2 *D = Dall + wig_offset(l);
 		const int w = 2 * l + 1;
 		const int lp = l - 1;
 		for(int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
@@ -462,60 +443,60 @@ __global__ void __launch_bounds__(ROT_THREADS) k_rotation_plan(int l_max, const 
 			if(mp > -l && mp < l) {
 				// (6.1), (6.4), (6.5)
 				if(abs(m) != l) {
-					const double2 t = cmul(D1(0, 0), DEL(Dp, lp, m, mp));
-					const double c = rc_a(l, m, mp);
+					const double2 t = cmul(D1(0, 0), WDEL(Dp, lp, m, mp));
+					const double c = wig_a(l, m, mp);
 					v.x += c * t.x;
 					v.y += c * t.y;
 				}
 				if(m > -l + 1) {
-					const double2 t = cmul(D1(1, 0), DEL(Dp, lp, m - 1, mp));
-					const double c = rc_b(l, m, mp);
+					const double2 t = cmul(D1(1, 0), WDEL(Dp, lp, m - 1, mp));
+					const double c = wig_b(l, m, mp);
 					v.x += c * t.x;
 					v.y += c * t.y;
 				}
 				if(-m > -l + 1) {
-					const double2 t = cmul(D1(-1, 0), DEL(Dp, lp, m + 1, mp));
-					const double c = rc_b(l, -m, mp);
+					const double2 t = cmul(D1(-1, 0), WDEL(Dp, lp, m + 1, mp));
+					const double c = wig_b(l, -m, mp);
 					v.x += c * t.x;
 					v.y += c * t.y;
 				}
 			} else if(mp == -l) {
 				// (6.9), (6.12), (6.13)
 				if(abs(m) != l) {
-					const double2 t = cmul(D1(0, -1), DEL(Dp, lp, m, mp + 1));
-					const double c = rc_c(l, m, -mp);
+					const double2 t = cmul(D1(0, -1), WDEL(Dp, lp, m, mp + 1));
+					const double c = wig_c(l, m, -mp);
 					v.x += c * t.x;
 					v.y += c * t.y;
 				}
 				if(m > -l + 1) {
-					const double2 t = cmul(D1(1, -1), DEL(Dp, lp, m - 1, mp + 1));
-					const double c = rc_d(l, m, -mp);
+					const double2 t = cmul(D1(1, -1), WDEL(Dp, lp, m - 1, mp + 1));
+					const double c = wig_d(l, m, -mp);
 					v.x += c * t.x;
 					v.y += c * t.y;
 				}
 				if(-m > -l + 1) {
-					const double2 t = cmul(D1(-1, -1), DEL(Dp, lp, m + 1, mp + 1));
-					const double c = rc_d(l, -m, -mp);
+					const double2 t = cmul(D1(-1, -1), WDEL(Dp, lp, m + 1, mp + 1));
+					const double c = wig_d(l, -m, -mp);
 					v.x += c * t.x;
 					v.y += c * t.y;
 				}
 			} else {
 				// mp == l: (6.14), (6.12), (6.13)
 				if(abs(m) != l) {
-					const double2 t = cmul(D1(0, 1), DEL(Dp, lp, m, mp - 1));
-					const double c = rc_c(l, m, mp);
+					const double2 t = cmul(D1(0, 1), WDEL(Dp, lp, m, mp - 1));
+					const double c = wig_c(l, m, mp);
 					v.x += c * t.x;
 					v.y += c * t.y;
 				}
 				if(m > -l + 1) {
-					const double2 t = cmul(D1(1, 1), DEL(Dp, lp, m - 1, mp - 1));
-					const double c = rc_d(l, m, mp);
+					const double2 t = cmul(D1(1, 1), WDEL(Dp, lp, m - 1, mp - 1));
+					const double c = wig_d(l, m, mp);
 					v.x += c * t.x;
 					v.y += c * t.y;
 				}
 				if(-m > -l + 1) {
-					const double2 t = cmul(D1(-1, 1), DEL(Dp, lp, m + 1, mp - 1));
-					const double c = rc_d(l, -m, mp);
+					const double2 t = cmul(D1(-1, 1), WDEL(Dp, lp, m + 1, mp - 1));
+					const double c = wig_d(l, -m, mp);
 					v.x += c * t.x;
 					v.y += c * t.y;
 				}
@@ -567,13 +548,13 @@ __global__ void k_rotate(int L, int polar, const double2 *Dall, const double2 *i
 		if(l == 0)
 			c = in[0];
 		else {
-			const double2 *D = Dall + d_rot_offset(l);
+			const double2 *D = Dall + wig_offset(l);
 			if(polar)
-				c = cmul(DEL(D, l, 0, mp), in[l]);
+				c = cmul(WDEL(D, l, 0, mp), in[l]);
 			else {
 				c = make_double2(0, 0);
 				for(int m = -l; m <= l; m++) {
-					const double2 t = cmul(DEL(D, l, m, mp), in[d_lmoffset(L, l, m)]);
+					const double2 t = cmul(WDEL(D, l, m, mp), in[d_lmoffset(L, l, m)]);
 					c.x += t.x;
 					c.y += t.y;
 				}
@@ -700,9 +681,9 @@ __global__ void k_rotate_sum(const DevJob *jobs, int n_jobs, int L, double2 *sky
 				c = cmul(J.rot[(size_t) l * l + (mp + l)], J.P[l]);
 			else {
 				c = make_double2(0, 0);
-				const double2 *D = J.rot + d_rot_offset(l);
+				const double2 *D = J.rot + wig_offset(l);
 				for(int m = -l; m <= l; m++) {
-					const double2 t = cmul(DEL(D, l, m, mp), J.P[d_lmoffset(J.l_max, l, m)]);
+					const double2 t = cmul(WDEL(D, l, m, mp), J.P[d_lmoffset(J.l_max, l, m)]);
 					c.x += t.x;
 					c.y += t.y;
 				}

@@ -26,6 +26,7 @@ void dfree(void *p);
 int h2d(void *dst, const void *src, size_t bytes);       // async on lib stream
 int d2h(void *dst, const void *src, size_t bytes);       // async on lib stream
 int dmemset(void *dst, int value, size_t bytes);         // async on lib stream
+int dmemset_async(void *dst, int value, size_t bytes, void *stream);  // NULL = lib stream
 
 // ---- FP64 plan construction -------------------------------------------
 // Polar delay table of one baseline (delay_product after
@@ -118,15 +119,25 @@ size_t sht_rowbest_bytes(const void *plan, int S);
 int sht_rows_argmax(void *plan, int S, const void *rowbest, double *theta, double *phi, double *value, void *stream);
 // mesh: device double2 [S][nt][nphi] -> coefficients (double2, layout
 // L_out/polar_out, stride ostride).  GL plans only (quadrature weights).
-int sht_analysis(void *plan, const void *mesh, int S, unsigned L_out, int polar_out, void *out, long long ostride, void *scratch, void *stream);
+// L_layout (>= L_out) is the l_max of the output's coefficient layout;
+// orders and degrees above L_out are left untouched
+int sht_analysis(void *plan, const void *mesh, int S, unsigned L_out, int polar_out, void *out, long long ostride, void *scratch, void *stream,
+		 unsigned L_layout = 0);
 // pixel-domain products of S pairs; the plan's grid must integrate degree
 // La + Lb + Ld exactly (GL rows >= (La+Lb+Ld+1)/2, columns > La+Lb+Ld)
 size_t sht_product_scratch_bytes(const void *plan, int S, unsigned La, int pa, unsigned Lb, int pb, unsigned Ld, int pd);
 int sht_product(void *plan, int S, const void *a, long long astride, unsigned La, int pa, const void *b, long long bstride, unsigned Lb, int pb, void *dest,
-		long long dstride, unsigned Ld, int pd, void *scratch, void *stream);
+		long long dstride, unsigned Ld, int pd, void *scratch, void *stream, unsigned Ld_layout = 0);
 // trust-region Newton refinement of the maximum of sign * Re f from
 // (theta0, phi0) per series; out [S][4] = theta, phi, Re f, angular
 // distance moved; status = converged | iterations << 1
+// ---- batched rotation (algebra.cu) -------------------------------------
+// out_s = rotation of series s (device double2, layout L/polar) by the
+// Wigner-D matrices of R_s (device [n][9] row-major); FP64 recursion,
+// FP32 (fp32_apply) or FP64 application; out non-polar [n][(L+1)^2]
+size_t rotate_batch_scratch_bytes(unsigned L, int n);
+int rotate_batch(const void *in, int n, unsigned L, int polar, const double *R, void *out, int fp32_apply, void *scratch, size_t scratch_bytes,
+		 void *stream);
 // in-place unnormalised DFT along the array index of n x stride host
 // complex values, e^{sign 2 pi i jk/n}
 int array_dft(int n, int stride, double *data, int sign);

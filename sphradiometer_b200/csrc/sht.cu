@@ -331,7 +331,8 @@ __global__ void k_sht_H(int nt, int nphi, int M, const Tin2 *mesh, const double 
 // One block per (order, series); warps over l, lanes over rows.
 // ---------------------------------------------------------------------------
 template <class T>
-__global__ void k_sht_A(int L_out, int polar_out, int M, int Ltab, int nt, const typename V2<T>::t *H, const T *tab, double2 *out, long long ostride)
+__global__ void k_sht_A(int L_out, int L_lay, int polar_out, int M, int Ltab, int nt, const typename V2<T>::t *H, const T *tab, double2 *out,
+			long long ostride)
 {
 	typedef typename V2<T>::t T2;
 	const int W = 2 * M + 1;
@@ -358,7 +359,7 @@ __global__ void k_sht_A(int L_out, int polar_out, int M, int Ltab, int nt, const
 			ai += __shfl_xor_sync(0xffffffffu, ai, o);
 		}
 		if(lane == 0)
-			out[(long long) s * ostride + (polar_out ? l : lmoff(L_out, l, m))] = make_double2(sg * (double) ar, sg * (double) ai);
+			out[(long long) s * ostride + (polar_out ? l : lmoff(L_lay, l, m))] = make_double2(sg * (double) ar, sg * (double) ai);
 	}
 }
 
@@ -792,8 +793,11 @@ size_t sht_rowbest_bytes(const void *plan, int S) { return (size_t) ((const ShtP
 // analysis of complex meshes [S][nt][nphi] (double2) into coefficients
 // (double2, layout L_out/polar_out, stride ostride); orders above the
 // analysis limit are zero-filled
-int sht_analysis(void *plan, const void *mesh, int S, unsigned L_out, int polar_out, void *out, long long ostride, void *scratch, void *stream)
+int sht_analysis(void *plan, const void *mesh, int S, unsigned L_out, int polar_out, void *out, long long ostride, void *scratch, void *stream,
+		 unsigned L_layout)
 {
+	if(L_layout < L_out)
+		L_layout = L_out;
 	ShtPlan *p = (ShtPlan *) plan;
 	cudaStream_t st = stream ? (cudaStream_t) stream : lstream();
 	if(L_out > p->L) {
@@ -813,12 +817,12 @@ int sht_analysis(void *plan, const void *mesh, int S, unsigned L_out, int polar_
 	if(p->fp32) {
 		k_sht_H<double2, float><<<grid, thr, (size_t) 2 * p->nphi * sizeof(float2), st>>>(p->nt, p->nphi, M, (const double2 *) mesh, p->d_w,
 												    (const float2 *) p->d_tw, (float2 *) scratch);
-		k_sht_A<float><<<agrid, 256, 0, st>>>((int) L_out, polar_out, M, (int) p->L, p->nt, (const float2 *) scratch, (const float *) p->d_tab,
+		k_sht_A<float><<<agrid, 256, 0, st>>>((int) L_out, (int) L_layout, polar_out, M, (int) p->L, p->nt, (const float2 *) scratch, (const float *) p->d_tab,
 								(double2 *) out, ostride);
 	} else {
 		k_sht_H<double2, double><<<grid, thr, (size_t) 2 * p->nphi * sizeof(double2), st>>>(p->nt, p->nphi, M, (const double2 *) mesh, p->d_w,
 												      (const double2 *) p->d_tw, (double2 *) scratch);
-		k_sht_A<double><<<agrid, 256, 0, st>>>((int) L_out, polar_out, M, (int) p->L, p->nt, (const double2 *) scratch,
+		k_sht_A<double><<<agrid, 256, 0, st>>>((int) L_out, (int) L_layout, polar_out, M, (int) p->L, p->nt, (const double2 *) scratch,
 								 (const double *) p->d_tab, (double2 *) out, ostride);
 	}
 	CK(cudaGetLastError());
@@ -849,9 +853,11 @@ size_t sht_product_scratch_bytes(const void *plan, int S, unsigned La, int pa, u
 }
 
 int sht_product(void *plan, int S, const void *a, long long astride, unsigned La, int pa, const void *b, long long bstride, unsigned Lb, int pb, void *dest,
-		long long dstride, unsigned Ld, int pd, void *scratch, void *stream)
+		long long dstride, unsigned Ld, int pd, void *scratch, void *stream, unsigned Ld_layout)
 {
 	ShtPlan *p = (ShtPlan *) plan;
+	if(Ld_layout < Ld)
+		Ld_layout = Ld;
 	cudaStream_t st = stream ? (cudaStream_t) stream : lstream();
 	if(S <= 0)
 		return 0;
@@ -897,10 +903,10 @@ int sht_product(void *plan, int S, const void *a, long long astride, unsigned La
 	const int pd_eff = pd || (pa && pb);
 	if(pd_eff != pd) {
 		// polar product into a non-polar destination: zero the rest first
-		k_zero2<double2><<<256, 256, 0, st>>>((long long) (Ld + 1) * (Ld + 1), (double2 *) dest, dstride, S);
+		k_zero2<double2><<<256, 256, 0, st>>>((long long) (Ld_layout + 1) * (Ld_layout + 1), (double2 *) dest, dstride, S);
 		CK(cudaGetLastError());
 	}
-	return sht_analysis(plan, mesh, S, Ld, pd_eff, dest, dstride, H, stream);
+	return sht_analysis(plan, mesh, S, Ld, pd_eff, dest, dstride, H, stream, Ld_layout);
 }
 
 int peak_refine(int S, unsigned L, int polar, const void *coeff, long long cstride, const double *theta0, const double *phi0, double sign, int max_iter,

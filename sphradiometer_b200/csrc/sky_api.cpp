@@ -2,9 +2,15 @@
 // over sht.cu; declared in sphradiometer_b200.h).
 #include <sphradiometer_b200.h>
 
+#include <cuda_runtime_api.h>
+
 #include "abi_common.h"
 
 using namespace sphrad;
+
+// A caller's NULL stream is CUDA's legacy default stream (the internal
+// functions take NULL as the library's own stream)
+static void *caller_stream(void *stream) { return stream ? stream : (void *) cudaStreamLegacy; }
 
 struct sphrad_sky_grid {
 	void *plan;
@@ -67,7 +73,7 @@ extern "C" int sphrad_sky_render(sphrad_sky_grid *g, const void *sky, int n_sky,
 		return -1;
 	const unsigned Luse = sky_l_max < g->l_max ? sky_l_max : g->l_max;
 	const long long stride = (long long) (sky_l_max + 1) * (sky_l_max + 1);
-	return sht_synthesis(g->plan, sky, n_sky, stride, sky_l_max, 0, Luse, kPixReal, out, scratch, stream, 1.0);
+	return sht_synthesis(g->plan, sky, n_sky, stride, sky_l_max, 0, Luse, kPixReal, out, scratch, caller_stream(stream), 1.0);
 }
 
 extern "C" int sphrad_sky_grid_argmax(sphrad_sky_grid *g, const void *sky, int n_sky, unsigned sky_l_max, unsigned l_use, double *theta, double *phi,
@@ -82,9 +88,9 @@ extern "C" int sphrad_sky_grid_argmax(sphrad_sky_grid *g, const void *sky, int n
 		Luse = g->l_max;
 	const long long stride = (long long) (sky_l_max + 1) * (sky_l_max + 1);
 	char *rb = (char *) scratch + align256(sht_scratch_bytes(g->plan, n_sky, (int) g->l_max));
-	if(sht_synthesis(g->plan, sky, n_sky, stride, sky_l_max, 0, Luse, kPixArgmax, rb, scratch, stream, 1.0))
+	if(sht_synthesis(g->plan, sky, n_sky, stride, sky_l_max, 0, Luse, kPixArgmax, rb, scratch, caller_stream(stream), 1.0))
 		return -1;
-	return sht_rows_argmax(g->plan, n_sky, rb, theta, phi, nullptr, stream);
+	return sht_rows_argmax(g->plan, n_sky, rb, theta, phi, nullptr, caller_stream(stream));
 }
 
 extern "C" int sphrad_sky_refine_peaks(const void *sky, int n_sky, unsigned sky_l_max, const double *theta0, const double *phi0, double *out, int *status,
@@ -93,7 +99,7 @@ extern "C" int sphrad_sky_refine_peaks(const void *sky, int n_sky, unsigned sky_
 	if(ensure_device())
 		return -1;
 	const long long stride = (long long) (sky_l_max + 1) * (sky_l_max + 1);
-	return peak_refine(n_sky, sky_l_max, 0, sky, stride, theta0, phi0, 1.0, 100, 1e-11, out, status, stream);
+	return peak_refine(n_sky, sky_l_max, 0, sky, stride, theta0, phi0, 1.0, 100, 1e-11, out, status, caller_stream(stream));
 }
 
 extern "C" int sphrad_sky_peaks(const void *sky, int n_sky, unsigned sky_l_max, double *out, int *status, void *stream)
@@ -101,5 +107,69 @@ extern "C" int sphrad_sky_peaks(const void *sky, int n_sky, unsigned sky_l_max, 
 	if(n_sky <= 0)
 		return 0;
 	const long long stride = (long long) (sky_l_max + 1) * (sky_l_max + 1);
-	return extremum((const double *) sky, stride, n_sky, sky_l_max, 0, 1.0, out, status, stream);
+	return extremum((const double *) sky, stride, n_sky, sky_l_max, 0, 1.0, out, status, caller_stream(stream));
+}
+
+// ---- batched spherical-harmonic algebra ------------------------------------
+extern "C" size_t sphrad_sh_rotate_batch_scratch_size(unsigned l_max, int n) { return rotate_batch_scratch_bytes(l_max, n); }
+
+extern "C" int sphrad_sh_rotate_batch(const void *in, int n, unsigned l_max, int polar, const double *R, void *out, int fp32_apply, void *scratch,
+				      size_t scratch_bytes, void *stream)
+{
+	return rotate_batch(in, n, l_max, polar ? 1 : 0, R, out, fp32_apply, scratch, scratch_bytes, caller_stream(stream));
+}
+
+struct sphrad_sh_product_grid {
+	void *plan;
+	unsigned la, lb, ld, lan;
+};
+
+extern "C" sphrad_sh_product_grid *sphrad_sh_product_grid_new(unsigned a_l_max, unsigned b_l_max, unsigned dest_l_max, int fp32)
+{
+	const unsigned lan = dest_l_max < a_l_max + b_l_max ? dest_l_max : a_l_max + b_l_max;
+	const unsigned deg = a_l_max + b_l_max + lan;
+	unsigned Lt = a_l_max > b_l_max ? a_l_max : b_l_max;
+	if(lan > Lt)
+		Lt = lan;
+	void *p = sht_plan_create(Lt, kGridGL, (int) (deg / 2 + 1), (int) deg + 1, fp32);
+	if(!p)
+		return NULL;
+	sphrad_sh_product_grid *g = (sphrad_sh_product_grid *) malloc(sizeof(*g));
+	if(!g) {
+		sht_plan_destroy(p);
+		return NULL;
+	}
+	*g = {p, a_l_max, b_l_max, dest_l_max, lan};
+	return g;
+}
+
+extern "C" void sphrad_sh_product_grid_free(sphrad_sh_product_grid *g)
+{
+	if(g)
+		sht_plan_destroy(g->plan);
+	free(g);
+}
+
+extern "C" size_t sphrad_sh_product_scratch_size(const sphrad_sh_product_grid *g, int n)
+{
+	return n > 0 ? sht_product_scratch_bytes(g->plan, n, g->la, 0, g->lb, 0, g->lan, 0) : 0;
+}
+
+extern "C" int sphrad_sh_product_batch(sphrad_sh_product_grid *g, const void *a, const void *b, int n, void *dest, void *scratch, size_t scratch_bytes,
+				       void *stream)
+{
+	if(n <= 0)
+		return 0;
+	if(scratch_bytes < sphrad_sh_product_scratch_size(g, n)) {
+		set_error("sphrad_sh_product_batch: scratch of %zu bytes, %zu needed", scratch_bytes, sphrad_sh_product_scratch_size(g, n));
+		return -1;
+	}
+	const long long as = (long long) (g->la + 1) * (g->la + 1), bs = (long long) (g->lb + 1) * (g->lb + 1);
+	const long long ds = (long long) (g->ld + 1) * (g->ld + 1);
+	if(g->lan < g->ld) {
+		// coefficients above the product's bandwidth are zero
+		if(dmemset_async(dest, 0, (size_t) n * ds * 16, caller_stream(stream)))
+			return -1;
+	}
+	return sht_product(g->plan, n, a, as, g->la, 0, b, bs, g->lb, 0, dest, ds, g->lan, 0, scratch, caller_stream(stream), g->ld);
 }
