@@ -186,6 +186,62 @@ size_t sphrad_sh_product_scratch_size(const sphrad_sh_product_grid *grid, int n)
 int sphrad_sh_product_batch(sphrad_sh_product_grid *grid, const void *a, const void *b, int n, void *dest, void *scratch, size_t scratch_bytes,
 			    void *cuda_stream);
 
+/* ---- learned peak proposal ---------------------------------------------
+ *
+ * A multilayer perceptron (338 -> 512 -> 512 -> 512 -> 3, GELU, bf16
+ * weights, FP32 accumulation; every layer a tcgen05 GEMM) that maps the
+ * l <= 12 a_lm of a sky (169 complex values, scaled to unit norm) to a
+ * proposed direction of its maximum.  No counterpart in the reference: the
+ * proposal seeds the extremizer (sh_series_extremize.c:273-360), which
+ * refines it, judges it, and falls back to a full-grid search when the
+ * proposal misses.  Training runs on the GPU by the same kernels (forward,
+ * backward, Adam); the loss is the mean of 1 - cos(angle to the target).
+ * Batches hold at most max_batch skies; device arrays throughout. */
+typedef struct sphrad_proposal sphrad_proposal;
+
+sphrad_proposal *sphrad_proposal_new(int max_batch, unsigned long long seed);
+void sphrad_proposal_free(sphrad_proposal *p);
+/* FP32 parameters (or gradients of the last backward pass), host arrays
+ * of sphrad_proposal_n_params() floats: W1 [512][338], b1, W2 [512][512],
+ * b2, W3 [512][512], b3, W4 [3][512], b4 (row-major, out x in). */
+size_t sphrad_proposal_n_params(void);
+int sphrad_proposal_get_params(sphrad_proposal *p, float *host);
+int sphrad_proposal_set_params(sphrad_proposal *p, const float *host);
+int sphrad_proposal_get_grads(sphrad_proposal *p, float *host);
+/* features: device float [n][338] from skies [n][(l_max+1)^2] (l_max >= 12) */
+int sphrad_proposal_sky_features(sphrad_proposal *p, const void *sky, int n, unsigned l_max, float *features, void *cuda_stream);
+/* load features (device [n][338]) as the next batch; for_training also
+ * keeps what the backward pass needs */
+int sphrad_proposal_load(sphrad_proposal *p, const float *features, int n, int for_training, void *cuda_stream);
+/* dir: device float [n][3] unit vectors (may be NULL) */
+int sphrad_proposal_forward(sphrad_proposal *p, int n, int for_training, float *dir, void *cuda_stream);
+/* gradients of the loss against targets (device float [n][3] unit vectors) */
+int sphrad_proposal_backward(sphrad_proposal *p, int n, const float *target, void *cuda_stream);
+int sphrad_proposal_adam(sphrad_proposal *p, float learning_rate, void *cuda_stream);
+/* mean loss of the last backward pass (synchronises) */
+float sphrad_proposal_loss(sphrad_proposal *p, int n);
+/* Skies of a 3-detector network are symmetric under reflection through the
+ * plane of its baselines (the delays depend on the source direction only
+ * through r_ij . s), so their maximum is defined up to that mirror image.
+ * normal: that plane's normal in the skies' frame, or NULL for none. */
+int sphrad_proposal_set_mirror(sphrad_proposal *p, const double *normal);
+/* Localisation of n skies (in the frame the network was trained in):
+ * proposal, FP64 refinement of the maximum of Re f from it, and its
+ * judgement on the coarse `judge` grid: accepted when the refinement
+ * converged, moved at most max_move_deg, reached a value f > 0 that no
+ * judge pixel exceeds, and every judge pixel farther than basin_deg from
+ * the refined peak (and from its mirror image) stays below
+ * f (1 - dominance); the rest get the full-grid search on `grid` (its
+ * pixel of largest Re f, then the same refinement).  out:
+ * device [n][4] as sphrad_sky_refine_peaks; status: device [n], bit 0
+ * converged, bits 1-23 iterations, bit 24 set for skies that fell back;
+ * *n_fallback (host) counts them.  Synchronises with the stream once per
+ * 16384 skies. */
+int sphrad_proposal_localise(sphrad_proposal *p, sphrad_sky_grid *judge, sphrad_sky_grid *grid, const void *sky, int n, unsigned l_max,
+			     double max_move_deg, double basin_deg, double dominance, double *out, int *status, int *n_fallback, void *cuda_stream);
+/* 0, or the code of a device-side wait that timed out */
+int sphrad_proposal_status(sphrad_proposal *p);
+
 #ifdef __cplusplus
 }
 #endif

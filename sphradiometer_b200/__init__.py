@@ -449,3 +449,117 @@ class ProductGrid:
             self.close()
         except Exception:
             pass
+
+
+# ---- learned peak proposal ---------------------------------------------------
+
+class Proposal:
+    """The learned peak proposal (sphrad_proposal_*): an MLP from the l <= 12
+    a_lm of a sky to a direction, trained and run by the library's tcgen05
+    kernels.  Tensors are CUDA tensors on the current stream."""
+
+    N_FEATURES = 338
+
+    def __init__(self, max_batch: int = 4096, seed: int = 1):
+        self.max_batch = int(max_batch)
+        self._p = _check(load().sphrad_proposal_new(self.max_batch, int(seed)), "sphrad_proposal_new")
+
+    @staticmethod
+    def n_params() -> int:
+        return int(load().sphrad_proposal_n_params())
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.n_params(), np.float32)
+        if load().sphrad_proposal_get_params(self._p, out.ctypes.data):
+            raise SphradError("sphrad_proposal_get_params: " + last_error())
+        return out
+
+    def set_params(self, theta: np.ndarray):
+        theta = np.ascontiguousarray(theta, np.float32)
+        assert theta.size == self.n_params()
+        if load().sphrad_proposal_set_params(self._p, theta.ctypes.data):
+            raise SphradError("sphrad_proposal_set_params: " + last_error())
+
+    def grads(self) -> np.ndarray:
+        import torch
+        torch.cuda.synchronize()
+        out = np.empty(self.n_params(), np.float32)
+        if load().sphrad_proposal_get_grads(self._p, out.ctypes.data):
+            raise SphradError("sphrad_proposal_get_grads: " + last_error())
+        return out
+
+    @staticmethod
+    def _st():
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+
+    def sky_features(self, sky, out=None):
+        import torch
+        n = sky.shape[0]
+        L = int(round(sky.shape[1] ** 0.5)) - 1
+        if out is None:
+            out = torch.empty((n, self.N_FEATURES), dtype=torch.float32, device=sky.device)
+        if load().sphrad_proposal_sky_features(self._p, sky.data_ptr(), n, L, out.data_ptr(), self._st()):
+            raise SphradError("sphrad_proposal_sky_features: " + last_error())
+        return out
+
+    def forward(self, features, training: bool = False):
+        import torch
+        n = features.shape[0]
+        feats = features.contiguous()
+        if load().sphrad_proposal_load(self._p, feats.data_ptr(), n, int(training), self._st()):
+            raise SphradError("sphrad_proposal_load: " + last_error())
+        d = torch.empty((n, 3), dtype=torch.float32, device=features.device)
+        if load().sphrad_proposal_forward(self._p, n, int(training), d.data_ptr(), self._st()):
+            raise SphradError("sphrad_proposal_forward: " + last_error())
+        return d
+
+    def train_step(self, features, target, lr: float) -> None:
+        """One Adam step on a batch; the loss is read with ``loss``."""
+        n = features.shape[0]
+        self.forward(features, training=True)
+        t = target.contiguous()
+        if load().sphrad_proposal_backward(self._p, n, t.data_ptr(), self._st()):
+            raise SphradError("sphrad_proposal_backward: " + last_error())
+        if lr > 0 and load().sphrad_proposal_adam(self._p, float(lr), self._st()):
+            raise SphradError("sphrad_proposal_adam: " + last_error())
+
+    def loss(self, n: int) -> float:
+        return float(load().sphrad_proposal_loss(self._p, int(n)))
+
+    def set_mirror(self, normal=None):
+        """Normal of the skies' mirror-symmetry plane (3-detector networks), or None."""
+        if normal is None:
+            load().sphrad_proposal_set_mirror(self._p, None)
+        else:
+            v = np.ascontiguousarray(normal, np.float64)
+            load().sphrad_proposal_set_mirror(self._p, v.ctypes.data)
+
+    def localise(self, judge: "SkyGrid", grid: "SkyGrid", sky, max_move_deg: float = 30.0, basin_deg: float = 6.0, dominance: float = 0.1):
+        """Returns (out [n][4], status [n], n_fallback)."""
+        import torch
+        n = sky.shape[0]
+        L = int(round(sky.shape[1] ** 0.5)) - 1
+        out = torch.empty((n, 4), dtype=torch.float64, device=sky.device)
+        st = torch.empty(n, dtype=torch.int32, device=sky.device)
+        nf = C.c_int(0)
+        if load().sphrad_proposal_localise(self._p, judge._g, grid._g, sky.data_ptr(), n, L, float(max_move_deg), float(basin_deg), float(dominance),
+                                           out.data_ptr(),
+                                           st.data_ptr(), C.byref(nf),
+                                           self._st()):
+            raise SphradError("sphrad_proposal_localise: " + last_error())
+        return out, st, nf.value
+
+    def status(self) -> int:
+        return load().sphrad_proposal_status(self._p)
+
+    def close(self):
+        if getattr(self, "_p", None):
+            load().sphrad_proposal_free(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

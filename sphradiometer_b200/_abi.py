@@ -171,6 +171,21 @@ SIGNATURES = {
     "sphrad_sh_product_grid_free": (None, [_vp]),
     "sphrad_sh_product_scratch_size": (_sz, [_vp, _i]),
     "sphrad_sh_product_batch": (_i, [_vp, _vp, _vp, _i, _vp, _vp, _sz, _vp]),
+    "sphrad_proposal_new": (_vp, [_i, C.c_ulonglong]),
+    "sphrad_proposal_free": (None, [_vp]),
+    "sphrad_proposal_n_params": (_sz, []),
+    "sphrad_proposal_get_params": (_i, [_vp, _vp]),
+    "sphrad_proposal_set_params": (_i, [_vp, _vp]),
+    "sphrad_proposal_get_grads": (_i, [_vp, _vp]),
+    "sphrad_proposal_sky_features": (_i, [_vp, _vp, _i, _u, _vp, _vp]),
+    "sphrad_proposal_load": (_i, [_vp, _vp, _i, _i, _vp]),
+    "sphrad_proposal_forward": (_i, [_vp, _i, _i, _vp, _vp]),
+    "sphrad_proposal_backward": (_i, [_vp, _i, _vp, _vp]),
+    "sphrad_proposal_adam": (_i, [_vp, C.c_float, _vp]),
+    "sphrad_proposal_loss": (C.c_float, [_vp, _i]),
+    "sphrad_proposal_localise": (_i, [_vp, _vp, _vp, _vp, _i, _u, _d, _d, _d, _vp, _vp, C.POINTER(_i), _vp]),
+    "sphrad_proposal_set_mirror": (_i, [_vp, _vp]),
+    "sphrad_proposal_status": (_i, [_vp]),
 }
 
 _lib = None

@@ -41,6 +41,7 @@
 #include <vector>
 
 #include "runtime.h"
+#include "tc_common.cuh"
 
 namespace sphrad {
 
@@ -66,130 +67,8 @@ constexpr int TC_MAXDET = 3;
 constexpr int A_TILE = TM * KE * 2;      // bytes of one bf16 A tile (4096)
 constexpr int CC_TS = 16;                // segments per CUDA-core block
 constexpr int CC_KC = 16;                // bins per CUDA-core stage
-constexpr unsigned long long kWaitCycles = 4000000000ull;  // ~2 s bound on every wait
 constexpr int kMaxChain = 64;            // most pipeline stages one tcgen05 CTA accumulates
 }  // namespace
-
-// ------------------------------------------------------------------------
-// PTX wrappers (sm_100a)
-// ------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t) __cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
-{
-	asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t bar)
-{
-	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_tx(uint32_t bar, uint32_t bytes)
-{
-	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity)
-{
-	uint32_t ok;
-	asm volatile(
-		"{\n\t.reg .pred P;\n\t"
-		"mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
-		"selp.u32 %0, 1, 0, P;\n\t}"
-		: "=r"(ok)
-		: "r"(bar), "r"(parity)
-		: "memory");
-	return ok != 0;
-}
-
-// bounded wait: false on timeout (sets the abort flag and the error word)
-// or when another role has aborted
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag, unsigned *err, unsigned code)
-{
-	const unsigned long long t0 = clock64();
-	while(true) {
-		if(mbar_try(bar, parity))
-			return true;
-		if(*abort_flag)
-			return false;
-		if(clock64() - t0 > kWaitCycles) {
-			*abort_flag = 1;
-			atomicExch(err, code);
-			return false;
-		}
-	}
-}
-
-// bounded wait that ignores the abort flag (draining copies in flight)
-__device__ __forceinline__ void mbar_drain(uint32_t bar, uint32_t parity)
-{
-	const unsigned long long t0 = clock64();
-	while(!mbar_try(bar, parity) && clock64() - t0 < kWaitCycles) {
-	}
-}
-
-__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int x, int y, int z)
-{
-	asm volatile(
-		"cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
-		"l"((uint64_t) map), "r"(bar), "r"(x), "r"(y), "r"(z)
-		: "memory");
-}
-
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
-{
-	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
-		     : "memory");
-}
-
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-// UMMA shared-memory descriptor, K-major, no swizzle: core matrices of
-// 8 rows x 16 bytes; LBO = byte step between core matrices along K, SBO =
-// byte step between 8-row groups; version field 1 (sm100).
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo)
-{
-	uint64_t d = 0;
-	d |= (uint64_t) ((saddr >> 4) & 0x3FFF);
-	d |= (uint64_t) ((lbo >> 4) & 0x3FFF) << 16;
-	d |= (uint64_t) ((sbo >> 4) & 0x3FFF) << 32;
-	d |= (uint64_t) 1 << 46;
-	return d;
-}
-
-__device__ __forceinline__ void umma_bf16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate)
-{
-	asm volatile(
-		"{\n\t.reg .pred p;\n\t"
-		"setp.ne.b32 p, %4, 0;\n\t"
-		"tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
-		"l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void umma_commit(uint32_t bar)
-{
-	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t *v)
-{
-	asm volatile(
-		"tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-		: "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]),
-		  "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-		: "r"(taddr));
-	asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
-__device__ __forceinline__ uint32_t pack_bf16(float lo_elem, float hi_elem)
-{
-	const __nv_bfloat16 a = __float2bfloat16_rn(lo_elem);
-	const __nv_bfloat16 b = __float2bfloat16_rn(hi_elem);
-	return (uint32_t) __bfloat16_as_ushort(a) | ((uint32_t) __bfloat16_as_ushort(b) << 16);
-}
 
 // ------------------------------------------------------------------------
 // tcgen05 contraction

@@ -107,6 +107,8 @@ enum PixOut { kPixComplex = 0, kPixReal = 1, kPixArgmax = 2 };
 void *sht_plan_create(unsigned L, int kind, int nt, int nphi, int fp32);
 void sht_plan_destroy(void *plan);
 int sht_plan_rows(const void *plan, double *theta);  // returns nt
+const double *sht_plan_theta_dev(const void *plan);  // device row co-latitudes
+int sht_plan_nphi(const void *plan);
 size_t sht_scratch_bytes(const void *plan, int S, int M);
 // coeff: device double2 [S][cstride] (layout L_in/polar), truncated at
 // Luse.  out: kPixComplex -> double2 (fp64 plan) or float2 (fp32 plan)
@@ -138,6 +140,23 @@ int sht_product(void *plan, int S, const void *a, long long astride, unsigned La
 size_t rotate_batch_scratch_bytes(unsigned L, int n);
 int rotate_batch(const void *in, int n, unsigned L, int polar, const double *R, void *out, int fp32_apply, void *scratch, size_t scratch_bytes,
 		 void *stream);
+// ---- learned peak proposal (mlp.cu) ------------------------------------
+void *mlp_create(int max_batch, unsigned long long seed);
+void mlp_destroy(void *plan);
+int mlp_rows_max(const void *plan);
+size_t mlp_n_params();
+int mlp_get(void *plan, float *host, int grads);
+int mlp_set(void *plan, const float *host);
+int mlp_sky_features(void *plan, const void *sky, int n, unsigned L, float *feat_out, void *stream);
+int mlp_load(void *plan, const float *feat, int n, int with_transpose, void *stream);
+int mlp_forward(void *plan, int n, int training, float *dir_out, void *stream);
+int mlp_backward(void *plan, int n, const float *target, void *stream);
+int mlp_adam(void *plan, float lr, void *stream);
+int mlp_loss(void *plan, float *host_loss, int n);
+int mlp_status(void *plan);
+int mlp_localise(void *plan, void *judge, void *grid, const void *sky, int n, unsigned L, double max_move, double basin, double dominance, double *out,
+		 int *status, int *n_fallback, void *stream);
+int mlp_set_mirror(void *plan, const double *normal);
 // in-place unnormalised DFT along the array index of n x stride host
 // complex values, e^{sign 2 pi i jk/n}
 int array_dft(int n, int stride, double *data, int sign);

@@ -557,12 +557,24 @@ __global__ void k_peak_refine(int S, int L, int polar, const double2 *coeff, lon
 		const PeakEval en = peak_eval(L, polar, c, tn, pn);
 		const double gn = sign * en.f;
 		if(gn >= g) {
+			// a short step that no longer raises the value is at the
+			// rounding floor of the evaluation: done
+			const bool stalled = len < 1e-7 && gn - g <= 1e-15 * fabs(g);
 			t = tn;
 			p = pn;
 			e = en;
 			g = gn;
 			radius = fmin(2 * radius, M_PI / 24);
+			if(stalled) {
+				converged = 1;
+				it++;
+				break;
+			}
 		} else {
+			if(len < 1e-8) {
+				converged = 1;
+				break;
+			}
 			radius = 0.25 * len;
 			if(radius < tol) {
 				converged = 1;
@@ -787,6 +799,9 @@ int sht_rows_argmax(void *plan, int S, const void *rowbest, double *theta, doubl
 	CK(cudaGetLastError());
 	return 0;
 }
+
+const double *sht_plan_theta_dev(const void *plan) { return ((const ShtPlan *) plan)->d_theta; }
+int sht_plan_nphi(const void *plan) { return ((const ShtPlan *) plan)->nphi; }
 
 size_t sht_rowbest_bytes(const void *plan, int S) { return (size_t) ((const ShtPlan *) plan)->nt * S * sizeof(RowBest); }
 

@@ -173,3 +173,88 @@ extern "C" int sphrad_sh_product_batch(sphrad_sh_product_grid *g, const void *a,
 	}
 	return sht_product(g->plan, n, a, as, g->la, 0, b, bs, g->lb, 0, dest, ds, g->lan, 0, scratch, caller_stream(stream), g->ld);
 }
+
+// ---- learned peak proposal ---------------------------------------------------
+struct sphrad_proposal {
+	void *mlp;
+};
+
+extern "C" sphrad_proposal *sphrad_proposal_new(int max_batch, unsigned long long seed)
+{
+	void *m = mlp_create(max_batch, seed);
+	if(!m)
+		return NULL;
+	sphrad_proposal *p = (sphrad_proposal *) malloc(sizeof(*p));
+	if(!p) {
+		mlp_destroy(m);
+		return NULL;
+	}
+	p->mlp = m;
+	return p;
+}
+
+extern "C" void sphrad_proposal_free(sphrad_proposal *p)
+{
+	if(p)
+		mlp_destroy(p->mlp);
+	free(p);
+}
+
+extern "C" size_t sphrad_proposal_n_params(void) { return mlp_n_params(); }
+extern "C" int sphrad_proposal_get_params(sphrad_proposal *p, float *host) { return mlp_get(p->mlp, host, 0); }
+extern "C" int sphrad_proposal_set_params(sphrad_proposal *p, const float *host) { return mlp_set(p->mlp, host); }
+extern "C" int sphrad_proposal_get_grads(sphrad_proposal *p, float *host) { return mlp_get(p->mlp, host, 1); }
+
+extern "C" int sphrad_proposal_sky_features(sphrad_proposal *p, const void *sky, int n, unsigned l_max, float *features, void *stream)
+{
+	return mlp_sky_features(p->mlp, sky, n, l_max, features, caller_stream(stream));
+}
+
+extern "C" int sphrad_proposal_load(sphrad_proposal *p, const float *features, int n, int for_training, void *stream)
+{
+	if(!features) {
+		set_error("sphrad_proposal_load: no features");
+		return -1;
+	}
+	return mlp_load(p->mlp, features, n, for_training, caller_stream(stream));
+}
+
+extern "C" int sphrad_proposal_forward(sphrad_proposal *p, int n, int for_training, float *dir, void *stream)
+{
+	return mlp_forward(p->mlp, n, for_training, dir, caller_stream(stream));
+}
+
+extern "C" int sphrad_proposal_backward(sphrad_proposal *p, int n, const float *target, void *stream)
+{
+	return mlp_backward(p->mlp, n, target, caller_stream(stream));
+}
+
+extern "C" int sphrad_proposal_adam(sphrad_proposal *p, float lr, void *stream) { return mlp_adam(p->mlp, lr, caller_stream(stream)); }
+
+extern "C" float sphrad_proposal_loss(sphrad_proposal *p, int n)
+{
+	float l = NAN;
+	if(mlp_loss(p->mlp, &l, n))
+		return NAN;
+	return l;
+}
+
+extern "C" int sphrad_proposal_set_mirror(sphrad_proposal *p, const double *normal) { return mlp_set_mirror(p->mlp, normal); }
+
+extern "C" int sphrad_proposal_localise(sphrad_proposal *p, sphrad_sky_grid *judge, sphrad_sky_grid *grid, const void *sky, int n, unsigned l_max,
+					double max_move_deg, double basin_deg, double dominance, double *out, int *status, int *n_fallback, void *stream)
+{
+	if(n <= 0) {
+		if(n_fallback)
+			*n_fallback = 0;
+		return 0;
+	}
+	if(!grid || grid->l_max < l_max || !judge || judge->l_max < l_max) {
+		set_error("sphrad_proposal_localise: the judge and fallback grids must cover l_max %u", l_max);
+		return -1;
+	}
+	return mlp_localise(p->mlp, judge->plan, grid->plan, sky, n, l_max, max_move_deg * M_PI / 180.0, basin_deg * M_PI / 180.0, dominance, out, status,
+			    n_fallback, caller_stream(stream));
+}
+
+extern "C" int sphrad_proposal_status(sphrad_proposal *p) { return mlp_status(p->mlp); }

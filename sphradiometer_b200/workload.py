@@ -201,3 +201,53 @@ def full_from_half(half, n: int) -> np.ndarray:
     idx = np.arange(1, (n + 1) // 2)
     full[..., n - idx] = np.conj(half[..., idx])
     return full
+
+
+def make_batch_torch(positions, n: int, dt: float, n_seg: int, seed: int, device="cuda", snr_range=(6.0, 30.0)):
+    """make_batch generated on the GPU with torch (same model: isotropic
+    Earth-fixed directions, SNR uniform in ``snr_range``, coloured noise,
+    the chirp delayed by r_det . s, whitening), for training and evaluation
+    sets of many segments.  Returns torch tensors: ``F`` (n_det x n_seg x
+    (n/2+1) complex128), ``theta``, ``phi``, ``snr``, ``gmst``."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    pos = torch.as_tensor(np.asarray(positions, np.float64), device=device)
+    nd = pos.shape[0]
+    K = n // 2 + 1
+    k = np.arange(K)
+    S = psd(k / (n * dt))
+    inband = S > 0
+    wh = np.zeros_like(S)
+    wh[inband] = 1.0 / np.sqrt(S[inband])
+    sigma = np.sqrt(S * n / (2 * dt) / 2.0)
+    Hf = np.fft.rfft(chirp(n, dt))
+    rho1 = np.sqrt(4.0 * np.sum(np.abs(Hf[inband] * dt) ** 2 / S[inband]) / (n * dt))
+    wh_t = torch.as_tensor(wh, device=device)
+    sig_t = torch.as_tensor(sigma, device=device)
+    Hf_t = torch.as_tensor(Hf, device=device)
+    kk = torch.arange(K, dtype=torch.float64, device=device)
+
+    def U(lo, hi):
+        return lo + (hi - lo) * torch.rand(n_seg, generator=g, dtype=torch.float64, device=device)
+
+    theta = torch.arccos(U(-1.0, 1.0))
+    phi = U(0.0, 2 * np.pi)
+    snr = U(snr_range[0], snr_range[1])
+    gmst = U(0.0, 2 * np.pi)
+    s_hat = torch.stack([torch.sin(theta) * torch.cos(phi), torch.sin(theta) * torch.sin(phi), torch.cos(theta)], dim=1)
+    tau = s_hat @ pos.T
+    amp = snr / rho1
+    F = torch.empty((nd, n_seg, K), dtype=torch.complex128, device=device)
+    for d in range(nd):
+        re = torch.randn((n_seg, K), generator=g, dtype=torch.float64, device=device)
+        im = torch.randn((n_seg, K), generator=g, dtype=torch.float64, device=device)
+        im[:, 0] = 0
+        if n % 2 == 0:
+            im[:, -1] = 0
+        nz = torch.complex(re, im) * sig_t[None, :]
+        sig = (amp[:, None] * Hf_t[None, :]) * torch.exp(1j * 2 * np.pi * tau[:, d:d + 1] * kk[None, :] / (dt * n))
+        if n % 2 == 0:
+            sig[:, -1] = sig[:, -1].real
+        F[d] = (nz + sig) * wh_t[None, :]
+    return dict(F=F, theta=theta, phi=phi, snr=snr, gmst=gmst)
