@@ -87,6 +87,14 @@ int sphrad_batch_integrate(sphrad_batch_plan *plan, const void *fseries, int n_s
  * sphrad_batch_integrate. */
 int sphrad_batch_integrate_noalloc(sphrad_batch_plan *plan, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky, void *cuda_stream);
 
+/* sphrad_batch_integrate with a split-K factor (0: the tuned or default
+ * one) and per-segment baseline factors: baseline_factor, device float
+ * [n_seg][n_baselines] or NULL, multiplies each segment's baseline terms
+ * (on top of the network mean 1/n_baselines), so a segment can use a subset
+ * of the network's baselines or weight them. */
+int sphrad_batch_integrate_weighted(sphrad_batch_plan *plan, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky, void *workspace,
+				    size_t workspace_bytes, void *cuda_stream, int split, const float *baseline_factor);
+
 /* The same with host buffers: copies in, integrates, copies out and
  * synchronises (library-owned device buffers).  Use pinned host memory for
  * full copy bandwidth. */
@@ -110,6 +118,45 @@ int sphrad_batch_set_timing_events(sphrad_batch_plan *plan, void *ev_begin, void
 /* 0 when no device-side wait has timed out, else the code of the wait that
  * gave up (synchronises with the device). */
 int sphrad_batch_status(sphrad_batch_plan *plan);
+
+/* ---- uneven batches ------------------------------------------------------
+ *
+ * Segments of one detector network with different DFT lengths, output
+ * l_max and baseline subsets, integrated by one call.  No counterpart in
+ * the reference (one segment of one complete network per call,
+ * correlator.c:993-1010).  Segments are bucketed by DFT length (pad each
+ * segment's time series with zeros to its bucket's length); each sky is the
+ * mean over the segment's own baselines, rotated to the Earth frame and
+ * truncated to the segment's l_max.  Baselines are numbered in the
+ * reference's order (1,0), (2,0), (2,1), (3,0), (3,1), (3,2), ...  Internally
+ * a segment's baselines are covered by sub-networks of at most three
+ * detectors, and every (bucket, sub-network) pair with segments is one job
+ * of the batched tcgen05 path; a call runs every job, and is captured into
+ * a CUDA graph on first use and replayed (the graph is rebuilt when the
+ * input or output pointer changes). */
+typedef struct sphrad_uneven_plan sphrad_uneven_plan;
+
+/* positions: [n_det][3] phase centres in light-seconds (2 <= n_det <= 8);
+ * bucket_n: DFT lengths; l_max: the largest segment l_max; precision as
+ * for sphrad_batch_plan_new. */
+sphrad_uneven_plan *sphrad_uneven_plan_new(const double *positions, int n_det, double delta_t, const int *bucket_n, int n_buckets, unsigned l_max,
+					   int precision);
+void sphrad_uneven_plan_free(sphrad_uneven_plan *plan);
+/* per segment: bucket index, baseline mask (bit k = baseline k) and l_max */
+int sphrad_uneven_set_segments(sphrad_uneven_plan *plan, int n_seg, const int *bucket, const unsigned *baseline_mask, const unsigned *l_max);
+/* packed layouts (host arrays of n_seg, or NULL): segment s's spectra start
+ * at in_offset[s] double complex elements, [n_det][bucket_n/2 + 1]; its sky
+ * at out_offset[s], (l_max_s + 1)^2 coefficients.  Returns n_seg. */
+int sphrad_uneven_layout(const sphrad_uneven_plan *plan, long long *in_offset, long long *out_offset, long long *in_total, long long *out_total);
+int sphrad_uneven_jobs(const sphrad_uneven_plan *plan);
+/* split-K of every job: > 0 fixed, 0 = each job's tuned (or default) value */
+int sphrad_uneven_set_split(sphrad_uneven_plan *plan, int split);
+/* tunes every job's split-K on these device spectra (CUDA events) */
+int sphrad_uneven_autotune(sphrad_uneven_plan *plan, const void *spectra, void *skies, void *cuda_stream);
+int sphrad_uneven_use_graph(sphrad_uneven_plan *plan, int on);
+/* spectra, skies: device arrays in the packed layouts */
+int sphrad_uneven_integrate(sphrad_uneven_plan *plan, const void *spectra, void *skies, void *cuda_stream);
+int sphrad_uneven_kernels_per_call(const sphrad_uneven_plan *plan);
 
 /* ---- sky grids and peak localisation (batched) -------------------------
  *

@@ -563,3 +563,83 @@ class Proposal:
             self.close()
         except Exception:
             pass
+
+
+# ---- uneven batches ------------------------------------------------------------
+
+class UnevenPlan:
+    """Segments of different DFT lengths, l_max and baseline subsets of one
+    network in one call (sphrad_uneven_*).  Spectra and skies are packed
+    1-D complex128 CUDA tensors in the layouts ``in_offset`` / ``out_offset``."""
+
+    def __init__(self, positions, delta_t: float, bucket_n, l_max: int, precision: str | int = "bf16x3"):
+        pos = np.ascontiguousarray(positions, np.float64)
+        self.n_det = pos.shape[0]
+        self.bucket_n = np.ascontiguousarray(bucket_n, np.int32)
+        self.l_max = int(l_max)
+        prec = PRECISIONS.get(precision, precision) if isinstance(precision, str) else int(precision)
+        self._p = _check(load().sphrad_uneven_plan_new(pos.ctypes.data, self.n_det, float(delta_t), self.bucket_n.ctypes.data, len(self.bucket_n),
+                                                       self.l_max, prec), "sphrad_uneven_plan_new")
+        self.n_seg = 0
+
+    def set_segments(self, bucket, mask, l_max):
+        b = np.ascontiguousarray(bucket, np.int32)
+        m = np.ascontiguousarray(mask, np.uint32)
+        l = np.ascontiguousarray(l_max, np.uint32)
+        n = len(b)
+        if load().sphrad_uneven_set_segments(self._p, n, b.ctypes.data, m.ctypes.data, l.ctypes.data):
+            raise SphradError("sphrad_uneven_set_segments: " + last_error())
+        self.n_seg = n
+        self.in_offset = np.empty(n, np.int64)
+        self.out_offset = np.empty(n, np.int64)
+        tot = (C.c_longlong(), C.c_longlong())
+        load().sphrad_uneven_layout(self._p, self.in_offset.ctypes.data, self.out_offset.ctypes.data, C.byref(tot[0]), C.byref(tot[1]))
+        self.in_total, self.out_total = tot[0].value, tot[1].value
+        self.seg_l_max = l.copy()
+
+    def jobs(self) -> int:
+        return load().sphrad_uneven_jobs(self._p)
+
+    def kernels_per_call(self) -> int:
+        return load().sphrad_uneven_kernels_per_call(self._p)
+
+    def set_split(self, split: int):
+        load().sphrad_uneven_set_split(self._p, int(split))
+
+    def use_graph(self, on: bool):
+        load().sphrad_uneven_use_graph(self._p, int(bool(on)))
+
+    def autotune(self, spectra, out=None):
+        import torch
+        out = self._out(spectra, out)
+        if load().sphrad_uneven_autotune(self._p, spectra.data_ptr(), out.data_ptr(), torch.cuda.current_stream().cuda_stream):
+            raise SphradError("sphrad_uneven_autotune: " + last_error())
+
+    def _out(self, spectra, out):
+        import torch
+        assert spectra.is_cuda and spectra.dtype == torch.complex128 and spectra.numel() >= self.in_total
+        if out is None:
+            out = torch.empty(self.out_total, dtype=torch.complex128, device=spectra.device)
+        return out
+
+    def integrate(self, spectra, out=None):
+        import torch
+        out = self._out(spectra, out)
+        if load().sphrad_uneven_integrate(self._p, spectra.data_ptr(), out.data_ptr(), torch.cuda.current_stream().cuda_stream):
+            raise SphradError("sphrad_uneven_integrate: " + last_error())
+        return out
+
+    def unpack(self, out) -> list:
+        o = out.cpu().numpy() if hasattr(out, "cpu") else np.asarray(out)
+        return [o[self.out_offset[s]:self.out_offset[s] + (int(self.seg_l_max[s]) + 1) ** 2] for s in range(self.n_seg)]
+
+    def close(self):
+        if getattr(self, "_p", None):
+            load().sphrad_uneven_plan_free(self._p)
+            self._p = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

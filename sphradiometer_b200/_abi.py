@@ -157,6 +157,17 @@ SIGNATURES = {
     "sphrad_batch_status": (_i, [_vp]),
     "sphrad_batch_set_timing_events": (_i, [_vp, _vp, _vp]),
     "sphrad_batch_integrate_noalloc": (_i, [_vp, _vp, _i, _ll, _vp, _vp, _vp]),
+    "sphrad_batch_integrate_weighted": (_i, [_vp, _vp, _i, _ll, _vp, _vp, _vp, _sz, _vp, _i, _vp]),
+    "sphrad_uneven_plan_new": (_vp, [_vp, _i, _d, _vp, _i, _u, _i]),
+    "sphrad_uneven_plan_free": (None, [_vp]),
+    "sphrad_uneven_set_segments": (_i, [_vp, _i, _vp, _vp, _vp]),
+    "sphrad_uneven_layout": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "sphrad_uneven_jobs": (_i, [_vp]),
+    "sphrad_uneven_set_split": (_i, [_vp, _i]),
+    "sphrad_uneven_autotune": (_i, [_vp, _vp, _vp, _vp]),
+    "sphrad_uneven_use_graph": (_i, [_vp, _i]),
+    "sphrad_uneven_integrate": (_i, [_vp, _vp, _vp, _vp]),
+    "sphrad_uneven_kernels_per_call": (_i, [_vp]),
     "sphrad_sky_grid_new": (_vp, [_u, _i, _i, _i, _i]),
     "sphrad_sky_grid_free": (None, [_vp]),
     "sphrad_sky_grid_rows": (_i, [_vp, _vp]),

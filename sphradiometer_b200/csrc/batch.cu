@@ -466,6 +466,7 @@ struct EpArgs {
 	const short *mq;        // m of output index q
 	const void *W;          // [B][nq] complex T: weight / n * D_b^l_{0 m}
 	const double *gmst;     // [S] or NULL
+	const float *segw;      // [S][B] extra per-segment baseline factors, or NULL
 	double2 *sky;           // [S][nq]
 };
 
@@ -478,8 +479,10 @@ __global__ void k_epilogue(const __grid_constant__ EpArgs e, T *acc)
 	T *sP = (T *) (sPh + 2 * e.L + 1);                              // [B][Lp1]
 	const int s = blockIdx.x;
 	T *row = acc + (size_t) s * e.B * e.accstride;
-	for(int i = threadIdx.x; i < e.B * e.Lp1; i += blockDim.x)
-		sP[i] = row[(i / e.Lp1) * e.accstride + i % e.Lp1];
+	for(int i = threadIdx.x; i < e.B * e.Lp1; i += blockDim.x) {
+		const int b = i / e.Lp1;
+		sP[i] = row[b * e.accstride + i % e.Lp1] * (e.segw ? (T) e.segw[(size_t) s * e.B + b] : (T) 1);
+	}
 	for(int m = (int) threadIdx.x - e.L; m <= e.L; m += blockDim.x) {
 		double sn = 0.0, cs = 1.0;
 		if(e.gmst)
@@ -729,11 +732,16 @@ void *batch_plan_create(const BatchPlanDesc &d, int precision)
 			if(stream_sync())
 				fail = true;
 			dfree(Dt64);
+			// a shallower X-operand ring when the delay-table tiles of a
+			// large l_max leave no room for four stages
+			if(!fail && P->npart == 2 && tc_smem_bytes(*P) > 227 * 1024)
+				P->nab = 3;
 			if(!fail && tc_smem_bytes(*P) > 227 * 1024) {
 				set_error("batch plan: shared-memory budget exceeded");
 				fail = true;
 			}
 			if(!fail && (cudaFuncSetAttribute(k_tc_contract<2, NF, 4, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
+				     cudaFuncSetAttribute(k_tc_contract<2, NF, 3, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
 				     cudaFuncSetAttribute(k_tc_contract<3, NF, 2, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess)) {
 				set_error("batch plan: cannot reserve %zu bytes of shared memory", tc_smem_bytes(*P));
 				fail = true;
@@ -795,7 +803,8 @@ int batch_set_split(void *pp, int S, int ks)
 	return 0;
 }
 
-int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream_v, int split)
+int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream_v, int split,
+	      const float *segw)
 {
 	BatchPlan *P = (BatchPlan *) pp;
 	cudaStream_t st = (cudaStream_t) stream_v;
@@ -864,7 +873,10 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 		if(P->npart == 3)
 			k_tc_contract<3, NF, 2, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		else
-			k_tc_contract<2, NF, 4, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			if(P->nab == 4)
+				k_tc_contract<2, NF, 4, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			else
+				k_tc_contract<2, NF, 3, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		if(P->ev_end)
 			cudaEventRecord(P->ev_end, st);
 		launches++;
@@ -921,6 +933,7 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 	e.mq = P->mq;
 	e.W = P->W;
 	e.gmst = gmst;
+	e.segw = segw;
 	e.sky = (double2 *) sky;
 	const size_t el = P->precision == kPrecFP64 ? sizeof(double) : sizeof(float);
 	const size_t esmem = (size_t) P->B * P->Lp1 * el + (2 * P->L + 1) * sizeof(double2);

@@ -716,6 +716,12 @@ extern "C" int sphrad_batch_integrate(sphrad_batch_plan *p, const void *fseries_
 	return batch_run(p->impl, fseries_dev, n_seg, ld, gmst_dev, sky_dev, workspace, workspace_bytes, stream, 0);
 }
 
+extern "C" int sphrad_batch_integrate_weighted(sphrad_batch_plan *p, const void *fseries_dev, int n_seg, long long ld, const double *gmst_dev, void *sky_dev,
+					       void *workspace, size_t workspace_bytes, void *stream, int split, const float *baseline_factor)
+{
+	return batch_run(p->impl, fseries_dev, n_seg, ld, gmst_dev, sky_dev, workspace, workspace_bytes, stream, split > 0 ? split : 0, baseline_factor);
+}
+
 extern "C" int sphrad_batch_integrate_host(sphrad_batch_plan *p, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky)
 {
 	return batch_run_host(p->impl, fseries, n_seg, ld, gmst, sky);

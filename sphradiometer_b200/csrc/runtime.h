@@ -91,10 +91,21 @@ void batch_plan_destroy(void *plan);
 unsigned batch_plan_l_max(const void *plan);
 int batch_plan_bins(const void *plan);  // bins read per spectrum row
 size_t batch_workspace_bytes(const void *plan, int S);
-int batch_run(void *plan, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream, int split);
+// segw: optional [S][B] factors on each segment's baselines (device)
+int batch_run(void *plan, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream, int split,
+	      const float *segw = nullptr);
 int batch_run_host(void *plan, const void *F_host, int S, long long ld, const double *gmst_host, void *sky_host);
 int batch_pick_split(const void *plan, int S);
 int batch_last_kernel_count(const void *plan);
+
+// ---- uneven batches (uneven.cu) -----------------------------------------
+// F[d][i][k] = in[in_off[seg[i]] + det[d] Ku + k] for a job of S segments
+// of n_sub detectors (device pointers; stream a cudaStream_t)
+int uneven_gather(int S, int n_sub, int Ku, long long ld, const int *seg, const long long *in_off, const int *det, const void *in, void *F, void *stream);
+// out[out_off[seg[i]] ...] += sky[i] truncated to l_max seg_L[seg[i]]
+int uneven_scatter(int S, unsigned L, const int *seg, const long long *out_off, const unsigned *seg_L, const void *sky, void *out, void *stream);
+int batch_autotune(void *plan, const void *F, int S, long long ld, void *sky, void *ws, size_t ws_bytes, void *stream);
+int batch_set_split(void *plan, int S, int split);
 
 // ---- spherical-harmonic transforms on theta x phi grids (sht.cu) -------
 // Gauss-Legendre nodes (decreasing x) and weights on [-1, 1] (host)

@@ -1,0 +1,445 @@
+// uneven_api.cpp -- uneven batches: segments of different DFT lengths,
+// output l_max and baseline subsets of one detector network integrated in
+// one call (declared in sphradiometer_b200.h; no reference counterpart --
+// the reference integrates one segment of one network per call,
+// correlator.c:993-1010, and its callers pad segments to a length ladder,
+// inspiral_sky_map.c's preprocessing).
+//
+// Plan: segments are bucketed by DFT length (the delay tables depend on
+// n).  Each segment's baselines are covered by sub-networks of at most
+// three detectors (the tcgen05 contraction's limit), greedily; every
+// (bucket, sub-network) pair with segments is a job: a batched plan of that
+// sub-network at the bucket's n and the plan's l_max, the job's segment
+// list and per-segment baseline factors (n_sub_baselines / B_s for the
+// segment's baselines assigned to the job, 0 otherwise, so each sky is the
+// mean over its own B_s baselines, correlator.c:1004).  A call zeroes the
+// packed outputs and runs every job: gather of its spectra, contraction,
+// epilogue, and addition into the outputs truncated to each segment's
+// l_max.  The whole sequence can be captured once into a CUDA graph and
+// replayed.
+#include <sphradiometer_b200.h>
+#include <sphradiometer/correlator.h>
+#include <sphradiometer/instrument.h>
+
+#include <cuda_runtime_api.h>
+
+#include <algorithm>
+#include <map>
+#include <vector>
+
+#include "abi_common.h"
+
+using namespace sphrad;
+
+namespace {
+
+struct Job {
+	int bucket = 0;
+	std::vector<int> det;        // detectors of the sub-network (increasing)
+	std::vector<int> gbl;        // global baseline ids of its baselines, in its plan's order
+	sphrad_batch_plan *bp = nullptr;
+	int S = 0, Ku = 0;
+	long long ld = 0;
+	std::vector<int> seg;        // host copies
+	std::vector<float> w;        // [S][nb_sub]
+	int *d_seg = nullptr;
+	float *d_w = nullptr;
+	int split = 0;               // tuned split (0 = heuristic)
+};
+
+}  // namespace
+
+struct sphrad_uneven_plan {
+	int n_det = 0;
+	double dt = 0;
+	std::vector<double> pos;
+	std::vector<int> bucket_n;
+	unsigned L = 0;
+	int precision = 0;
+	int nbl = 0;                                     // baselines of the full network
+	std::vector<std::pair<int, int>> bl;             // global baseline id -> (i, j), i > j
+	// sub-networks: detector lists; per (bucket, sub) a batched plan
+	std::vector<std::vector<int>> subs;
+	std::map<std::pair<int, int>, sphrad_batch_plan *> plans;
+	std::vector<void *> net_objs;                    // instruments, baselines, network plans to free
+	// segments
+	int n_seg = 0;
+	std::vector<unsigned> segL;
+	std::vector<long long> in_off, out_off;
+	long long in_total = 0, out_total = 0;
+	long long *d_in_off = nullptr, *d_out_off = nullptr;
+	unsigned *d_segL = nullptr;
+	std::vector<Job> jobs;
+	// shared job buffers (jobs run in sequence)
+	void *F = nullptr, *sky = nullptr, *ws = nullptr;
+	size_t F_bytes = 0, sky_bytes = 0, ws_bytes = 0;
+	int fixed_split = 0;
+	// graph
+	int use_graph = 1;
+	cudaStream_t cap = nullptr;
+	cudaGraph_t graph = nullptr;
+	cudaGraphExec_t exec = nullptr;
+	const void *g_in = nullptr;
+	void *g_out = nullptr;
+	int g_split = -1;
+	int kernels = 0;
+};
+
+static void drop_graph(sphrad_uneven_plan *p)
+{
+	if(p->exec)
+		cudaGraphExecDestroy(p->exec);
+	if(p->graph)
+		cudaGraphDestroy(p->graph);
+	p->exec = nullptr;
+	p->graph = nullptr;
+	p->g_in = nullptr;
+	p->g_out = nullptr;
+}
+
+static void drop_jobs(sphrad_uneven_plan *p)
+{
+	for(Job &j : p->jobs) {
+		dfree(j.d_seg);
+		dfree(j.d_w);
+	}
+	p->jobs.clear();
+	dfree(p->d_in_off);
+	dfree(p->d_out_off);
+	dfree(p->d_segL);
+	p->d_in_off = p->d_out_off = nullptr;
+	p->d_segL = nullptr;
+	dfree(p->F);
+	dfree(p->sky);
+	dfree(p->ws);
+	p->F = p->sky = p->ws = nullptr;
+	p->F_bytes = p->sky_bytes = p->ws_bytes = 0;
+	drop_graph(p);
+}
+
+extern "C" void sphrad_uneven_plan_free(sphrad_uneven_plan *p)
+{
+	if(!p)
+		return;
+	drop_jobs(p);
+	for(auto &kv : p->plans)
+		sphrad_batch_plan_free(kv.second);
+	// network objects: plan, baselines, instruments (in creation order of
+	// triples: [inst_array, baselines, plan] per (bucket, sub))
+	for(size_t i = 0; i + 2 < p->net_objs.size(); i += 3) {
+		correlator_network_plan_fd_free((struct correlator_network_plan_fd *) p->net_objs[i + 2]);
+		correlator_network_baselines_free((struct correlator_network_baselines *) p->net_objs[i + 1]);
+		instrument_array_free((struct instrument_array *) p->net_objs[i]);
+	}
+	if(p->cap)
+		cudaStreamDestroy(p->cap);
+	delete p;
+}
+
+extern "C" sphrad_uneven_plan *sphrad_uneven_plan_new(const double *positions, int n_det, double delta_t, const int *bucket_n, int n_buckets, unsigned l_max,
+						     int precision)
+{
+	if(n_det < 2 || n_det > 8 || n_buckets < 1 || !positions || !bucket_n) {
+		set_error("sphrad_uneven_plan_new: %d detectors, %d buckets", n_det, n_buckets);
+		return NULL;
+	}
+	if(ensure_device())
+		return NULL;
+	sphrad_uneven_plan *p = new sphrad_uneven_plan;
+	p->n_det = n_det;
+	p->dt = delta_t;
+	p->pos.assign(positions, positions + 3 * n_det);
+	p->bucket_n.assign(bucket_n, bucket_n + n_buckets);
+	p->L = l_max;
+	p->precision = precision;
+	for(int i = 1; i < n_det; i++)
+		for(int j = 0; j < i; j++)
+			p->bl.push_back({i, j});
+	p->nbl = (int) p->bl.size();
+	// sub-networks of min(3, n_det) detectors
+	if(n_det <= 3) {
+		std::vector<int> all;
+		for(int d = 0; d < n_det; d++)
+			all.push_back(d);
+		p->subs.push_back(all);
+	} else {
+		for(int a = 0; a < n_det; a++)
+			for(int b = a + 1; b < n_det; b++)
+				for(int c = b + 1; c < n_det; c++)
+					p->subs.push_back({a, b, c});
+	}
+	if(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking) != cudaSuccess) {
+		set_error("sphrad_uneven_plan_new: stream creation failed");
+		sphrad_uneven_plan_free(p);
+		return NULL;
+	}
+	return p;
+}
+
+// global baseline id of (i, j), i > j, in the reference's order
+static int gid(int i, int j) { return i * (i - 1) / 2 + j; }
+
+static sphrad_batch_plan *plan_for(sphrad_uneven_plan *p, int bucket, int sub)
+{
+	auto key = std::make_pair(bucket, sub);
+	auto it = p->plans.find(key);
+	if(it != p->plans.end())
+		return it->second;
+	const std::vector<int> &dets = p->subs[sub];
+	struct instrument_array *ia = instrument_array_new(0);
+	if(!ia)
+		return NULL;
+	for(int d : dets) {
+		struct instrument *ins = instrument_new(p->pos[3 * d], p->pos[3 * d + 1], p->pos[3 * d + 2], NULL);
+		if(!ins || !instrument_array_append(ia, ins)) {
+			instrument_array_free(ia);
+			return NULL;
+		}
+	}
+	struct correlator_network_baselines *nb = correlator_network_baselines_new(ia);
+	struct correlator_network_plan_fd *np = nb ? correlator_network_plan_fd_new_l(nb, p->bucket_n[bucket], p->dt, p->L) : NULL;
+	sphrad_batch_plan *bp = np ? sphrad_batch_plan_new(np, p->precision) : NULL;
+	p->net_objs.push_back(ia);
+	p->net_objs.push_back(nb);
+	p->net_objs.push_back(np);
+	if(!bp)
+		return NULL;
+	p->plans[key] = bp;
+	return bp;
+}
+
+extern "C" int sphrad_uneven_set_segments(sphrad_uneven_plan *p, int n_seg, const int *bucket, const unsigned *mask, const unsigned *l_max)
+{
+	drop_jobs(p);
+	if(n_seg < 0) {
+		set_error("sphrad_uneven_set_segments: %d segments", n_seg);
+		return -1;
+	}
+	p->n_seg = n_seg;
+	p->segL.assign(l_max, l_max + n_seg);
+	p->in_off.resize(n_seg);
+	p->out_off.resize(n_seg);
+	long long io = 0, oo = 0;
+	const int nb_sub = p->n_det <= 3 ? p->nbl : 3;
+	// job index per (bucket, sub)
+	std::map<std::pair<int, int>, int> job_of;
+	for(int s = 0; s < n_seg; s++) {
+		const int b = bucket[s];
+		if(b < 0 || b >= (int) p->bucket_n.size() || l_max[s] > p->L) {
+			set_error("sphrad_uneven_set_segments: segment %d has bucket %d, l_max %u", s, b, l_max[s]);
+			return -1;
+		}
+		const unsigned full = p->nbl >= 32 ? 0xFFFFFFFFu : ((1u << p->nbl) - 1);
+		const unsigned m = mask[s] & full;
+		const int Bs = __builtin_popcount(m);
+		if(Bs == 0) {
+			set_error("sphrad_uneven_set_segments: segment %d has no baseline", s);
+			return -1;
+		}
+		const int Ku = p->bucket_n[b] / 2 + 1;
+		p->in_off[s] = io;
+		io += (long long) p->n_det * Ku;
+		p->out_off[s] = oo;
+		oo += (long long) (l_max[s] + 1) * (l_max[s] + 1);
+		// greedy cover of the segment's baselines by sub-networks
+		unsigned left = m;
+		while(left) {
+			int best = -1, best_cnt = 0;
+			for(int t = 0; t < (int) p->subs.size(); t++) {
+				int cnt = 0;
+				const std::vector<int> &d = p->subs[t];
+				for(size_t x = 0; x < d.size(); x++)
+					for(size_t y = 0; y < x; y++)
+						cnt += (left >> gid(d[x], d[y])) & 1;
+				if(cnt > best_cnt) {
+					best_cnt = cnt;
+					best = t;
+				}
+			}
+			auto key = std::make_pair(b, best);
+			auto it = job_of.find(key);
+			int ji;
+			if(it == job_of.end()) {
+				ji = (int) p->jobs.size();
+				job_of[key] = ji;
+				Job j;
+				j.bucket = b;
+				j.det = p->subs[best];
+				// the sub-network plan's baseline order: (1,0), (2,0), (2,1)
+				for(size_t x = 1; x < j.det.size(); x++)
+					for(size_t y = 0; y < x; y++)
+						j.gbl.push_back(gid(j.det[x], j.det[y]));
+				j.Ku = Ku;
+				j.ld = Ku;
+				p->jobs.push_back(j);
+			} else
+				ji = it->second;
+			Job &j = p->jobs[ji];
+			j.seg.push_back(s);
+			for(int g : j.gbl) {
+				const bool take = (left >> g) & 1;
+				j.w.push_back(take ? (float) nb_sub / (float) Bs : 0.f);
+				if(take)
+					left &= ~(1u << g);
+			}
+		}
+	}
+	p->in_total = io;
+	p->out_total = oo;
+	// device tables and shared buffers
+	size_t Fb = 0, skb = 0, wsb = 0;
+	const size_t nq = (size_t) (p->L + 1) * (p->L + 1);
+	for(Job &j : p->jobs) {
+		j.S = (int) j.seg.size();
+		j.bp = plan_for(p, j.bucket, (int) (std::find(p->subs.begin(), p->subs.end(), j.det) - p->subs.begin()));
+		if(!j.bp)
+			return -1;
+		j.d_seg = (int *) dmalloc(j.S * sizeof(int));
+		j.d_w = (float *) dmalloc(j.w.size() * sizeof(float));
+		if(!j.d_seg || !j.d_w || h2d(j.d_seg, j.seg.data(), j.S * sizeof(int)) || h2d(j.d_w, j.w.data(), j.w.size() * sizeof(float)))
+			return -1;
+		Fb = std::max(Fb, (size_t) (j.det.size() * j.S * j.ld * 16));
+		skb = std::max(skb, (size_t) j.S * nq * 16);
+		wsb = std::max(wsb, sphrad_batch_workspace_size(j.bp, j.S));
+	}
+	p->d_in_off = (long long *) dmalloc((n_seg > 0 ? n_seg : 1) * sizeof(long long));
+	p->d_out_off = (long long *) dmalloc((n_seg > 0 ? n_seg : 1) * sizeof(long long));
+	p->d_segL = (unsigned *) dmalloc((n_seg > 0 ? n_seg : 1) * sizeof(unsigned));
+	p->F = dmalloc(Fb);
+	p->sky = dmalloc(skb);
+	p->ws = dmalloc(wsb);
+	p->F_bytes = Fb;
+	p->sky_bytes = skb;
+	p->ws_bytes = wsb;
+	if(!p->d_in_off || !p->d_out_off || !p->d_segL || !p->F || !p->sky || !p->ws)
+		return -1;
+	if(n_seg > 0 && (h2d(p->d_in_off, p->in_off.data(), n_seg * sizeof(long long)) || h2d(p->d_out_off, p->out_off.data(), n_seg * sizeof(long long)) ||
+			 h2d(p->d_segL, p->segL.data(), n_seg * sizeof(unsigned))))
+		return -1;
+	if(dmemset(p->ws, 0, wsb) || stream_sync())
+		return -1;
+	return 0;
+}
+
+extern "C" int sphrad_uneven_layout(const sphrad_uneven_plan *p, long long *in_offset, long long *out_offset, long long *in_total, long long *out_total)
+{
+	if(in_offset)
+		std::copy(p->in_off.begin(), p->in_off.end(), in_offset);
+	if(out_offset)
+		std::copy(p->out_off.begin(), p->out_off.end(), out_offset);
+	if(in_total)
+		*in_total = p->in_total;
+	if(out_total)
+		*out_total = p->out_total;
+	return p->n_seg;
+}
+
+extern "C" int sphrad_uneven_jobs(const sphrad_uneven_plan *p) { return (int) p->jobs.size(); }
+
+static int split_of(const sphrad_uneven_plan *p, const Job &j)
+{
+	if(p->fixed_split > 0)
+		return p->fixed_split;
+	return j.split;
+}
+
+// the job sequence on stream st
+static int run_jobs(sphrad_uneven_plan *p, const void *in, void *out, cudaStream_t st)
+{
+	int k = 0;
+	if(cudaMemsetAsync(out, 0, (size_t) p->out_total * 16, st) != cudaSuccess) {
+		set_error("uneven: memset failed");
+		return -1;
+	}
+	for(Job &j : p->jobs) {
+		if(uneven_gather(j.S, (int) j.det.size(), j.Ku, j.ld, j.d_seg, p->d_in_off, j.det.data(), in, p->F, st))
+			return -1;
+		if(sphrad_batch_integrate_weighted(j.bp, p->F, j.S, j.ld, NULL, p->sky, p->ws, p->ws_bytes, st, split_of(p, j), j.d_w))
+			return -1;
+		k += 1 + sphrad_batch_kernels_per_call(j.bp);
+		if(uneven_scatter(j.S, p->L, j.d_seg, p->d_out_off, p->d_segL, p->sky, out, st))
+			return -1;
+		k++;
+	}
+	p->kernels = k;
+	return 0;
+}
+
+extern "C" int sphrad_uneven_set_split(sphrad_uneven_plan *p, int split)
+{
+	p->fixed_split = split > 0 ? split : 0;
+	drop_graph(p);
+	return 0;
+}
+
+extern "C" int sphrad_uneven_use_graph(sphrad_uneven_plan *p, int on)
+{
+	p->use_graph = on ? 1 : 0;
+	drop_graph(p);
+	return 0;
+}
+
+extern "C" int sphrad_uneven_autotune(sphrad_uneven_plan *p, const void *in, void *out, void *stream)
+{
+	cudaStream_t st = stream ? (cudaStream_t) stream : cudaStreamLegacy;
+	(void) out;
+	for(Job &j : p->jobs) {
+		if(uneven_gather(j.S, (int) j.det.size(), j.Ku, j.ld, j.d_seg, p->d_in_off, j.det.data(), in, p->F, st))
+			return -1;
+		const int ks = sphrad_batch_autotune(j.bp, p->F, j.S, j.ld, p->sky, p->ws, p->ws_bytes, st);
+		if(ks < 0)
+			return -1;
+		j.split = ks;
+	}
+	drop_graph(p);
+	return 0;
+}
+
+extern "C" int sphrad_uneven_integrate(sphrad_uneven_plan *p, const void *in, void *out, void *stream)
+{
+	cudaStream_t st = stream ? (cudaStream_t) stream : cudaStreamLegacy;
+	if(p->n_seg == 0)
+		return 0;
+	if(!p->use_graph)
+		return run_jobs(p, in, out, st);
+	if(!p->exec || p->g_in != in || p->g_out != out) {
+		drop_graph(p);
+		// capture on the plan's own stream, ordered after the caller's work
+		cudaEvent_t ev;
+		if(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess || cudaEventRecord(ev, st) != cudaSuccess ||
+		   cudaStreamWaitEvent(p->cap, ev, 0) != cudaSuccess) {
+			set_error("uneven: cannot order the capture stream");
+			return -1;
+		}
+		cudaEventDestroy(ev);
+		if(cudaStreamBeginCapture(p->cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+			set_error("uneven: stream capture failed to start");
+			return -1;
+		}
+		const int rc = run_jobs(p, in, out, p->cap);
+		cudaGraph_t g = nullptr;
+		const cudaError_t ec = cudaStreamEndCapture(p->cap, &g);
+		if(rc || ec != cudaSuccess || !g) {
+			if(g)
+				cudaGraphDestroy(g);
+			if(!rc)
+				set_error("uneven: stream capture failed (%s)", cudaGetErrorString(ec));
+			return -1;
+		}
+		p->graph = g;
+		if(cudaGraphInstantiate(&p->exec, g, 0) != cudaSuccess) {
+			set_error("uneven: graph instantiation failed");
+			drop_graph(p);
+			return -1;
+		}
+		p->g_in = in;
+		p->g_out = out;
+	}
+	if(cudaGraphLaunch(p->exec, st) != cudaSuccess) {
+		set_error("uneven: graph launch failed");
+		return -1;
+	}
+	return 0;
+}
+
+extern "C" int sphrad_uneven_kernels_per_call(const sphrad_uneven_plan *p) { return p->kernels; }

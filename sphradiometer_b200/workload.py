@@ -251,3 +251,51 @@ def make_batch_torch(positions, n: int, dt: float, n_seg: int, seed: int, device
             sig[:, -1] = sig[:, -1].real
         F[d] = (nz + sig) * wh_t[None, :]
     return dict(F=F, theta=theta, phi=phi, snr=snr, gmst=gmst)
+
+
+UNEVEN_BUCKETS = (1024, 2048, 4096, 8192, 16384)
+UNEVEN_L = (16, 24, 32, 40, 48)
+
+
+def make_uneven_batch(positions, n_seg: int, seed: int, fs: float = 4096.0, t_range=(0.25, 4.0), l_choices=UNEVEN_L, n_base=(2, 4),
+                      buckets=UNEVEN_BUCKETS, snr_range=(6.0, 30.0), device="cuda"):
+    """The uneven workload: per segment a duration log-uniform in
+    ``t_range`` at ``fs`` (its time series zero-padded to the next DFT length
+    of ``buckets``), an l_max from ``l_choices``, 2-4 of the network's
+    baselines, and a chirp injection (SNR uniform in ``snr_range``,
+    isotropic direction) in coloured, whitened noise.  Returns a dict:
+    ``bucket``, ``n_samples``, ``l_max``, ``mask`` (numpy, per segment) and
+    ``spectra``: a packed complex128 tensor, segment after segment, each
+    [n_det][bucket_n/2 + 1] (the layout sphrad_uneven_layout reports)."""
+    import torch
+    rng = rng_for(seed)
+    pos = np.asarray(positions, np.float64)
+    nd = len(pos)
+    nbl = nd * (nd - 1) // 2
+    dt = 1.0 / fs
+    T = np.exp(rng.uniform(np.log(t_range[0]), np.log(t_range[1]), n_seg))
+    nsamp = np.maximum(1, np.round(T * fs).astype(np.int64))
+    bucket = np.array([int(np.searchsorted(buckets, x)) for x in nsamp])
+    bucket = np.minimum(bucket, len(buckets) - 1)
+    lmax = rng.choice(np.asarray(l_choices), n_seg).astype(np.uint32)
+    mask = np.zeros(n_seg, np.uint32)
+    for s in range(n_seg):
+        k = int(rng.integers(n_base[0], n_base[1] + 1))
+        for b in rng.choice(nbl, size=min(k, nbl), replace=False):
+            mask[s] |= np.uint32(1 << int(b))
+    spectra_parts = [None] * n_seg
+    for bi, nb in enumerate(buckets):
+        idx = np.nonzero(bucket == bi)[0]
+        if idx.size == 0:
+            continue
+        b = make_batch_torch(pos, nb, dt, idx.size, seed * 7919 + bi, device=device, snr_range=snr_range)
+        F = b["F"]                                              # [nd][S][K]
+        x = torch.fft.irfft(F, n=nb, dim=2)
+        keep = torch.as_tensor(nsamp[idx], device=device)[None, :, None]
+        t = torch.arange(nb, device=device)[None, None, :]
+        x = torch.where(t < keep, x, torch.zeros_like(x))
+        F = torch.fft.rfft(x, dim=2)
+        for r, s in enumerate(idx):
+            spectra_parts[s] = F[:, r, :].reshape(-1)
+    spectra = torch.cat(spectra_parts)
+    return dict(bucket=bucket, n_samples=nsamp, l_max=lmax, mask=mask, spectra=spectra, buckets=np.asarray(buckets))
