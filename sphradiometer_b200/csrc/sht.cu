@@ -17,9 +17,10 @@
 //              (times (-1)^m for m < 0: Y_{l,-m} = (-1)^m conj(Y_lm))
 //   azimuth    f(theta_i, phi_j) = sum_m F_m(theta_i) e^{i m phi_j}
 // and the reverse for analysis.  The azimuthal sums run directly over the
-// 2M+1 non-zero orders with an exact integer twiddle index (m j) mod nphi,
-// which also folds orders above the grid's Nyquist limit exactly as
-// evaluating e^{i m phi_j} would.  Legendre tables are built in FP64 by the
+// 2M+1 non-zero orders -- synthesis by Horner's rule in e^{i phi_j},
+// analysis with an exact integer twiddle index (m j) mod nphi -- so orders
+// above the grid's Nyquist limit fold exactly as evaluating e^{i m phi_j}
+// would.  Legendre tables are built in FP64 by the
 // standard normalised three-term recurrence (GSL's sphPlm convention,
 // Condon-Shortley phase) and stored in the transform's arithmetic type.
 #include <cuda_runtime.h>
@@ -27,6 +28,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -158,7 +160,8 @@ __global__ void k_sht_F(int L_in, int polar, const Tin2 *coeff, long long cstrid
 
 // ---------------------------------------------------------------------------
 // azimuthal synthesis, one block per (row i, series s):
-//   v_j = sum_m F_m e^{2 pi i (m j mod nphi) / nphi}
+//   v_j = sum_m F_m e^{i m phi_j}, phi_j = 2 pi j / nphi, by Horner's rule in
+//   e^{i phi_j} (stable for |z| = 1: rounding grows with the order count)
 // MODE 0: complex mesh out (OutT2 = T2 or double2)
 // MODE 1: real part out as float
 // MODE 2: per-row arg max of sign * Re v (value, column) into rowbest
@@ -191,23 +194,40 @@ __global__ void k_sht_pix(int nt, int nphi, int M, const typename V2<T>::t *F, c
 	__syncthreads();
 	double best = -INFINITY;
 	int bestj = 0;
-	const int mstart = ((-M) % nphi + nphi) % nphi;
 	for(int j = threadIdx.x; j < nphi; j += blockDim.x) {
-		int idx = (int) (((long long) mstart * j) % nphi);
-		T vr = 0, vi = 0, wr = 0, wi = 0;
-		for(int k = 0; k < W; k++) {
-			const T2 e = tws[idx];
+		// Horner in z = e^{i phi_j}: sum_k F_k z^k, k = m + M, then the
+		// factor e^{-i M phi_j}; one broadcast read of F per order
+		const T2 z = tws[j];
+		T vr = Fs[W - 1].x, vi = Fs[W - 1].y, wr = 0, wi = 0;
+		if(MODE == 3) {
+			wr = F2s[W - 1].x;
+			wi = F2s[W - 1].y;
+		}
+		for(int k = W - 2; k >= 0; k--) {
 			const T2 f = Fs[k];
-			vr += f.x * e.x - f.y * e.y;
-			vi += f.x * e.y + f.y * e.x;
+			const T nr = vr * z.x - vi * z.y + f.x;
+			const T ni = vr * z.y + vi * z.x + f.y;
+			vr = nr;
+			vi = ni;
 			if(MODE == 3) {
 				const T2 g = F2s[k];
-				wr += g.x * e.x - g.y * e.y;
-				wi += g.x * e.y + g.y * e.x;
+				const T qr = wr * z.x - wi * z.y + g.x;
+				const T qi = wr * z.y + wi * z.x + g.y;
+				wr = qr;
+				wi = qi;
 			}
-			idx += j;
-			if(idx >= nphi)
-				idx -= nphi;
+		}
+		{
+			const T2 e = tws[(int) (((long long) M * j) % nphi)];  // e^{+i M phi_j}; multiply by its conjugate
+			T tr = vr * e.x + vi * e.y, ti = vi * e.x - vr * e.y;
+			vr = tr;
+			vi = ti;
+			if(MODE == 3) {
+				tr = wr * e.x + wi * e.y;
+				ti = wi * e.x - wr * e.y;
+				wr = tr;
+				wi = ti;
+			}
 		}
 		if(MODE == 0)
 			out[row * nphi + j] = OutT{vr, vi};
@@ -390,29 +410,33 @@ struct PeakEval {
 	double f, ft, fp, ftt, ftp, fpp;
 };
 
-__device__ void peak_eval_order(int L, int polar, const double2 *c, int m, double x, double st, double phi, PeakEval &acc)
+// recurrence coefficients of order m, degree l (table [tab_off(L, 1, m) + l - m]):
+// a, b of lambda_l = a x lambda_{l-1} - b lambda_{l-2} (l = m+1: a =
+// sqrt(2m+3), b = 0) and c_l = sqrt((2l+1)(l^2 - m^2)/(2l-1)) of the
+// derivative; lnpre[m] is the log normalisation of lambda_m^m
+struct RecCoef {
+	double a, b, c;
+};
+
+__device__ void peak_eval_order(int L, int polar, const double2 *c, int m, double x, double st, double phi, const RecCoef *rc, const double *lnpre,
+				PeakEval &acc)
 {
-	const double lp = lnpre_mm(m);
-	double lam = exp(lp + m * log(st));
+	double lam = exp(lnpre[m] + m * log(st));
 	if(m & 1)
 		lam = -lam;
 	double lam_prev = 0;
 	double Ar = 0, Ai = 0, A1r = 0, A1i = 0, A2r = 0, A2i = 0;
 	double Br = 0, Bi = 0, B1r = 0, B1i = 0, B2r = 0, B2i = 0;
 	const double inv_s = 1.0 / st, cot = x / st, m2s = (double) m * m * inv_s * inv_s;
+	const RecCoef *r = rc + tab_off(L, 1, m) - m;
 	for(int l = m; l <= L; l++) {
-		if(l == m + 1) {
-			lam_prev = lam;
-			lam = x * sqrt(2.0 * m + 3.0) * lam;
-		} else if(l > m + 1) {
-			const double a = sqrt((2.0 * l + 1.0) * (2.0 * l - 1.0) / ((double) (l - m) * (l + m)));
-			const double b = sqrt((2.0 * l + 1.0) * (l + m - 1.0) * (l - m - 1.0) / ((2.0 * l - 3.0) * (l - m) * (l + m)));
-			const double p = a * x * lam - b * lam_prev;
+		const RecCoef k = r[l];
+		if(l > m) {
+			const double p = k.a * x * lam - k.b * lam_prev;
 			lam_prev = lam;
 			lam = p;
 		}
-		const double cl = (l > m) ? sqrt((2.0 * l + 1.0) * ((double) l * l - (double) m * m) / (2.0 * l - 1.0)) : 0.0;
-		const double d1 = (l * x * lam - cl * lam_prev) * inv_s;
+		const double d1 = (l * x * lam - k.c * lam_prev) * inv_s;
 		const double d2 = -cot * d1 - ((double) l * (l + 1) - m2s) * lam;
 		const double2 cp = c[polar ? l : lmoff(L, l, m)];
 		Ar += cp.x * lam;
@@ -456,7 +480,7 @@ __device__ void peak_eval_order(int L, int polar, const double2 *c, int m, doubl
 	acc.ftp += -m * ImA1 + m * ImB1;
 }
 
-__device__ PeakEval peak_eval(int L, int polar, const double2 *c, double theta, double phi)
+__device__ PeakEval peak_eval(int L, int polar, const double2 *c, double theta, double phi, const RecCoef *rc, const double *lnpre)
 {
 	PeakEval e = {0, 0, 0, 0, 0, 0};
 	double st, x;
@@ -467,9 +491,9 @@ __device__ PeakEval peak_eval(int L, int polar, const double2 *c, double theta, 
 	const int M = polar ? 0 : L;
 	// pair order k with M - k so lanes carry equal recurrence lengths
 	for(int k = lane; k <= M / 2; k += 32) {
-		peak_eval_order(L, polar, c, k, x, st, phi, e);
+		peak_eval_order(L, polar, c, k, x, st, phi, rc, lnpre, e);
 		if(M - k != k)
-			peak_eval_order(L, polar, c, M - k, x, st, phi, e);
+			peak_eval_order(L, polar, c, M - k, x, st, phi, rc, lnpre, e);
 	}
 	for(int o = 16; o; o >>= 1) {
 		e.f += __shfl_xor_sync(0xffffffffu, e.f, o);
@@ -505,8 +529,24 @@ __device__ double ang_dist(double t1, double p1, double t2, double p2)
 }
 
 __global__ void k_peak_refine(int S, int L, int polar, const double2 *coeff, long long cstride, const double *theta0, const double *phi0, double sign,
-			      int max_iter, double tol, double *out /* [S][4] */, int *status)
+			      int max_iter, double tol, double *out /* [S][4] */, int *status, const RecCoef *rc_g, const double *lnpre_g, int n_rc)
 {
+	// the tables in shared memory when they fit (n_rc > 0), else read
+	// from global memory
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const RecCoef *rc = rc_g;
+	const double *lnpre = lnpre_g;
+	if(n_rc > 0) {
+		RecCoef *rcs = (RecCoef *) smem_raw;
+		double *lps = (double *) (rcs + n_rc);
+		for(int i = threadIdx.x; i < n_rc; i += blockDim.x)
+			rcs[i] = rc_g[i];
+		for(int i = threadIdx.x; i <= L; i += blockDim.x)
+			lps[i] = lnpre_g[i];
+		__syncthreads();
+		rc = rcs;
+		lnpre = lps;
+	}
 	const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
 	if(s >= S)
 		return;
@@ -522,7 +562,7 @@ __global__ void k_peak_refine(int S, int L, int polar, const double2 *coeff, lon
 	condition_tp(t, p);
 	const double ts = t, ps = p;
 	double radius = M_PI / 24;
-	PeakEval e = peak_eval(L, polar, c, t, p);
+	PeakEval e = peak_eval(L, polar, c, t, p, rc, lnpre);
 	double g = sign * e.f;
 	int it = 0, converged = 0;
 	for(; it < max_iter; it++) {
@@ -554,7 +594,7 @@ __global__ void k_peak_refine(int S, int L, int polar, const double2 *coeff, lon
 		}
 		double tn = t + du, pn = p + dv / st;
 		condition_tp(tn, pn);
-		const PeakEval en = peak_eval(L, polar, c, tn, pn);
+		const PeakEval en = peak_eval(L, polar, c, tn, pn, rc, lnpre);
 		const double gn = sign * en.f;
 		if(gn >= g) {
 			// a short step that no longer raises the value is at the
@@ -924,15 +964,77 @@ int sht_product(void *plan, int S, const void *a, long long astride, unsigned La
 	return sht_analysis(plan, mesh, S, Ld, pd_eff, dest, dstride, H, stream, Ld_layout);
 }
 
+// recurrence tables of the refinement, per (device, l_max), built on the
+// host in FP64 and kept for the process
+struct RecTable {
+	RecCoef *rc = nullptr;
+	double *lnpre = nullptr;
+	int n = 0;
+};
+static std::mutex g_rec_mu;
+static std::map<std::pair<int, unsigned>, RecTable> g_rec;
+
+static int rec_table(unsigned L, RecTable *out)
+{
+	const int dev = current_device();
+	std::lock_guard<std::mutex> lk(g_rec_mu);
+	auto key = std::make_pair(dev, L);
+	auto it = g_rec.find(key);
+	if(it != g_rec.end()) {
+		*out = it->second;
+		return 0;
+	}
+	const int n = (int) tab_off((int) L, 1, (int) L + 1);
+	std::vector<RecCoef> rc(n);
+	std::vector<double> lp(L + 1);
+	for(int m = 0; m <= (int) L; m++) {
+		double v = 0.5 * log((2.0 * m + 1.0) / (4.0 * M_PI));
+		for(int k = 1; k <= m; k++)
+			v += 0.5 * log((2.0 * k - 1.0) / (2.0 * k));
+		lp[m] = v;
+		for(int l = m; l <= (int) L; l++) {
+			RecCoef c = {0, 0, 0};
+			if(l == m + 1)
+				c.a = sqrt(2.0 * m + 3.0);
+			else if(l > m + 1) {
+				c.a = sqrt((2.0 * l + 1.0) * (2.0 * l - 1.0) / ((double) (l - m) * (l + m)));
+				c.b = sqrt((2.0 * l + 1.0) * (l + m - 1.0) * (l - m - 1.0) / ((2.0 * l - 3.0) * (l - m) * (l + m)));
+			}
+			if(l > m)
+				c.c = sqrt((2.0 * l + 1.0) * ((double) l * l - (double) m * m) / (2.0 * l - 1.0));
+			rc[tab_off((int) L, 1, m) + l - m] = c;
+		}
+	}
+	RecTable t;
+	t.n = n;
+	t.rc = (RecCoef *) dmalloc(n * sizeof(RecCoef));
+	t.lnpre = (double *) dmalloc((L + 1) * sizeof(double));
+	if(!t.rc || !t.lnpre || h2d(t.rc, rc.data(), n * sizeof(RecCoef)) || h2d(t.lnpre, lp.data(), (L + 1) * sizeof(double)) || stream_sync()) {
+		dfree(t.rc);
+		dfree(t.lnpre);
+		return -1;
+	}
+	g_rec[key] = t;
+	*out = t;
+	return 0;
+}
+
 int peak_refine(int S, unsigned L, int polar, const void *coeff, long long cstride, const double *theta0, const double *phi0, double sign, int max_iter,
 		double tol, double *out, int *status, void *stream)
 {
 	cudaStream_t st = stream ? (cudaStream_t) stream : lstream();
 	if(S <= 0)
 		return 0;
+	RecTable t;
+	if(rec_table(L, &t))
+		return -1;
+	size_t sm = (size_t) t.n * sizeof(RecCoef) + (L + 1) * sizeof(double);
+	const bool staged = sm <= kMaxDynSmem;
+	if(!staged)
+		sm = 0;
 	const int wpb = 4;
-	k_peak_refine<<<(S + wpb - 1) / wpb, 32 * wpb, 0, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out,
-								 status);
+	k_peak_refine<<<(S + wpb - 1) / wpb, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out,
+								  status, t.rc, t.lnpre, staged ? t.n : 0);
 	CK(cudaGetLastError());
 	return 0;
 }
