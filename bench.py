@@ -226,7 +226,8 @@ def accuracy_report(S, net, base, n_check: int, positions):
     gd = torch.from_numpy(base["gmst"][:n_check].copy()).cuda()
     out = {"segments": n_check,
            "metric": "[relative L2 of the a_lm vs the FP64 oracle over the sample, worst sky, worst peak-direction error in degrees "
-                     "(same FP64 localisation of the GPU sky and of the oracle sky, up to the mirror image)]",
+                     "(same FP64 localisation of the GPU sky and of the oracle sky, up to the mirror image), skies whose localisation "
+                     "switched between two maxima of equal height to 1e-4 ([angle, relative height gap]), excluded from the worst error]",
            "localiser_vs_oracle_extremizer": {"same_maximum": int(sum(e < 1e-5 for e in loc)), "of": n_check,
                                               "note": "both refine from the l<=6 14x14 mesh's best pixel; where they part, they reach different local maxima"}}
     for prec in ("fp64", "fp32", "bf16x3", "bf16x6"):
@@ -236,7 +237,22 @@ def accuracy_report(S, net, base, n_check: int, positions):
         sky, pk = sky_d.cpu().numpy(), pk.cpu().numpy()
         bp.close()
         worst = max(np.linalg.norm(sky[s] - ref[s]) / np.linalg.norm(ref[s]) for s in range(n_check))
-        out[prec] = [float(np.linalg.norm(sky - ref) / np.linalg.norm(ref)), float(worst), float(max(peak_err(pk[s], s) for s in range(n_check)))]
+        # a sky whose localisation lands on another maximum of (to 1e-4)
+        # the same height is degenerate: the precision only decides which
+        # of two equal peaks the coarse search starts in
+        errs, degenerate = [], []
+        for s in range(n_check):
+            e_ = peak_err(pk[s], s)
+            if e_ > 0.1:
+                fa = O.eval_at(ref[s], L_MAX, False, pk[s, 0], pk[s, 1]).real
+                fb = O.eval_at(ref[s], L_MAX, False, pk_ref[s, 0], pk_ref[s, 1]).real
+                gap = abs(fa - fb) / abs(fb)
+                if gap < 1e-4:
+                    degenerate.append([round(e_, 3), float(gap)])
+                    continue
+            errs.append(e_)
+        out[prec] = [float(np.linalg.norm(sky - ref) / np.linalg.norm(ref)), float(worst), float(max(errs) if errs else 0.0),
+                     {"degenerate_skies": degenerate}]
     return out
 
 
@@ -631,6 +647,7 @@ def run(args):
             "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "bf16x3 (fp32 accumulate)" if prec == "bf16x3" else prec, "data": "synthetic (seeded whitened noise + chirp injections)",
             "config": {"workload": WORKLOAD, "segments_per_step": n_seg, "precision": prec, "split_k": split,
+                       "pipeline_variant": S.load().sphrad_batch_pipeline(bp._p, n_seg),
                        "l2": f"inputs larger than L2: ring of {n_ring} distinct batches, {n_ring * batch_bytes / 2**20:.0f} MiB",
                        "parallelism": f"replicas x{world} (segments sharded, no collective)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

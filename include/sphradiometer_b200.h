@@ -109,6 +109,10 @@ int sphrad_batch_set_split(sphrad_batch_plan *plan, int n_seg, int split);
  * the chosen split or -1. */
 int sphrad_batch_autotune(sphrad_batch_plan *plan, const void *fseries, int n_seg, long long ld, void *sky, void *workspace, size_t workspace_bytes,
 			  void *cuda_stream);
+/* Pipeline variant chosen by sphrad_batch_autotune for n_seg (tcgen05
+ * paths): 0 = 2-deep spectrum ring with a 4-deep X-operand ring, 1 = 3-deep
+ * spectrum ring with a 2-deep X-operand ring. */
+int sphrad_batch_pipeline(const sphrad_batch_plan *plan, int n_seg);
 /* Kernels launched by the last integrate call. */
 int sphrad_batch_kernels_per_call(const sphrad_batch_plan *plan);
 /* Profiling hook: when set (cudaEvent_t handles, or NULL to clear), every

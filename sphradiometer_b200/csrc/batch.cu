@@ -508,6 +508,98 @@ __global__ void k_epilogue(const __grid_constant__ EpArgs e, T *acc)
 	}
 }
 
+// The same epilogue for the FP32 paths with at most EB baselines: blocks
+// stay resident and loop over segments, every thread owns up to QMAX fixed
+// output coefficients (q = tid + k * blockDim) and keeps their weights and
+// (l, m) in registers, so the per-segment work is one shared row of partial
+// sums, one phase table and coalesced FP64 stores.
+constexpr int EPI2_THREADS = 256;
+constexpr int EB = 3;
+
+template <int QMAX>
+__global__ void __launch_bounds__(EPI2_THREADS) k_epilogue_f32(const __grid_constant__ EpArgs e, float *acc)
+{
+	// two buffers of partial sums and of the segment's base phase
+	// e^{-i gmst}: the next segment's are fetched while the current one is
+	// written
+	extern __shared__ __align__(16) uint8_t ep_smem[];
+	double2 *sPh = (double2 *) ep_smem;              // [2L+1]
+	double2 *sBase = sPh + 2 * e.L + 1;              // [2]
+	float *sP = (float *) (sBase + 2);               // [2][B][Lp1]
+	const int nP = e.B * e.Lp1;
+	float2 w[QMAX][EB];
+	short ql[QMAX], qm[QMAX];
+	const float2 *W = (const float2 *) e.W;
+#pragma unroll
+	for(int k = 0; k < QMAX; k++) {
+		const int q = threadIdx.x + k * EPI2_THREADS;
+		const bool in = q < e.nq;
+		ql[k] = in ? e.lq[q] : 0;
+		qm[k] = in ? e.mq[q] : 0;
+#pragma unroll
+		for(int b = 0; b < EB; b++)
+			w[k][b] = (in && b < e.B) ? W[(size_t) b * e.nq + q] : make_float2(0.f, 0.f);
+	}
+	auto fetch = [&](int s, int buf) {
+		const float *row = acc + (size_t) s * e.B * e.accstride;
+		float *dst = sP + buf * nP;
+		for(int i = threadIdx.x; i < nP; i += blockDim.x) {
+			const int b = i / e.Lp1;
+			dst[i] = __ldcg(&row[b * e.accstride + i % e.Lp1]) * (e.segw ? e.segw[(size_t) s * e.B + b] : 1.f);
+		}
+		if(threadIdx.x == blockDim.x - 1) {
+			double sn = 0.0, cs = 1.0;
+			if(e.gmst)
+				sincos(-e.gmst[s], &sn, &cs);
+			sBase[buf] = make_double2(cs, sn);
+		}
+	};
+	int it = 0;
+	if((int) blockIdx.x < e.S)
+		fetch(blockIdx.x, 0);
+	for(int s = blockIdx.x; s < e.S; s += gridDim.x, it++) {
+		const int buf = it & 1;
+		__syncthreads();  // this segment's buffer is complete; the phase table is free
+		const int sn_ = s + gridDim.x;
+		if(sn_ < e.S)
+			fetch(sn_, buf ^ 1);
+		// e^{-i m gmst} = base^m by binary powers (|m| <= L), FP64
+		for(int m = (int) threadIdx.x - e.L; m <= e.L; m += blockDim.x) {
+			const double2 z = sBase[buf];
+			double2 r = make_double2(1.0, 0.0), pw = make_double2(z.x, m < 0 ? -z.y : z.y);
+			for(int k = m < 0 ? -m : m; k; k >>= 1) {
+				if(k & 1)
+					r = make_double2(r.x * pw.x - r.y * pw.y, r.x * pw.y + r.y * pw.x);
+				pw = make_double2(pw.x * pw.x - pw.y * pw.y, 2 * pw.x * pw.y);
+			}
+			sPh[m + e.L] = r;
+		}
+		// leave the workspace zeroed for the next launch (read at the fetch)
+		float *row = acc + (size_t) s * e.B * e.accstride;
+		for(int i = threadIdx.x; i < e.B * e.accstride; i += blockDim.x)
+			row[i] = 0.f;
+		__syncthreads();  // phase table ready
+		const float *cP = sP + buf * nP;
+		double2 *out = e.sky + (size_t) s * e.nq;
+#pragma unroll
+		for(int k = 0; k < QMAX; k++) {
+			const int q = threadIdx.x + k * EPI2_THREADS;
+			if(q < e.nq) {
+				float re = 0.f, im = 0.f;
+#pragma unroll
+				for(int b = 0; b < EB; b++)
+					if(b < e.B) {
+						const float pv = cP[b * e.Lp1 + ql[k]];
+						re += w[k][b].x * pv;
+						im += w[k][b].y * pv;
+					}
+				const double2 ph = sPh[qm[k] + e.L];
+				out[q] = make_double2((double) re * ph.x - (double) im * ph.y, (double) re * ph.y + (double) im * ph.x);
+			}
+		}
+	}
+}
+
 // ------------------------------------------------------------------------
 // plan
 // ------------------------------------------------------------------------
@@ -524,8 +616,12 @@ struct BatchPlan {
 	void *W = nullptr;         // [B][nq] complex T
 	short *lq = nullptr, *mq = nullptr;
 	unsigned *err = nullptr;
-	// tuned split per S
+	// tuned split per S, and the pipeline variant (ring depths) per S:
+	// 0 = the plan's default rings, 1 = a 3-deep spectrum ring with a
+	// 2-deep X-operand ring (more bytes in flight per SM)
 	std::map<int, int> split;
+	std::map<int, int> pipe;
+	int nf0 = NF, nab0 = 4;
 	// optional CUDA events recorded around the contraction kernel
 	cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
 	int last_kernels = 0;
@@ -736,11 +832,14 @@ void *batch_plan_create(const BatchPlanDesc &d, int precision)
 			// large l_max leave no room for four stages
 			if(!fail && P->npart == 2 && tc_smem_bytes(*P) > 227 * 1024)
 				P->nab = 3;
+			P->nf0 = P->nf;
+			P->nab0 = P->nab;
 			if(!fail && tc_smem_bytes(*P) > 227 * 1024) {
 				set_error("batch plan: shared-memory budget exceeded");
 				fail = true;
 			}
 			if(!fail && (cudaFuncSetAttribute(k_tc_contract<2, NF, 4, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
+				     cudaFuncSetAttribute(k_tc_contract<2, 3, 2, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
 				     cudaFuncSetAttribute(k_tc_contract<2, NF, 3, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
 				     cudaFuncSetAttribute(k_tc_contract<3, NF, 2, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess)) {
 				set_error("batch plan: cannot reserve %zu bytes of shared memory", tc_smem_bytes(*P));
@@ -804,7 +903,7 @@ int batch_set_split(void *pp, int S, int ks)
 }
 
 int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream_v, int split,
-	      const float *segw)
+	      const float *segw, int pipe_variant)
 {
 	BatchPlan *P = (BatchPlan *) pp;
 	cudaStream_t st = (cudaStream_t) stream_v;
@@ -868,15 +967,29 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 		a.acc = (float *) ws;
 		a.err = P->err;
 		const int tiles = (S + TM - 1) / TM;
+		// pipeline variant for this batch size (tuned), within the
+		// shared-memory budget
+		P->nf = P->nf0;
+		P->nab = P->nab0;
+		const int variant = pipe_variant >= 0 ? pipe_variant : (P->pipe.count(S) ? P->pipe[S] : 0);
+		if(variant == 1 && P->npart == 2) {
+			P->nf = 3;
+			P->nab = 2;
+			if(tc_smem_bytes(*P) > 227 * 1024) {
+				P->nf = P->nf0;
+				P->nab = P->nab0;
+			}
+		}
 		if(P->ev_begin)
 			cudaEventRecord(P->ev_begin, st);
 		if(P->npart == 3)
 			k_tc_contract<3, NF, 2, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+		else if(P->nf == 3)
+			k_tc_contract<2, 3, 2, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+		else if(P->nab == 4)
+			k_tc_contract<2, NF, 4, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		else
-			if(P->nab == 4)
-				k_tc_contract<2, NF, 4, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
-			else
-				k_tc_contract<2, NF, 3, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			k_tc_contract<2, NF, 3, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		if(P->ev_end)
 			cudaEventRecord(P->ev_end, st);
 		launches++;
@@ -937,7 +1050,20 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 	e.sky = (double2 *) sky;
 	const size_t el = P->precision == kPrecFP64 ? sizeof(double) : sizeof(float);
 	const size_t esmem = (size_t) P->B * P->Lp1 * el + (2 * P->L + 1) * sizeof(double2);
-	if(P->precision == kPrecFP64)
+	const int qmax = (P->nq + EPI2_THREADS - 1) / EPI2_THREADS;
+	if(P->precision != kPrecFP64 && P->B <= EB && qmax <= 10) {
+		int sms = 148, dev = 0;
+		cudaGetDevice(&dev);
+		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+		// resident blocks only (4 per SM by registers at QMAX 5, 2 at 10)
+		const int per_sm = qmax <= 5 ? 4 : 2;
+		const int grid = S < per_sm * sms ? S : per_sm * sms;
+		const size_t esm2 = (size_t) (2 * P->L + 1 + 2) * sizeof(double2) + (size_t) 2 * P->B * P->Lp1 * sizeof(float);
+		if(qmax <= 5)
+			k_epilogue_f32<5><<<grid, EPI2_THREADS, esm2, st>>>(e, (float *) ws);
+		else
+			k_epilogue_f32<10><<<grid, EPI2_THREADS, esm2, st>>>(e, (float *) ws);
+	} else if(P->precision == kPrecFP64)
 		k_epilogue<double><<<S, 128, esmem, st>>>(e, (double *) ws);
 	else
 		k_epilogue<float><<<S, 128, esmem, st>>>(e, (float *) ws);
@@ -973,28 +1099,39 @@ int batch_autotune(void *pp, const void *F, int S, long long ld, void *sky, void
 	cudaEvent_t e0, e1;
 	CKB(cudaEventCreate(&e0));
 	CKB(cudaEventCreate(&e1));
-	int best = cand[0];
+	int best = cand[0], best_v = 0;
 	float best_ms = 1e30f;
-	for(int ks : cand) {
-		if(batch_run(P, F, S, ld, nullptr, sky, ws, ws_bytes, st, ks))
-			return -1;
-		CKB(cudaEventRecord(e0, st));
-		for(int r = 0; r < 3; r++)
-			if(batch_run(P, F, S, ld, nullptr, sky, ws, ws_bytes, st, ks))
+	const int n_var = (is_tc(P->precision) && P->npart == 2) ? 2 : 1;
+	for(int v = 0; v < n_var; v++)
+		for(int ks : cand) {
+			if(batch_run(P, F, S, ld, nullptr, sky, ws, ws_bytes, st, ks, nullptr, v))
 				return -1;
-		CKB(cudaEventRecord(e1, st));
-		CKB(cudaEventSynchronize(e1));
-		float ms = 0;
-		CKB(cudaEventElapsedTime(&ms, e0, e1));
-		if(ms < best_ms) {
-			best_ms = ms;
-			best = ks;
+			CKB(cudaEventRecord(e0, st));
+			for(int r = 0; r < 3; r++)
+				if(batch_run(P, F, S, ld, nullptr, sky, ws, ws_bytes, st, ks, nullptr, v))
+					return -1;
+			CKB(cudaEventRecord(e1, st));
+			CKB(cudaEventSynchronize(e1));
+			float ms = 0;
+			CKB(cudaEventElapsedTime(&ms, e0, e1));
+			if(ms < best_ms) {
+				best_ms = ms;
+				best = ks;
+				best_v = v;
+			}
 		}
-	}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
 	P->split[S] = best;
+	P->pipe[S] = best_v;
 	return best;
+}
+
+int batch_pipe_variant(const void *pp, int S)
+{
+	const BatchPlan *P = (const BatchPlan *) pp;
+	auto it = P->pipe.find(S);
+	return it == P->pipe.end() ? 0 : it->second;
 }
 
 int batch_set_timing_events(void *pp, void *ev_begin, void *ev_end)

@@ -92,8 +92,11 @@ unsigned batch_plan_l_max(const void *plan);
 int batch_plan_bins(const void *plan);  // bins read per spectrum row
 size_t batch_workspace_bytes(const void *plan, int S);
 // segw: optional [S][B] factors on each segment's baselines (device)
+// pipe_variant: -1 = the tuned one for S (default 0), else 0 / 1 (see
+// batch.cu: ring depths of the tcgen05 pipeline)
 int batch_run(void *plan, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream, int split,
-	      const float *segw = nullptr);
+	      const float *segw = nullptr, int pipe_variant = -1);
+int batch_pipe_variant(const void *plan, int S);
 int batch_run_host(void *plan, const void *F_host, int S, long long ld, const double *gmst_host, void *sky_host);
 int batch_pick_split(const void *plan, int S);
 int batch_last_kernel_count(const void *plan);
