@@ -88,6 +88,18 @@ __device__ __forceinline__ float gelu_grad(float z)
 // rows x 16 B, LBO 128 (K direction), SBO 256 (8-row groups)
 __device__ __forceinline__ uint32_t tile_off(int R, int r, int c) { return (uint32_t) ((c >> 1) * (R * 32) + (r >> 3) * 256 + (c & 1) * 128 + (r & 7) * 16); }
 
+// 16-byte asynchronous copies global -> shared (cp.async): the operand
+// tiles of later K chunks load while the tensor core works on earlier ones
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src)
+{
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+constexpr int GSTAGES = 4;  // operand ring depth (K chunks in shared memory)
+
 template <int NT, int EPI>
 __global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ GemmArgs g)
 {
@@ -96,8 +108,8 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ Gemm
 	constexpr uint32_t NCOLS = NT < 32 ? 32 : NT;
 	extern __shared__ uint8_t smem_raw[];
 	uint8_t *smem = (uint8_t *) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
-	uint8_t *sA = smem, *sB = smem + 2 * A_BYTES;
-	__shared__ __align__(8) uint64_t bars[2];
+	uint8_t *sA = smem, *sB = smem + GSTAGES * A_BYTES;
+	__shared__ __align__(8) uint64_t bars[GSTAGES];
 	__shared__ uint32_t tslot;
 	__shared__ int abort_flag;
 
@@ -105,8 +117,8 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ Gemm
 	const int tiles_n = g.N / NT;
 	const int m0 = (blockIdx.x / tiles_n) * GM, n0 = (blockIdx.x % tiles_n) * NT;
 	if(tid == 0) {
-		mbar_init(smem_u32(&bars[0]), 1);
-		mbar_init(smem_u32(&bars[1]), 1);
+		for(int i = 0; i < GSTAGES; i++)
+			mbar_init(smem_u32(&bars[i]), 1);
 		abort_flag = 0;
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
@@ -118,41 +130,59 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ Gemm
 	const uint32_t tmem = tslot;
 	const uint32_t idesc = idesc_bf16(GM, NT);
 	const int nk = g.K / GK;
-	bool ok = true;
-	int issued = -1;  // last chunk whose MMAs were issued
-	for(int kc = 0; kc < nk && ok; kc++) {
-		const int b = kc & 1;
-		if(kc >= 2)
-			ok = mbar_wait(smem_u32(&bars[b]), ((kc >> 1) - 1) & 1, &abort_flag, g.err, 1);
-		ok = __syncthreads_and(ok);
-		if(!ok)
-			break;
-		uint8_t *a_s = sA + b * A_BYTES, *b_s = sB + b * B_BYTES;
+	// every thread issues its share of chunk kc's 16-byte copies
+	auto load = [&](int kc) {
+		const int b = kc % GSTAGES;
+		const uint32_t a_s = smem_u32(sA + b * A_BYTES), b_s = smem_u32(sB + b * B_BYTES);
 		const __nv_bfloat16 *Ag = g.A + (long long) m0 * g.lda + (long long) kc * GK;
 		for(int i = tid; i < GM * 8; i += G_THREADS) {
 			const int r = i >> 3, c = i & 7;
-			*(uint4 *) (a_s + tile_off(GM, r, c)) = *(const uint4 *) (Ag + (long long) r * g.lda + c * 8);
+			cp_async16(a_s + tile_off(GM, r, c), Ag + (long long) r * g.lda + c * 8);
 		}
 		const __nv_bfloat16 *Bg = g.B + (long long) n0 * g.ldb + (long long) kc * GK;
 		for(int i = tid; i < NT * 8; i += G_THREADS) {
 			const int r = i >> 3, c = i & 7;
-			*(uint4 *) (b_s + tile_off(NT, r, c)) = *(const uint4 *) (Bg + (long long) r * g.ldb + c * 8);
+			cp_async16(b_s + tile_off(NT, r, c), Bg + (long long) r * g.ldb + c * 8);
 		}
+	};
+	for(int s = 0; s < GSTAGES - 1; s++) {
+		if(s < nk)
+			load(s);
+		cp_async_commit();
+	}
+	bool ok = true;
+	int issued = -1;  // last chunk whose MMAs were issued
+	for(int kc = 0; kc < nk; kc++) {
+		const int b = kc % GSTAGES;
+		// chunk kc is complete for this thread; hand it to the async proxy
+		cp_async_wait<GSTAGES - 2>();
 		fence_proxy_async();
 		__syncthreads();
 		if(tid == 0) {
 			tc_fence_after();
-			const uint32_t a0 = smem_u32(a_s), b0 = smem_u32(b_s);
+			const uint32_t a0 = smem_u32(sA + b * A_BYTES), b0 = smem_u32(sB + b * B_BYTES);
 #pragma unroll
 			for(int s = 0; s < GK / 16; s++)
 				umma_bf16(tmem, umma_desc(a0 + s * GM * 32, 128, 256), umma_desc(b0 + s * NT * 32, 128, 256), idesc, (kc > 0 || s > 0) ? 1u : 0u);
 			umma_commit(smem_u32(&bars[b]));
 		}
 		issued = kc;
+		// refill the slot chunk kc - 1 used, once its MMAs are done
+		const int nx = kc + GSTAGES - 1;
+		if(nx < nk) {
+			if(kc >= 1)
+				ok = mbar_wait(smem_u32(&bars[(kc - 1) % GSTAGES]), ((kc - 1) / GSTAGES) & 1, &abort_flag, g.err, 1);
+			ok = __syncthreads_and(ok);
+			if(!ok)
+				break;
+			load(nx);
+		}
+		cp_async_commit();
 	}
+	cp_async_wait_all();
 	// the last commit covers every MMA of the tile
 	if(ok && nk > 0)
-		ok = mbar_wait(smem_u32(&bars[(nk - 1) & 1]), ((nk - 1) >> 1) & 1, &abort_flag, g.err, 2);
+		ok = mbar_wait(smem_u32(&bars[(nk - 1) % GSTAGES]), ((nk - 1) / GSTAGES) & 1, &abort_flag, g.err, 2);
 	tc_fence_after();
 	ok = __syncthreads_and(ok && !abort_flag);
 	if(ok) {
@@ -219,7 +249,7 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ Gemm
 		atomicExch(g.err, 3u);
 		// let the MMAs in flight finish before the accumulator is freed
 		if(issued >= 0)
-			mbar_drain(smem_u32(&bars[issued & 1]), (issued >> 1) & 1);
+			mbar_drain(smem_u32(&bars[issued % GSTAGES]), (issued / GSTAGES) & 1);
 	}
 	tc_fence_before();
 	__syncthreads();
@@ -542,7 +572,7 @@ struct Mlp {
 
 int mlp_refresh(void *plan, void *stream);
 
-static size_t smem_bytes(int NT) { return 1024 + 2 * (GM * GK * 2) + 2 * (NT * GK * 2); }
+static size_t smem_bytes(int NT) { return 1024 + (size_t) GSTAGES * (GM * GK * 2 + NT * GK * 2); }
 
 template <int NT, int EPI>
 static int launch_gemm(const GemmArgs &g, cudaStream_t st)

@@ -19,6 +19,7 @@ def main():
     ap.add_argument("--calls", type=int, default=5)
     ap.add_argument("--precision", default="bf16x3")
     ap.add_argument("--split", type=int, default=0)
+    ap.add_argument("--autotune", action="store_true", help="use the autotuned split-K and pipeline variant")
     args = ap.parse_args()
     import torch
 
@@ -33,7 +34,9 @@ def main():
     idx = np.arange(args.segments) % base["F"].shape[1]
     F = torch.from_numpy(np.ascontiguousarray(base["F"][:, idx, :])).cuda()
     g = torch.from_numpy(base["gmst"][idx].copy()).cuda()
-    if args.split:
+    if args.autotune:
+        bp.autotune(F)
+    elif args.split:
         bp.set_split(args.segments, args.split)
     out = bp.integrate(F, g)
     torch.cuda.synchronize()
@@ -44,7 +47,8 @@ def main():
     b.record()
     torch.cuda.synchronize()
     ms = a.elapsed_time(b) / args.calls
-    print(f"segments {args.segments} split {bp.split(args.segments)} precision {args.precision}: {ms:.4f} ms/call, "
+    print(f"segments {args.segments} split {bp.split(args.segments)} variant {S.load().sphrad_batch_pipeline(bp._p, args.segments)} "
+          f"precision {args.precision}: {ms:.4f} ms/call, "
           f"{args.segments / ms * 1e3:.3e} maps/s, status {bp.status()}")
 
 
