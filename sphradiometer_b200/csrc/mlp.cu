@@ -74,6 +74,7 @@ struct GemmArgs {
 	const float *Zin;       // GeluBwd: pre-activation [M][ldz]
 	long long ldz;
 	float *colsum;          // GeluBwd: += column sums of dZ (may be NULL)
+	int ksplit;             // StoreF32: K split over blockIdx.y, FP32 atomics into a zeroed C
 	unsigned *err;
 };
 
@@ -129,10 +130,16 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ Gemm
 	tc_fence_after();
 	const uint32_t tmem = tslot;
 	const uint32_t idesc = idesc_bf16(GM, NT);
-	const int nk = g.K / GK;
+	// this CTA's K chunks: all of them, or one of ksplit ranges
+	const int nk_all = g.K / GK;
+	const int ks = g.ksplit > 1 ? g.ksplit : 1;
+	const int per = (nk_all + ks - 1) / ks;
+	const int kbeg = blockIdx.y * per;
+	const int nk = kbeg >= nk_all ? 0 : (nk_all - kbeg < per ? nk_all - kbeg : per);
 	// every thread issues its share of chunk kc's 16-byte copies
-	auto load = [&](int kc) {
-		const int b = kc % GSTAGES;
+	auto load = [&](int kc_local) {
+		const int kc = kbeg + kc_local;
+		const int b = kc_local % GSTAGES;
 		const uint32_t a_s = smem_u32(sA + b * A_BYTES), b_s = smem_u32(sB + b * B_BYTES);
 		const __nv_bfloat16 *Ag = g.A + (long long) m0 * g.lda + (long long) kc * GK;
 		for(int i = tid; i < GM * 8; i += G_THREADS) {
@@ -185,7 +192,7 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ Gemm
 		ok = mbar_wait(smem_u32(&bars[(nk - 1) % GSTAGES]), ((nk - 1) / GSTAGES) & 1, &abort_flag, g.err, 2);
 	tc_fence_after();
 	ok = __syncthreads_and(ok && !abort_flag);
-	if(ok) {
+	if(ok && nk > 0) {
 		const int r = warp * 32 + lane;
 		const int m = m0 + r;
 		for(int c0 = 0; c0 < NT; c0 += 16) {
@@ -194,9 +201,17 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ Gemm
 			const int nb = n0 + c0;
 			if(EPI == kEpiStoreF32) {
 				float *dst = g.C + (long long) m * g.ldc + nb;
+				if(ks > 1) {
 #pragma unroll
-				for(int j = 0; j < 16; j += 4)
-					*(float4 *) (dst + j) = make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]), __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
+					for(int j = 0; j < 16; j += 4)
+						atomicAdd((float4 *) (dst + j), make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]), __uint_as_float(v[j + 2]),
+											    __uint_as_float(v[j + 3])));
+				} else {
+#pragma unroll
+					for(int j = 0; j < 16; j += 4)
+						*(float4 *) (dst + j) =
+							make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]), __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
+				}
 			} else if(EPI == kEpiBias) {
 				float *dst = g.C + (long long) m * g.ldc + nb;
 #pragma unroll
@@ -245,7 +260,7 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ Gemm
 				}
 			}
 		}
-	} else if(tid == 0) {
+	} else if(tid == 0 && nk > 0) {
 		atomicExch(g.err, 3u);
 		// let the MMAs in flight finish before the accumulator is freed
 		if(issued >= 0)
@@ -583,8 +598,23 @@ static int launch_gemm(const GemmArgs &g, cudaStream_t st)
 	}
 	const size_t sm = smem_bytes(NT);
 	CKM(cudaFuncSetAttribute(k_gemm<NT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm));
-	const unsigned grid = (unsigned) (g.M / GM) * (unsigned) (g.N / NT);
-	k_gemm<NT, EPI><<<grid, G_THREADS, sm, st>>>(g);
+	const unsigned tiles = (unsigned) (g.M / GM) * (unsigned) (g.N / NT);
+	GemmArgs h = g;
+	h.ksplit = 1;
+	if(EPI == kEpiStoreF32) {
+		// few output tiles over a long K (the weight gradients, K = batch):
+		// split K so about two CTAs per SM work, each on >= 4 chunks
+		const int nk = g.K / GK;
+		int ks = (int) (296 / tiles);
+		if(ks > nk / 4)
+			ks = nk / 4;
+		if(ks > 1) {
+			h.ksplit = ks;
+			CKM(cudaMemsetAsync(g.C, 0, (size_t) g.M * g.ldc * sizeof(float), st));
+		}
+	}
+	dim3 grid(tiles, h.ksplit);
+	k_gemm<NT, EPI><<<grid, G_THREADS, sm, st>>>(h);
 	CKM(cudaGetLastError());
 	return 0;
 }
@@ -753,7 +783,7 @@ int mlp_forward(void *plan, int n, int training, float *dir_out, void *stream)
 		g.HT = training ? p->HT[i] : nullptr;
 		g.ldht = R;
 		g.err = p->err;
-		if(launch_gemm<128, kEpiBiasGelu>(g, st))
+		if(launch_gemm<64, kEpiBiasGelu>(g, st))
 			return -1;
 		in = p->H[i];
 		kin = HID;
@@ -832,7 +862,7 @@ int mlp_backward(void *plan, int n, const float *target, void *stream)
 		g.ldht = R;
 		g.colsum = p->gb[i];
 		g.err = p->err;
-		if(launch_gemm<128, kEpiGeluBwd>(g, st))
+		if(launch_gemm<64, kEpiGeluBwd>(g, st))
 			return -1;
 		// dW_i = dZ_i^T A_{i-1}
 		GemmArgs w = {};
