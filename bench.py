@@ -71,6 +71,25 @@ def profiled_traffic(segments: int):
     return float(m.group(1)) * segments if m else None
 
 
+def partial_sum_rows(n_seg: int, n_stages: int, ctas: int, max_chain: int = 64) -> int:
+    """Segment rows written as FP32 partial sums by one tcgen05 contraction
+    launch: its CTAs take equal contiguous ranges of the (tile, stage) units
+    and flush one piece per run of stages inside a tile (cut into pieces of
+    at most max_chain stages); a piece writes the tile's valid rows."""
+    tiles = -(-n_seg // 128)
+    units = tiles * n_stages
+    rows = 0
+    for c in range(ctas):
+        u0, u1 = units * c // ctas, units * (c + 1) // ctas
+        u = u0
+        while u < u1:
+            t = u // n_stages
+            end = min(u1, (t + 1) * n_stages)
+            rows += -(-(end - u) // max_chain) * min(128, n_seg - 128 * t)
+            u = end
+    return rows
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -537,7 +556,11 @@ def run(args):
     else:
         d_bytes = K * 3 * (L_MAX + 1) * (16 if prec == "fp64" else 8)
         acc_el = 8 if prec == "fp64" else 4
-    alg_bytes = N_DET * n_seg * K * 16 + d_bytes + split * n_seg * 3 * accstride * acc_el
+    if prec == "bf16x3":
+        ps_rows = partial_sum_rows(n_seg, -(-K // 8), bp.ctas(n_seg))
+    else:
+        ps_rows = split * n_seg
+    alg_bytes = N_DET * n_seg * K * 16 + d_bytes + ps_rows * 3 * accstride * acc_el
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / mean_k / 1e9
 
@@ -644,6 +667,7 @@ def run(args):
             "dtype": "bf16x3 (fp32 accumulate)" if prec == "bf16x3" else prec, "data": "synthetic (seeded whitened noise + chirp injections)",
             "config": {"workload": WORKLOAD, "segments_per_step": n_seg, "precision": prec, "split_k": split,
                        "pipeline_variant": S.load().sphrad_batch_pipeline(bp._p, n_seg),
+                       "contraction_ctas": bp.ctas(n_seg) if prec.startswith("bf16") else None,
                        "l2": f"inputs larger than L2: ring of {n_ring} distinct batches, {n_ring * batch_bytes / 2**20:.0f} MiB",
                        "parallelism": f"replicas x{world} (segments sharded, no collective)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

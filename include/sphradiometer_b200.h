@@ -101,12 +101,23 @@ int sphrad_batch_integrate_weighted(sphrad_batch_plan *plan, const void *fseries
 int sphrad_batch_integrate_host(sphrad_batch_plan *plan, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky);
 
 /* Split-K factor used for n_seg segments: the value stored by
- * sphrad_batch_set_split / sphrad_batch_autotune, else a heuristic. */
+ * sphrad_batch_set_split / sphrad_batch_autotune, else a heuristic.  For
+ * the tcgen05 paths this is the CTA count divided by the 128-segment tiles,
+ * rounded. */
 int sphrad_batch_get_split(const sphrad_batch_plan *plan, int n_seg);
+/* Pins the split-K factor for n_seg (0 = back to the heuristic): every
+ * 128-segment tile's frequency stages are cut into `split` equal ranges. */
 int sphrad_batch_set_split(sphrad_batch_plan *plan, int n_seg, int split);
-/* Times the candidate split factors on the given device data (timed with
+/* CTAs of the tcgen05 contraction for n_seg segments (tcgen05 paths): each
+ * takes an equal contiguous range of the (tile, stage) units, so the count
+ * need not be a multiple of the tiles. */
+int sphrad_batch_get_ctas(const sphrad_batch_plan *plan, int n_seg);
+/* Pins the CTA count for n_seg (0 = back to the heuristic); -1 for a
+ * plan without the tcgen05 path. */
+int sphrad_batch_set_ctas(sphrad_batch_plan *plan, int n_seg, int ctas);
+/* Times the candidate work splits on the given device data (timed with
  * CUDA events on the stream) and stores the fastest for n_seg.  Returns
- * the chosen split or -1. */
+ * the split-K factor equivalent to the choice, or -1. */
 int sphrad_batch_autotune(sphrad_batch_plan *plan, const void *fseries, int n_seg, long long ld, void *sky, void *workspace, size_t workspace_bytes,
 			  void *cuda_stream);
 /* Pipeline variant chosen by sphrad_batch_autotune for n_seg (tcgen05

@@ -203,6 +203,15 @@ class BatchPlan:
     def set_split(self, n_seg: int, split: int):
         load().sphrad_batch_set_split(self._p, n_seg, split)
 
+    def ctas(self, n_seg: int) -> int:
+        """CTAs of the tcgen05 contraction for n_seg segments."""
+        return load().sphrad_batch_get_ctas(self._p, n_seg)
+
+    def set_ctas(self, n_seg: int, ctas: int):
+        """Pin the tcgen05 contraction's CTA count for n_seg (0 = default)."""
+        if load().sphrad_batch_set_ctas(self._p, n_seg, ctas) < 0:
+            raise SphradError("sphrad_batch_set_ctas: " + last_error())
+
     def kernels_per_call(self) -> int:
         return load().sphrad_batch_kernels_per_call(self._p)
 

@@ -151,6 +151,8 @@ SIGNATURES = {
     "sphrad_batch_integrate": (_i, [_vp, _vp, _i, _ll, _vp, _vp, _vp, _sz, _vp]),
     "sphrad_batch_integrate_host": (_i, [_vp, _vp, _i, _ll, _vp, _vp]),
     "sphrad_batch_get_split": (_i, [_vp, _i]),
+    "sphrad_batch_get_ctas": (_i, [_vp, _i]),
+    "sphrad_batch_set_ctas": (_i, [_vp, _i, _i]),
     "sphrad_batch_set_split": (_i, [_vp, _i, _i]),
     "sphrad_batch_autotune": (_i, [_vp, _vp, _i, _ll, _vp, _vp, _sz, _vp]),
     "sphrad_batch_kernels_per_call": (_i, [_vp]),

@@ -34,6 +34,7 @@
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -74,7 +75,7 @@ constexpr int kMaxChain = 64;            // most pipeline stages one tcgen05 CTA
 // tcgen05 contraction
 // ------------------------------------------------------------------------
 struct TcArgs {
-	int S, n_det, B, Kst, ks, npad, tmem_cols, accstride;
+	int S, n_det, B, Kst, tiles, npad, tmem_cols, accstride;
 	int bi[TC_MAXB], bj[TC_MAXB];
 	const uint8_t *bops;   // [Kst][B][NPART][npad * KE bf16], UMMA layout
 	float *acc;            // [S][B][accstride]
@@ -112,6 +113,39 @@ __device__ __forceinline__ void split_pair(float re, float im, uint32_t *w)
 //   NPART = 2: hi x [hi|lo] -> [0|1], lo x hi -> 1
 //   NPART = 3: hi x [hi|mid|lo] -> [0|1|2], mid x [hi|mid] -> [1|2], lo x hi -> 2
 
+// Work split ("stream-K"): the tiles x Kst (tile, stage) units, tile-major,
+// are cut into gridDim.x equal contiguous ranges, one per CTA, so every CTA
+// streams the same number of stages whatever the tile count.  A range is
+// accumulated in pieces: the part of the range inside one tile is cut into
+// the fewest equal pieces of at most kMaxChain stages (FP32 rounding of the
+// TMEM chain); each piece's sums go to the workspace by atomics, and the
+// spectra and operand rings keep streaming across piece boundaries.
+// Launching tiles x ks CTAs reproduces the classic split-K cut (ks equal
+// stage ranges per tile).
+struct PieceCursor {
+	int u0, u1, Kst;
+	int pstart = 0, plen = 1, send = 0;  // current piece start and length, end of the run in this tile
+	// stage u of the range (called for u0, u0 + 1, ...): is it the first /
+	// last stage of its piece?
+	__device__ __forceinline__ void step(int u, bool &first, bool &last)
+	{
+		if(u == u0 || u % Kst == 0) {
+			const int tend = (u / Kst + 1) * Kst;
+			send = u1 < tend ? u1 : tend;
+			const int len = send - u;
+			const int np = (len + kMaxChain - 1) / kMaxChain;
+			plen = (len + np - 1) / np;
+			pstart = u;
+			first = true;
+		} else {
+			first = u - pstart == plen;
+			if(first)
+				pstart = u;
+		}
+		last = u + 1 == send || u + 1 - pstart == plen;
+	}
+};
+
 template <int NPART, int NFS, int NABS, int NBS>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_constant__ CUtensorMap tmF, const __grid_constant__ TcArgs a)
 {
@@ -131,15 +165,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	uint64_t *ab_empty = ab_full + NABS;     // X operand consumed by the MMAs
 	uint64_t *b_full = ab_empty + NABS;      // delay-table operand landed (bulk copy)
 	uint64_t *b_empty = b_full + NBS;       // delay-table operand consumed by the MMAs
-	uint64_t *acc_full = b_empty + NBS;
-	uint32_t *tslot = (uint32_t *) (acc_full + 1);
+	uint64_t *acc_full = b_empty + NBS;     // a piece's sums complete in TMEM
+	uint64_t *acc_empty = acc_full + 1;     // ... and read out by the epilogue warps
+	uint64_t *mma_done = acc_empty + 1;     // every MMA of the CTA retired
+	uint32_t *tslot = (uint32_t *) (mma_done + 1);
 	volatile int *abort_flag = (volatile int *) (tslot + 1);
 
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const int tile = blockIdx.x / a.ks, split = blockIdx.x % a.ks;
-	const int k_begin = (int) ((long long) a.Kst * split / a.ks);
-	const int k_end = (int) ((long long) a.Kst * (split + 1) / a.ks);
-	const int nst = k_end - k_begin;
+	const long long units = (long long) a.tiles * a.Kst;
+	const int u0 = (int) (units * blockIdx.x / gridDim.x);
+	const int u1 = (int) (units * (blockIdx.x + 1) / gridDim.x);
+	const int nst = u1 - u0;
 
 	if(threadIdx.x == 0) {
 		for(int i = 0; i < NFS; i++) {
@@ -155,6 +191,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			mbar_init(smem_u32(&b_empty[i]), 1);
 		}
 		mbar_init(smem_u32(acc_full), 1);
+		mbar_init(smem_u32(acc_empty), CONV_WARPS);
+		mbar_init(smem_u32(mma_done), 1);
 		*abort_flag = 0;
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
@@ -170,17 +208,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	if(warp == 0) {
 		// ---------------- producer: spectra only ----------------
 		// Runs NFS stages ahead of the converters, gated only by their
-		// release of the ring slot.
+		// release of the ring slot, across piece boundaries.
 		if(lane == 0) {
 			int issued = 0;
 			for(int it = 0; it < nst; it++) {
-				const int st = k_begin + it;
+				const int u = u0 + it;
 				const int fs = it % NFS;
 				const uint32_t fph = (it / NFS) & 1;
 				if(!mbar_wait(smem_u32(&f_empty[fs]), fph ^ 1, abort_flag, a.err, 1))
 					break;
 				mbar_arrive_tx(smem_u32(&f_full[fs]), f_stage);
-				tma_load_3d(smem_u32(sF + fs * f_stage), &tmF, smem_u32(&f_full[fs]), st * 2 * KB, tile * TM, 0);
+				tma_load_3d(smem_u32(sF + fs * f_stage), &tmF, smem_u32(&f_full[fs]), (u % a.Kst) * 2 * KB, (u / a.Kst) * TM, 0);
 				issued = it + 1;
 			}
 			// drain the loads that may still be in flight
@@ -196,11 +234,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 #pragma unroll
 			for(int i = 0; i < NPART; i++)
 				idesc[i] = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (((NPART - i) * a.npad) >> 3) << 17) | ((uint32_t) (TM >> 4) << 24);
+			PieceCursor pc{u0, u1, a.Kst};
+			int piece = 0;
 			for(int it = 0; it < nst; it++) {
+				bool first, last;
+				pc.step(u0 + it, first, last);
 				const int as = it % NABS;
 				const uint32_t aph = (it / NABS) & 1;
 				const int bs = it % NBS;
 				const uint32_t bph = (it / NBS) & 1;
+				// a new piece overwrites the accumulators: the epilogue warps
+				// must have read the previous piece out
+				if(first && piece > 0 && !mbar_wait(smem_u32(acc_empty), (piece - 1) & 1, abort_flag, a.err, 8))
+					break;
 				if(!mbar_wait(smem_u32(&ab_full[as]), aph, abort_flag, a.err, 3))
 					break;
 				if(!mbar_wait(smem_u32(&b_full[bs]), bph, abort_flag, a.err, 4))
@@ -213,12 +259,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 #pragma unroll
 					for(int i = 0; i < NPART; i++)
 						umma_bf16(d0 + (uint32_t) (i * a.npad), umma_desc(a0 + i * A_TILE, 128, 256), umma_desc(b0, 128, 256), idesc[i],
-							  (it > 0 || i > 0) ? 1u : 0u);
+							  (!first || i > 0) ? 1u : 0u);
 				}
 				umma_commit(smem_u32(&ab_empty[as]));
 				umma_commit(smem_u32(&b_empty[bs]));
+				if(last) {
+					umma_commit(smem_u32(acc_full));
+					piece++;
+				}
 			}
-			umma_commit(smem_u32(acc_full));
+			// nothing may still write TMEM when it is released
+			umma_commit(smem_u32(mma_done));
+			mbar_drain(smem_u32(mma_done), 0);
 		}
 	} else if(warp == TC_THREADS / 32 - 1) {
 		// ---------------- producer: delay-table operand ----------------
@@ -230,14 +282,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 				if(!mbar_wait(smem_u32(&b_empty[bs]), ((it / NBS) & 1) ^ 1, abort_flag, a.err, 2))
 					break;
 				mbar_arrive_tx(smem_u32(&b_full[bs]), ab_bytes);
-				bulk_g2s(smem_u32(sB + bs * ab_bytes), a.bops + (size_t) (k_begin + it) * ab_bytes, ab_bytes, smem_u32(&b_full[bs]));
+				bulk_g2s(smem_u32(sB + bs * ab_bytes), a.bops + (size_t) ((u0 + it) % a.Kst) * ab_bytes, ab_bytes, smem_u32(&b_full[bs]));
 				issued = it + 1;
 			}
 			for(int it = (issued > NBS ? issued - NBS : 0); it < issued; it++)
 				mbar_drain(smem_u32(&b_full[it % NBS]), (it / NBS) & 1);
 		}
 	} else {
-		// ---------------- converters, then epilogue ----------------
+		// ---------------- converters, and the epilogue of every piece ----------------
 		// CONV_WARPS warps, four per SM sub-partition: thread t handles tile
 		// row r = t % 128 and bin pair g = t / 128 (bins 2g, 2g+1 of the
 		// stage: half g % 2 of k-core-matrix g / 2 of the UMMA tile)
@@ -246,7 +298,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 		const int r = t & (TM - 1);
 		const int g = t >> 7;
 		const int roff = (r >> 3) * 256 + (r & 7) * 16 + (g >> 1) * 128 + (g & 1) * 8;
+		PieceCursor pc{u0, u1, a.Kst};
+		int piece = 0;
 		for(int it = 0; it < nst; it++) {
+			bool first, last;
+			pc.step(u0 + it, first, last);
 			const int fs = it % NFS;
 			const uint32_t fph = (it / NFS) & 1;
 			const bool okf = mbar_wait(smem_u32(&f_full[fs]), fph, abort_flag, a.err, 5);
@@ -297,17 +353,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			__syncwarp();
 			if(lane == 0)
 				mbar_arrive(smem_u32(&ab_full[as]));
-		}
-		// epilogue: TMEM -> registers -> FP32 atomics into the workspace.
-		// Warps w and w + 4 share TMEM lane quarter w % 4 and split the
-		// baselines between them.
-		const bool got = mbar_wait(smem_u32(acc_full), 0, abort_flag, a.err, 7);
-		tc_fence_after();
-		const bool ok = __all_sync(0xffffffffu, got && !*abort_flag && nst > 0);
-		if(ok) {
+			if(!last)
+				continue;
+			// epilogue of the piece: TMEM -> registers -> FP32 atomics into
+			// the workspace.  Warps w and w + 4 share TMEM lane quarter
+			// w % 4 and split the baselines between them.
+			const bool got = mbar_wait(smem_u32(acc_full), piece & 1, abort_flag, a.err, 7);
+			tc_fence_after();
+			if(!__all_sync(0xffffffffu, got))
+				break;
 			const int q = warp & 3;
-			const int row = q * 32 + lane;
-			const int s = tile * TM + row;
+			const int s = ((u0 + it) / a.Kst) * TM + q * 32 + lane;
 			for(int b = (warp - 2) >> 2; b < a.B; b += CONV_WARPS / 4) {
 				for(int c0 = 0; c0 < a.accstride; c0 += 16) {
 					uint32_t v[16], w[16];
@@ -331,6 +387,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 					}
 				}
 			}
+			tc_fence_before();
+			__syncwarp();
+			if(lane == 0)
+				mbar_arrive(smem_u32(acc_empty));
+			piece++;
 		}
 	}
 	tc_fence_before();
@@ -616,10 +677,13 @@ struct BatchPlan {
 	void *W = nullptr;         // [B][nq] complex T
 	short *lq = nullptr, *mq = nullptr;
 	unsigned *err = nullptr;
-	// tuned split per S, and the pipeline variant (ring depths) per S:
-	// 0 = the plan's default rings, 1 = a 3-deep spectrum ring with a
-	// 2-deep X-operand ring (more bytes in flight per SM)
+	// tuned or pinned split per S, the tcgen05 path's CTA count per S
+	// (its stage ranges need not align with tiles), and the pipeline
+	// variant (ring depths) per S: 0 = the plan's default rings, 1 = a
+	// 3-deep spectrum ring with a 2-deep X-operand ring (more bytes in
+	// flight per SM)
 	std::map<int, int> split;
+	std::map<int, int> ctas;
 	std::map<int, int> pipe;
 	int nf0 = NF, nab0 = 4;
 	// optional CUDA events recorded around the contraction kernel
@@ -655,7 +719,7 @@ static size_t tc_smem_bytes(const BatchPlan &P)
 	const size_t f = (size_t) P.nf * P.n_det * TM * 128;
 	const size_t aa = (size_t) P.nab * P.B * P.npart * A_TILE;
 	const size_t bb = (size_t) P.nb * P.B * P.npart * P.npad * KE * 2;
-	const size_t bars = 8 * (2 * P.nf + 2 * P.nab + 2 * P.nb + 1) + 16;
+	const size_t bars = 8 * (2 * P.nf + 2 * P.nab + 2 * P.nb + 3) + 16;
 	// 1 KB for aligning the base, 4 KB of slack past the last tile
 	return 1024 + f + aa + bb + bars + 4096;
 }
@@ -863,24 +927,40 @@ size_t batch_workspace_bytes(const void *pp, int S)
 	return (size_t) (S > 0 ? S : 0) * P->B * P->accstride * el;
 }
 
+static int sm_count()
+{
+	int sms = 148, dev = 0;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	return sms;
+}
+
+// CTAs of the tcgen05 contraction for S segments: the pinned or tuned
+// count, else one per SM with at least four stages each
+int batch_pick_ctas(const void *pp, int S)
+{
+	const BatchPlan *P = (const BatchPlan *) pp;
+	auto it = P->ctas.find(S);
+	if(it != P->ctas.end())
+		return it->second;
+	const long long units = (long long) ((S + TM - 1) / TM) * P->Kst;
+	long long g = units / 4;
+	g = g < sm_count() ? g : sm_count();
+	return g > 0 ? (int) g : 1;
+}
+
 int batch_pick_split(const void *pp, int S)
 {
 	const BatchPlan *P = (const BatchPlan *) pp;
 	auto it = P->split.find(S);
 	if(it != P->split.end())
 		return it->second;
-	int sms = 148;
-	int dev = 0;
-	cudaGetDevice(&dev);
-	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	const int sms = sm_count();
 	if(is_tc(P->precision)) {
+		// stages per CTA in units of a tile's stages, rounded
 		const int tiles = (S + TM - 1) / TM;
-		int ks = sms / tiles;
-		if(ks < 1)
-			ks = 1;
-		if(ks > P->Kst / 4)
-			ks = P->Kst / 4 > 0 ? P->Kst / 4 : 1;
-		return ks;
+		const int ks = (batch_pick_ctas(P, S) + tiles / 2) / tiles;
+		return ks > 0 ? ks : 1;
 	}
 	const int blocks = (S + CC_TS - 1) / CC_TS;
 	const int nch = (P->Ku + CC_KC - 1) / CC_KC;
@@ -895,10 +975,32 @@ int batch_pick_split(const void *pp, int S)
 int batch_set_split(void *pp, int S, int ks)
 {
 	BatchPlan *P = (BatchPlan *) pp;
-	if(ks <= 0)
+	if(ks <= 0) {
 		P->split.erase(S);
-	else
+		P->ctas.erase(S);
+	} else {
 		P->split[S] = ks;
+		P->ctas[S] = ((S + TM - 1) / TM) * ks;
+	}
+	return 0;
+}
+
+int batch_set_ctas(void *pp, int S, int ctas)
+{
+	BatchPlan *P = (BatchPlan *) pp;
+	if(!is_tc(P->precision)) {
+		set_error("batch_set_ctas: only the tcgen05 paths take a CTA count");
+		return -1;
+	}
+	if(ctas <= 0) {
+		P->ctas.erase(S);
+		P->split.erase(S);
+	} else {
+		const int tiles = (S + TM - 1) / TM;
+		const int ks = (ctas + tiles / 2) / tiles;
+		P->ctas[S] = ctas;
+		P->split[S] = ks > 0 ? ks : 1;
+	}
 	return 0;
 }
 
@@ -917,20 +1019,15 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 		set_error("batch_run: workspace of %zu bytes needed", batch_workspace_bytes(P, S));
 		return -1;
 	}
-	int ks = split > 0 ? split : batch_pick_split(P, S);
-	if(is_tc(P->precision)) {
-		// keep each CTA's TMEM accumulation chain short (FP32 rounding)
-		const int min_ks = (P->Kst + kMaxChain - 1) / kMaxChain;
-		ks = ks < min_ks ? min_ks : ks;
-	}
+	const int ks = split > 0 ? split : batch_pick_split(P, S);
 	int launches = 0;
 	if(is_tc(P->precision)) {
 		if(((uintptr_t) F & 15) || ((ld * 16) & 15)) {
 			set_error("batch_run: spectra must be 16-byte aligned");
 			return -1;
 		}
-		if(ks > P->Kst) {
-			set_error("batch_run: split %d above %d stages", ks, P->Kst);
+		if(split > P->Kst) {
+			set_error("batch_run: split %d above %d stages", split, P->Kst);
 			return -1;
 		}
 		if(P->tm_ptr != F || P->tm_S != S || P->tm_ld != ld) {
@@ -955,7 +1052,6 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 		a.n_det = P->n_det;
 		a.B = P->B;
 		a.Kst = P->Kst;
-		a.ks = ks;
 		a.npad = P->npad;
 		a.tmem_cols = P->tmem_cols;
 		a.accstride = P->accstride;
@@ -967,6 +1063,10 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 		a.acc = (float *) ws;
 		a.err = P->err;
 		const int tiles = (S + TM - 1) / TM;
+		a.tiles = tiles;
+		// CTAs: an explicit split-K factor ks cuts every tile's stages into
+		// ks ranges; otherwise the tuned or default count
+		const int ctas = split > 0 ? tiles * split : batch_pick_ctas(P, S);
 		// pipeline variant for this batch size (tuned), within the
 		// shared-memory budget
 		P->nf = P->nf0;
@@ -983,13 +1083,13 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 		if(P->ev_begin)
 			cudaEventRecord(P->ev_begin, st);
 		if(P->npart == 3)
-			k_tc_contract<3, NF, 2, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			k_tc_contract<3, NF, 2, 3><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		else if(P->nf == 3)
-			k_tc_contract<2, 3, 2, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			k_tc_contract<2, 3, 2, 3><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		else if(P->nab == 4)
-			k_tc_contract<2, NF, 4, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			k_tc_contract<2, NF, 4, 3><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		else
-			k_tc_contract<2, NF, 3, 3><<<tiles * ks, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			k_tc_contract<2, NF, 3, 3><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		if(P->ev_end)
 			cudaEventRecord(P->ev_end, st);
 		launches++;
@@ -1073,22 +1173,29 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 	return 0;
 }
 
-// Times every candidate split-K factor (3 launches each, CUDA events on the
-// caller's stream, after one warm-up) and keeps the fastest for S.
+// Times every candidate work split (3 launches each, CUDA events on the
+// caller's stream, after one warm-up) and keeps the fastest for S.  The
+// tcgen05 path's candidates are CTA counts: whole multiples of the SM count
+// (equal stage ranges across tile boundaries) and tiles x ks for split-K
+// factors ks (ranges aligned with tiles); the CUDA-core path's are split-K
+// factors.  Returns the split-K factor equivalent to the choice.
 int batch_autotune(void *pp, const void *F, int S, long long ld, void *sky, void *ws, size_t ws_bytes, void *stream_v)
 {
 	BatchPlan *P = (BatchPlan *) pp;
 	cudaStream_t st = (cudaStream_t) stream_v;
-	int sms = 148, dev = 0;
-	cudaGetDevice(&dev);
-	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	const int sms = sm_count();
+	const bool tc = is_tc(P->precision);
+	const int tiles = (S + TM - 1) / TM;
 	std::vector<int> cand;
-	if(is_tc(P->precision)) {
-		const int tiles = (S + TM - 1) / TM;
-		const int min_ks = (P->Kst + kMaxChain - 1) / kMaxChain;
-		for(int ks = min_ks; ks <= P->Kst / 2 && (tiles * ks <= 4 * sms || ks == min_ks); ks++)
-			if(ks <= min_ks + 8 || tiles * ks <= 2 * sms)
-				cand.push_back(ks);
+	if(tc) {
+		const long long units = (long long) tiles * P->Kst;
+		for(int k = 1; k <= 3; k++)
+			if((long long) k * sms <= units)
+				cand.push_back(k * sms);
+		for(int ks = 1; tiles * ks <= 2 * sms && ks <= P->Kst; ks++)
+			if(ks <= 12 || (ks % 4 == 0 && ks <= 32) || ks % 16 == 0)
+				if(std::find(cand.begin(), cand.end(), tiles * ks) == cand.end())
+					cand.push_back(tiles * ks);
 	} else {
 		const int nch = (P->Ku + CC_KC - 1) / CC_KC;
 		for(int ks = 1; ks <= nch && ks <= 64; ks *= 2)
@@ -1101,14 +1208,18 @@ int batch_autotune(void *pp, const void *F, int S, long long ld, void *sky, void
 	CKB(cudaEventCreate(&e1));
 	int best = cand[0], best_v = 0;
 	float best_ms = 1e30f;
-	const int n_var = (is_tc(P->precision) && P->npart == 2) ? 2 : 1;
+	const int n_var = (tc && P->npart == 2) ? 2 : 1;
 	for(int v = 0; v < n_var; v++)
-		for(int ks : cand) {
-			if(batch_run(P, F, S, ld, nullptr, sky, ws, ws_bytes, st, ks, nullptr, v))
+		for(int c : cand) {
+			// the tcgen05 candidates run through the plan's CTA count for S
+			if(tc)
+				P->ctas[S] = c;
+			const int arg = tc ? 0 : c;
+			if(batch_run(P, F, S, ld, nullptr, sky, ws, ws_bytes, st, arg, nullptr, v))
 				return -1;
 			CKB(cudaEventRecord(e0, st));
 			for(int r = 0; r < 3; r++)
-				if(batch_run(P, F, S, ld, nullptr, sky, ws, ws_bytes, st, ks, nullptr, v))
+				if(batch_run(P, F, S, ld, nullptr, sky, ws, ws_bytes, st, arg, nullptr, v))
 					return -1;
 			CKB(cudaEventRecord(e1, st));
 			CKB(cudaEventSynchronize(e1));
@@ -1116,15 +1227,20 @@ int batch_autotune(void *pp, const void *F, int S, long long ld, void *sky, void
 			CKB(cudaEventElapsedTime(&ms, e0, e1));
 			if(ms < best_ms) {
 				best_ms = ms;
-				best = ks;
+				best = c;
 				best_v = v;
 			}
 		}
 	cudaEventDestroy(e0);
 	cudaEventDestroy(e1);
-	P->split[S] = best;
+	if(tc) {
+		P->ctas[S] = best;
+		const int ks = (best + tiles / 2) / tiles;
+		P->split[S] = ks > 0 ? ks : 1;
+	} else
+		P->split[S] = best;
 	P->pipe[S] = best_v;
-	return best;
+	return P->split[S];
 }
 
 int batch_pipe_variant(const void *pp, int S)

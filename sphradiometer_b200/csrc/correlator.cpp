@@ -731,6 +731,8 @@ extern "C" int sphrad_batch_integrate_host(sphrad_batch_plan *p, const void *fse
 extern "C" int sphrad_batch_set_split(sphrad_batch_plan *p, int n_seg, int split) { return batch_set_split(p->impl, n_seg, split); }
 extern "C" int sphrad_batch_pipeline(const sphrad_batch_plan *p, int n_seg) { return batch_pipe_variant(p->impl, n_seg); }
 extern "C" int sphrad_batch_get_split(const sphrad_batch_plan *p, int n_seg) { return batch_pick_split(p->impl, n_seg); }
+extern "C" int sphrad_batch_get_ctas(const sphrad_batch_plan *p, int n_seg) { return batch_pick_ctas(p->impl, n_seg); }
+extern "C" int sphrad_batch_set_ctas(sphrad_batch_plan *p, int n_seg, int ctas) { return batch_set_ctas(p->impl, n_seg, ctas); }
 extern "C" int sphrad_batch_kernels_per_call(const sphrad_batch_plan *p) { return batch_last_kernel_count(p->impl); }
 
 extern "C" int sphrad_batch_autotune(sphrad_batch_plan *p, const void *fseries_dev, int n_seg, long long ld, void *sky_dev, void *workspace, size_t workspace_bytes,

@@ -99,6 +99,8 @@ int batch_run(void *plan, const void *F, int S, long long ld, const double *gmst
 int batch_pipe_variant(const void *plan, int S);
 int batch_run_host(void *plan, const void *F_host, int S, long long ld, const double *gmst_host, void *sky_host);
 int batch_pick_split(const void *plan, int S);
+int batch_pick_ctas(const void *plan, int S);  // CTAs of the tcgen05 contraction
+int batch_set_ctas(void *plan, int S, int ctas);  // 0 = back to the heuristic
 int batch_last_kernel_count(const void *plan);
 
 // ---- uneven batches (uneven.cu) -----------------------------------------

@@ -386,10 +386,10 @@ extern "C" int sphrad_uneven_autotune(sphrad_uneven_plan *p, const void *in, voi
 	for(Job &j : p->jobs) {
 		if(uneven_gather(j.S, (int) j.det.size(), j.Ku, j.ld, j.d_seg, p->d_in_off, j.det.data(), in, p->F, st))
 			return -1;
-		const int ks = sphrad_batch_autotune(j.bp, p->F, j.S, j.ld, p->sky, p->ws, p->ws_bytes, st);
-		if(ks < 0)
+		// the job's plan keeps the tuned work split for j.S
+		if(sphrad_batch_autotune(j.bp, p->F, j.S, j.ld, p->sky, p->ws, p->ws_bytes, st) < 0)
 			return -1;
-		j.split = ks;
+		j.split = 0;
 	}
 	drop_graph(p);
 	return 0;
