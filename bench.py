@@ -80,8 +80,7 @@ def partial_sum_rows(n_seg: int, n_stages: int, ctas: int, max_chain: int = 64) 
     units = tiles * n_stages
     rows = 0
     for c in range(ctas):
-        u0, u1 = units * c // ctas, units * (c + 1) // ctas
-        u = u0
+        u, u1 = units * c // ctas, units * (c + 1) // ctas
         while u < u1:
             t = u // n_stages
             end = min(u1, (t + 1) * n_stages)

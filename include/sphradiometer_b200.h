@@ -122,8 +122,14 @@ int sphrad_batch_autotune(sphrad_batch_plan *plan, const void *fseries, int n_se
 			  void *cuda_stream);
 /* Pipeline variant chosen by sphrad_batch_autotune for n_seg (tcgen05
  * paths): 0 = 2-deep spectrum ring with a 4-deep X-operand ring, 1 = 3-deep
- * spectrum ring with a 2-deep X-operand ring. */
+ * spectrum ring with a 2-deep X-operand ring, 2 = 4-deep spectrum ring with
+ * a 4-deep X-operand ring in tensor memory (bf16x3; a plan whose tensor
+ * memory or shared memory cannot hold it runs variant 0).  Variants give
+ * the same results up to the order of FP32 partial-sum atomics. */
 int sphrad_batch_pipeline(const sphrad_batch_plan *plan, int n_seg);
+/* Pins the variant for n_seg (-1 = back to the default); -1 for a variant
+ * above 2. */
+int sphrad_batch_set_pipeline(sphrad_batch_plan *plan, int n_seg, int variant);
 /* Kernels launched by the last integrate call. */
 int sphrad_batch_kernels_per_call(const sphrad_batch_plan *plan);
 /* Profiling hook: when set (cudaEvent_t handles, or NULL to clear), every

@@ -159,7 +159,8 @@ class BatchPlan:
         import torch
         assert F.is_cuda and F.dtype == torch.complex128 and F.dim() == 3 and F.stride(2) == 1
         n_det, n_seg, ld = F.shape
-        assert F.stride(1) == ld and F.stride(0) == n_seg * ld, "spectra must be contiguous [n_det][n_seg][ld]"
+        # the stride of a size-1 dimension carries no layout
+        assert (n_seg == 1 or F.stride(1) == ld) and (n_det == 1 or F.stride(0) == n_seg * ld), "spectra must be contiguous [n_det][n_seg][ld]"
         nq = (self.l_max + 1) ** 2
         if out is None:
             out = torch.empty((n_seg, nq), dtype=torch.complex128, device=F.device)
@@ -202,6 +203,15 @@ class BatchPlan:
 
     def set_split(self, n_seg: int, split: int):
         load().sphrad_batch_set_split(self._p, n_seg, split)
+
+    def pipeline(self, n_seg: int) -> int:
+        """Pipeline variant of the tcgen05 contraction for n_seg segments."""
+        return load().sphrad_batch_pipeline(self._p, n_seg)
+
+    def set_pipeline(self, n_seg: int, variant: int):
+        """Pin the pipeline variant for n_seg (-1 = default)."""
+        if load().sphrad_batch_set_pipeline(self._p, n_seg, variant) < 0:
+            raise SphradError("sphrad_batch_set_pipeline: " + last_error())
 
     def ctas(self, n_seg: int) -> int:
         """CTAs of the tcgen05 contraction for n_seg segments."""

@@ -157,6 +157,7 @@ SIGNATURES = {
     "sphrad_batch_autotune": (_i, [_vp, _vp, _i, _ll, _vp, _vp, _sz, _vp]),
     "sphrad_batch_kernels_per_call": (_i, [_vp]),
     "sphrad_batch_pipeline": (_i, [_vp, _i]),
+    "sphrad_batch_set_pipeline": (_i, [_vp, _i, _i]),
     "sphrad_batch_status": (_i, [_vp]),
     "sphrad_batch_set_timing_events": (_i, [_vp, _vp, _vp]),
     "sphrad_batch_integrate_noalloc": (_i, [_vp, _vp, _i, _ll, _vp, _vp, _vp]),

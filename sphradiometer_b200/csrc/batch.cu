@@ -74,8 +74,19 @@ constexpr int kMaxChain = 64;            // most pipeline stages one tcgen05 CTA
 // ------------------------------------------------------------------------
 // tcgen05 contraction
 // ------------------------------------------------------------------------
+struct EpArgs {
+	int S, B, Lp1, L, accstride, nq;
+	const short *lq;        // l of output index q
+	const short *mq;        // m of output index q
+	const void *W;          // [B][nq] complex T: weight / n * D_b^l_{0 m}
+	const double *gmst;     // [S] or NULL
+	const float *segw;      // [S][B] extra per-segment baseline factors, or NULL
+	double2 *sky;           // [S][nq]
+};
+
 struct TcArgs {
 	int S, n_det, B, Kst, tiles, npad, tmem_cols, accstride;
+	int acol;              // first TMEM column of the X-operand ring (X in tensor memory)
 	int bi[TC_MAXB], bj[TC_MAXB];
 	const uint8_t *bops;   // [Kst][B][NPART][npad * KE bf16], UMMA layout
 	float *acc;            // [S][B][accstride]
@@ -146,7 +157,7 @@ struct PieceCursor {
 	}
 };
 
-template <int NPART, int NFS, int NABS, int NBS>
+template <int NPART, int NFS, int NABS, int NBS, bool ATM>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_constant__ CUtensorMap tmF, const __grid_constant__ TcArgs a)
 {
 	extern __shared__ uint8_t smem_raw[];
@@ -157,7 +168,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	const int ab_bytes = a.B * NPART * btile;
 	uint8_t *sF = smem;
 	uint8_t *sA = sF + NFS * f_stage;
-	uint8_t *sB = sA + NABS * a.B * NPART * A_TILE;
+	uint8_t *sB = sA + (ATM ? 0 : NABS * a.B * NPART * A_TILE);
 	uint64_t *bars = (uint64_t *) (sB + NBS * ab_bytes);
 	uint64_t *f_full = bars;                // spectra landed (TMA)
 	uint64_t *f_empty = f_full + NFS;       // spectra read by the converters
@@ -254,12 +265,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 				tc_fence_after();
 				for(int b = 0; b < a.B; b++) {
 					const uint32_t d0 = tmem + (uint32_t) (b * NPART * a.npad);
-					const uint32_t a0 = smem_u32(sA + (as * a.B + b) * NPART * A_TILE);
 					const uint32_t b0 = smem_u32(sB + bs * ab_bytes + b * NPART * btile);
 #pragma unroll
-					for(int i = 0; i < NPART; i++)
-						umma_bf16(d0 + (uint32_t) (i * a.npad), umma_desc(a0 + i * A_TILE, 128, 256), umma_desc(b0, 128, 256), idesc[i],
-							  (!first || i > 0) ? 1u : 0u);
+					for(int i = 0; i < NPART; i++) {
+						const uint32_t acc_on = (!first || i > 0) ? 1u : 0u;
+						if constexpr(ATM) {
+							// X part i of baseline b: KE / 2 columns of the ring slot
+							const uint32_t a0 = tmem + (uint32_t) (a.acol + ((as * a.B + b) * NPART + i) * (KE / 2));
+							umma_bf16_tmem_a(d0 + (uint32_t) (i * a.npad), a0, umma_desc(b0, 128, 256), idesc[i], acc_on);
+						} else {
+							const uint32_t a0 = smem_u32(sA + ((as * a.B + b) * NPART + i) * A_TILE);
+							umma_bf16(d0 + (uint32_t) (i * a.npad), umma_desc(a0, 128, 256), umma_desc(b0, 128, 256), idesc[i], acc_on);
+						}
+					}
 				}
 				umma_commit(smem_u32(&ab_empty[as]));
 				umma_commit(smem_u32(&b_empty[bs]));
@@ -290,13 +308,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 		}
 	} else {
 		// ---------------- converters, and the epilogue of every piece ----------------
-		// CONV_WARPS warps, four per SM sub-partition: thread t handles tile
-		// row r = t % 128 and bin pair g = t / 128 (bins 2g, 2g+1 of the
-		// stage: half g % 2 of k-core-matrix g / 2 of the UMMA tile)
+		// CONV_WARPS warps, four per SM sub-partition: a thread handles tile
+		// row r = 32 (warp % 4) + lane (TMEM lane r, which warps w with
+		// w % 4 == r / 32 reach) and bin pair g = (warp - 2) / 4 (bins 2g,
+		// 2g+1 of the stage: half g % 2 of k-core-matrix g / 2 of the
+		// shared-memory UMMA tile, or columns 2g, 2g+1 of the TMEM one)
 		constexpr int BPT = KB / (CONV_WARPS / 4);  // bins per thread
-		const int t = threadIdx.x - 64;
-		const int r = t & (TM - 1);
-		const int g = t >> 7;
+		const int r = (warp & 3) * 32 + lane;
+		const int g = (warp - 2) >> 2;
 		const int roff = (r >> 3) * 256 + (r & 7) * 16 + (g >> 1) * 128 + (g & 1) * 8;
 		PieceCursor pc{u0, u1, a.Kst};
 		int piece = 0;
@@ -331,6 +350,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			const bool oke = mbar_wait(smem_u32(&ab_empty[as]), aph ^ 1, abort_flag, a.err, 6);
 			if(!__all_sync(0xffffffffu, oke))
 				break;
+			if constexpr(ATM)
+				tc_fence_after();  // the MMAs that read the slot have retired
 #pragma unroll
 			for(int b = 0; b < TC_MAXB3; b++) {
 				if(b >= a.B)
@@ -344,12 +365,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 					// X = fb * conj(fa)
 					split_pair<NPART>(fmaf(fb.x, fa.x, fb.y * fa.y), fmaf(fb.y, fa.x, -fb.x * fa.y), part[c]);
 				}
-				uint8_t *t0 = sA + (as * a.B + b) * NPART * A_TILE + roff;
+				if constexpr(ATM) {
+					const uint32_t t0 = tmem + ((uint32_t) ((warp & 3) * 32) << 16) + (uint32_t) (a.acol + (as * a.B + b) * NPART * (KE / 2) + 2 * g);
 #pragma unroll
-				for(int q = 0; q < NPART; q++)
-					*(uint2 *) (t0 + q * A_TILE) = make_uint2(part[0][q], part[1][q]);
+					for(int q = 0; q < NPART; q++)
+						tmem_st2(t0 + (uint32_t) (q * (KE / 2)), part[0][q], part[1][q]);
+				} else {
+					uint8_t *t0 = sA + (as * a.B + b) * NPART * A_TILE + roff;
+#pragma unroll
+					for(int q = 0; q < NPART; q++)
+						*(uint2 *) (t0 + q * A_TILE) = make_uint2(part[0][q], part[1][q]);
+				}
 			}
-			fence_proxy_async();
+			if constexpr(ATM) {
+				tmem_wait_st();
+				tc_fence_before();
+			} else
+				fence_proxy_async();
 			__syncwarp();
 			if(lane == 0)
 				mbar_arrive(smem_u32(&ab_full[as]));
@@ -521,15 +553,6 @@ __global__ void k_cc_contract(const __grid_constant__ CcArgs c)
 // ------------------------------------------------------------------------
 // epilogue: normalisation, rotation, network sum, z rotation
 // ------------------------------------------------------------------------
-struct EpArgs {
-	int S, B, Lp1, L, accstride, nq;
-	const short *lq;        // l of output index q
-	const short *mq;        // m of output index q
-	const void *W;          // [B][nq] complex T: weight / n * D_b^l_{0 m}
-	const double *gmst;     // [S] or NULL
-	const float *segw;      // [S][B] extra per-segment baseline factors, or NULL
-	double2 *sky;           // [S][nq]
-};
 
 template <class T>
 __global__ void k_epilogue(const __grid_constant__ EpArgs e, T *acc)
@@ -570,24 +593,28 @@ __global__ void k_epilogue(const __grid_constant__ EpArgs e, T *acc)
 }
 
 // The same epilogue for the FP32 paths with at most EB baselines: blocks
-// stay resident and loop over segments, every thread owns up to QMAX fixed
-// output coefficients (q = tid + k * blockDim) and keeps their weights and
-// (l, m) in registers, so the per-segment work is one shared row of partial
-// sums, one phase table and coalesced FP64 stores.
+// stay resident and loop over batches of EPG consecutive segments, every
+// thread owns up to QMAX fixed output coefficients (q = tid + k * blockDim)
+// and keeps their weights and (l, m) in registers.  Per batch the block
+// fetches the next batch's partial sums (stored [segment][l] as float4 over
+// the baselines, one shared-memory load per output) and phase tables
+// e^{-i m gmst} for m >= 0 (FP64 sincospi of m gmst / pi) into the other
+// buffer, re-zeroes the current batch's workspace rows and writes its
+// coefficients with coalesced FP64 stores: one barrier per batch, and the
+// index arithmetic of the fetch is fixed per thread.
 constexpr int EPI2_THREADS = 256;
 constexpr int EB = 3;
+constexpr int EPG = 4;
+constexpr int EPF = 4;  // partial sums fetched per thread per batch (EPG B (L+1) <= 1024)
 
 template <int QMAX>
-__global__ void __launch_bounds__(EPI2_THREADS) k_epilogue_f32(const __grid_constant__ EpArgs e, float *acc)
+__global__ void __launch_bounds__(EPI2_THREADS, QMAX <= 5 ? 3 : 2) k_epilogue_f32(const __grid_constant__ EpArgs e, float *acc)
 {
-	// two buffers of partial sums and of the segment's base phase
-	// e^{-i gmst}: the next segment's are fetched while the current one is
-	// written
 	extern __shared__ __align__(16) uint8_t ep_smem[];
-	double2 *sPh = (double2 *) ep_smem;              // [2L+1]
-	double2 *sBase = sPh + 2 * e.L + 1;              // [2]
-	float *sP = (float *) (sBase + 2);               // [2][B][Lp1]
-	const int nP = e.B * e.Lp1;
+	const int nph = e.L + 1;
+	const int rowf = e.B * e.accstride;                  // floats per workspace row
+	double2 *sPh = (double2 *) ep_smem;                  // [2][EPG][L+1]
+	float4 *sP = (float4 *) (sPh + 2 * EPG * nph);       // [2][EPG][L+1] over baselines
 	float2 w[QMAX][EB];
 	short ql[QMAX], qm[QMAX];
 	const float2 *W = (const float2 *) e.W;
@@ -601,61 +628,83 @@ __global__ void __launch_bounds__(EPI2_THREADS) k_epilogue_f32(const __grid_cons
 		for(int b = 0; b < EB; b++)
 			w[k][b] = (in && b < e.B) ? W[(size_t) b * e.nq + q] : make_float2(0.f, 0.f);
 	}
-	auto fetch = [&](int s, int buf) {
-		const float *row = acc + (size_t) s * e.B * e.accstride;
-		float *dst = sP + buf * nP;
-		for(int i = threadIdx.x; i < nP; i += blockDim.x) {
-			const int b = i / e.Lp1;
-			dst[i] = __ldcg(&row[b * e.accstride + i % e.Lp1]) * (e.segw ? e.segw[(size_t) s * e.B + b] : 1.f);
+	// this thread's share of a batch's partial sums: source offset from the
+	// batch's first workspace row, destination float in the buffer, segment
+	// g and baseline b (or -1)
+	int f_src[EPF], f_dst[EPF];
+	short f_g[EPF], f_b[EPF];
+	const int nfetch = EPG * e.B * e.Lp1;
+#pragma unroll
+	for(int k = 0; k < EPF; k++) {
+		const int i = threadIdx.x + k * EPI2_THREADS;
+		f_g[k] = -1;
+		f_b[k] = 0;
+		f_src[k] = f_dst[k] = 0;
+		if(i < nfetch) {
+			const int g = i / (e.B * e.Lp1), r = i - g * e.B * e.Lp1, b = r / e.Lp1, l = r - b * e.Lp1;
+			f_g[k] = (short) g;
+			f_b[k] = (short) b;
+			f_src[k] = g * rowf + b * e.accstride + l;
+			f_dst[k] = (g * nph + l) * 4 + b;
 		}
-		if(threadIdx.x == blockDim.x - 1) {
+	}
+	// phase entries of a batch: thread i < EPG (L+1) computes segment i / (L+1), m = i % (L+1)
+	const int ph_g = threadIdx.x / nph, ph_m = threadIdx.x - ph_g * nph;
+	const bool ph_on = threadIdx.x < EPG * nph;
+	const int nb = (e.S + EPG - 1) / EPG;
+	auto fetch = [&](int j, int buf) {
+		const int s0 = j * EPG;
+		const float *rows = acc + (size_t) s0 * rowf;
+		float *dP = (float *) (sP + buf * EPG * nph);
+#pragma unroll
+		for(int k = 0; k < EPF; k++)
+			if(f_g[k] >= 0 && s0 + f_g[k] < e.S)
+				dP[f_dst[k]] = __ldcg(rows + f_src[k]) * (e.segw ? e.segw[(size_t) (s0 + f_g[k]) * e.B + f_b[k]] : 1.f);
+		if(ph_on) {
 			double sn = 0.0, cs = 1.0;
-			if(e.gmst)
-				sincos(-e.gmst[s], &sn, &cs);
-			sBase[buf] = make_double2(cs, sn);
+			if(e.gmst && s0 + ph_g < e.S)
+				sincospi(-(double) ph_m * (e.gmst[s0 + ph_g] * (1.0 / M_PI)), &sn, &cs);
+			sPh[(buf * EPG + ph_g) * nph + ph_m] = make_double2(cs, sn);
 		}
 	};
 	int it = 0;
-	if((int) blockIdx.x < e.S)
+	if((int) blockIdx.x < nb)
 		fetch(blockIdx.x, 0);
-	for(int s = blockIdx.x; s < e.S; s += gridDim.x, it++) {
+	for(int j = blockIdx.x; j < nb; j += gridDim.x, it++) {
 		const int buf = it & 1;
-		__syncthreads();  // this segment's buffer is complete; the phase table is free
-		const int sn_ = s + gridDim.x;
-		if(sn_ < e.S)
-			fetch(sn_, buf ^ 1);
-		// e^{-i m gmst} = base^m by binary powers (|m| <= L), FP64
-		for(int m = (int) threadIdx.x - e.L; m <= e.L; m += blockDim.x) {
-			const double2 z = sBase[buf];
-			double2 r = make_double2(1.0, 0.0), pw = make_double2(z.x, m < 0 ? -z.y : z.y);
-			for(int k = m < 0 ? -m : m; k; k >>= 1) {
-				if(k & 1)
-					r = make_double2(r.x * pw.x - r.y * pw.y, r.x * pw.y + r.y * pw.x);
-				pw = make_double2(pw.x * pw.x - pw.y * pw.y, 2 * pw.x * pw.y);
-			}
-			sPh[m + e.L] = r;
-		}
+		__syncthreads();  // batch j's buffers are complete; the other pair is free
+		if(j + (int) gridDim.x < nb)
+			fetch(j + gridDim.x, buf ^ 1);
 		// leave the workspace zeroed for the next launch (read at the fetch)
-		float *row = acc + (size_t) s * e.B * e.accstride;
-		for(int i = threadIdx.x; i < e.B * e.accstride; i += blockDim.x)
-			row[i] = 0.f;
-		__syncthreads();  // phase table ready
-		const float *cP = sP + buf * nP;
-		double2 *out = e.sky + (size_t) s * e.nq;
+		const int s0 = j * EPG;
+		const int ns = e.S - s0 < EPG ? e.S - s0 : EPG;
+		float4 *rows = (float4 *) (acc + (size_t) s0 * rowf);
+		for(int i = threadIdx.x; i < ns * rowf / 4; i += blockDim.x)
+			rows[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+		for(int g = 0; g < ns; g++) {
+			const float4 *cP = sP + (buf * EPG + g) * nph;
+			const double2 *cPh = sPh + (buf * EPG + g) * nph;
+			double2 *out = e.sky + (size_t) (s0 + g) * e.nq;
 #pragma unroll
-		for(int k = 0; k < QMAX; k++) {
-			const int q = threadIdx.x + k * EPI2_THREADS;
-			if(q < e.nq) {
-				float re = 0.f, im = 0.f;
-#pragma unroll
-				for(int b = 0; b < EB; b++)
-					if(b < e.B) {
-						const float pv = cP[b * e.Lp1 + ql[k]];
-						re += w[k][b].x * pv;
-						im += w[k][b].y * pv;
+			for(int k = 0; k < QMAX; k++) {
+				const int q = threadIdx.x + k * EPI2_THREADS;
+				if(q < e.nq) {
+					const float4 pv = cP[ql[k]];
+					float re = w[k][0].x * pv.x, im = w[k][0].y * pv.x;
+					if(EB > 1) {
+						re = fmaf(w[k][1].x, pv.y, re);
+						im = fmaf(w[k][1].y, pv.y, im);
 					}
-				const double2 ph = sPh[qm[k] + e.L];
-				out[q] = make_double2((double) re * ph.x - (double) im * ph.y, (double) re * ph.y + (double) im * ph.x);
+					if(EB > 2) {
+						re = fmaf(w[k][2].x, pv.z, re);
+						im = fmaf(w[k][2].y, pv.z, im);
+					}
+					// e^{-i m gmst}: the table holds m >= 0, negative m is its conjugate
+					double2 ph = cPh[qm[k] < 0 ? -qm[k] : qm[k]];
+					if(qm[k] < 0)
+						ph.y = -ph.y;
+					out[q] = make_double2((double) re * ph.x - (double) im * ph.y, (double) re * ph.y + (double) im * ph.x);
+				}
 			}
 		}
 	}
@@ -681,7 +730,9 @@ struct BatchPlan {
 	// (its stage ranges need not align with tiles), and the pipeline
 	// variant (ring depths) per S: 0 = the plan's default rings, 1 = a
 	// 3-deep spectrum ring with a 2-deep X-operand ring (more bytes in
-	// flight per SM)
+	// flight per SM), 2 = a 4-deep spectrum ring with a 4-deep X-operand
+	// ring in tensor memory (shared memory holds spectra and delay-table
+	// operands only)
 	std::map<int, int> split;
 	std::map<int, int> ctas;
 	std::map<int, int> pipe;
@@ -714,10 +765,10 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode()
 
 static bool is_tc(int precision) { return precision == kPrecBF16x3 || precision == kPrecBF16x6; }
 
-static size_t tc_smem_bytes(const BatchPlan &P)
+static size_t tc_smem_bytes(const BatchPlan &P, bool x_in_tmem = false)
 {
 	const size_t f = (size_t) P.nf * P.n_det * TM * 128;
-	const size_t aa = (size_t) P.nab * P.B * P.npart * A_TILE;
+	const size_t aa = x_in_tmem ? 0 : (size_t) P.nab * P.B * P.npart * A_TILE;
 	const size_t bb = (size_t) P.nb * P.B * P.npart * P.npad * KE * 2;
 	const size_t bars = 8 * (2 * P.nf + 2 * P.nab + 2 * P.nb + 3) + 16;
 	// 1 KB for aligning the base, 4 KB of slack past the last tile
@@ -902,10 +953,11 @@ void *batch_plan_create(const BatchPlanDesc &d, int precision)
 				set_error("batch plan: shared-memory budget exceeded");
 				fail = true;
 			}
-			if(!fail && (cudaFuncSetAttribute(k_tc_contract<2, NF, 4, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
-				     cudaFuncSetAttribute(k_tc_contract<2, 3, 2, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
-				     cudaFuncSetAttribute(k_tc_contract<2, NF, 3, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
-				     cudaFuncSetAttribute(k_tc_contract<3, NF, 2, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess)) {
+			if(!fail && (cudaFuncSetAttribute(k_tc_contract<2, NF, 4, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
+				     cudaFuncSetAttribute(k_tc_contract<2, 3, 2, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
+				     cudaFuncSetAttribute(k_tc_contract<2, NF, 3, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
+				     cudaFuncSetAttribute(k_tc_contract<3, NF, 2, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
+				     cudaFuncSetAttribute(k_tc_contract<2, 4, 4, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess)) {
 				set_error("batch plan: cannot reserve %zu bytes of shared memory", tc_smem_bytes(*P));
 				fail = true;
 			}
@@ -1021,6 +1073,20 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 	}
 	const int ks = split > 0 ? split : batch_pick_split(P, S);
 	int launches = 0;
+	EpArgs e;
+	e.S = S;
+	e.B = P->B;
+	e.Lp1 = P->Lp1;
+	e.L = P->L;
+	e.accstride = P->accstride;
+	e.nq = P->nq;
+	e.lq = P->lq;
+	e.mq = P->mq;
+	e.W = P->W;
+	e.gmst = gmst;
+	e.segw = segw;
+	e.sky = (double2 *) sky;
+
 	if(is_tc(P->precision)) {
 		if(((uintptr_t) F & 15) || ((ld * 16) & 15)) {
 			set_error("batch_run: spectra must be 16-byte aligned");
@@ -1072,6 +1138,8 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 		P->nf = P->nf0;
 		P->nab = P->nab0;
 		const int variant = pipe_variant >= 0 ? pipe_variant : (P->pipe.count(S) ? P->pipe[S] : 0);
+		bool x_tmem = false;
+		a.acol = 0;
 		if(variant == 1 && P->npart == 2) {
 			P->nf = 3;
 			P->nab = 2;
@@ -1079,17 +1147,32 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 				P->nf = P->nf0;
 				P->nab = P->nab0;
 			}
+		} else if(variant == 2 && P->npart == 2) {
+			// X ring after the accumulators, within the 512 TMEM columns
+			const int acol = (P->npart * P->B * P->npad + 31) & ~31;
+			P->nf = 4;
+			P->nab = 4;
+			if(acol + P->nab * P->B * P->npart * (KE / 2) <= 512 && tc_smem_bytes(*P, true) <= 227 * 1024) {
+				x_tmem = true;
+				a.acol = acol;
+				a.tmem_cols = 512;
+			} else {
+				P->nf = P->nf0;
+				P->nab = P->nab0;
+			}
 		}
 		if(P->ev_begin)
 			cudaEventRecord(P->ev_begin, st);
-		if(P->npart == 3)
-			k_tc_contract<3, NF, 2, 3><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+		if(x_tmem)
+			k_tc_contract<2, 4, 4, 3, true><<<ctas, TC_THREADS, tc_smem_bytes(*P, true), st>>>(P->tm, a);
+		else if(P->npart == 3)
+			k_tc_contract<3, NF, 2, 3, false><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		else if(P->nf == 3)
-			k_tc_contract<2, 3, 2, 3><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			k_tc_contract<2, 3, 2, 3, false><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		else if(P->nab == 4)
-			k_tc_contract<2, NF, 4, 3><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			k_tc_contract<2, NF, 4, 3, false><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		else
-			k_tc_contract<2, NF, 3, 3><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			k_tc_contract<2, NF, 3, 3, false><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		if(P->ev_end)
 			cudaEventRecord(P->ev_end, st);
 		launches++;
@@ -1135,30 +1218,18 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 			cudaEventRecord(P->ev_end, st);
 		launches++;
 	}
-	EpArgs e;
-	e.S = S;
-	e.B = P->B;
-	e.Lp1 = P->Lp1;
-	e.L = P->L;
-	e.accstride = P->accstride;
-	e.nq = P->nq;
-	e.lq = P->lq;
-	e.mq = P->mq;
-	e.W = P->W;
-	e.gmst = gmst;
-	e.segw = segw;
-	e.sky = (double2 *) sky;
 	const size_t el = P->precision == kPrecFP64 ? sizeof(double) : sizeof(float);
 	const size_t esmem = (size_t) P->B * P->Lp1 * el + (2 * P->L + 1) * sizeof(double2);
 	const int qmax = (P->nq + EPI2_THREADS - 1) / EPI2_THREADS;
-	if(P->precision != kPrecFP64 && P->B <= EB && qmax <= 10) {
+	if(P->precision != kPrecFP64 && P->B <= EB && qmax <= 10 && EPG * P->B * P->Lp1 <= EPF * EPI2_THREADS && EPG * (P->L + 1) <= EPI2_THREADS) {
 		int sms = 148, dev = 0;
 		cudaGetDevice(&dev);
 		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-		// resident blocks only (4 per SM by registers at QMAX 5, 2 at 10)
-		const int per_sm = qmax <= 5 ? 4 : 2;
-		const int grid = S < per_sm * sms ? S : per_sm * sms;
-		const size_t esm2 = (size_t) (2 * P->L + 1 + 2) * sizeof(double2) + (size_t) 2 * P->B * P->Lp1 * sizeof(float);
+		// resident blocks only (3 per SM by registers at QMAX 5, 2 at 10)
+		const int per_sm = qmax <= 5 ? 3 : 2;
+		const int nbatch = (S + EPG - 1) / EPG;
+		const int grid = nbatch < per_sm * sms ? nbatch : per_sm * sms;
+		const size_t esm2 = (size_t) 2 * EPG * (P->L + 1) * (sizeof(double2) + sizeof(float4));
 		if(qmax <= 5)
 			k_epilogue_f32<5><<<grid, EPI2_THREADS, esm2, st>>>(e, (float *) ws);
 		else
@@ -1208,7 +1279,7 @@ int batch_autotune(void *pp, const void *F, int S, long long ld, void *sky, void
 	CKB(cudaEventCreate(&e1));
 	int best = cand[0], best_v = 0;
 	float best_ms = 1e30f;
-	const int n_var = (tc && P->npart == 2) ? 2 : 1;
+	const int n_var = (tc && P->npart == 2) ? 3 : 1;
 	for(int v = 0; v < n_var; v++)
 		for(int c : cand) {
 			// the tcgen05 candidates run through the plan's CTA count for S
@@ -1241,6 +1312,16 @@ int batch_autotune(void *pp, const void *F, int S, long long ld, void *sky, void
 		P->split[S] = best;
 	P->pipe[S] = best_v;
 	return P->split[S];
+}
+
+int batch_set_pipe_variant(void *pp, int S, int variant)
+{
+	BatchPlan *P = (BatchPlan *) pp;
+	if(variant < 0)
+		P->pipe.erase(S);
+	else
+		P->pipe[S] = variant;
+	return 0;
 }
 
 int batch_pipe_variant(const void *pp, int S)

@@ -21,6 +21,7 @@ namespace sphrad {
 const double *rotation_plan_flat_for(const struct sh_series_rotation_plan *plan, std::vector<dcplx> &scratch);
 int batch_set_split(void *plan, int S, int ks);
 int batch_pipe_variant(const void *plan, int S);
+int batch_set_pipe_variant(void *plan, int S, int variant);
 int batch_check_error(void *plan, unsigned *code);
 int batch_set_timing_events(void *plan, void *ev_begin, void *ev_end);
 int batch_run_noalloc(void *plan, const void *F, int S, long long ld, const double *gmst, void *sky, void *stream);
@@ -730,6 +731,14 @@ extern "C" int sphrad_batch_integrate_host(sphrad_batch_plan *p, const void *fse
 
 extern "C" int sphrad_batch_set_split(sphrad_batch_plan *p, int n_seg, int split) { return batch_set_split(p->impl, n_seg, split); }
 extern "C" int sphrad_batch_pipeline(const sphrad_batch_plan *p, int n_seg) { return batch_pipe_variant(p->impl, n_seg); }
+extern "C" int sphrad_batch_set_pipeline(sphrad_batch_plan *p, int n_seg, int variant)
+{
+	if(variant > 2) {
+		set_error("sphrad_batch_set_pipeline: variant %d is not 0, 1 or 2", variant);
+		return -1;
+	}
+	return batch_set_pipe_variant(p->impl, n_seg, variant);
+}
 extern "C" int sphrad_batch_get_split(const sphrad_batch_plan *p, int n_seg) { return batch_pick_split(p->impl, n_seg); }
 extern "C" int sphrad_batch_get_ctas(const sphrad_batch_plan *p, int n_seg) { return batch_pick_ctas(p->impl, n_seg); }
 extern "C" int sphrad_batch_set_ctas(sphrad_batch_plan *p, int n_seg, int ctas) { return batch_set_ctas(p->impl, n_seg, ctas); }

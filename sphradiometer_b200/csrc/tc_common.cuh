@@ -110,6 +110,26 @@ __device__ __forceinline__ void umma_bf16(uint32_t dtmem, uint64_t adesc, uint64
 		"l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
+// the same MMA with the A operand in tensor memory (K-major: row m in lane
+// m, bf16 elements k = 2c, 2c + 1 packed in column c, even k in the low half)
+__device__ __forceinline__ void umma_bf16_tmem_a(uint32_t dtmem, uint32_t atmem, uint64_t bdesc, uint32_t idesc, uint32_t accumulate)
+{
+	asm volatile(
+		"{\n\t.reg .pred p;\n\t"
+		"setp.ne.b32 p, %4, 0;\n\t"
+		"tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}" ::"r"(dtmem),
+		"r"(atmem), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+// two consecutive 32-bit columns of this thread's lane (warp w may store to
+// lanes 32 (w % 4) .. 32 (w % 4) + 31 only)
+__device__ __forceinline__ void tmem_st2(uint32_t taddr, uint32_t v0, uint32_t v1)
+{
+	asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1, %2};" ::"r"(taddr), "r"(v0), "r"(v1) : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
 __device__ __forceinline__ void umma_commit(uint32_t bar)
 {
 	asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");

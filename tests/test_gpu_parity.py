@@ -234,12 +234,13 @@ def test_batched_ragged_sizes_and_splits(lib, c1, prec):
     bp.close()
 
 
-@pytest.mark.parametrize("prec", ["bf16x3", "bf16x6"])
-def test_batched_work_ranges_across_tiles(lib, c1, prec):
+@pytest.mark.parametrize("prec,variant", [("bf16x3", 0), ("bf16x3", 1), ("bf16x3", 2), ("bf16x6", 0)])
+def test_batched_work_ranges_across_tiles(lib, c1, prec, variant):
     """CTA counts whose (tile, stage) ranges start and end inside tiles:
     one CTA for all 3 tiles (pieces cut at tile boundaries and every 64
     stages), counts that divide nothing, one stage per CTA, and more CTAs
-    than stages (idle CTAs)."""
+    than stages (idle CTAs), in every pipeline variant (2: X operand in
+    tensor memory)."""
     import torch
     bp = lib.BatchPlan(c1["net"], prec)
     S = 300
@@ -247,6 +248,8 @@ def test_batched_work_ranges_across_tiles(lib, c1, prec):
     F = torch.from_numpy(np.ascontiguousarray(c1["batch"]["F"][:, idx, :])).cuda()
     g = torch.from_numpy(c1["batch"]["gmst"][idx].copy()).cuda()
     units = 3 * ((c1["n"] // 2 + 1 + 7) // 8)
+    bp.set_pipeline(S, variant)
+    assert bp.pipeline(S) == variant
     for ctas in (1, 7, 148, units, units + 29):
         bp.set_ctas(S, ctas)
         assert bp.ctas(S) == ctas
@@ -254,6 +257,7 @@ def test_batched_work_ranges_across_tiles(lib, c1, prec):
         errs = [rel_l2(sky[s], c1["ref"][idx[s]]) for s in range(S)]
         assert max(errs) < TOLS[prec][1], (ctas, max(errs))
     bp.set_ctas(S, 0)
+    bp.set_pipeline(S, -1)
     assert bp.status() == 0
     bp.close()
 
