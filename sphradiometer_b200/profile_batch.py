@@ -20,6 +20,8 @@ def main():
     ap.add_argument("--precision", default="bf16x3")
     ap.add_argument("--split", type=int, default=0)
     ap.add_argument("--autotune", action="store_true", help="use the autotuned split-K and pipeline variant")
+    ap.add_argument("--ctas", type=int, default=0, help="pin the tcgen05 contraction's CTA count")
+    ap.add_argument("--pipeline", type=int, default=-1, help="pin the tcgen05 pipeline variant (0, 1, 2)")
     args = ap.parse_args()
     import torch
 
@@ -38,6 +40,10 @@ def main():
         bp.autotune(F)
     elif args.split:
         bp.set_split(args.segments, args.split)
+    if args.ctas:
+        bp.set_ctas(args.segments, args.ctas)
+    if args.pipeline >= 0:
+        bp.set_pipeline(args.segments, args.pipeline)
     out = bp.integrate(F, g)
     torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -47,7 +53,8 @@ def main():
     b.record()
     torch.cuda.synchronize()
     ms = a.elapsed_time(b) / args.calls
-    print(f"segments {args.segments} split {bp.split(args.segments)} variant {S.load().sphrad_batch_pipeline(bp._p, args.segments)} "
+    print(f"segments {args.segments} split {bp.split(args.segments)} ctas {bp.ctas(args.segments) if args.precision.startswith('bf16') else '-'} "
+          f"variant {bp.pipeline(args.segments)} "
           f"precision {args.precision}: {ms:.4f} ms/call, "
           f"{args.segments / ms * 1e3:.3e} maps/s, status {bp.status()}")
 
