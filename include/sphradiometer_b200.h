@@ -140,6 +140,42 @@ int sphrad_batch_set_timing_events(sphrad_batch_plan *plan, void *ev_begin, void
  * gave up (synchronises with the device). */
 int sphrad_batch_status(sphrad_batch_plan *plan);
 
+/* ---- time series to spectra ---------------------------------------------
+ *
+ * Replaces the FFTW step ahead of the correlator,
+ * correlator_tseries_to_fseries_plan / correlator_tseries_to_fseries
+ * (correlator.c:216-231: the unnormalised forward real-to-complex DFT
+ * X[k] = sum_t x[t] e^{-2 pi i k t / n}, upper half completed by Hermitian
+ * symmetry), together with the caller's whitening X[k] /= sqrt(S(k))
+ * (sphradiometer_demo.c:456-460).  FP64 on the GPU, n a power of two from
+ * 8 to 16384.  psd: n/2+1 one-sided values S(k) at frequencies k / (n dt),
+ * or NULL for no whitening; bins whose S(k) is not positive and finite are
+ * set to zero (the reference caller divides by sqrt(0) there).  A plan is
+ * freed with sphrad_fseries_plan_free where the reference frees its FFTW
+ * plan with fftw_destroy_plan. */
+typedef struct sphrad_fseries_plan sphrad_fseries_plan;
+sphrad_fseries_plan *sphrad_fseries_plan_new(int n, const double *psd);
+void sphrad_fseries_plan_free(sphrad_fseries_plan *plan);
+/* rows device time series (row r at tseries + r * ldt doubles; 16-byte
+ * aligned base, ldt even and >= n) -> rows device half spectra (double
+ * complex, row r at fseries + r * ldf elements, bins 0 .. n/2, ldf >=
+ * n/2 + 1): the layout sphrad_batch_integrate reads.  Asynchronous on
+ * cuda_stream (NULL = the legacy default stream). */
+int sphrad_tseries_to_fseries(sphrad_fseries_plan *plan, const double *tseries, int rows, long long ldt, void *fseries, long long ldf,
+			      void *cuda_stream);
+/* Host drop-in for correlator_tseries_to_fseries: n host samples -> the
+ * full n-element host spectrum (double complex), X[n-k] = conj X[k] as in
+ * correlator.c:228-229, whitened when the plan has a psd.  Synchronous. */
+int sphrad_tseries_to_fseries_host(sphrad_fseries_plan *plan, const double *tseries, void *fseries);
+/* Time series straight to skies: sphrad_tseries_to_fseries into the front
+ * of the workspace, then sphrad_batch_integrate on those spectra.
+ * tseries: device [n_det][n_seg][ldt] doubles; the plans must share n.
+ * No counterpart in the reference (a caller there runs the FFT, whitening
+ * and correlator per segment on the host). */
+size_t sphrad_batch_tseries_workspace_size(const sphrad_batch_plan *plan, int n_seg);
+int sphrad_batch_integrate_tseries(sphrad_batch_plan *plan, sphrad_fseries_plan *fseries_plan, const double *tseries, int n_seg, long long ldt,
+				   const double *gmst, void *sky, void *workspace, size_t workspace_bytes, void *cuda_stream);
+
 /* ---- uneven batches ------------------------------------------------------
  *
  * Segments of one detector network with different DFT lengths, output

@@ -172,6 +172,27 @@ class BatchPlan:
             raise SphradError("sphrad_batch_integrate: " + last_error())
         return out
 
+    def integrate_tseries(self, fplan: "FseriesPlan", x, gmst=None, out=None, stream=None):
+        """Skies from real time series: x a float64 CUDA tensor
+        [n_det][n_seg][ldt] (ldt even, >= n), transformed and whitened by
+        fplan on the GPU, then integrated (sphrad_batch_integrate_tseries)."""
+        import torch
+        assert x.is_cuda and x.dtype == torch.float64 and x.dim() == 3 and x.stride(2) == 1
+        n_det, n_seg, ldt = x.shape
+        assert (n_seg == 1 or x.stride(1) == ldt) and (n_det == 1 or x.stride(0) == n_seg * ldt), "time series must be contiguous [n_det][n_seg][ldt]"
+        nq = (self.l_max + 1) ** 2
+        if out is None:
+            out = torch.empty((n_seg, nq), dtype=torch.complex128, device=x.device)
+        need = load().sphrad_batch_tseries_workspace_size(self._p, n_seg)
+        if getattr(self, "_tws", None) is None or self._tws.numel() < need:
+            self._tws = torch.zeros(max(need, 16), dtype=torch.uint8, device="cuda")
+        st = stream if stream is not None else torch.cuda.current_stream()
+        rc = load().sphrad_batch_integrate_tseries(self._p, fplan._p, x.data_ptr(), n_seg, ldt, gmst.data_ptr() if gmst is not None else None,
+                                                   out.data_ptr(), self._tws.data_ptr(), self._tws.numel(), st.cuda_stream)
+        if rc:
+            raise SphradError("sphrad_batch_integrate_tseries: " + last_error())
+        return out
+
     def integrate_host(self, F_host: np.ndarray, gmst_host: np.ndarray | None = None, out: np.ndarray | None = None):
         n_det, n_seg, ld = F_host.shape
         assert F_host.flags.c_contiguous and F_host.dtype == np.complex128
@@ -242,6 +263,47 @@ class BatchPlan:
 
 GRID_GL = 0
 GRID_CELL = 1
+
+
+class FseriesPlan:
+    """Real time series to (whitened) half spectra on the GPU
+    (sphrad_fseries_plan_*, sphrad_tseries_to_fseries)."""
+
+    def __init__(self, n: int, psd: np.ndarray | None = None):
+        self.n = int(n)
+        self._psd = None if psd is None else np.ascontiguousarray(psd, dtype=np.float64)
+        if self._psd is not None:
+            assert self._psd.shape == (self.n // 2 + 1,)
+        ptr = self._psd.ctypes.data if self._psd is not None else None
+        self._p = _check(load().sphrad_fseries_plan_new(self.n, ptr), "sphrad_fseries_plan_new")
+
+    def transform(self, x, out=None, stream=None):
+        """x: float64 CUDA tensor [..., n] (rows contiguous); returns
+        complex128 [..., n/2 + 1]."""
+        import torch
+        assert x.is_cuda and x.dtype == torch.float64 and x.shape[-1] == self.n and x.is_contiguous()
+        rows = x.numel() // self.n
+        if out is None:
+            out = torch.empty(tuple(x.shape[:-1]) + (self.n // 2 + 1,), dtype=torch.complex128, device=x.device)
+        st = stream if stream is not None else torch.cuda.current_stream()
+        if load().sphrad_tseries_to_fseries(self._p, x.data_ptr(), rows, self.n, out.data_ptr(), self.n // 2 + 1, st.cuda_stream):
+            raise SphradError("sphrad_tseries_to_fseries: " + last_error())
+        return out
+
+    def transform_host(self, x: np.ndarray) -> np.ndarray:
+        """One host series -> the full n-bin spectrum (drop-in for
+        correlator_tseries_to_fseries)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        assert x.shape == (self.n,)
+        out = np.empty(self.n, dtype=np.complex128)
+        if load().sphrad_tseries_to_fseries_host(self._p, x.ctypes.data, out.ctypes.data):
+            raise SphradError("sphrad_tseries_to_fseries_host: " + last_error())
+        return out
+
+    def close(self):
+        if self._p:
+            load().sphrad_fseries_plan_free(self._p)
+            self._p = None
 
 
 class SkyGrid:

@@ -158,6 +158,13 @@ SIGNATURES = {
     "sphrad_batch_kernels_per_call": (_i, [_vp]),
     "sphrad_batch_pipeline": (_i, [_vp, _i]),
     "sphrad_batch_set_pipeline": (_i, [_vp, _i, _i]),
+    # time series to spectra
+    "sphrad_fseries_plan_new": (_vp, [_i, _vp]),
+    "sphrad_fseries_plan_free": (None, [_vp]),
+    "sphrad_tseries_to_fseries": (_i, [_vp, _vp, _i, _ll, _vp, _ll, _vp]),
+    "sphrad_tseries_to_fseries_host": (_i, [_vp, _vp, _vp]),
+    "sphrad_batch_tseries_workspace_size": (_sz, [_vp, _i]),
+    "sphrad_batch_integrate_tseries": (_i, [_vp, _vp, _vp, _i, _ll, _vp, _vp, _vp, _sz, _vp]),
     "sphrad_batch_status": (_i, [_vp]),
     "sphrad_batch_set_timing_events": (_i, [_vp, _vp, _vp]),
     "sphrad_batch_integrate_noalloc": (_i, [_vp, _vp, _i, _ll, _vp, _vp, _vp]),

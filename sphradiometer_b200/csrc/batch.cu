@@ -794,6 +794,8 @@ void batch_plan_destroy(void *pp)
 }
 
 unsigned batch_plan_l_max(const void *p) { return ((const BatchPlan *) p)->L; }
+int batch_plan_n_det(const void *p) { return ((const BatchPlan *) p)->n_det; }
+int batch_plan_n(const void *p) { return ((const BatchPlan *) p)->n; }
 int batch_plan_bins(const void *p) { return ((const BatchPlan *) p)->Ku; }
 int batch_last_kernel_count(const void *p) { return ((const BatchPlan *) p)->last_kernels; }
 

@@ -8,6 +8,8 @@
 #include <sphradiometer/correlator.h>
 #include <sphradiometer_b200.h>
 
+#include <cuda_runtime_api.h>
+
 #include <cmath>
 #include <map>
 #include <mutex>
@@ -753,6 +755,80 @@ extern "C" int sphrad_batch_autotune(sphrad_batch_plan *p, const void *fseries_d
 extern "C" int sphrad_batch_integrate_noalloc(sphrad_batch_plan *p, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky, void *stream)
 {
 	return batch_run_noalloc(p->impl, fseries, n_seg, ld, gmst, sky, stream);
+}
+
+// ------------------------------------------------------------------------
+// time series to spectra (correlator.c:216-231) and whitening
+// ------------------------------------------------------------------------
+struct sphrad_fseries_plan {
+	void *impl;
+};
+
+extern "C" sphrad_fseries_plan *sphrad_fseries_plan_new(int n, const double *psd)
+{
+	void *impl = fseries_plan_create(n, psd);
+	if(!impl)
+		return NULL;
+	sphrad_fseries_plan *p = (sphrad_fseries_plan *) malloc(sizeof(*p));
+	if(!p) {
+		fseries_plan_destroy(impl);
+		return NULL;
+	}
+	p->impl = impl;
+	return p;
+}
+
+extern "C" void sphrad_fseries_plan_free(sphrad_fseries_plan *p)
+{
+	if(p)
+		fseries_plan_destroy(p->impl);
+	free(p);
+}
+
+extern "C" int sphrad_tseries_to_fseries(sphrad_fseries_plan *p, const double *tseries, int rows, long long ldt, void *fseries, long long ldf, void *stream)
+{
+	return fseries_run(p->impl, tseries, rows, ldt, fseries, ldf, stream ? stream : (void *) cudaStreamLegacy);
+}
+
+extern "C" int sphrad_tseries_to_fseries_host(sphrad_fseries_plan *p, const double *tseries, void *fseries)
+{
+	if(!tseries || !fseries) {
+		set_error("sphrad_tseries_to_fseries_host: NULL series");
+		return -1;
+	}
+	return fseries_run_host(p->impl, tseries, (double *) fseries);
+}
+
+static size_t align256(size_t b) { return (b + 255) & ~(size_t) 255; }
+
+extern "C" size_t sphrad_batch_tseries_workspace_size(const sphrad_batch_plan *p, int n_seg)
+{
+	if(n_seg <= 0)
+		return 0;
+	const size_t spectra = (size_t) batch_plan_n_det(p->impl) * n_seg * batch_plan_bins(p->impl) * 16;
+	return align256(spectra) + batch_workspace_bytes(p->impl, n_seg);
+}
+
+extern "C" int sphrad_batch_integrate_tseries(sphrad_batch_plan *p, sphrad_fseries_plan *fp, const double *tseries, int n_seg, long long ldt, const double *gmst,
+					      void *sky, void *workspace, size_t workspace_bytes, void *stream)
+{
+	if(n_seg <= 0)
+		return 0;
+	if(fseries_plan_n(fp->impl) != batch_plan_n(p->impl)) {
+		set_error("sphrad_batch_integrate_tseries: spectrum plan n = %d, integration plan n = %d", fseries_plan_n(fp->impl), batch_plan_n(p->impl));
+		return -1;
+	}
+	const size_t need = sphrad_batch_tseries_workspace_size(p, n_seg);
+	if(!workspace || workspace_bytes < need) {
+		set_error("sphrad_batch_integrate_tseries: workspace of %zu bytes needed", need);
+		return -1;
+	}
+	void *st = stream ? stream : (void *) cudaStreamLegacy;
+	const int n_det = batch_plan_n_det(p->impl), ku = batch_plan_bins(p->impl);
+	const size_t spectra = (size_t) n_det * n_seg * ku * 16;
+	if(fseries_run(fp->impl, tseries, n_det * n_seg, ldt, workspace, ku, st))
+		return -1;
+	return batch_run(p->impl, workspace, n_seg, ku, gmst, sky, (char *) workspace + align256(spectra), workspace_bytes - align256(spectra), st, 0);
 }
 
 extern "C" int sphrad_batch_set_timing_events(sphrad_batch_plan *p, void *ev_begin, void *ev_end)

@@ -103,6 +103,22 @@ int batch_pick_ctas(const void *plan, int S);  // CTAs of the tcgen05 contractio
 int batch_set_ctas(void *plan, int S, int ctas);  // 0 = back to the heuristic
 int batch_last_kernel_count(const void *plan);
 
+int batch_plan_n_det(const void *plan);
+int batch_plan_n(const void *plan);  // DFT length of a segment
+
+// ---- time series to half spectra (fseries.cu) --------------------------
+// n a power of two, 8 .. 16384; psd: n/2+1 one-sided values (whitening
+// X[k] /= sqrt(psd[k]); non-positive or non-finite bins are zeroed) or NULL
+void *fseries_plan_create(int n, const double *psd);
+void fseries_plan_destroy(void *plan);
+int fseries_plan_n(const void *plan);
+// rows device series (row r at ts + r ldt doubles, 16-byte aligned, ldt
+// even) -> device half spectra (row r at out + r ldf complex, n/2+1 bins)
+int fseries_run(void *plan, const double *ts, int rows, long long ldt, void *out, long long ldf, void *stream);
+// one host series -> the full n-bin host spectrum (upper half by Hermitian
+// symmetry); synchronous
+int fseries_run_host(void *plan, const double *ts_host, double *fs_host);
+
 // ---- uneven batches (uneven.cu) -----------------------------------------
 // F[d][i][k] = in[in_off[seg[i]] + det[d] Ku + k] for a job of S segments
 // of n_sub detectors (device pointers; stream a cudaStream_t)

@@ -193,6 +193,26 @@ def make_batch(positions, n: int, dt: float, n_seg: int, seed: int, snr_range=(6
     return dict(F=F, theta=theta, phi=phi, snr=snr, gmst=gmst)
 
 
+def make_tseries_batch(positions, n: int, dt: float, n_seg: int, seed: int, snr_range=(6.0, 30.0)):
+    """The batch of ``make_batch`` as raw detector time series: coloured
+    noise plus the delayed chirp, before any whitening.  Returns a dict
+    with ``x`` (n_det x n_seg x n float64), ``psd`` (the one-sided S(k) at
+    k / (n dt), k <= n/2, zero outside the 20-1000 Hz band), ``F`` (the
+    whitened half spectra rfft(x) / sqrt(S), zero out of band) and ``gmst``."""
+    b = make_batch(positions, n, dt, n_seg, seed, snr_range)
+    K = n // 2 + 1
+    S = psd(np.arange(K) / (n * dt))
+    inband = S > 0
+    wh = np.zeros_like(S)
+    wh[inband] = 1.0 / np.sqrt(S[inband])
+    # undo the whitening in band; out of band the raw series carries no power
+    U = np.zeros_like(b["F"])
+    U[..., inband] = b["F"][..., inband] / wh[inband]
+    x = np.fft.irfft(U, n, axis=-1)
+    F = np.fft.rfft(x, axis=-1) * wh
+    return dict(x=np.ascontiguousarray(x), psd=np.where(inband, S, 0.0), F=F, gmst=b["gmst"])
+
+
 def full_from_half(half, n: int) -> np.ndarray:
     """Hermitian completion of n/2+1 bins to n bins (last axis)."""
     half = np.asarray(half)
