@@ -333,6 +333,52 @@ def sky_stage_rates(S, sky, reps: int = 5):
     return {"render_64x128_fp32_maps_per_s": render, "localise_maps_per_s": peaks}
 
 
+def tseries_report(S, n_seg: int, reps: int = 10):
+    """c1 from raw time series (the FFT + whitening ahead of the
+    correlator): the transform kernel alone, with its algorithmic bytes
+    n_det n_seg (8 n + 16 (n/2 + 1)) per launch against the measured HBM
+    peak, and time series -> skies (transform + contraction + epilogue).
+    512 distinct generated segments are tiled to n_seg (inputs above L2)."""
+    import torch
+    from sphradiometer_b200 import workload as W
+    pos = positions()
+    n, K = N_SAMPLES, N_SAMPLES // 2 + 1
+    b = W.make_tseries_batch(pos, n, DT, 512, seed=5)
+    idx = np.arange(n_seg) % 512
+    x = torch.from_numpy(np.ascontiguousarray(b["x"][:, idx, :])).cuda()
+    g = torch.from_numpy(b["gmst"][idx].copy()).cuda()
+    net = S.Network(pos, n, DT, l_max=L_MAX)
+    bp = S.BatchPlan(net, "bf16x3")
+    fp = S.FseriesPlan(n, b["psd"])
+    spectra = fp.transform(x)
+    bp.autotune(spectra)
+    sky = bp.integrate_tseries(fp, x, g)
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(reps):
+        fp.transform(x, out=spectra)
+    e.record(st)
+    torch.cuda.synchronize()
+    t_fft = a.elapsed_time(e) / reps / 1e3
+    a.record(st)
+    for _ in range(reps):
+        bp.integrate_tseries(fp, x, g, out=sky)
+    e.record(st)
+    torch.cuda.synchronize()
+    t_all = a.elapsed_time(e) / reps / 1e3
+    peak, kind = measured_peaks()
+    fft_bytes = N_DET * n_seg * (8 * n + 16 * K)
+    out = {"segments": n_seg, "fft_whiten_ms": t_fft * 1e3, "fft_whiten_GBps": fft_bytes / t_fft / 1e9,
+           "fft_whiten_frac_of_hbm_peak": fft_bytes / t_fft / 1e9 / peak, "tseries_to_sky_maps_per_s": n_seg / t_all,
+           "status": bp.status()}
+    fp.close()
+    bp.close()
+    net.close()
+    return out
+
+
 def c2_report(S, steps: int = 10):
     """Uneven batches: 4096 segments of a 4-detector network, durations
     log-uniform in 0.25-4 s at 4096 Hz (DFT lengths 1024-16384), l_max from
@@ -653,6 +699,7 @@ def run(args):
         extra["accuracy"] = accuracy_report(S, net, base, min(32, base["F"].shape[1]), pos)
         extra["c0"] = c0_report(S)
         extra.update(sky_stage_rates(S, out))
+        extra["c1_from_time_series"] = guarded(tseries_report, S, n_seg)
         if not args.quick:
             extra["c2_uneven"] = guarded(c2_report, S)
             extra["c3_sh_algebra"] = guarded(c3_report, S)

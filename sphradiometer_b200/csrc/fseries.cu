@@ -14,7 +14,10 @@
 // for k = 0 .. N, the whitening factor, and a coalesced store of the n/2+1
 // bins in the layout the batched integrator reads.  The shared buffer is
 // padded by one 16-byte slot per 8 points so that the strided butterfly
-// accesses of every pass are free of bank conflicts.
+// accesses of every pass are free of bank conflicts.  Every twiddle factor
+// of the passes and of the split is a power of e^{-2 pi i / n}: a thread
+// reads its base power from a table of the n powers (built on the host in
+// FP64) and forms the others by complex multiplication (a few roundings).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -85,11 +88,12 @@ __device__ __forceinline__ void dft_small(double2 *v)
 
 // One Stockham pass of radix R over the N padded points in s; Ns is the
 // product of the earlier radices.  Group j (< N / R) reads points
-// j + r N/R, multiplies point r by e^{-2 pi i r (j mod Ns) / (Ns R)}, takes
-// the R-point DFT and writes point r to (j - j mod Ns) R + j mod Ns + r Ns.
+// j + r N/R, multiplies point r by w^r, w = e^{-2 pi i (j mod Ns) / (Ns R)}
+// = tw[(j mod Ns) n / (Ns R)] (tw[m] = e^{-2 pi i m / n}), takes the R-point
+// DFT and writes point r to (j - j mod Ns) R + j mod Ns + r Ns.
 // G groups per thread at most; every group is read before any is written.
 template <int R, int G>
-__device__ __forceinline__ void stockham_pass(double2 *s, int N, int Ns)
+__device__ __forceinline__ void stockham_pass(double2 *s, int N, int Ns, const double2 *__restrict__ tw, int n)
 {
 	const int groups = N / R;
 	double2 v[G][R];
@@ -108,14 +112,13 @@ __device__ __forceinline__ void stockham_pass(double2 *s, int N, int Ns)
 		if(j < groups) {
 			const int k = j & (Ns - 1);
 			if(k) {
-				double sn, cs;
-				sincospi(-2.0 * k / ((double) Ns * R), &sn, &cs);
-				const double2 w = make_double2(cs, sn);
+				const double2 w = __ldg(tw + k * (n / (Ns * R)));
 				double2 p = w;
 #pragma unroll
 				for(int r = 1; r < R; r++) {
 					v[gi][r] = cmul(v[gi][r], p);
-					p = cmul(p, w);
+					if(r + 1 < R)
+						p = cmul(p, w);
 				}
 			}
 			dft_small<R>(v[gi]);
@@ -128,7 +131,8 @@ __device__ __forceinline__ void stockham_pass(double2 *s, int N, int Ns)
 	__syncthreads();
 }
 
-__global__ void __launch_bounds__(1024) k_rfft_whiten(const double *ts, long long ldt, int n, const double *wk, double2 *out, long long ldf)
+__global__ void __launch_bounds__(1024) k_rfft_whiten(const double *ts, long long ldt, int n, const double2 *__restrict__ tw, const double *wk, double2 *out,
+						   long long ldf)
 {
 	extern __shared__ double2 s_fft[];
 	const int N = n >> 1;
@@ -138,24 +142,26 @@ __global__ void __launch_bounds__(1024) k_rfft_whiten(const double *ts, long lon
 	__syncthreads();
 	int Ns = 1, rem = N;
 	while(rem >= 8) {
-		stockham_pass<8, 1>(s_fft, N, Ns);
+		stockham_pass<8, 1>(s_fft, N, Ns, tw, n);
 		Ns *= 8;
 		rem >>= 3;
 	}
 	if(rem == 4)
-		stockham_pass<4, 2>(s_fft, N, Ns);
+		stockham_pass<4, 2>(s_fft, N, Ns, tw, n);
 	else if(rem == 2)
-		stockham_pass<2, 4>(s_fft, N, Ns);
+		stockham_pass<2, 4>(s_fft, N, Ns, tw, n);
 	double2 *dst = out + (size_t) blockIdx.x * ldf;
-	for(int k = threadIdx.x; k <= N; k += blockDim.x) {
+	// e^{-2 pi i k / n} for this thread's k = tid, tid + blockDim, ...
+	// (indices reduced below n: a block can be wider than n for small n)
+	const double2 wstep = __ldg(tw + (blockDim.x & (n - 1)));
+	double2 wk_ = (int) threadIdx.x <= N ? __ldg(tw + threadIdx.x) : make_double2(1.0, 0.0);
+	for(int k = threadIdx.x; k <= N; k += blockDim.x, wk_ = cmul(wk_, wstep)) {
 		const double2 zk = s_fft[pad8(k & (N - 1))];
 		const double2 zc = s_fft[pad8((N - k) & (N - 1))];
 		// E = (Z[k] + conj Z[N-k]) / 2, O = (Z[k] - conj Z[N-k]) / 2i
 		const double2 E = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y - zc.y));
 		const double2 O = make_double2(0.5 * (zk.y + zc.y), -0.5 * (zk.x - zc.x));
-		double sn, cs;
-		sincospi(-2.0 * k / n, &sn, &cs);
-		double2 X = cadd(E, cmul(make_double2(cs, sn), O));
+		double2 X = cadd(E, cmul(wk_, O));
 		if(wk) {
 			const double f = wk[k];
 			X = make_double2(f * X.x, f * X.y);
@@ -167,6 +173,7 @@ __global__ void __launch_bounds__(1024) k_rfft_whiten(const double *ts, long lon
 struct FseriesPlan {
 	int n = 0;
 	double *wk = nullptr;  // device whitening factors [n/2+1], or NULL
+	double2 *tw = nullptr;  // device twiddles e^{-2 pi i m / n}, m < n
 	double *hbuf = nullptr;  // device buffer of the host entry point: n doubles + (n/2+1) complex
 };
 
@@ -183,7 +190,28 @@ void *fseries_plan_create(int n, const double *psd)
 	FseriesPlan *P = new FseriesPlan();
 	P->n = n;
 	bool fail = false;
-	if(psd) {
+	{
+		// FP64 powers of e^{-2 pi i / n}; exact at the quarter turns
+		std::vector<double> t(2 * (size_t) n);
+		for(int m = 0; m < n; m++) {
+			double c, s;
+			if(4 * m % n == 0) {
+				const int q = 4 * m / n;
+				c = q == 0 ? 1.0 : (q == 2 ? -1.0 : 0.0);
+				s = q == 1 ? -1.0 : (q == 3 ? 1.0 : 0.0);
+			} else {
+				const double a = -2.0 * M_PI * m / n;
+				c = std::cos(a);
+				s = std::sin(a);
+			}
+			t[2 * m] = c;
+			t[2 * m + 1] = s;
+		}
+		P->tw = (double2 *) dmalloc(t.size() * sizeof(double));
+		if(!P->tw || h2d(P->tw, t.data(), t.size() * sizeof(double)) || stream_sync())
+			fail = true;
+	}
+	if(!fail && psd) {
 		// 1 / sqrt(S(k)); bins whose S is not positive and finite are zeroed
 		std::vector<double> w(n / 2 + 1);
 		for(int k = 0; k <= n / 2; k++)
@@ -209,6 +237,7 @@ void fseries_plan_destroy(void *p)
 	if(!P)
 		return;
 	dfree(P->wk);
+	dfree(P->tw);
 	dfree(P->hbuf);
 	delete P;
 }
@@ -232,7 +261,7 @@ int fseries_run(void *p, const double *ts, int rows, long long ldt, void *out, l
 	int threads = N / 8;
 	threads = threads < 32 ? 32 : (threads > 1024 ? 1024 : threads);
 	const size_t smem = (size_t) (N + N / 8) * sizeof(double2);
-	k_rfft_whiten<<<rows, threads, smem, (cudaStream_t) stream>>>(ts, ldt, n, P->wk, (double2 *) out, ldf);
+	k_rfft_whiten<<<rows, threads, smem, (cudaStream_t) stream>>>(ts, ldt, n, P->tw, P->wk, (double2 *) out, ldf);
 	const cudaError_t e = cudaGetLastError();
 	if(e != cudaSuccess) {
 		set_error("tseries to fseries: launch failed (%s)", cudaGetErrorString(e));

@@ -46,6 +46,27 @@ void *get_plan(unsigned L, int kind, int nt, int nphi, int fp32)
 	return p;
 }
 
+// Grow-only device scratch of the batched extremizer, one set per device:
+// a call holds the lock until its work on the stream has finished, so the
+// buffers are reused without a device allocation per call
+struct ExtremumScratch {
+	std::mutex mu;
+	std::map<int, std::vector<std::pair<void *, size_t>>> bufs;  // device -> buffers
+};
+ExtremumScratch g_ext;
+
+void *ext_buffer(std::vector<std::pair<void *, size_t>> &v, size_t i, size_t need)
+{
+	if(v.size() <= i)
+		v.resize(i + 1, {nullptr, 0});
+	if(v[i].second < need || !v[i].first) {
+		dfree(v[i].first);
+		v[i].first = dmalloc(need);
+		v[i].second = v[i].first ? need : 0;
+	}
+	return v[i].first;
+}
+
 // RAII device buffer over the runtime allocator
 struct Dev {
 	void *p = nullptr;
@@ -328,15 +349,18 @@ int sphrad::extremum(const double *coeff_dev, long long cstride, int S, unsigned
 	if(!plan)
 		return -1;
 	const int M = polar ? 0 : (int) Lc;
-	Dev ds(sht_scratch_bytes(plan, S, M)), drb(sht_rowbest_bytes(plan, S)), dt((size_t) S * 2 * sizeof(double));
-	if(!ds.p || !drb.p || !dt.p)
+	std::lock_guard<std::mutex> lk(g_ext.mu);
+	auto &bufs = g_ext.bufs[current_device()];
+	void *ds = ext_buffer(bufs, 0, sht_scratch_bytes(plan, S, M)), *drb = ext_buffer(bufs, 1, sht_rowbest_bytes(plan, S)),
+	     *dt = ext_buffer(bufs, 2, (size_t) S * 2 * sizeof(double));
+	if(!ds || !drb || !dt)
 		return -1;
-	double *t0 = (double *) dt.p, *p0 = t0 + S;
-	if(sht_synthesis(plan, coeff_dev, S, cstride, L, polar, Lc, kPixArgmax, drb.p, ds.p, stream, sign) ||
-	   sht_rows_argmax(plan, S, drb.p, t0, p0, nullptr, stream) ||
+	double *t0 = (double *) dt, *p0 = t0 + S;
+	if(sht_synthesis(plan, coeff_dev, S, cstride, L, polar, Lc, kPixArgmax, drb, ds, stream, sign) ||
+	   sht_rows_argmax(plan, S, drb, t0, p0, nullptr, stream) ||
 	   peak_refine(S, L, polar, coeff_dev, cstride, t0, p0, sign, 100, 1e-11, out_dev, status_dev, stream))
 		return -1;
-	// the scratch buffers are released on return
+	// the scratch is reused by the next call once this one has finished
 	return sync_stream(stream);
 }
 

@@ -14,6 +14,8 @@ stages:
             of N (k_gemm and its epilogues)
   uneven    the uneven batch of N segments (gathers, k_tc_contract,
             k_epilogue, scatters)
+  fseries   3 x N c1 time series (n = 4096) to whitened half spectra
+            (k_rfft_whiten)
 
 Each stage builds its inputs, runs once untimed, then ``--calls`` times and
 prints the mean device time per call (CUDA events).
@@ -38,7 +40,7 @@ def c1_skies(S, W, n):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("stage", choices=["render", "peaks", "rotate", "product", "mlp", "uneven"])
+    ap.add_argument("stage", choices=["render", "peaks", "rotate", "product", "mlp", "uneven", "fseries"])
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--calls", type=int, default=3)
     args = ap.parse_args()
@@ -91,6 +93,14 @@ def main():
         T = (T / np.linalg.norm(T, axis=1, keepdims=True)).astype(np.float32)
         Xd, Td = torch.from_numpy(X).cuda(), torch.from_numpy(T).cuda()
         run = lambda: p.train_step(Xd, Td, 1e-4)  # noqa: E731
+    elif args.stage == "fseries":
+        pos = W.random_positions(3, W.R_EARTH_S, W.rng_for(2))
+        b = W.make_tseries_batch(pos, 4096, 1.0 / 4096, 256, seed=5)
+        x = torch.from_numpy(np.ascontiguousarray(b["x"][:, np.arange(n) % 256, :])).cuda()
+        fp = S.FseriesPlan(4096, b["psd"])
+        keep = [fp]
+        out = torch.empty((3, n, 2049), dtype=torch.complex128, device="cuda")
+        run = lambda: fp.transform(x, out=out)  # noqa: E731
     else:
         pos = W.random_positions(4, W.R_EARTH_S, W.rng_for(9))
         batch = W.make_uneven_batch(pos, n, seed=11)
