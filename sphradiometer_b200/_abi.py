@@ -142,6 +142,14 @@ SIGNATURES = {
     "correlator_baseline_integrate_power_fd": (_P(sh_series), [_vp, _vp, _P(correlator_plan_fd)]),
     "correlator_network_integrate_power_fd": (_P(sh_series), [_P(sh_series), _P(_vp), _P(correlator_network_plan_fd)]),
     "sphrad_b200_plan_fd_touch": (None, [_P(correlator_plan_fd)]),
+    # precalculated plans on disk
+    "make_precalc_directories": (_i, [C.c_char_p, _i]),
+    "write_precalc_time_series_length": (_i, [_u, C.c_char_p]),
+    "read_precalc_time_series_length": (_i, [_P(_u), C.c_char_p]),
+    "write_precalc_correlator_network_plan_fd": (_i, [_P(correlator_network_plan_fd), _P(correlator_network_plan_fd), C.c_char_p]),
+    "read_precalc_correlator_network_baselines": (_P(correlator_network_baselines), [_P(instrument_array), C.c_char_p]),
+    "read_precalc_correlator_network_plan_fd": (_i, [_P(correlator_network_plan_fd), _P(correlator_network_plan_fd), _P(correlator_network_baselines), _i,
+                                                      C.c_char_p]),
     # batched extension
     "sphrad_batch_plan_new": (_vp, [_P(correlator_network_plan_fd), _i]),
     "sphrad_batch_plan_free": (None, [_vp]),

@@ -12,6 +12,8 @@
 
 typedef double _Complex dcplx;
 
+struct sh_series_rotation_plan;
+
 namespace sphrad {
 
 inline double cre(dcplx z) { return __real__ z; }
@@ -43,6 +45,11 @@ void unregister_owner(const void *owner);
 void note_write(const void *p);
 uint64_t owner_generation(const void *owner);
 void bump_owner(const void *owner);
+
+// rotation plan over a malloc'ed flat block of the matrices l = 1 .. l_max
+// (matrix l at rot_offset(l), element (m, m') at (2l+1)(m'+l) + (m+l)); the
+// plan takes the block over
+::sh_series_rotation_plan *rotation_plan_adopt_flat(unsigned l_max, dcplx *flat);
 
 // host Legendre functions (GSL sphPlm convention, Condon-Shortley phase):
 // out[l - m] for l = m .. l_max

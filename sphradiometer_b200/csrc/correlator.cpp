@@ -6,6 +6,7 @@
 // construction and integration run on the GPU (runtime.cu, batch.cu);
 // these functions manage the host structs and their device mirrors.
 #include <sphradiometer/correlator.h>
+#include <sphradiometer/inspiral_sky_map.h>
 #include <sphradiometer_b200.h>
 
 #include <cuda_runtime_api.h>
@@ -842,4 +843,353 @@ extern "C" int sphrad_batch_status(sphrad_batch_plan *p)
 	if(batch_check_error(p->impl, &code))
 		return -1;
 	return (int) code;
+}
+
+// ------------------------------------------------------------------------
+// precalculated plans on disk (inspiral_sky_map.c:1113-1811)
+// ------------------------------------------------------------------------
+// The reference's raw-binary directory tree, field by field in the order
+// its reader and writer use, so that plans cached by the reference load
+// here without recomputing delay tables, and plans built here can be
+// cached in its format.  Under <dir>/correlator_network_plan_fd:
+//   correlator_network_baselines/n_baselines.dat          int
+//   correlator_network_baselines/baselines/<i>/correlator_baseline.dat
+//                                     int index_a, int index_b, double theta, double phi
+//   correlator_network_baselines/baselines/<i>/d.dat      double[3] (gsl_vector_fwrite)
+//   correlator_plan_fd/<i>/correlator_plan_fd.dat         double delta_t, int transient
+//   correlator_plan_fd/<i>/rotation_plan/l_max.dat        unsigned
+//   correlator_plan_fd/<i>/rotation_plan/D.dat            the (2l+1)^2 complex matrices,
+//                                     l = 1 .. l_max, element (m, m') at (2l+1)(m'+l) + (m+l)
+//   correlator_plan_fd/<i>/delay_product_{p,n}/sh_series_array.dat
+//                                     unsigned l_max, int polar, int n, int stride,
+//                                     n * stride complex coefficients
+// and <dir>/time_series_length.dat (unsigned).  "p" and "n" are the plans
+// of positive and negative frequencies of the inspiral pipeline; they share
+// the baselines and the rotation plan.  Native byte order, as fread/fwrite.
+#include <cerrno>
+#include <string>
+#include <sys/stat.h>
+
+namespace {
+
+std::string base_dir(const char *dir, int i)
+{
+	return std::string(dir) + "/correlator_network_plan_fd/correlator_network_baselines/baselines/" + std::to_string(i);
+}
+
+std::string plan_dir(const char *dir, int i) { return std::string(dir) + "/correlator_network_plan_fd/correlator_plan_fd/" + std::to_string(i); }
+
+struct File {
+	FILE *f;
+	File(const std::string &path, const char *mode) : f(fopen(path.c_str(), mode)) {}
+	~File()
+	{
+		if(f)
+			fclose(f);
+	}
+};
+
+// read exactly n items or fail with the file named
+bool get(File &fl, void *dst, size_t size, size_t n, const std::string &path)
+{
+	if(!fl.f || fread(dst, size, n, fl.f) != n) {
+		set_error("precalc: cannot read %zu x %zu bytes from %s", n, size, path.c_str());
+		return false;
+	}
+	return true;
+}
+
+bool put(File &fl, const void *src, size_t size, size_t n, const std::string &path)
+{
+	if(!fl.f || fwrite(src, size, n, fl.f) != n) {
+		set_error("precalc: cannot write %s", path.c_str());
+		return false;
+	}
+	return true;
+}
+
+bool make_dir(const std::string &path, bool exist_ok)
+{
+	if(mkdir(path.c_str(), S_IRWXU | S_IRWXG | S_IRWXO) == 0 || (exist_ok && errno == EEXIST))
+		return true;
+	set_error("precalc: cannot make directory %s", path.c_str());
+	return false;
+}
+
+bool write_array(const struct sh_series_array *a, const std::string &path)
+{
+	File fl(path, "wb");
+	return put(fl, &a->l_max, sizeof(a->l_max), 1, path) && put(fl, &a->polar, sizeof(a->polar), 1, path) && put(fl, &a->n, sizeof(a->n), 1, path) &&
+	       put(fl, &a->stride, sizeof(a->stride), 1, path) && put(fl, a->coeff, sizeof(dcplx), (size_t) a->n * a->stride, path);
+}
+
+struct sh_series_array *read_array(const std::string &path)
+{
+	File fl(path, "rb");
+	unsigned l_max = 0;
+	int polar = 0, n = 0, stride = 0;
+	if(!get(fl, &l_max, sizeof(l_max), 1, path) || !get(fl, &polar, sizeof(polar), 1, path) || !get(fl, &n, sizeof(n), 1, path) ||
+	   !get(fl, &stride, sizeof(stride), 1, path))
+		return NULL;
+	if(n <= 0 || (size_t) stride != length(l_max, polar)) {
+		set_error("precalc: %s holds %d series of stride %d for l_max %u (%s)", path.c_str(), n, stride, l_max, polar ? "polar" : "non-polar");
+		return NULL;
+	}
+	struct sh_series_array *a = sh_series_array_new(n, l_max, polar);
+	if(!a)
+		return NULL;
+	if(!get(fl, a->coeff, sizeof(dcplx), (size_t) n * stride, path)) {
+		sh_series_array_free(a);
+		return NULL;
+	}
+	return a;
+}
+
+}  // namespace
+
+extern "C" int make_precalc_directories(char *precalc_path, int n_ifo)
+{
+	// the reference's tree (inspiral_sky_map.c:1458-1560): every directory
+	// must be new; n_ifo numbered directories under baselines/,
+	// correlator_plan_fd/ and psh_series/
+	const std::string r(precalc_path);
+	const std::string net = r + "/correlator_network_plan_fd";
+	if(!make_dir(r, false) || !make_dir(net, false) || !make_dir(net + "/correlator_network_baselines", false) ||
+	   !make_dir(net + "/correlator_network_baselines/baselines", false))
+		return -1;
+	for(int k = 0; k < n_ifo; k++)
+		if(!make_dir(base_dir(precalc_path, k), false))
+			return -1;
+	if(!make_dir(net + "/correlator_plan_fd", false))
+		return -1;
+	for(int k = 0; k < n_ifo; k++) {
+		const std::string p = plan_dir(precalc_path, k);
+		if(!make_dir(p, false) || !make_dir(p + "/delay_product_n", false) || !make_dir(p + "/delay_product_p", false) ||
+		   !make_dir(p + "/rotation_plan", false))
+			return -1;
+	}
+	const std::string ac = r + "/autocorrelator_network_plan_fd";
+	if(!make_dir(ac, false) || !make_dir(ac + "/psh_series", false))
+		return -1;
+	for(int k = 0; k < n_ifo; k++) {
+		const std::string p = ac + "/psh_series/" + std::to_string(k);
+		if(!make_dir(p, false) || !make_dir(p + "/sh_series_n", false) || !make_dir(p + "/sh_series_p", false))
+			return -1;
+	}
+	return make_dir(r + "/sh_series", false) ? 0 : -1;
+}
+
+extern "C" int write_precalc_time_series_length(unsigned int length, char *parent_dir)
+{
+	const std::string path = std::string(parent_dir) + "/time_series_length.dat";
+	File fl(path, "wb");
+	return put(fl, &length, sizeof(length), 1, path) ? 0 : -1;
+}
+
+extern "C" int read_precalc_time_series_length(unsigned int *length, char *parent_dir)
+{
+	const std::string path = std::string(parent_dir) + "/time_series_length.dat";
+	File fl(path, "rb");
+	return get(fl, length, sizeof(*length), 1, path) ? 0 : -1;
+}
+
+extern "C" int write_precalc_correlator_network_plan_fd(const struct correlator_network_plan_fd *fdplansp, const struct correlator_network_plan_fd *fdplansn,
+							char *parent_dir)
+{
+	const struct correlator_network_baselines *nb = fdplansp->baselines;
+	const std::string net = std::string(parent_dir) + "/correlator_network_plan_fd";
+	{
+		const std::string path = net + "/correlator_network_baselines/n_baselines.dat";
+		File fl(path, "wb");
+		if(!put(fl, &nb->n_baselines, sizeof(nb->n_baselines), 1, path))
+			return -1;
+	}
+	for(int i = 0; i < nb->n_baselines; i++) {
+		// directories beyond the ones make_precalc_directories made (it
+		// makes one per instrument) are made here
+		const struct correlator_baseline *b = nb->baselines[i];
+		const std::string bd = base_dir(parent_dir, i), pd = plan_dir(parent_dir, i);
+		if(!make_dir(bd, true) || !make_dir(pd, true) || !make_dir(pd + "/rotation_plan", true) || !make_dir(pd + "/delay_product_p", true) ||
+		   !make_dir(pd + "/delay_product_n", true))
+			return -1;
+		{
+			const std::string path = bd + "/correlator_baseline.dat";
+			File fl(path, "wb");
+			if(!put(fl, &b->index_a, sizeof(b->index_a), 1, path) || !put(fl, &b->index_b, sizeof(b->index_b), 1, path) ||
+			   !put(fl, &b->theta, sizeof(b->theta), 1, path) || !put(fl, &b->phi, sizeof(b->phi), 1, path))
+				return -1;
+		}
+		{
+			const std::string path = bd + "/d.dat";
+			double d[3];
+			for(int k = 0; k < 3; k++)
+				d[k] = b->d->data[k * b->d->stride];
+			File fl(path, "wb");
+			if(!put(fl, d, sizeof(double), 3, path))
+				return -1;
+		}
+		const struct correlator_plan_fd *pp = fdplansp->plans[i], *pn = fdplansn->plans[i];
+		{
+			const std::string path = pd + "/correlator_plan_fd.dat";
+			File fl(path, "wb");
+			if(!put(fl, &pp->delta_t, sizeof(pp->delta_t), 1, path) || !put(fl, &pp->transient, sizeof(pp->transient), 1, path))
+				return -1;
+		}
+		{
+			const std::string path = pd + "/rotation_plan/l_max.dat";
+			File fl(path, "wb");
+			if(!put(fl, &pp->rotation_plan->l_max, sizeof(pp->rotation_plan->l_max), 1, path))
+				return -1;
+		}
+		{
+			const std::string path = pd + "/rotation_plan/D.dat";
+			File fl(path, "wb");
+			for(unsigned l = 1; l <= pp->rotation_plan->l_max; l++)
+				if(!put(fl, pp->rotation_plan->D[l] - ((size_t) (2 * l + 1) * l + l), sizeof(dcplx), (size_t) (2 * l + 1) * (2 * l + 1), path))
+					return -1;
+		}
+		if(!write_array(pp->delay_product, pd + "/delay_product_p/sh_series_array.dat") ||
+		   !write_array(pn->delay_product, pd + "/delay_product_n/sh_series_array.dat"))
+			return -1;
+	}
+	return 0;
+}
+
+extern "C" struct correlator_network_baselines *read_precalc_correlator_network_baselines(const struct instrument_array *instruments, char *parent_dir)
+{
+	int nb = 0;
+	{
+		const std::string path = std::string(parent_dir) + "/correlator_network_plan_fd/correlator_network_baselines/n_baselines.dat";
+		File fl(path, "rb");
+		if(!get(fl, &nb, sizeof(nb), 1, path))
+			return NULL;
+	}
+	if(nb <= 0) {
+		set_error("precalc: %d baselines", nb);
+		return NULL;
+	}
+	struct correlator_network_baselines *net = (struct correlator_network_baselines *) malloc(sizeof(*net));
+	struct correlator_baseline **v = (struct correlator_baseline **) calloc(nb, sizeof(*v));
+	bool ok = net && v;
+	for(int i = 0; ok && i < nb; i++) {
+		const std::string path = base_dir(parent_dir, i) + "/correlator_baseline.dat";
+		File fl(path, "rb");
+		int a = 0, b = 0;
+		double theta = 0, phi = 0;
+		ok = get(fl, &a, sizeof(a), 1, path) && get(fl, &b, sizeof(b), 1, path) && get(fl, &theta, sizeof(theta), 1, path) &&
+		     get(fl, &phi, sizeof(phi), 1, path);
+		if(ok)
+			v[i] = correlator_baseline_new(instruments, a, b);
+		// the cached direction must be the one these instruments give
+		// (inspiral_sky_map.c:1145-1150)
+		if(ok && (!v[i] || v[i]->theta != theta || v[i]->phi != phi)) {
+			set_error("precalc: baseline %d (%d, %d) does not match the instruments", i, a, b);
+			ok = false;
+		}
+	}
+	if(!ok) {
+		for(int i = 0; v && i < nb; i++)
+			correlator_baseline_free(v[i]);
+		free(v);
+		free(net);
+		return NULL;
+	}
+	net->baselines = v;
+	net->n_baselines = nb;
+	return net;
+}
+
+extern "C" int read_precalc_correlator_network_plan_fd(struct correlator_network_plan_fd *fdplansp, struct correlator_network_plan_fd *fdplansn,
+						       const struct correlator_network_baselines *baselines, int tseries_length, char *parent_dir)
+{
+	if(!fdplansp || !fdplansn || !baselines || tseries_length <= 0) {
+		set_error("read_precalc_correlator_network_plan_fd: plans must be allocated and the length positive");
+		return -1;
+	}
+	const int nb = baselines->n_baselines;
+	struct correlator_plan_fd **pp = (struct correlator_plan_fd **) calloc(nb, sizeof(*pp));
+	struct correlator_plan_fd **pn = (struct correlator_plan_fd **) calloc(nb, sizeof(*pn));
+	bool ok = pp && pn;
+	for(int i = 0; ok && i < nb; i++) {
+		const std::string pd = plan_dir(parent_dir, i);
+		double delta_t = 0;
+		int transient = 0;
+		unsigned l_max = 0;
+		{
+			const std::string path = pd + "/correlator_plan_fd.dat";
+			File fl(path, "rb");
+			ok = get(fl, &delta_t, sizeof(delta_t), 1, path) && get(fl, &transient, sizeof(transient), 1, path);
+		}
+		if(ok) {
+			const std::string path = pd + "/rotation_plan/l_max.dat";
+			File fl(path, "rb");
+			ok = get(fl, &l_max, sizeof(l_max), 1, path);
+		}
+		struct sh_series_rotation_plan *rot = NULL;
+		if(ok) {
+			const std::string path = pd + "/rotation_plan/D.dat";
+			const size_t len = rot_offset(l_max + 1);
+			dcplx *flat = (dcplx *) malloc((len ? len : 1) * sizeof(dcplx));
+			File fl(path, "rb");
+			ok = flat && get(fl, flat, sizeof(dcplx), len, path);
+			if(ok)
+				rot = rotation_plan_adopt_flat(l_max, flat);
+			ok = ok && rot;
+			if(!rot)
+				free(flat);
+		}
+		struct sh_series_array *dp = ok ? read_array(pd + "/delay_product_p/sh_series_array.dat") : NULL;
+		struct sh_series_array *dn = dp ? read_array(pd + "/delay_product_n/sh_series_array.dat") : NULL;
+		ok = ok && dp && dn;
+		if(ok && (dn->n != dp->n || dn->l_max != dp->l_max || dn->polar != dp->polar)) {
+			set_error("precalc: positive and negative delay tables of baseline %d differ in shape", i);
+			ok = false;
+		}
+		if(ok) {
+			pp[i] = (struct correlator_plan_fd *) calloc(1, sizeof(**pp));
+			pn[i] = (struct correlator_plan_fd *) calloc(1, sizeof(**pn));
+			ok = pp[i] && pn[i];
+		}
+		if(ok) {
+			// the plans own the tables from here on (freed with them on failure)
+			pp[i]->delay_product = dp;
+			pn[i]->delay_product = dn;
+			pp[i]->rotation_plan = rot;
+			pn[i]->rotation_plan = sh_series_rotation_plan_copy(rot);
+			rot = NULL;
+			dp = dn = NULL;
+			for(struct correlator_plan_fd *p : {pp[i], pn[i]}) {
+				p->baseline = baselines->baselines[i];
+				p->delta_t = delta_t;
+				p->transient = transient;
+				// scratch of the integrator (inspiral_sky_map.c:1316-1323)
+				p->fseries_product = (dcplx *) calloc(tseries_length, sizeof(dcplx));
+				p->power_1d = p->rotation_plan ? sh_series_new(p->rotation_plan->l_max, p->delay_product->polar) : NULL;
+				ok = ok && p->rotation_plan && p->fseries_product && p->power_1d;
+			}
+			if(ok) {
+				plan_register(pp[i]);
+				plan_register(pn[i]);
+			}
+		} else {
+			if(rot)
+				sh_series_rotation_plan_free(rot);
+			sh_series_array_free(dp);
+			sh_series_array_free(dn);
+		}
+	}
+	if(!ok) {
+		for(int i = 0; i < nb && pp && pn; i++) {
+			correlator_plan_fd_free(pp[i]);
+			correlator_plan_fd_free(pn[i]);
+		}
+		free(pp);
+		free(pn);
+		return -1;
+	}
+	fdplansp->baselines = (struct correlator_network_baselines *) baselines;
+	fdplansn->baselines = (struct correlator_network_baselines *) baselines;
+	fdplansp->plans = pp;
+	fdplansn->plans = pn;
+	return 0;
 }

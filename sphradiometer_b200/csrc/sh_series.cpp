@@ -619,6 +619,16 @@ extern "C" void sh_series_rotation_plan_free(struct sh_series_rotation_plan *pla
 	free(plan);
 }
 
+// a plan over a malloc'ed flat block of matrices l = 1 .. l_max (taken
+// over by the plan: freed with it)
+::sh_series_rotation_plan *sphrad::rotation_plan_adopt_flat(unsigned l_max, dcplx *flat)
+{
+	struct sh_series_rotation_plan *p = rotation_plan_from_flat(l_max, flat);
+	if(p)
+		bump_owner(p);
+	return p;
+}
+
 extern "C" struct sh_series_rotation_plan *sh_series_rotation_plan_copy(const struct sh_series_rotation_plan *plan)
 {
 	std::vector<dcplx> scratch;
