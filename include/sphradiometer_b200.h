@@ -176,6 +176,29 @@ size_t sphrad_batch_tseries_workspace_size(const sphrad_batch_plan *plan, int n_
 int sphrad_batch_integrate_tseries(sphrad_batch_plan *plan, sphrad_fseries_plan *fseries_plan, const double *tseries, int n_seg, long long ldt,
 				   const double *gmst, void *sky, void *workspace, size_t workspace_bytes, void *cuda_stream);
 
+/* ---- projection operator of the inspiral path ----------------------------
+ *
+ * correlator_network_plan_mult_by_projection (inspiral_sky_map.c:423-549)
+ * with the antenna patterns supplied by the caller: for every baseline
+ * (a, b) and frequency bin j < n, the function
+ *     P_ab = u_a conj(u_b) / sum_k |u_k|^2 - delta_ab,
+ *     u_k = (F+_k + i beta Fx_k) / psd[j][k],   |u_k|^2 = (F+_k^2 + beta^2 Fx_k^2) / psd[j][k]^2
+ * (CBCProjectionMatrix, :342-364) is sampled on the reference's mesh for
+ * the delay kernels' l_max L (rows theta_i = acos x_i for the 2(L+1)
+ * Gauss-Legendre nodes x_i in decreasing order, columns phi_j = 2 pi j /
+ * (2(L+1)), as sh_series_to_mesh lays them out), projected onto l <= L,
+ * rotated into the baseline frame (sh_series_invrot_matrix) and multiplied
+ * into bin j's polar delay kernel; the plan's kernels become non-polar,
+ * power_1d non-polar at L, and each rotation plan a full rotation into the
+ * Earth frame (sh_series_rot_matrix).  Every bin of a baseline is processed
+ * on the GPU in batches.
+ * fplus, fcross: [n_det][2(L+1)][2(L+1)] doubles, F+ and Fx of every
+ * detector at the polarisation angle of interest (the reference evaluates
+ * LAL's XLALComputeDetAMResponse there, with gmst 0); psd[j][k]: bin j,
+ * detector k.  All baselines must share L and n.  0 on success, -1 on
+ * failure (the plan is unchanged up to the failing baseline). */
+int sphrad_network_plan_mult_by_projection(struct correlator_network_plan_fd *plan, double beta, const double *fplus, const double *fcross, double **psd);
+
 /* ---- uneven batches ------------------------------------------------------
  *
  * Segments of one detector network with different DFT lengths, output

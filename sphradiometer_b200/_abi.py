@@ -142,6 +142,7 @@ SIGNATURES = {
     "correlator_baseline_integrate_power_fd": (_P(sh_series), [_vp, _vp, _P(correlator_plan_fd)]),
     "correlator_network_integrate_power_fd": (_P(sh_series), [_P(sh_series), _P(_vp), _P(correlator_network_plan_fd)]),
     "sphrad_b200_plan_fd_touch": (None, [_P(correlator_plan_fd)]),
+    "sphrad_network_plan_mult_by_projection": (_i, [_P(correlator_network_plan_fd), _d, _vp, _vp, _vp]),
     # precalculated plans on disk
     "make_precalc_directories": (_i, [C.c_char_p, _i]),
     "write_precalc_time_series_length": (_i, [_u, C.c_char_p]),

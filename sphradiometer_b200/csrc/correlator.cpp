@@ -1193,3 +1193,66 @@ extern "C" int read_precalc_correlator_network_plan_fd(struct correlator_network
 	fdplansn->plans = pn;
 	return 0;
 }
+
+// ------------------------------------------------------------------------
+// projection operator (inspiral_sky_map.c:387-549)
+// ------------------------------------------------------------------------
+extern "C" int sphrad_network_plan_mult_by_projection(struct correlator_network_plan_fd *plan, double beta, const double *fplus, const double *fcross,
+						      double **psd)
+{
+	if(!plan || !fplus || !fcross || !psd) {
+		set_error("sphrad_network_plan_mult_by_projection: NULL argument");
+		return -1;
+	}
+	const struct correlator_network_baselines *nb = plan->baselines;
+	const int n_det = instrument_array_len(nb->baselines[0]->instruments);
+	const struct sh_series_array *d0 = plan->plans[0]->delay_product;
+	const unsigned L = d0->l_max;
+	const int n = d0->n;
+	for(int i = 0; i < nb->n_baselines; i++) {
+		const struct sh_series_array *d = plan->plans[i]->delay_product;
+		if(!d->polar || d->l_max != L || d->n != n) {
+			set_error("sphrad_network_plan_mult_by_projection: baselines need polar delay kernels of one l_max and length");
+			return -1;
+		}
+	}
+	std::vector<double> S((size_t) n * n_det);
+	for(int j = 0; j < n; j++)
+		for(int k = 0; k < n_det; k++)
+			S[(size_t) j * n_det + k] = psd[j][k];
+	for(int i = 0; i < nb->n_baselines; i++) {
+		struct correlator_plan_fd *p = plan->plans[i];
+		const struct correlator_baseline *bl = nb->baselines[i];
+		// the projection is rotated into the frame in which the delay
+		// kernel was built (the baseline along z, :488-500)
+		double *Rinv = sh_series_invrot_matrix(bl->theta, bl->phi);
+		struct sh_series_array *res = sh_series_array_new(n, L, 0);
+		if(!Rinv || !res || projection_multiply(n, L, n_det, fplus, fcross, S.data(), bl->index_a, bl->index_b, beta, Rinv, (const double *) p->delay_product->coeff,
+							    (double *) res->coeff)) {
+			free(Rinv);
+			sh_series_array_free(res);
+			return -1;
+		}
+		free(Rinv);
+		// the power is no longer azimuthally symmetric about the baseline:
+		// non-polar storage at the kernel's l_max and a full rotation into
+		// the Earth frame (:501-531)
+		double *R = sh_series_rot_matrix(bl->theta, bl->phi);
+		struct sh_series_rotation_plan *rp = NULL;
+		if(!R || !sh_series_set_polar(p->power_1d, 0) || !sh_series_resize(p->power_1d, L) || !(rp = sh_series_rotation_plan_new(p->power_1d, R))) {
+			free(R);
+			sh_series_array_free(res);
+			set_error("sphrad_network_plan_mult_by_projection: rotation plan of baseline %d failed", i);
+			return -1;
+		}
+		free(R);
+		forget_mirror(p);
+		unregister_owner(p);
+		sh_series_array_free(p->delay_product);
+		p->delay_product = res;
+		sh_series_rotation_plan_free(p->rotation_plan);
+		p->rotation_plan = rp;
+		plan_register(p);
+	}
+	return 0;
+}

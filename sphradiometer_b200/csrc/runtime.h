@@ -119,6 +119,15 @@ int fseries_run(void *plan, const double *ts, int rows, long long ldt, void *out
 // symmetry); synchronous
 int fseries_run_host(void *plan, const double *ts_host, double *fs_host);
 
+// ---- projection operator x delay kernel (projection.cu) ----------------
+// For every bin j < n: the projection P_ab of bin j (antenna patterns
+// fp / fc [n_det][2(L+1)][2(L+1)] on the reference mesh of L, psd
+// [n][n_det], CBC parameter beta), analysed to l <= L, rotated by the 3x3
+// Rinv and multiplied into the bin's polar delay kernel (delay_host, host
+// [n][L+1] complex); out_host: host [n][(L+1)^2] complex, truncated at L
+int projection_multiply(int n, unsigned L, int n_det, const double *fp_host, const double *fc_host, const double *psd_host, int a, int b, double beta,
+			const double *Rinv, const double *delay_host, double *out_host);
+
 // ---- uneven batches (uneven.cu) -----------------------------------------
 // F[d][i][k] = in[in_off[seg[i]] + det[d] Ku + k] for a job of S segments
 // of n_sub detectors (device pointers; stream a cudaStream_t)
