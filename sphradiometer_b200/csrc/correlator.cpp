@@ -663,8 +663,57 @@ extern "C" struct sh_series *correlator_network_integrate_power_fd(struct sh_ser
 // batched extension API
 // ------------------------------------------------------------------------
 struct sphrad_batch_plan {
-	void *impl;
+	void *impl;  // polar delay kernels: the batched path of batch.cu
+	void *np;    // non-polar kernels (projection operator): nonpolar.cu
 };
+
+// plans of projected (non-polar) kernels: one complex contraction per
+// segment over all bins of all baselines, rotation folded into the kernels
+static sphrad_batch_plan *batch_plan_new_nonpolar(const struct correlator_network_plan_fd *plan, int precision)
+{
+	const int nb = plan->baselines->n_baselines;
+	if(precision != SPHRAD_PREC_FP64 && precision != SPHRAD_PREC_FP32) {
+		set_error("sphrad_batch_plan_new: plans with non-polar delay kernels run in FP64 or FP32");
+		return NULL;
+	}
+	const unsigned L = plan->plans[0]->delay_product->l_max;
+	const int n = plan->plans[0]->delay_product->n;
+	std::vector<int> bi(nb), bj(nb);
+	std::vector<const double *> D(nb), rot(nb);
+	std::vector<std::vector<dcplx>> scratch(nb);
+	for(int b = 0; b < nb; b++) {
+		const struct correlator_plan_fd *p = plan->plans[b];
+		if(p->delay_product->polar || p->delay_product->l_max != L || p->delay_product->n != n || p->rotation_plan->l_max < L) {
+			set_error("sphrad_batch_plan_new: non-polar delay kernels must share l_max and length, with rotation plans up to l_max");
+			return NULL;
+		}
+		bi[b] = plan->baselines->baselines[b]->index_a;
+		bj[b] = plan->baselines->baselines[b]->index_b;
+		D[b] = (const double *) p->delay_product->coeff;
+		rot[b] = (const double *) rotation_plan_flat_for(p->rotation_plan, scratch[b]);
+	}
+	void *np = np_plan_create(instrument_array_len(plan->baselines->baselines[0]->instruments), nb, bi.data(), bj.data(), n, L, D.data(), rot.data(),
+				  precision == SPHRAD_PREC_FP64);
+	if(!np)
+		return NULL;
+	sphrad_batch_plan *bp = (sphrad_batch_plan *) malloc(sizeof(*bp));
+	if(!bp) {
+		np_plan_destroy(np);
+		return NULL;
+	}
+	bp->impl = NULL;
+	bp->np = np;
+	return bp;
+}
+
+// the entry points of the polar path that a non-polar plan does not take
+#define NEED_POLAR(p, what)                                                                          \
+	do {                                                                                          \
+		if(!(p)->impl) {                                                                      \
+			set_error("%s: not available for plans with non-polar delay kernels", what); \
+			return -1;                                                                    \
+		}                                                                                     \
+	} while(0)
 
 extern "C" sphrad_batch_plan *sphrad_batch_plan_new(const struct correlator_network_plan_fd *plan, int precision)
 {
@@ -673,6 +722,8 @@ extern "C" sphrad_batch_plan *sphrad_batch_plan_new(const struct correlator_netw
 		set_error("sphrad_batch_plan_new: %d baselines (1..%d supported)", nb, kMaxBaselines);
 		return NULL;
 	}
+	if(!plan->plans[0]->delay_product->polar)
+		return batch_plan_new_nonpolar(plan, precision);
 	BatchPlanDesc d;
 	d.n_det = instrument_array_len(plan->baselines->baselines[0]->instruments);
 	d.n_baselines = nb;
@@ -701,60 +752,78 @@ extern "C" sphrad_batch_plan *sphrad_batch_plan_new(const struct correlator_netw
 		return NULL;
 	}
 	bp->impl = impl;
+	bp->np = NULL;
 	return bp;
 }
 
 extern "C" void sphrad_batch_plan_free(sphrad_batch_plan *p)
 {
-	if(p)
+	if(p) {
 		batch_plan_destroy(p->impl);
+		np_plan_destroy(p->np);
+	}
 	free(p);
 }
 
-extern "C" unsigned sphrad_batch_plan_l_max(const sphrad_batch_plan *p) { return batch_plan_l_max(p->impl); }
-extern "C" int sphrad_batch_plan_bins(const sphrad_batch_plan *p) { return batch_plan_bins(p->impl); }
-extern "C" size_t sphrad_batch_workspace_size(const sphrad_batch_plan *p, int n_seg) { return batch_workspace_bytes(p->impl, n_seg); }
+extern "C" unsigned sphrad_batch_plan_l_max(const sphrad_batch_plan *p) { return p->impl ? batch_plan_l_max(p->impl) : np_plan_l_max(p->np); }
+extern "C" int sphrad_batch_plan_bins(const sphrad_batch_plan *p) { return p->impl ? batch_plan_bins(p->impl) : np_plan_n(p->np); }
+extern "C" size_t sphrad_batch_workspace_size(const sphrad_batch_plan *p, int n_seg) { return p->impl ? batch_workspace_bytes(p->impl, n_seg) : 0; }
 
 extern "C" int sphrad_batch_integrate(sphrad_batch_plan *p, const void *fseries_dev, int n_seg, long long ld, const double *gmst_dev, void *sky_dev, void *workspace,
 				      size_t workspace_bytes, void *stream)
 {
+	if(!p->impl)
+		return np_run(p->np, fseries_dev, n_seg, ld, gmst_dev, sky_dev, stream);
 	return batch_run(p->impl, fseries_dev, n_seg, ld, gmst_dev, sky_dev, workspace, workspace_bytes, stream, 0);
 }
 
 extern "C" int sphrad_batch_integrate_weighted(sphrad_batch_plan *p, const void *fseries_dev, int n_seg, long long ld, const double *gmst_dev, void *sky_dev,
 					       void *workspace, size_t workspace_bytes, void *stream, int split, const float *baseline_factor)
 {
+	NEED_POLAR(p, "sphrad_batch_integrate_weighted");
 	return batch_run(p->impl, fseries_dev, n_seg, ld, gmst_dev, sky_dev, workspace, workspace_bytes, stream, split > 0 ? split : 0, baseline_factor);
 }
 
 extern "C" int sphrad_batch_integrate_host(sphrad_batch_plan *p, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky)
 {
+	NEED_POLAR(p, "sphrad_batch_integrate_host");
 	return batch_run_host(p->impl, fseries, n_seg, ld, gmst, sky);
 }
 
-extern "C" int sphrad_batch_set_split(sphrad_batch_plan *p, int n_seg, int split) { return batch_set_split(p->impl, n_seg, split); }
-extern "C" int sphrad_batch_pipeline(const sphrad_batch_plan *p, int n_seg) { return batch_pipe_variant(p->impl, n_seg); }
+extern "C" int sphrad_batch_set_split(sphrad_batch_plan *p, int n_seg, int split)
+{
+	NEED_POLAR(p, "sphrad_batch_set_split");
+	return batch_set_split(p->impl, n_seg, split);
+}
+extern "C" int sphrad_batch_pipeline(const sphrad_batch_plan *p, int n_seg) { return p->impl ? batch_pipe_variant(p->impl, n_seg) : 0; }
 extern "C" int sphrad_batch_set_pipeline(sphrad_batch_plan *p, int n_seg, int variant)
 {
 	if(variant > 2) {
 		set_error("sphrad_batch_set_pipeline: variant %d is not 0, 1 or 2", variant);
 		return -1;
 	}
+	NEED_POLAR(p, "sphrad_batch_set_pipeline");
 	return batch_set_pipe_variant(p->impl, n_seg, variant);
 }
-extern "C" int sphrad_batch_get_split(const sphrad_batch_plan *p, int n_seg) { return batch_pick_split(p->impl, n_seg); }
-extern "C" int sphrad_batch_get_ctas(const sphrad_batch_plan *p, int n_seg) { return batch_pick_ctas(p->impl, n_seg); }
-extern "C" int sphrad_batch_set_ctas(sphrad_batch_plan *p, int n_seg, int ctas) { return batch_set_ctas(p->impl, n_seg, ctas); }
-extern "C" int sphrad_batch_kernels_per_call(const sphrad_batch_plan *p) { return batch_last_kernel_count(p->impl); }
+extern "C" int sphrad_batch_get_split(const sphrad_batch_plan *p, int n_seg) { return p->impl ? batch_pick_split(p->impl, n_seg) : 1; }
+extern "C" int sphrad_batch_get_ctas(const sphrad_batch_plan *p, int n_seg) { return p->impl ? batch_pick_ctas(p->impl, n_seg) : 0; }
+extern "C" int sphrad_batch_set_ctas(sphrad_batch_plan *p, int n_seg, int ctas)
+{
+	NEED_POLAR(p, "sphrad_batch_set_ctas");
+	return batch_set_ctas(p->impl, n_seg, ctas);
+}
+extern "C" int sphrad_batch_kernels_per_call(const sphrad_batch_plan *p) { return p->impl ? batch_last_kernel_count(p->impl) : 1; }
 
 extern "C" int sphrad_batch_autotune(sphrad_batch_plan *p, const void *fseries_dev, int n_seg, long long ld, void *sky_dev, void *workspace, size_t workspace_bytes,
 				     void *stream)
 {
+	NEED_POLAR(p, "sphrad_batch_autotune");
 	return batch_autotune(p->impl, fseries_dev, n_seg, ld, sky_dev, workspace, workspace_bytes, stream);
 }
 
 extern "C" int sphrad_batch_integrate_noalloc(sphrad_batch_plan *p, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky, void *stream)
 {
+	NEED_POLAR(p, "sphrad_batch_integrate_noalloc");
 	return batch_run_noalloc(p->impl, fseries, n_seg, ld, gmst, sky, stream);
 }
 
@@ -804,7 +873,7 @@ static size_t align256(size_t b) { return (b + 255) & ~(size_t) 255; }
 
 extern "C" size_t sphrad_batch_tseries_workspace_size(const sphrad_batch_plan *p, int n_seg)
 {
-	if(n_seg <= 0)
+	if(n_seg <= 0 || !p->impl)
 		return 0;
 	const size_t spectra = (size_t) batch_plan_n_det(p->impl) * n_seg * batch_plan_bins(p->impl) * 16;
 	return align256(spectra) + batch_workspace_bytes(p->impl, n_seg);
@@ -813,6 +882,7 @@ extern "C" size_t sphrad_batch_tseries_workspace_size(const sphrad_batch_plan *p
 extern "C" int sphrad_batch_integrate_tseries(sphrad_batch_plan *p, sphrad_fseries_plan *fp, const double *tseries, int n_seg, long long ldt, const double *gmst,
 					      void *sky, void *workspace, size_t workspace_bytes, void *stream)
 {
+	NEED_POLAR(p, "sphrad_batch_integrate_tseries");
 	if(n_seg <= 0)
 		return 0;
 	if(fseries_plan_n(fp->impl) != batch_plan_n(p->impl)) {
@@ -834,12 +904,15 @@ extern "C" int sphrad_batch_integrate_tseries(sphrad_batch_plan *p, sphrad_fseri
 
 extern "C" int sphrad_batch_set_timing_events(sphrad_batch_plan *p, void *ev_begin, void *ev_end)
 {
+	NEED_POLAR(p, "sphrad_batch_set_timing_events");
 	return batch_set_timing_events(p->impl, ev_begin, ev_end);
 }
 
 extern "C" int sphrad_batch_status(sphrad_batch_plan *p)
 {
 	unsigned code = 0;
+	if(!p->impl)
+		return 0;  // the non-polar path has no device-side waits
 	if(batch_check_error(p->impl, &code))
 		return -1;
 	return (int) code;

@@ -76,6 +76,24 @@ def test_projection_plan_and_integration_match_numpy():
         Pk = (F[j] * np.conj(F[i])) @ net.delay_table(k) / n
         ref += O.rotate(Pk, L, False, O.rotation_plan(L, O.rot_matrix(bl.theta, bl.phi))) / 3
     assert np.max(np.abs(sky - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+    # the batched integrator on the projected plans: full (non-Hermitian)
+    # spectra of many segments, GMST phases, FP64 and FP32
+    import torch
+    Sg = 70
+    Fb = rng.normal(size=(3, Sg, n)) + 1j * rng.normal(size=(3, Sg, n))
+    gm = rng.uniform(0, 2 * np.pi, Sg)
+    refs = np.array([O.rotate_z(net.integrate(Fb[:, s, :]), L, False, gm[s]) for s in range(Sg)])
+    for prec, tol in (("fp64", 1e-12), ("fp32", 1e-5)):
+        bp = S.BatchPlan(net, prec)
+        assert bp.l_max == L and bp.bins == n
+        got = bp.integrate(torch.from_numpy(np.ascontiguousarray(Fb)).cuda(), torch.from_numpy(gm).cuda()).cpu().numpy()
+        err = np.linalg.norm(got - refs) / np.linalg.norm(refs)
+        assert err < tol, (prec, err)
+        assert bp.status() == 0 and bp.kernels_per_call() == 1
+        bp.close()
+    with pytest.raises(S.SphradError):
+        S.BatchPlan(net, "bf16x3")
     net.close()
 
 
