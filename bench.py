@@ -379,6 +379,50 @@ def tseries_report(S, n_seg: int, reps: int = 10):
     return out
 
 
+def projection_report(S, n_seg: int = 1024, reps: int = 3):
+    """The projection-operator (inspiral) path on the c1 network: the plan
+    transform (every bin's projection mesh, analysis, rotation and product,
+    3 baselines x 4096 bins at l_max 32, on the GPU) and the batched
+    integration with the resulting non-polar kernels (complex contraction
+    over all bins, 8 B n (l_max+1)^2 flops per segment) in FP32 and FP64.
+    Antenna patterns are smooth synthetic stand-ins (no LAL here)."""
+    import ctypes as C
+    import torch
+    from sphradiometer_b200 import workload as W
+    pos = positions()
+    n = N_SAMPLES
+    net = S.Network(pos, n, DT, l_max=L_MAX)
+    rng = np.random.default_rng(3)
+    fp, fc = W.pattern_meshes(L_MAX, N_DET, rng)
+    psd = np.ascontiguousarray(rng.uniform(0.5, 2.0, size=(n, N_DET)))
+    rows = (C.POINTER(C.c_double) * n)(*[np.ctypeslib.as_ctypes(psd[j]) for j in range(n)])
+    t0 = time.perf_counter()
+    if S.load().sphrad_network_plan_mult_by_projection(net.plan, 1.0, fp.ctypes.data, fc.ctypes.data, C.cast(rows, C.c_void_p)):
+        raise RuntimeError(S.last_error())
+    t_plan = time.perf_counter() - t0
+    F = torch.from_numpy(np.ascontiguousarray(rng.normal(size=(N_DET, n_seg, n)) + 1j * rng.normal(size=(N_DET, n_seg, n)))).cuda()
+    g = torch.rand(n_seg, dtype=torch.float64, device="cuda") * 6.28
+    out = {"plan_transform_s": t_plan, "segments": n_seg}
+    flops = 8.0 * 3 * n * (L_MAX + 1) ** 2 * n_seg
+    for prec in ("fp32", "fp64"):
+        bp = S.BatchPlan(net, prec)
+        sky = bp.integrate(F, g)
+        torch.cuda.synchronize()
+        st = torch.cuda.current_stream()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        for _ in range(reps):
+            bp.integrate(F, g, out=sky)
+        e.record(st)
+        torch.cuda.synchronize()
+        t = a.elapsed_time(e) / reps / 1e3
+        out[f"{prec}_maps_per_s"] = n_seg / t
+        out[f"{prec}_tflops"] = flops / t / 1e12
+        bp.close()
+    net.close()
+    return out
+
+
 def c2_report(S, steps: int = 10):
     """Uneven batches: 4096 segments of a 4-detector network, durations
     log-uniform in 0.25-4 s at 4096 Hz (DFT lengths 1024-16384), l_max from
@@ -702,6 +746,7 @@ def run(args):
         extra["c1_from_time_series"] = guarded(tseries_report, S, n_seg)
         if not args.quick:
             extra["c2_uneven"] = guarded(c2_report, S)
+            extra["projection_path"] = guarded(projection_report, S)
             extra["c3_sh_algebra"] = guarded(c3_report, S)
             extra["c4_learned_proposal"] = guarded(c4_report, S)
 

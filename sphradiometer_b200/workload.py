@@ -213,6 +213,23 @@ def make_tseries_batch(positions, n: int, dt: float, n_seg: int, seed: int, snr_
     return dict(x=np.ascontiguousarray(x), psd=np.where(inband, S, 0.0), F=F, gmst=b["gmst"])
 
 
+def pattern_meshes(l_max: int, n_det: int, rng: np.random.Generator):
+    """Smooth synthetic stand-ins for the antenna patterns F+ and Fx of
+    n_det detectors (quadrupolar in phi, as real patterns are, with a
+    per-detector orientation), sampled on the reference's mesh of l_max:
+    rows acos x_i for the 2(l_max+1) Gauss-Legendre nodes in decreasing
+    order, columns 2 pi j / (2(l_max+1)).  Returns (fplus, fcross), each
+    n_det x nt x nt."""
+    nt = 2 * (l_max + 1)
+    x, _ = np.polynomial.legendre.leggauss(nt)
+    th = np.arccos(x[::-1])[:, None]
+    ph = 2 * np.pi * np.arange(nt)[None, :] / nt
+    c = rng.uniform(0, 2 * np.pi, n_det)
+    fp = np.stack([0.5 * (1 + np.cos(th) ** 2) * np.cos(2 * ph + c[k]) + 0.1 * k for k in range(n_det)])
+    fc = np.stack([np.cos(th) * np.sin(2 * ph + c[k]) for k in range(n_det)])
+    return np.ascontiguousarray(fp), np.ascontiguousarray(fc)
+
+
 def full_from_half(half, n: int) -> np.ndarray:
     """Hermitian completion of n/2+1 bins to n bins (last axis)."""
     half = np.asarray(half)
