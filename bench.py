@@ -384,7 +384,9 @@ def projection_report(S, n_seg: int = 1024, reps: int = 3):
     transform (every bin's projection mesh, analysis, rotation and product,
     3 baselines x 4096 bins at l_max 32, on the GPU) and the batched
     integration with the resulting non-polar kernels (complex contraction
-    over all bins, 8 B n (l_max+1)^2 flops per segment) in FP32 and FP64.
+    over all bins, 8 B n (l_max+1)^2 flops per segment) on the tensor cores
+    (bf16x3: three bf16 MMAs per product, so the tensor pipe does 3x the
+    reported flops) and in FP32 and FP64 on CUDA cores.
     Antenna patterns are smooth synthetic stand-ins (no LAL here)."""
     import ctypes as C
     import torch
@@ -404,7 +406,7 @@ def projection_report(S, n_seg: int = 1024, reps: int = 3):
     g = torch.rand(n_seg, dtype=torch.float64, device="cuda") * 6.28
     out = {"plan_transform_s": t_plan, "segments": n_seg}
     flops = 8.0 * 3 * n * (L_MAX + 1) ** 2 * n_seg
-    for prec in ("fp32", "fp64"):
+    for prec in ("bf16x3", "fp32", "fp64"):
         bp = S.BatchPlan(net, prec)
         sky = bp.integrate(F, g)
         torch.cuda.synchronize()

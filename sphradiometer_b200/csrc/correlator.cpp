@@ -672,8 +672,8 @@ struct sphrad_batch_plan {
 static sphrad_batch_plan *batch_plan_new_nonpolar(const struct correlator_network_plan_fd *plan, int precision)
 {
 	const int nb = plan->baselines->n_baselines;
-	if(precision != SPHRAD_PREC_FP64 && precision != SPHRAD_PREC_FP32) {
-		set_error("sphrad_batch_plan_new: plans with non-polar delay kernels run in FP64 or FP32");
+	if(precision != SPHRAD_PREC_FP64 && precision != SPHRAD_PREC_FP32 && precision != SPHRAD_PREC_BF16X3) {
+		set_error("sphrad_batch_plan_new: plans with non-polar delay kernels run in FP64, FP32 or bf16x3");
 		return NULL;
 	}
 	const unsigned L = plan->plans[0]->delay_product->l_max;
@@ -693,7 +693,7 @@ static sphrad_batch_plan *batch_plan_new_nonpolar(const struct correlator_networ
 		rot[b] = (const double *) rotation_plan_flat_for(p->rotation_plan, scratch[b]);
 	}
 	void *np = np_plan_create(instrument_array_len(plan->baselines->baselines[0]->instruments), nb, bi.data(), bj.data(), n, L, D.data(), rot.data(),
-				  precision == SPHRAD_PREC_FP64);
+				  precision);
 	if(!np)
 		return NULL;
 	sphrad_batch_plan *bp = (sphrad_batch_plan *) malloc(sizeof(*bp));
@@ -767,13 +767,16 @@ extern "C" void sphrad_batch_plan_free(sphrad_batch_plan *p)
 
 extern "C" unsigned sphrad_batch_plan_l_max(const sphrad_batch_plan *p) { return p->impl ? batch_plan_l_max(p->impl) : np_plan_l_max(p->np); }
 extern "C" int sphrad_batch_plan_bins(const sphrad_batch_plan *p) { return p->impl ? batch_plan_bins(p->impl) : np_plan_n(p->np); }
-extern "C" size_t sphrad_batch_workspace_size(const sphrad_batch_plan *p, int n_seg) { return p->impl ? batch_workspace_bytes(p->impl, n_seg) : 0; }
+extern "C" size_t sphrad_batch_workspace_size(const sphrad_batch_plan *p, int n_seg)
+{
+	return p->impl ? batch_workspace_bytes(p->impl, n_seg) : np_ws_bytes(p->np, n_seg);
+}
 
 extern "C" int sphrad_batch_integrate(sphrad_batch_plan *p, const void *fseries_dev, int n_seg, long long ld, const double *gmst_dev, void *sky_dev, void *workspace,
 				      size_t workspace_bytes, void *stream)
 {
 	if(!p->impl)
-		return np_run(p->np, fseries_dev, n_seg, ld, gmst_dev, sky_dev, stream);
+		return np_run(p->np, fseries_dev, n_seg, ld, gmst_dev, sky_dev, workspace, workspace_bytes, stream);
 	return batch_run(p->impl, fseries_dev, n_seg, ld, gmst_dev, sky_dev, workspace, workspace_bytes, stream, 0);
 }
 
@@ -912,7 +915,7 @@ extern "C" int sphrad_batch_status(sphrad_batch_plan *p)
 {
 	unsigned code = 0;
 	if(!p->impl)
-		return 0;  // the non-polar path has no device-side waits
+		return np_status(p->np);
 	if(batch_check_error(p->impl, &code))
 		return -1;
 	return (int) code;

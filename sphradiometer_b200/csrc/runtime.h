@@ -131,13 +131,16 @@ int projection_multiply(int n, unsigned L, int n_det, const double *fp_host, con
 // ---- batched integration with non-polar kernels (nonpolar.cu) ---------
 // D[b]: host [n][(L+1)^2] complex non-polar delay kernels; rot[b]: host
 // flat Wigner plans up to L; fp64: contraction arithmetic (else FP32)
-void *np_plan_create(int n_det, int B, const int *bi, const int *bj, int n, unsigned L, const double *const *D, const double *const *rot, int fp64);
+void *np_plan_create(int n_det, int B, const int *bi, const int *bj, int n, unsigned L, const double *const *D, const double *const *rot, int precision);
 void np_plan_destroy(void *plan);
 unsigned np_plan_l_max(const void *plan);
 int np_plan_n(const void *plan);
 // F: device [n_det][S][ld] complex full spectra (ld >= n); sky device
-// [S][(L+1)^2]; gmst device [S] or NULL; asynchronous on stream
-int np_run(void *plan, const void *F, int S, long long ld, const double *gmst, void *sky, void *stream);
+// [S][(L+1)^2]; gmst device [S] or NULL; ws: np_ws_bytes (the split
+// operand of the bf16x3 path, 0 otherwise); asynchronous on stream
+size_t np_ws_bytes(const void *plan, int S);
+int np_run(void *plan, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream);
+int np_status(void *plan);  // 0, or the code of a device wait that gave up
 
 // ---- uneven batches (uneven.cu) -----------------------------------------
 // F[d][i][k] = in[in_off[seg[i]] + det[d] Ku + k] for a job of S segments

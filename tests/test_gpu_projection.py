@@ -84,16 +84,17 @@ def test_projection_plan_and_integration_match_numpy():
     Fb = rng.normal(size=(3, Sg, n)) + 1j * rng.normal(size=(3, Sg, n))
     gm = rng.uniform(0, 2 * np.pi, Sg)
     refs = np.array([O.rotate_z(net.integrate(Fb[:, s, :]), L, False, gm[s]) for s in range(Sg)])
-    for prec, tol in (("fp64", 1e-12), ("fp32", 1e-5)):
+    for prec, tol in (("fp64", 1e-12), ("fp32", 1e-5), ("bf16x3", 1e-5)):
         bp = S.BatchPlan(net, prec)
         assert bp.l_max == L and bp.bins == n
         got = bp.integrate(torch.from_numpy(np.ascontiguousarray(Fb)).cuda(), torch.from_numpy(gm).cuda()).cpu().numpy()
         err = np.linalg.norm(got - refs) / np.linalg.norm(refs)
-        assert err < tol, (prec, err)
-        assert bp.status() == 0 and bp.kernels_per_call() == 1
+        worst = max(np.linalg.norm(got[s] - refs[s]) / np.linalg.norm(refs[s]) for s in range(Sg))
+        assert err < tol and worst < 3 * tol, (prec, err, worst)
+        assert bp.status() == 0
         bp.close()
     with pytest.raises(S.SphradError):
-        S.BatchPlan(net, "bf16x3")
+        S.BatchPlan(net, "bf16x6")
     net.close()
 
 
@@ -108,4 +109,38 @@ def test_projection_refuses_mixed_plans():
     assert L_.sphrad_network_plan_mult_by_projection(net.plan, 1.0, fp.ctypes.data, fp.ctypes.data, C.cast(rows, C.c_void_p)) == 0
     # a second projection needs polar kernels: refused
     assert L_.sphrad_network_plan_mult_by_projection(net.plan, 1.0, fp.ctypes.data, fp.ctypes.data, C.cast(rows, C.c_void_p)) < 0
+    net.close()
+
+
+def test_nonpolar_tensor_core_path_across_tiles():
+    """The bf16x3 path of projected plans over several 128-segment tiles,
+    two 256-column tiles and 24 K stages, against the FP64 batched path
+    (itself checked against the drop-in integrator above)."""
+    import torch
+    import sphradiometer_b200 as S
+    L_ = S.load()
+    rng = np.random.default_rng(21)
+    pos = W.random_positions(3, 0.02, W.rng_for(7))
+    n, dt, L = 256, 1.0 / 512, 12
+    net = S.Network(pos, n, dt, l_max=L)
+    assert all(net.baseline_l_max(k) == L for k in range(3))
+    fp, fc = W.pattern_meshes(L, 3, rng)
+    psd = rng.uniform(0.5, 2.0, size=(n, 3))
+    rows = (C.POINTER(C.c_double) * n)(*[np.ctypeslib.as_ctypes(psd[j]) for j in range(n)])
+    assert L_.sphrad_network_plan_mult_by_projection(net.plan, 0.4, fp.ctypes.data, fc.ctypes.data, C.cast(rows, C.c_void_p)) == 0
+    Sg = 300
+    Fb = torch.from_numpy(np.ascontiguousarray(rng.normal(size=(3, Sg, n)) + 1j * rng.normal(size=(3, Sg, n)))).cuda()
+    gm = torch.from_numpy(rng.uniform(0, 2 * np.pi, Sg)).cuda()
+    ref = S.BatchPlan(net, "fp64")
+    r = ref.integrate(Fb, gm).cpu().numpy()
+    bp = S.BatchPlan(net, "bf16x3")
+    got = bp.integrate(Fb, gm).cpu().numpy()
+    again = bp.integrate(Fb, gm).cpu().numpy()
+    err = np.linalg.norm(got - r) / np.linalg.norm(r)
+    worst = max(np.linalg.norm(got[s] - r[s]) / np.linalg.norm(r[s]) for s in range(Sg))
+    assert err < 1e-5 and worst < 3e-5, (err, worst)
+    assert np.array_equal(got, again)  # no atomics: every call is bit-identical
+    assert bp.status() == 0
+    bp.close()
+    ref.close()
     net.close()
