@@ -16,6 +16,8 @@ stages:
             k_epilogue, scatters)
   fseries   3 x N c1 time series (n = 4096) to whitened half spectra
             (k_rfft_whiten)
+  nonpolar  N segments through projected (non-polar) c1 plans on the
+            tensor cores (k_np_build_a, k_np_tc)
 
 Each stage builds its inputs, runs once untimed, then ``--calls`` times and
 prints the mean device time per call (CUDA events).
@@ -40,7 +42,7 @@ def c1_skies(S, W, n):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("stage", choices=["render", "peaks", "rotate", "product", "mlp", "uneven", "fseries"])
+    ap.add_argument("stage", choices=["render", "peaks", "rotate", "product", "mlp", "uneven", "fseries", "nonpolar"])
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--calls", type=int, default=3)
     args = ap.parse_args()
@@ -93,6 +95,21 @@ def main():
         T = (T / np.linalg.norm(T, axis=1, keepdims=True)).astype(np.float32)
         Xd, Td = torch.from_numpy(X).cuda(), torch.from_numpy(T).cuda()
         run = lambda: p.train_step(Xd, Td, 1e-4)  # noqa: E731
+    elif args.stage == "nonpolar":
+        import ctypes as C
+        pos = W.random_positions(3, W.R_EARTH_S, W.rng_for(2))
+        net = S.Network(pos, 4096, 1.0 / 4096, l_max=32)
+        rng = np.random.default_rng(3)
+        fp, fc = W.pattern_meshes(32, 3, rng)
+        psd = np.ascontiguousarray(rng.uniform(0.5, 2.0, size=(4096, 3)))
+        rows = (C.POINTER(C.c_double) * 4096)(*[np.ctypeslib.as_ctypes(psd[j]) for j in range(4096)])
+        assert S.load().sphrad_network_plan_mult_by_projection(net.plan, 1.0, fp.ctypes.data, fc.ctypes.data, C.cast(rows, C.c_void_p)) == 0
+        bp = S.BatchPlan(net, "bf16x3")
+        F = torch.from_numpy(np.ascontiguousarray(rng.normal(size=(3, n, 4096)) + 1j * rng.normal(size=(3, n, 4096)))).cuda()
+        g = torch.rand(n, dtype=torch.float64, device="cuda")
+        out = torch.empty((n, 33 * 33), dtype=torch.complex128, device="cuda")
+        keep = [net, bp, rows]
+        run = lambda: bp.integrate(F, g, out=out)  # noqa: E731
     elif args.stage == "fseries":
         pos = W.random_positions(3, W.R_EARTH_S, W.rng_for(2))
         b = W.make_tseries_batch(pos, 4096, 1.0 / 4096, 256, seed=5)
