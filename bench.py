@@ -425,6 +425,59 @@ def projection_report(S, n_seg: int = 1024, reps: int = 3):
     return out
 
 
+def td_report(S, reps: int = 5, oracle_samples: int = 1500):
+    """The time-domain correlator on the reference's validation setup
+    (test/correlator_validate.c:222-308: 4 detectors, 512 Hz, one dump
+    interval of samples, square windows of amplitude 1 / (n - 2 transient)),
+    through correlator_network_integrate_power_td from host series (copies
+    inside the timed region), against the oracle's per-sample loop
+    (sample dot products, Gaunt products, windowed sum; one thread) on the
+    first ``oracle_samples`` samples of every baseline."""
+    from oracle import oracle as O
+    from sphradiometer_b200 import workload as W
+    rng = np.random.Generator(np.random.Philox(11))
+    pos = W.random_positions(4, W.R_EARTH_S, rng)
+    dt = 1.0 / 512
+    t0 = time.perf_counter()
+    net = S.TimeDomainNetwork(pos, dt)
+    t_plan = time.perf_counter() - t0
+    sky_l = net.l_max
+    n = int(86164.0 / sky_l / 20 / dt)
+    ts = rng.normal(size=(4, n))
+    wins = []
+    for k in range(net.n_baselines):
+        m = n - 2 * net.transient(k)
+        wins.append(np.full(m, 1.0 / m))
+    sky = net.integrate(ts, wins)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        net.integrate(ts, wins)
+    t = (time.perf_counter() - t0) / reps
+    # oracle on a bounded sample of every baseline, and the library on the same
+    el, got, ref, k = 0.0, 0.0, 0.0, 0
+    for i in range(1, 4):
+        for j in range(i):
+            b = net.baseline(k)
+            d = np.array([b.d.contents.data[q] for q in range(3)])
+            dl = float(np.linalg.norm(d))
+            pl, tr = net.power_l_max(k), net.transient(k)
+            w = np.full(oracle_samples, 1.0 / oracle_samples)
+            Rot = O.rotation_plan(pl, O.rot_matrix(b.theta, b.phi))
+            t1 = time.perf_counter()
+            r = O.baseline_integrate_power_td(ts[i][:oracle_samples + 2 * tr], ts[j][:oracle_samples + 2 * tr], w, dl, dt, pl, Rot)
+            el += time.perf_counter() - t1
+            g = net.integrate_baseline(k, ts[i][:oracle_samples + 2 * tr], ts[j][:oracle_samples + 2 * tr], w)
+            got = max(got, float(np.max(np.abs(g - r))))
+            ref = max(ref, float(np.max(np.abs(r))))
+            k += 1
+    oracle_rate = oracle_samples / el  # network samples/s (all baselines per sample)
+    net.close()
+    return {"detectors": 4, "baselines": 6, "samples": n, "sample_rate_hz": 512, "sky_l_max": sky_l, "plan_s": t_plan,
+            "ms_per_dump": t * 1e3, "samples_per_s": n / t, "sky_abs_max": float(np.max(np.abs(sky))),
+            "oracle_samples_per_s": oracle_rate, "oracle_sample": f"{oracle_samples} samples x 6 baselines, C oracle, 1 thread",
+            "max_rel_err_vs_oracle": got / ref}
+
+
 def c2_report(S, steps: int = 10):
     """Uneven batches: 4096 segments of a 4-detector network, durations
     log-uniform in 0.25-4 s at 4096 Hz (DFT lengths 1024-16384), l_max from
@@ -749,6 +802,7 @@ def run(args):
         if not args.quick:
             extra["c2_uneven"] = guarded(c2_report, S)
             extra["projection_path"] = guarded(projection_report, S)
+            extra["time_domain_correlator"] = guarded(td_report, S)
             extra["c3_sh_algebra"] = guarded(c3_report, S)
             extra["c4_learned_proposal"] = guarded(c4_report, S)
 

@@ -14,14 +14,24 @@
  * writes into delay_product->coeff directly must call
  * sphrad_b200_plan_fd_touch() afterwards.
  *
- * The time-domain plans and integrators (correlator_plan_td_*,
- * correlator_*_integrate_power_td) and the FFTW plan helpers
- * (correlator_*tseries_to_fseries*) are not part of this library.
+ * Time-domain plans keep the reference's fields too: proj_a and proj_b
+ * are the polar projection matrices of the phase centres +-|d|/2 z-hat,
+ * built on the GPU.  The time-domain integrator reads proj_a, proj_b and
+ * rotation_plan on every call; it forms all samples' series, the
+ * window-weighted sum of their outer products and the Gaunt contraction
+ * of that sum as FP64 CUDA kernels, so the per-sample scratch series
+ * (sample_a, sample_b, product) are allocated with the reference's shapes
+ * but not written.  power_1d receives the unrotated integrated power, as
+ * in the reference.
+ *
+ * The FFTW plan helpers (correlator_*tseries_to_fseries*) are not part of
+ * this library; sphrad_fseries_* in sphradiometer_b200.h replace them.
  */
 #ifndef SPHRADIOMETER_B200_CORRELATOR_H
 #define SPHRADIOMETER_B200_CORRELATOR_H
 
 #include <sphradiometer/instrument.h>
+#include <sphradiometer/projection.h>
 #include <sphradiometer/sh_series.h>
 
 #ifdef __cplusplus
@@ -37,6 +47,21 @@ struct correlator_baseline {
 	gsl_vector *d;
 	double theta;
 	double phi;
+};
+
+/* reference correlator.h:79-91 */
+struct correlator_plan_td {
+	const struct correlator_baseline *baseline;
+	double delta_t;
+	int transient;
+	struct sh_series_array *proj_a;
+	struct sh_series_array *proj_b;
+	struct sh_series *sample_a;
+	struct sh_series *sample_b;
+	struct sh_series *product;
+	struct sh_series *power_1d;
+	struct sh_series_product_plan *product_plan;
+	struct sh_series_rotation_plan *rotation_plan;
 };
 
 /* reference correlator.h:548-556 */
@@ -56,6 +81,12 @@ struct correlator_network_baselines {
 	int n_baselines;
 };
 
+/* reference correlator.h:138-141 */
+struct correlator_network_plan_td {
+	struct correlator_network_baselines *baselines;
+	struct correlator_plan_td **plans;
+};
+
 /* reference correlator.h:586-589 */
 struct correlator_network_plan_fd {
 	struct correlator_network_baselines *baselines;
@@ -72,10 +103,6 @@ int correlator_transient(const struct sh_series_array *, const struct sh_series_
 double *correlator_tukey_window_new(int, int, int, double);
 double *correlator_square_window_new(int, int, double);
 
-/* projection matrix sizing (reference projection.h, projection.c:56-87) */
-int projection_matrix_n_elements(double, double);
-unsigned int projection_matrix_l_max(double, double);
-
 /* baselines (reference correlator.h:657-671, correlator.c:262-322, 720-818) */
 struct correlator_baseline *correlator_baseline_new(const struct instrument_array *, int, int);
 void correlator_baseline_free(struct correlator_baseline *);
@@ -84,6 +111,19 @@ struct correlator_network_baselines *correlator_network_baselines_new(const stru
 void correlator_network_baselines_free(struct correlator_network_baselines *);
 struct correlator_network_baselines *correlator_network_baselines_copy(const struct correlator_network_baselines *);
 unsigned int correlator_network_l_max(struct correlator_network_baselines *, double);
+
+/* TD plans (reference correlator.h:238-249, correlator.c:325-418, 820-858) */
+struct correlator_plan_td *correlator_plan_td_new(const struct correlator_baseline *, double);
+void correlator_plan_td_free(struct correlator_plan_td *);
+struct correlator_network_plan_td *correlator_network_plan_td_new(struct correlator_network_baselines *, double);
+void correlator_network_plan_td_free(struct correlator_network_plan_td *);
+
+/* TD integrators (reference correlator.h:263, 269; correlator.c:648-673,
+ * 967-984).  The baseline integrator returns NULL when n is below
+ * 2 * transient; the network one when the sky's l_max is below a
+ * baseline's power l_max or the sky is polar. */
+struct sh_series *correlator_baseline_integrate_power_td(const double *, const double *, const double *, int, struct correlator_plan_td *);
+struct sh_series *correlator_network_integrate_power_td(struct sh_series *, double **, int, double **, struct correlator_network_plan_td *);
 
 /* FD plans (reference correlator.h:682-697, correlator.c:424-591, 866-959).
  * correlator_plan_fd_new() builds the plan at the baseline's native

@@ -85,6 +85,8 @@ def lib():
         L.orc_projection_taps.argtypes = [d, d, i, u, _dp]
         L.orc_delay_product.restype = i
         L.orc_delay_product.argtypes = [d, d, i, u, _cp]
+        L.orc_baseline_integrate_power_td.restype = i
+        L.orc_baseline_integrate_power_td.argtypes = [_dp, _dp, _dp, i, d, d, u, _cp, _cp]
         L.orc_baseline_integrate_power_fd.restype = i
         L.orc_baseline_integrate_power_fd.argtypes = [_cp, _cp, i, _cp, u, _cp, _cp]
         L.orc_vector_direction.argtypes = [_dp, C.POINTER(d), C.POINTER(d)]
@@ -298,6 +300,24 @@ def baseline_integrate_power_fd(a, b, D, l_max, Rot) -> np.ndarray:
     n = len(a)
     rc = lib().orc_baseline_integrate_power_fd(_c(a), _c(b), n, _c(D).ravel(), l_max, _c(Rot), out)
     assert rc == 0
+    return out
+
+
+def td_power_l_max(d_len: float, dt: float) -> int:
+    """correlator.c:336-339: the time-domain plan's power l_max."""
+    return min(power_l_max_naive(d_len, dt), 2 * projection_l_max(d_len / 2, dt))
+
+
+def baseline_integrate_power_td(a, b, window, d_len: float, dt: float, l_max: int, Rot) -> np.ndarray:
+    """Time-domain cross power of one baseline (correlator.c:648-673),
+    rotated with the flat rotation plan Rot of degree l_max."""
+    out = np.zeros(length(l_max, False), np.complex128)
+    a = np.ascontiguousarray(a, np.float64)
+    b = np.ascontiguousarray(b, np.float64)
+    w = np.ascontiguousarray(window, np.float64)
+    rc = lib().orc_baseline_integrate_power_td(a, b, w, len(a), d_len, dt, l_max, _c(Rot), out)
+    if rc:
+        raise ValueError("time series shorter than twice the transient")
     return out
 
 

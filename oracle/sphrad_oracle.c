@@ -893,6 +893,68 @@ int orc_network_integrate_power_fd(int n_det, const double complex *const *fseri
 	return 0;
 }
 
+/* correlator.c:325-400 and 648-673: the time-domain correlator of a
+ * baseline of length d_len (seconds), as the reference runs it.  The
+ * projections are the polar taps of +-d_len/2 z-hat; for each of the
+ * n - 2 transient samples the two samples' series are formed
+ * (sh_series_array_dot, sh_series_array.c:407-426), multiplied with the
+ * Gaunt microcode (sh_series_product.c:250-266) into degree
+ * min(l_max, 2 a_l_max) and added, times the window, into power_1d,
+ * which is then rotated with Rot.  l_max is the plan's power l_max.
+ * Returns -1 when n < 2 transient. */
+int orc_baseline_integrate_power_td(const double *a, const double *b, const double *window, int n, double d_len, double delta_t, unsigned l_max,
+				    const double complex *Rot, double complex *power_2d)
+{
+	const double r = d_len / 2;
+	const unsigned a_l = orc_projection_l_max(r, delta_t);
+	const int n_el = orc_projection_n_elements(r, delta_t);
+	const int transient = (n_el - 1) / 2;
+	const int T = n - 2 * transient;
+	if(T < 0 || delta_t <= 0)
+		return -1;
+	const int A = a_l + 1;
+	const unsigned dl = l_max < 2 * a_l ? l_max : 2 * a_l;
+	double *ta = malloc((size_t) n_el * A * sizeof(*ta));
+	double *tb = malloc((size_t) n_el * A * sizeof(*tb));
+	orc_projection_taps(+r, delta_t, n_el, a_l, ta);
+	orc_projection_taps(-r, delta_t, n_el, a_l, tb);
+	const long n_ops = orc_product_plan_length(dl, 1, a_l, 1, a_l, 1);
+	double *f = malloc((n_ops ? n_ops : 1) * sizeof(*f));
+	int *d_off = malloc((n_ops ? n_ops : 1) * sizeof(*d_off));
+	int *a_off = malloc((n_ops ? n_ops : 1) * sizeof(*a_off));
+	int *b_off = malloc((n_ops ? n_ops : 1) * sizeof(*b_off));
+	orc_product_plan(dl, 1, a_l, 1, a_l, 1, f, d_off, a_off, b_off);
+	double complex *sa = malloc(A * sizeof(*sa)), *sb = malloc(A * sizeof(*sb));
+	double complex *prod = malloc((dl + 1) * sizeof(*prod));
+	double complex *p1 = calloc(l_max + 1, sizeof(*p1));
+	for(int t = 0; t < T; t++) {
+		for(int l = 0; l < A; l++)
+			sa[l] = sb[l] = 0.0;
+		for(int e = 0; e < n_el; e++) {
+			const double va = a[t + e], vb = b[t + e];
+			for(int l = 0; l < A; l++) {
+				sa[l] += ta[(size_t) e * A + l] * va;
+				sb[l] += tb[(size_t) e * A + l] * vb;
+			}
+		}
+		orc_product_microcode(prod, dl, 1, sa, sb, n_ops, f, d_off, a_off, b_off);
+		for(unsigned l = 0; l <= dl; l++)
+			p1[l] += window[t] * prod[l];
+	}
+	const int rc = orc_rotate(power_2d, p1, l_max, 1, Rot);
+	free(p1);
+	free(prod);
+	free(sb);
+	free(sa);
+	free(b_off);
+	free(a_off);
+	free(d_off);
+	free(f);
+	free(tb);
+	free(ta);
+	return rc;
+}
+
 /* instrument.c:90-100 */
 void orc_vector_direction(const double *v, double *theta, double *phi)
 {

@@ -80,6 +80,8 @@ int orc_delay_product(double d_len, double delta_t, int n, unsigned l_max, doubl
 /* correlator (correlator.c:681-711, 993-1010).  D is the baseline's
  * n x (l_max + 1) polar delay table, Rot its rotation plan. */
 int orc_baseline_integrate_power_fd(const double complex *a, const double complex *b, int n, const double complex *D, unsigned l_max, const double complex *Rot, double complex *power_2d);
+int orc_baseline_integrate_power_td(const double *a, const double *b, const double *window, int n, double d_len, double delta_t, unsigned l_max,
+				    const double complex *Rot, double complex *power_2d);
 int orc_network_integrate_power_fd(int n_det, const double complex *const *fseries, int n, const double complex *const *D, unsigned l_max, const double complex *const *Rot, double complex *sky);
 
 /* baseline geometry: instrument.c:90-100, 210-218 */

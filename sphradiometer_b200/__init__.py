@@ -129,6 +129,113 @@ class Network:
             pass
 
 
+class TimeDomainNetwork:
+    """A detector network with its time-domain correlation plan
+    (correlator_network_plan_td_new, correlator.c:820-858).
+
+    ``positions``: n_det x 3 phase centres in light-seconds.
+    """
+
+    def __init__(self, positions, delta_t: float):
+        L = load()
+        self.delta_t = float(delta_t)
+        self._inst = _check(L.instrument_array_new(0), "instrument_array_new")
+        for p in np.asarray(positions, np.float64):
+            _check(L.instrument_array_append(self._inst, _check(L.instrument_new(p[0], p[1], p[2], None), "instrument_new")),
+                   "instrument_array_append")
+        self._bl = _check(L.correlator_network_baselines_new(self._inst), "correlator_network_baselines_new")
+        self._plan = _check(L.correlator_network_plan_td_new(self._bl, self.delta_t), "correlator_network_plan_td_new")
+        self.n_baselines = self._bl.contents.n_baselines
+
+    def baseline(self, k: int):
+        return self._bl.contents.baselines[k].contents
+
+    def plan_td(self, k: int):
+        return self._plan.contents.plans[k]
+
+    def transient(self, k: int) -> int:
+        return self.plan_td(k).contents.transient
+
+    def power_l_max(self, k: int) -> int:
+        return self.plan_td(k).contents.power_1d.contents.l_max
+
+    @property
+    def l_max(self) -> int:
+        return max(self.power_l_max(k) for k in range(self.n_baselines))
+
+    def projections(self, k: int):
+        p = self.plan_td(k).contents
+        return array_to_numpy(p.proj_a), array_to_numpy(p.proj_b)
+
+    def rotation_flat(self, k: int) -> np.ndarray:
+        return rotation_plan_flat(self.plan_td(k).contents.rotation_plan)
+
+    def integrate(self, tseries, windows, sky_l_max: int | None = None) -> np.ndarray:
+        """correlator_network_integrate_power_td: tseries is n_det x n
+        samples, windows one array of n - 2 transient weights per baseline.
+        Returns the sky a_lm."""
+        L = load()
+        ts = [np.ascontiguousarray(t, np.float64) for t in tseries]
+        ws = [np.ascontiguousarray(w, np.float64) for w in windows]
+        tp = (C.c_void_p * len(ts))(*[t.ctypes.data for t in ts])
+        wp = (C.c_void_p * len(ws))(*[w.ctypes.data for w in ws])
+        lm = self.l_max if sky_l_max is None else sky_l_max
+        sky = _check(L.sh_series_new_zero(lm, 0), "sh_series_new_zero")
+        try:
+            _check(L.correlator_network_integrate_power_td(sky, tp, len(ts[0]), wp, self._plan), "correlator_network_integrate_power_td")
+            return series_to_numpy(sky)
+        finally:
+            L.sh_series_free(sky)
+
+    def integrate_baseline(self, k: int, a, b, window) -> np.ndarray:
+        """correlator_baseline_integrate_power_td of baseline k."""
+        L = load()
+        a = np.ascontiguousarray(a, np.float64)
+        b = np.ascontiguousarray(b, np.float64)
+        w = np.ascontiguousarray(window, np.float64)
+        out = _check(L.correlator_baseline_integrate_power_td(a.ctypes.data, b.ctypes.data, w.ctypes.data, len(a), self.plan_td(k)),
+                     "correlator_baseline_integrate_power_td")
+        try:
+            return series_to_numpy(out)
+        finally:
+            L.sh_series_free(out)
+
+    def close(self):
+        L = load()
+        if getattr(self, "_plan", None):
+            L.correlator_network_plan_td_free(self._plan)
+            self._plan = None
+        if getattr(self, "_bl", None):
+            L.correlator_network_baselines_free(self._bl)
+            self._bl = None
+        if getattr(self, "_inst", None):
+            L.instrument_array_free(self._inst)
+            self._inst = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def projection_matrix_delay(phase_centre, n: int, l_max: int, delta_t: float) -> np.ndarray:
+    """projection_matrix_delay (projection.c:110-131): n x length(l_max,
+    polar) coefficients of the sinc delay taps of a phase centre
+    (light-seconds); polar when it lies on the z axis."""
+    L = load()
+    p = np.asarray(phase_centre, np.float64)
+    inst = _check(L.instrument_new(p[0], p[1], p[2], None), "instrument_new")
+    try:
+        arr = _check(L.projection_matrix_delay(int(n), int(l_max), inst.contents.phase_centre, float(delta_t)), "projection_matrix_delay")
+        try:
+            return array_to_numpy(arr)
+        finally:
+            L.sh_series_array_free(arr)
+    finally:
+        L.instrument_free(inst)
+
+
 class BatchPlan:
     """Batched device-resident integrator over a Network (sphrad_batch_*).
 

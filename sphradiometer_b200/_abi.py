@@ -56,6 +56,14 @@ class correlator_plan_fd(C.Structure):
                 ("power_1d", C.POINTER(sh_series)), ("rotation_plan", C.POINTER(sh_series_rotation_plan))]
 
 
+class correlator_plan_td(C.Structure):
+    _fields_ = [("baseline", C.POINTER(correlator_baseline)), ("delta_t", C.c_double), ("transient", C.c_int),
+                ("proj_a", C.POINTER(sh_series_array)), ("proj_b", C.POINTER(sh_series_array)),
+                ("sample_a", C.POINTER(sh_series)), ("sample_b", C.POINTER(sh_series)), ("product", C.POINTER(sh_series)),
+                ("power_1d", C.POINTER(sh_series)), ("product_plan", C.c_void_p),
+                ("rotation_plan", C.POINTER(sh_series_rotation_plan))]
+
+
 class correlator_network_baselines(C.Structure):
     _fields_ = [("baselines", C.POINTER(C.POINTER(correlator_baseline))), ("n_baselines", C.c_int)]
 
@@ -63,6 +71,11 @@ class correlator_network_baselines(C.Structure):
 class correlator_network_plan_fd(C.Structure):
     _fields_ = [("baselines", C.POINTER(correlator_network_baselines)),
                 ("plans", C.POINTER(C.POINTER(correlator_plan_fd)))]
+
+
+class correlator_network_plan_td(C.Structure):
+    _fields_ = [("baselines", C.POINTER(correlator_network_baselines)),
+                ("plans", C.POINTER(C.POINTER(correlator_plan_td)))]
 
 
 class _Cplx(C.Structure):
@@ -124,6 +137,7 @@ SIGNATURES = {
     "sh_series_array_reverse_fft": (_P(sh_series_array), [_P(sh_series_array)]),
     # instruments and correlator
     "instrument_new": (_P(instrument), [_d, _d, _d, _vp]),
+    "instrument_free": (None, [_P(instrument)]),
     "instrument_array_new": (_P(instrument_array), [_i]),
     "instrument_array_append": (_P(instrument), [_P(instrument_array), _P(instrument)]),
     "instrument_array_free": (None, [_P(instrument_array)]),
@@ -142,6 +156,16 @@ SIGNATURES = {
     "correlator_baseline_integrate_power_fd": (_P(sh_series), [_vp, _vp, _P(correlator_plan_fd)]),
     "correlator_network_integrate_power_fd": (_P(sh_series), [_P(sh_series), _P(_vp), _P(correlator_network_plan_fd)]),
     "sphrad_b200_plan_fd_touch": (None, [_P(correlator_plan_fd)]),
+    "correlator_plan_td_new": (_P(correlator_plan_td), [_P(correlator_baseline), _d]),
+    "correlator_plan_td_free": (None, [_P(correlator_plan_td)]),
+    "correlator_network_plan_td_new": (_P(correlator_network_plan_td), [_P(correlator_network_baselines), _d]),
+    "correlator_network_plan_td_free": (None, [_P(correlator_network_plan_td)]),
+    "correlator_baseline_integrate_power_td": (_P(sh_series), [_vp, _vp, _vp, _i, _P(correlator_plan_td)]),
+    "correlator_network_integrate_power_td": (_P(sh_series), [_P(sh_series), _P(_vp), _i, _P(_vp), _P(correlator_network_plan_td)]),
+    "projection_matrix_n_elements": (_i, [_d, _d]),
+    "projection_matrix_l_max": (_u, [_d, _d]),
+    "projection_matrix_delay": (_P(sh_series_array), [_u, _u, _P(gsl_vector), _d]),
+    "projection_delay_element": (_d, [_d, _d, _vp]),
     "sphrad_network_plan_mult_by_projection": (_i, [_P(correlator_network_plan_fd), _d, _vp, _vp, _vp]),
     # precalculated plans on disk
     "make_precalc_directories": (_i, [C.c_char_p, _i]),

@@ -11,7 +11,9 @@
 
 #include <cuda_runtime_api.h>
 
+#include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -656,6 +658,232 @@ extern "C" struct sh_series *correlator_network_integrate_power_fd(struct sh_ser
 	if(integrate_fd(jobs.data(), nb, sky->l_max, (double *) sky->coeff))
 		return NULL;
 	note_write(sky->coeff);
+	return sky;
+}
+
+// ------------------------------------------------------------------------
+// projection matrices (projection.c:99-131)
+// ------------------------------------------------------------------------
+extern "C" double projection_delay_element(double theta, double phi, void *data)
+{
+	const struct projection_delay_element_data *e = (const struct projection_delay_element_data *) data;
+	const double pi_x = M_PI * (e->j - e->k - vector_r_dot_s(e->r, theta, phi) / e->delta_t);
+	return pi_x == 0.0 ? 1.0 : sin(pi_x) / pi_x;
+}
+
+extern "C" struct sh_series_array *projection_matrix_delay(unsigned int n, unsigned int l_max, const gsl_vector *phase_centre, double delta_t)
+{
+	const double r[3] = {vget(phase_centre, 0), vget(phase_centre, 1), vget(phase_centre, 2)};
+	const int polar = r[0] == 0.0 && r[1] == 0.0;
+	struct sh_series_array *m = sh_series_array_new((int) n, l_max, polar);
+	if(!m || n == 0)
+		return m;
+	const size_t len = length(l_max, polar);
+	int rc;
+	if(polar) {
+		std::vector<double> taps((size_t) n * len);
+		rc = projection_taps(r[2], delta_t, (int) n, (int) len, taps.data());
+		if(!rc)
+			for(size_t i = 0; i < n; i++)
+				for(size_t l = 0; l < len; l++)
+					m->coeff[i * m->stride + l] = taps[i * len + l];
+	} else {
+		std::vector<dcplx> full((size_t) n * len);
+		rc = projection_taps_full(r, delta_t, (int) n, l_max, (double *) full.data());
+		if(!rc)
+			for(size_t i = 0; i < n; i++)
+				memcpy(m->coeff + i * m->stride, full.data() + i * len, len * sizeof(dcplx));
+	}
+	if(rc) {
+		sh_series_array_free(m);
+		return NULL;
+	}
+	return m;
+}
+
+// ------------------------------------------------------------------------
+// time-domain plans and integrators (correlator.c:325-418, 648-673,
+// 820-858, 967-984)
+// ------------------------------------------------------------------------
+extern "C" void correlator_plan_td_free(struct correlator_plan_td *p)
+{
+	if(p) {
+		sh_series_rotation_plan_free(p->rotation_plan);
+		sh_series_product_plan_free(p->product_plan);
+		sh_series_free(p->power_1d);
+		sh_series_free(p->product);
+		sh_series_free(p->sample_b);
+		sh_series_free(p->sample_a);
+		sh_series_array_free(p->proj_b);
+		sh_series_array_free(p->proj_a);
+	}
+	free(p);
+}
+
+extern "C" struct correlator_plan_td *correlator_plan_td_new(const struct correlator_baseline *baseline, double delta_t)
+{
+	if(!(delta_t > 0)) {
+		set_error("correlator_plan_td_new: bad sample interval %g", delta_t);
+		return NULL;
+	}
+	const double d_len = vector_magnitude(baseline->d);
+	const unsigned a_l = projection_matrix_l_max(d_len / 2, delta_t), b_l = a_l;
+	// power_l_max need not exceed a_l_max + b_l_max (correlator.c:336-339)
+	unsigned P = correlator_baseline_power_l_max(baseline, delta_t);
+	if(P > a_l + b_l)
+		P = a_l + b_l;
+	const int n_el = projection_matrix_n_elements(d_len / 2, delta_t);
+	struct correlator_plan_td *p = (struct correlator_plan_td *) calloc(1, sizeof(*p));
+	gsl_vector *dp = vec3_alloc();
+	double *R = sh_series_rot_matrix(baseline->theta, baseline->phi);
+	if(!p || !dp || !R)
+		goto fail;
+	p->baseline = baseline;
+	p->delta_t = delta_t;
+	// phase centres +|d|/2 z-hat and -|d|/2 z-hat
+	vset(dp, 2, +d_len / 2);
+	p->proj_a = projection_matrix_delay(n_el, a_l, dp, delta_t);
+	vset(dp, 2, -d_len / 2);
+	p->proj_b = projection_matrix_delay(n_el, b_l, dp, delta_t);
+	p->sample_a = sh_series_new_zero(a_l, 1);
+	p->sample_b = sh_series_new_zero(b_l, 1);
+	p->product = sh_series_new_zero(P, 1);
+	p->power_1d = sh_series_new_zero(P, 1);
+	if(!p->proj_a || !p->proj_b || !p->sample_a || !p->sample_b || !p->product || !p->power_1d)
+		goto fail;
+	p->product_plan = sh_series_product_plan_new(p->power_1d, p->sample_a, p->sample_b);
+	p->rotation_plan = sh_series_rotation_plan_new(p->power_1d, R);
+	if(!p->product_plan || !p->rotation_plan)
+		goto fail;
+	p->transient = correlator_transient(p->proj_a, p->proj_b);
+	free(R);
+	vec3_free(dp);
+	return p;
+fail:
+	free(R);
+	vec3_free(dp);
+	correlator_plan_td_free(p);
+	return NULL;
+}
+
+extern "C" struct correlator_network_plan_td *correlator_network_plan_td_new(struct correlator_network_baselines *baselines, double delta_t)
+{
+	struct correlator_network_plan_td *p = (struct correlator_network_plan_td *) malloc(sizeof(*p));
+	struct correlator_plan_td **plans = (struct correlator_plan_td **) calloc(baselines->n_baselines > 0 ? baselines->n_baselines : 1, sizeof(*plans));
+	if(!p || !plans) {
+		free(p);
+		free(plans);
+		return NULL;
+	}
+	for(int i = 0; i < baselines->n_baselines; i++) {
+		plans[i] = correlator_plan_td_new(baselines->baselines[i], delta_t);
+		if(!plans[i]) {
+			while(--i >= 0)
+				correlator_plan_td_free(plans[i]);
+			free(plans);
+			free(p);
+			return NULL;
+		}
+	}
+	p->baselines = baselines;
+	p->plans = plans;
+	return p;
+}
+
+extern "C" void correlator_network_plan_td_free(struct correlator_network_plan_td *p)
+{
+	if(p) {
+		for(int i = 0; i < p->baselines->n_baselines; i++)
+			correlator_plan_td_free(p->plans[i]);
+		free(p->plans);
+	}
+	free(p);
+}
+
+// contiguous complex copy of an array's series (stride may exceed length)
+static std::vector<dcplx> array_taps(const struct sh_series_array *a)
+{
+	const size_t len = length(a->l_max, a->polar);
+	std::vector<dcplx> out((size_t) a->n * len);
+	for(int i = 0; i < a->n; i++)
+		memcpy(out.data() + (size_t) i * len, a->coeff + (size_t) i * a->stride, len * sizeof(dcplx));
+	return out;
+}
+
+// power_1d of one baseline over n samples (correlator.c:648-668)
+static int td_power(const double *a, const double *b, const double *window, int n, struct correlator_plan_td *plan)
+{
+	const struct sh_series_array *pa = plan->proj_a, *pb = plan->proj_b;
+	struct sh_series *p1 = plan->power_1d;
+	if(!pa->polar || !pb->polar || !p1->polar || pa->l_max != plan->sample_a->l_max || pb->l_max != plan->sample_b->l_max) {
+		set_error("correlator_baseline_integrate_power_td: plan's projections and series disagree");
+		return -1;
+	}
+	const int T = n - 2 * plan->transient;
+	if(T < 0) {
+		set_error("correlator_baseline_integrate_power_td: %d samples, transient %d", n, plan->transient);
+		return -1;
+	}
+	if(pa->n > 2 * plan->transient + 1 || pb->n > 2 * plan->transient + 1) {
+		set_error("correlator_baseline_integrate_power_td: projections longer than the transient allows");
+		return -1;
+	}
+	// the product stops at min(power_1d l_max, a_l_max + b_l_max)
+	// (sh_series_product_plan_new); higher degrees stay zero
+	const unsigned Lp = std::min(p1->l_max, pa->l_max + pb->l_max);
+	const std::vector<dcplx> ta = array_taps(pa), tb = array_taps(pb);
+	const long long n_x = (long long) T + std::max(pa->n, pb->n) - 1;
+	sh_series_zero(p1);
+	if(td_power_1d(T, pa->n, pb->n, (int) pa->l_max + 1, (int) pb->l_max + 1, (const double *) ta.data(), (const double *) tb.data(), a, b, n_x, window, Lp,
+		       (double *) p1->coeff))
+		return -1;
+	note_write(p1->coeff);
+	return 0;
+}
+
+extern "C" struct sh_series *correlator_baseline_integrate_power_td(const double *a, const double *b, const double *window, int n,
+								    struct correlator_plan_td *plan)
+{
+	if(td_power(a, b, window, n, plan))
+		return NULL;
+	struct sh_series *out = sh_series_new(plan->power_1d->l_max, 0);
+	if(!out || !sh_series_rotate(out, plan->power_1d, plan->rotation_plan)) {
+		sh_series_free(out);
+		return NULL;
+	}
+	return out;
+}
+
+extern "C" struct sh_series *correlator_network_integrate_power_td(struct sh_series *sky, double **tseries, int n, double **windows,
+								   struct correlator_network_plan_td *plan)
+{
+	const int nb = plan->baselines->n_baselines;
+	if(nb <= 0 || sky->polar) {
+		set_error("correlator_network_integrate_power_td: empty network or polar sky");
+		return NULL;
+	}
+	for(int k = 0; k < nb; k++)
+		if(plan->plans[k]->power_1d->l_max > sky->l_max) {
+			set_error("correlator_network_integrate_power_td: sky l_max below a baseline's");
+			return NULL;
+		}
+	const int nd = instrument_array_len(plan->baselines->baselines[0]->instruments);
+	if(nd * (nd - 1) / 2 != nb) {
+		set_error("correlator_network_integrate_power_td: network and instrument count disagree");
+		return NULL;
+	}
+	sh_series_zero(sky);
+	int k = 0;
+	for(int i = 1; i < nd; i++)
+		for(int j = 0; j < i; j++, k++) {
+			struct sh_series *p2 = correlator_baseline_integrate_power_td(tseries[i], tseries[j], windows[k], n, plan->plans[k]);
+			if(!p2)
+				return NULL;
+			const bool ok = sh_series_add(sky, 1.0 / nb, p2) != NULL;
+			sh_series_free(p2);
+			if(!ok)
+				return NULL;
+		}
 	return sky;
 }
 

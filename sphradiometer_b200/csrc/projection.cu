@@ -17,6 +17,7 @@
 // analysis transform, the rotation and the pixel-domain product.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "runtime.h"
@@ -107,6 +108,74 @@ int projection_multiply(int n, unsigned L, int n_det, const double *fp_host, con
 	}
 	sht_plan_destroy(mesh_plan);
 	sht_plan_destroy(prod_plan);
+	return rc;
+}
+
+}  // namespace sphrad
+
+// ------------------------------------------------------------------------
+// projection matrix of an off-axis phase centre (projection.c:99-131): each
+// tap's sinc(pi (-k - r.s / dt)) is sampled on the reference's mesh of
+// l_max L and analysed, a chunk of taps per batched transform
+// ------------------------------------------------------------------------
+namespace sphrad {
+
+namespace {
+
+__global__ void k_delay_mesh(const double *__restrict__ theta, int nt, int nphi, double rx, double ry, double rz, double dt, int k0, int nb,
+			     double2 *__restrict__ mesh)
+{
+	const long long npix = (long long) nt * nphi, total = (long long) nb * npix;
+	for(long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < total; i += (long long) gridDim.x * blockDim.x) {
+		const int c = (int) (i / npix);
+		const long long p = i - (long long) c * npix;
+		const int it = (int) (p / nphi), jp = (int) (p - (long long) it * nphi);
+		double st, ct, sp, cp;
+		sincos(theta[it], &st, &ct);
+		sincospi(2.0 * jp / nphi, &sp, &cp);
+		const double rs = rx * st * cp + ry * st * sp + rz * ct;
+		const double pi_x = M_PI * (0 - (k0 + c) - rs / dt);
+		mesh[i] = make_double2(pi_x == 0.0 ? 1.0 : sin(pi_x) / pi_x, 0.0);
+	}
+}
+
+}  // namespace
+
+int projection_taps_full(const double *r, double delta_t, int n_el, unsigned L, double *series_host)
+{
+	if(!(delta_t > 0) || n_el <= 0) {
+		set_error("projection matrix: bad sample interval %g or %d taps", delta_t, n_el);
+		return -1;
+	}
+	if(ensure_device())
+		return -1;
+	const int nt = 2 * ((int) L + 1), nphi = nt;
+	const size_t len = (size_t) (L + 1) * (L + 1), npix = (size_t) nt * nphi;
+	void *plan = sht_plan_create(L, kGridGL, nt, nphi, 0);
+	if(!plan)
+		return -1;
+	int chunk = (int) std::max<size_t>(1, std::min<size_t>((size_t) 256 << 20, (size_t) 64 * npix * 16) / (npix * 16));
+	if(chunk > n_el)
+		chunk = n_el;
+	int rc = -1;
+	{
+		const size_t scr = sht_scratch_bytes(plan, chunk, (int) L);
+		DevBuf dmesh((size_t) chunk * npix * 16), dout((size_t) chunk * len * 16), dscr(scr);
+		bool ok = dmesh.p && dout.p && dscr.p;
+		void *st = lib_stream();
+		const int k_first = -(n_el - 1) / 2;
+		for(int t0 = 0; ok && t0 < n_el; t0 += chunk) {
+			const int c = n_el - t0 < chunk ? n_el - t0 : chunk;
+			k_delay_mesh<<<592, 256, 0, (cudaStream_t) st>>>(sht_plan_theta_dev(plan), nt, nphi, r[0], r[1], r[2], delta_t, k_first + t0, c,
+									   (double2 *) dmesh.p);
+			ok = cudaGetLastError() == cudaSuccess && !sht_analysis(plan, dmesh.p, c, L, 0, dout.p, (long long) len, dscr.p, st) &&
+			     !d2h(series_host + (size_t) t0 * len * 2, dout.p, (size_t) c * len * 16) && !stream_sync();
+			if(!ok)
+				set_error("projection matrix: GPU stage failed at taps %d..%d", t0, t0 + c - 1);
+		}
+		rc = ok ? 0 : -1;
+	}
+	sht_plan_destroy(plan);
 	return rc;
 }
 

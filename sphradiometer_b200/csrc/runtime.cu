@@ -11,6 +11,7 @@
 //   integration      correlator.c:681-711 and 993-1010
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -919,6 +920,293 @@ int array_dotc(int n, int stride, const double *coeff, const double *vec, int ve
 	if(d2h(result, dout.p, stride * sizeof(double2)))
 		return -1;
 	return stream_sync();
+}
+
+}  // namespace sphrad
+
+namespace sphrad {
+
+// ------------------------------------------------------------------------
+// time-domain correlator (correlator.c:325-400, 648-673)
+//
+// The reference loops over the n - 2 transient samples: it forms each
+// sample's polar series on both sides (sh_series_array_dot of the
+// projection taps with the series from that sample), multiplies them
+// (sh_series_product) and adds the product, times the window, into
+// power_1d.  The product is bilinear, so the window-weighted sum of
+// products is the product contraction of one matrix,
+//     C[l1][l2] = sum_t w[t] Sa[t][l1] Sb[t][l2],
+// and power_1d[L] = sum_{l1,l2} C[l1][l2] int Y_L0 Y_l1,0 Y_l2,0, which a
+// Gauss-Legendre rule in cos(theta) of (P + La + Lb) / 2 + 1 nodes
+// integrates exactly (the quadrature of the pixel-domain product,
+// sh_series_product.c:269-329).  Samples and C are tiled FP64 kernels;
+// the per-sample product loop disappears.
+// ------------------------------------------------------------------------
+int projection_taps(double r, double delta_t, int n_el, int A, double *taps_host)
+{
+	if(!(delta_t > 0) || n_el <= 0 || A <= 0) {
+		set_error("projection taps: bad sample interval %g or shape %d x %d", delta_t, n_el, A);
+		return -1;
+	}
+	const int nt = 2 * A;
+	if(ensure_device())
+		return -1;
+	DBuf x(nt * sizeof(double)), w(nt * sizeof(double)), P((size_t) nt * A * sizeof(double)), PT((size_t) nt * A * sizeof(double)),
+		taps((size_t) n_el * A * sizeof(double));
+	if(!x.p || !w.p || !P.p || !PT.p || !taps.p)
+		return -1;
+	cudaStream_t s = S();
+	k_gl_nodes<<<(nt / 2 + 127) / 128, 128, 0, s>>>(nt, x.as<double>(), w.as<double>());
+	k_plm0_table<<<(nt + 127) / 128, 128, 0, s>>>(nt, x.as<double>(), A, P.as<double>(), PT.as<double>());
+	k_taps<<<n_el, 256, nt * sizeof(double), s>>>(r, delta_t, n_el, A, nt, x.as<double>(), w.as<double>(), P.as<double>(), A, taps.as<double>());
+	CK(cudaGetLastError());
+	if(d2h(taps_host, taps.p, (size_t) n_el * A * sizeof(double)) || stream_sync())
+		return -1;
+	return 0;
+}
+
+namespace {
+
+constexpr int kTdTT = 64, kTdTL = 32, kTdTE = 32;  // samples tile: t x l, taps chunk
+
+// S[t][l] = sum_e taps[e][l] x[t + e], t < T, l < A (sh_series_array_dot
+// from each sample, sh_series_array.c:407-426).  Block: 64 samples x 32
+// harmonics, 256 threads, 8 samples per thread.
+__global__ void __launch_bounds__(256) k_td_samples(int T, int n_el, int A, const double2 *__restrict__ taps, const double *__restrict__ x, double2 *__restrict__ S)
+{
+	__shared__ double2 s_tap[kTdTE][kTdTL];
+	__shared__ double s_x[kTdTT + kTdTE];
+	const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+	const int t0 = blockIdx.x * kTdTT, l0 = blockIdx.y * kTdTL;
+	double2 acc[8];
+#pragma unroll
+	for(int k = 0; k < 8; k++)
+		acc[k] = make_double2(0.0, 0.0);
+	for(int e0 = 0; e0 < n_el; e0 += kTdTE) {
+		for(int i = threadIdx.x; i < kTdTE * kTdTL; i += blockDim.x) {
+			const int e = e0 + i / kTdTL, l = l0 + i % kTdTL;
+			s_tap[i / kTdTL][i % kTdTL] = (e < n_el && l < A) ? taps[(size_t) e * A + l] : make_double2(0.0, 0.0);
+		}
+		// samples with t < T and e < n_el read x below T + n_el - 1, the
+		// length of the staged series; the rest of the window is zero
+		for(int j = threadIdx.x; j < kTdTT + kTdTE; j += blockDim.x) {
+			const long long idx = (long long) t0 + e0 + j;
+			s_x[j] = idx < (long long) T + n_el - 1 ? x[idx] : 0.0;
+		}
+		__syncthreads();
+		const int ne = n_el - e0 < kTdTE ? n_el - e0 : kTdTE;
+		for(int e = 0; e < ne; e++) {
+			const double2 c = s_tap[e][tx];
+#pragma unroll
+			for(int k = 0; k < 8; k++) {
+				const double v = s_x[ty + 8 * k + e];
+				acc[k].x += c.x * v;
+				acc[k].y += c.y * v;
+			}
+		}
+		__syncthreads();
+	}
+	const int l = l0 + tx;
+	if(l < A)
+#pragma unroll
+		for(int k = 0; k < 8; k++) {
+			const int t = t0 + ty + 8 * k;
+			if(t < T)
+				S[(size_t) t * A + l] = acc[k];
+		}
+}
+
+// partial C over the sample range of blockIdx.z:
+// part[z][l1][l2] = sum_t w[t] Sa[t][l1] Sb[t][l2].  Block: 32 x 32
+// outputs, 256 threads, 4 per thread.
+__global__ void __launch_bounds__(256) k_td_cross(int T, int t_per, int Aa, int Ab, const double *__restrict__ w, const double2 *__restrict__ Sa,
+						  const double2 *__restrict__ Sb, double2 *__restrict__ part)
+{
+	__shared__ double2 s_a[32][33];
+	__shared__ double2 s_b[32][32];
+	const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+	const int l10 = blockIdx.y * 32, l20 = blockIdx.x * 32;
+	const int tb = blockIdx.z * t_per, te = tb + t_per < T ? tb + t_per : T;
+	double2 acc[4];
+#pragma unroll
+	for(int k = 0; k < 4; k++)
+		acc[k] = make_double2(0.0, 0.0);
+	for(int t0 = tb; t0 < te; t0 += 32) {
+		for(int i = threadIdx.x; i < 32 * 32; i += blockDim.x) {
+			const int tt = i / 32, j = i % 32, t = t0 + tt;
+			const bool ok = t < te;
+			const double wt = ok ? w[t] : 0.0;
+			const double2 a = (ok && l10 + j < Aa) ? Sa[(size_t) t * Aa + l10 + j] : make_double2(0.0, 0.0);
+			const double2 b = (ok && l20 + j < Ab) ? Sb[(size_t) t * Ab + l20 + j] : make_double2(0.0, 0.0);
+			s_a[tt][j] = a;
+			s_b[tt][j] = make_double2(wt * b.x, wt * b.y);
+		}
+		__syncthreads();
+#pragma unroll 4
+		for(int tt = 0; tt < 32; tt++) {
+			const double2 b = s_b[tt][tx];
+#pragma unroll
+			for(int k = 0; k < 4; k++) {
+				const double2 a = s_a[tt][ty + 8 * k];
+				acc[k].x += a.x * b.x - a.y * b.y;
+				acc[k].y += a.x * b.y + a.y * b.x;
+			}
+		}
+		__syncthreads();
+	}
+	const int l2 = l20 + tx;
+	if(l2 < Ab)
+#pragma unroll
+		for(int k = 0; k < 4; k++) {
+			const int l1 = l10 + ty + 8 * k;
+			if(l1 < Aa)
+				part[((size_t) blockIdx.z * Aa + l1) * Ab + l2] = acc[k];
+		}
+}
+
+// C = sum over the partials, in a fixed order
+__global__ void k_td_reduce(int nz, size_t len, const double2 *__restrict__ part, double2 *__restrict__ C)
+{
+	for(size_t i = blockIdx.x * (size_t) blockDim.x + threadIdx.x; i < len; i += (size_t) gridDim.x * blockDim.x) {
+		double2 acc = part[i];
+		for(int z = 1; z < nz; z++) {
+			const double2 v = part[(size_t) z * len + i];
+			acc.x += v.x;
+			acc.y += v.y;
+		}
+		C[i] = acc;
+	}
+}
+
+// q[i] = sum_{l1,l2} P~_l1(x_i) C[l1][l2] P~_l2(x_i), one block per node
+__global__ void k_td_node(int nq, int LP, int Aa, int Ab, const double *__restrict__ P, const double2 *__restrict__ C, double2 *__restrict__ q)
+{
+	__shared__ double2 s_red[256];
+	const int i = blockIdx.x;
+	const double *Pi = P + (size_t) i * LP;
+	double2 acc = make_double2(0.0, 0.0);
+	for(int l2 = threadIdx.x; l2 < Ab; l2 += blockDim.x) {
+		double2 g = make_double2(0.0, 0.0);
+		for(int l1 = 0; l1 < Aa; l1++) {
+			const double2 c = C[(size_t) l1 * Ab + l2];
+			g.x += Pi[l1] * c.x;
+			g.y += Pi[l1] * c.y;
+		}
+		acc.x += g.x * Pi[l2];
+		acc.y += g.y * Pi[l2];
+	}
+	s_red[threadIdx.x] = acc;
+	__syncthreads();
+	for(int s = blockDim.x / 2; s > 0; s >>= 1) {
+		if(threadIdx.x < s) {
+			s_red[threadIdx.x].x += s_red[threadIdx.x + s].x;
+			s_red[threadIdx.x].y += s_red[threadIdx.x + s].y;
+		}
+		__syncthreads();
+	}
+	if(threadIdx.x == 0)
+		q[i] = s_red[0];
+}
+
+// power[L] = 2 pi sum_i w_i q_i P~_L(x_i), L <= Lp
+__global__ void k_td_power(int nq, int LP, int Lp, const double *__restrict__ wq, const double *__restrict__ P, const double2 *__restrict__ q, double2 *__restrict__ power)
+{
+	const int L = blockIdx.x * blockDim.x + threadIdx.x;
+	if(L > Lp)
+		return;
+	double2 acc = make_double2(0.0, 0.0);
+	for(int i = 0; i < nq; i++) {
+		const double f = wq[i] * P[(size_t) i * LP + L];
+		acc.x += f * q[i].x;
+		acc.y += f * q[i].y;
+	}
+	power[L] = make_double2(2.0 * M_PI * acc.x, 2.0 * M_PI * acc.y);
+}
+
+// a typed view of a piece of the arena
+struct TdSpan {
+	void *p;
+	template <class T_> T_ *as() const { return (T_ *) p; }
+};
+
+// grow-only device arena of the time-domain integrator, per device
+struct TdArena {
+	std::mutex mu;
+	std::unordered_map<int, std::pair<void *, size_t>> bufs;
+	void *get(size_t need)
+	{
+		int dev = 0;
+		cudaGetDevice(&dev);
+		auto &b = bufs[dev];
+		if(b.second < need || !b.first) {
+			dfree(b.first);
+			b.first = dmalloc(need);
+			b.second = b.first ? need : 0;
+		}
+		return b.first;
+	}
+};
+TdArena g_td_arena;
+
+}  // namespace
+
+int td_power_1d(int T, int n_ela, int n_elb, int Aa, int Ab, const double *taps_a, const double *taps_b, const double *xa, const double *xb, long long n_x,
+		const double *w, unsigned Lp, double *power_host)
+{
+	if(T < 0 || n_ela <= 0 || n_elb <= 0 || Aa <= 0 || Ab <= 0 || (long long) T + n_ela - 1 > n_x || (long long) T + n_elb - 1 > n_x) {
+		set_error("time-domain correlator: %d samples of %lld with %d- and %d-tap projections", T, n_x, n_ela, n_elb);
+		return -1;
+	}
+	if(T == 0) {
+		memset(power_host, 0, ((size_t) Lp + 1) * 2 * sizeof(double));
+		return 0;
+	}
+	if(ensure_device())
+		return -1;
+	const int La = Aa - 1, Lb = Ab - 1;
+	const int nq = ((int) Lp + La + Lb) / 2 + 1;
+	const int LP = std::max(std::max(Aa, Ab), (int) Lp + 1);
+	// split the sample sum so that about two blocks per SM run
+	int dev = 0, sms = 148;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	const int tiles = ((Aa + 31) / 32) * ((Ab + 31) / 32);
+	int nz = (2 * sms + tiles - 1) / tiles;
+	nz = std::max(1, std::min(nz, (T + 255) / 256));
+	const int t_per = ((T + nz - 1) / nz + 31) / 32 * 32;
+	nz = (T + t_per - 1) / t_per;
+	const size_t clen = (size_t) Aa * Ab;
+	// one grow-only device arena per device, held for the whole call
+	const size_t sizes[15] = {(size_t) n_ela * Aa * 16, (size_t) n_elb * Ab * 16, (size_t) (T + n_ela - 1) * 8, (size_t) (T + n_elb - 1) * 8, (size_t) T * 8,
+				  (size_t) T * Aa * 16,	      (size_t) T * Ab * 16,	  (size_t) nz * clen * 16,	 clen * 16,			(size_t) nq * 8,
+				  (size_t) nq * 8,	      (size_t) nq * LP * 8,	  (size_t) nq * LP * 8,	 (size_t) nq * 16,		((size_t) Lp + 1) * 16};
+	size_t offs[15], total = 0;
+	for(int i = 0; i < 15; i++) {
+		offs[i] = total;
+		total += (sizes[i] + 255) / 256 * 256;
+	}
+	std::lock_guard<std::mutex> lock(g_td_arena.mu);
+	char *base = (char *) g_td_arena.get(total);
+	if(!base)
+		return -1;
+	TdSpan dta{base + offs[0]}, dtb{base + offs[1]}, dxa{base + offs[2]}, dxb{base + offs[3]}, dw{base + offs[4]}, dSa{base + offs[5]}, dSb{base + offs[6]},
+		dpart{base + offs[7]}, dC{base + offs[8]}, dx{base + offs[9]}, dwq{base + offs[10]}, dP{base + offs[11]}, dPT{base + offs[12]}, dq{base + offs[13]},
+		dpow{base + offs[14]};
+	if(h2d(dta.p, taps_a, sizes[0]) || h2d(dtb.p, taps_b, sizes[1]) || h2d(dxa.p, xa, sizes[2]) || h2d(dxb.p, xb, sizes[3]) || h2d(dw.p, w, sizes[4]))
+		return -1;
+	cudaStream_t s = S();
+	k_td_samples<<<dim3((T + kTdTT - 1) / kTdTT, (Aa + kTdTL - 1) / kTdTL), 256, 0, s>>>(T, n_ela, Aa, dta.as<double2>(), dxa.as<double>(), dSa.as<double2>());
+	k_td_samples<<<dim3((T + kTdTT - 1) / kTdTT, (Ab + kTdTL - 1) / kTdTL), 256, 0, s>>>(T, n_elb, Ab, dtb.as<double2>(), dxb.as<double>(), dSb.as<double2>());
+	k_td_cross<<<dim3((Ab + 31) / 32, (Aa + 31) / 32, nz), 256, 0, s>>>(T, t_per, Aa, Ab, dw.as<double>(), dSa.as<double2>(), dSb.as<double2>(), dpart.as<double2>());
+	k_td_reduce<<<(int) std::min<size_t>((clen + 255) / 256, 1024), 256, 0, s>>>(nz, clen, dpart.as<double2>(), dC.as<double2>());
+	k_gl_nodes<<<(nq / 2 + 1 + 127) / 128, 128, 0, s>>>(nq, dx.as<double>(), dwq.as<double>());
+	k_plm0_table<<<(nq + 127) / 128, 128, 0, s>>>(nq, dx.as<double>(), LP, dP.as<double>(), dPT.as<double>());
+	k_td_node<<<nq, 256, 0, s>>>(nq, LP, Aa, Ab, dP.as<double>(), dC.as<double2>(), dq.as<double2>());
+	k_td_power<<<((int) Lp + 1 + 127) / 128, 128, 0, s>>>(nq, LP, (int) Lp, dwq.as<double>(), dP.as<double>(), dq.as<double2>(), dpow.as<double2>());
+	CK(cudaGetLastError());
+	if(d2h(power_host, dpow.p, ((size_t) Lp + 1) * 16) || stream_sync())
+		return -1;
+	return 0;
 }
 
 }  // namespace sphrad

@@ -128,6 +128,20 @@ int fseries_run_host(void *plan, const double *ts_host, double *fs_host);
 int projection_multiply(int n, unsigned L, int n_det, const double *fp_host, const double *fc_host, const double *psd_host, int a, int b, double beta,
 			const double *Rinv, const double *delay_host, double *out_host);
 
+// ---- time-domain correlator (runtime.cu) --------------------------------
+// polar projection taps of a phase centre at r z-hat (projection.c:99-131):
+// host [n_el][A], tap t at delay t - (n_el - 1) / 2, degrees l < A
+int projection_taps(double r, double delta_t, int n_el, int A, double *taps_host);
+// the same for any phase centre (rx, ry, rz) as full series of l_max L:
+// host complex [n_el][(L + 1)^2] (projection.cu)
+int projection_taps_full(const double *r, double delta_t, int n_el, unsigned L, double *series_host);
+// window-weighted sum over samples t < T of the polar products of
+// S_a[t] = sum_e taps_a[e] x_a[t + e] and S_b[t] (correlator.c:648-668),
+// truncated to l <= Lp <= (Aa - 1) + (Ab - 1).  taps: complex [n_el][A];
+// x: n_x >= T + n_el - 1 samples; power_host: complex [Lp + 1]
+int td_power_1d(int T, int n_ela, int n_elb, int Aa, int Ab, const double *taps_a, const double *taps_b, const double *xa, const double *xb, long long n_x,
+		const double *w, unsigned Lp, double *power_host);
+
 // ---- batched integration with non-polar kernels (nonpolar.cu) ---------
 // D[b]: host [n][(L+1)^2] complex non-polar delay kernels; rot[b]: host
 // flat Wigner plans up to L; fp64: contraction arithmetic (else FP32)

@@ -181,6 +181,41 @@ def test_fd_correlator_against_analytic_noise_solution():
         assert 10 * np.log10(O.rms_error(sky, sol_lo, sky_l)) <= -21.0
 
 
+def test_td_correlator_against_analytic_noise_solution():
+    """The time-domain leg of the same validation (correlator_validate.c:
+    238, 265-268, 308, 374): square windows of n - 2 transient samples with
+    amplitude 1 / (n - 2 transient); RMS(TD - order-reduced exact) must be
+    <= -21 dB of the variance.  One GMST: the oracle runs the reference's
+    per-sample loop."""
+    rng = np.random.Generator(np.random.Philox(11))
+    pos = W.random_positions(4, W.R_EARTH_S, rng)
+    dt = 1.0 / 512
+    pairs = [(i, j) for i in range(1, 4) for j in range(i)]
+    sky_l = max(O.power_l_max_naive(float(np.linalg.norm(pos[i] - pos[j])), dt) for i, j in pairs)
+    n = int((86164.0 / sky_l / 20) / dt)
+    gmst = np.pi / 3
+    ts = np.zeros((4, n))
+    inj = W.gaussian_white_noise(n, 1.0, rng)
+    for k in range(4):
+        W.inject_into(pos[k], ts[k], inj, dt, 0.0, 0.0, gmst)
+    sky = np.zeros(O.length(sky_l, False), np.complex128)
+    bls = []
+    for i, j in pairs:
+        d = pos[i] - pos[j]
+        dl = float(np.linalg.norm(d))
+        th, ph = O.vector_direction(d)
+        pl = O.td_power_l_max(dl, dt)
+        tr = (O.projection_n_elements(dl / 2, dt) - 1) // 2
+        win = np.full(n - 2 * tr, 1.0 / (n - 2 * tr))
+        p = O.baseline_integrate_power_td(ts[i], ts[j], win, dl, dt, pl, O.rotation_plan(pl, O.rot_matrix(th, ph)))
+        sky += O.assign(p, pl, False, sky_l, False) / len(pairs)
+        bls.append(dict(d_len=dl, theta=th, phi=ph))
+    sky = O.rotate_z(sky, sky_l, False, gmst)
+    sol = sum(_noise_solution(b, 2 * sky_l, 1.0, dt, 0.0, 0.0, gmst) for b in bls) / len(bls)
+    sol_lo = O.assign(sol, 2 * sky_l, False, sky_l, False)
+    assert 10 * np.log10(O.rms_error(sky, sol_lo, sky_l)) <= -21.0
+
+
 def test_delay_table_is_hermitian_along_bins():
     """Real taps give D[n-k] = conj(D[k]) (correlator.c:482-489)."""
     D = O.delay_product(0.0101, 1.0 / 1024, 256, 12)
