@@ -379,7 +379,7 @@ def tseries_report(S, n_seg: int, reps: int = 10):
     return out
 
 
-def projection_report(S, n_seg: int = 1024, reps: int = 3):
+def projection_report(S, n_seg: int = 4096, reps: int = 3):
     """The projection-operator (inspiral) path on the c1 network: the plan
     transform (every bin's projection mesh, analysis, rotation and product,
     3 baselines x 4096 bins at l_max 32, on the GPU) and the batched

@@ -743,6 +743,7 @@ struct BatchPlan {
 	// host-buffer path scratch
 	void *hF = nullptr, *hG = nullptr, *hSky = nullptr, *hWs = nullptr;
 	size_t hF_bytes = 0, hG_bytes = 0, hSky_bytes = 0, hWs_bytes = 0;
+	cudaStream_t hStream2 = nullptr;  // second copy/compute stream of that path
 	// tensor map cache
 	const void *tm_ptr = nullptr;
 	int tm_S = -1;
@@ -790,6 +791,8 @@ void batch_plan_destroy(void *pp)
 	dfree(P->hG);
 	dfree(P->hSky);
 	dfree(P->hWs);
+	if(P->hStream2)
+		cudaStreamDestroy(P->hStream2);
 	delete P;
 }
 
@@ -1424,24 +1427,49 @@ int batch_run_host(void *pp, const void *F_host, int S, long long ld, const doub
 	BatchPlan *P = (BatchPlan *) pp;
 	if(S <= 0)
 		return 0;
-	cudaStream_t st = (cudaStream_t) lib_stream();
-	const size_t fbytes = (size_t) P->n_det * S * ld * 16;
-	const size_t sbytes = (size_t) S * P->nq * 16;
-	const size_t wbytes = batch_workspace_bytes(P, S);
-	if(grow(&P->hF, &P->hF_bytes, fbytes) || grow(&P->hSky, &P->hSky_bytes, sbytes) || grow(&P->hG, &P->hG_bytes, (size_t) S * 8))
-		return -1;
-	if(P->hWs_bytes < wbytes) {
-		if(grow(&P->hWs, &P->hWs_bytes, wbytes))
-			return -1;
-		CKB(cudaMemsetAsync(P->hWs, 0, wbytes, st));
+	// chunks of at least 512 segments alternate between two streams, so
+	// that the host-to-device copy of one chunk overlaps the kernels and
+	// the device-to-host copy of the one before (copy engines of both
+	// directions at once); small batches take one chunk
+	const int nchunk = S >= 1024 ? std::min(8, S / 512) : 1;
+	const int cs = (S + nchunk - 1) / nchunk;
+	const int nslot = nchunk > 1 ? 2 : 1;
+	cudaStream_t st[2] = {(cudaStream_t) lib_stream(), nullptr};
+	if(nslot > 1) {
+		if(!P->hStream2)
+			CKB(cudaStreamCreateWithFlags(&P->hStream2, cudaStreamNonBlocking));
+		st[1] = P->hStream2;
 	}
-	CKB(cudaMemcpyAsync(P->hF, F_host, fbytes, cudaMemcpyHostToDevice, st));
-	if(gmst_host)
-		CKB(cudaMemcpyAsync(P->hG, gmst_host, (size_t) S * 8, cudaMemcpyHostToDevice, st));
-	if(batch_run(P, P->hF, S, ld, gmst_host ? (const double *) P->hG : nullptr, P->hSky, P->hWs, P->hWs_bytes, st, 0))
+	const size_t fchunk = (size_t) P->n_det * cs * ld * 16, schunk = (size_t) cs * P->nq * 16, gchunk = (size_t) cs * 8;
+	const size_t wchunk = (batch_workspace_bytes(P, cs) + 255) / 256 * 256;
+	if(grow(&P->hF, &P->hF_bytes, nslot * fchunk) || grow(&P->hSky, &P->hSky_bytes, nslot * schunk) || grow(&P->hG, &P->hG_bytes, nslot * gchunk))
 		return -1;
-	CKB(cudaMemcpyAsync(sky_host, P->hSky, sbytes, cudaMemcpyDeviceToHost, st));
-	CKB(cudaStreamSynchronize(st));
+	if(P->hWs_bytes < nslot * wchunk) {
+		// the integrator leaves its split-K scratch zeroed; a new one starts so
+		if(grow(&P->hWs, &P->hWs_bytes, nslot * wchunk))
+			return -1;
+		CKB(cudaMemsetAsync(P->hWs, 0, P->hWs_bytes, st[0]));
+		CKB(cudaStreamSynchronize(st[0]));
+	}
+	for(int c = 0; c < nchunk; c++) {
+		const int s0 = c * cs, n = std::min(cs, S - s0);
+		if(n <= 0)
+			break;
+		const int k = c % nslot;
+		char *dF = (char *) P->hF + k * fchunk, *dSky = (char *) P->hSky + k * schunk, *dWs = (char *) P->hWs + k * wchunk;
+		double *dG = (double *) ((char *) P->hG + k * gchunk);
+		// detector rows of this chunk: [n_det][n][ld] from [n_det][S][ld]
+		CKB(cudaMemcpy2DAsync(dF, (size_t) n * ld * 16, (const char *) F_host + (size_t) s0 * ld * 16, (size_t) S * ld * 16, (size_t) n * ld * 16, P->n_det,
+				      cudaMemcpyHostToDevice, st[k]));
+		if(gmst_host)
+			CKB(cudaMemcpyAsync(dG, gmst_host + s0, (size_t) n * 8, cudaMemcpyHostToDevice, st[k]));
+		if(batch_run(P, dF, n, ld, gmst_host ? dG : nullptr, dSky, dWs, wchunk, st[k], 0))
+			return -1;
+		CKB(cudaMemcpyAsync((char *) sky_host + (size_t) s0 * P->nq * 16, dSky, (size_t) n * P->nq * 16, cudaMemcpyDeviceToHost, st[k]));
+	}
+	CKB(cudaStreamSynchronize(st[0]));
+	if(nslot > 1)
+		CKB(cudaStreamSynchronize(st[1]));
 	unsigned code = 0;
 	if(batch_check_error(P, &code))
 		return -1;

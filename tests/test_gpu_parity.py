@@ -270,6 +270,23 @@ def test_batched_host_entry_point(lib, c1):
     bp.close()
 
 
+def test_batched_host_entry_point_in_chunks(lib, c1):
+    """1573 segments go through the host path in three chunks on two
+    streams (525, 525, 523); twice, so the second call reuses the scratch
+    the first left behind."""
+    bp = lib.BatchPlan(c1["net"], "bf16x3")
+    S = 1573
+    idx = np.arange(S) % c1["batch"]["F"].shape[1]
+    Fh = np.ascontiguousarray(c1["batch"]["F"][:, idx, :])
+    g = np.ascontiguousarray(c1["batch"]["gmst"][idx])
+    for _ in range(2):
+        sky = bp.integrate_host(Fh, g)
+        errs = [rel_l2(sky[s], c1["ref"][idx[s]]) for s in range(S)]
+        assert max(errs) < 1e-5
+    assert bp.status() == 0
+    bp.close()
+
+
 def test_batched_autotune_keeps_results(lib, c1):
     import torch
     bp = lib.BatchPlan(c1["net"], "bf16x3")
