@@ -421,6 +421,30 @@ def projection_report(S, n_seg: int = 4096, reps: int = 3):
         out[f"{prec}_maps_per_s"] = n_seg / t
         out[f"{prec}_tflops"] = flops / t / 1e12
         bp.close()
+    # generate_alm_skys for n_seg events at once: complex SNR series of
+    # every detector -> spectra -> the skies of both projection signs
+    # (x 8 B, + log prior, GMST rotation), bf16x3
+    net_n = S.Network(pos, n, DT, l_max=L_MAX)
+    if S.load().sphrad_network_plan_mult_by_projection(net_n.plan, -1.0, fp.ctypes.data, fc.ctypes.data, C.cast(rows, C.c_void_p)):
+        raise RuntimeError(S.last_error())
+    bp, bn = S.BatchPlan(net, "bf16x3"), S.BatchPlan(net_n, "bf16x3")
+    fpl = S.FseriesPlan(n)
+    z = torch.complex(torch.randn(N_DET, n_seg, n, dtype=torch.float64, device="cuda"), torch.randn(N_DET, n_seg, n, dtype=torch.float64, device="cuda"))
+    prior = torch.zeros((L_MAX + 1) ** 2, dtype=torch.complex128, device="cuda")
+    S.batch_generate_alm_skys(bp, bn, fpl, z, g, prior)
+    torch.cuda.synchronize()
+    a.record(st)
+    for _ in range(reps):
+        S.batch_generate_alm_skys(bp, bn, fpl, z, g, prior)
+    e.record(st)
+    torch.cuda.synchronize()
+    t = a.elapsed_time(e) / reps / 1e3
+    out["alm_skys_events_per_s"] = n_seg / t
+    out["alm_skys_note"] = "events/s: both skies of an event (plus and minus projection) from complex series, bf16x3"
+    fpl.close()
+    bp.close()
+    bn.close()
+    net_n.close()
     net.close()
     return out
 

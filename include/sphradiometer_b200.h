@@ -167,6 +167,17 @@ int sphrad_tseries_to_fseries(sphrad_fseries_plan *plan, const double *tseries, 
  * full n-element host spectrum (double complex), X[n-k] = conj X[k] as in
  * correlator.c:228-229, whitened when the plan has a psd.  Synchronous. */
 int sphrad_tseries_to_fseries_host(sphrad_fseries_plan *plan, const double *tseries, void *fseries);
+/* Complex series (correlator_ctseries_to_fseries_plan /
+ * correlator_ctseries_to_fseries, correlator.c:235-244: FFTW's unnormalised
+ * forward DFT of n complex points, X[k] = sum_t z[t] e^{-2 pi i k t / n}):
+ * rows device series of n points (row r at ctseries + r * ldt double
+ * complex, ldt >= n) -> rows device spectra of n bins (row r at fseries +
+ * r * ldf, ldf >= n).  n up to 8192 (one CTA per series); the plan's psd,
+ * if any, is not applied (the reference's inspiral path does not whiten).
+ * Asynchronous on cuda_stream (NULL = the legacy default stream). */
+int sphrad_ctseries_to_fseries(sphrad_fseries_plan *plan, const void *ctseries, int rows, long long ldt, void *fseries, long long ldf, void *cuda_stream);
+/* Host drop-in: n host points -> n host bins.  Synchronous. */
+int sphrad_ctseries_to_fseries_host(sphrad_fseries_plan *plan, const void *ctseries, void *fseries);
 /* Time series straight to skies: sphrad_tseries_to_fseries into the front
  * of the workspace, then sphrad_batch_integrate on those spectra.
  * tseries: device [n_det][n_seg][ldt] doubles; the plans must share n.
@@ -198,6 +209,32 @@ int sphrad_batch_integrate_tseries(sphrad_batch_plan *plan, sphrad_fseries_plan 
  * detector k.  All baselines must share L and n.  0 on success, -1 on
  * failure (the plan is unchanged up to the failing baseline). */
 int sphrad_network_plan_mult_by_projection(struct correlator_network_plan_fd *plan, double beta, const double *fplus, const double *fcross, double **psd);
+
+/* Sky maps of the inspiral path, generate_alm_skys (inspiral_sky_map.c:
+ * 942-1101) with generate_alm_sky (:869-939), over plain arrays instead of
+ * LAL series: the complex (SNR) series of every detector, series[k] with n
+ * points, are Fourier transformed on the GPU (correlator_ctseries_to_fseries);
+ * for each of the two projected network plans (positive and negative
+ * polarisation sign) the sky is
+ *     rotate_z(2 * 4 n_baselines * correlator_network_integrate_power_fd + logprior, gmst)
+ * at the prior's l_max.  gmst: what the reference computes from the series'
+ * epoch with LAL (gmst_from_epoch_and_offset at the series' midpoint).  The
+ * plans are projected plans (sphrad_network_plan_mult_by_projection) of n
+ * bins.  *skyp and *skyn are new series, as in the reference.  0 or -1. */
+int sphrad_generate_alm_skys(struct sh_series **skyp, struct sh_series **skyn, struct correlator_network_plan_fd *plansp,
+			     struct correlator_network_plan_fd *plansn, const double _Complex *const *series, int n, double gmst,
+			     const struct sh_series *logprior);
+/* The same for n_ev events at once, device-resident: batch plans of the two
+ * projected networks (sphrad_batch_plan_new on each), a spectrum plan of n,
+ * ctseries: device [n_det][n_ev][ldt] double complex, gmst: device [n_ev]
+ * or NULL, logprior: device (L+1)^2 double complex (the l_max of the plans)
+ * or NULL; sky_p, sky_n: device [n_ev][(L+1)^2] double complex.  The
+ * workspace holds the spectra and the integrators' scratch.  Asynchronous
+ * on cuda_stream. */
+size_t sphrad_batch_alm_skys_workspace_size(const sphrad_batch_plan *plan_p, const sphrad_batch_plan *plan_n, int n_ev);
+int sphrad_batch_generate_alm_skys(sphrad_batch_plan *plan_p, sphrad_batch_plan *plan_n, sphrad_fseries_plan *fseries_plan, const void *ctseries, int n_ev,
+				   long long ldt, const double *gmst, const void *logprior, void *sky_p, void *sky_n, void *workspace,
+				   size_t workspace_bytes, void *cuda_stream);
 
 /* ---- uneven batches ------------------------------------------------------
  *

@@ -219,6 +219,52 @@ class TimeDomainNetwork:
             pass
 
 
+def generate_alm_skys(net_p: Network, net_n: Network, series, gmst: float, logprior) -> tuple[np.ndarray, np.ndarray]:
+    """sphrad_generate_alm_skys (inspiral_sky_map.c:869-1101): series is
+    n_det x n complex SNR series, net_p / net_n the networks whose plans were
+    multiplied by the projection of each polarisation sign, logprior the
+    (L+1)^2 prior coefficients.  Returns (sky_p, sky_n)."""
+    L = load()
+    z = [np.ascontiguousarray(s, np.complex128) for s in series]
+    ptrs = (C.c_void_p * len(z))(*[s.ctypes.data for s in z])
+    lp = np.asarray(logprior, np.complex128)
+    l_max = int(round(np.sqrt(lp.size))) - 1
+    prior = numpy_to_series(lp, l_max, False)
+    sp, sn = C.POINTER(_abi.sh_series)(), C.POINTER(_abi.sh_series)()
+    try:
+        if L.sphrad_generate_alm_skys(C.byref(sp), C.byref(sn), net_p.plan, net_n.plan, ptrs, len(z[0]), float(gmst), prior):
+            raise SphradError("sphrad_generate_alm_skys: " + last_error())
+        out = (series_to_numpy(sp), series_to_numpy(sn))
+        L.sh_series_free(sp)
+        L.sh_series_free(sn)
+        return out
+    finally:
+        L.sh_series_free(prior)
+
+
+def batch_generate_alm_skys(bp_p: "BatchPlan", bp_n: "BatchPlan", fplan: "FseriesPlan", ctseries, gmst=None, logprior=None, stream=None):
+    """sphrad_batch_generate_alm_skys: ctseries complex128 CUDA
+    [n_det][n_ev][n]; gmst float64 CUDA [n_ev] or None; logprior complex128
+    CUDA [(L+1)^2] or None.  Returns (sky_p, sky_n), complex128 CUDA
+    [n_ev][(L+1)^2]."""
+    import torch
+    L = load()
+    assert ctseries.is_cuda and ctseries.dtype == torch.complex128 and ctseries.is_contiguous()
+    n_det, n_ev, ldt = ctseries.shape
+    nq = (bp_p.l_max + 1) ** 2
+    sky_p = torch.empty((n_ev, nq), dtype=torch.complex128, device=ctseries.device)
+    sky_n = torch.empty_like(sky_p)
+    need = L.sphrad_batch_alm_skys_workspace_size(bp_p._p, bp_n._p, n_ev)
+    ws = torch.empty(max(need, 16), dtype=torch.uint8, device=ctseries.device)
+    st = stream if stream is not None else torch.cuda.current_stream()
+    g = gmst.data_ptr() if gmst is not None else None
+    pr = logprior.data_ptr() if logprior is not None else None
+    if L.sphrad_batch_generate_alm_skys(bp_p._p, bp_n._p, fplan._p, ctseries.data_ptr(), n_ev, ldt, g, pr, sky_p.data_ptr(), sky_n.data_ptr(), ws.data_ptr(),
+                                        ws.numel(), st.cuda_stream):
+        raise SphradError("sphrad_batch_generate_alm_skys: " + last_error())
+    return sky_p, sky_n
+
+
 def projection_matrix_delay(phase_centre, n: int, l_max: int, delta_t: float) -> np.ndarray:
     """projection_matrix_delay (projection.c:110-131): n x length(l_max,
     polar) coefficients of the sinc delay taps of a phase centre
@@ -395,6 +441,29 @@ class FseriesPlan:
         st = stream if stream is not None else torch.cuda.current_stream()
         if load().sphrad_tseries_to_fseries(self._p, x.data_ptr(), rows, self.n, out.data_ptr(), self.n // 2 + 1, st.cuda_stream):
             raise SphradError("sphrad_tseries_to_fseries: " + last_error())
+        return out
+
+    def transform_complex(self, z, out=None, stream=None):
+        """z: complex128 CUDA tensor [..., n] (rows contiguous), n <= 8192;
+        returns the unnormalised forward DFTs, complex128 [..., n]
+        (correlator_ctseries_to_fseries)."""
+        import torch
+        assert z.is_cuda and z.dtype == torch.complex128 and z.shape[-1] == self.n and z.is_contiguous()
+        rows = z.numel() // self.n
+        if out is None:
+            out = torch.empty_like(z)
+        st = stream if stream is not None else torch.cuda.current_stream()
+        if load().sphrad_ctseries_to_fseries(self._p, z.data_ptr(), rows, self.n, out.data_ptr(), self.n, st.cuda_stream):
+            raise SphradError("sphrad_ctseries_to_fseries: " + last_error())
+        return out
+
+    def transform_complex_host(self, z: np.ndarray) -> np.ndarray:
+        """One host complex series -> its n-bin spectrum."""
+        z = np.ascontiguousarray(z, dtype=np.complex128)
+        assert z.shape == (self.n,)
+        out = np.empty(self.n, dtype=np.complex128)
+        if load().sphrad_ctseries_to_fseries_host(self._p, z.ctypes.data, out.ctypes.data):
+            raise SphradError("sphrad_ctseries_to_fseries_host: " + last_error())
         return out
 
     def transform_host(self, x: np.ndarray) -> np.ndarray:

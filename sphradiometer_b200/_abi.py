@@ -196,6 +196,12 @@ SIGNATURES = {
     "sphrad_fseries_plan_free": (None, [_vp]),
     "sphrad_tseries_to_fseries": (_i, [_vp, _vp, _i, _ll, _vp, _ll, _vp]),
     "sphrad_tseries_to_fseries_host": (_i, [_vp, _vp, _vp]),
+    "sphrad_ctseries_to_fseries": (_i, [_vp, _vp, _i, _ll, _vp, _ll, _vp]),
+    "sphrad_ctseries_to_fseries_host": (_i, [_vp, _vp, _vp]),
+    "sphrad_generate_alm_skys": (_i, [_P(_P(sh_series)), _P(_P(sh_series)), _P(correlator_network_plan_fd), _P(correlator_network_plan_fd), _P(_vp), _i, _d,
+                                      _P(sh_series)]),
+    "sphrad_batch_alm_skys_workspace_size": (_sz, [_vp, _vp, _i]),
+    "sphrad_batch_generate_alm_skys": (_i, [_vp, _vp, _vp, _vp, _i, _ll, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "sphrad_batch_tseries_workspace_size": (_sz, [_vp, _i]),
     "sphrad_batch_integrate_tseries": (_i, [_vp, _vp, _vp, _i, _ll, _vp, _vp, _vp, _sz, _vp]),
     "sphrad_batch_status": (_i, [_vp]),

@@ -1100,6 +1100,21 @@ extern "C" int sphrad_tseries_to_fseries_host(sphrad_fseries_plan *p, const doub
 	return fseries_run_host(p->impl, tseries, (double *) fseries);
 }
 
+// complex series (correlator_ctseries_to_fseries, correlator.c:235-244)
+extern "C" int sphrad_ctseries_to_fseries(sphrad_fseries_plan *p, const void *ctseries, int rows, long long ldt, void *fseries, long long ldf, void *stream)
+{
+	return fseries_run_complex(p->impl, ctseries, rows, ldt, fseries, ldf, stream ? stream : (void *) cudaStreamLegacy);
+}
+
+extern "C" int sphrad_ctseries_to_fseries_host(sphrad_fseries_plan *p, const void *ctseries, void *fseries)
+{
+	if(!ctseries || !fseries) {
+		set_error("sphrad_ctseries_to_fseries_host: NULL series");
+		return -1;
+	}
+	return fseries_run_complex_host(p->impl, (const double *) ctseries, 1, (double *) fseries);
+}
+
 static size_t align256(size_t b) { return (b + 255) & ~(size_t) 255; }
 
 extern "C" size_t sphrad_batch_tseries_workspace_size(const sphrad_batch_plan *p, int n_seg)
@@ -1495,6 +1510,109 @@ extern "C" int read_precalc_correlator_network_plan_fd(struct correlator_network
 	fdplansn->baselines = (struct correlator_network_baselines *) baselines;
 	fdplansp->plans = pp;
 	fdplansn->plans = pn;
+	return 0;
+}
+
+// ------------------------------------------------------------------------
+// inspiral sky maps (generate_alm_sky / generate_alm_skys,
+// inspiral_sky_map.c:869-1101)
+// ------------------------------------------------------------------------
+// integrate, x 2 for the upper triangle of the projection, x 4 n_baselines,
+// + log prior, rotate by the GMST (:877-936)
+static int alm_sky(struct sh_series *sky, struct correlator_network_plan_fd *plans, dcplx **fseries, double gmst, const struct sh_series *logprior)
+{
+	if(!correlator_network_integrate_power_fd(sky, fseries, plans))
+		return -1;
+	if(!sh_series_scale(sky, 2.0) || !sh_series_scale(sky, plans->baselines->n_baselines * 4.0) || (logprior && !sh_series_add(sky, 1.0, logprior)) ||
+	   !sh_series_rotate_z(sky, sky, gmst))
+		return -1;
+	return 0;
+}
+
+extern "C" int sphrad_generate_alm_skys(struct sh_series **skyp, struct sh_series **skyn, struct correlator_network_plan_fd *plansp,
+					struct correlator_network_plan_fd *plansn, const dcplx *const *series, int n, double gmst, const struct sh_series *logprior)
+{
+	if(!skyp || !skyn || !plansp || !plansn || !series || !logprior || n <= 0) {
+		set_error("sphrad_generate_alm_skys: NULL argument or empty series");
+		return -1;
+	}
+	const int n_det = instrument_array_len(plansp->baselines->baselines[0]->instruments);
+	if(plansp->plans[0]->delay_product->n != n || plansn->plans[0]->delay_product->n != n) {
+		set_error("sphrad_generate_alm_skys: plans of %d bins for series of %d samples", plansp->plans[0]->delay_product->n, n);
+		return -1;
+	}
+	// Fourier transform every detector's series on the GPU (:960-980)
+	sphrad_fseries_plan *fp = sphrad_fseries_plan_new(n, NULL);
+	if(!fp)
+		return -1;
+	std::vector<dcplx> ts((size_t) n_det * n), fs((size_t) n_det * n);
+	for(int k = 0; k < n_det; k++)
+		memcpy(ts.data() + (size_t) k * n, series[k], (size_t) n * sizeof(dcplx));
+	const int rc = fseries_run_complex_host(fp->impl, (const double *) ts.data(), n_det, (double *) fs.data());
+	sphrad_fseries_plan_free(fp);
+	if(rc)
+		return -1;
+	std::vector<dcplx *> fptr(n_det);
+	for(int k = 0; k < n_det; k++)
+		fptr[k] = fs.data() + (size_t) k * n;
+	// the sky of each projection sign at the prior's l_max (:1069-1081)
+	*skyp = sh_series_new_zero(logprior->l_max, 0);
+	*skyn = sh_series_new_zero(logprior->l_max, 0);
+	if(!*skyp || !*skyn || alm_sky(*skyp, plansp, fptr.data(), gmst, logprior) || alm_sky(*skyn, plansn, fptr.data(), gmst, logprior)) {
+		sh_series_free(*skyp);
+		sh_series_free(*skyn);
+		*skyp = *skyn = NULL;
+		return -1;
+	}
+	return 0;
+}
+
+extern "C" size_t sphrad_batch_alm_skys_workspace_size(const sphrad_batch_plan *plan_p, const sphrad_batch_plan *plan_n, int n_ev)
+{
+	if(n_ev <= 0 || !plan_p->np || !plan_n->np)
+		return 0;
+	const size_t spectra = (size_t) np_plan_n_det(plan_p->np) * n_ev * np_plan_n(plan_p->np) * 16;
+	return align256(spectra) + std::max(np_ws_bytes(plan_p->np, n_ev), np_ws_bytes(plan_n->np, n_ev));
+}
+
+extern "C" int sphrad_batch_generate_alm_skys(sphrad_batch_plan *plan_p, sphrad_batch_plan *plan_n, sphrad_fseries_plan *fp, const void *ctseries, int n_ev,
+					      long long ldt, const double *gmst, const void *logprior, void *sky_p, void *sky_n, void *workspace,
+					      size_t workspace_bytes, void *stream)
+{
+	if(!plan_p->np || !plan_n->np) {
+		set_error("sphrad_batch_generate_alm_skys: plans of projected (non-polar) networks needed");
+		return -1;
+	}
+	if(n_ev <= 0)
+		return 0;
+	const int n = np_plan_n(plan_p->np);
+	if(np_plan_n(plan_n->np) != n || fseries_plan_n(fp->impl) != n || np_plan_l_max(plan_n->np) != np_plan_l_max(plan_p->np) ||
+	   np_plan_n_det(plan_n->np) != np_plan_n_det(plan_p->np)) {
+		set_error("sphrad_batch_generate_alm_skys: plans disagree in length, l_max or detectors");
+		return -1;
+	}
+	const size_t need = sphrad_batch_alm_skys_workspace_size(plan_p, plan_n, n_ev);
+	if(!workspace || workspace_bytes < need) {
+		set_error("sphrad_batch_generate_alm_skys: workspace of %zu bytes needed", need);
+		return -1;
+	}
+	void *st = stream ? stream : (void *) cudaStreamLegacy;
+	const int n_det = np_plan_n_det(plan_p->np);
+	const size_t spectra = align256((size_t) n_det * n_ev * n * 16);
+	char *F = (char *) workspace, *ws = F + spectra;
+	const size_t ws_bytes = workspace_bytes - spectra;
+	// [n_det][n_ev][ldt] series -> [n_det][n_ev][n] spectra
+	if(fseries_run_complex(fp->impl, ctseries, n_det * n_ev, ldt, F, n, st))
+		return -1;
+	struct {
+		sphrad_batch_plan *plan;
+		void *sky;
+	} sides[2] = {{plan_p, sky_p}, {plan_n, sky_n}};
+	for(auto &sd : sides) {
+		const double factor = 8.0 * np_plan_baselines(sd.plan->np);
+		if(np_run(sd.plan->np, F, n_ev, n, gmst, sd.sky, ws, ws_bytes, st) || np_alm_finish(sd.plan->np, n_ev, factor, logprior, gmst, sd.sky, st))
+			return -1;
+	}
 	return 0;
 }
 

@@ -18,6 +18,8 @@
 // of the passes and of the split is a power of e^{-2 pi i / n}: a thread
 // reads its base power from a table of the n powers (built on the host in
 // FP64) and forms the others by complex multiplication (a few roundings).
+// Complex series (correlator_ctseries_to_fseries) take the same passes over
+// all n points of a plan of n, without the split (k_cfft).
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -170,6 +172,39 @@ __global__ void __launch_bounds__(1024) k_rfft_whiten(const double *ts, long lon
 	}
 }
 
+// complex series (correlator_ctseries_to_fseries, correlator.c:235-244: an
+// unnormalised forward DFT of n complex points): the same Stockham passes
+// over all n points, no split; one CTA per series, n <= kMaxFftPoints
+__global__ void __launch_bounds__(1024) k_cfft(const double2 *ts, long long ldt, int n, const double2 *__restrict__ tw, double2 *out, long long ldf)
+{
+	extern __shared__ double2 s_fft[];
+	const double2 *src = ts + (size_t) blockIdx.x * ldt;
+	for(int t = threadIdx.x; t < n; t += blockDim.x)
+		s_fft[pad8(t)] = src[t];
+	__syncthreads();
+	int Ns = 1, rem = n;
+	while(rem >= 8) {
+		stockham_pass<8, 1>(s_fft, n, Ns, tw, n);
+		Ns *= 8;
+		rem >>= 3;
+	}
+	if(rem == 4)
+		stockham_pass<4, 2>(s_fft, n, Ns, tw, n);
+	else if(rem == 2)
+		stockham_pass<2, 4>(s_fft, n, Ns, tw, n);
+	double2 *dst = out + (size_t) blockIdx.x * ldf;
+	for(int k = threadIdx.x; k < n; k += blockDim.x)
+		dst[k] = s_fft[pad8(k)];
+}
+
+struct DevScratch {
+	void *p = nullptr;
+	explicit DevScratch(size_t bytes) { p = dmalloc(bytes); }
+	~DevScratch() { dfree(p); }
+	DevScratch(const DevScratch &) = delete;
+	DevScratch &operator=(const DevScratch &) = delete;
+};
+
 struct FseriesPlan {
 	int n = 0;
 	double *wk = nullptr;  // device whitening factors [n/2+1], or NULL
@@ -220,7 +255,8 @@ void *fseries_plan_create(int n, const double *psd)
 		if(!P->wk || h2d(P->wk, w.data(), w.size() * sizeof(double)) || stream_sync())
 			fail = true;
 	}
-	if(!fail && cudaFuncSetAttribute(k_rfft_whiten, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess) {
+	if(!fail && (cudaFuncSetAttribute(k_rfft_whiten, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
+		     cudaFuncSetAttribute(k_cfft, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess)) {
 		set_error("fseries plan: cannot reserve shared memory");
 		fail = true;
 	}
@@ -267,6 +303,48 @@ int fseries_run(void *p, const double *ts, int rows, long long ldt, void *out, l
 		set_error("tseries to fseries: launch failed (%s)", cudaGetErrorString(e));
 		return -1;
 	}
+	return 0;
+}
+
+int fseries_run_complex(void *p, const void *ts, int rows, long long ldt, void *out, long long ldf, void *stream)
+{
+	FseriesPlan *P = (FseriesPlan *) p;
+	const int n = P->n;
+	if(rows <= 0)
+		return 0;
+	if(n > kMaxFftPoints) {
+		set_error("ctseries to fseries: complex transforms take n <= %d points (plan of %d)", kMaxFftPoints, n);
+		return -1;
+	}
+	if(ldt < n || ((uintptr_t) ts & 15) || ldf < n || ((uintptr_t) out & 15)) {
+		set_error("ctseries to fseries: rows of %d points need 16-byte aligned bases and strides >= n (got %lld, %lld)", n, ldt, ldf);
+		return -1;
+	}
+	int threads = n / 8;
+	threads = threads < 32 ? 32 : (threads > 1024 ? 1024 : threads);
+	const size_t smem = (size_t) (n + n / 8) * sizeof(double2);
+	k_cfft<<<rows, threads, smem, (cudaStream_t) stream>>>((const double2 *) ts, ldt, n, P->tw, (double2 *) out, ldf);
+	const cudaError_t e = cudaGetLastError();
+	if(e != cudaSuccess) {
+		set_error("ctseries to fseries: launch failed (%s)", cudaGetErrorString(e));
+		return -1;
+	}
+	return 0;
+}
+
+int fseries_run_complex_host(void *p, const double *ts_host, int rows, double *fs_host)
+{
+	FseriesPlan *P = (FseriesPlan *) p;
+	const int n = P->n;
+	if(rows <= 0)
+		return 0;
+	const size_t bytes = (size_t) rows * n * 16;
+	DevScratch d(2 * bytes);
+	if(!d.p)
+		return -1;
+	char *din = (char *) d.p, *dout = din + bytes;
+	if(h2d(din, ts_host, bytes) || fseries_run_complex(P, din, rows, n, dout, n, lib_stream()) || d2h(fs_host, dout, bytes) || stream_sync())
+		return -1;
 	return 0;
 }
 

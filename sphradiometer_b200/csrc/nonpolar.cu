@@ -30,6 +30,7 @@
 // columns and streams the K stages through a 2-deep ring by bulk copies.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "runtime.h"
@@ -159,6 +160,25 @@ __global__ void __launch_bounds__(NP_THREADS) k_np_contract(const __grid_constan
 			const double re = acc[r][i].x, im = acc[r][i].y;
 			sky[(size_t) s * a.nq + q] = make_double2(re * cs - im * sn, re * sn + im * cs);
 		}
+	}
+}
+
+// the tail of generate_alm_sky (inspiral_sky_map.c:895-936) on S skies
+// that the integration already rotated by their GMST:
+//     sky = factor sky + rotate_z(prior, gmst),  rotate_z: (l, m) x e^{-i m gmst}
+__global__ void k_alm_finish(int S, int nq, const short *__restrict__ mq, double factor, const double2 *__restrict__ prior, const double *__restrict__ gmst,
+			     double2 *__restrict__ sky)
+{
+	const long long total = (long long) S * nq;
+	for(long long i = blockIdx.x * (long long) blockDim.x + threadIdx.x; i < total; i += (long long) gridDim.x * blockDim.x) {
+		const int s = (int) (i / nq), q = (int) (i - (long long) s * nq);
+		double sn = 0.0, cs = 1.0;
+		if(gmst)
+			sincospi(-(double) mq[q] * gmst[s] * (1.0 / M_PI), &sn, &cs);
+		double2 p = prior ? prior[q] : make_double2(0.0, 0.0);
+		p = make_double2(p.x * cs - p.y * sn, p.x * sn + p.y * cs);
+		const double2 v = sky[i];
+		sky[i] = make_double2(factor * v.x + p.x, factor * v.y + p.y);
 	}
 }
 
@@ -368,6 +388,7 @@ struct NpPlan {
 	int2 *pairs = nullptr;    // device (bi, bj) per baseline
 	unsigned *err = nullptr;
 	int Kst = 0, ntiles = 0;
+	int n_det = 0;
 };
 
 }  // namespace
@@ -386,6 +407,7 @@ void *np_plan_create(int n_det, int B, const int *bi, const int *bj, int n, unsi
 	}
 	NpPlan *P = new NpPlan();
 	P->precision = precision;
+	P->n_det = n_det;
 	const int nq = (int) ((L + 1) * (L + 1));
 	P->a.S = 0;
 	P->a.n = n;
@@ -501,6 +523,25 @@ int np_status(void *p)
 	if(cudaMemcpy(&h, P->err, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess)
 		return -1;
 	return (int) h;
+}
+
+int np_plan_baselines(const void *p) { return ((const NpPlan *) p)->a.B; }
+int np_plan_n_det(const void *p) { return ((const NpPlan *) p)->n_det; }
+
+int np_alm_finish(void *p, int S, double factor, const void *prior, const double *gmst, void *sky, void *stream)
+{
+	NpPlan *P = (NpPlan *) p;
+	if(S <= 0)
+		return 0;
+	const long long total = (long long) S * P->a.nq;
+	const int grid = (int) std::min<long long>((total + 255) / 256, 1184);
+	k_alm_finish<<<grid, 256, 0, (cudaStream_t) stream>>>(S, P->a.nq, P->mq, factor, (const double2 *) prior, gmst, (double2 *) sky);
+	const cudaError_t e = cudaGetLastError();
+	if(e != cudaSuccess) {
+		set_error("alm sky finish: launch failed (%s)", cudaGetErrorString(e));
+		return -1;
+	}
+	return 0;
 }
 
 int np_run(void *p, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream)

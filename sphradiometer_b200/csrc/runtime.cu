@@ -1064,38 +1064,11 @@ __global__ void __launch_bounds__(256) k_td_cross(int T, int t_per, int Aa, int 
 		}
 }
 
-// C = sum over the partials, in a fixed order
-__global__ void k_td_reduce(int nz, size_t len, const double2 *__restrict__ part, double2 *__restrict__ C)
-{
-	for(size_t i = blockIdx.x * (size_t) blockDim.x + threadIdx.x; i < len; i += (size_t) gridDim.x * blockDim.x) {
-		double2 acc = part[i];
-		for(int z = 1; z < nz; z++) {
-			const double2 v = part[(size_t) z * len + i];
-			acc.x += v.x;
-			acc.y += v.y;
-		}
-		C[i] = acc;
-	}
-}
-
-// q[i] = sum_{l1,l2} P~_l1(x_i) C[l1][l2] P~_l2(x_i), one block per node
-__global__ void k_td_node(int nq, int LP, int Aa, int Ab, const double *__restrict__ P, const double2 *__restrict__ C, double2 *__restrict__ q)
+// fixed-order sum of a 256-thread block's values (thread 0 gets it)
+__device__ double2 td_block_sum(double2 v)
 {
 	__shared__ double2 s_red[256];
-	const int i = blockIdx.x;
-	const double *Pi = P + (size_t) i * LP;
-	double2 acc = make_double2(0.0, 0.0);
-	for(int l2 = threadIdx.x; l2 < Ab; l2 += blockDim.x) {
-		double2 g = make_double2(0.0, 0.0);
-		for(int l1 = 0; l1 < Aa; l1++) {
-			const double2 c = C[(size_t) l1 * Ab + l2];
-			g.x += Pi[l1] * c.x;
-			g.y += Pi[l1] * c.y;
-		}
-		acc.x += g.x * Pi[l2];
-		acc.y += g.y * Pi[l2];
-	}
-	s_red[threadIdx.x] = acc;
+	s_red[threadIdx.x] = v;
 	__syncthreads();
 	for(int s = blockDim.x / 2; s > 0; s >>= 1) {
 		if(threadIdx.x < s) {
@@ -1104,23 +1077,71 @@ __global__ void k_td_node(int nq, int LP, int Aa, int Ab, const double *__restri
 		}
 		__syncthreads();
 	}
-	if(threadIdx.x == 0)
-		q[i] = s_red[0];
+	return s_red[0];
 }
 
-// power[L] = 2 pi sum_i w_i q_i P~_L(x_i), L <= Lp
-__global__ void k_td_power(int nq, int LP, int Lp, const double *__restrict__ wq, const double *__restrict__ P, const double2 *__restrict__ q, double2 *__restrict__ power)
+// C = sum over the partials: one warp per element, lanes over the
+// partials, a fixed shuffle tree (the same order on every run)
+__global__ void k_td_reduce(int nz, size_t len, const double2 *__restrict__ part, double2 *__restrict__ C)
 {
-	const int L = blockIdx.x * blockDim.x + threadIdx.x;
-	if(L > Lp)
-		return;
+	const size_t w = (blockIdx.x * (size_t) blockDim.x + threadIdx.x) >> 5;
+	const int lane = threadIdx.x & 31;
+	if(w >= len)
+		return;  // whole warps leave together
 	double2 acc = make_double2(0.0, 0.0);
-	for(int i = 0; i < nq; i++) {
-		const double f = wq[i] * P[(size_t) i * LP + L];
+	for(int z = lane; z < nz; z += 32) {
+		const double2 v = part[(size_t) z * len + w];
+		acc.x += v.x;
+		acc.y += v.y;
+	}
+#pragma unroll
+	for(int o = 16; o > 0; o >>= 1) {
+		acc.x += __shfl_xor_sync(0xffffffffu, acc.x, o);
+		acc.y += __shfl_xor_sync(0xffffffffu, acc.y, o);
+	}
+	if(lane == 0)
+		C[w] = acc;
+}
+
+// q[i] = sum_{l1,l2} P~_l1(x_i) C[l1][l2] P~_l2(x_i), one 256-thread block
+// per node: lanes over l2, the 8 warps over l1
+__global__ void __launch_bounds__(256) k_td_node(int nq, int LP, int Aa, int Ab, const double *__restrict__ P, const double2 *__restrict__ C,
+						 double2 *__restrict__ q)
+{
+	const int i = blockIdx.x, lane = threadIdx.x & 31, grp = threadIdx.x >> 5;
+	const double *Pi = P + (size_t) i * LP;
+	double2 acc = make_double2(0.0, 0.0);
+	for(int l2 = lane; l2 < Ab; l2 += 32) {
+		double2 g = make_double2(0.0, 0.0);
+		for(int l1 = grp; l1 < Aa; l1 += 8) {
+			const double2 c = C[(size_t) l1 * Ab + l2];
+			g.x += Pi[l1] * c.x;
+			g.y += Pi[l1] * c.y;
+		}
+		acc.x += g.x * Pi[l2];
+		acc.y += g.y * Pi[l2];
+	}
+	const double2 t = td_block_sum(acc);
+	if(threadIdx.x == 0)
+		q[i] = t;
+}
+
+// power[L] = 2 pi sum_i w_i q_i P~_L(x_i), one 256-thread block per L <= Lp
+// (PT: the degree-major table, PT[L][i])
+__global__ void __launch_bounds__(256) k_td_power(int nq, const double *__restrict__ wq, const double *__restrict__ PT, const double2 *__restrict__ q,
+						  double2 *__restrict__ power)
+{
+	const int L = blockIdx.x;
+	const double *PL = PT + (size_t) L * nq;
+	double2 acc = make_double2(0.0, 0.0);
+	for(int i = threadIdx.x; i < nq; i += blockDim.x) {
+		const double f = wq[i] * PL[i];
 		acc.x += f * q[i].x;
 		acc.y += f * q[i].y;
 	}
-	power[L] = make_double2(2.0 * M_PI * acc.x, 2.0 * M_PI * acc.y);
+	const double2 t = td_block_sum(acc);
+	if(threadIdx.x == 0)
+		power[L] = make_double2(2.0 * M_PI * t.x, 2.0 * M_PI * t.y);
 }
 
 // a typed view of a piece of the arena
@@ -1166,13 +1187,13 @@ int td_power_1d(int T, int n_ela, int n_elb, int Aa, int Ab, const double *taps_
 	const int La = Aa - 1, Lb = Ab - 1;
 	const int nq = ((int) Lp + La + Lb) / 2 + 1;
 	const int LP = std::max(std::max(Aa, Ab), (int) Lp + 1);
-	// split the sample sum so that about two blocks per SM run
+	// split the sample sum so that about four blocks per SM run
 	int dev = 0, sms = 148;
 	cudaGetDevice(&dev);
 	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 	const int tiles = ((Aa + 31) / 32) * ((Ab + 31) / 32);
-	int nz = (2 * sms + tiles - 1) / tiles;
-	nz = std::max(1, std::min(nz, (T + 255) / 256));
+	int nz = (4 * sms + tiles - 1) / tiles;
+	nz = std::max(1, std::min(nz, (T + 63) / 64));
 	const int t_per = ((T + nz - 1) / nz + 31) / 32 * 32;
 	nz = (T + t_per - 1) / t_per;
 	const size_t clen = (size_t) Aa * Ab;
@@ -1198,11 +1219,11 @@ int td_power_1d(int T, int n_ela, int n_elb, int Aa, int Ab, const double *taps_
 	k_td_samples<<<dim3((T + kTdTT - 1) / kTdTT, (Aa + kTdTL - 1) / kTdTL), 256, 0, s>>>(T, n_ela, Aa, dta.as<double2>(), dxa.as<double>(), dSa.as<double2>());
 	k_td_samples<<<dim3((T + kTdTT - 1) / kTdTT, (Ab + kTdTL - 1) / kTdTL), 256, 0, s>>>(T, n_elb, Ab, dtb.as<double2>(), dxb.as<double>(), dSb.as<double2>());
 	k_td_cross<<<dim3((Ab + 31) / 32, (Aa + 31) / 32, nz), 256, 0, s>>>(T, t_per, Aa, Ab, dw.as<double>(), dSa.as<double2>(), dSb.as<double2>(), dpart.as<double2>());
-	k_td_reduce<<<(int) std::min<size_t>((clen + 255) / 256, 1024), 256, 0, s>>>(nz, clen, dpart.as<double2>(), dC.as<double2>());
+	k_td_reduce<<<(int) ((clen * 32 + 255) / 256), 256, 0, s>>>(nz, clen, dpart.as<double2>(), dC.as<double2>());
 	k_gl_nodes<<<(nq / 2 + 1 + 127) / 128, 128, 0, s>>>(nq, dx.as<double>(), dwq.as<double>());
 	k_plm0_table<<<(nq + 127) / 128, 128, 0, s>>>(nq, dx.as<double>(), LP, dP.as<double>(), dPT.as<double>());
 	k_td_node<<<nq, 256, 0, s>>>(nq, LP, Aa, Ab, dP.as<double>(), dC.as<double2>(), dq.as<double2>());
-	k_td_power<<<((int) Lp + 1 + 127) / 128, 128, 0, s>>>(nq, LP, (int) Lp, dwq.as<double>(), dP.as<double>(), dq.as<double2>(), dpow.as<double2>());
+	k_td_power<<<(int) Lp + 1, 256, 0, s>>>(nq, dwq.as<double>(), dPT.as<double>(), dq.as<double2>(), dpow.as<double2>());
 	CK(cudaGetLastError());
 	if(d2h(power_host, dpow.p, ((size_t) Lp + 1) * 16) || stream_sync())
 		return -1;

@@ -118,6 +118,11 @@ int fseries_run(void *plan, const double *ts, int rows, long long ldt, void *out
 // one host series -> the full n-bin host spectrum (upper half by Hermitian
 // symmetry); synchronous
 int fseries_run_host(void *plan, const double *ts_host, double *fs_host);
+// rows complex device series of n points (row r at ts + r ldt complex) ->
+// their unnormalised forward DFTs (row r at out + r ldf), n <= 8192
+int fseries_run_complex(void *plan, const void *ts, int rows, long long ldt, void *out, long long ldf, void *stream);
+// rows contiguous host series -> host spectra; synchronous
+int fseries_run_complex_host(void *plan, const double *ts_host, int rows, double *fs_host);
 
 // ---- projection operator x delay kernel (projection.cu) ----------------
 // For every bin j < n: the projection P_ab of bin j (antenna patterns
@@ -155,6 +160,11 @@ int np_plan_n(const void *plan);
 size_t np_ws_bytes(const void *plan, int S);
 int np_run(void *plan, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream);
 int np_status(void *plan);  // 0, or the code of a device wait that gave up
+int np_plan_baselines(const void *plan);
+int np_plan_n_det(const void *plan);
+// sky[s] = factor sky[s] + rotate_z(prior, gmst[s]) for S skies of the
+// plan's layout; prior: device (L+1)^2 complex or NULL; gmst device or NULL
+int np_alm_finish(void *plan, int S, double factor, const void *prior, const double *gmst, void *sky, void *stream);
 
 // ---- uneven batches (uneven.cu) -----------------------------------------
 // F[d][i][k] = in[in_off[seg[i]] + det[d] Ku + k] for a job of S segments

@@ -18,6 +18,9 @@ stages:
             (k_rfft_whiten)
   nonpolar  N segments through projected (non-polar) c1 plans on the
             tensor cores (k_np_build_a, k_np_tc)
+  td        the time-domain network correlator on the reference's
+            validation setup (4 detectors, 512 Hz, N = 32438 samples; host
+            series): k_td_samples, k_td_cross, k_td_node, k_td_power
 
 Each stage builds its inputs, runs once untimed, then ``--calls`` times and
 prints the mean device time per call (CUDA events).
@@ -42,7 +45,7 @@ def c1_skies(S, W, n):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("stage", choices=["render", "peaks", "rotate", "product", "mlp", "uneven", "fseries", "nonpolar"])
+    ap.add_argument("stage", choices=["render", "peaks", "rotate", "product", "mlp", "uneven", "fseries", "nonpolar", "td"])
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--calls", type=int, default=3)
     args = ap.parse_args()
@@ -110,6 +113,14 @@ def main():
         out = torch.empty((n, 33 * 33), dtype=torch.complex128, device="cuda")
         keep = [net, bp, rows]
         run = lambda: bp.integrate(F, g, out=out)  # noqa: E731
+    elif args.stage == "td":
+        rng = np.random.Generator(np.random.Philox(11))
+        pos = W.random_positions(4, W.R_EARTH_S, rng)
+        net = S.TimeDomainNetwork(pos, 1.0 / 512)
+        ts = rng.normal(size=(4, n))
+        wins = [np.full(n - 2 * net.transient(k), 1.0 / (n - 2 * net.transient(k))) for k in range(net.n_baselines)]
+        keep = [net]
+        run = lambda: net.integrate(ts, wins)  # noqa: E731
     elif args.stage == "fseries":
         pos = W.random_positions(3, W.R_EARTH_S, W.rng_for(2))
         b = W.make_tseries_batch(pos, 4096, 1.0 / 4096, 256, seed=5)
