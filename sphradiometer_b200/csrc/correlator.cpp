@@ -854,6 +854,28 @@ extern "C" struct sh_series *correlator_baseline_integrate_power_td(const double
 	return out;
 }
 
+// rows D^l_{0 m'} (m' = -l .. l at offset l^2, l = 0 row 1) of a rotation
+// plan, the polar rotation of sh_series_rotate (sh_series_rotation.c:566-577)
+static int polar_rotation_rows(const struct sh_series_rotation_plan *rp, unsigned L, std::vector<dcplx> &rows)
+{
+	if(rp->l_max < L) {
+		set_error("time-domain correlator: rotation plan l_max %u below the power's %u", rp->l_max, L);
+		return -1;
+	}
+	std::vector<dcplx> scratch;
+	const double *flat = (const double *) rotation_plan_flat_for(rp, scratch);
+	rows.assign(((size_t) L + 1) * (L + 1), mk(0.0, 0.0));
+	rows[0] = mk(1.0, 0.0);
+	for(unsigned l = 1; l <= L; l++) {
+		const double *Dl = flat + 2 * rot_offset(l);
+		for(int mp = -(int) l; mp <= (int) l; mp++) {
+			const size_t e = (size_t) (2 * l + 1) * (mp + l) + l;
+			rows[(size_t) l * l + mp + l] = mk(Dl[2 * e], Dl[2 * e + 1]);
+		}
+	}
+	return 0;
+}
+
 extern "C" struct sh_series *correlator_network_integrate_power_td(struct sh_series *sky, double **tseries, int n, double **windows,
 								   struct correlator_network_plan_td *plan)
 {
@@ -862,28 +884,61 @@ extern "C" struct sh_series *correlator_network_integrate_power_td(struct sh_ser
 		set_error("correlator_network_integrate_power_td: empty network or polar sky");
 		return NULL;
 	}
-	for(int k = 0; k < nb; k++)
-		if(plan->plans[k]->power_1d->l_max > sky->l_max) {
-			set_error("correlator_network_integrate_power_td: sky l_max below a baseline's");
-			return NULL;
-		}
 	const int nd = instrument_array_len(plan->baselines->baselines[0]->instruments);
 	if(nd * (nd - 1) / 2 != nb) {
 		set_error("correlator_network_integrate_power_td: network and instrument count disagree");
 		return NULL;
 	}
-	sh_series_zero(sky);
+	// every baseline in one device pass: series uploaded once, all
+	// baselines' samples, sums and contractions queued, the rotations and
+	// the network mean in one kernel (correlator.c:967-984)
+	std::vector<TdBaseline> bl(nb);
+	std::vector<std::vector<dcplx>> ta(nb), tb(nb), rows(nb);
 	int k = 0;
 	for(int i = 1; i < nd; i++)
 		for(int j = 0; j < i; j++, k++) {
-			struct sh_series *p2 = correlator_baseline_integrate_power_td(tseries[i], tseries[j], windows[k], n, plan->plans[k]);
-			if(!p2)
+			struct correlator_plan_td *p = plan->plans[k];
+			const struct sh_series_array *pa = p->proj_a, *pb = p->proj_b;
+			if(!pa->polar || !pb->polar || !p->power_1d->polar || pa->l_max != p->sample_a->l_max || pb->l_max != p->sample_b->l_max ||
+			   pa->n > 2 * p->transient + 1 || pb->n > 2 * p->transient + 1) {
+				set_error("correlator_network_integrate_power_td: plan %d's projections and series disagree", k);
 				return NULL;
-			const bool ok = sh_series_add(sky, 1.0 / nb, p2) != NULL;
-			sh_series_free(p2);
-			if(!ok)
+			}
+			if(p->power_1d->l_max > sky->l_max) {
+				set_error("correlator_network_integrate_power_td: sky l_max below a baseline's");
 				return NULL;
+			}
+			const int T = n - 2 * p->transient;
+			if(T < 0) {
+				set_error("correlator_network_integrate_power_td: %d samples, transient %d", n, p->transient);
+				return NULL;
+			}
+			ta[k] = array_taps(pa);
+			tb[k] = array_taps(pb);
+			const unsigned Lp = std::min(p->power_1d->l_max, pa->l_max + pb->l_max);
+			if(polar_rotation_rows(p->rotation_plan, Lp, rows[k]))
+				return NULL;
+			sh_series_zero(p->power_1d);
+			TdBaseline &B = bl[k];
+			B.T = T;
+			B.n_ela = pa->n;
+			B.n_elb = pb->n;
+			B.Aa = (int) pa->l_max + 1;
+			B.Ab = (int) pb->l_max + 1;
+			B.det_a = i;
+			B.det_b = j;
+			B.taps_a = (const double *) ta[k].data();
+			B.taps_b = (const double *) tb[k].data();
+			B.window = windows[k];
+			B.Lp = Lp;
+			B.rot_rows = (const double *) rows[k].data();
+			B.power_host = (double *) p->power_1d->coeff;
 		}
+	if(td_network(bl.data(), nb, nd, n, (const double *const *) tseries, 1.0 / nb, sky->l_max, (double *) sky->coeff))
+		return NULL;
+	for(k = 0; k < nb; k++)
+		note_write(plan->plans[k]->power_1d->coeff);
+	note_write(sky->coeff);
 	return sky;
 }
 

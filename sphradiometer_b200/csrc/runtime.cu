@@ -972,6 +972,10 @@ constexpr int kTdTT = 64, kTdTL = 32, kTdTE = 32;  // samples tile: t x l, taps 
 // S[t][l] = sum_e taps[e][l] x[t + e], t < T, l < A (sh_series_array_dot
 // from each sample, sh_series_array.c:407-426).  Block: 64 samples x 32
 // harmonics, 256 threads, 8 samples per thread.
+// REAL: every tap is real (the polar projections of a phase centre on the
+// z axis are), so only the real parts are formed; the imaginary parts are
+// written as zeros
+template <bool REAL>
 __global__ void __launch_bounds__(256) k_td_samples(int T, int n_el, int A, const double2 *__restrict__ taps, const double *__restrict__ x, double2 *__restrict__ S)
 {
 	__shared__ double2 s_tap[kTdTE][kTdTL];
@@ -1001,7 +1005,8 @@ __global__ void __launch_bounds__(256) k_td_samples(int T, int n_el, int A, cons
 			for(int k = 0; k < 8; k++) {
 				const double v = s_x[ty + 8 * k + e];
 				acc[k].x += c.x * v;
-				acc[k].y += c.y * v;
+				if(!REAL)
+					acc[k].y += c.y * v;
 			}
 		}
 		__syncthreads();
@@ -1018,7 +1023,9 @@ __global__ void __launch_bounds__(256) k_td_samples(int T, int n_el, int A, cons
 
 // partial C over the sample range of blockIdx.z:
 // part[z][l1][l2] = sum_t w[t] Sa[t][l1] Sb[t][l2].  Block: 32 x 32
-// outputs, 256 threads, 4 per thread.
+// outputs, 256 threads, 4 per thread.  REAL: the samples are real (real
+// taps), so are C's entries.
+template <bool REAL>
 __global__ void __launch_bounds__(256) k_td_cross(int T, int t_per, int Aa, int Ab, const double *__restrict__ w, const double2 *__restrict__ Sa,
 						  const double2 *__restrict__ Sb, double2 *__restrict__ part)
 {
@@ -1048,8 +1055,12 @@ __global__ void __launch_bounds__(256) k_td_cross(int T, int t_per, int Aa, int 
 #pragma unroll
 			for(int k = 0; k < 4; k++) {
 				const double2 a = s_a[tt][ty + 8 * k];
-				acc[k].x += a.x * b.x - a.y * b.y;
-				acc[k].y += a.x * b.y + a.y * b.x;
+				if(REAL)
+					acc[k].x += a.x * b.x;
+				else {
+					acc[k].x += a.x * b.x - a.y * b.y;
+					acc[k].y += a.x * b.y + a.y * b.x;
+				}
 			}
 		}
 		__syncthreads();
@@ -1171,10 +1182,104 @@ TdArena g_td_arena;
 
 }  // namespace
 
+// shapes of one baseline's time-domain pass
+struct TdShape {
+	int T, n_ela, n_elb, Aa, Ab, nq, LP, nz, t_per;
+	unsigned Lp;
+	size_t clen;
+	bool real;  // every tap real
+};
+
+// true when every imaginary part of the complex [n][A] taps is zero
+static bool taps_real(const double *taps, int n, int A)
+{
+	for(size_t i = 0; i < (size_t) n * A; i++)
+		if(taps[2 * i + 1] != 0.0)
+			return false;
+	return true;
+}
+
+static TdShape td_shape(int T, int n_ela, int n_elb, int Aa, int Ab, unsigned Lp, bool real)
+{
+	TdShape h;
+	h.real = real;
+	h.T = T;
+	h.n_ela = n_ela;
+	h.n_elb = n_elb;
+	h.Aa = Aa;
+	h.Ab = Ab;
+	h.Lp = Lp;
+	h.nq = ((int) Lp + (Aa - 1) + (Ab - 1)) / 2 + 1;
+	h.LP = std::max(std::max(Aa, Ab), (int) Lp + 1);
+	h.clen = (size_t) Aa * Ab;
+	// split the sample sum so that about four blocks per SM run
+	int dev = 0, sms = 148;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	const int tiles = ((Aa + 31) / 32) * ((Ab + 31) / 32);
+	int nz = (4 * sms + tiles - 1) / tiles;
+	nz = std::max(1, std::min(nz, (T + 63) / 64));
+	h.t_per = ((T + nz - 1) / nz + 31) / 32 * 32;
+	h.nz = std::max(1, (T + h.t_per - 1) / h.t_per);
+	return h;
+}
+
+// device scratch of one pass: taps a, taps b, window, S_a, S_b, partials,
+// C, nodes, weights, P, PT, q, power
+constexpr int kTdBufs = 13;
+
+static void td_sizes(const TdShape &h, size_t *sz)
+{
+	const size_t T = (size_t) h.T;
+	const size_t v[kTdBufs] = {(size_t) h.n_ela * h.Aa * 16, (size_t) h.n_elb * h.Ab * 16, T * 8, T * h.Aa * 16, T * h.Ab * 16, (size_t) h.nz * h.clen * 16,
+				   h.clen * 16, (size_t) h.nq * 8, (size_t) h.nq * 8, (size_t) h.nq * h.LP * 8, (size_t) h.nq * h.LP * 8, (size_t) h.nq * 16,
+				   ((size_t) h.Lp + 1) * 16};
+	for(int i = 0; i < kTdBufs; i++)
+		sz[i] = (v[i] + 255) / 256 * 256;
+}
+
+// the kernels of one pass; xa, xb: device series; b[]: the buffers of
+// td_sizes; power_1d lands in b[12]
+static int td_launch(const TdShape &h, const double *xa, const double *xb, char *const *b, cudaStream_t s)
+{
+	const int T = h.T, Aa = h.Aa, Ab = h.Ab, nq = h.nq, LP = h.LP;
+	if(T == 0) {
+		CK(cudaMemsetAsync(b[12], 0, ((size_t) h.Lp + 1) * 16, s));
+		return 0;
+	}
+	const double2 *ta = (const double2 *) b[0], *tb = (const double2 *) b[1];
+	const double *w = (const double *) b[2];
+	double2 *Sa = (double2 *) b[3], *Sb = (double2 *) b[4], *part = (double2 *) b[5], *C = (double2 *) b[6], *q = (double2 *) b[11], *pw = (double2 *) b[12];
+	double *x = (double *) b[7], *wq = (double *) b[8], *P = (double *) b[9], *PT = (double *) b[10];
+	const dim3 ga((T + kTdTT - 1) / kTdTT, (Aa + kTdTL - 1) / kTdTL), gb((T + kTdTT - 1) / kTdTT, (Ab + kTdTL - 1) / kTdTL),
+		gc((Ab + 31) / 32, (Aa + 31) / 32, h.nz);
+	if(h.real) {
+		k_td_samples<true><<<ga, 256, 0, s>>>(T, h.n_ela, Aa, ta, xa, Sa);
+		k_td_samples<true><<<gb, 256, 0, s>>>(T, h.n_elb, Ab, tb, xb, Sb);
+		k_td_cross<true><<<gc, 256, 0, s>>>(T, h.t_per, Aa, Ab, w, Sa, Sb, part);
+	} else {
+		k_td_samples<false><<<ga, 256, 0, s>>>(T, h.n_ela, Aa, ta, xa, Sa);
+		k_td_samples<false><<<gb, 256, 0, s>>>(T, h.n_elb, Ab, tb, xb, Sb);
+		k_td_cross<false><<<gc, 256, 0, s>>>(T, h.t_per, Aa, Ab, w, Sa, Sb, part);
+	}
+	k_td_reduce<<<(int) ((h.clen * 32 + 255) / 256), 256, 0, s>>>(h.nz, h.clen, part, C);
+	k_gl_nodes<<<(nq / 2 + 1 + 127) / 128, 128, 0, s>>>(nq, x, wq);
+	k_plm0_table<<<(nq + 127) / 128, 128, 0, s>>>(nq, x, LP, P, PT);
+	k_td_node<<<nq, 256, 0, s>>>(nq, LP, Aa, Ab, P, C, q);
+	k_td_power<<<(int) h.Lp + 1, 256, 0, s>>>(nq, wq, PT, q, pw);
+	CK(cudaGetLastError());
+	return 0;
+}
+
+static bool td_valid(int T, int n_ela, int n_elb, int Aa, int Ab, long long n_x)
+{
+	return T >= 0 && n_ela > 0 && n_elb > 0 && Aa > 0 && Ab > 0 && (long long) T + n_ela - 1 <= n_x && (long long) T + n_elb - 1 <= n_x;
+}
+
 int td_power_1d(int T, int n_ela, int n_elb, int Aa, int Ab, const double *taps_a, const double *taps_b, const double *xa, const double *xb, long long n_x,
 		const double *w, unsigned Lp, double *power_host)
 {
-	if(T < 0 || n_ela <= 0 || n_elb <= 0 || Aa <= 0 || Ab <= 0 || (long long) T + n_ela - 1 > n_x || (long long) T + n_elb - 1 > n_x) {
+	if(!td_valid(T, n_ela, n_elb, Aa, Ab, n_x)) {
 		set_error("time-domain correlator: %d samples of %lld with %d- and %d-tap projections", T, n_x, n_ela, n_elb);
 		return -1;
 	}
@@ -1184,50 +1289,115 @@ int td_power_1d(int T, int n_ela, int n_elb, int Aa, int Ab, const double *taps_
 	}
 	if(ensure_device())
 		return -1;
-	const int La = Aa - 1, Lb = Ab - 1;
-	const int nq = ((int) Lp + La + Lb) / 2 + 1;
-	const int LP = std::max(std::max(Aa, Ab), (int) Lp + 1);
-	// split the sample sum so that about four blocks per SM run
-	int dev = 0, sms = 148;
-	cudaGetDevice(&dev);
-	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-	const int tiles = ((Aa + 31) / 32) * ((Ab + 31) / 32);
-	int nz = (4 * sms + tiles - 1) / tiles;
-	nz = std::max(1, std::min(nz, (T + 63) / 64));
-	const int t_per = ((T + nz - 1) / nz + 31) / 32 * 32;
-	nz = (T + t_per - 1) / t_per;
-	const size_t clen = (size_t) Aa * Ab;
+	const TdShape h = td_shape(T, n_ela, n_elb, Aa, Ab, Lp, taps_real(taps_a, n_ela, Aa) && taps_real(taps_b, n_elb, Ab));
+	size_t sz[kTdBufs];
+	td_sizes(h, sz);
+	const size_t xa_b = ((size_t) (T + n_ela - 1) * 8 + 255) / 256 * 256, xb_b = ((size_t) (T + n_elb - 1) * 8 + 255) / 256 * 256;
+	size_t total = xa_b + xb_b;
+	for(int i = 0; i < kTdBufs; i++)
+		total += sz[i];
 	// one grow-only device arena per device, held for the whole call
-	const size_t sizes[15] = {(size_t) n_ela * Aa * 16, (size_t) n_elb * Ab * 16, (size_t) (T + n_ela - 1) * 8, (size_t) (T + n_elb - 1) * 8, (size_t) T * 8,
-				  (size_t) T * Aa * 16,	      (size_t) T * Ab * 16,	  (size_t) nz * clen * 16,	 clen * 16,			(size_t) nq * 8,
-				  (size_t) nq * 8,	      (size_t) nq * LP * 8,	  (size_t) nq * LP * 8,	 (size_t) nq * 16,		((size_t) Lp + 1) * 16};
-	size_t offs[15], total = 0;
-	for(int i = 0; i < 15; i++) {
-		offs[i] = total;
-		total += (sizes[i] + 255) / 256 * 256;
+	std::lock_guard<std::mutex> lock(g_td_arena.mu);
+	char *base = (char *) g_td_arena.get(total);
+	if(!base)
+		return -1;
+	char *dxa = base, *dxb = base + xa_b, *b[kTdBufs];
+	size_t o = xa_b + xb_b;
+	for(int i = 0; i < kTdBufs; i++) {
+		b[i] = base + o;
+		o += sz[i];
+	}
+	if(h2d(b[0], taps_a, (size_t) n_ela * Aa * 16) || h2d(b[1], taps_b, (size_t) n_elb * Ab * 16) || h2d(dxa, xa, (size_t) (T + n_ela - 1) * 8) ||
+	   h2d(dxb, xb, (size_t) (T + n_elb - 1) * 8) || h2d(b[2], w, (size_t) T * 8))
+		return -1;
+	if(td_launch(h, (const double *) dxa, (const double *) dxb, b, S()))
+		return -1;
+	if(d2h(power_host, b[12], ((size_t) Lp + 1) * 16) || stream_sync())
+		return -1;
+	return 0;
+}
+
+int td_network(const TdBaseline *bl, int nb, int n_det, long long n, const double *const *series, double weight, unsigned sky_L, double *sky_host)
+{
+	if(nb <= 0 || n_det <= 0 || n <= 0) {
+		set_error("time-domain network: %d baselines, %d detectors, %lld samples", nb, n_det, n);
+		return -1;
+	}
+	for(int k = 0; k < nb; k++) {
+		const TdBaseline &B = bl[k];
+		if(!td_valid(B.T, B.n_ela, B.n_elb, B.Aa, B.Ab, n) || B.det_a < 0 || B.det_a >= n_det || B.det_b < 0 || B.det_b >= n_det || B.Lp > sky_L ||
+		   B.Lp > (unsigned) (B.Aa - 1 + B.Ab - 1)) {
+			set_error("time-domain network: baseline %d does not fit (%d samples of %lld, l_max %u of %u)", k, B.T, n, B.Lp, sky_L);
+			return -1;
+		}
+	}
+	if(ensure_device())
+		return -1;
+	// arena: series, sky, jobs, then per baseline its pass buffers and rotation rows
+	std::vector<TdShape> sh(nb);
+	std::vector<size_t> sz((size_t) nb * kTdBufs), rot_b(nb);
+	const size_t ser_b = ((size_t) n_det * n * 8 + 255) / 256 * 256, sky_len = ((size_t) sky_L + 1) * (sky_L + 1);
+	const size_t sky_b = (sky_len * 16 + 255) / 256 * 256, job_b = ((size_t) nb * sizeof(DevJob) + 255) / 256 * 256;
+	size_t total = ser_b + sky_b + job_b;
+	for(int k = 0; k < nb; k++) {
+		sh[k] = td_shape(bl[k].T, bl[k].n_ela, bl[k].n_elb, bl[k].Aa, bl[k].Ab, bl[k].Lp,
+				 taps_real(bl[k].taps_a, bl[k].n_ela, bl[k].Aa) && taps_real(bl[k].taps_b, bl[k].n_elb, bl[k].Ab));
+		td_sizes(sh[k], &sz[(size_t) k * kTdBufs]);
+		for(int i = 0; i < kTdBufs; i++)
+			total += sz[(size_t) k * kTdBufs + i];
+		rot_b[k] = (((size_t) bl[k].Lp + 1) * (bl[k].Lp + 1) * 16 + 255) / 256 * 256;
+		total += rot_b[k];
 	}
 	std::lock_guard<std::mutex> lock(g_td_arena.mu);
 	char *base = (char *) g_td_arena.get(total);
 	if(!base)
 		return -1;
-	TdSpan dta{base + offs[0]}, dtb{base + offs[1]}, dxa{base + offs[2]}, dxb{base + offs[3]}, dw{base + offs[4]}, dSa{base + offs[5]}, dSb{base + offs[6]},
-		dpart{base + offs[7]}, dC{base + offs[8]}, dx{base + offs[9]}, dwq{base + offs[10]}, dP{base + offs[11]}, dPT{base + offs[12]}, dq{base + offs[13]},
-		dpow{base + offs[14]};
-	if(h2d(dta.p, taps_a, sizes[0]) || h2d(dtb.p, taps_b, sizes[1]) || h2d(dxa.p, xa, sizes[2]) || h2d(dxb.p, xb, sizes[3]) || h2d(dw.p, w, sizes[4]))
-		return -1;
+	char *dser = base, *dsky = base + ser_b, *djobs = dsky + sky_b;
+	size_t o = ser_b + sky_b + job_b;
+	for(int d = 0; d < n_det; d++)
+		if(h2d(dser + (size_t) d * n * 8, series[d], (size_t) n * 8))
+			return -1;
 	cudaStream_t s = S();
-	k_td_samples<<<dim3((T + kTdTT - 1) / kTdTT, (Aa + kTdTL - 1) / kTdTL), 256, 0, s>>>(T, n_ela, Aa, dta.as<double2>(), dxa.as<double>(), dSa.as<double2>());
-	k_td_samples<<<dim3((T + kTdTT - 1) / kTdTT, (Ab + kTdTL - 1) / kTdTL), 256, 0, s>>>(T, n_elb, Ab, dtb.as<double2>(), dxb.as<double>(), dSb.as<double2>());
-	k_td_cross<<<dim3((Ab + 31) / 32, (Aa + 31) / 32, nz), 256, 0, s>>>(T, t_per, Aa, Ab, dw.as<double>(), dSa.as<double2>(), dSb.as<double2>(), dpart.as<double2>());
-	k_td_reduce<<<(int) ((clen * 32 + 255) / 256), 256, 0, s>>>(nz, clen, dpart.as<double2>(), dC.as<double2>());
-	k_gl_nodes<<<(nq / 2 + 1 + 127) / 128, 128, 0, s>>>(nq, dx.as<double>(), dwq.as<double>());
-	k_plm0_table<<<(nq + 127) / 128, 128, 0, s>>>(nq, dx.as<double>(), LP, dP.as<double>(), dPT.as<double>());
-	k_td_node<<<nq, 256, 0, s>>>(nq, LP, Aa, Ab, dP.as<double>(), dC.as<double2>(), dq.as<double2>());
-	k_td_power<<<(int) Lp + 1, 256, 0, s>>>(nq, dwq.as<double>(), dPT.as<double>(), dq.as<double2>(), dpow.as<double2>());
-	CK(cudaGetLastError());
-	if(d2h(power_host, dpow.p, ((size_t) Lp + 1) * 16) || stream_sync())
+	std::vector<DevJob> dj(nb);
+	std::vector<char *> pw(nb);
+	for(int k = 0; k < nb; k++) {
+		const TdBaseline &B = bl[k];
+		char *b[kTdBufs];
+		for(int i = 0; i < kTdBufs; i++) {
+			b[i] = base + o;
+			o += sz[(size_t) k * kTdBufs + i];
+		}
+		char *drot = base + o;
+		o += rot_b[k];
+		const size_t rl = ((size_t) B.Lp + 1) * (B.Lp + 1);
+		if(h2d(b[0], B.taps_a, (size_t) B.n_ela * B.Aa * 16) || h2d(b[1], B.taps_b, (size_t) B.n_elb * B.Ab * 16) ||
+		   (B.T > 0 && h2d(b[2], B.window, (size_t) B.T * 8)) || h2d(drot, B.rot_rows, rl * 16))
+			return -1;
+		if(td_launch(sh[k], (const double *) (dser + (size_t) B.det_a * n * 8), (const double *) (dser + (size_t) B.det_b * n * 8), b, s))
+			return -1;
+		// the rotation and network sum (correlator.c:665-670, 976-981) as
+		// the FD integrator's: power_1d is already normalised (n = 1)
+		DevJob &J = dj[k];
+		memset(&J, 0, sizeof(J));
+		J.rot = (const double2 *) drot;
+		J.P = (double2 *) b[12];
+		J.n = 1;
+		J.stride = (int) B.Lp + 1;
+		J.l_max = (int) B.Lp;
+		J.polar = 1;
+		J.weight = weight;
+		pw[k] = b[12];
+	}
+	if(h2d(djobs, dj.data(), (size_t) nb * sizeof(DevJob)))
 		return -1;
-	return 0;
+	k_rotate_sum<<<2 * sky_L + 1, 64, 0, s>>>((const DevJob *) djobs, nb, (int) sky_L, (double2 *) dsky);
+	CK(cudaGetLastError());
+	if(d2h(sky_host, dsky, sky_len * 16))
+		return -1;
+	for(int k = 0; k < nb; k++)
+		if(bl[k].power_host && d2h(bl[k].power_host, pw[k], ((size_t) bl[k].Lp + 1) * 16))
+			return -1;
+	return stream_sync();
 }
 
 }  // namespace sphrad

@@ -146,6 +146,21 @@ int projection_taps_full(const double *r, double delta_t, int n_el, unsigned L, 
 // x: n_x >= T + n_el - 1 samples; power_host: complex [Lp + 1]
 int td_power_1d(int T, int n_ela, int n_elb, int Aa, int Ab, const double *taps_a, const double *taps_b, const double *xa, const double *xb, long long n_x,
 		const double *w, unsigned Lp, double *power_host);
+// one baseline of a network pass
+struct TdBaseline {
+	int T, n_ela, n_elb, Aa, Ab;
+	int det_a, det_b;        // rows of the series
+	const double *taps_a;    // host complex [n_ela][Aa]
+	const double *taps_b;    // host complex [n_elb][Ab]
+	const double *window;    // host [T]
+	unsigned Lp;             // power l_max
+	const double *rot_rows;  // host complex [(Lp+1)^2]: row l at l^2, D^l_{0 m'} for m' = -l .. l
+	double *power_host;      // host complex [Lp + 1] out (unrotated), or NULL
+};
+// the whole network in one device pass (correlator.c:967-984): every
+// baseline's power_1d, rotated and summed with weight into the sky
+// (host complex [(sky_L+1)^2]); series: n_det host rows of n samples
+int td_network(const TdBaseline *bl, int nb, int n_det, long long n, const double *const *series, double weight, unsigned sky_L, double *sky_host);
 
 // ---- batched integration with non-polar kernels (nonpolar.cu) ---------
 // D[b]: host [n][(L+1)^2] complex non-polar delay kernels; rot[b]: host

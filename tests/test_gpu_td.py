@@ -97,7 +97,8 @@ def test_baseline_integrator_matches_oracle():
 
 
 def test_network_integrator_matches_oracle():
-    """3 detectors, Tukey windows, sky at the network's l_max."""
+    """3 detectors, Tukey windows, the sky at the network's l_max and two
+    degrees above it; each plan's power_1d keeps its unrotated sum."""
     import sphradiometer_b200 as S
     dt = 1.0 / 512
     pos = W.random_positions(3, W.R_EARTH_S, W.rng_for(32))
@@ -105,7 +106,7 @@ def test_network_integrator_matches_oracle():
     rng = np.random.Generator(np.random.Philox(6))
     n = 2 * max(net.transient(k) for k in range(3)) + 257
     ts = rng.normal(size=(3, n))
-    wins, ref = [], np.zeros(O.length(net.l_max, False), np.complex128)
+    wins, ref, p1 = [], np.zeros(O.length(net.l_max, False), np.complex128), []
     k = 0
     for i in range(1, 3):
         for j in range(i):
@@ -119,9 +120,15 @@ def test_network_integrator_matches_oracle():
             pl = net.power_l_max(k)
             p = O.baseline_integrate_power_td(ts[i], ts[j], w, dl, dt, pl, O.rotation_plan(pl, O.rot_matrix(th, ph)))
             ref += O.assign(p, pl, False, net.l_max, False) / 3
+            u = O.baseline_integrate_power_td(ts[i], ts[j], w, dl, dt, pl, O.rotation_plan(pl, O.rot_matrix(0.0, 0.0)))
+            p1.append(O.assign(u, pl, False, pl, True))
             k += 1
     got = net.integrate(ts, wins)
     assert _rel(got, ref) < TOL
+    for k in range(3):
+        assert _rel(S.series_to_numpy(net.plan_td(k).contents.power_1d), p1[k]) < TOL
+    big = net.integrate(ts, wins, sky_l_max=net.l_max + 2)
+    assert _rel(big, O.assign(ref, net.l_max, False, net.l_max + 2, False)) < TOL
     net.close()
 
 
@@ -138,4 +145,43 @@ def test_edge_lengths():
     assert not np.any(got)
     with pytest.raises(S.SphradError):
         net.integrate_baseline(0, ts[1][:-1], ts[0][:-1], np.zeros(1))
+    net.close()
+
+
+def test_complex_taps_follow_the_reference_loop():
+    """A caller may write complex coefficients into proj_a / proj_b; the
+    integrator then forms complex samples and products (the path that real
+    taps skip), checked against a numpy restatement of the reference's loop
+    (sh_series_array_dot per sample, Gaunt-microcode products, windowed
+    sum, rotation)."""
+    import ctypes as C
+    import sphradiometer_b200 as S
+    dt = 1.0 / 512
+    pos = W.random_positions(2, W.R_EARTH_S, W.rng_for(34))
+    net = S.TimeDomainNetwork(pos, dt)
+    p = net.plan_td(0).contents
+    rng = np.random.Generator(np.random.Philox(9))
+    views = []
+    for arr in (p.proj_a.contents, p.proj_b.contents):
+        buf = (C.c_double * (2 * arr.n * arr.stride)).from_address(arr.coeff)
+        v = np.frombuffer(buf, dtype=np.complex128).reshape(arr.n, arr.stride)
+        v += 0.05j * rng.normal(size=v.shape) * np.abs(v).max()
+        views.append(v.copy())
+    ta, tb = views
+    La, Lb = ta.shape[1] - 1, tb.shape[1] - 1
+    pl, tr = net.power_l_max(0), net.transient(0)
+    n = 2 * tr + 97
+    ts = rng.normal(size=(2, n))
+    win = rng.uniform(0.5, 1.5, n - 2 * tr)
+    got = net.integrate_baseline(0, ts[1], ts[0], win)
+    plan = O.product_plan(pl, True, La, True, Lb, True)
+    p1 = np.zeros(pl + 1, np.complex128)
+    for t in range(n - 2 * tr):
+        sa = ta.T @ ts[1][t:t + ta.shape[0]]
+        sb = tb.T @ ts[0][t:t + tb.shape[0]]
+        p1 += win[t] * O.product_microcode(sa, La, True, sb, Lb, True, pl, True, plan)
+    b = net.baseline(0)
+    ref = O.rotate(p1, pl, True, O.rotation_plan(pl, O.rot_matrix(b.theta, b.phi)))
+    assert np.max(np.abs(p1.imag)) > 1e-3 * np.max(np.abs(p1))  # the taps' imaginary parts matter
+    assert _rel(got, ref) < TOL
     net.close()
