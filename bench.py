@@ -656,6 +656,7 @@ def run(args):
     import torch.distributed as dist
     import sphradiometer_b200 as S
     from sphradiometer_b200 import workload as W
+    from sphradiometer_b200.replicas import whole_job_rate
 
     rank, world, local = env_rank()
     if world > 1:
@@ -708,13 +709,11 @@ def run(args):
     S.load().sphrad_batch_set_timing_events(bp._p, None, None)
     elapsed_ms = t_begin.elapsed_time(t_end)
     kern_ms = [a.elapsed_time(b) for a, b in ev]
+    # whole-job rate over the slowest rank's device time
+    value, elapsed_ms = whole_job_rate(n_seg, args.steps, elapsed_ms, dev)
     if world > 1:
-        t = torch.tensor([elapsed_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(t.item())
         dist.barrier()
     status = bp.status()
-    value = world * n_seg * args.steps / (elapsed_ms / 1e3)
     kernels = bp.kernels_per_call()
 
     # roofline of the contraction kernel: algorithmic bytes per launch =
