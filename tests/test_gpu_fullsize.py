@@ -14,7 +14,9 @@ long per segment:
 * the integrator is bilinear in the spectra: scaling one detector's spectra
   by c scales the skies by c (exact in FP64 up to rounding);
 * the host-buffer entry point (chunks on two streams) returns the device
-  entry point's skies."""
+  entry point's skies up to the two runs' own split-precision errors (the
+  chunks change the accumulation order), each within the bf16x3 bound of
+  the FP64 batch."""
 import numpy as np
 import pytest
 
@@ -88,6 +90,6 @@ def test_host_entry_point_matches_device(full):
     bp = S.BatchPlan(full["net"], "bf16x3")
     dev = bp.integrate(full["F"], full["g"]).cpu().numpy()
     host = bp.integrate_host(np.ascontiguousarray(full["F"].cpu().numpy()), full["g"].cpu().numpy())
-    assert _worst(host, dev) < 1e-6
+    assert _worst(host, dev) < 1e-5
     assert _worst(host, full["ref"]) < 3e-5
     bp.close()
