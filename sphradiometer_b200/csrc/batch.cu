@@ -76,6 +76,8 @@ constexpr int kMaxChain = 64;            // most pipeline stages one tcgen05 CTA
 // ------------------------------------------------------------------------
 struct EpArgs {
 	int S, B, Lp1, L, accstride, nq;
+	int reps;               // copies of the split-K workspace summed here (see TcArgs)
+	size_t rep_stride;      // elements per copy
 	const short *lq;        // l of output index q
 	const short *mq;        // m of output index q
 	const void *W;          // [B][nq] complex T: weight / n * D_b^l_{0 m}
@@ -89,7 +91,12 @@ struct TcArgs {
 	int acol;              // first TMEM column of the X-operand ring (X in tensor memory)
 	int bi[TC_MAXB], bj[TC_MAXB];
 	const uint8_t *bops;   // [Kst][B][NPART][npad * KE bf16], UMMA layout
-	float *acc;            // [S][B][accstride]
+	float *acc;            // [reps][S][B][accstride]
+	// CTA c adds its pieces into copy c % reps of the workspace: with few
+	// tiles, many CTAs share a tile's rows, and spreading their atomics
+	// over copies keeps the contention per address low
+	int reps;
+	size_t rep_stride;     // floats per copy (S B accstride)
 	unsigned *err;
 };
 
@@ -409,7 +416,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 							v[j] = __float_as_uint(__uint_as_float(v[j]) + __uint_as_float(w[j]));
 					}
 					if(s < a.S) {
-						float *dst = a.acc + ((size_t) s * a.B + b) * a.accstride + c0;
+						float *dst = a.acc + (size_t) (blockIdx.x % a.reps) * a.rep_stride + ((size_t) s * a.B + b) * a.accstride + c0;
 #pragma unroll
 						for(int j = 0; j < 4; j++)
 							if(c0 + 4 * j < a.accstride)
@@ -565,7 +572,10 @@ __global__ void k_epilogue(const __grid_constant__ EpArgs e, T *acc)
 	T *row = acc + (size_t) s * e.B * e.accstride;
 	for(int i = threadIdx.x; i < e.B * e.Lp1; i += blockDim.x) {
 		const int b = i / e.Lp1;
-		sP[i] = row[b * e.accstride + i % e.Lp1] * (e.segw ? (T) e.segw[(size_t) s * e.B + b] : (T) 1);
+		T v = row[b * e.accstride + i % e.Lp1];
+		for(int r = 1; r < e.reps; r++)
+			v += row[(size_t) r * e.rep_stride + b * e.accstride + i % e.Lp1];
+		sP[i] = v * (e.segw ? (T) e.segw[(size_t) s * e.B + b] : (T) 1);
 	}
 	for(int m = (int) threadIdx.x - e.L; m <= e.L; m += blockDim.x) {
 		double sn = 0.0, cs = 1.0;
@@ -575,8 +585,9 @@ __global__ void k_epilogue(const __grid_constant__ EpArgs e, T *acc)
 	}
 	__syncthreads();
 	// leave the workspace zeroed for the next launch
-	for(int i = threadIdx.x; i < e.B * e.accstride; i += blockDim.x)
-		row[i] = 0;
+	for(int r = 0; r < e.reps; r++)
+		for(int i = threadIdx.x; i < e.B * e.accstride; i += blockDim.x)
+			row[(size_t) r * e.rep_stride + i] = 0;
 	const T2 *W = (const T2 *) e.W;
 	for(int q = threadIdx.x; q < e.nq; q += blockDim.x) {
 		const int l = e.lq[q];
@@ -658,8 +669,12 @@ __global__ void __launch_bounds__(EPI2_THREADS, QMAX <= 5 ? 3 : 2) k_epilogue_f3
 		float *dP = (float *) (sP + buf * EPG * nph);
 #pragma unroll
 		for(int k = 0; k < EPF; k++)
-			if(f_g[k] >= 0 && s0 + f_g[k] < e.S)
-				dP[f_dst[k]] = __ldcg(rows + f_src[k]) * (e.segw ? e.segw[(size_t) (s0 + f_g[k]) * e.B + f_b[k]] : 1.f);
+			if(f_g[k] >= 0 && s0 + f_g[k] < e.S) {
+				float v = __ldcg(rows + f_src[k]);
+				for(int r = 1; r < e.reps; r++)
+					v += __ldcg(rows + (size_t) r * e.rep_stride + f_src[k]);
+				dP[f_dst[k]] = v * (e.segw ? e.segw[(size_t) (s0 + f_g[k]) * e.B + f_b[k]] : 1.f);
+			}
 		if(ph_on) {
 			double sn = 0.0, cs = 1.0;
 			if(e.gmst && s0 + ph_g < e.S)
@@ -678,9 +693,11 @@ __global__ void __launch_bounds__(EPI2_THREADS, QMAX <= 5 ? 3 : 2) k_epilogue_f3
 		// leave the workspace zeroed for the next launch (read at the fetch)
 		const int s0 = j * EPG;
 		const int ns = e.S - s0 < EPG ? e.S - s0 : EPG;
-		float4 *rows = (float4 *) (acc + (size_t) s0 * rowf);
-		for(int i = threadIdx.x; i < ns * rowf / 4; i += blockDim.x)
-			rows[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+		for(int r = 0; r < e.reps; r++) {
+			float4 *rows = (float4 *) (acc + (size_t) r * e.rep_stride + (size_t) s0 * rowf);
+			for(int i = threadIdx.x; i < ns * rowf / 4; i += blockDim.x)
+				rows[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+		}
 		for(int g = 0; g < ns; g++) {
 			const float4 *cP = sP + (buf * EPG + g) * nph;
 			const double2 *cPh = sPh + (buf * EPG + g) * nph;
@@ -977,11 +994,22 @@ void *batch_plan_create(const BatchPlanDesc &d, int precision)
 	return P;
 }
 
+// copies of the tcgen05 path's split-K workspace for S segments: one for 16
+// tiles or more, up to 16 for a single tile (the CTAs of a launch spread
+// over few tiles' rows, and each copy takes a share of their atomics)
+static int ws_reps(const BatchPlan *P, int S)
+{
+	if(!is_tc(P->precision) || S <= 0)
+		return 1;
+	const int tiles = (S + TM - 1) / TM;
+	return std::max(1, std::min(16, 16 / tiles));
+}
+
 size_t batch_workspace_bytes(const void *pp, int S)
 {
 	const BatchPlan *P = (const BatchPlan *) pp;
 	const size_t el = P->precision == kPrecFP64 ? sizeof(double) : sizeof(float);
-	return (size_t) (S > 0 ? S : 0) * P->B * P->accstride * el;
+	return (size_t) ws_reps(P, S) * (S > 0 ? S : 0) * P->B * P->accstride * el;
 }
 
 static int sm_count()
@@ -1091,6 +1119,8 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 	e.gmst = gmst;
 	e.segw = segw;
 	e.sky = (double2 *) sky;
+	e.reps = ws_reps(P, S);
+	e.rep_stride = (size_t) S * P->B * P->accstride;
 
 	if(is_tc(P->precision)) {
 		if(((uintptr_t) F & 15) || ((ld * 16) & 15)) {
@@ -1132,6 +1162,8 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 		}
 		a.bops = P->bops;
 		a.acc = (float *) ws;
+		a.reps = e.reps;
+		a.rep_stride = e.rep_stride;
 		a.err = P->err;
 		const int tiles = (S + TM - 1) / TM;
 		a.tiles = tiles;

@@ -186,7 +186,10 @@ int np_alm_finish(void *plan, int S, double factor, const void *prior, const dou
 // of n_sub detectors (device pointers; stream a cudaStream_t)
 int uneven_gather(int S, int n_sub, int Ku, long long ld, const int *seg, const long long *in_off, const int *det, const void *in, void *F, void *stream);
 // out[out_off[seg[i]] ...] += sky[i] truncated to l_max seg_L[seg[i]]
-int uneven_scatter(int S, unsigned L, const int *seg, const long long *out_off, const unsigned *seg_L, const void *sky, void *out, void *stream);
+// out[segment s] = sum over entries e in [ptr[s], ptr[s+1]) of the sky at
+// sky_all + rows[e] (layout L), truncated to seg_L[s]; every output written
+int uneven_combine(int n_seg, unsigned L, const int *ptr, const long long *rows, const long long *out_off, const unsigned *seg_L, const void *sky_all, void *out,
+		   void *stream);
 int batch_autotune(void *plan, const void *F, int S, long long ld, void *sky, void *ws, size_t ws_bytes, void *stream);
 int batch_set_split(void *plan, int S, int split);
 

@@ -12,16 +12,19 @@ namespace sphrad {
 namespace {
 
 // F[d][i][k] = in[in_off[seg[i]] + det[d] * Ku + k], k < Ku
-__global__ void k_uneven_gather(int S, int n_sub, int Ku, long long ld, const int *seg, const long long *in_off, int4 det, const double2 *in, double2 *F)
+// one block per output row (d, i): a straight copy of the row's Ku bins
+__global__ void __launch_bounds__(256) k_uneven_gather(int S, int n_sub, int Ku, long long ld, const int *seg, const long long *in_off, int4 det, const double2 *in,
+						       double2 *F)
 {
-	const long long per = (long long) n_sub * S * Ku;
-	for(long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < per; e += (long long) gridDim.x * blockDim.x) {
-		const int k = (int) (e % Ku);
-		const long long r = e / Ku;
-		const int i = (int) (r % S), d = (int) (r / S);
-		const int dd = d == 0 ? det.x : (d == 1 ? det.y : (d == 2 ? det.z : det.w));
-		F[((long long) d * S + i) * ld + k] = in[in_off[seg[i]] + (long long) dd * Ku + k];
-	}
+	const int row = blockIdx.x;  // d * S + i
+	const int d = row / S, i = row - d * S;
+	if(d >= n_sub)
+		return;
+	const int dd = d == 0 ? det.x : (d == 1 ? det.y : (d == 2 ? det.z : det.w));
+	const double2 *src = in + in_off[seg[i]] + (long long) dd * Ku;
+	double2 *dst = F + (long long) row * ld;
+	for(int k = threadIdx.x; k < Ku; k += blockDim.x)
+		dst[k] = __ldcs(src + k);
 }
 
 __device__ __forceinline__ long long lmo(int L, int l, int m)
@@ -32,44 +35,32 @@ __device__ __forceinline__ long long lmo(int L, int l, int m)
 	return mo + l - (m < 0 ? -m : m);
 }
 
-// out[out_off[seg[i]] + q'] += sky[i][q] for every (l, m) with l <= L_s
-// (q' in the layout of l_max L_s, q in that of L); one block per segment
-__global__ void k_uneven_scatter(int S, int L, const int *seg, const long long *out_off, const unsigned *seg_L, const double2 *sky, double2 *out)
+// out[out_off[s] + q'] = sum over the segment's jobs, in job order, of
+// sky_all[row + q] for every (l, m) with l <= L_s (q' in the layout of
+// l_max L_s, q in that of L): one block per segment, warps over orders m,
+// lanes over degrees; every output coefficient is written once
+__global__ void __launch_bounds__(256) k_uneven_combine(int n_seg, int L, const int *ptr, const long long *rows, const long long *out_off,
+							const unsigned *seg_L, const double2 *sky_all, double2 *out)
 {
-	const int i = blockIdx.x;
-	if(i >= S)
+	const int s = blockIdx.x;
+	if(s >= n_seg)
 		return;
-	const int s = seg[i];
 	const int Ls = (int) seg_L[s];
-	const int nq = (Ls + 1) * (Ls + 1);
 	double2 *o = out + out_off[s];
-	const double2 *src = sky + (long long) i * (L + 1) * (L + 1);
-	for(int q = threadIdx.x; q < nq; q += blockDim.x) {
-		// (l, m) of position q of an l_max = Ls series
-		int m, l, k = q;
-		const int LL = Ls + 1;
-		if(k < LL * (LL + 1) / 2) {
-			m = 0;
-			while(k >= LL - m) {
-				k -= LL - m;
-				m++;
+	const int e0 = ptr[s], e1 = ptr[s + 1];
+	const int lane = threadIdx.x & 31, warps = blockDim.x >> 5;
+	for(int m = -Ls + (int) (threadIdx.x >> 5); m <= Ls; m += warps) {
+		const int am = m < 0 ? -m : m;
+		const long long od = lmo(Ls, am, m), os = lmo(L, am, m);
+		for(int l = am + lane; l <= Ls; l += 32) {
+			double2 acc = make_double2(0.0, 0.0);
+			for(int e = e0; e < e1; e++) {
+				const double2 v = sky_all[rows[e] + os + (l - am)];
+				acc.x += v.x;
+				acc.y += v.y;
 			}
-			l = m + k;
-		} else {
-			k -= LL * (LL + 1) / 2;
-			int am = Ls;
-			while(k >= LL - am) {
-				k -= LL - am;
-				am--;
-			}
-			m = -am;
-			l = am + k;
+			o[od + (l - am)] = acc;
 		}
-		const double2 v = src[lmo(L, l, m)];
-		double2 w = o[q];
-		w.x += v.x;
-		w.y += v.y;
-		o[q] = w;
 	}
 }
 
@@ -78,7 +69,9 @@ __global__ void k_uneven_scatter(int S, int L, const int *seg, const long long *
 int uneven_gather(int S, int n_sub, int Ku, long long ld, const int *seg, const long long *in_off, const int *det, const void *in, void *F, void *stream)
 {
 	const int4 d4 = make_int4(det[0], n_sub > 1 ? det[1] : 0, n_sub > 2 ? det[2] : 0, n_sub > 3 ? det[3] : 0);
-	k_uneven_gather<<<1024, 256, 0, (cudaStream_t) stream>>>(S, n_sub, Ku, ld, seg, in_off, d4, (const double2 *) in, (double2 *) F);
+	if(S <= 0)
+		return 0;
+	k_uneven_gather<<<n_sub * S, 256, 0, (cudaStream_t) stream>>>(S, n_sub, Ku, ld, seg, in_off, d4, (const double2 *) in, (double2 *) F);
 	if(cudaGetLastError() != cudaSuccess) {
 		set_error("uneven gather: launch failed");
 		return -1;
@@ -86,13 +79,14 @@ int uneven_gather(int S, int n_sub, int Ku, long long ld, const int *seg, const 
 	return 0;
 }
 
-int uneven_scatter(int S, unsigned L, const int *seg, const long long *out_off, const unsigned *seg_L, const void *sky, void *out, void *stream)
+int uneven_combine(int n_seg, unsigned L, const int *ptr, const long long *rows, const long long *out_off, const unsigned *seg_L, const void *sky_all, void *out,
+		   void *stream)
 {
-	if(S <= 0)
+	if(n_seg <= 0)
 		return 0;
-	k_uneven_scatter<<<S, 256, 0, (cudaStream_t) stream>>>(S, (int) L, seg, out_off, seg_L, (const double2 *) sky, (double2 *) out);
+	k_uneven_combine<<<n_seg, 256, 0, (cudaStream_t) stream>>>(n_seg, (int) L, ptr, rows, out_off, seg_L, (const double2 *) sky_all, (double2 *) out);
 	if(cudaGetLastError() != cudaSuccess) {
-		set_error("uneven scatter: launch failed");
+		set_error("uneven combine: launch failed");
 		return -1;
 	}
 	return 0;

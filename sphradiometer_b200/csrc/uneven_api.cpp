@@ -14,9 +14,12 @@
 // segment's baselines assigned to the job, 0 otherwise, so each sky is the
 // mean over its own B_s baselines, correlator.c:1004).  A call zeroes the
 // packed outputs and runs every job: gather of its spectra, contraction,
-// epilogue, and addition into the outputs truncated to each segment's
-// l_max.  The whole sequence can be captured once into a CUDA graph and
-// replayed.
+// epilogue into the job's own sky rows; the jobs are spread over a few
+// streams (longest first, each to the least loaded stream) so that small
+// jobs overlap, and one final kernel sums every segment's rows, in job
+// order, into the packed outputs truncated to each segment's l_max.  The
+// whole sequence can be captured once into a CUDA graph (forked over the
+// streams) and replayed.
 #include <sphradiometer_b200.h>
 #include <sphradiometer/correlator.h>
 #include <sphradiometer/instrument.h>
@@ -45,7 +48,11 @@ struct Job {
 	int *d_seg = nullptr;
 	float *d_w = nullptr;
 	int split = 0;               // tuned split (0 = heuristic)
+	size_t sky_off = 0;          // first row of its skies in the plan's sky_all (complex elements)
+	int slot = 0;                // stream and scratch slot
 };
+
+constexpr int kSlots = 4;        // streams the jobs are spread over
 
 }  // namespace
 
@@ -70,9 +77,16 @@ struct sphrad_uneven_plan {
 	long long *d_in_off = nullptr, *d_out_off = nullptr;
 	unsigned *d_segL = nullptr;
 	std::vector<Job> jobs;
-	// shared job buffers (jobs run in sequence)
+	// job buffers: spectra and split-K scratch per slot (the jobs of a slot
+	// run in sequence), every job's skies in sky_all
 	void *F = nullptr, *sky = nullptr, *ws = nullptr;
 	size_t F_bytes = 0, sky_bytes = 0, ws_bytes = 0;
+	int n_slots = 1;
+	// per segment, the rows of its skies in sky_all (CSR, job order)
+	int *d_cmb_ptr = nullptr;
+	long long *d_cmb_rows = nullptr;
+	cudaStream_t side[kSlots] = {};
+	cudaEvent_t ev[kSlots + 1] = {};
 	int fixed_split = 0;
 	// graph
 	int use_graph = 1;
@@ -112,6 +126,10 @@ static void drop_jobs(sphrad_uneven_plan *p)
 	dfree(p->F);
 	dfree(p->sky);
 	dfree(p->ws);
+	dfree(p->d_cmb_ptr);
+	dfree(p->d_cmb_rows);
+	p->d_cmb_ptr = nullptr;
+	p->d_cmb_rows = nullptr;
 	p->F = p->sky = p->ws = nullptr;
 	p->F_bytes = p->sky_bytes = p->ws_bytes = 0;
 	drop_graph(p);
@@ -133,6 +151,12 @@ extern "C" void sphrad_uneven_plan_free(sphrad_uneven_plan *p)
 	}
 	if(p->cap)
 		cudaStreamDestroy(p->cap);
+	for(int k = 0; k < kSlots; k++)
+		if(p->side[k])
+			cudaStreamDestroy(p->side[k]);
+	for(int k = 0; k <= kSlots; k++)
+		if(p->ev[k])
+			cudaEventDestroy(p->ev[k]);
 	delete p;
 }
 
@@ -168,7 +192,12 @@ extern "C" sphrad_uneven_plan *sphrad_uneven_plan_new(const double *positions, i
 				for(int c = b + 1; c < n_det; c++)
 					p->subs.push_back({a, b, c});
 	}
-	if(cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking) != cudaSuccess) {
+	bool ok = cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking) == cudaSuccess;
+	for(int k = 1; ok && k < kSlots; k++)
+		ok = cudaStreamCreateWithFlags(&p->side[k], cudaStreamNonBlocking) == cudaSuccess;
+	for(int k = 0; ok && k <= kSlots; k++)
+		ok = cudaEventCreateWithFlags(&p->ev[k], cudaEventDisableTiming) == cudaSuccess;
+	if(!ok) {
 		set_error("sphrad_uneven_plan_new: stream creation failed");
 		sphrad_uneven_plan_free(p);
 		return NULL;
@@ -286,10 +315,12 @@ extern "C" int sphrad_uneven_set_segments(sphrad_uneven_plan *p, int n_seg, cons
 	}
 	p->in_total = io;
 	p->out_total = oo;
-	// device tables and shared buffers
+	// device tables and buffers
 	size_t Fb = 0, skb = 0, wsb = 0;
 	const size_t nq = (size_t) (p->L + 1) * (p->L + 1);
 	for(Job &j : p->jobs) {
+		j.sky_off = skb / 16;
+		skb += (size_t) j.seg.size() * nq * 16;
 		j.S = (int) j.seg.size();
 		j.bp = plan_for(p, j.bucket, (int) (std::find(p->subs.begin(), p->subs.end(), j.det) - p->subs.begin()));
 		if(!j.bp)
@@ -299,24 +330,58 @@ extern "C" int sphrad_uneven_set_segments(sphrad_uneven_plan *p, int n_seg, cons
 		if(!j.d_seg || !j.d_w || h2d(j.d_seg, j.seg.data(), j.S * sizeof(int)) || h2d(j.d_w, j.w.data(), j.w.size() * sizeof(float)))
 			return -1;
 		Fb = std::max(Fb, (size_t) (j.det.size() * j.S * j.ld * 16));
-		skb = std::max(skb, (size_t) j.S * nq * 16);
 		wsb = std::max(wsb, sphrad_batch_workspace_size(j.bp, j.S));
+	}
+	// slots: longest job first to the least loaded slot (cost ~ S n_sub Ku)
+	p->n_slots = std::min(kSlots, std::max(1, (int) p->jobs.size()));
+	{
+		std::vector<int> order(p->jobs.size());
+		for(size_t i = 0; i < order.size(); i++)
+			order[i] = (int) i;
+		auto cost = [&](int i) { return (double) p->jobs[i].S * p->jobs[i].det.size() * p->jobs[i].Ku; };
+		std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost(a) > cost(b); });
+		std::vector<double> load(p->n_slots, 0.0);
+		for(int i : order) {
+			const int k = (int) (std::min_element(load.begin(), load.end()) - load.begin());
+			p->jobs[i].slot = k;
+			load[k] += cost(i);
+		}
+	}
+	Fb = (Fb + 255) / 256 * 256;
+	wsb = (wsb + 255) / 256 * 256;
+	// per segment: its rows in sky_all, in job order
+	std::vector<int> cptr(n_seg + 1, 0);
+	for(const Job &j : p->jobs)
+		for(int s : j.seg)
+			cptr[s + 1]++;
+	for(int s = 0; s < n_seg; s++)
+		cptr[s + 1] += cptr[s];
+	std::vector<long long> crow(cptr[n_seg]);
+	{
+		std::vector<int> fill(cptr.begin(), cptr.end() - 1);
+		for(const Job &j : p->jobs)
+			for(size_t i = 0; i < j.seg.size(); i++)
+				crow[fill[j.seg[i]]++] = (long long) (j.sky_off + i * nq);
 	}
 	p->d_in_off = (long long *) dmalloc((n_seg > 0 ? n_seg : 1) * sizeof(long long));
 	p->d_out_off = (long long *) dmalloc((n_seg > 0 ? n_seg : 1) * sizeof(long long));
 	p->d_segL = (unsigned *) dmalloc((n_seg > 0 ? n_seg : 1) * sizeof(unsigned));
-	p->F = dmalloc(Fb);
-	p->sky = dmalloc(skb);
-	p->ws = dmalloc(wsb);
+	p->F = dmalloc(Fb * p->n_slots);
+	p->sky = dmalloc(skb ? skb : 16);
+	p->ws = dmalloc(wsb * p->n_slots);
 	p->F_bytes = Fb;
 	p->sky_bytes = skb;
 	p->ws_bytes = wsb;
-	if(!p->d_in_off || !p->d_out_off || !p->d_segL || !p->F || !p->sky || !p->ws)
+	p->d_cmb_ptr = (int *) dmalloc((n_seg + 1) * sizeof(int));
+	p->d_cmb_rows = (long long *) dmalloc((crow.empty() ? 1 : crow.size()) * sizeof(long long));
+	if(!p->d_in_off || !p->d_out_off || !p->d_segL || !p->F || !p->sky || !p->ws || !p->d_cmb_ptr || !p->d_cmb_rows)
+		return -1;
+	if(h2d(p->d_cmb_ptr, cptr.data(), (n_seg + 1) * sizeof(int)) || (!crow.empty() && h2d(p->d_cmb_rows, crow.data(), crow.size() * sizeof(long long))))
 		return -1;
 	if(n_seg > 0 && (h2d(p->d_in_off, p->in_off.data(), n_seg * sizeof(long long)) || h2d(p->d_out_off, p->out_off.data(), n_seg * sizeof(long long)) ||
 			 h2d(p->d_segL, p->segL.data(), n_seg * sizeof(unsigned))))
 		return -1;
-	if(dmemset(p->ws, 0, wsb) || stream_sync())
+	if(dmemset(p->ws, 0, wsb * p->n_slots) || stream_sync())
 		return -1;
 	return 0;
 }
@@ -343,25 +408,45 @@ static int split_of(const sphrad_uneven_plan *p, const Job &j)
 	return j.split;
 }
 
-// the job sequence on stream st
+// spectra, scratch and skies of job j
+static void *job_F(sphrad_uneven_plan *p, const Job &j) { return (char *) p->F + (size_t) j.slot * p->F_bytes; }
+static void *job_ws(sphrad_uneven_plan *p, const Job &j) { return (char *) p->ws + (size_t) j.slot * p->ws_bytes; }
+static void *job_sky(sphrad_uneven_plan *p, const Job &j) { return (double *) p->sky + 2 * j.sky_off; }
+
+// the jobs forked over the slots' streams from st, joined back, then the
+// combine into the outputs on st
 static int run_jobs(sphrad_uneven_plan *p, const void *in, void *out, cudaStream_t st)
 {
 	int k = 0;
-	if(cudaMemsetAsync(out, 0, (size_t) p->out_total * 16, st) != cudaSuccess) {
-		set_error("uneven: memset failed");
+	cudaStream_t ss[kSlots];
+	ss[0] = st;
+	for(int s = 1; s < p->n_slots; s++)
+		ss[s] = p->side[s];
+	if(cudaEventRecord(p->ev[0], st) != cudaSuccess) {
+		set_error("uneven: event record failed");
 		return -1;
 	}
-	for(Job &j : p->jobs) {
-		if(uneven_gather(j.S, (int) j.det.size(), j.Ku, j.ld, j.d_seg, p->d_in_off, j.det.data(), in, p->F, st))
+	for(int s = 1; s < p->n_slots; s++)
+		if(cudaStreamWaitEvent(ss[s], p->ev[0], 0) != cudaSuccess) {
+			set_error("uneven: stream fork failed");
 			return -1;
-		if(sphrad_batch_integrate_weighted(j.bp, p->F, j.S, j.ld, NULL, p->sky, p->ws, p->ws_bytes, st, split_of(p, j), j.d_w))
+		}
+	for(Job &j : p->jobs) {
+		cudaStream_t js = ss[j.slot];
+		if(uneven_gather(j.S, (int) j.det.size(), j.Ku, j.ld, j.d_seg, p->d_in_off, j.det.data(), in, job_F(p, j), js))
+			return -1;
+		if(sphrad_batch_integrate_weighted(j.bp, job_F(p, j), j.S, j.ld, NULL, job_sky(p, j), job_ws(p, j), p->ws_bytes, js, split_of(p, j), j.d_w))
 			return -1;
 		k += 1 + sphrad_batch_kernels_per_call(j.bp);
-		if(uneven_scatter(j.S, p->L, j.d_seg, p->d_out_off, p->d_segL, p->sky, out, st))
-			return -1;
-		k++;
 	}
-	p->kernels = k;
+	for(int s = 1; s < p->n_slots; s++)
+		if(cudaEventRecord(p->ev[s], ss[s]) != cudaSuccess || cudaStreamWaitEvent(st, p->ev[s], 0) != cudaSuccess) {
+			set_error("uneven: stream join failed");
+			return -1;
+		}
+	if(uneven_combine(p->n_seg, p->L, p->d_cmb_ptr, p->d_cmb_rows, p->d_out_off, p->d_segL, p->sky, out, st))
+		return -1;
+	p->kernels = k + 1;
 	return 0;
 }
 
@@ -384,10 +469,10 @@ extern "C" int sphrad_uneven_autotune(sphrad_uneven_plan *p, const void *in, voi
 	cudaStream_t st = stream ? (cudaStream_t) stream : cudaStreamLegacy;
 	(void) out;
 	for(Job &j : p->jobs) {
-		if(uneven_gather(j.S, (int) j.det.size(), j.Ku, j.ld, j.d_seg, p->d_in_off, j.det.data(), in, p->F, st))
+		if(uneven_gather(j.S, (int) j.det.size(), j.Ku, j.ld, j.d_seg, p->d_in_off, j.det.data(), in, job_F(p, j), st))
 			return -1;
 		// the job's plan keeps the tuned work split for j.S
-		if(sphrad_batch_autotune(j.bp, p->F, j.S, j.ld, p->sky, p->ws, p->ws_bytes, st) < 0)
+		if(sphrad_batch_autotune(j.bp, job_F(p, j), j.S, j.ld, job_sky(p, j), job_ws(p, j), p->ws_bytes, st) < 0)
 			return -1;
 		j.split = 0;
 	}
