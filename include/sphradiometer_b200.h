@@ -326,9 +326,11 @@ int sphrad_sky_peaks(const void *sky, int n_sky, unsigned sky_l_max, double *out
  *
  * Rotation: out[s] = sh_series_rotate(in[s], plan of R[s]) for n series
  * (sh_series_rotation.c:287-422, 546-589), without materialising the
- * plans: each series' Wigner-D matrices are built by the reference's FP64
- * recursion from its 3x3 rotation matrix and applied at once, in FP32
- * (fp32_apply = 1) or FP64.  in: device [n][len] double complex (len =
+ * plans: the reference's Wigner-D matrices factor as
+ * Z(-alpha) P* Delta E(beta) Delta^T P Z(-gamma) through the fixed matrix
+ * Delta = D(R_y(pi/2)) (built once by the reference's recursion) and the
+ * Euler angles of R[s]; the two products with Delta run in FP32
+ * (fp32_apply = 1) or FP64, the phases in FP64.  in: device [n][len] double complex (len =
  * l_max + 1 when polar, else (l_max+1)^2); R: device [n][9] doubles,
  * row-major as euler_rotation_matrix returns them; out: device
  * [n][(l_max+1)^2] double complex (non-polar). */

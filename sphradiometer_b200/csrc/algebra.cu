@@ -1,23 +1,27 @@
 // algebra.cu -- batched spherical-harmonic algebra: rotation of many
-// series, each by its own rotation, with the Wigner-D matrices built per
-// series in FP64 and applied in FP32 or FP64 without materialising the
-// plans in memory.
+// series, each by its own rotation, applied in FP32 or FP64 without
+// materialising any per-series Wigner-D matrix.
 //
 // Reference algorithms (cannon-zz/sphradiometer): sh_series_rotation_plan_new
 // and its recursion, sh_series_rotation.c:287-422 (Choi, Ivanic, Gordon &
 // Ruedenberg), and sh_series_rotate, sh_series_rotation.c:546-589.
 //
-// One block per series (grid-stride): degree l's matrix is computed from
-// degree l-1's and the l = 1 matrix (one element per thread, FP64), written
-// to a two-level ring in global memory that stays in L2, and applied at
-// once, c'_{l m'} = sum_m D^l_{m m'} c_{l m}, one warp per output order m'.
-// The recursion's coefficients depend only on (l, m, m') and are read from
-// a table built once per l_max.
+// The reference's matrices factor through one fixed real matrix per
+// degree, Delta = D(R_y(pi/2)) (built once by the reference's recursion):
+// for R = euler_rotation_matrix(gamma, beta, alpha),
+//     D^l(R)^T = Z(-alpha) P* Delta E(beta) Delta^T P Z(-gamma),
+// Z(x) = diag(e^{i m x}), P = diag(i^m), E(b) = diag(e^{i k b}), so a
+// series is rotated by two dense real matrix products per degree and three
+// diagonal phases (FP64), the products shared by a block of series with
+// Delta in shared memory.  The Euler angles come from R (atan2 of its
+// entries).
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <map>
 #include <mutex>
+#include <vector>
+#include <algorithm>
 
 #include "runtime.h"
 #include "wigner.cuh"
@@ -35,52 +39,6 @@ namespace sphrad {
 
 namespace {
 
-// coefficients of element (m, m') of degree l >= 2: the terms
-//   c0 D1(0, j) Dp(m, q) + cp D1(1, j) Dp(m-1, q) + cn D1(-1, j) Dp(m+1, q)
-// with j = 0, q = m' inside, j = -1, q = m'+1 at m' = -l, j = +1, q = m'-1
-// at m' = l (zero where the term is absent)
-struct WigCoef {
-	double c0, cp, cn;
-};
-
-__global__ void k_wig_coef(int L, WigCoef *tab)
-{
-	const int l = blockIdx.x + 2;
-	if(l > L)
-		return;
-	const int w = 2 * l + 1;
-	WigCoef *t = tab + wig_offset(l);
-	for(int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
-		const int m = idx % w - l;
-		const int mp = idx / w - l;
-		WigCoef c = {0, 0, 0};
-		if(mp > -l && mp < l) {
-			if(abs(m) != l)
-				c.c0 = wig_a(l, m, mp);
-			if(m > -l + 1)
-				c.cp = wig_b(l, m, mp);
-			if(-m > -l + 1)
-				c.cn = wig_b(l, -m, mp);
-		} else {
-			const int amp = mp < 0 ? -mp : mp;
-			if(abs(m) != l)
-				c.c0 = wig_c(l, m, amp);
-			if(m > -l + 1)
-				c.cp = wig_d(l, m, amp);
-			if(-m > -l + 1)
-				c.cn = wig_d(l, -m, amp);
-		}
-		t[idx] = c;
-	}
-}
-
-__device__ __forceinline__ double2 cmadd(double2 acc, double c, double2 a, double2 b)
-{
-	// acc + c * a * b
-	const double re = a.x * b.x - a.y * b.y, im = a.x * b.y + a.y * b.x;
-	return make_double2(acc.x + c * re, acc.y + c * im);
-}
-
 __device__ __forceinline__ long long lm_off(int L, int l, int m)
 {
 	const long long LL = L + 1;
@@ -89,137 +47,214 @@ __device__ __forceinline__ long long lm_off(int L, int l, int m)
 	return mo + l - (m < 0 ? -m : m);
 }
 
-constexpr int kRotThreads = 512;
+// first element of degree l's (2l+1)^2 block: sum_{j<l} (2j+1)^2 for l >= 1
+__device__ __forceinline__ long long blk_off(int l) { return l <= 1 ? 0 : (4LL * l * l * l - l - 3) / 3; }
 
-template <class TA>
-__global__ void __launch_bounds__(kRotThreads) k_rotate_batch(int n, int L, int polar, const double2 *in, long long istride, const double *R_all,
-							      const WigCoef *coef, double2 *ring, double2 *out)
+template <class T> struct Cx;
+template <> struct Cx<float> {
+	using type = float2;
+};
+template <> struct Cx<double> {
+	using type = double2;
+};
+
+// Euler angles of each rotation matrix R = euler_rotation_matrix(gamma,
+// beta, alpha) (sh_series_rotation.c:104-153: R[2] = cos(alpha) sin(beta),
+// R[5] = sin(alpha) sin(beta), R[6] = -sin(beta) cos(gamma), R[7] =
+// sin(beta) sin(gamma), R[8] = cos(beta)); at sin(beta) = 0 only alpha +-
+// gamma is defined and gamma = 0 is taken.  abg[s] = (alpha, beta, gamma).
+__global__ void k_euler(int n, const double *__restrict__ R_all, double *__restrict__ abg)
 {
-	__shared__ double2 d1[9];
-	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-	const size_t lvl = (size_t) (2 * L + 1) * (2 * L + 1);
-	double2 *bufA = ring + 2 * lvl * blockIdx.x, *bufB = bufA + lvl;
+	const int s = blockIdx.x * blockDim.x + threadIdx.x;
+	if(s >= n)
+		return;
+	const double *R = R_all + 9 * (size_t) s;
+	const double sb = hypot(R[2], R[5]);
+	const double b = atan2(sb, R[8]);
+	double a, g;
+	if(sb > 1e-14) {
+		a = atan2(R[5], R[2]);
+		g = atan2(R[7], -R[6]);
+	} else {
+		const double sgn = R[8] >= 0 ? 1.0 : -1.0;
+		g = 0.0;
+		a = atan2(R[3] * sgn, R[0] * sgn);
+	}
+	abg[3 * (size_t) s] = a;
+	abg[3 * (size_t) s + 1] = b;
+	abg[3 * (size_t) s + 2] = g;
+}
+
+// c * e^{i phi} * i^q (q taken mod 4) in FP64
+__device__ __forceinline__ double2 phase_mul(double2 c, double phi, int q)
+{
+	double sn, cs;
+	sincos(phi, &sn, &cs);
+	double2 v = make_double2(c.x * cs - c.y * sn, c.x * sn + c.y * cs);
+	switch(q & 3) {
+	case 1: return make_double2(-v.y, v.x);
+	case 2: return make_double2(-v.x, -v.y);
+	case 3: return make_double2(v.y, -v.x);
+	default: return v;
+	}
+}
+
+// Rotation of G series at degree l (blockIdx.y) through the factorisation of
+// the reference's Wigner-D matrices (sh_series_rotation.c:287-422) by the
+// fixed real matrix Delta = D(R_y(pi/2)):
+//     c' = Z(-alpha) P* Delta E(beta) Delta^T P Z(-gamma) c,
+// Z(x) = diag(e^{i m x}), P = diag(i^m), E(b) = diag(e^{i k b}), which is
+// c'_{l m'} = sum_m D^l_{m m'} c_{l m} (sh_series_rotation.c:546-589) for
+// the plan of R.  The phases are formed in FP64; the two products with Delta
+// run in T with Delta in shared memory (Delta[m][k] at m (2l+1) + k).
+template <class T, int G>
+__global__ void __launch_bounds__(128) k_rotate_fac(int n, int L, int polar, const double2 *__restrict__ in, long long istride,
+						    const double *__restrict__ abg, const T *__restrict__ delta, int dglobal, double2 *__restrict__ out)
+{
+	using T2 = typename Cx<T>::type;
+	extern __shared__ __align__(16) unsigned char rot_smem[];
+	const int l = blockIdx.y, w = 2 * l + 1, s0 = blockIdx.x * G;
 	const long long ostride = (long long) (L + 1) * (L + 1);
-	for(int s = blockIdx.x; s < n; s += gridDim.x) {
-		const double2 *c = in + (long long) s * istride;
-		double2 *o = out + (long long) s * ostride;
-		__syncthreads();  // previous series done with d1 and the ring
-		if(threadIdx.x == 0)
-			wig_d1(R_all + 9 * (size_t) s, d1);
-		if(threadIdx.x == 32)
-			o[0] = c[0];
-		__syncthreads();
-		// l = 1 from d1 directly; the ring's first level holds it
-		double2 *Dp = bufA, *Dc = bufB;
-		if(L >= 1) {
-			if(threadIdx.x < 9)
-				Dp[threadIdx.x] = d1[threadIdx.x];
+	if(l == 0) {
+		for(int g = threadIdx.x; g < G; g += blockDim.x)
+			if(s0 + g < n)
+				out[(long long) (s0 + g) * ostride] = in[(long long) (s0 + g) * istride];
+		return;
+	}
+	T2 *sU = (T2 *) rot_smem;        // [G][w]: P Z(-gamma) c
+	T2 *sV = sU + G * w;             // [G][w]: E Delta^T (...)
+	const T *Dl = delta + blk_off(l);
+	// Delta in shared memory, or read from the (L2-resident) table when a
+	// degree's block does not fit
+	T *sD = (T *) (sV + G * w);      // [w][w]
+	if(!dglobal)
+		for(int i = threadIdx.x; i < w * w; i += blockDim.x)
+			sD[i] = Dl[i];
+	const T *D = dglobal ? Dl : sD;
+	for(int i = threadIdx.x; i < G * w; i += blockDim.x) {
+		const int g = i / w, mi = i - g * w, m = mi - l, s = s0 + g;
+		double2 c = make_double2(0.0, 0.0);
+		if(s < n) {
+			const double2 *cs = in + (long long) s * istride;
+			if(!polar)
+				c = cs[lm_off(L, l, m)];
+			else if(m == 0)
+				c = cs[l];
+			c = phase_mul(c, -(double) m * abg[3 * (size_t) s + 2], m);
 		}
-		for(int l = 1; l <= L; l++) {
-			const int w = 2 * l + 1;
-			double2 *D = (l == 1) ? Dp : Dc;
-			if(l >= 2) {
-				const WigCoef *t = coef + wig_offset(l);
-				const int lp = l - 1;
-				for(int idx = threadIdx.x; idx < w * w; idx += blockDim.x) {
-					const int m = idx % w - l;
-					const int mp = idx / w - l;
-					const int j = (mp == -l) ? -1 : (mp == l ? 1 : 0);
-					const int q = mp - j;  // m' column of level l-1: m'+1 at -l, m'-1 at +l
-					const WigCoef k = t[idx];
-					double2 v = make_double2(0, 0);
-					if(k.c0 != 0.0)
-						v = cmadd(v, k.c0, d1[(j + 1) * 3 + 1], WDEL(Dp, lp, m, q));
-					if(k.cp != 0.0)
-						v = cmadd(v, k.cp, d1[(j + 1) * 3 + 2], WDEL(Dp, lp, m - 1, q));
-					if(k.cn != 0.0)
-						v = cmadd(v, k.cn, d1[(j + 1) * 3 + 0], WDEL(Dp, lp, m + 1, q));
-					D[idx] = v;
-				}
+		sU[i] = T2{(T) c.x, (T) c.y};
+	}
+	__syncthreads();
+	for(int k = threadIdx.x; k < w; k += blockDim.x) {
+		T2 acc[G];
+#pragma unroll
+		for(int g = 0; g < G; g++)
+			acc[g] = T2{(T) 0, (T) 0};
+		for(int m = 0; m < w; m++) {
+			const T d = D[m * w + k];
+#pragma unroll
+			for(int g = 0; g < G; g++) {
+				const T2 u = sU[g * w + m];
+				acc[g].x += d * u.x;
+				acc[g].y += d * u.y;
 			}
-			__syncthreads();
-			// apply: warp per output order m', lanes over m
-			for(int mpi = warp; mpi < w; mpi += nw) {
-				const int mp = mpi - l;
-				TA ar = 0, ai = 0;
-				if(polar) {
-					if(lane == 0) {
-						const double2 d = WDEL(D, l, 0, mp);
-						const double2 x = c[l];
-						ar = (TA) d.x * (TA) x.x - (TA) d.y * (TA) x.y;
-						ai = (TA) d.x * (TA) x.y + (TA) d.y * (TA) x.x;
-					}
-				} else {
-					for(int m = -l + lane; m <= l; m += 32) {
-						const double2 d = WDEL(D, l, m, mp);
-						const double2 x = c[lm_off(L, l, m)];
-						const TA dr = (TA) d.x, di = (TA) d.y, xr = (TA) x.x, xi = (TA) x.y;
-						ar += dr * xr - di * xi;
-						ai += dr * xi + di * xr;
-					}
-				}
-				for(int off = 16; off; off >>= 1) {
-					ar += __shfl_xor_sync(0xffffffffu, ar, off);
-					ai += __shfl_xor_sync(0xffffffffu, ai, off);
-				}
-				if(lane == 0)
-					o[lm_off(L, l, mp)] = make_double2((double) ar, (double) ai);
+		}
+#pragma unroll
+		for(int g = 0; g < G; g++) {
+			const int s = s0 + g;
+			double sn = 0.0, cs = 1.0;
+			if(s < n)
+				sincos((double) (k - l) * abg[3 * (size_t) s + 1], &sn, &cs);
+			const T c = (T) cs, sv = (T) sn;
+			sV[g * w + k] = T2{acc[g].x * c - acc[g].y * sv, acc[g].x * sv + acc[g].y * c};
+		}
+	}
+	__syncthreads();
+	for(int mi = threadIdx.x; mi < w; mi += blockDim.x) {
+		const int m = mi - l;
+		T2 acc[G];
+#pragma unroll
+		for(int g = 0; g < G; g++)
+			acc[g] = T2{(T) 0, (T) 0};
+		for(int k = 0; k < w; k++) {
+			const T d = D[mi * w + k];
+#pragma unroll
+			for(int g = 0; g < G; g++) {
+				const T2 v = sV[g * w + k];
+				acc[g].x += d * v.x;
+				acc[g].y += d * v.y;
 			}
-			if(l >= 2) {
-				double2 *tmp = Dp;
-				Dp = Dc;
-				Dc = tmp;
-			} else {
-				Dc = bufB;
-			}
+		}
+#pragma unroll
+		for(int g = 0; g < G; g++) {
+			const int s = s0 + g;
+			if(s < n)
+				out[(long long) s * ostride + lm_off(L, l, m)] =
+					phase_mul(make_double2((double) acc[g].x, (double) acc[g].y), -(double) m * abg[3 * (size_t) s], -m);
 		}
 	}
 }
 
-struct CoefTable {
-	WigCoef *d = nullptr;
+constexpr int kRotG32 = 16, kRotG64 = 8;  // series per block
+
+// Delta = D(R_y(pi/2)) of every degree up to L, real, [l block][m][k], in
+// FP64 and FP32; built once per device (a table for a larger L serves a
+// smaller one: the blocks do not depend on L)
+struct DeltaTable {
+	double *d64 = nullptr;
+	float *d32 = nullptr;
 	int L = -1;
 };
-std::mutex g_coef_mu;
-std::map<int, CoefTable> g_coef;  // by device
+std::mutex g_delta_mu;
+std::map<int, DeltaTable> g_delta;  // by device
 
 }  // namespace
 
-static int coef_table(int L, const WigCoef **out, cudaStream_t st)
+static int delta_table(int L, const double **d64, const float **d32)
 {
 	const int dev = current_device();
-	std::lock_guard<std::mutex> lk(g_coef_mu);
-	CoefTable &t = g_coef[dev];
+	std::lock_guard<std::mutex> lk(g_delta_mu);
+	DeltaTable &t = g_delta[dev];
 	if(t.L < L) {
-		dfree(t.d);
-		t.d = nullptr;
+		dfree(t.d64);
+		dfree(t.d32);
+		t.d64 = nullptr;
+		t.d32 = nullptr;
 		t.L = -1;
-		const size_t n = wig_offset(L + 1) + 1;
-		t.d = (WigCoef *) dmalloc(n * sizeof(WigCoef));
-		if(!t.d)
+		const size_t len = rot_offset((unsigned) L + 1);
+		// R_y(pi/2) as euler_rotation_matrix(0, pi/2, 0) builds it
+		const double R[9] = {0.0, 0.0, 1.0, 0.0, 1.0, 0.0, -1.0, 0.0, 0.0};
+		std::vector<double> flat(2 * (len ? len : 1));
+		if(L >= 1 && build_rotation_plan((unsigned) L, R, flat.data()))
 			return -1;
-		if(L >= 2)
-			k_wig_coef<<<L - 1, 256, 0, st>>>(L, t.d);
-		CK(cudaGetLastError());
-		CK(cudaStreamSynchronize(st));
+		// flat: element (m, k) of degree l at rot_offset(l) + (2l+1)(k+l) + (m+l);
+		// table: [m][k] row-major
+		std::vector<double> h64(len ? len : 1, 0.0);
+		std::vector<float> h32(len ? len : 1, 0.f);
+		for(int l = 1; l <= L; l++) {
+			const size_t o = rot_offset((unsigned) l), w = 2 * (size_t) l + 1;
+			for(size_t m = 0; m < w; m++)
+				for(size_t k = 0; k < w; k++) {
+					const double v = flat[2 * (o + w * k + m)];
+					h64[o + m * w + k] = v;
+					h32[o + m * w + k] = (float) v;
+				}
+		}
+		t.d64 = (double *) dmalloc(h64.size() * sizeof(double));
+		t.d32 = (float *) dmalloc(h32.size() * sizeof(float));
+		if(!t.d64 || !t.d32 || h2d(t.d64, h64.data(), h64.size() * sizeof(double)) || h2d(t.d32, h32.data(), h32.size() * sizeof(float)) || stream_sync())
+			return -1;
 		t.L = L;
 	}
-	*out = t.d;
+	*d64 = t.d64;
+	*d32 = t.d32;
 	return 0;
-}
-
-static int rotate_grid(int n)
-{
-	int dev = 0, sms = 148;
-	cudaGetDevice(&dev);
-	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-	return n < sms ? n : sms;
 }
 
 size_t rotate_batch_scratch_bytes(unsigned L, int n)
 {
-	const size_t lvl = (size_t) (2 * L + 1) * (2 * L + 1);
-	return (size_t) rotate_grid(n > 0 ? n : 1) * 2 * lvl * sizeof(double2);
+	(void) L;
+	return ((size_t) (n > 0 ? n : 1) * 3 * sizeof(double) + 255) / 256 * 256;
 }
 
 int rotate_batch(const void *in, int n, unsigned L, int polar, const double *R, void *out, int fp32_apply, void *scratch, size_t scratch_bytes,
@@ -234,17 +269,32 @@ int rotate_batch(const void *in, int n, unsigned L, int polar, const double *R, 
 		set_error("rotate batch: scratch of %zu bytes, %zu needed", scratch_bytes, rotate_batch_scratch_bytes(L, n));
 		return -1;
 	}
-	const WigCoef *coef = nullptr;
-	if(coef_table((int) L, &coef, st))
+	const double *d64 = nullptr;
+	const float *d32 = nullptr;
+	if(delta_table((int) L, &d64, &d32))
 		return -1;
 	const long long istride = polar ? (long long) L + 1 : (long long) (L + 1) * (L + 1);
-	const int grid = rotate_grid(n);
-	if(fp32_apply)
-		k_rotate_batch<float><<<grid, kRotThreads, 0, st>>>(n, (int) L, polar, (const double2 *) in, istride, R, coef, (double2 *) scratch,
-								    (double2 *) out);
-	else
-		k_rotate_batch<double><<<grid, kRotThreads, 0, st>>>(n, (int) L, polar, (const double2 *) in, istride, R, coef, (double2 *) scratch,
-								     (double2 *) out);
+	double *abg = (double *) scratch;
+	k_euler<<<(n + 127) / 128, 128, 0, st>>>(n, R, abg);
+	const int w = 2 * (int) L + 1;
+	const size_t kMaxSmem = 200 * 1024;
+	if(fp32_apply) {
+		size_t smem = (size_t) 2 * kRotG32 * w * sizeof(float2) + (size_t) w * w * sizeof(float);
+		const int dglobal = smem > kMaxSmem;
+		if(dglobal)
+			smem = (size_t) 2 * kRotG32 * w * sizeof(float2);
+		CK(cudaFuncSetAttribute(k_rotate_fac<float, kRotG32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) std::max(smem, (size_t) 48 * 1024)));
+		k_rotate_fac<float, kRotG32><<<dim3((n + kRotG32 - 1) / kRotG32, L + 1), 128, smem, st>>>(n, (int) L, polar, (const double2 *) in, istride, abg,
+													   d32, dglobal, (double2 *) out);
+	} else {
+		size_t smem = (size_t) 2 * kRotG64 * w * sizeof(double2) + (size_t) w * w * sizeof(double);
+		const int dglobal = smem > kMaxSmem;
+		if(dglobal)
+			smem = (size_t) 2 * kRotG64 * w * sizeof(double2);
+		CK(cudaFuncSetAttribute(k_rotate_fac<double, kRotG64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) std::max(smem, (size_t) 48 * 1024)));
+		k_rotate_fac<double, kRotG64><<<dim3((n + kRotG64 - 1) / kRotG64, L + 1), 128, smem, st>>>(n, (int) L, polar, (const double2 *) in, istride, abg,
+													     d64, dglobal, (double2 *) out);
+	}
 	CK(cudaGetLastError());
 	return 0;
 }
