@@ -160,18 +160,21 @@ __global__ void __launch_bounds__(128) k_rotate_fac(int n, int L, int polar, con
 			}
 		}
 #pragma unroll
-		for(int g = 0; g < G; g++) {
-			const int s = s0 + g;
-			double sn = 0.0, cs = 1.0;
-			if(s < n)
-				sincos((double) (k - l) * abg[3 * (size_t) s + 1], &sn, &cs);
-			const T c = (T) cs, sv = (T) sn;
-			sV[g * w + k] = T2{acc[g].x * c - acc[g].y * sv, acc[g].x * sv + acc[g].y * c};
+		for(int g = 0; g < G; g++)
+			sV[g * w + k] = acc[g];
+	}
+	__syncthreads();
+	// E(beta): e^{i k beta} (FP64 phases), in place
+	for(int i = threadIdx.x; i < G * w; i += blockDim.x) {
+		const int g = i / w, k = i - g * w, s = s0 + g;
+		if(s < n) {
+			const T2 v = sV[i];
+			const double2 r = phase_mul(make_double2((double) v.x, (double) v.y), (double) (k - l) * abg[3 * (size_t) s + 1], 0);
+			sV[i] = T2{(T) r.x, (T) r.y};
 		}
 	}
 	__syncthreads();
 	for(int mi = threadIdx.x; mi < w; mi += blockDim.x) {
-		const int m = mi - l;
 		T2 acc[G];
 #pragma unroll
 		for(int g = 0; g < G; g++)
@@ -186,11 +189,16 @@ __global__ void __launch_bounds__(128) k_rotate_fac(int n, int L, int polar, con
 			}
 		}
 #pragma unroll
-		for(int g = 0; g < G; g++) {
-			const int s = s0 + g;
-			if(s < n)
-				out[(long long) s * ostride + lm_off(L, l, m)] =
-					phase_mul(make_double2((double) acc[g].x, (double) acc[g].y), -(double) m * abg[3 * (size_t) s], -m);
+		for(int g = 0; g < G; g++)
+			sU[g * w + mi] = acc[g];
+	}
+	__syncthreads();
+	// (-i)^m e^{-i m alpha} (FP64 phases) and the output
+	for(int i = threadIdx.x; i < G * w; i += blockDim.x) {
+		const int g = i / w, mi = i - g * w, m = mi - l, s = s0 + g;
+		if(s < n) {
+			const T2 v = sU[i];
+			out[(long long) s * ostride + lm_off(L, l, m)] = phase_mul(make_double2((double) v.x, (double) v.y), -(double) m * abg[3 * (size_t) s], -m);
 		}
 	}
 }

@@ -7,7 +7,7 @@ stages:
   peaks     the reference localisation of N c1 skies (k_sht_pix argmax,
             k_peak_refine)
   rotate    N series at l_max 48 rotated by their own Euler angles, FP32
-            application (k_rotate_batch)
+            application (k_euler, k_rotate_fac)
   product   N / 2 pairwise products at l_max 48, FP32 (k_sht_F, k_sht_pix,
             k_sht_H, k_sht_A)
   mlp       forward and backward passes of the proposal network on a batch
