@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -1161,10 +1162,29 @@ struct TdSpan {
 	template <class T_> T_ *as() const { return (T_ *) p; }
 };
 
-// grow-only device arena of the time-domain integrator, per device
+// grow-only device arena of the time-domain integrator, per device, and
+// grow-only pinned host staging buffers (one upload, one download per call)
 struct TdArena {
 	std::mutex mu;
 	std::unordered_map<int, std::pair<void *, size_t>> bufs;
+	void *hup = nullptr, *hdown = nullptr;
+	size_t hup_n = 0, hdown_n = 0;
+	static void *pinned(void **p, size_t *have, size_t need)
+	{
+		if(*have < need || !*p) {
+			if(*p)
+				cudaFreeHost(*p);
+			*p = nullptr;
+			*have = 0;
+			if(cudaMallocHost(p, need ? need : 16) != cudaSuccess) {
+				*p = nullptr;
+				set_error("time-domain correlator: cannot allocate %zu bytes of pinned host memory", need);
+				return nullptr;
+			}
+			*have = need;
+		}
+		return *p;
+	}
 	void *get(size_t need)
 	{
 		int dev = 0;
@@ -1333,48 +1353,60 @@ int td_network(const TdBaseline *bl, int nb, int n_det, long long n, const doubl
 	}
 	if(ensure_device())
 		return -1;
-	// arena: series, sky, jobs, then per baseline its pass buffers and rotation rows
+	// device arena: an upload region (series, jobs, then per baseline taps a,
+	// taps b, window, rotation rows) filled by one copy from pinned staging,
+	// a download region (sky, then per baseline power_1d) read back by one
+	// copy, and the scratch of every baseline's pass
 	std::vector<TdShape> sh(nb);
-	std::vector<size_t> sz((size_t) nb * kTdBufs), rot_b(nb);
+	std::vector<size_t> sz((size_t) nb * kTdBufs), rot_b(nb), up_off(nb), pw_off(nb), sc_off(nb);
 	const size_t ser_b = ((size_t) n_det * n * 8 + 255) / 256 * 256, sky_len = ((size_t) sky_L + 1) * (sky_L + 1);
 	const size_t sky_b = (sky_len * 16 + 255) / 256 * 256, job_b = ((size_t) nb * sizeof(DevJob) + 255) / 256 * 256;
-	size_t total = ser_b + sky_b + job_b;
+	size_t up = ser_b + job_b, down = sky_b, scratch = 0;
 	for(int k = 0; k < nb; k++) {
 		sh[k] = td_shape(bl[k].T, bl[k].n_ela, bl[k].n_elb, bl[k].Aa, bl[k].Ab, bl[k].Lp,
 				 taps_real(bl[k].taps_a, bl[k].n_ela, bl[k].Aa) && taps_real(bl[k].taps_b, bl[k].n_elb, bl[k].Ab));
+		const size_t *z = &sz[(size_t) k * kTdBufs];
 		td_sizes(sh[k], &sz[(size_t) k * kTdBufs]);
-		for(int i = 0; i < kTdBufs; i++)
-			total += sz[(size_t) k * kTdBufs + i];
 		rot_b[k] = (((size_t) bl[k].Lp + 1) * (bl[k].Lp + 1) * 16 + 255) / 256 * 256;
-		total += rot_b[k];
+		up_off[k] = up;
+		up += z[0] + z[1] + z[2] + rot_b[k];
+		pw_off[k] = down;
+		down += z[12];
+		sc_off[k] = scratch;
+		for(int i = 3; i < 12; i++)
+			scratch += z[i];
 	}
 	std::lock_guard<std::mutex> lock(g_td_arena.mu);
-	char *base = (char *) g_td_arena.get(total);
-	if(!base)
+	char *base = (char *) g_td_arena.get(up + down + scratch);
+	char *hup = (char *) TdArena::pinned(&g_td_arena.hup, &g_td_arena.hup_n, up);
+	char *hdown = (char *) TdArena::pinned(&g_td_arena.hdown, &g_td_arena.hdown_n, down);
+	if(!base || !hup || !hdown)
 		return -1;
-	char *dser = base, *dsky = base + ser_b, *djobs = dsky + sky_b;
-	size_t o = ser_b + sky_b + job_b;
+	char *dser = base, *djobs = base + ser_b, *dsky = base + up;
 	for(int d = 0; d < n_det; d++)
-		if(h2d(dser + (size_t) d * n * 8, series[d], (size_t) n * 8))
-			return -1;
-	cudaStream_t s = S();
+		memcpy(hup + (size_t) d * n * 8, series[d], (size_t) n * 8);
 	std::vector<DevJob> dj(nb);
-	std::vector<char *> pw(nb);
+	std::vector<std::array<char *, kTdBufs>> bufs(nb);
 	for(int k = 0; k < nb; k++) {
 		const TdBaseline &B = bl[k];
-		char *b[kTdBufs];
-		for(int i = 0; i < kTdBufs; i++) {
+		const size_t *z = &sz[(size_t) k * kTdBufs];
+		char **b = bufs[k].data();
+		b[0] = base + up_off[k];
+		b[1] = b[0] + z[0];
+		b[2] = b[1] + z[1];
+		char *drot = b[2] + z[2];
+		size_t o = up + down + sc_off[k];
+		for(int i = 3; i < 12; i++) {
 			b[i] = base + o;
-			o += sz[(size_t) k * kTdBufs + i];
+			o += z[i];
 		}
-		char *drot = base + o;
-		o += rot_b[k];
-		const size_t rl = ((size_t) B.Lp + 1) * (B.Lp + 1);
-		if(h2d(b[0], B.taps_a, (size_t) B.n_ela * B.Aa * 16) || h2d(b[1], B.taps_b, (size_t) B.n_elb * B.Ab * 16) ||
-		   (B.T > 0 && h2d(b[2], B.window, (size_t) B.T * 8)) || h2d(drot, B.rot_rows, rl * 16))
-			return -1;
-		if(td_launch(sh[k], (const double *) (dser + (size_t) B.det_a * n * 8), (const double *) (dser + (size_t) B.det_b * n * 8), b, s))
-			return -1;
+		b[12] = base + up + pw_off[k];
+		char *h = hup + up_off[k];
+		memcpy(h, B.taps_a, (size_t) B.n_ela * B.Aa * 16);
+		memcpy(h + z[0], B.taps_b, (size_t) B.n_elb * B.Ab * 16);
+		if(B.T > 0)
+			memcpy(h + z[0] + z[1], B.window, (size_t) B.T * 8);
+		memcpy(h + z[0] + z[1] + z[2], B.rot_rows, ((size_t) B.Lp + 1) * (B.Lp + 1) * 16);
 		// the rotation and network sum (correlator.c:665-670, 976-981) as
 		// the FD integrator's: power_1d is already normalised (n = 1)
 		DevJob &J = dj[k];
@@ -1386,18 +1418,25 @@ int td_network(const TdBaseline *bl, int nb, int n_det, long long n, const doubl
 		J.l_max = (int) B.Lp;
 		J.polar = 1;
 		J.weight = weight;
-		pw[k] = b[12];
 	}
-	if(h2d(djobs, dj.data(), (size_t) nb * sizeof(DevJob)))
-		return -1;
+	memcpy(hup + ser_b, dj.data(), (size_t) nb * sizeof(DevJob));
+	cudaStream_t s = S();
+	CK(cudaMemcpyAsync(base, hup, up, cudaMemcpyHostToDevice, s));
+	for(int k = 0; k < nb; k++) {
+		const TdBaseline &B = bl[k];
+		if(td_launch(sh[k], (const double *) (dser + (size_t) B.det_a * n * 8), (const double *) (dser + (size_t) B.det_b * n * 8), bufs[k].data(), s))
+			return -1;
+	}
 	k_rotate_sum<<<2 * sky_L + 1, 64, 0, s>>>((const DevJob *) djobs, nb, (int) sky_L, (double2 *) dsky);
 	CK(cudaGetLastError());
-	if(d2h(sky_host, dsky, sky_len * 16))
+	CK(cudaMemcpyAsync(hdown, dsky, down, cudaMemcpyDeviceToHost, s));
+	if(stream_sync())
 		return -1;
+	memcpy(sky_host, hdown, sky_len * 16);
 	for(int k = 0; k < nb; k++)
-		if(bl[k].power_host && d2h(bl[k].power_host, pw[k], ((size_t) bl[k].Lp + 1) * 16))
-			return -1;
-	return stream_sync();
+		if(bl[k].power_host)
+			memcpy(bl[k].power_host, hdown + pw_off[k], ((size_t) bl[k].Lp + 1) * 16);
+	return 0;
 }
 
 }  // namespace sphrad
