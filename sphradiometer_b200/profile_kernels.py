@@ -13,7 +13,9 @@ stages:
   mlp       forward and backward passes of the proposal network on a batch
             of N (k_gemm and its epilogues)
   uneven    the uneven batch of N segments (gathers, k_tc_contract,
-            k_epilogue, scatters)
+            k_epilogue_f32, k_uneven_combine), default split
+  uneven_tuned  the same after autotuning, every call inside the NVTX
+            range "final" (capture with --nvtx --nvtx-include "final/")
   fseries   3 x N c1 time series (n = 4096) to whitened half spectra
             (k_rfft_whiten)
   nonpolar  N segments through projected (non-polar) c1 plans on the
@@ -45,7 +47,7 @@ def c1_skies(S, W, n):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("stage", choices=["render", "peaks", "rotate", "product", "mlp", "uneven", "fseries", "nonpolar", "td"])
+    ap.add_argument("stage", choices=["render", "peaks", "rotate", "product", "mlp", "uneven", "uneven_tuned", "fseries", "nonpolar", "td"])
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--calls", type=int, default=3)
     args = ap.parse_args()
@@ -134,10 +136,18 @@ def main():
         batch = W.make_uneven_batch(pos, n, seed=11)
         plan = S.UnevenPlan(pos, 1.0 / 4096, batch["buckets"], 48)
         plan.set_segments(batch["bucket"], batch["mask"], batch["l_max"])
-        plan.use_graph(False)
         keep = [plan, batch]
         out = torch.empty(plan.out_total, dtype=torch.complex128, device="cuda")
-        run = lambda: plan.integrate(batch["spectra"], out=out)  # noqa: E731
+        if args.stage == "uneven_tuned":
+            plan.autotune(batch["spectra"], out)
+        plan.use_graph(False)
+
+        def run():
+            if args.stage == "uneven_tuned":
+                torch.cuda.nvtx.range_push("final")
+            plan.integrate(batch["spectra"], out=out)
+            if args.stage == "uneven_tuned":
+                torch.cuda.nvtx.range_pop()
     run()
     torch.cuda.synchronize()
     st = torch.cuda.current_stream()
