@@ -359,7 +359,7 @@ int sphrad_sh_product_batch(sphrad_sh_product_grid *grid, const void *a, const v
  * l <= 12 a_lm of a sky (169 complex values, scaled to unit norm) to a
  * proposed direction of its maximum.  No counterpart in the reference: the
  * proposal seeds the extremizer (sh_series_extremize.c:273-360), which
- * refines it, judges it, and falls back to a full-grid search when the
+ * refines it, vets it, and falls back to a full-grid search when the
  * proposal misses.  Training runs on the GPU by the same kernels (forward,
  * backward, Adam); the loss is the mean of 1 - cos(angle to the target).
  * Batches hold at most max_batch skies; device arrays throughout. */
@@ -393,9 +393,9 @@ float sphrad_proposal_loss(sphrad_proposal *p, int n);
 int sphrad_proposal_set_mirror(sphrad_proposal *p, const double *normal);
 /* Localisation of n skies (in the frame the network was trained in):
  * proposal, FP64 refinement of the maximum of Re f from it, and its
- * judgement on the coarse `judge` grid: accepted when the refinement
+ * vetting on the coarse `vet` grid: accepted when the refinement
  * converged, moved at most max_move_deg, reached a value f > 0 that no
- * judge pixel exceeds, and every judge pixel farther than basin_deg from
+ * vet pixel exceeds, and every vet pixel farther than basin_deg from
  * the refined peak (and from its mirror image) stays below
  * f (1 - dominance); the rest get the full-grid search on `grid` (its
  * pixel of largest Re f, then the same refinement).  out:
@@ -403,7 +403,7 @@ int sphrad_proposal_set_mirror(sphrad_proposal *p, const double *normal);
  * converged, bits 1-23 iterations, bit 24 set for skies that fell back;
  * *n_fallback (host) counts them.  Synchronises with the stream once per
  * 16384 skies. */
-int sphrad_proposal_localise(sphrad_proposal *p, sphrad_sky_grid *judge, sphrad_sky_grid *grid, const void *sky, int n, unsigned l_max,
+int sphrad_proposal_localise(sphrad_proposal *p, sphrad_sky_grid *vet, sphrad_sky_grid *grid, const void *sky, int n, unsigned l_max,
 			     double max_move_deg, double basin_deg, double dominance, double *out, int *status, int *n_fallback, void *cuda_stream);
 /* 0, or the code of a device-side wait that timed out */
 int sphrad_proposal_status(sphrad_proposal *p);

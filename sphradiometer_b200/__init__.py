@@ -792,7 +792,7 @@ class Proposal:
             v = np.ascontiguousarray(normal, np.float64)
             load().sphrad_proposal_set_mirror(self._p, v.ctypes.data)
 
-    def localise(self, judge: "SkyGrid", grid: "SkyGrid", sky, max_move_deg: float = 30.0, basin_deg: float = 6.0, dominance: float = 0.1):
+    def localise(self, vet: "SkyGrid", grid: "SkyGrid", sky, max_move_deg: float = 30.0, basin_deg: float = 6.0, dominance: float = 0.1):
         """Returns (out [n][4], status [n], n_fallback)."""
         import torch
         n = sky.shape[0]
@@ -800,7 +800,7 @@ class Proposal:
         out = torch.empty((n, 4), dtype=torch.float64, device=sky.device)
         st = torch.empty(n, dtype=torch.int32, device=sky.device)
         nf = C.c_int(0)
-        if load().sphrad_proposal_localise(self._p, judge._g, grid._g, sky.data_ptr(), n, L, float(max_move_deg), float(basin_deg), float(dominance),
+        if load().sphrad_proposal_localise(self._p, vet._g, grid._g, sky.data_ptr(), n, L, float(max_move_deg), float(basin_deg), float(dominance),
                                            out.data_ptr(),
                                            st.data_ptr(), C.byref(nf),
                                            self._st()):

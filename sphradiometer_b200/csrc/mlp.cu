@@ -444,14 +444,14 @@ __global__ void k_dir_to_tp(int n, const float *dir, double *theta, double *phi)
 	phi[r] = p < 0 ? p + 2 * M_PI : p;
 }
 
-// Judgement of a refined proposal on the rendered judge grid (one block per
+// Vetting of a refined proposal on the rendered vet grid (one block per
 // sky): the pixels within `basin` of the refined peak (or of its mirror
 // image through the plane with normal `mirror`, when given) are its basin.
 // Accepted when the refinement converged, moved at most max_move from the
 // proposal, no pixel exceeds the refined value, and every pixel outside
 // the basin stays below it by dominance * |value|: the plain full-grid
 // search then starts in the same basin.  The rest are listed for it.
-__global__ void k_judge(int n, const float *gridv, const double *theta_rows, int nt, int nphi, const double *out, const int *status, double max_move,
+__global__ void k_vet(int n, const float *gridv, const double *theta_rows, int nt, int nphi, const double *out, const int *status, double max_move,
 			double cos_basin, double3 mirror, double dominance, int *list, int *count)
 {
 	const int r = blockIdx.x;
@@ -552,10 +552,10 @@ struct Mlp {
 	double *t0 = nullptr, *p0 = nullptr, *fb_out = nullptr;
 	int *list = nullptr, *count = nullptr, *fb_status = nullptr;
 	double2 *fb_sky = nullptr;
-	float *judge_vals = nullptr;
+	float *vet_vals = nullptr;
 	void *fb_scratch = nullptr;
 	size_t fb_scratch_len = 0;
-	int loc_nt = 0, loc_np = 0;   // judge grid the buffers were sized for
+	int loc_nt = 0, loc_np = 0;   // vet grid the buffers were sized for
 	long long loc_stride = 0;     // coefficients per sky they were sized for
 	double3 mirror = {0, 0, 0};
 	std::vector<void *> allocs;
@@ -568,12 +568,12 @@ struct Mlp {
 	}
 	void free_loc()
 	{
-		for(void *q : {(void *) t0, (void *) p0, (void *) fb_out, (void *) list, (void *) fb_status, (void *) fb_sky, (void *) judge_vals})
+		for(void *q : {(void *) t0, (void *) p0, (void *) fb_out, (void *) list, (void *) fb_status, (void *) fb_sky, (void *) vet_vals})
 			dfree(q);
 		t0 = p0 = fb_out = nullptr;
 		list = fb_status = nullptr;
 		fb_sky = nullptr;
-		judge_vals = nullptr;
+		vet_vals = nullptr;
 		loc_cap = 0;
 	}
 	template <class T> T *alloc(size_t n)
@@ -973,8 +973,8 @@ int mlp_status(void *plan)
 
 // Localisation of n device skies in passes of up to kLocPass: proposals
 // chunk by chunk (the network's batch capacity), then one refinement, one
-// judgement and one full-grid search over the whole pass, so no kernel
-// waits on a short chunk's slowest sky.  judge and grid are sht plans
+// vetting and one full-grid search over the whole pass, so no kernel
+// waits on a short chunk's slowest sky.  vet and grid are sht plans
 // covering l_max.
 constexpr int kLocPass = 16384;
 
@@ -984,13 +984,13 @@ static size_t argmax_scratch(void *grid, int n, int M, size_t *rb_off)
 	return *rb_off + sht_rowbest_bytes(grid, n);
 }
 
-static int loc_buffers(Mlp *p, void *judge, void *grid, unsigned L, int cap)
+static int loc_buffers(Mlp *p, void *vet, void *grid, unsigned L, int cap)
 {
 	const long long stride = (long long) (L + 1) * (L + 1);
-	const int nt = sht_plan_rows(judge, nullptr), np = sht_plan_nphi(judge);
+	const int nt = sht_plan_rows(vet, nullptr), np = sht_plan_nphi(vet);
 	size_t o1, o2;
-	const size_t scr = std::max(std::max(argmax_scratch(grid, cap, (int) L, &o1), argmax_scratch(judge, cap, (int) L, &o2)),
-				    sht_scratch_bytes(judge, cap, (int) L));
+	const size_t scr = std::max(std::max(argmax_scratch(grid, cap, (int) L, &o1), argmax_scratch(vet, cap, (int) L, &o2)),
+				    sht_scratch_bytes(vet, cap, (int) L));
 	if(scr > p->fb_scratch_len) {
 		dfree(p->fb_scratch);
 		p->fb_scratch = dmalloc(scr);
@@ -1009,8 +1009,8 @@ static int loc_buffers(Mlp *p, void *judge, void *grid, unsigned L, int cap)
 	p->list = (int *) dmalloc(cap * sizeof(int));
 	p->fb_status = (int *) dmalloc(cap * sizeof(int));
 	p->fb_sky = (double2 *) dmalloc((size_t) cap * stride * sizeof(double2));
-	p->judge_vals = (float *) dmalloc((size_t) cap * nt * np * sizeof(float));
-	if(!p->t0 || !p->p0 || !p->fb_out || !p->list || !p->fb_status || !p->fb_sky || !p->judge_vals) {
+	p->vet_vals = (float *) dmalloc((size_t) cap * nt * np * sizeof(float));
+	if(!p->t0 || !p->p0 || !p->fb_out || !p->list || !p->fb_status || !p->fb_sky || !p->vet_vals) {
 		p->free_loc();
 		return -1;
 	}
@@ -1028,7 +1028,7 @@ int mlp_set_mirror(void *plan, const double *normal)
 	return 0;
 }
 
-int mlp_localise(void *plan, void *judge, void *grid, const void *sky, int n, unsigned L, double max_move, double basin, double dominance, double *out,
+int mlp_localise(void *plan, void *vet, void *grid, const void *sky, int n, unsigned L, double max_move, double basin, double dominance, double *out,
 		 int *status, int *n_fallback, void *stream)
 {
 	Mlp *p = (Mlp *) plan;
@@ -1040,9 +1040,9 @@ int mlp_localise(void *plan, void *judge, void *grid, const void *sky, int n, un
 			*n_fallback = 0;
 		return 0;
 	}
-	if(loc_buffers(p, judge, grid, L, pass))
+	if(loc_buffers(p, vet, grid, L, pass))
 		return -1;
-	const int nt = sht_plan_rows(judge, nullptr), np = sht_plan_nphi(judge);
+	const int nt = sht_plan_rows(vet, nullptr), np = sht_plan_nphi(vet);
 	int total_fb = 0;
 	for(int s0 = 0; s0 < n; s0 += pass) {
 		const int sn = n - s0 < pass ? n - s0 : pass;
@@ -1059,10 +1059,10 @@ int mlp_localise(void *plan, void *judge, void *grid, const void *sky, int n, un
 		}
 		if(peak_refine(sn, L, 0, sp, stride, p->t0, p->p0, 1.0, 100, 1e-10, op, stp, stream))
 			return -1;
-		if(sht_synthesis(judge, sp, sn, stride, L, 0, L, kPixReal, p->judge_vals, p->fb_scratch, stream, 1.0))
+		if(sht_synthesis(vet, sp, sn, stride, L, 0, L, kPixReal, p->vet_vals, p->fb_scratch, stream, 1.0))
 			return -1;
 		CKM(cudaMemsetAsync(p->count, 0, 4, st));
-		k_judge<<<sn, 256, 0, st>>>(sn, p->judge_vals, sht_plan_theta_dev(judge), nt, np, op, stp, max_move, cos(basin), p->mirror, dominance, p->list,
+		k_vet<<<sn, 256, 0, st>>>(sn, p->vet_vals, sht_plan_theta_dev(vet), nt, np, op, stp, max_move, cos(basin), p->mirror, dominance, p->list,
 					    p->count);
 		CKM(cudaGetLastError());
 		int cnt = 0;

@@ -251,7 +251,7 @@ int mlp_backward(void *plan, int n, const float *target, void *stream);
 int mlp_adam(void *plan, float lr, void *stream);
 int mlp_loss(void *plan, float *host_loss, int n);
 int mlp_status(void *plan);
-int mlp_localise(void *plan, void *judge, void *grid, const void *sky, int n, unsigned L, double max_move, double basin, double dominance, double *out,
+int mlp_localise(void *plan, void *vet, void *grid, const void *sky, int n, unsigned L, double max_move, double basin, double dominance, double *out,
 		 int *status, int *n_fallback, void *stream);
 int mlp_set_mirror(void *plan, const double *normal);
 // in-place unnormalised DFT along the array index of n x stride host

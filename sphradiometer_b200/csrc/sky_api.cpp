@@ -241,7 +241,7 @@ extern "C" float sphrad_proposal_loss(sphrad_proposal *p, int n)
 
 extern "C" int sphrad_proposal_set_mirror(sphrad_proposal *p, const double *normal) { return mlp_set_mirror(p->mlp, normal); }
 
-extern "C" int sphrad_proposal_localise(sphrad_proposal *p, sphrad_sky_grid *judge, sphrad_sky_grid *grid, const void *sky, int n, unsigned l_max,
+extern "C" int sphrad_proposal_localise(sphrad_proposal *p, sphrad_sky_grid *vet, sphrad_sky_grid *grid, const void *sky, int n, unsigned l_max,
 					double max_move_deg, double basin_deg, double dominance, double *out, int *status, int *n_fallback, void *stream)
 {
 	if(n <= 0) {
@@ -249,11 +249,11 @@ extern "C" int sphrad_proposal_localise(sphrad_proposal *p, sphrad_sky_grid *jud
 			*n_fallback = 0;
 		return 0;
 	}
-	if(!grid || grid->l_max < l_max || !judge || judge->l_max < l_max) {
-		set_error("sphrad_proposal_localise: the judge and fallback grids must cover l_max %u", l_max);
+	if(!grid || grid->l_max < l_max || !vet || vet->l_max < l_max) {
+		set_error("sphrad_proposal_localise: the vet and fallback grids must cover l_max %u", l_max);
 		return -1;
 	}
-	return mlp_localise(p->mlp, judge->plan, grid->plan, sky, n, l_max, max_move_deg * M_PI / 180.0, basin_deg * M_PI / 180.0, dominance, out, status,
+	return mlp_localise(p->mlp, vet->plan, grid->plan, sky, n, l_max, max_move_deg * M_PI / 180.0, basin_deg * M_PI / 180.0, dominance, out, status,
 			    n_fallback, caller_stream(stream));
 }
 

@@ -54,13 +54,13 @@ def angle(u, v):
 class Generator:
     """Skies of the c1-style network in the Earth frame, with labels."""
 
-    def __init__(self, S, positions, precision: str = "bf16x3", chunk: int = 8192, judge_rows: int = 24):
+    def __init__(self, S, positions, precision: str = "bf16x3", chunk: int = 8192, vet_rows: int = 24):
         self.S = S
         self.positions = np.asarray(positions, np.float64)
         self.net = S.Network(self.positions, N_SAMPLES, DT, l_max=L_MAX)
         self.bp = S.BatchPlan(self.net, precision)
         self.grid = S.SkyGrid(L_MAX, 64, 128, kind="cell", fp32=True)
-        self.judge = S.SkyGrid(L_MAX, judge_rows, 2 * judge_rows, kind="cell", fp32=True)
+        self.vet = S.SkyGrid(L_MAX, vet_rows, 2 * vet_rows, kind="cell", fp32=True)
         self.nrm = plane_normal(self.positions)
         self.chunk = chunk
 
@@ -89,7 +89,7 @@ class Generator:
         return feats, targets
 
     def close(self):
-        for o in (self.judge, self.grid, self.bp, self.net):
+        for o in (self.vet, self.grid, self.bp, self.net):
             o.close()
 
 
@@ -129,7 +129,7 @@ def evaluate(S, gen: Generator, prop, n: int, seed: int, max_move_deg: float = 3
     feats = prop.sky_features(sky)
     dirs = torch.cat([prop.forward(feats[c0:c0 + prop.max_batch]) for c0 in range(0, n, prop.max_batch)])
     prop.set_mirror(gen.nrm)
-    out, st, nfb = prop.localise(gen.judge, gen.grid, sky, max_move_deg, basin_deg, dominance)
+    out, st, nfb = prop.localise(gen.vet, gen.grid, sky, max_move_deg, basin_deg, dominance)
     vr = canonical(unit(ref[:, 0], ref[:, 1]), gen.nrm)
     vo = canonical(unit(out[:, 0], out[:, 1]), gen.nrm)
     vp = canonical(dirs.double(), gen.nrm)
@@ -146,7 +146,7 @@ def evaluate(S, gen: Generator, prop, n: int, seed: int, max_move_deg: float = 3
     t_grid = a.elapsed_time(b) / 1e3 / reps
     t0 = time.perf_counter()
     for _ in range(reps):
-        prop.localise(gen.judge, gen.grid, sky, max_move_deg, basin_deg, dominance)
+        prop.localise(gen.vet, gen.grid, sky, max_move_deg, basin_deg, dominance)
     torch.cuda.synchronize()
     t_prop = (time.perf_counter() - t0) / reps
     q = torch.quantile(perr.float(), torch.tensor([0.5, 0.9, 0.99], device=perr.device)).cpu().numpy()

@@ -133,7 +133,7 @@ def test_learned_proposal_localisation(S):
     print("trained", ev, "losses", losses)
     assert losses[-1] < 0.7 * losses[0]
     assert ev["agree_within_0.5deg"] >= 0.99
-    assert ev0["agree_within_0.5deg"] >= 0.99  # the judge protects an untrained network too
+    assert ev0["agree_within_0.5deg"] >= 0.99  # the vetting protects an untrained network too
     assert ev["fallback_rate"] < ev0["fallback_rate"] - 0.2
     assert ev["proposal_err_deg_p50_p90_p99"][0] < 10.0
     assert prop.status() == 0
