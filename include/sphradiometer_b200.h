@@ -96,8 +96,12 @@ int sphrad_batch_integrate_weighted(sphrad_batch_plan *plan, const void *fseries
 				    size_t workspace_bytes, void *cuda_stream, int split, const float *baseline_factor);
 
 /* The same with host buffers: copies in, integrates, copies out and
- * synchronises (library-owned device buffers).  Use pinned host memory for
- * full copy bandwidth. */
+ * synchronises (library-owned device buffers).  From 1024 segments on, the
+ * batch is cut into chunks of at least 512 segments that alternate between
+ * two streams, so that one chunk's host-to-device copy overlaps the kernels
+ * and the device-to-host copy of the one before.  Use pinned host memory
+ * for full copy bandwidth (and for the overlap: copies from pageable
+ * memory are staged synchronously). */
 int sphrad_batch_integrate_host(sphrad_batch_plan *plan, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky);
 
 /* Split-K factor used for n_seg segments: the value stored by
