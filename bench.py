@@ -145,6 +145,20 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def oracle_tables(pos):
+    """The oracle's own (delay table, rotation plan) of every baseline of the
+    workload's network, in the library's baseline order (i > j)."""
+    from oracle import oracle as O
+    tables = []
+    for i in range(1, N_DET):
+        for j in range(i):
+            d = pos[i] - pos[j]
+            th, ph = O.vector_direction(d)
+            tables.append((O.delay_product(float(np.linalg.norm(d)), DT, N_SAMPLES, L_MAX),
+                           O.rotation_plan(L_MAX, O.rot_matrix(th, ph))))
+    return tables
+
+
 def cpu_oracle_rate(net_tables, F_half, gmst, budget_s: float, threads: int):
     """Maps/s of the CPU oracle (C, FP64) integrating segments exactly as
     correlator_network_integrate_power_fd + sh_series_rotate_z do, on
@@ -231,7 +245,7 @@ def accuracy_report(S, net, base, n_check: int, positions):
     from oracle import oracle as O
     from sphradiometer_b200 import workload as W
     pairs = [(1, 0), (2, 0), (2, 1)]
-    tabs = [(net.delay_table(k), net.rotation_flat(k)) for k in range(3)]
+    tabs = oracle_tables(positions)
     ref = np.zeros((n_check, (L_MAX + 1) ** 2), np.complex128)
     for s in range(n_check):
         F = W.full_from_half(base["F"][:, s, :], N_SAMPLES)
@@ -622,13 +636,7 @@ def run_reference(args):
     from oracle import oracle as O
     from sphradiometer_b200 import workload as W
     pos = positions()
-    tables = []
-    for i in range(1, N_DET):
-        for j in range(i):
-            d = pos[i] - pos[j]
-            th, ph = O.vector_direction(d)
-            tables.append((O.delay_product(float(np.linalg.norm(d)), DT, N_SAMPLES, L_MAX),
-                           O.rotation_plan(L_MAX, O.rot_matrix(th, ph))))
+    tables = oracle_tables(pos)
     batch = W.make_batch(pos, N_SAMPLES, DT, 64, seed=1234)
     threads = os.cpu_count() or 1
     rates = []
@@ -816,8 +824,8 @@ def run(args):
             bp64.close()
 
         # accuracy of every precision against the FP64 oracle on a sample of
-        # segments (the oracle integrates the same delay tables, which the
-        # tests check against the oracle's own tables)
+        # segments (the oracle integrates on its own delay tables and
+        # rotation plans)
         extra["accuracy"] = accuracy_report(S, net, base, min(32, base["F"].shape[1]), pos)
         extra["c0"] = c0_report(S)
         extra.update(sky_stage_rates(S, out))
@@ -830,7 +838,7 @@ def run(args):
             extra["c4_learned_proposal"] = guarded(c4_report, S)
 
         # CPU baseline: the oracle on the host cores, bounded sample
-        tables = [(net.delay_table(k), net.rotation_flat(k)) for k in range(3)]
+        tables = oracle_tables(pos)
         threads = os.cpu_count() or 1
         rate, nmaps, el = cpu_oracle_rate(tables, base["F"], base["gmst"], args.cpu_seconds, threads)
         cpu = {"value": rate, "unit": "maps/s", "cores": threads, "kind": "port",

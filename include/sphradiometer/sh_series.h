@@ -159,6 +159,11 @@ struct sh_series *sh_series_rotate_z(struct sh_series *, const struct sh_series 
 /* extremization (reference sh_series.h:369, sh_series_extremize.c:273) */
 double sh_series_real_minimum(const struct sh_series *, double *, double *);
 
+/* text output (reference sh_series.h:379, sh_series_io.c:53-70): one line
+ * "(l,m) = re + I im" (%.17g) per non-zero coefficient, in order of l then
+ * m; a single "(0,0) = 0 + I 0" line when all are zero */
+void sh_series_print(FILE *, const struct sh_series *);
+
 /* sh_series_array (reference sh_series.h:399-428, sh_series_array.c) */
 struct sh_series_array *sh_series_array_new(int, unsigned int, int);
 void sh_series_array_free(struct sh_series_array *);

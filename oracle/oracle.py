@@ -95,6 +95,8 @@ def lib():
         L.orc_find_near_minimum.argtypes = [_cp, u, i, u, C.POINTER(d), C.POINTER(d)]
         L.orc_real_maximum.restype = d
         L.orc_real_maximum.argtypes = [_cp, u, i, C.POINTER(d), C.POINTER(d)]
+        L.orc_real_minimum_ref.restype = d
+        L.orc_real_minimum_ref.argtypes = [_cp, u, i, C.POINTER(d), C.POINTER(d)]
         _lib = L
     return _lib
 
@@ -367,8 +369,18 @@ def find_near_minimum(a, l_max, polar, l_lowpass=6):
 
 
 def real_maximum(a, l_max, polar):
+    """max Re a by the reference's method (l <= 6 start, BFGS2) with the
+    gradient in the minimiser's own co-ordinates; (value, theta, phi)."""
     t, p = C.c_double(), C.c_double()
     v = lib().orc_real_maximum(_c(a), l_max, int(polar), C.byref(t), C.byref(p))
+    return v, t.value, p.value
+
+
+def real_minimum_ref(a, l_max, polar):
+    """sh_series_real_minimum as the reference runs it (its gradient
+    convention; theta, phi unconditioned); (value, theta, phi)."""
+    t, p = C.c_double(), C.c_double()
+    v = lib().orc_real_minimum_ref(_c(a), l_max, int(polar), C.byref(t), C.byref(p))
     return v, t.value, p.value
 
 

@@ -15,6 +15,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include "sphrad_oracle.h"
+#include "ref_shims/bfgs2.h"
 
 #ifndef M_PI
 #define M_PI 3.14159265358979323846
@@ -1022,83 +1023,114 @@ static void condition_theta_phi(double *theta, double *phi)
 		*phi += 2 * M_PI;
 }
 
-static double neg_re(const double complex *a, unsigned l_max, int polar, double t, double p)
+/* Re f, d/dtheta Re f and (1/sin theta) d/dphi Re f at (theta, phi): the
+ * value and the two gradient components the reference's dfunc() forms
+ * (sh_series_extremize.c:115-150) from the series sin(theta) df/dtheta
+ * and df/dphi (sh_series_deriv.c:531-543), here from the Legendre
+ * derivative sin(theta) dP~_l^m/dtheta = l x P~_l^m
+ * - sqrt((2l+1)(l^2-m^2)/(2l-1)) P~_{l-1}^m. */
+static void re_value_grad(const double complex *a, unsigned l_max, int polar, double theta, double phi, double *f, double *u, double *v)
 {
-	condition_theta_phi(&t, &p);
-	return -creal(orc_eval(a, l_max, polar, t, p));
+	const double x = cos(theta), st = sin(theta);
+	double *P = malloc((l_max + 1) * sizeof(*P));
+	double complex val = 0.0, dth = 0.0, dph = 0.0;
+	const int mmax = polar ? 0 : (int) l_max;
+	for(int m = -mmax; m <= mmax; m++) {
+		const int am = abs(m);
+		orc_sphPlm_array(l_max, am, x, P);
+		const double sgn = (m < 0 && (am & 1)) ? -1.0 : 1.0;
+		const double complex e = sgn * (cos(m * phi) + I * sin(m * phi));
+		for(unsigned l = am; l <= l_max; l++) {
+			const double complex c = a[orc_lmoffset(l_max, l, m)];
+			const double p = P[l - am];
+			const double pm1 = l > (unsigned) am ? P[l - 1 - am] : 0.0;
+			const double s_dp = l * x * p - (l > (unsigned) am ? sqrt((2.0 * l + 1.0) * ((double) l * l - (double) m * m) / (2.0 * l - 1.0)) * pm1 : 0.0);
+			val += c * e * p;
+			dth += c * e * s_dp;
+			dph += c * e * p * (I * m);
+		}
+	}
+	free(P);
+	*f = creal(val);
+	*u = creal(dth) / st;
+	*v = creal(dph) / st;
 }
 
-/* Maximum of Re f.  The reference minimises with GSL's BFGS2 from the
- * coarse point (sh_series_extremize.c:273-360); its own test asserts
- * nothing, so this refinement is the oracle's own: a quasi-Newton
- * (BFGS) iteration on (theta, phi) with central-difference gradients and
- * a backtracking line search, from the same coarse start. */
-double orc_real_maximum(const double complex *a, unsigned l_max, int polar, double *theta, double *phi)
+struct extremize_params {
+	const double complex *a;
+	unsigned l_max;
+	int polar;
+};
+
+/* func() and dfunc() of sh_series_extremize.c:115-150: the series at the
+ * conditioned co-ordinates, x = (theta, phi) left as the minimiser has it,
+ * gradient (d/dtheta, (1/sin theta) d/dphi) -- the components along the
+ * unit vectors, which are not the derivatives in the minimiser's
+ * co-ordinates (theta, phi) */
+static void extremize_fdf_ref(const double *xv, void *params, double *f, double *g)
 {
-	double complex *neg = malloc(orc_length(l_max, polar) * sizeof(*neg));
-	for(size_t i = 0; i < orc_length(l_max, polar); i++)
-		neg[i] = -a[i];
-	double t, p;
-	orc_find_near_minimum(neg, l_max, polar, 6, &t, &p);
-	free(neg);
-	double H[4] = {1, 0, 0, 1};
-	const double h = 1e-6;
-	double fx = neg_re(a, l_max, polar, t, p);
-	double g[2];
-	g[0] = (neg_re(a, l_max, polar, t + h, p) - neg_re(a, l_max, polar, t - h, p)) / (2 * h);
-	g[1] = (neg_re(a, l_max, polar, t, p + h) - neg_re(a, l_max, polar, t, p - h)) / (2 * h);
-	for(int it = 0; it < 200; it++) {
-		double d[2] = {-(H[0] * g[0] + H[1] * g[1]), -(H[2] * g[0] + H[3] * g[1])};
-		double slope = d[0] * g[0] + d[1] * g[1];
-		if(slope >= 0) {
-			H[0] = H[3] = 1;
-			H[1] = H[2] = 0;
-			d[0] = -g[0];
-			d[1] = -g[1];
-			slope = d[0] * g[0] + d[1] * g[1];
-		}
-		/* limit the step to pi/24 as the reference's initial step */
-		const double dn = sqrt(d[0] * d[0] + d[1] * d[1]);
-		double step = dn > M_PI / 24 ? (M_PI / 24) / dn : 1.0;
-		double tn = t, pn = p, fn = fx;
-		for(int ls = 0; ls < 60; ls++) {
-			tn = t + step * d[0];
-			pn = p + step * d[1];
-			fn = neg_re(a, l_max, polar, tn, pn);
-			if(fn <= fx + 1e-4 * step * slope)
-				break;
-			step *= 0.5;
-		}
-		if(!(fn <= fx)) {
+	const struct extremize_params *ep = params;
+	double t = xv[0], p = xv[1];
+	condition_theta_phi(&t, &p);
+	re_value_grad(ep->a, ep->l_max, ep->polar, t, p, f, &g[0], &g[1]);
+}
+
+/* the same value with the gradient in the co-ordinates themselves,
+ * (d/dtheta, d/dphi) */
+static void extremize_fdf_coord(const double *xv, void *params, double *f, double *g)
+{
+	const struct extremize_params *ep = params;
+	double t = xv[0], p = xv[1];
+	condition_theta_phi(&t, &p);
+	re_value_grad(ep->a, ep->l_max, ep->polar, t, p, f, &g[0], &g[1]);
+	g[1] *= sin(t);
+}
+
+/* the l <= 6 start, then the BFGS2 restatement of ref_shims/bfgs2.h (first
+ * step pi/24, line tolerance 0.001, at most 100 iterations, stop at
+ * |gradient| < 1e-3); minimises Re a; x left unconditioned */
+static double minimise_bfgs2(const double complex *a, unsigned l_max, int polar, bfgs2_eval_fn fdf, double *theta, double *phi)
+{
+	double x0[2];
+	if(isnan(orc_find_near_minimum(a, l_max, polar, 6, &x0[0], &x0[1])))
+		return NAN;
+	struct extremize_params ep = {a, l_max, polar};
+	struct bfgs2 s;
+	bfgs2_set(&s, 2, fdf, &ep, x0, M_PI / 24., 0.001);
+	for(int iter = 0; iter < 100; iter++) {
+		if(bfgs2_iterate(&s))
 			break;
-		}
-		double gn[2];
-		gn[0] = (neg_re(a, l_max, polar, tn + h, pn) - neg_re(a, l_max, polar, tn - h, pn)) / (2 * h);
-		gn[1] = (neg_re(a, l_max, polar, tn, pn + h) - neg_re(a, l_max, polar, tn, pn - h)) / (2 * h);
-		const double s[2] = {tn - t, pn - p};
-		const double y[2] = {gn[0] - g[0], gn[1] - g[1]};
-		const double sy = s[0] * y[0] + s[1] * y[1];
-		if(sy > 1e-300) {
-			/* BFGS update of the inverse Hessian */
-			const double Hy[2] = {H[0] * y[0] + H[1] * y[1], H[2] * y[0] + H[3] * y[1]};
-			const double yHy = y[0] * Hy[0] + y[1] * Hy[1];
-			const double c1 = (sy + yHy) / (sy * sy);
-			H[0] += c1 * s[0] * s[0] - (Hy[0] * s[0] + s[0] * Hy[0]) / sy;
-			H[1] += c1 * s[0] * s[1] - (Hy[0] * s[1] + s[0] * Hy[1]) / sy;
-			H[2] += c1 * s[1] * s[0] - (Hy[1] * s[0] + s[1] * Hy[0]) / sy;
-			H[3] += c1 * s[1] * s[1] - (Hy[1] * s[1] + s[1] * Hy[1]) / sy;
-		}
-		const double moved = sqrt(s[0] * s[0] + s[1] * s[1]);
-		t = tn;
-		p = pn;
-		fx = fn;
-		g[0] = gn[0];
-		g[1] = gn[1];
-		if(moved < 1e-10 || sqrt(g[0] * g[0] + g[1] * g[1]) < 1e-10 * (1 + fabs(fx)))
+		if(sqrt(s.g[0] * s.g[0] + s.g[1] * s.g[1]) < 1e-3)
 			break;
 	}
+	*theta = s.x[0];
+	*phi = s.x[1];
+	return s.f;
+}
+
+/* sh_series_real_minimum (sh_series_extremize.c:273-360) as the reference
+ * runs it: its gradient convention, and (theta, phi) returned as the
+ * minimiser leaves them (not conditioned). */
+double orc_real_minimum_ref(const double complex *a, unsigned l_max, int polar, double *theta, double *phi)
+{
+	return minimise_bfgs2(a, l_max, polar, extremize_fdf_ref, theta, phi);
+}
+
+/* Maximum of Re a: the reference's method (l <= 6 start, BFGS2 with the
+ * same parameters) on -a, with the gradient taken in the minimiser's own
+ * co-ordinates so that the line search's slope is the true one; returns
+ * max Re a and its conditioned co-ordinates. */
+double orc_real_maximum(const double complex *a, unsigned l_max, int polar, double *theta, double *phi)
+{
+	const size_t len = orc_length(l_max, polar);
+	double complex *neg = malloc(len * sizeof(*neg));
+	for(size_t i = 0; i < len; i++)
+		neg[i] = -a[i];
+	double t, p;
+	const double v = minimise_bfgs2(neg, l_max, polar, extremize_fdf_coord, &t, &p);
+	free(neg);
 	condition_theta_phi(&t, &p);
 	*theta = t;
 	*phi = p;
-	return -fx;
+	return -v;
 }

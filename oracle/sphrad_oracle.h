@@ -92,8 +92,13 @@ void orc_vector_direction(const double *v, double *theta, double *phi);
 void orc_render_grid(const double complex *a, unsigned l_max, int polar, int ntheta, int nphi, double *grid);
 
 /* peak finding (sh_series_extremize.c:168-360): coarse search on the
- * l = 6 mesh, then a quasi-Newton refinement of the real part */
+ * l = 6 mesh, then the BFGS2 restatement of ref_shims/bfgs2.h.
+ * orc_real_minimum_ref is sh_series_real_minimum as the reference runs it
+ * (gradient components along the unit vectors, co-ordinates returned
+ * unconditioned); orc_real_maximum maximises Re a with the gradient in the
+ * minimiser's own co-ordinates and returns conditioned co-ordinates. */
 double orc_find_near_minimum(const double complex *a, unsigned l_max, int polar, unsigned l_lowpass, double *theta, double *phi);
+double orc_real_minimum_ref(const double complex *a, unsigned l_max, int polar, double *theta, double *phi);
 double orc_real_maximum(const double complex *a, unsigned l_max, int polar, double *theta, double *phi);
 
 #endif

@@ -300,6 +300,24 @@ extern "C" dcplx sh_series_set(struct sh_series *series, unsigned int l, int m, 
 	return series->coeff[lmoffset(series->l_max, l, m)] = val;
 }
 
+extern "C" void sh_series_print(FILE *f, const struct sh_series *series)
+{
+	const int L = (int) series->l_max;
+	int written = 0;
+	for(int l = 0; l <= L; l++) {
+		const int mm = series->polar ? 0 : l;
+		for(int m = -mm; m <= mm; m++) {
+			const dcplx c = series->coeff[series->polar ? (size_t) l : lmoffset(series->l_max, l, m)];
+			if(cre(c) == 0.0 && cim(c) == 0.0)
+				continue;
+			fprintf(f, "(%d,%d) = %.17g + I %.17g\n", l, m, cre(c), cim(c));
+			written++;
+		}
+	}
+	if(!written)
+		fprintf(f, "(%d,%d) = %.17g + I %.17g\n", 0, 0, 0.0, 0.0);
+}
+
 extern "C" int sh_series_is_nan(const struct sh_series *s)
 {
 	for(size_t i = 0; i < length(s->l_max, s->polar); i++)

@@ -133,18 +133,13 @@ def test_integrate_tseries_bf16x3_matches_oracle(S, c1t):
     x = torch.from_numpy(b["x"]).cuda()
     g = torch.from_numpy(b["gmst"].copy()).cuda()
     got = bp.integrate_tseries(fp, x, g).cpu().numpy()
-    # oracle skies from numpy spectra, on the library's delay tables (checked
-    # against the oracle's own elsewhere)
-    tabs = [(net.delay_table(k), net.rotation_flat(k)) for k in range(3)]
-    pairs = [(1, 0), (2, 0), (2, 1)]
+    # oracle skies from numpy spectra, on the oracle's own plan
+    oplan = O.NetworkPlan(c1t["pos"], n, 1.0 / n, L)
     segs = range(0, 40, 4)
     errs, num, den = [], 0.0, 0.0
     for s in segs:
         F = W.full_from_half(b["F"][:, s, :], n)
-        ref = np.zeros((L + 1) ** 2, np.complex128)
-        for k, (i, j) in enumerate(pairs):
-            ref += O.baseline_integrate_power_fd(F[i], F[j], tabs[k][0], L, tabs[k][1]) / 3
-        ref = O.rotate_z(ref, L, False, b["gmst"][s])
+        ref = O.rotate_z(oplan.integrate(F), L, False, b["gmst"][s])
         errs.append(np.linalg.norm(got[s] - ref) / np.linalg.norm(ref))
         num += np.linalg.norm(got[s] - ref) ** 2
         den += np.linalg.norm(ref) ** 2

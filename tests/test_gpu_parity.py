@@ -180,17 +180,39 @@ def c1(lib):
     n, dt, L = 4096, 1.0 / 4096, 32
     net = lib.Network(pos, n, dt, l_max=L)
     batch = W.make_batch(pos, n, dt, 64, seed=77)
-    # oracle skies on the library's delay tables (the tables themselves are
-    # checked against the oracle above)
-    tabs = [(net.delay_table(k), net.rotation_flat(k)) for k in range(3)]
-    pairs = [(1, 0), (2, 0), (2, 1)]
+    # oracle skies on the oracle's own delay tables and rotation plans
+    oplan = O.NetworkPlan(pos, n, dt, L)
     ref = np.zeros((64, (L + 1) ** 2), np.complex128)
     for s in range(64):
         F = W.full_from_half(batch["F"][:, s, :], n)
-        for k, (i, j) in enumerate(pairs):
-            ref[s] += O.baseline_integrate_power_fd(F[i], F[j], tabs[k][0], L, tabs[k][1]) / 3
-        ref[s] = O.rotate_z(ref[s], L, False, batch["gmst"][s])
-    return dict(net=net, batch=batch, ref=ref, n=n, L=L)
+        ref[s] = O.rotate_z(oplan.integrate(F), L, False, batch["gmst"][s])
+    return dict(net=net, batch=batch, ref=ref, n=n, L=L, oplan=oplan)
+
+
+def test_c1_delay_tables_and_rotations_match_oracle(lib, c1):
+    """The headline plan: 2 R_E-scale baselines at 4096 Hz built directly at
+    l_max 32 (native power l_max ~547, 297 taps), against the oracle's own
+    correlator_plan_fd_new + set_l restatement (correlator.c:424-519,
+    571-591)."""
+    net, oplan = c1["net"], c1["oplan"]
+    for k, b in enumerate(oplan.baselines):
+        assert net.baseline_l_max(k) == b["l"]
+        assert rel_l2(net.delay_table(k), b["D"]) < 1e-10, k
+        assert rel_l2(net.rotation_flat(k), b["Rot"]) < 1e-12, k
+
+
+def test_largest_uneven_bucket_delay_table_matches_oracle(lib):
+    """The largest bucket of the uneven workload: n = 16384 at 4096 Hz,
+    l_max 48, a near-diameter baseline."""
+    pos = W.random_positions(4, W.R_EARTH_S, W.rng_for(9))
+    n, dt, L = 16384, 1.0 / 4096, 48
+    net = lib.Network(pos, n, dt, l_max=L)
+    d = pos[3] - pos[0]
+    ref = O.delay_product(float(np.linalg.norm(d)), dt, n, L)
+    got = net.delay_table(3)
+    assert got.shape == ref.shape
+    assert rel_l2(got, ref) < 1e-10
+    net.close()
 
 
 # (precision, relative L2 over the whole batch, worst single sky)

@@ -2,8 +2,8 @@
 and baseline subsets of a 4-detector network in one call) against the
 FP64 oracle, per segment: the mean over the segment's own baselines of the
 oracle's correlator_baseline_integrate_power_fd at the segment's padded
-DFT length (on the library's delay tables and rotations, which other tests
-check against the oracle's own), truncated to the segment's l_max.
+DFT length (on the oracle's own delay tables and rotation plans),
+truncated to the segment's l_max.
 
 Tolerances: bf16x3 contraction, relative L2 <= 1e-5 over the batch and
 3e-5 per sky; FP64 contraction 1e-10.  Graph replay and direct launches
@@ -45,9 +45,10 @@ def oracle_skies(S, pos, batch, plan, Lplan):
     for s in range(len(batch["bucket"])):
         nb = int(batch["buckets"][batch["bucket"][s]])
         if nb not in tables:
-            net = S.Network(pos, nb, DT, l_max=Lplan)
-            tables[nb] = [(net.delay_table(k), net.rotation_flat(k), net.baseline_l_max(k)) for k in range(len(pr))]
-            net.close()
+            # the oracle's own delay tables and rotation plans, in the same
+            # baseline order (i > j, i ascending)
+            op = O.NetworkPlan(pos, nb, DT, Lplan)
+            tables[nb] = [(b["D"], b["Rot"], b["l"]) for b in op.baselines]
         Ku = nb // 2 + 1
         half = sp[plan.in_offset[s]:plan.in_offset[s] + nd * Ku].reshape(nd, Ku)
         F = W.full_from_half(half, nb)
