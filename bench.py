@@ -22,6 +22,7 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import math
 import os
 import re
 import statistics
@@ -39,6 +40,7 @@ METRIC = "sky maps/sec @ l_max=32, 3 baselines: split-prec batched vs FP64 plain
 N_SAMPLES, DT, L_MAX, N_DET = 4096, 1.0 / 4096, 32, 3
 WORKLOAD = ("c1: 3-detector network on an Earth-radius sphere (3 baselines), 1 s segments at 4096 Hz "
             "(n=4096, 2049 unique bins), l_max=32 (1089 a_lm), per-segment GMST rotation")
+CLOCK_WINDOW_S = 1.2  # seconds of timed blocks under the clock sampler
 L2_BYTES = 126 * 2 ** 20
 
 
@@ -157,6 +159,92 @@ def oracle_tables(pos):
             tables.append((O.delay_product(float(np.linalg.norm(d)), DT, N_SAMPLES, L_MAX),
                            O.rotation_plan(L_MAX, O.rot_matrix(th, ph))))
     return tables
+
+
+class ReferenceTimer:
+    """Times the reference's own C (oracle/_ref: cannon-zz/sphradiometer
+    src/lib compiled unmodified against the project's FFTW/GSL/LAL
+    stand-ins): correlator_network_integrate_power_fd + sh_series_rotate_z
+    per segment, as its correlator_validate.c:311-320 times them, one plan
+    copy (correlator_network_plan_fd_copy) per host thread.  The plan is
+    built by correlator_network_plan_fd_new at a short length and given the
+    full-length delay tables of the oracle (equal to the reference's own to
+    ~1e-14, tests/test_ref_pin.py), which skips the reference's ~2-minute
+    native-l plan build; the timed code is the reference's.
+    ``available`` is False where oracle/_ref is not built."""
+
+    def __init__(self, pos, tables, F_half, gmst):
+        from oracle import oracle as O
+        from oracle import ref as R
+        from sphradiometer_b200 import workload as W
+        self.available = R.available()
+        if not self.available:
+            return
+        self.lib = R.lib()
+        self.net = R.Network(pos, 8, DT, L_MAX)
+        self.net.set_delay_tables([t[0] for t in tables])
+        n = N_SAMPLES
+        self.full = [np.ascontiguousarray(W.full_from_half(F_half[:, s, :], n)) for s in range(min(F_half.shape[1], 64))]
+        self.gmst = np.asarray(gmst, np.float64)
+        # the reference on these tables reproduces the oracle's sky
+        chk = O.rotate_z(O.NetworkPlan(pos, n, DT, L_MAX).integrate(self.full[0]), L_MAX, False, float(self.gmst[0]))
+        got = R.rotate_z(self.net.integrate(self.full[0], L_MAX), L_MAX, False, float(self.gmst[0]))
+        assert np.linalg.norm(got - chk) <= 1e-10 * np.linalg.norm(chk), "reference plan with replaced tables disagrees"
+
+    def rate(self, budget_s: float, threads: int):
+        lib, full, gmst = self.lib, self.full, self.gmst
+        done = [0] * threads
+        stop = time.perf_counter() + budget_s
+
+        def work(tid):
+            cp = lib.ref_network_copy(self.net._p)
+            sky, out = lib.ref_series_new(L_MAX, 0), lib.ref_series_new(L_MAX, 0)
+            k = tid
+            while time.perf_counter() < stop:
+                if lib.ref_network_integrate_rotz(cp, full[k % len(full)], float(gmst[k % len(gmst)]), sky, out):
+                    raise RuntimeError("reference integration failed")
+                done[tid] += 1
+                k += threads
+            lib.ref_series_free(sky)
+            lib.ref_series_free(out)
+            lib.ref_network_copy_free(cp)
+
+        t0 = time.perf_counter()
+        ths = [threading.Thread(target=work, args=(t,)) for t in range(threads)]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        el = time.perf_counter() - t0
+        return sum(done) / el, sum(done), el
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline_rates(pos, tables, F_half, gmst, budget_s: float):
+    """The CPU baseline on all host threads and on one: the reference's own
+    C where oracle/_ref is built (kind "reference"), else the oracle's
+    restatement (kind "port")."""
+    threads = os.cpu_count() or 1
+    rt = ReferenceTimer(pos, tables, F_half, gmst)
+    if rt.available:
+        kind, what = "reference", "the reference's C (correlator_network_integrate_power_fd + sh_series_rotate_z)"
+        r, r1 = rt.rate(budget_s, threads), rt.rate(max(2.0, budget_s / 4), 1)
+    else:
+        kind, what = "port", "the C oracle (FP64 restatement)"
+        r = cpu_oracle_rate(tables, F_half, gmst, budget_s, threads)
+        r1 = cpu_oracle_rate(tables, F_half, gmst, max(2.0, budget_s / 4), 1)
+    return {"value": r[0], "unit": "maps/s", "cores": threads, "kind": kind, "value_1_core": r1[0], "cpu_model": cpu_model(),
+            "sample": f"{r[1]} skies of this workload in {r[2]:.1f} s on {threads} threads, {r1[1]} in {r1[2]:.1f} s on one; {what}, FP64"}
 
 
 def cpu_oracle_rate(net_tables, F_half, gmst, budget_s: float, threads: int):
@@ -628,21 +716,28 @@ def guarded(fn, *a, **k):
 
 
 def run_reference(args):
-    """--impl reference: the CPU oracle (FP64 restatement of the reference's
-    own CPU path) on all host cores."""
+    """--impl reference: the reference's own CPU path on all host cores --
+    its C compiled unmodified against the project's stand-ins (oracle/_ref,
+    ReferenceTimer), or the oracle's restatement of it where that build is
+    absent."""
     rank, world, _ = env_rank()
     if rank != 0:
         return 0
-    from oracle import oracle as O
     from sphradiometer_b200 import workload as W
     pos = positions()
     tables = oracle_tables(pos)
     batch = W.make_batch(pos, N_SAMPLES, DT, 64, seed=1234)
     threads = os.cpu_count() or 1
+    rt = ReferenceTimer(pos, tables, batch["F"], batch["gmst"])
+    kind = "reference" if rt.available else "port"
+    what = "the reference's C (correlator_network_integrate_power_fd + sh_series_rotate_z)" if rt.available else "the C oracle"
     rates = []
     per_step = max(2.0, min(10.0, 60.0 / max(1, args.steps + args.warmup)))
     for it in range(args.warmup + args.steps):
-        r, cnt, el = cpu_oracle_rate(tables, batch["F"], batch["gmst"], per_step, threads)
+        if rt.available:
+            r, cnt, el = rt.rate(per_step, threads)
+        else:
+            r, cnt, el = cpu_oracle_rate(tables, batch["F"], batch["gmst"], per_step, threads)
         if it >= args.warmup:
             rates.append(r)
     value = statistics.median(rates)
@@ -651,8 +746,8 @@ def run_reference(args):
         "warmup": args.warmup, "ms_per_step": 1000.0 * per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded whitened noise + chirp injections)",
         "config": {"workload": WORKLOAD, "segments_per_sample": 64},
-        "cpu_baseline": {"value": value, "unit": "maps/s", "cores": threads, "kind": "port",
-                         "sample": f"each step: {per_step:.0f} s of segments integrated by the C oracle on {threads} threads"},
+        "cpu_baseline": {"value": value, "unit": "maps/s", "cores": threads, "kind": kind, "cpu_model": cpu_model(),
+                         "sample": f"each step: {per_step:.0f} s of segments integrated by {what} on {threads} threads"},
         "e2e": {"value": value, "unit": "maps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -664,7 +759,7 @@ def run(args):
     import torch.distributed as dist
     import sphradiometer_b200 as S
     from sphradiometer_b200 import workload as W
-    from sphradiometer_b200.replicas import whole_job_rate
+    from sphradiometer_b200.replicas import max_over_ranks, whole_job_rate
 
     rank, world, local = env_rank()
     if world > 1:
@@ -704,18 +799,38 @@ def run(args):
         a_.record(st)
         b_.record(st)
     t_begin, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(dev.index) as clk:
+
+    def timed_block(record_kernels: bool) -> float:
+        # exactly K steps, barrier + synchronize on both sides, device time
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
         t_begin.record(st)
         for s in range(args.steps):
-            S.load().sphrad_batch_set_timing_events(bp._p, C.c_void_p(ev[s][0].cuda_event), C.c_void_p(ev[s][1].cuda_event))
+            if record_kernels:
+                S.load().sphrad_batch_set_timing_events(bp._p, C.c_void_p(ev[s][0].cuda_event), C.c_void_p(ev[s][1].cuda_event))
             bp.integrate(ring[s % n_ring], gm[s % n_ring], out=out)
         t_end.record(st)
         torch.cuda.synchronize()
-    S.load().sphrad_batch_set_timing_events(bp._p, None, None)
-    elapsed_ms = t_begin.elapsed_time(t_end)
+        if record_kernels:
+            S.load().sphrad_batch_set_timing_events(bp._p, None, None)
+        if world > 1:
+            dist.barrier()
+        return t_begin.elapsed_time(t_end)
+
+    # The K-step block is repeated back to back until the timed blocks span
+    # at least CLOCK_WINDOW_S, so that the clock sampler (200 ms period)
+    # sees the GPU under this load; every rank runs the same number of
+    # blocks (from the slowest rank's first block), and the reported time
+    # is the median block's, max over ranks.
+    with ClockSampler(dev.index) as clk:
+        blocks = [timed_block(True)]
+        first = max_over_ranks(blocks[0], dev)
+        n_blocks = max(1, min(2000, int(math.ceil(CLOCK_WINDOW_S * 1e3 / max(first, 1e-3)))))
+        for _ in range(n_blocks - 1):
+            blocks.append(timed_block(False))
+    per_block = [max_over_ranks(b, dev) for b in blocks] if world > 1 else blocks
+    elapsed_ms = statistics.median(per_block)
     kern_ms = [a.elapsed_time(b) for a, b in ev]
     # whole-job rate over the slowest rank's device time
     value, elapsed_ms = whole_job_rate(n_seg, args.steps, elapsed_ms, dev)
@@ -726,8 +841,9 @@ def run(args):
 
     # roofline of the contraction kernel: algorithmic bytes per launch =
     # spectra (n_det x bins x 16 B per segment) + the delay-table operand
-    # (read once per launch) + FP32 partial sums (B x accstride x 4 B per
-    # segment per split)
+    # (read once per launch); the split-K partial sums (B x accstride
+    # elements per segment and accumulation piece) are the implementation's
+    # own traffic and are reported beside it, not counted
     mean_k = statistics.mean(kern_ms) / 1e3
     accstride = ((L_MAX + 1) + 3) & ~3
     if prec == "bf16x3":
@@ -741,7 +857,8 @@ def run(args):
         ps_rows = partial_sum_rows(n_seg, -(-K // 8), bp.ctas(n_seg))
     else:
         ps_rows = split * n_seg
-    alg_bytes = N_DET * n_seg * K * 16 + d_bytes + ps_rows * 3 * accstride * acc_el
+    alg_bytes = N_DET * n_seg * K * 16 + d_bytes
+    partial_sum_bytes = ps_rows * 3 * accstride * acc_el
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / mean_k / 1e9
 
@@ -837,12 +954,8 @@ def run(args):
             extra["c3_sh_algebra"] = guarded(c3_report, S)
             extra["c4_learned_proposal"] = guarded(c4_report, S)
 
-        # CPU baseline: the oracle on the host cores, bounded sample
-        tables = oracle_tables(pos)
-        threads = os.cpu_count() or 1
-        rate, nmaps, el = cpu_oracle_rate(tables, base["F"], base["gmst"], args.cpu_seconds, threads)
-        cpu = {"value": rate, "unit": "maps/s", "cores": threads, "kind": "port",
-               "sample": f"{nmaps} skies of this workload in {el:.1f} s (C oracle, FP64, {threads} threads)"}
+        # CPU baseline on the host cores, bounded sample
+        cpu = cpu_baseline_rates(pos, oracle_tables(pos), base["F"], base["gmst"], args.cpu_seconds)
 
     if rank == 0:
         line = {
@@ -853,11 +966,14 @@ def run(args):
                        "pipeline_variant": S.load().sphrad_batch_pipeline(bp._p, n_seg),
                        "contraction_ctas": bp.ctas(n_seg) if prec.startswith("bf16") else None,
                        "l2": f"inputs larger than L2: ring of {n_ring} distinct batches, {n_ring * batch_bytes / 2**20:.0f} MiB",
+                       "timing": f"median of {len(per_block)} back-to-back timed blocks of exactly {args.steps} steps (max over ranks), "
+                                 f"clocks sampled across them",
                        "parallelism": f"replicas x{world} (segments sharded, no collective)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": profiled_traffic(n_seg), "kernel": "k_tc_contract" if prec == "bf16x3" else "k_cc_contract",
+                         "traffic": profiled_traffic(n_seg), "kernel": "k_tc_contract" if prec == "bf16x3" else "k_cc_stream",
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
-                         "algorithmic_bytes_per_launch": alg_bytes, "mean_launch_ms": mean_k * 1e3},
+                         "algorithmic_bytes_per_launch": alg_bytes, "partial_sum_bytes_per_launch": partial_sum_bytes,
+                         "mean_launch_ms": mean_k * 1e3},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": kernels * args.steps, "clocks": clk.summary(), "device_status": status,
         }
         line.update(extra)

@@ -183,6 +183,13 @@ struct sh_series_array *sh_series_array_reverse_fft(struct sh_series_array *);
 /* Library diagnostics (no reference counterpart): the message of the
  * last failure on this thread, or "" */
 const char *sphrad_b200_last_error(void);
+/* Failure-detection tests (no reference counterpart): with n > 0, the n-th
+ * next allocation the library makes -- device memory, or the host memory
+ * of the objects this interface returns -- fails as if memory had run out,
+ * once; 0 disarms.  Exercises the reference's contract that constructors
+ * and operations return NULL on failure and never abort (e.g.
+ * correlator.c:387-399). */
+int sphrad_b200_inject_allocation_failure(long n);
 
 #ifdef __cplusplus
 #undef complex

@@ -140,9 +140,20 @@ int sphrad_batch_kernels_per_call(const sphrad_batch_plan *plan);
  * integrate call records ev_begin just before and ev_end just after the
  * contraction kernel on the call's stream. */
 int sphrad_batch_set_timing_events(sphrad_batch_plan *plan, void *ev_begin, void *ev_end);
-/* 0 when no device-side wait has timed out, else the code of the wait that
- * gave up (synchronises with the device). */
+/* 0 when no device-side wait has timed out since the last call of this
+ * function, else the code of the wait that gave up; reading clears it
+ * (synchronises with the device).  A call whose wait gave up has returned
+ * with its outputs undefined; the plan stays usable. */
 int sphrad_batch_status(sphrad_batch_plan *plan);
+/* Bound of every device-side wait of the contraction kernels, in SM clock
+ * cycles (0: the default, about 2 s at the B200's clock).  Polar plans. */
+int sphrad_batch_set_wait_limit(sphrad_batch_plan *plan, unsigned long long cycles);
+/* Failure-detection hook for tests (tcgen05 plans): the spectrum producer
+ * of the contraction's first CTA skips loading stage `stage` of its range
+ * (-1: off), so the wait on that stage runs out; with a short wait limit
+ * the call returns, sphrad_batch_status reports the code, and later calls
+ * with the hook off are unaffected. */
+int sphrad_batch_test_withhold_stage(sphrad_batch_plan *plan, int stage);
 
 /* ---- time series to spectra ---------------------------------------------
  *
@@ -291,33 +302,66 @@ int sphrad_uneven_kernels_per_call(const sphrad_uneven_plan *plan);
  * Skies are device arrays [n_sky][(sky_l_max+1)^2] of double complex in
  * the reference's m-major order (what sphrad_batch_integrate writes). */
 enum {
-	SPHRAD_GRID_GL = 0,   /* Gauss-Legendre rows of the reference's meshes
-			       * (sh_series_trans.c:149-196), increasing theta */
-	SPHRAD_GRID_CELL = 1  /* theta_i = pi (i + 1/2) / ntheta */
+	SPHRAD_GRID_GL = 0,      /* Gauss-Legendre rows of the reference's meshes
+				  * (sh_series_trans.c:149-196), increasing theta */
+	SPHRAD_GRID_CELL = 1,    /* theta_i = pi (i + 1/2) / ntheta */
+	SPHRAD_GRID_HEALPIX = 2  /* HEALPix-like ring grid, RING pixel order (the
+				  * map sh_series_write_healpix_map renders,
+				  * sh_series_healpix.cc:245-286): ntheta is nside,
+				  * nphi is ignored; 4 nside - 1 iso-latitude rings,
+				  * 4i pixels on polar ring i, 4 nside in the belt,
+				  * 12 nside^2 pixels in all (Gorski et al. 2005) */
 };
 typedef struct sphrad_sky_grid sphrad_sky_grid;
 
-/* Tables for l <= l_max on the grid; columns are phi_j = 2 pi j / nphi.
- * fp32 = 1 transforms in FP32, 0 in FP64.  NULL on failure. */
+/* Tables for l <= l_max on the grid; columns are phi_j = 2 pi j / nphi
+ * (ring grids: each ring's own longitudes).  fp32 = 1 transforms in FP32,
+ * 0 in FP64.  NULL on failure. */
 sphrad_sky_grid *sphrad_sky_grid_new(unsigned l_max, int kind, int ntheta, int nphi, int fp32);
 void sphrad_sky_grid_free(sphrad_sky_grid *grid);
-/* Number of rows; their co-latitudes into theta (host, may be NULL). */
+/* Number of rows (rings); their co-latitudes into theta (host, may be
+ * NULL). */
 int sphrad_sky_grid_rows(const sphrad_sky_grid *grid, double *theta);
+/* Pixels of one rendered sky: ntheta x nphi, or 12 nside^2 for rings. */
+long long sphrad_sky_grid_pixels(const sphrad_sky_grid *grid);
+/* The reference's HEALPix resolution for a series of degree l_max
+ * (lmax2nside, sh_series_healpix.cc:220-238): the smallest power of two
+ * not below ceil(l_max / 2 + 0.75); -1 on overflow. */
+int sphrad_healpix_nside(unsigned l_max);
 /* Device scratch for n_sky skies (render and arg max). */
 size_t sphrad_sky_grid_scratch_size(const sphrad_sky_grid *grid, int n_sky);
-/* out: device float [n_sky][ntheta][nphi] = Re f of each sky truncated at
- * min(sky_l_max, the grid's l_max). */
+/* out: device float [n_sky][ntheta][nphi] (ring grids: [n_sky][12
+ * nside^2], RING order) = Re f of each sky truncated at min(sky_l_max, the
+ * grid's l_max). */
 int sphrad_sky_render(sphrad_sky_grid *grid, const void *sky, int n_sky, unsigned sky_l_max, float *out, void *scratch, size_t scratch_bytes,
 		      void *cuda_stream);
 /* Grid pixel of the largest Re f of each sky truncated at l_use: device
  * theta[n_sky], phi[n_sky] (ties go to the first pixel in row-major
- * order, as the reference's scan, sh_series_extremize.c:214-229). */
+ * order, as the reference's scan, sh_series_extremize.c:214-229).  Not on
+ * ring grids. */
 int sphrad_sky_grid_argmax(sphrad_sky_grid *grid, const void *sky, int n_sky, unsigned sky_l_max, unsigned l_use, double *theta, double *phi,
 			   void *scratch, size_t scratch_bytes, void *cuda_stream);
-/* Local maximum of Re f near (theta0, phi0), FP64 trust-region Newton
- * iterations on analytic derivatives.  out: device [n_sky][4] = theta,
- * phi, Re f there, angle moved from the start (rad); status: device
- * [n_sky], bit 0 set when converged, iteration count in the bits above. */
+/* Refinement used by the localisers below (process-wide; not thread-safe
+ * against concurrent localisation):
+ *   SPHRAD_REFINE_BFGS2 (default): the reference extremizer's minimiser,
+ *     GSL's vector_bfgs2 restated (Fletcher's line search, memoryless BFGS
+ *     directions; first step pi/24, line tolerance 0.001, <= 100
+ *     iterations, stop at |gradient| < 1e-3; sh_series_extremize.c:
+ *     314-338), with the gradient taken in the co-ordinates (theta, phi);
+ *   SPHRAD_REFINE_NEWTON: trust-region Newton steps on analytic first and
+ *     second derivatives in the local orthonormal frame.
+ * sh_series_real_minimum keeps the reference's own gradient convention
+ * (components along the unit vectors) whatever is chosen here.  Returns 0,
+ * or -1 for an unknown method. */
+enum { SPHRAD_REFINE_NEWTON = 0, SPHRAD_REFINE_BFGS2 = 1 };
+int sphrad_sky_set_refinement(int method);
+int sphrad_sky_refinement(void);
+/* Local maximum of Re f near (theta0, phi0) by the chosen refinement, FP64
+ * on analytic derivatives.  out: device [n_sky][4] = theta, phi, Re f
+ * there, angle moved from the start (rad); status: device [n_sky], bit 0
+ * set when the refinement stopped by its own test rather than at its
+ * iteration limit (BFGS2: gradient below 1e-3, or no step left that
+ * makes progress), iteration count in the bits above. */
 int sphrad_sky_refine_peaks(const void *sky, int n_sky, unsigned sky_l_max, const double *theta0, const double *phi0, double *out, int *status,
 			    void *cuda_stream);
 /* The reference's localisation applied to every sky (its extremizer on

@@ -60,6 +60,14 @@ def lib():
         L.ref_real_minimum.argtypes = [cp, u, i, C.POINTER(d), C.POINTER(d)]
         L.ref_product.argtypes = [cp, u, i, cp, u, i, u, i, cp]
         L.ref_to_mesh.argtypes = [cp, u, i, cp]
+        L.ref_network_set_delay_table.argtypes = [vp, i, i, cp]
+        L.ref_network_copy.restype = vp
+        L.ref_network_copy.argtypes = [vp]
+        L.ref_network_copy_free.argtypes = [vp]
+        L.ref_network_integrate_rotz.argtypes = [vp, cp, d, vp, vp]
+        L.ref_series_new.restype = vp
+        L.ref_series_new.argtypes = [u, i]
+        L.ref_series_free.argtypes = [vp]
         _lib = L
     return _lib
 
@@ -117,6 +125,16 @@ class Network:
         out = np.zeros(rot_len(self.baseline_l_max(k)), np.complex128)
         lib().ref_network_rotation(self._p, k, out)
         return out
+
+    def set_delay_tables(self, tables):
+        """Give every baseline the n x (l_max+1) delay table tables[k] (the
+        plan's own l_max), through the reference's own allocators; the
+        network then integrates spectra of that length."""
+        for k, D in enumerate(tables):
+            D = _c(D)
+            if lib().ref_network_set_delay_table(self._p, k, D.shape[0], D):
+                raise RuntimeError("delay table replacement failed")
+        self.n = tables[0].shape[0]
 
     def integrate(self, fseries, sky_l_max: int) -> np.ndarray:
         """correlator_network_integrate_power_fd; fseries is n_det x n."""

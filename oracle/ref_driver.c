@@ -223,3 +223,84 @@ int ref_to_mesh(const double complex *a, unsigned l_max, int polar, double compl
 	sh_series_free(s);
 	return rc;
 }
+
+/* replace baseline k's delay table by an n-row table of the plan's own
+ * l_max and polarity (sh_series_array_new + copy), and its cross-spectrum
+ * scratch by one of n entries -- the public plan fields a caller of the
+ * reference may replace (inspiral_sky_map.c:416-417 swaps delay_product);
+ * every baseline must be given the same n before integrating */
+int ref_network_set_delay_table(void *p, int k, int n, const double complex *D)
+{
+	struct ref_network *net = p;
+	struct correlator_plan_fd *plan = net->plan->plans[k];
+	struct sh_series_array *d = sh_series_array_new(n, plan->delay_product->l_max, plan->delay_product->polar);
+	double complex *fsp = malloc((size_t) n * sizeof(*fsp));
+	if(!d || !fsp) {
+		sh_series_array_free(d);
+		free(fsp);
+		return -1;
+	}
+	const size_t len = sh_series_length(d->l_max, d->polar);
+	for(int i = 0; i < n; i++)
+		memcpy(d->series[i].coeff, D + (size_t) i * len, len * sizeof(*D));
+	sh_series_array_free(plan->delay_product);
+	free(plan->fseries_product);
+	plan->delay_product = d;
+	plan->fseries_product = fsp;
+	net->n = n;
+	return 0;
+}
+
+/* an independent copy of the network's plan (correlator_network_plan_fd_copy:
+ * own scratch, shared baselines), for use on another thread */
+void *ref_network_copy(void *p)
+{
+	struct ref_network *net = p, *c = calloc(1, sizeof(*c));
+	if(!c)
+		return NULL;
+	*c = *net;
+	c->instruments = NULL;	/* borrowed from net */
+	c->baselines = NULL;
+	c->plan = correlator_network_plan_fd_copy(net->plan);
+	if(!c->plan) {
+		free(c);
+		return NULL;
+	}
+	return c;
+}
+
+/* frees a copy made by ref_network_copy (its plan only) */
+void ref_network_copy_free(void *p)
+{
+	struct ref_network *c = p;
+	if(c)
+		correlator_network_plan_fd_free(c->plan);
+	free(c);
+}
+
+/* one segment as the reference's callers time it (correlator_validate.c:
+ * 311-320): correlator_network_integrate_power_fd into sky, then
+ * sh_series_rotate_z by the GMST into out; sky and out are caller-made
+ * non-polar series of degree sky_l_max (sh_series_new) */
+int ref_network_integrate_rotz(void *p, const double complex *fseries, double gmst, void *sky, void *out)
+{
+	struct ref_network *net = p;
+	double complex *f[8];
+	if(net->n_det > 8)
+		return -1;
+	for(int i = 0; i < net->n_det; i++)
+		f[i] = (double complex *) fseries + (size_t) i * net->n;
+	if(!correlator_network_integrate_power_fd(sky, f, net->plan))
+		return -1;
+	return sh_series_rotate_z(out, sky, gmst) ? 0 : -1;
+}
+
+void *ref_series_new(unsigned l_max, int polar)
+{
+	return sh_series_new(l_max, polar);
+}
+
+void ref_series_free(void *s)
+{
+	sh_series_free(s);
+}

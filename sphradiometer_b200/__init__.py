@@ -416,6 +416,7 @@ class BatchPlan:
 
 GRID_GL = 0
 GRID_CELL = 1
+GRID_HEALPIX = 2
 
 
 class FseriesPlan:
@@ -485,21 +486,26 @@ class FseriesPlan:
 class SkyGrid:
     """Batched inverse SHT onto a theta x phi grid (sphrad_sky_grid_*).
 
-    ``kind``: "gl" (the reference's Gauss-Legendre mesh rows) or "cell"
-    (theta_i = pi (i + 1/2) / ntheta); columns phi_j = 2 pi j / nphi.
-    ``render(sky)``: sky a complex128 CUDA tensor [n_sky][(L+1)^2] -> float32
-    [n_sky][ntheta][nphi] = Re f.  ``argmax(sky, l_use)`` -> (theta, phi)
-    float64 CUDA tensors of each sky's best pixel.
+    ``kind``: "gl" (the reference's Gauss-Legendre mesh rows), "cell"
+    (theta_i = pi (i + 1/2) / ntheta), columns phi_j = 2 pi j / nphi; or
+    "healpix" (ntheta = nside, nphi ignored: 4 nside - 1 rings, 12 nside^2
+    pixels in RING order).  ``render(sky)``: sky a complex128 CUDA tensor
+    [n_sky][(L+1)^2] -> float32 [n_sky][ntheta][nphi] (healpix: [n_sky][12
+    nside^2]) = Re f.  ``argmax(sky, l_use)`` -> (theta, phi) float64 CUDA
+    tensors of each sky's best pixel (not on healpix grids).
     """
 
-    def __init__(self, l_max: int, ntheta: int, nphi: int, kind: str = "cell", fp32: bool = True):
+    def __init__(self, l_max: int, ntheta: int, nphi: int = 0, kind: str = "cell", fp32: bool = True):
         self.l_max, self.ntheta, self.nphi = int(l_max), int(ntheta), int(nphi)
-        k = GRID_GL if kind == "gl" else GRID_CELL
+        self.kind = kind
+        k = {"gl": GRID_GL, "cell": GRID_CELL, "healpix": GRID_HEALPIX}[kind]
         self._g = _check(load().sphrad_sky_grid_new(self.l_max, k, self.ntheta, self.nphi, 1 if fp32 else 0), "sphrad_sky_grid_new")
+        self.n_rows = load().sphrad_sky_grid_rows(self._g, None)
+        self.n_pixels = load().sphrad_sky_grid_pixels(self._g)
         self._scratch = None
 
     def rows(self) -> np.ndarray:
-        th = np.empty(self.ntheta, np.float64)
+        th = np.empty(self.n_rows, np.float64)
         load().sphrad_sky_grid_rows(self._g, th.ctypes.data)
         return th
 
@@ -521,7 +527,8 @@ class SkyGrid:
         assert sky.is_cuda and sky.dtype == torch.complex128 and sky.is_contiguous()
         n = sky.shape[0]
         if out is None:
-            out = torch.empty((n, self.ntheta, self.nphi), dtype=torch.float32, device=sky.device)
+            shape = (n, self.n_pixels) if self.kind == "healpix" else (n, self.ntheta, self.nphi)
+            out = torch.empty(shape, dtype=torch.float32, device=sky.device)
         scr = self._scr(n)
         rc = load().sphrad_sky_render(self._g, sky.data_ptr(), n, self._sky_l(sky), out.data_ptr(), scr.data_ptr(), scr.numel(),
                                       torch.cuda.current_stream().cuda_stream)

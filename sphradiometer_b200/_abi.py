@@ -89,6 +89,7 @@ _u, _i, _d, _ll, _sz = C.c_uint, C.c_int, C.c_double, C.c_longlong, C.c_size_t
 # name: (restype, argtypes)
 SIGNATURES = {
     "sphrad_b200_last_error": (C.c_char_p, []),
+    "sphrad_b200_inject_allocation_failure": (_i, [C.c_long]),
     # sh_series basics
     "sh_series_new": (_P(sh_series), [_u, _i]),
     "sh_series_new_zero": (_P(sh_series), [_u, _i]),
@@ -205,6 +206,8 @@ SIGNATURES = {
     "sphrad_batch_tseries_workspace_size": (_sz, [_vp, _i]),
     "sphrad_batch_integrate_tseries": (_i, [_vp, _vp, _vp, _i, _ll, _vp, _vp, _vp, _sz, _vp]),
     "sphrad_batch_status": (_i, [_vp]),
+    "sphrad_batch_set_wait_limit": (_i, [_vp, C.c_ulonglong]),
+    "sphrad_batch_test_withhold_stage": (_i, [_vp, _i]),
     "sphrad_batch_set_timing_events": (_i, [_vp, _vp, _vp]),
     "sphrad_batch_integrate_noalloc": (_i, [_vp, _vp, _i, _ll, _vp, _vp, _vp]),
     "sphrad_batch_integrate_weighted": (_i, [_vp, _vp, _i, _ll, _vp, _vp, _vp, _sz, _vp, _i, _vp]),
@@ -221,11 +224,15 @@ SIGNATURES = {
     "sphrad_sky_grid_new": (_vp, [_u, _i, _i, _i, _i]),
     "sphrad_sky_grid_free": (None, [_vp]),
     "sphrad_sky_grid_rows": (_i, [_vp, _vp]),
+    "sphrad_sky_grid_pixels": (C.c_longlong, [_vp]),
+    "sphrad_healpix_nside": (_i, [_u]),
     "sphrad_sky_grid_scratch_size": (_sz, [_vp, _i]),
     "sphrad_sky_render": (_i, [_vp, _vp, _i, _u, _vp, _vp, _sz, _vp]),
     "sphrad_sky_grid_argmax": (_i, [_vp, _vp, _i, _u, _u, _vp, _vp, _vp, _sz, _vp]),
     "sphrad_sky_refine_peaks": (_i, [_vp, _i, _u, _vp, _vp, _vp, _vp, _vp]),
     "sphrad_sky_peaks": (_i, [_vp, _i, _u, _vp, _vp, _vp]),
+    "sphrad_sky_set_refinement": (_i, [_i]),
+    "sphrad_sky_refinement": (_i, []),
     "sphrad_sh_rotate_batch_scratch_size": (_sz, [_u, _i]),
     "sphrad_sh_rotate_batch": (_i, [_vp, _i, _u, _i, _vp, _vp, _i, _vp, _sz, _vp]),
     "sphrad_sh_product_grid_new": (_vp, [_u, _u, _u, _i]),

@@ -59,4 +59,10 @@ void gl_nodes(int n, double *x, double *w);
 // Wigner 3-j symbols for integer arguments
 double wigner_3j(int j1, int j2, int j3, int m1, int m2, int m3);
 
+// host allocations of the C-ABI objects, subject to the allocation-failure
+// injection of set_alloc_fault()
+inline void *xmalloc(size_t n) { return alloc_fault_due() ? nullptr : malloc(n); }
+inline void *xcalloc(size_t n, size_t m) { return alloc_fault_due() ? nullptr : calloc(n, m); }
+inline void *xrealloc(void *p, size_t n) { return alloc_fault_due() ? nullptr : realloc(p, n); }
+
 }  // namespace sphrad

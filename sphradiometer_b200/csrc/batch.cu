@@ -98,6 +98,8 @@ struct TcArgs {
 	int reps;
 	size_t rep_stride;     // floats per copy (S B accstride)
 	unsigned *err;
+	unsigned long long wait;  // bound of every wait, clock cycles
+	int hold;              // failure-detection tests: stage of CTA 0's range whose spectra are never loaded (-1: none)
 };
 
 // Split the complex value (re, im) into NPART packed bf16x2 words (re in the
@@ -168,7 +170,10 @@ template <int NPART, int NFS, int NABS, int NBS, bool ATM>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_constant__ CUtensorMap tmF, const __grid_constant__ TcArgs a)
 {
 	extern __shared__ uint8_t smem_raw[];
-	uint8_t *smem = (uint8_t *) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
+	// aligned by an offset on the shared array itself, so that accesses
+	// through it stay shared-memory accesses (an integer round trip would
+	// make them generic)
+	uint8_t *smem = smem_raw + ((1024 - ((uintptr_t) smem_raw & 1023)) & 1023);
 	const int f_slab = TM * 128;
 	const int f_stage = a.n_det * f_slab;
 	const int btile = a.npad * KE * 2;
@@ -233,15 +238,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 				const int u = u0 + it;
 				const int fs = it % NFS;
 				const uint32_t fph = (it / NFS) & 1;
-				if(!mbar_wait(smem_u32(&f_empty[fs]), fph ^ 1, abort_flag, a.err, 1))
+				if(!mbar_wait(smem_u32(&f_empty[fs]), fph ^ 1, abort_flag, a.err, 1, a.wait))
 					break;
+				if(it == a.hold && blockIdx.x == 0) {
+					// withheld on request: the stage's barrier never
+					// completes, so the converters' wait on it runs out
+					issued = it + 1;
+					continue;
+				}
 				mbar_arrive_tx(smem_u32(&f_full[fs]), f_stage);
 				tma_load_3d(smem_u32(sF + fs * f_stage), &tmF, smem_u32(&f_full[fs]), (u % a.Kst) * 2 * KB, (u / a.Kst) * TM, 0);
 				issued = it + 1;
 			}
 			// drain the loads that may still be in flight
 			for(int it = (issued > NFS ? issued - NFS : 0); it < issued; it++)
-				mbar_drain(smem_u32(&f_full[it % NFS]), (it / NFS) & 1);
+				mbar_drain(smem_u32(&f_full[it % NFS]), (it / NFS) & 1, a.wait);
 		}
 	} else if(warp == 1) {
 		// ---------------- MMA issuer ----------------
@@ -263,11 +274,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 				const uint32_t bph = (it / NBS) & 1;
 				// a new piece overwrites the accumulators: the epilogue warps
 				// must have read the previous piece out
-				if(first && piece > 0 && !mbar_wait(smem_u32(acc_empty), (piece - 1) & 1, abort_flag, a.err, 8))
+				if(first && piece > 0 && !mbar_wait(smem_u32(acc_empty), (piece - 1) & 1, abort_flag, a.err, 8, a.wait))
 					break;
-				if(!mbar_wait(smem_u32(&ab_full[as]), aph, abort_flag, a.err, 3))
+				if(!mbar_wait(smem_u32(&ab_full[as]), aph, abort_flag, a.err, 3, a.wait))
 					break;
-				if(!mbar_wait(smem_u32(&b_full[bs]), bph, abort_flag, a.err, 4))
+				if(!mbar_wait(smem_u32(&b_full[bs]), bph, abort_flag, a.err, 4, a.wait))
 					break;
 				tc_fence_after();
 				for(int b = 0; b < a.B; b++) {
@@ -295,7 +306,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			}
 			// nothing may still write TMEM when it is released
 			umma_commit(smem_u32(mma_done));
-			mbar_drain(smem_u32(mma_done), 0);
+			mbar_drain(smem_u32(mma_done), 0, a.wait);
 		}
 	} else if(warp == TC_THREADS / 32 - 1) {
 		// ---------------- producer: delay-table operand ----------------
@@ -304,14 +315,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			int issued = 0;
 			for(int it = 0; it < nst; it++) {
 				const int bs = it % NBS;
-				if(!mbar_wait(smem_u32(&b_empty[bs]), ((it / NBS) & 1) ^ 1, abort_flag, a.err, 2))
+				if(!mbar_wait(smem_u32(&b_empty[bs]), ((it / NBS) & 1) ^ 1, abort_flag, a.err, 2, a.wait))
 					break;
 				mbar_arrive_tx(smem_u32(&b_full[bs]), ab_bytes);
 				bulk_g2s(smem_u32(sB + bs * ab_bytes), a.bops + (size_t) ((u0 + it) % a.Kst) * ab_bytes, ab_bytes, smem_u32(&b_full[bs]));
 				issued = it + 1;
 			}
 			for(int it = (issued > NBS ? issued - NBS : 0); it < issued; it++)
-				mbar_drain(smem_u32(&b_full[it % NBS]), (it / NBS) & 1);
+				mbar_drain(smem_u32(&b_full[it % NBS]), (it / NBS) & 1, a.wait);
 		}
 	} else {
 		// ---------------- converters, and the epilogue of every piece ----------------
@@ -331,7 +342,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			pc.step(u0 + it, first, last);
 			const int fs = it % NFS;
 			const uint32_t fph = (it / NFS) & 1;
-			const bool okf = mbar_wait(smem_u32(&f_full[fs]), fph, abort_flag, a.err, 5);
+			const bool okf = mbar_wait(smem_u32(&f_full[fs]), fph, abort_flag, a.err, 5, a.wait);
 			if(!__all_sync(0xffffffffu, okf))
 				break;
 			// this thread's bins of every detector, rounded to FP32
@@ -354,7 +365,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 				mbar_arrive(smem_u32(&f_empty[fs]));
 			const int as = it % NABS;
 			const uint32_t aph = (it / NABS) & 1;
-			const bool oke = mbar_wait(smem_u32(&ab_empty[as]), aph ^ 1, abort_flag, a.err, 6);
+			const bool oke = mbar_wait(smem_u32(&ab_empty[as]), aph ^ 1, abort_flag, a.err, 6, a.wait);
 			if(!__all_sync(0xffffffffu, oke))
 				break;
 			if constexpr(ATM)
@@ -397,7 +408,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			// epilogue of the piece: TMEM -> registers -> FP32 atomics into
 			// the workspace.  Warps w and w + 4 share TMEM lane quarter
 			// w % 4 and split the baselines between them.
-			const bool got = mbar_wait(smem_u32(acc_full), piece & 1, abort_flag, a.err, 7);
+			const bool got = mbar_wait(smem_u32(acc_full), piece & 1, abort_flag, a.err, 7, a.wait);
 			tc_fence_after();
 			if(!__all_sync(0xffffffffu, got))
 				break;
@@ -554,6 +565,253 @@ __global__ void k_cc_contract(const __grid_constant__ CcArgs c)
 		for(int s = 0; s < CC_TS; s++)
 			if(s0 + s < c.S)
 				atomicAdd(&out[((size_t) (s0 + s) * c.B + b) * c.accstride + l], acc[s]);
+	}
+}
+
+// ------------------------------------------------------------------------
+// CUDA-core contraction, streamed (FP32 or FP64), up to 3 detectors
+// ------------------------------------------------------------------------
+// The tcgen05 path's spectrum stream (TMA boxes of 8 bins x 128 segments x
+// every detector, 128B swizzle, the same stream-K cut of (tile, stage)
+// units over the CTAs) feeding CUDA-core FMAs:
+//   warp 0          TMA producer of the spectra ring (NFS stages);
+//   warp 1          bulk-copy producer of the delay-table ring: per stage
+//                   a [KE][B][NPL] block of T (row 2k: w_k Re D, row 2k+1:
+//                   -w_k Im D, l zero-padded to NPL = 12 G), L2-resident;
+//   warps 2 ..      compute warps, one per (baseline b, l-group g of 12):
+//                   each stage they first form together X_b = F_j conj(F_i)
+//                   in FP64 for all 128 rows x 8 bins of every baseline
+//                   into a double-buffered operand sA[b][k][row] of T, meet
+//                   at a bounded mbarrier, then thread (lane) accumulates
+//                   rows 4 lane .. 4 lane + 3 x l 12 g .. 12 g + 11 of
+//                   baseline b: per k one vector load of 4 X values and
+//                   three (FP64: six) broadcast vector loads of 12 D values
+//                   for 48 FMAs.
+// Partial sums leave at the end of each piece (the part of the CTA's range
+// inside one tile) by atomics into the split-K workspace [S][B][accstride].
+constexpr int CCS_LG = 12;  // l per compute warp
+
+struct CcsArgs {
+	int S, n_det, B, Kst, tiles, G, accstride;
+	int bi[3], bj[3];
+	const void *dops;  // [Kst][KE][B][NPL] T
+	void *acc;         // [S][B][accstride] T
+	unsigned *err;
+	unsigned long long wait;  // bound of every wait, clock cycles
+};
+
+template <class T, int NFS, int NWMAX>
+__global__ void __launch_bounds__(32 * (2 + NWMAX), 1) k_cc_stream(const __grid_constant__ CUtensorMap tmF, const __grid_constant__ CcsArgs a)
+{
+	extern __shared__ uint8_t smem_raw[];
+	// aligned by an offset on the shared array itself, so that accesses
+	// through it stay shared-memory accesses (an integer round trip would
+	// make them generic)
+	uint8_t *smem = smem_raw + ((1024 - ((uintptr_t) smem_raw & 1023)) & 1023);
+	constexpr int NDS = 2;  // delay-table ring depth
+	const int NW = a.B * a.G;
+	const int NPL = a.G * CCS_LG;
+	const int f_slab = TM * 128;
+	const int f_stage = a.n_det * f_slab;
+	const int a_stage = a.B * KE * TM;                 // elements of T
+	const int d_stage = KE * a.B * NPL;                // elements of T
+	uint8_t *sF = smem;
+	T *sA = (T *) (sF + NFS * f_stage);                // [2][B][KE][TM]
+	T *sD = sA + 2 * a_stage;                          // [NDS][KE][B][NPL]
+	uint64_t *bars = (uint64_t *) (sD + NDS * d_stage);  // 16-byte aligned: d_stage * sizeof(T) is
+	uint64_t *f_full = bars;
+	uint64_t *f_empty = f_full + NFS;
+	uint64_t *d_full = f_empty + NFS;
+	uint64_t *d_empty = d_full + NDS;
+	uint64_t *x_ready = d_empty + NDS;                 // [2] the operand of a stage is complete
+	volatile int *abort_flag = (volatile int *) (x_ready + 2);
+
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const long long units = (long long) a.tiles * a.Kst;
+	const int u0 = (int) (units * blockIdx.x / gridDim.x);
+	const int u1 = (int) (units * (blockIdx.x + 1) / gridDim.x);
+	const int nst = u1 - u0;
+
+	if(threadIdx.x == 0) {
+		for(int i = 0; i < NFS; i++) {
+			mbar_init(smem_u32(&f_full[i]), 1);
+			mbar_init(smem_u32(&f_empty[i]), NW);
+		}
+		for(int i = 0; i < NDS; i++) {
+			mbar_init(smem_u32(&d_full[i]), 1);
+			mbar_init(smem_u32(&d_empty[i]), NW);
+		}
+		for(int i = 0; i < 2; i++)
+			mbar_init(smem_u32(&x_ready[i]), NW);
+		*abort_flag = 0;
+		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+	}
+	__syncthreads();
+
+	if(warp == 0) {
+		if(lane == 0) {
+			int issued = 0;
+			for(int it = 0; it < nst; it++) {
+				const int u = u0 + it;
+				const int fs = it % NFS;
+				if(!mbar_wait(smem_u32(&f_empty[fs]), ((it / NFS) & 1) ^ 1, abort_flag, a.err, 11, a.wait))
+					break;
+				mbar_arrive_tx(smem_u32(&f_full[fs]), f_stage);
+				tma_load_3d(smem_u32(sF + fs * f_stage), &tmF, smem_u32(&f_full[fs]), (u % a.Kst) * 2 * KB, (u / a.Kst) * TM, 0);
+				issued = it + 1;
+			}
+			for(int it = (issued > NFS ? issued - NFS : 0); it < issued; it++)
+				mbar_drain(smem_u32(&f_full[it % NFS]), (it / NFS) & 1, a.wait);
+		}
+		return;
+	}
+	if(warp == 1) {
+		if(lane == 0) {
+			const uint32_t bytes = (uint32_t) (d_stage * sizeof(T));
+			int issued = 0;
+			for(int it = 0; it < nst; it++) {
+				const int ds = it % NDS;
+				if(!mbar_wait(smem_u32(&d_empty[ds]), ((it / NDS) & 1) ^ 1, abort_flag, a.err, 12, a.wait))
+					break;
+				mbar_arrive_tx(smem_u32(&d_full[ds]), bytes);
+				bulk_g2s(smem_u32(sD + ds * d_stage), (const T *) a.dops + (size_t) ((u0 + it) % a.Kst) * d_stage, bytes, smem_u32(&d_full[ds]));
+				issued = it + 1;
+			}
+			for(int it = (issued > NDS ? issued - NDS : 0); it < issued; it++)
+				mbar_drain(smem_u32(&d_full[it % NDS]), (it / NDS) & 1, a.wait);
+		}
+		return;
+	}
+	const int cw = warp - 2;
+	if(cw >= NW)
+		return;
+	const int ctid = cw * 32 + lane, nct = NW * 32;
+	const int b = cw / a.G, g = cw % a.G;
+	const int l0 = g * CCS_LG;
+	T acc[4][CCS_LG];
+#pragma unroll
+	for(int r = 0; r < 4; r++)
+#pragma unroll
+		for(int j = 0; j < CCS_LG; j++)
+			acc[r][j] = 0;
+	int cur_tile = u0 / a.Kst;
+	for(int it = 0; it < nst; it++) {
+		const int u = u0 + it;
+		const int fs = it % NFS;
+		const int xb = it & 1;
+		// ---- form X of every baseline for this stage ----
+		const bool okf = mbar_wait(smem_u32(&f_full[fs]), (it / NFS) & 1, abort_flag, a.err, 13, a.wait);
+		if(!__all_sync(0xffffffffu, okf))
+			break;
+		T *xa = sA + xb * a_stage;
+		for(int p = ctid; p < TM * KB; p += nct) {
+			const int r = p & (TM - 1), c = p >> 7;
+			const uint8_t *base = sF + fs * f_stage + r * 128 + ((c ^ (r & 7)) << 4);
+			double2 f[3];
+#pragma unroll
+			for(int d = 0; d < 3; d++)
+				f[d] = d < a.n_det ? *(const double2 *) (base + d * f_slab) : make_double2(0, 0);
+#pragma unroll
+			for(int bb = 0; bb < 3; bb++) {
+				if(bb >= a.B)
+					break;
+				const int ia = a.bi[bb], ib = a.bj[bb];
+				const double2 fa = ia == 0 ? f[0] : (ia == 1 ? f[1] : f[2]);
+				const double2 fb = ib == 0 ? f[0] : (ib == 1 ? f[1] : f[2]);
+				xa[(bb * KE + 2 * c) * TM + r] = (T) fma(fb.x, fa.x, fb.y * fa.y);
+				xa[(bb * KE + 2 * c + 1) * TM + r] = (T) fma(fb.y, fa.x, -fb.x * fa.y);
+			}
+		}
+		__syncwarp();
+		if(lane == 0) {
+			mbar_arrive(smem_u32(&f_empty[fs]));
+			mbar_arrive(smem_u32(&x_ready[xb]));
+		}
+		const bool okx = mbar_wait(smem_u32(&x_ready[xb]), (it >> 1) & 1, abort_flag, a.err, 14, a.wait);
+		const int ds = it % NDS;
+		const bool okd = okx && mbar_wait(smem_u32(&d_full[ds]), (it / NDS) & 1, abort_flag, a.err, 15, a.wait);
+		if(!__all_sync(0xffffffffu, okd))
+			break;
+		// ---- accumulate ----
+		const T *ap = xa + (size_t) b * KE * TM + 4 * lane;
+		const T *dp = sD + ds * d_stage + b * NPL + l0;
+#pragma unroll 2
+		for(int k = 0; k < KE; k++) {
+			T x[4], dv[CCS_LG];
+			if constexpr(sizeof(T) == 4) {
+				const float4 v = *(const float4 *) (ap + k * TM);
+				x[0] = v.x, x[1] = v.y, x[2] = v.z, x[3] = v.w;
+#pragma unroll
+				for(int q = 0; q < CCS_LG / 4; q++) {
+					const float4 w = *(const float4 *) (dp + k * a.B * NPL + 4 * q);
+					dv[4 * q] = w.x, dv[4 * q + 1] = w.y, dv[4 * q + 2] = w.z, dv[4 * q + 3] = w.w;
+				}
+			} else {
+				const double2 v0 = *(const double2 *) (ap + k * TM), v1 = *(const double2 *) (ap + k * TM + 2);
+				x[0] = v0.x, x[1] = v0.y, x[2] = v1.x, x[3] = v1.y;
+#pragma unroll
+				for(int q = 0; q < CCS_LG / 2; q++) {
+					const double2 w = *(const double2 *) (dp + k * a.B * NPL + 2 * q);
+					dv[2 * q] = w.x, dv[2 * q + 1] = w.y;
+				}
+			}
+#pragma unroll
+			for(int r = 0; r < 4; r++)
+#pragma unroll
+				for(int j = 0; j < CCS_LG; j++)
+					acc[r][j] = fma(x[r], dv[j], acc[r][j]);
+		}
+		__syncwarp();
+		if(lane == 0)
+			mbar_arrive(smem_u32(&d_empty[ds]));
+		// ---- flush at the end of the range's part in this tile ----
+		const bool last = (u + 1 == u1) || ((u + 1) % a.Kst == 0);
+		if(last) {
+			const int tile = cur_tile;
+			cur_tile = (u + 1) / a.Kst;
+#pragma unroll
+			for(int r = 0; r < 4; r++) {
+				const int s = tile * TM + 4 * lane + r;
+				if(s < a.S) {
+					T *dst = (T *) a.acc + ((size_t) s * a.B + b) * a.accstride + l0;
+#pragma unroll
+					for(int q = 0; q < CCS_LG / 4; q++) {
+						if(l0 + 4 * q >= a.accstride)
+							break;
+						if constexpr(sizeof(T) == 4)
+							atomicAdd((float4 *) (dst + 4 * q), make_float4(acc[r][4 * q], acc[r][4 * q + 1], acc[r][4 * q + 2], acc[r][4 * q + 3]));
+						else
+#pragma unroll
+							for(int j = 0; j < 4; j++)
+								atomicAdd((double *) dst + 4 * q + j, (double) acc[r][4 * q + j]);
+					}
+				}
+#pragma unroll
+				for(int j = 0; j < CCS_LG; j++)
+					acc[r][j] = 0;
+			}
+		}
+	}
+}
+
+// delay-table operand of k_cc_stream: stage st, real k kk (bin st*KB + kk/2,
+// re/im = kk%2), baseline b, l (zero beyond Lp1 and Ku)
+template <class T>
+__global__ void k_build_dops(int Kst, int B, int NPL, int Lp1, int Ku, const double2 *Dt, T *dops)
+{
+	const long long total = (long long) Kst * KE * B * NPL;
+	for(long long idx = blockIdx.x * (long long) blockDim.x + threadIdx.x; idx < total; idx += (long long) gridDim.x * blockDim.x) {
+		const int l = idx % NPL;
+		const int b = (idx / NPL) % B;
+		const int kk = (idx / ((long long) NPL * B)) % KE;
+		const int st = idx / ((long long) NPL * B * KE);
+		const int bin = st * KB + kk / 2;
+		double v = 0.0;
+		if(l < Lp1 && bin < Ku) {
+			const double2 d = Dt[((size_t) bin * B + b) * Lp1 + l];
+			v = (kk & 1) ? -d.y : d.x;
+		}
+		dops[idx] = (T) v;
 	}
 }
 
@@ -738,6 +996,8 @@ struct BatchPlan {
 	// device tables
 	void *Dt = nullptr;        // [Ku][B][Lp1] complex (T of the CUDA-core path)
 	uint8_t *bops = nullptr;   // tcgen05 operand table
+	void *dops = nullptr;      // streamed CUDA-core operand table [Kst][KE][B][12 ccG] (T), or null
+	int ccG = 0;               // l-groups of 12 of the streamed CUDA-core path
 	int Kst = 0, npad = 0, tmem_cols = 0;
 	int npart = 2, nf = NF, nab = 3, nb = 5;  // bf16 parts per operand; spectrum, X-operand and D-operand ring depths
 	void *W = nullptr;         // [B][nq] complex T
@@ -754,6 +1014,10 @@ struct BatchPlan {
 	std::map<int, int> ctas;
 	std::map<int, int> pipe;
 	int nf0 = NF, nab0 = 4;
+	// bound of the device-side waits (0: kWaitCycles, about 2 s) and the
+	// failure-detection hook (a stage of CTA 0 whose spectra are withheld)
+	unsigned long long wait_limit = 0;
+	int hold_stage = -1;
 	// optional CUDA events recorded around the contraction kernel
 	cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
 	int last_kernels = 0;
@@ -783,6 +1047,26 @@ static PFN_cuTensorMapEncodeTiled_v12000 get_encode()
 
 static bool is_tc(int precision) { return precision == kPrecBF16x3 || precision == kPrecBF16x6; }
 
+// paths that stream (tile, stage) units through TMA with a CTA count:
+// tcgen05, and the streamed CUDA-core contraction (FP32 / FP64, <= 3
+// detectors)
+static bool is_stream(const BatchPlan *P) { return is_tc(P->precision) || P->dops != nullptr; }
+
+constexpr int CCS_NWMAX_F32 = 15;  // compute warps: l_max <= 59 with 3 baselines
+constexpr int CCS_NWMAX_F64 = 9;   // l_max <= 35 with 3 baselines
+constexpr int CCS_NFS_F32 = 3, CCS_NFS_F64 = 2;
+
+static size_t ccs_smem_bytes(const BatchPlan &P)
+{
+	const bool dbl = P.precision == kPrecFP64;
+	const size_t el = dbl ? sizeof(double) : sizeof(float);
+	const size_t f = (size_t) (dbl ? CCS_NFS_F64 : CCS_NFS_F32) * P.n_det * TM * 128;
+	const size_t aa = (size_t) 2 * P.B * KE * TM * el;
+	const size_t dd = (size_t) 2 * KE * P.B * P.ccG * CCS_LG * el;
+	const size_t bars = 8 * (2 * CCS_NFS_F32 + 2 * 2 + 2) + 16;
+	return 1024 + f + aa + dd + 8 + bars;
+}
+
 static size_t tc_smem_bytes(const BatchPlan &P, bool x_in_tmem = false)
 {
 	const size_t f = (size_t) P.nf * P.n_det * TM * 128;
@@ -800,6 +1084,7 @@ void batch_plan_destroy(void *pp)
 		return;
 	dfree(P->Dt);
 	dfree(P->bops);
+	dfree(P->dops);
 	dfree(P->W);
 	dfree(P->lq);
 	dfree(P->mq);
@@ -985,6 +1270,39 @@ void *batch_plan_create(const BatchPlanDesc &d, int precision)
 			}
 		}
 	}
+	if(!fail && !is_tc(precision) && d.n_det <= 3 && B <= 3 && get_encode()) {
+		// the streamed CUDA-core contraction, where its compute warps
+		// (baselines x l-groups of 12) fit the kernel
+		const int G = (Lp1 + CCS_LG - 1) / CCS_LG;
+		if(B * G <= (dbl ? CCS_NWMAX_F64 : CCS_NWMAX_F32)) {
+			P->Kst = (Ku + KB - 1) / KB;
+			P->ccG = G;
+			void *Dt64 = nullptr;
+			up(&Dt64, Dt.data(), Dt.size() * sizeof(double));
+			const size_t nel = (size_t) P->Kst * KE * B * G * CCS_LG;
+			P->dops = dmalloc(nel * (dbl ? sizeof(double) : sizeof(float)));
+			if(!fail && P->dops) {
+				if(dbl)
+					k_build_dops<double><<<512, 256, 0, (cudaStream_t) lib_stream()>>>(P->Kst, B, G * CCS_LG, Lp1, Ku, (const double2 *) Dt64, (double *) P->dops);
+				else
+					k_build_dops<float><<<512, 256, 0, (cudaStream_t) lib_stream()>>>(P->Kst, B, G * CCS_LG, Lp1, Ku, (const double2 *) Dt64, (float *) P->dops);
+				if(cudaGetLastError() != cudaSuccess)
+					fail = true;
+			} else
+				fail = true;
+			if(stream_sync())
+				fail = true;
+			dfree(Dt64);
+			cudaError_t ra = dbl ? cudaFuncSetAttribute(k_cc_stream<double, CCS_NFS_F64, CCS_NWMAX_F64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024)
+					     : cudaFuncSetAttribute(k_cc_stream<float, CCS_NFS_F32, CCS_NWMAX_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+			if(!fail && (ccs_smem_bytes(*P) > 227 * 1024 || ra != cudaSuccess)) {
+				// the tiled CUDA-core kernel serves this plan instead
+				dfree(P->dops);
+				P->dops = nullptr;
+				P->ccG = 0;
+			}
+		}
+	}
 	if(!fail && stream_sync())
 		fail = true;
 	if(fail) {
@@ -1041,7 +1359,7 @@ int batch_pick_split(const void *pp, int S)
 	if(it != P->split.end())
 		return it->second;
 	const int sms = sm_count();
-	if(is_tc(P->precision)) {
+	if(is_stream(P)) {
 		// stages per CTA in units of a tile's stages, rounded
 		const int tiles = (S + TM - 1) / TM;
 		const int ks = (batch_pick_ctas(P, S) + tiles / 2) / tiles;
@@ -1073,8 +1391,8 @@ int batch_set_split(void *pp, int S, int ks)
 int batch_set_ctas(void *pp, int S, int ctas)
 {
 	BatchPlan *P = (BatchPlan *) pp;
-	if(!is_tc(P->precision)) {
-		set_error("batch_set_ctas: only the tcgen05 paths take a CTA count");
+	if(!is_stream(P)) {
+		set_error("batch_set_ctas: only the streamed paths (tcgen05, and FP32/FP64 for up to 3 detectors) take a CTA count");
 		return -1;
 	}
 	if(ctas <= 0) {
@@ -1086,6 +1404,29 @@ int batch_set_ctas(void *pp, int S, int ctas)
 		P->ctas[S] = ctas;
 		P->split[S] = ks > 0 ? ks : 1;
 	}
+	return 0;
+}
+
+// tensor map of the spectra [n_det][S][ld] (FP64 pairs): boxes of 8 bins x
+// 128 segments x every detector, 128B swizzle, zero fill past the edges
+static int ensure_tmap(BatchPlan *P, const void *F, int S, long long ld)
+{
+	if(P->tm_ptr == F && P->tm_S == S && P->tm_ld == ld)
+		return 0;
+	cuuint64_t gdim[3] = {(cuuint64_t) 2 * P->Ku, (cuuint64_t) S, (cuuint64_t) P->n_det};
+	cuuint64_t gstr[2] = {(cuuint64_t) ld * 16, (cuuint64_t) S * ld * 16};
+	cuuint32_t box[3] = {2 * KB, TM, (cuuint32_t) P->n_det};
+	cuuint32_t estr[3] = {1, 1, 1};
+	CUresult r = get_encode()(&P->tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void *>(F), gdim, gstr, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+				  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+	if(r != CUDA_SUCCESS) {
+		set_error("batch_run: cuTensorMapEncodeTiled failed (%d)", (int) r);
+		P->tm_ptr = nullptr;
+		return -1;
+	}
+	P->tm_ptr = F;
+	P->tm_S = S;
+	P->tm_ld = ld;
 	return 0;
 }
 
@@ -1131,22 +1472,8 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 			set_error("batch_run: split %d above %d stages", split, P->Kst);
 			return -1;
 		}
-		if(P->tm_ptr != F || P->tm_S != S || P->tm_ld != ld) {
-			cuuint64_t gdim[3] = {(cuuint64_t) 2 * P->Ku, (cuuint64_t) S, (cuuint64_t) P->n_det};
-			cuuint64_t gstr[2] = {(cuuint64_t) ld * 16, (cuuint64_t) S * ld * 16};
-			cuuint32_t box[3] = {2 * KB, TM, (cuuint32_t) P->n_det};
-			cuuint32_t estr[3] = {1, 1, 1};
-			CUresult r = get_encode()(&P->tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void *>(F), gdim, gstr, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-						  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-			if(r != CUDA_SUCCESS) {
-				set_error("batch_run: cuTensorMapEncodeTiled failed (%d)", (int) r);
-				P->tm_ptr = nullptr;
-				return -1;
-			}
-			P->tm_ptr = F;
-			P->tm_S = S;
-			P->tm_ld = ld;
-		}
+		if(ensure_tmap(P, F, S, ld))
+			return -1;
 		TcArgs a;
 		memset(&a, 0, sizeof(a));
 		a.S = S;
@@ -1162,6 +1489,8 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 		}
 		a.bops = P->bops;
 		a.acc = (float *) ws;
+		a.wait = P->wait_limit ? P->wait_limit : kWaitCycles;
+		a.hold = P->hold_stage;
 		a.reps = e.reps;
 		a.rep_stride = e.rep_stride;
 		a.err = P->err;
@@ -1210,6 +1539,42 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 			k_tc_contract<2, NF, 4, 3, false><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
 		else
 			k_tc_contract<2, NF, 3, 3, false><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+		if(P->ev_end)
+			cudaEventRecord(P->ev_end, st);
+		launches++;
+	} else if(P->dops && !((uintptr_t) F & 15)) {
+		if(split > P->Kst) {
+			set_error("batch_run: split %d above %d stages", split, P->Kst);
+			return -1;
+		}
+		if(ensure_tmap(P, F, S, ld))
+			return -1;
+		CcsArgs c;
+		memset(&c, 0, sizeof(c));
+		c.S = S;
+		c.n_det = P->n_det;
+		c.B = P->B;
+		c.Kst = P->Kst;
+		c.G = P->ccG;
+		c.accstride = P->accstride;
+		for(int b = 0; b < P->B; b++) {
+			c.bi[b] = P->bi[b];
+			c.bj[b] = P->bj[b];
+		}
+		c.dops = P->dops;
+		c.acc = ws;
+		c.err = P->err;
+		c.wait = P->wait_limit ? P->wait_limit : kWaitCycles;
+		const int tiles = (S + TM - 1) / TM;
+		c.tiles = tiles;
+		const int ctas = split > 0 ? tiles * split : batch_pick_ctas(P, S);
+		const int threads = 32 * (2 + P->B * P->ccG);
+		if(P->ev_begin)
+			cudaEventRecord(P->ev_begin, st);
+		if(P->precision == kPrecFP64)
+			k_cc_stream<double, CCS_NFS_F64, CCS_NWMAX_F64><<<ctas, threads, ccs_smem_bytes(*P), st>>>(P->tm, c);
+		else
+			k_cc_stream<float, CCS_NFS_F32, CCS_NWMAX_F32><<<ctas, threads, ccs_smem_bytes(*P), st>>>(P->tm, c);
 		if(P->ev_end)
 			cudaEventRecord(P->ev_end, st);
 		launches++;
@@ -1292,7 +1657,7 @@ int batch_autotune(void *pp, const void *F, int S, long long ld, void *sky, void
 	BatchPlan *P = (BatchPlan *) pp;
 	cudaStream_t st = (cudaStream_t) stream_v;
 	const int sms = sm_count();
-	const bool tc = is_tc(P->precision);
+	const bool tc = is_stream(P);
 	const int tiles = (S + TM - 1) / TM;
 	std::vector<int> cand;
 	if(tc) {
@@ -1316,7 +1681,7 @@ int batch_autotune(void *pp, const void *F, int S, long long ld, void *sky, void
 	CKB(cudaEventCreate(&e1));
 	int best = cand[0], best_v = 0;
 	float best_ms = 1e30f;
-	const int n_var = (tc && P->npart == 2) ? 3 : 1;
+	const int n_var = (is_tc(P->precision) && P->npart == 2) ? 3 : 1;
 	for(int v = 0; v < n_var; v++)
 		for(int c : cand) {
 			// the tcgen05 candidates run through the plan's CTA count for S
@@ -1435,12 +1800,33 @@ int batch_run_noalloc(void *pp, const void *F, int S, long long ld, const double
 	return batch_run(P, F, S, ld, gmst, sky, ws, kNoAllocScratchBytes, stream_v, 0);
 }
 
-int batch_check_error(void *pp, unsigned *code)
+int batch_check_error(void *pp, unsigned *code, bool clear)
 {
 	BatchPlan *P = (BatchPlan *) pp;
 	unsigned h = 0;
 	CKB(cudaMemcpy(&h, P->err, sizeof(h), cudaMemcpyDeviceToHost));
 	*code = h;
+	if(clear && h) {
+		const unsigned z = 0;
+		CKB(cudaMemcpy(P->err, &z, sizeof(z), cudaMemcpyHostToDevice));
+	}
+	return 0;
+}
+
+int batch_set_wait_limit(void *pp, unsigned long long cycles)
+{
+	((BatchPlan *) pp)->wait_limit = cycles;
+	return 0;
+}
+
+int batch_set_hold_stage(void *pp, int stage)
+{
+	BatchPlan *P = (BatchPlan *) pp;
+	if(!is_tc(P->precision)) {
+		set_error("batch_set_hold_stage: only the tcgen05 contraction takes the hook");
+		return -1;
+	}
+	P->hold_stage = stage < 0 ? -1 : stage;
 	return 0;
 }
 
@@ -1503,7 +1889,7 @@ int batch_run_host(void *pp, const void *F_host, int S, long long ld, const doub
 	if(nslot > 1)
 		CKB(cudaStreamSynchronize(st[1]));
 	unsigned code = 0;
-	if(batch_check_error(P, &code))
+	if(batch_check_error(P, &code, true))
 		return -1;
 	if(code) {
 		set_error("batch_run_host: device pipeline timed out (code %u)", code);

@@ -27,7 +27,9 @@ const double *rotation_plan_flat_for(const struct sh_series_rotation_plan *plan,
 int batch_set_split(void *plan, int S, int ks);
 int batch_pipe_variant(const void *plan, int S);
 int batch_set_pipe_variant(void *plan, int S, int variant);
-int batch_check_error(void *plan, unsigned *code);
+int batch_check_error(void *plan, unsigned *code, bool clear);
+int batch_set_wait_limit(void *plan, unsigned long long cycles);
+int batch_set_hold_stage(void *plan, int stage);
 int batch_set_timing_events(void *plan, void *ev_begin, void *ev_end);
 int batch_run_noalloc(void *plan, const void *F, int S, long long ld, const double *gmst, void *sky, void *stream);
 int batch_autotune(void *plan, const void *F, int S, long long ld, void *sky, void *ws, size_t ws_bytes, void *stream);
@@ -38,9 +40,9 @@ int batch_autotune(void *plan, const void *F, int S, long long ld, void *sky, vo
 // ------------------------------------------------------------------------
 static gsl_vector *vec3_alloc()
 {
-	gsl_vector *v = (gsl_vector *) malloc(sizeof(*v));
-	gsl_block *b = (gsl_block *) malloc(sizeof(*b));
-	double *d = (double *) calloc(3, sizeof(double));
+	gsl_vector *v = (gsl_vector *) xmalloc(sizeof(*v));
+	gsl_block *b = (gsl_block *) xmalloc(sizeof(*b));
+	double *d = (double *) xcalloc(3, sizeof(double));
 	if(!v || !b || !d) {
 		free(v);
 		free(b);
@@ -96,7 +98,7 @@ extern "C" void vector_direction(const gsl_vector *v, double *theta, double *phi
 
 extern "C" struct instrument *instrument_new(double x, double y, double z, void *data)
 {
-	struct instrument *n = (struct instrument *) malloc(sizeof(*n));
+	struct instrument *n = (struct instrument *) xmalloc(sizeof(*n));
 	gsl_vector *pc = vec3_alloc();
 	if(!n || !pc) {
 		free(n);
@@ -143,8 +145,8 @@ extern "C" gsl_vector *instrument_baseline(const struct instrument *a, const str
 
 extern "C" struct instrument_array *instrument_array_new(int n)
 {
-	struct instrument_array *a = (struct instrument_array *) malloc(sizeof(*a));
-	struct instrument **v = (struct instrument **) calloc(n > 0 ? n : 1, sizeof(*v));
+	struct instrument_array *a = (struct instrument_array *) xmalloc(sizeof(*a));
+	struct instrument **v = (struct instrument **) xcalloc(n > 0 ? n : 1, sizeof(*v));
 	if(!a || !v) {
 		free(a);
 		free(v);
@@ -176,7 +178,7 @@ extern "C" struct instrument *instrument_array_set(struct instrument_array *a, i
 
 extern "C" struct instrument *instrument_array_append(struct instrument_array *a, struct instrument *i)
 {
-	struct instrument **v = (struct instrument **) realloc(a->instruments, (a->n + 1) * sizeof(*v));
+	struct instrument **v = (struct instrument **) xrealloc(a->instruments, (a->n + 1) * sizeof(*v));
 	if(!v) {
 		instrument_free(i);
 		return NULL;
@@ -247,7 +249,7 @@ extern "C" double *correlator_square_window_new(const int n, const int zero_samp
 {
 	if(2 * zero_samples > n || zero_samples < 0)
 		return NULL;
-	double *w = (double *) malloc((n > 0 ? n : 1) * sizeof(double));
+	double *w = (double *) xmalloc((n > 0 ? n : 1) * sizeof(double));
 	if(!w)
 		return NULL;
 	for(int i = 0; i < n; i++)
@@ -259,7 +261,7 @@ extern "C" double *correlator_tukey_window_new(const int n, const int zero_sampl
 {
 	if(2 * (zero_samples + taper_samples) > n || zero_samples < 0)
 		return NULL;
-	double *w = (double *) malloc((n > 0 ? n : 1) * sizeof(double));
+	double *w = (double *) xmalloc((n > 0 ? n : 1) * sizeof(double));
 	if(!w)
 		return NULL;
 	const double dtheta = M_PI_2 / taper_samples;
@@ -283,7 +285,7 @@ extern "C" struct correlator_baseline *correlator_baseline_new(const struct inst
 	const struct instrument *b = instrument_array_get(instruments, index_b);
 	if(!a || !b)
 		return NULL;
-	struct correlator_baseline *n = (struct correlator_baseline *) malloc(sizeof(*n));
+	struct correlator_baseline *n = (struct correlator_baseline *) xmalloc(sizeof(*n));
 	gsl_vector *d = instrument_baseline(a, b);
 	if(!n || !d) {
 		vec3_free(d);
@@ -307,7 +309,7 @@ extern "C" void correlator_baseline_free(struct correlator_baseline *b)
 
 extern "C" struct correlator_baseline *correlator_baseline_copy(const struct correlator_baseline *b)
 {
-	struct correlator_baseline *n = (struct correlator_baseline *) malloc(sizeof(*n));
+	struct correlator_baseline *n = (struct correlator_baseline *) xmalloc(sizeof(*n));
 	if(!n)
 		return NULL;
 	*n = *b;
@@ -325,8 +327,8 @@ extern "C" struct correlator_network_baselines *correlator_network_baselines_new
 {
 	const int nd = instrument_array_len(instruments);
 	const int nb = nd * (nd - 1) / 2;
-	struct correlator_network_baselines *n = (struct correlator_network_baselines *) malloc(sizeof(*n));
-	struct correlator_baseline **v = (struct correlator_baseline **) calloc(nb > 0 ? nb : 1, sizeof(*v));
+	struct correlator_network_baselines *n = (struct correlator_network_baselines *) xmalloc(sizeof(*n));
+	struct correlator_baseline **v = (struct correlator_baseline **) xcalloc(nb > 0 ? nb : 1, sizeof(*v));
 	if(!n || !v) {
 		free(n);
 		free(v);
@@ -361,11 +363,11 @@ extern "C" void correlator_network_baselines_free(struct correlator_network_base
 
 extern "C" struct correlator_network_baselines *correlator_network_baselines_copy(const struct correlator_network_baselines *n)
 {
-	struct correlator_network_baselines *c = (struct correlator_network_baselines *) malloc(sizeof(*c));
+	struct correlator_network_baselines *c = (struct correlator_network_baselines *) xmalloc(sizeof(*c));
 	if(!c)
 		return NULL;
 	*c = *n;
-	c->baselines = (struct correlator_baseline **) calloc(n->n_baselines > 0 ? n->n_baselines : 1, sizeof(*c->baselines));
+	c->baselines = (struct correlator_baseline **) xcalloc(n->n_baselines > 0 ? n->n_baselines : 1, sizeof(*c->baselines));
 	if(!c->baselines) {
 		free(c);
 		return NULL;
@@ -416,8 +418,8 @@ static struct correlator_plan_fd *plan_fd_build(const struct correlator_baseline
 	if(l_req < L)
 		L = l_req;
 	const int n_el = projection_matrix_n_elements(r, delta_t);
-	struct correlator_plan_fd *p = (struct correlator_plan_fd *) calloc(1, sizeof(*p));
-	dcplx *fsp = (dcplx *) calloc(n, sizeof(dcplx));
+	struct correlator_plan_fd *p = (struct correlator_plan_fd *) xcalloc(1, sizeof(*p));
+	dcplx *fsp = (dcplx *) xcalloc(n, sizeof(dcplx));
 	struct sh_series_array *dp = sh_series_array_new(n, L, 1);
 	struct sh_series *p1 = sh_series_new_zero(L, 1);
 	double *R = sh_series_rot_matrix(baseline->theta, baseline->phi);
@@ -473,11 +475,11 @@ extern "C" void correlator_plan_fd_free(struct correlator_plan_fd *p)
 
 extern "C" struct correlator_plan_fd *correlator_plan_fd_copy(const struct correlator_plan_fd *plan)
 {
-	struct correlator_plan_fd *n = (struct correlator_plan_fd *) malloc(sizeof(*n));
+	struct correlator_plan_fd *n = (struct correlator_plan_fd *) xmalloc(sizeof(*n));
 	if(!n)
 		return NULL;
 	*n = *plan;
-	n->fseries_product = (dcplx *) malloc((size_t) plan->delay_product->n * sizeof(dcplx));
+	n->fseries_product = (dcplx *) xmalloc((size_t) plan->delay_product->n * sizeof(dcplx));
 	n->delay_product = sh_series_array_copy(plan->delay_product);
 	n->power_1d = sh_series_copy(plan->power_1d);
 	n->rotation_plan = sh_series_rotation_plan_copy(plan->rotation_plan);
@@ -516,8 +518,8 @@ extern "C" void sphrad_b200_plan_fd_touch(struct correlator_plan_fd *plan)
 
 extern "C" struct correlator_network_plan_fd *correlator_network_plan_fd_new_l(struct correlator_network_baselines *baselines, int n, double delta_t, unsigned l_max)
 {
-	struct correlator_network_plan_fd *np = (struct correlator_network_plan_fd *) malloc(sizeof(*np));
-	struct correlator_plan_fd **plans = (struct correlator_plan_fd **) calloc(baselines->n_baselines > 0 ? baselines->n_baselines : 1, sizeof(*plans));
+	struct correlator_network_plan_fd *np = (struct correlator_network_plan_fd *) xmalloc(sizeof(*np));
+	struct correlator_plan_fd **plans = (struct correlator_plan_fd **) xcalloc(baselines->n_baselines > 0 ? baselines->n_baselines : 1, sizeof(*plans));
 	if(!np || !plans) {
 		free(np);
 		free(plans);
@@ -555,11 +557,11 @@ extern "C" void correlator_network_plan_fd_free(struct correlator_network_plan_f
 
 extern "C" struct correlator_network_plan_fd *correlator_network_plan_fd_copy(const struct correlator_network_plan_fd *p)
 {
-	struct correlator_network_plan_fd *n = (struct correlator_network_plan_fd *) malloc(sizeof(*n));
+	struct correlator_network_plan_fd *n = (struct correlator_network_plan_fd *) xmalloc(sizeof(*n));
 	if(!n)
 		return NULL;
 	*n = *p;
-	n->plans = (struct correlator_plan_fd **) calloc(p->baselines->n_baselines > 0 ? p->baselines->n_baselines : 1, sizeof(*n->plans));
+	n->plans = (struct correlator_plan_fd **) xcalloc(p->baselines->n_baselines > 0 ? p->baselines->n_baselines : 1, sizeof(*n->plans));
 	if(!n->plans) {
 		free(n);
 		return NULL;
@@ -733,7 +735,7 @@ extern "C" struct correlator_plan_td *correlator_plan_td_new(const struct correl
 	if(P > a_l + b_l)
 		P = a_l + b_l;
 	const int n_el = projection_matrix_n_elements(d_len / 2, delta_t);
-	struct correlator_plan_td *p = (struct correlator_plan_td *) calloc(1, sizeof(*p));
+	struct correlator_plan_td *p = (struct correlator_plan_td *) xcalloc(1, sizeof(*p));
 	gsl_vector *dp = vec3_alloc();
 	double *R = sh_series_rot_matrix(baseline->theta, baseline->phi);
 	if(!p || !dp || !R)
@@ -768,8 +770,8 @@ fail:
 
 extern "C" struct correlator_network_plan_td *correlator_network_plan_td_new(struct correlator_network_baselines *baselines, double delta_t)
 {
-	struct correlator_network_plan_td *p = (struct correlator_network_plan_td *) malloc(sizeof(*p));
-	struct correlator_plan_td **plans = (struct correlator_plan_td **) calloc(baselines->n_baselines > 0 ? baselines->n_baselines : 1, sizeof(*plans));
+	struct correlator_network_plan_td *p = (struct correlator_network_plan_td *) xmalloc(sizeof(*p));
+	struct correlator_plan_td **plans = (struct correlator_plan_td **) xcalloc(baselines->n_baselines > 0 ? baselines->n_baselines : 1, sizeof(*plans));
 	if(!p || !plans) {
 		free(p);
 		free(plans);
@@ -979,7 +981,7 @@ static sphrad_batch_plan *batch_plan_new_nonpolar(const struct correlator_networ
 				  precision);
 	if(!np)
 		return NULL;
-	sphrad_batch_plan *bp = (sphrad_batch_plan *) malloc(sizeof(*bp));
+	sphrad_batch_plan *bp = (sphrad_batch_plan *) xmalloc(sizeof(*bp));
 	if(!bp) {
 		np_plan_destroy(np);
 		return NULL;
@@ -1029,7 +1031,7 @@ extern "C" sphrad_batch_plan *sphrad_batch_plan_new(const struct correlator_netw
 	void *impl = batch_plan_create(d, precision);
 	if(!impl)
 		return NULL;
-	sphrad_batch_plan *bp = (sphrad_batch_plan *) malloc(sizeof(*bp));
+	sphrad_batch_plan *bp = (sphrad_batch_plan *) xmalloc(sizeof(*bp));
 	if(!bp) {
 		batch_plan_destroy(impl);
 		return NULL;
@@ -1125,7 +1127,7 @@ extern "C" sphrad_fseries_plan *sphrad_fseries_plan_new(int n, const double *psd
 	void *impl = fseries_plan_create(n, psd);
 	if(!impl)
 		return NULL;
-	sphrad_fseries_plan *p = (sphrad_fseries_plan *) malloc(sizeof(*p));
+	sphrad_fseries_plan *p = (sphrad_fseries_plan *) xmalloc(sizeof(*p));
 	if(!p) {
 		fseries_plan_destroy(impl);
 		return NULL;
@@ -1214,9 +1216,21 @@ extern "C" int sphrad_batch_status(sphrad_batch_plan *p)
 	unsigned code = 0;
 	if(!p->impl)
 		return np_status(p->np);
-	if(batch_check_error(p->impl, &code))
+	if(batch_check_error(p->impl, &code, true))
 		return -1;
 	return (int) code;
+}
+
+extern "C" int sphrad_batch_set_wait_limit(sphrad_batch_plan *p, unsigned long long cycles)
+{
+	NEED_POLAR(p, "sphrad_batch_set_wait_limit");
+	return batch_set_wait_limit(p->impl, cycles);
+}
+
+extern "C" int sphrad_batch_test_withhold_stage(sphrad_batch_plan *p, int stage)
+{
+	NEED_POLAR(p, "sphrad_batch_test_withhold_stage");
+	return batch_set_hold_stage(p->impl, stage);
 }
 
 // ------------------------------------------------------------------------
@@ -1442,8 +1456,8 @@ extern "C" struct correlator_network_baselines *read_precalc_correlator_network_
 		set_error("precalc: %d baselines", nb);
 		return NULL;
 	}
-	struct correlator_network_baselines *net = (struct correlator_network_baselines *) malloc(sizeof(*net));
-	struct correlator_baseline **v = (struct correlator_baseline **) calloc(nb, sizeof(*v));
+	struct correlator_network_baselines *net = (struct correlator_network_baselines *) xmalloc(sizeof(*net));
+	struct correlator_baseline **v = (struct correlator_baseline **) xcalloc(nb, sizeof(*v));
 	bool ok = net && v;
 	for(int i = 0; ok && i < nb; i++) {
 		const std::string path = base_dir(parent_dir, i) + "/correlator_baseline.dat";
@@ -1481,8 +1495,8 @@ extern "C" int read_precalc_correlator_network_plan_fd(struct correlator_network
 		return -1;
 	}
 	const int nb = baselines->n_baselines;
-	struct correlator_plan_fd **pp = (struct correlator_plan_fd **) calloc(nb, sizeof(*pp));
-	struct correlator_plan_fd **pn = (struct correlator_plan_fd **) calloc(nb, sizeof(*pn));
+	struct correlator_plan_fd **pp = (struct correlator_plan_fd **) xcalloc(nb, sizeof(*pp));
+	struct correlator_plan_fd **pn = (struct correlator_plan_fd **) xcalloc(nb, sizeof(*pn));
 	bool ok = pp && pn;
 	for(int i = 0; ok && i < nb; i++) {
 		const std::string pd = plan_dir(parent_dir, i);
@@ -1503,7 +1517,7 @@ extern "C" int read_precalc_correlator_network_plan_fd(struct correlator_network
 		if(ok) {
 			const std::string path = pd + "/rotation_plan/D.dat";
 			const size_t len = rot_offset(l_max + 1);
-			dcplx *flat = (dcplx *) malloc((len ? len : 1) * sizeof(dcplx));
+			dcplx *flat = (dcplx *) xmalloc((len ? len : 1) * sizeof(dcplx));
 			File fl(path, "rb");
 			ok = flat && get(fl, flat, sizeof(dcplx), len, path);
 			if(ok)
@@ -1520,8 +1534,8 @@ extern "C" int read_precalc_correlator_network_plan_fd(struct correlator_network
 			ok = false;
 		}
 		if(ok) {
-			pp[i] = (struct correlator_plan_fd *) calloc(1, sizeof(**pp));
-			pn[i] = (struct correlator_plan_fd *) calloc(1, sizeof(**pn));
+			pp[i] = (struct correlator_plan_fd *) xcalloc(1, sizeof(**pp));
+			pn[i] = (struct correlator_plan_fd *) xcalloc(1, sizeof(**pn));
 			ok = pp[i] && pn[i];
 		}
 		if(ok) {
@@ -1537,7 +1551,7 @@ extern "C" int read_precalc_correlator_network_plan_fd(struct correlator_network
 				p->delta_t = delta_t;
 				p->transient = transient;
 				// scratch of the integrator (inspiral_sky_map.c:1316-1323)
-				p->fseries_product = (dcplx *) calloc(tseries_length, sizeof(dcplx));
+				p->fseries_product = (dcplx *) xcalloc(tseries_length, sizeof(dcplx));
 				p->power_1d = p->rotation_plan ? sh_series_new(p->rotation_plan->l_max, p->delay_product->polar) : NULL;
 				ok = ok && p->rotation_plan && p->fseries_product && p->power_1d;
 			}

@@ -108,7 +108,10 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ Gemm
 	constexpr int B_BYTES = NT * GK * 2;
 	constexpr uint32_t NCOLS = NT < 32 ? 32 : NT;
 	extern __shared__ uint8_t smem_raw[];
-	uint8_t *smem = (uint8_t *) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
+	// aligned by an offset on the shared array itself, so that accesses
+	// through it stay shared-memory accesses (an integer round trip would
+	// make them generic)
+	uint8_t *smem = smem_raw + ((1024 - ((uintptr_t) smem_raw & 1023)) & 1023);
 	uint8_t *sA = smem, *sB = smem + GSTAGES * A_BYTES;
 	__shared__ __align__(8) uint64_t bars[GSTAGES];
 	__shared__ uint32_t tslot;

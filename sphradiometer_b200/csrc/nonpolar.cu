@@ -276,7 +276,10 @@ struct NptArgs {
 __global__ void __launch_bounds__(NPT_THREADS, 1) k_np_tc(const __grid_constant__ NptArgs a)
 {
 	extern __shared__ uint8_t smem_raw[];
-	uint8_t *smem = (uint8_t *) (((uintptr_t) smem_raw + 1023) & ~(uintptr_t) 1023);
+	// aligned by an offset on the shared array itself, so that accesses
+	// through it stay shared-memory accesses (an integer round trip would
+	// make them generic)
+	uint8_t *smem = smem_raw + ((1024 - ((uintptr_t) smem_raw & 1023)) & 1023);
 	constexpr int stage_bytes = 2 * NPT_A_PART + 2 * NPT_B_PART;
 	uint64_t *full = (uint64_t *) (smem + NPT_STAGES * stage_bytes);
 	uint64_t *empty = full + NPT_STAGES;

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <array>
 #include <cmath>
 #include <cstdarg>
@@ -110,8 +111,30 @@ int stream_sync()
 	return 0;
 }
 
+static std::atomic<long> g_alloc_fault{0};
+
+int set_alloc_fault(long n)
+{
+	g_alloc_fault.store(n > 0 ? n : 0);
+	return 0;
+}
+
+bool alloc_fault_due()
+{
+	long v = g_alloc_fault.load();
+	while(v > 0) {
+		if(g_alloc_fault.compare_exchange_weak(v, v - 1))
+			return v == 1;
+	}
+	return false;
+}
+
 void *dmalloc(size_t bytes)
 {
+	if(alloc_fault_due()) {
+		set_error("cudaMalloc(%zu): injected allocation failure", bytes);
+		return nullptr;
+	}
 	void *p = nullptr;
 	cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
 	if(e != cudaSuccess) {
@@ -622,6 +645,54 @@ int rotate_series(unsigned l_max, int polar, const double *series, const double 
 // ------------------------------------------------------------------------
 // FP64 frequency-domain integration (correlator.c:681-711, 993-1010)
 // ------------------------------------------------------------------------
+namespace {
+// a typed view of a piece of the arena
+struct TdSpan {
+	void *p;
+	template <class T_> T_ *as() const { return (T_ *) p; }
+};
+
+// grow-only device arena, per device, and grow-only pinned host staging
+// buffers (one upload, one download per call) of the drop-in integrators:
+// calls after the first allocate nothing while their sizes do not grow
+struct TdArena {
+	std::mutex mu;
+	std::unordered_map<int, std::pair<void *, size_t>> bufs;
+	void *hup = nullptr, *hdown = nullptr;
+	size_t hup_n = 0, hdown_n = 0;
+	static void *pinned(void **p, size_t *have, size_t need)
+	{
+		if(*have < need || !*p) {
+			if(*p)
+				cudaFreeHost(*p);
+			*p = nullptr;
+			*have = 0;
+			if(cudaMallocHost(p, need ? need : 16) != cudaSuccess) {
+				*p = nullptr;
+				set_error("cannot allocate %zu bytes of pinned host memory", need);
+				return nullptr;
+			}
+			*have = need;
+		}
+		return *p;
+	}
+	void *get(size_t need)
+	{
+		int dev = 0;
+		cudaGetDevice(&dev);
+		auto &b = bufs[dev];
+		if(b.second < need || !b.first) {
+			dfree(b.first);
+			b.first = dmalloc(need);
+			b.second = b.first ? need : 0;
+		}
+		return b.first;
+	}
+};
+TdArena g_td_arena;
+TdArena g_fd_arena;
+}  // namespace
+
 struct DevJob {
 	const double2 *a, *b;   // spectra
 	const double2 *D;       // n x stride delay table
@@ -634,16 +705,23 @@ struct DevJob {
 
 constexpr int XS_CHUNK = 64;
 
-// cross-spectrum X[k] = b[k] conj(a[k]) and P[j] += sum_k X[k] D[k][j] over
-// a chunk of bins (sh_series_array.c:437-456 inner loop order transposed)
-__global__ void k_xspec_dot(const DevJob *jobs)
+// cross-spectrum X[k] = b[k] conj(a[k]) and P[j] += sum_k X[k] D[k][j]
+// (sh_series_array.c:437-456) over a chunk of XD_ROWS bins of one baseline
+// per block: the block forms the chunk's X once in shared memory; warp w
+// takes bins w, w + XD_WARPS, ... with its lanes over 32 consecutive j (rows
+// of D read coalesced), the warps' partial sums meet in shared memory and
+// one FP64 atomic per j and block leaves
+constexpr int XD_ROWS = 64, XD_WARPS = 8;
+
+__global__ void __launch_bounds__(32 * XD_WARPS) k_xdot(const DevJob *jobs)
 {
 	const DevJob J = jobs[blockIdx.y];
-	const int k0 = blockIdx.x * XS_CHUNK;
+	const int k0 = blockIdx.x * XD_ROWS;
 	if(k0 >= J.n)
 		return;
-	__shared__ double2 s_x[XS_CHUNK];
-	const int kc = min(XS_CHUNK, J.n - k0);
+	__shared__ double2 s_x[XD_ROWS];
+	__shared__ double2 s_red[XD_WARPS][32];
+	const int kc = min(XD_ROWS, J.n - k0);
 	for(int k = threadIdx.x; k < kc; k += blockDim.x) {
 		const double2 v = cmulc(J.b[k0 + k], J.a[k0 + k]);
 		s_x[k] = v;
@@ -651,24 +729,49 @@ __global__ void k_xspec_dot(const DevJob *jobs)
 			J.X[k0 + k] = v;
 	}
 	__syncthreads();
-	for(int j = threadIdx.x; j < J.stride; j += blockDim.x) {
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	for(int j0 = 0; j0 < J.stride; j0 += 32) {
+		const int j = j0 + lane;
 		double2 acc = make_double2(0, 0);
-		const double2 *d = J.D + (size_t) k0 * J.stride + j;
-		for(int k = 0; k < kc; k++) {
-			const double2 t = cmul(d[(size_t) k * J.stride], s_x[k]);
-			acc.x += t.x;
-			acc.y += t.y;
+		if(j < J.stride) {
+			const double2 *d = J.D + (size_t) k0 * J.stride + j;
+#pragma unroll 4
+			for(int k = warp; k < kc; k += XD_WARPS) {
+				const double2 t = cmul(d[(size_t) k * J.stride], s_x[k]);
+				acc.x += t.x;
+				acc.y += t.y;
+			}
 		}
-		atomicAdd(&J.P[j].x, acc.x);
-		atomicAdd(&J.P[j].y, acc.y);
+		s_red[warp][lane] = acc;
+		__syncthreads();
+		if(warp == 0 && j < J.stride) {
+			double2 v = s_red[0][lane];
+			for(int w = 1; w < XD_WARPS; w++) {
+				v.x += s_red[w][lane].x;
+				v.y += s_red[w][lane].y;
+			}
+			atomicAdd(&J.P[j].x, v.x);
+			atomicAdd(&J.P[j].y, v.y);
+		}
+		__syncthreads();
 	}
 }
 
-// sky_{l m'} = sum_b weight_b / n_b * (rotated P_b)_{l m'}; also rescales
-// P_b to power_1d = P_b / n_b (grid: m' + L, threads over l)
-__global__ void k_rotate_sum(const DevJob *jobs, int n_jobs, int L, double2 *sky)
+// sky_{l m'} = sum_b weight_b / n_b * (rotated P_b)_{l m'} (grid: m' + L,
+// threads over l); with pw set, block b < n_jobs also writes baseline b's
+// power_1d = P_b / n_b to pw + b * pw_stride
+__global__ void k_rotate_sum(const DevJob *jobs, int n_jobs, int L, double2 *sky, double2 *pw = nullptr, int pw_stride = 0)
 {
+	if(pw && (int) blockIdx.x < n_jobs) {
+		const DevJob &J = jobs[blockIdx.x];
+		for(int j = threadIdx.x; j < J.stride; j += blockDim.x) {
+			const double2 p = J.P[j];
+			pw[(size_t) blockIdx.x * pw_stride + j] = make_double2(p.x / J.n, p.y / J.n);
+		}
+	}
 	const int mp = (int) blockIdx.x - L;
+	if(mp > L)
+		return;
 	for(int l = abs(mp) + threadIdx.x; l <= L; l += blockDim.x) {
 		double2 acc = make_double2(0, 0);
 		for(int b = 0; b < n_jobs; b++) {
@@ -694,15 +797,6 @@ __global__ void k_rotate_sum(const DevJob *jobs, int n_jobs, int L, double2 *sky
 			acc.y += s * c.y;
 		}
 		sky[d_lmoffset(L, l, mp)] = acc;
-	}
-}
-
-__global__ void k_scale_power(const DevJob *jobs, double2 *out, int out_stride)
-{
-	const DevJob J = jobs[blockIdx.x];
-	for(int j = threadIdx.x; j < J.stride; j += blockDim.x) {
-		const double2 p = J.P[j];
-		out[(size_t) blockIdx.x * out_stride + j] = make_double2(p.x / J.n, p.y / J.n);
 	}
 }
 
@@ -813,17 +907,36 @@ int integrate_fd(const BaselineJob *jobs, int n_jobs, unsigned sky_l_max, double
 	for(size_t i = 0; i < uniq.size(); i++)
 		spec_total += uniq_n[i];
 	const size_t sky_len = (size_t) (sky_l_max + 1) * (sky_l_max + 1);
-	DBuf spec(spec_total * sizeof(double2)), X(x_total * sizeof(double2)), P(p_total * sizeof(double2));
-	DBuf pw((size_t) n_jobs * max_stride * sizeof(double2)), dsky(sky_len * sizeof(double2)), djobs(n_jobs * sizeof(DevJob));
-	if(!spec.p || !X.p || !P.p || !pw.p || !dsky.p || !djobs.p)
+	// one grow-only device arena per device, held for the call: an upload
+	// region (unique spectra, job table) filled by one copy from pinned
+	// staging, a download region (sky, power_1d rows, cross spectra) read
+	// back by one copy, and the partial sums P
+	auto al = [](size_t b) { return (b + 255) & ~(size_t) 255; };
+	const size_t up_spec = al(spec_total * sizeof(double2));
+	const size_t up_bytes = up_spec + al(n_jobs * sizeof(DevJob));
+	const size_t dn_sky = al(sky_len * sizeof(double2));
+	const size_t dn_pw = al((size_t) n_jobs * max_stride * sizeof(double2));
+	const size_t dn_bytes = dn_sky + dn_pw + x_total * sizeof(double2);
+	const size_t p_bytes = p_total * sizeof(double2);
+	std::lock_guard<std::mutex> lock(g_fd_arena.mu);
+	char *base = (char *) g_fd_arena.get(up_bytes + al(dn_bytes) + p_bytes);
+	char *hup = (char *) TdArena::pinned(&g_fd_arena.hup, &g_fd_arena.hup_n, up_bytes);
+	char *hdown = (char *) TdArena::pinned(&g_fd_arena.hdown, &g_fd_arena.hdown_n, dn_bytes);
+	if(!base || !hup || !hdown)
 		return -1;
+	double2 *spec = (double2 *) base;
+	DevJob *djobs = (DevJob *) (base + up_spec);
+	char *down = base + up_bytes;
+	double2 *dsky = (double2 *) down;
+	double2 *pw = (double2 *) (down + dn_sky);
+	double2 *X = (double2 *) (down + dn_sky + dn_pw);
+	double2 *P = (double2 *) (base + up_bytes + al(dn_bytes));
 	std::vector<size_t> uoff(uniq.size());
 	{
 		size_t o = 0;
 		for(size_t i = 0; i < uniq.size(); i++) {
 			uoff[i] = o;
-			if(h2d(spec.as<double2>() + o, uniq[i], uniq_n[i] * sizeof(double2)))
-				return -1;
+			memcpy(hup + o * sizeof(double2), uniq[i], uniq_n[i] * sizeof(double2));
 			o += uniq_n[i];
 		}
 	}
@@ -836,12 +949,12 @@ int integrate_fd(const BaselineJob *jobs, int n_jobs, unsigned sky_l_max, double
 			if(refresh_mirror(J, m))
 				return -1;
 			DevJob &d = dj[i];
-			d.a = spec.as<double2>() + uoff[ia[i]];
-			d.b = spec.as<double2>() + uoff[ib[i]];
+			d.a = spec + uoff[ia[i]];
+			d.b = spec + uoff[ib[i]];
 			d.D = m.D;
 			d.rot = m.rot;
-			d.X = X.as<double2>() + xo;
-			d.P = P.as<double2>() + po;
+			d.X = X + xo;
+			d.P = P + po;
 			d.n = J.n;
 			d.stride = J.stride;
 			d.l_max = (int) J.l_max;
@@ -851,25 +964,28 @@ int integrate_fd(const BaselineJob *jobs, int n_jobs, unsigned sky_l_max, double
 			po += J.stride;
 		}
 	}
-	if(h2d(djobs.p, dj.data(), n_jobs * sizeof(DevJob)) || dmemset(P.p, 0, p_total * sizeof(double2)))
-		return -1;
-	dim3 g1((max_n + XS_CHUNK - 1) / XS_CHUNK, n_jobs);
-	k_xspec_dot<<<g1, 128, 0, S()>>>(djobs.as<DevJob>());
-	k_rotate_sum<<<2 * sky_l_max + 1, 64, 0, S()>>>(djobs.as<DevJob>(), n_jobs, (int) sky_l_max, dsky.as<double2>());
-	k_scale_power<<<n_jobs, 128, 0, S()>>>(djobs.as<DevJob>(), pw.as<double2>(), max_stride);
+	memcpy(hup + up_spec, dj.data(), n_jobs * sizeof(DevJob));
+	CK(cudaMemcpyAsync(base, hup, up_bytes, cudaMemcpyHostToDevice, S()));
+	CK(cudaMemsetAsync(P, 0, p_bytes, S()));
+	dim3 g1((max_n + XD_ROWS - 1) / XD_ROWS, n_jobs);
+	k_xdot<<<g1, 32 * XD_WARPS, 0, S()>>>(djobs);
+	const int rgrid = (int) (2 * sky_l_max + 1) > n_jobs ? (int) (2 * sky_l_max + 1) : n_jobs;
+	k_rotate_sum<<<rgrid, 64, 0, S()>>>(djobs, n_jobs, (int) sky_l_max, dsky, pw, max_stride);
 	CK(cudaGetLastError());
-	if(d2h(sky, dsky.p, sky_len * sizeof(double2)))
+	CK(cudaMemcpyAsync(hdown, down, dn_bytes, cudaMemcpyDeviceToHost, S()));
+	if(stream_sync())
 		return -1;
+	memcpy(sky, hdown, sky_len * sizeof(double2));
 	xo = 0;
 	for(int i = 0; i < n_jobs; i++) {
 		const BaselineJob &J = jobs[i];
-		if(J.power_1d && d2h(J.power_1d, pw.as<double2>() + (size_t) i * max_stride, J.stride * sizeof(double2)))
-			return -1;
-		if(J.fseries_product && d2h(J.fseries_product, X.as<double2>() + xo, J.n * sizeof(double2)))
-			return -1;
+		if(J.power_1d)
+			memcpy(J.power_1d, hdown + dn_sky + (size_t) i * max_stride * sizeof(double2), J.stride * sizeof(double2));
+		if(J.fseries_product)
+			memcpy(J.fseries_product, hdown + dn_sky + dn_pw + xo * sizeof(double2), J.n * sizeof(double2));
 		xo += J.n;
 	}
-	return stream_sync();
+	return 0;
 }
 
 // ------------------------------------------------------------------------
@@ -1156,49 +1272,6 @@ __global__ void __launch_bounds__(256) k_td_power(int nq, const double *__restri
 		power[L] = make_double2(2.0 * M_PI * t.x, 2.0 * M_PI * t.y);
 }
 
-// a typed view of a piece of the arena
-struct TdSpan {
-	void *p;
-	template <class T_> T_ *as() const { return (T_ *) p; }
-};
-
-// grow-only device arena of the time-domain integrator, per device, and
-// grow-only pinned host staging buffers (one upload, one download per call)
-struct TdArena {
-	std::mutex mu;
-	std::unordered_map<int, std::pair<void *, size_t>> bufs;
-	void *hup = nullptr, *hdown = nullptr;
-	size_t hup_n = 0, hdown_n = 0;
-	static void *pinned(void **p, size_t *have, size_t need)
-	{
-		if(*have < need || !*p) {
-			if(*p)
-				cudaFreeHost(*p);
-			*p = nullptr;
-			*have = 0;
-			if(cudaMallocHost(p, need ? need : 16) != cudaSuccess) {
-				*p = nullptr;
-				set_error("time-domain correlator: cannot allocate %zu bytes of pinned host memory", need);
-				return nullptr;
-			}
-			*have = need;
-		}
-		return *p;
-	}
-	void *get(size_t need)
-	{
-		int dev = 0;
-		cudaGetDevice(&dev);
-		auto &b = bufs[dev];
-		if(b.second < need || !b.first) {
-			dfree(b.first);
-			b.first = dmalloc(need);
-			b.second = b.first ? need : 0;
-		}
-		return b.first;
-	}
-};
-TdArena g_td_arena;
 
 }  // namespace
 

@@ -22,6 +22,11 @@ int stream_sync();
 int sync_stream(void *stream);  // a caller's cudaStream_t, NULL = library stream
 
 void *dmalloc(size_t bytes);  // NULL + error on failure
+// allocation-failure injection (host-side failure detection tests): when
+// armed with n > 0, the n-th next allocation the library makes (device,
+// or host allocations of the C-ABI objects) fails as if memory ran out
+int set_alloc_fault(long n);
+bool alloc_fault_due();
 void dfree(void *p);
 int h2d(void *dst, const void *src, size_t bytes);       // async on lib stream
 int d2h(void *dst, const void *src, size_t bytes);       // async on lib stream
@@ -196,7 +201,23 @@ int batch_set_split(void *plan, int S, int split);
 // ---- spherical-harmonic transforms on theta x phi grids (sht.cu) -------
 // Gauss-Legendre nodes (decreasing x) and weights on [-1, 1] (host)
 void gl_nodes(int n, double *x, double *w);
-enum GridKind { kGridGL = 0, kGridEquiangular = 1 };
+enum GridKind { kGridGL = 0, kGridEquiangular = 1, kGridRing = 2 };
+// HEALPix ring grid of nside N (kGridRing: the plan's nt is N): rings
+// i = 1 .. 4N - 1, z_i = 1 - i^2/(3N^2) (i < N), 4/3 - 2i/(3N) (N <= i <=
+// 3N), mirrored south; 4i pixels on polar ring i (4(4N - i) south), 4N in
+// the belt; pixel j of a ring at phi = (j + 1/2) pi / (2i) on polar rings
+// and (j + (1 - (i + N) mod 2) / 2) pi / (2N) in the belt (the HEALPix
+// RING scheme, Gorski et al. 2005, ApJ 622, 759)
+inline int ring_npix(int N, int i) { return i < N ? 4 * i : (i > 3 * N ? 4 * (4 * N - i) : 4 * N); }
+inline long long ring_first_pixel(int N, int i)
+{
+	if(i <= N)
+		return 2LL * i * (i - 1);
+	if(i <= 3 * N)
+		return 2LL * N * (N - 1) + 4LL * N * (i - N);
+	const int k = 4 * N - i;  // south ring k counted from the pole: rings after it hold 2k(k-1) pixels
+	return 12LL * N * N - 2LL * (k + 1) * k;
+}
 enum PixOut { kPixComplex = 0, kPixReal = 1, kPixArgmax = 2 };
 // Tables for l <= L on an nt x nphi grid: GL rows (the reference's mesh
 // rows, increasing theta) or cell-centre rows theta_i = pi (i + 1/2) / nt;
@@ -260,8 +281,14 @@ int array_dft(int n, int stride, double *data, int sign);
 // the reference's extremization (l <= 6 mesh search, then refinement) of
 // the maximum of sign * Re f for S device series; returns after the work
 // on stream (NULL = library stream) has finished (host C++, sh_algebra.cpp)
-int extremum(const double *coeff_dev, long long cstride, int S, unsigned L, int polar, double sign, double *out_dev, int *status_dev, void *stream);
+// method: -1 = the process-wide refinement (peak_refine_method()), 0 =
+// trust-region Newton, 1 = BFGS2 (gradient in the co-ordinates), 2 = BFGS2
+// as the reference's sh_series_real_minimum runs it
+int extremum(const double *coeff_dev, long long cstride, int S, unsigned L, int polar, double sign, double *out_dev, int *status_dev, void *stream,
+	     int method = -1);
 int peak_refine(int S, unsigned L, int polar, const void *coeff, long long cstride, const double *theta0, const double *phi0, double sign, int max_iter,
-		double tol, double *out, int *status, void *stream);
+		double tol, double *out, int *status, void *stream, int method = -1);
+int peak_refine_method();
+int set_peak_refine_method(int method);
 
 }  // namespace sphrad

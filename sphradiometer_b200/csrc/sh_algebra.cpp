@@ -181,8 +181,8 @@ extern "C" double sh_series_wigner_3j(int ja, int jb, int jc, int ma, int mb, in
 static int mesh_coords(unsigned l_max, int *ntheta, int *nphi, double **cos_theta, double **weights)
 {
 	const int nt = 2 * ((int) l_max + 1);
-	double *x = (double *) malloc(nt * sizeof(double));
-	double *w = (double *) malloc(nt * sizeof(double));
+	double *x = (double *) xmalloc(nt * sizeof(double));
+	double *w = (double *) xmalloc(nt * sizeof(double));
 	if(!x || !w) {
 		free(x);
 		free(w);
@@ -203,7 +203,7 @@ extern "C" dcplx *sh_series_mesh_new(unsigned int l_max, int *ntheta, int *nphi,
 {
 	if(mesh_coords(l_max, ntheta, nphi, cos_theta_array, cos_theta_weights))
 		return NULL;
-	dcplx *mesh = (dcplx *) malloc((size_t) *ntheta * *nphi * sizeof(dcplx));
+	dcplx *mesh = (dcplx *) xmalloc((size_t) *ntheta * *nphi * sizeof(dcplx));
 	if(mesh)
 		return mesh;
 	free(*cos_theta_array);
@@ -227,7 +227,7 @@ extern "C" dcplx *sh_series_to_mesh(const struct sh_series *series, int *ntheta,
 		*cos_theta_array = NULL;
 	if(mesh_coords(series->l_max, &nt, &np, &x, NULL))
 		return NULL;
-	dcplx *mesh = (dcplx *) malloc((size_t) nt * np * sizeof(dcplx));
+	dcplx *mesh = (dcplx *) xmalloc((size_t) nt * np * sizeof(dcplx));
 	void *plan = get_plan(series->l_max, kGridGL, nt, np, 0);
 	const size_t clen = length(series->l_max, series->polar);
 	const int M = series->polar ? 0 : (int) series->l_max;
@@ -281,7 +281,7 @@ extern "C" struct sh_series *sh_series_from_mesh(struct sh_series *series, dcplx
 // ------------------------------------------------------------------------
 extern "C" struct sh_series_product_plan *sh_series_product_plan_new(const struct sh_series *dest, const struct sh_series *a, const struct sh_series *b)
 {
-	struct sh_series_product_plan *p = (struct sh_series_product_plan *) malloc(sizeof(*p));
+	struct sh_series_product_plan *p = (struct sh_series_product_plan *) xmalloc(sizeof(*p));
 	if(!p)
 		return NULL;
 	p->a_l_max = a->l_max;
@@ -338,10 +338,13 @@ extern "C" struct sh_series *sh_series_product(struct sh_series *dest, const str
 // ------------------------------------------------------------------------
 // extremization (sh_series_extremize.c:168-360): brute-force search of the
 // l <= 6 low-passed series on its 14 x 14 mesh, then local refinement of
-// the full series from the best pixel
+// the full series from the best pixel.  sh_series_real_minimum refines as
+// the reference does (BFGS2 with its gradient convention, co-ordinates
+// returned unconditioned); the batched localisers use the process-wide
+// method (BFGS2 with the gradient in the co-ordinates by default)
 // ------------------------------------------------------------------------
 int sphrad::extremum(const double *coeff_dev, long long cstride, int S, unsigned L, int polar, double sign, double *out_dev, int *status_dev,
-		    void *stream)
+		    void *stream, int method)
 {
 	const unsigned Lc = L < 6 ? L : 6;
 	const int nt = 2 * ((int) Lc + 1);
@@ -358,7 +361,7 @@ int sphrad::extremum(const double *coeff_dev, long long cstride, int S, unsigned
 	double *t0 = (double *) dt, *p0 = t0 + S;
 	if(sht_synthesis(plan, coeff_dev, S, cstride, L, polar, Lc, kPixArgmax, drb, ds, stream, sign) ||
 	   sht_rows_argmax(plan, S, drb, t0, p0, nullptr, stream) ||
-	   peak_refine(S, L, polar, coeff_dev, cstride, t0, p0, sign, 100, 1e-11, out_dev, status_dev, stream))
+	   peak_refine(S, L, polar, coeff_dev, cstride, t0, p0, sign, 100, 1e-11, out_dev, status_dev, stream, method))
 		return -1;
 	// the scratch is reused by the next call once this one has finished
 	return sync_stream(stream);
@@ -370,7 +373,7 @@ extern "C" double sh_series_real_minimum(const struct sh_series *series, double 
 	Dev dc(clen * sizeof(dcplx)), dout(4 * sizeof(double)), dst(sizeof(int));
 	double out[4];
 	if(!dc.p || !dout.p || !dst.p || h2d(dc.p, series->coeff, clen * sizeof(dcplx)) ||
-	   extremum((const double *) dc.p, (long long) clen, 1, series->l_max, series->polar, -1.0, (double *) dout.p, (int *) dst.p, nullptr) ||
+	   extremum((const double *) dc.p, (long long) clen, 1, series->l_max, series->polar, -1.0, (double *) dout.p, (int *) dst.p, nullptr, 2) ||
 	   d2h(out, dout.p, sizeof(out)) || stream_sync())
 		return NAN;
 	*theta = out[0];

@@ -147,6 +147,8 @@ void gl_nodes(int n, double *x, double *w)
 
 extern "C" const char *sphrad_b200_last_error(void) { return sphrad::last_error(); }
 
+extern "C" int sphrad_b200_inject_allocation_failure(long n) { return sphrad::set_alloc_fault(n); }
+
 // ------------------------------------------------------------------------
 // Y_lm (sh_series_trans.c:65-114)
 // ------------------------------------------------------------------------
@@ -190,8 +192,8 @@ extern "C" dcplx *sh_series_Yconj_array(dcplx *array, unsigned int l_max, int m,
 // ------------------------------------------------------------------------
 extern "C" struct sh_series *sh_series_new(unsigned int l_max, int polar)
 {
-	struct sh_series *s = (struct sh_series *) malloc(sizeof(*s));
-	dcplx *c = (dcplx *) malloc(length(l_max, polar) * sizeof(dcplx));
+	struct sh_series *s = (struct sh_series *) xmalloc(sizeof(*s));
+	dcplx *c = (dcplx *) xmalloc(length(l_max, polar) * sizeof(dcplx));
 	if(!s || !c) {
 		free(s);
 		free(c);
@@ -205,8 +207,8 @@ extern "C" struct sh_series *sh_series_new(unsigned int l_max, int polar)
 
 extern "C" struct sh_series *sh_series_new_zero(unsigned int l_max, int polar)
 {
-	struct sh_series *s = (struct sh_series *) malloc(sizeof(*s));
-	dcplx *c = (dcplx *) calloc(length(l_max, polar), sizeof(dcplx));
+	struct sh_series *s = (struct sh_series *) xmalloc(sizeof(*s));
+	dcplx *c = (dcplx *) xcalloc(length(l_max, polar), sizeof(dcplx));
 	if(!s || !c) {
 		free(s);
 		free(c);
@@ -247,7 +249,7 @@ extern "C" struct sh_series *sh_series_resize(struct sh_series *series, unsigned
 	if(l_max == series->l_max)
 		return series;
 	struct sh_series wrapper = *series;
-	dcplx *c = (dcplx *) malloc(length(l_max, series->polar) * sizeof(dcplx));
+	dcplx *c = (dcplx *) xmalloc(length(l_max, series->polar) * sizeof(dcplx));
 	if(!c)
 		return NULL;
 	struct sh_series dst = {l_max, series->polar, c};
@@ -271,7 +273,7 @@ extern "C" struct sh_series *sh_series_set_polar(struct sh_series *series, int p
 	polar = polar ? 1 : 0;
 	if(series->polar == polar)
 		return series;
-	dcplx *c = (dcplx *) realloc(series->coeff, length(series->l_max, polar) * sizeof(dcplx));
+	dcplx *c = (dcplx *) xrealloc(series->coeff, length(series->l_max, polar) * sizeof(dcplx));
 	if(!c)
 		return NULL;
 	if(!polar)
@@ -504,7 +506,7 @@ extern "C" struct sh_series *sh_series_impulse(unsigned int l_max, double theta,
 // ------------------------------------------------------------------------
 extern "C" double *euler_rotation_matrix(double gamma, double beta, double alpha)
 {
-	double *R = (double *) malloc(9 * sizeof(double));
+	double *R = (double *) xmalloc(9 * sizeof(double));
 	if(!R)
 		return NULL;
 	const double ca = cos(alpha), sa = sin(alpha), cb = cos(beta), sb = sin(beta), cg = cos(gamma), sg = sin(gamma);
@@ -538,8 +540,8 @@ std::map<const void *, RotBlock> g_rot_blocks;  // plan -> flat block (NULL if p
 
 static struct sh_series_rotation_plan *rotation_plan_from_flat(unsigned l_max, dcplx *flat)
 {
-	struct sh_series_rotation_plan *plan = (struct sh_series_rotation_plan *) malloc(sizeof(*plan));
-	dcplx **D = (dcplx **) malloc((l_max ? l_max : 1) * sizeof(dcplx *));
+	struct sh_series_rotation_plan *plan = (struct sh_series_rotation_plan *) xmalloc(sizeof(*plan));
+	dcplx **D = (dcplx **) xmalloc((l_max ? l_max : 1) * sizeof(dcplx *));
 	if(!plan || !D) {
 		free(plan);
 		free(D);
@@ -589,7 +591,7 @@ extern "C" struct sh_series_rotation_plan *sh_series_rotation_plan_new(const str
 {
 	const unsigned L = series->l_max;
 	const size_t len = rot_offset(L + 1);
-	dcplx *flat = (dcplx *) malloc((len ? len : 1) * sizeof(dcplx));
+	dcplx *flat = (dcplx *) xmalloc((len ? len : 1) * sizeof(dcplx));
 	if(!flat)
 		return NULL;
 	if(L >= 1 && build_rotation_plan(L, R, (double *) flat)) {
@@ -652,7 +654,7 @@ extern "C" struct sh_series_rotation_plan *sh_series_rotation_plan_copy(const st
 	std::vector<dcplx> scratch;
 	const dcplx *src = rotation_plan_flat(plan, scratch);
 	const size_t len = rot_offset(plan->l_max + 1);
-	dcplx *flat = (dcplx *) malloc((len ? len : 1) * sizeof(dcplx));
+	dcplx *flat = (dcplx *) xmalloc((len ? len : 1) * sizeof(dcplx));
 	if(!flat)
 		return NULL;
 	memcpy(flat, src, len * sizeof(dcplx));
@@ -738,9 +740,9 @@ extern "C" struct sh_series *sh_series_rotate_z(struct sh_series *result, const 
 extern "C" struct sh_series_array *sh_series_array_new(int n, unsigned int l_max, int polar)
 {
 	polar = polar ? 1 : 0;
-	struct sh_series_array *a = (struct sh_series_array *) malloc(sizeof(*a));
-	struct sh_series *s = (struct sh_series *) malloc((n > 0 ? n : 1) * sizeof(*s));
-	dcplx *c = (dcplx *) malloc(((size_t) (n > 0 ? n : 1)) * length(l_max, polar) * sizeof(dcplx));
+	struct sh_series_array *a = (struct sh_series_array *) xmalloc(sizeof(*a));
+	struct sh_series *s = (struct sh_series *) xmalloc((n > 0 ? n : 1) * sizeof(*s));
+	dcplx *c = (dcplx *) xmalloc(((size_t) (n > 0 ? n : 1)) * length(l_max, polar) * sizeof(dcplx));
 	if(!a || !s || !c) {
 		free(a);
 		free(s);
@@ -778,10 +780,10 @@ extern "C" struct sh_series_array *sh_series_array_set_len(struct sh_series_arra
 {
 	if(n == a->n)
 		return a;
-	dcplx *c = (dcplx *) realloc(a->coeff, (size_t) (n > 0 ? n : 1) * a->stride * sizeof(dcplx));
+	dcplx *c = (dcplx *) xrealloc(a->coeff, (size_t) (n > 0 ? n : 1) * a->stride * sizeof(dcplx));
 	if(!c)
 		return NULL;
-	struct sh_series *s = (struct sh_series *) realloc(a->series, (n > 0 ? n : 1) * sizeof(*s));
+	struct sh_series *s = (struct sh_series *) xrealloc(a->series, (n > 0 ? n : 1) * sizeof(*s));
 	if(!s) {
 		a->coeff = c;
 		array_relink(a);
@@ -800,7 +802,7 @@ extern "C" struct sh_series_array *sh_series_array_set_len(struct sh_series_arra
 static struct sh_series_array *array_reshape(struct sh_series_array *a, unsigned l_max, int polar)
 {
 	const int stride = (int) length(l_max, polar);
-	dcplx *c = (dcplx *) malloc((size_t) (a->n > 0 ? a->n : 1) * stride * sizeof(dcplx));
+	dcplx *c = (dcplx *) xmalloc((size_t) (a->n > 0 ? a->n : 1) * stride * sizeof(dcplx));
 	if(!c)
 		return NULL;
 	for(int i = 0; i < a->n; i++) {

@@ -25,6 +25,7 @@
 // Condon-Shortley phase) and stored in the transform's arithmetic type.
 #include <cuda_runtime.h>
 
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -418,6 +419,7 @@ struct RecCoef {
 	double a, b, c;
 };
 
+template <bool H>
 __device__ void peak_eval_order(int L, int polar, const double2 *c, int m, double x, double st, double phi, const RecCoef *rc, const double *lnpre,
 				PeakEval &acc)
 {
@@ -437,22 +439,26 @@ __device__ void peak_eval_order(int L, int polar, const double2 *c, int m, doubl
 			lam = p;
 		}
 		const double d1 = (l * x * lam - k.c * lam_prev) * inv_s;
-		const double d2 = -cot * d1 - ((double) l * (l + 1) - m2s) * lam;
+		const double d2 = H ? -cot * d1 - ((double) l * (l + 1) - m2s) * lam : 0.0;
 		const double2 cp = c[polar ? l : lmoff(L, l, m)];
 		Ar += cp.x * lam;
 		Ai += cp.y * lam;
 		A1r += cp.x * d1;
 		A1i += cp.y * d1;
-		A2r += cp.x * d2;
-		A2i += cp.y * d2;
+		if(H) {
+			A2r += cp.x * d2;
+			A2i += cp.y * d2;
+		}
 		if(m > 0) {
 			const double2 cn = c[lmoff(L, l, -m)];
 			Br += cn.x * lam;
 			Bi += cn.y * lam;
 			B1r += cn.x * d1;
 			B1i += cn.y * d1;
-			B2r += cn.x * d2;
-			B2i += cn.y * d2;
+			if(H) {
+				B2r += cn.x * d2;
+				B2i += cn.y * d2;
+			}
 		}
 	}
 	if(m & 1) {
@@ -480,6 +486,7 @@ __device__ void peak_eval_order(int L, int polar, const double2 *c, int m, doubl
 	acc.ftp += -m * ImA1 + m * ImB1;
 }
 
+template <bool H>
 __device__ PeakEval peak_eval(int L, int polar, const double2 *c, double theta, double phi, const RecCoef *rc, const double *lnpre)
 {
 	PeakEval e = {0, 0, 0, 0, 0, 0};
@@ -491,17 +498,19 @@ __device__ PeakEval peak_eval(int L, int polar, const double2 *c, double theta, 
 	const int M = polar ? 0 : L;
 	// pair order k with M - k so lanes carry equal recurrence lengths
 	for(int k = lane; k <= M / 2; k += 32) {
-		peak_eval_order(L, polar, c, k, x, st, phi, rc, lnpre, e);
+		peak_eval_order<H>(L, polar, c, k, x, st, phi, rc, lnpre, e);
 		if(M - k != k)
-			peak_eval_order(L, polar, c, M - k, x, st, phi, rc, lnpre, e);
+			peak_eval_order<H>(L, polar, c, M - k, x, st, phi, rc, lnpre, e);
 	}
 	for(int o = 16; o; o >>= 1) {
 		e.f += __shfl_xor_sync(0xffffffffu, e.f, o);
 		e.ft += __shfl_xor_sync(0xffffffffu, e.ft, o);
 		e.fp += __shfl_xor_sync(0xffffffffu, e.fp, o);
-		e.ftt += __shfl_xor_sync(0xffffffffu, e.ftt, o);
-		e.ftp += __shfl_xor_sync(0xffffffffu, e.ftp, o);
-		e.fpp += __shfl_xor_sync(0xffffffffu, e.fpp, o);
+		if(H) {
+			e.ftt += __shfl_xor_sync(0xffffffffu, e.ftt, o);
+			e.ftp += __shfl_xor_sync(0xffffffffu, e.ftp, o);
+			e.fpp += __shfl_xor_sync(0xffffffffu, e.fpp, o);
+		}
 	}
 	return e;
 }
@@ -528,8 +537,228 @@ __device__ double ang_dist(double t1, double p1, double t2, double p2)
 	return atan2(sqrt(cx * cx + cy * cy + cz * cz), x1 * x2 + y1 * y2 + z1 * z2);
 }
 
+// ---------------------------------------------------------------------------
+// BFGS2 refinement, the minimiser the reference's extremizer drives (GSL's
+// gsl_multimin_fdfminimizer_vector_bfgs2, sh_series_extremize.c:273-360:
+// first step pi/24, line tolerance 0.001, at most 100 iterations, stop at
+// |gradient| < 1e-3), restated from the published algorithm GSL documents
+// for it: memoryless BFGS search directions (Shanno 1978) with the line
+// search of Fletcher, Practical Methods of Optimization (2nd ed.),
+// algorithms 2.6.2 (bracketing) and 2.6.4 (sectioning), rho = 0.01,
+// sigma = the line tolerance, tau1 = 9, tau2 = 0.05, tau3 = 0.5, trial
+// steps from the cubic (or, without phi' at the far end, quadratic)
+// interpolant of phi, and Fletcher's round-off stop.  One warp per series:
+// every lane holds the same state, the evaluation is warp-collective.
+//
+// The objective h(x) = -sign Re f at x = (theta, phi) brought back onto the
+// sphere (condition_tp).  Its gradient is either the derivatives in the
+// minimiser's own co-ordinates (d/dtheta, d/dphi) -- the localiser's
+// choice -- or, as the reference's dfunc() forms it, the components along
+// the unit vectors (d/dtheta, (1/sin theta) d/dphi), which makes the line
+// search's slope differ from the true one away from the equator.
+// ---------------------------------------------------------------------------
+struct PeakFdf {
+	int L, polar;
+	const double2 *c;
+	const RecCoef *rc;
+	const double *lnpre;
+	double sign;
+	bool unit_grad;
+	__device__ void operator()(const double *x, double &h, double *g) const
+	{
+		double t = x[0], p = x[1];
+		condition_tp(t, p);
+		const PeakEval e = peak_eval<false>(L, polar, c, t, p, rc, lnpre);
+		h = -sign * e.f;
+		g[0] = -sign * e.ft;
+		g[1] = -sign * (unit_grad ? e.fp / sin(t) : e.fp);
+	}
+};
+
+struct Bfgs2 {
+	double x[2], g[2], f;  // current point
+	double p[2];           // search direction
+	double pnorm, gnorm, fp0, delta_f, step, sigma;
+};
+
+__device__ __forceinline__ double dot2(const double *a, const double *b) { return a[0] * b[0] + a[1] * b[1]; }
+
+__device__ void bfgs2_steepest(Bfgs2 &s)
+{
+	s.gnorm = sqrt(dot2(s.g, s.g));
+	s.p[0] = s.gnorm > 0.0 ? -s.g[0] / s.gnorm : 0.0;
+	s.p[1] = s.gnorm > 0.0 ? -s.g[1] / s.gnorm : 0.0;
+	s.pnorm = sqrt(dot2(s.p, s.p));
+	s.fp0 = dot2(s.p, s.g);
+}
+
+// minimiser of the interpolating polynomial of phi on [a, b] (in alpha
+// units) over [lo, hi]; fpb NaN = phi' at b not known (quadratic)
+__device__ double bfgs2_interp(double a, double fa, double fpa, double b, double fb, double fpb, double lo, double hi)
+{
+	const double w = b - a;
+	double zlo = (lo - a) / w, zhi = (hi - a) / w;
+	if(zlo > zhi) {
+		const double t = zlo;
+		zlo = zhi;
+		zhi = t;
+	}
+	const double d0 = fpa * w, dF = fb - fa;
+	double c2, c3;
+	if(isnan(fpb)) {
+		c2 = dF - d0;
+		c3 = 0.0;
+	} else {
+		const double d1 = fpb * w;
+		c2 = 3.0 * dF - 2.0 * d0 - d1;
+		c3 = d0 + d1 - 2.0 * dF;
+	}
+	auto poly = [&](double z) { return fa + z * (d0 + z * (c2 + z * c3)); };
+	double zb = zlo, vb = poly(zlo), v = poly(zhi);
+	if(v < vb) {
+		zb = zhi;
+		vb = v;
+	}
+	double roots[2];
+	int nr = 0;
+	if(c3 == 0.0) {
+		if(c2 != 0.0)
+			roots[nr++] = -d0 / (2.0 * c2);
+	} else {
+		const double A = 3.0 * c3, B = 2.0 * c2, C = d0;
+		const double disc = B * B - 4.0 * A * C;
+		if(disc >= 0.0) {
+			const double sq = sqrt(disc);
+			const double q = -0.5 * (B + (B >= 0.0 ? sq : -sq));
+			if(q != 0.0) {
+				roots[nr++] = q / A;
+				roots[nr++] = C / q;
+			} else
+				roots[nr++] = -B / (2.0 * A);
+		}
+	}
+	for(int i = 0; i < nr; i++)
+		if(roots[i] > zlo && roots[i] < zhi) {
+			v = poly(roots[i]);
+			if(v < vb) {
+				zb = roots[i];
+				vb = v;
+			}
+		}
+	return a + zb * w;
+}
+
+template <class Fdf>
+__device__ void bfgs2_probe(const Bfgs2 &s, const Fdf &fdf, double alpha, double *xa, double &fa, double *ga, double &fpa)
+{
+	xa[0] = s.x[0] + alpha * s.p[0];
+	xa[1] = s.x[1] + alpha * s.p[1];
+	fdf(xa, fa, ga);
+	fpa = dot2(ga, s.p);
+}
+
+// Fletcher 2.6.2 + 2.6.4: true with the accepted point
+template <class Fdf>
+__device__ bool bfgs2_line(const Bfgs2 &s, const Fdf &fdf, double alpha1, double &alpha_out, double *xo, double &fo, double *go)
+{
+	const double rho = 0.01, sigma = s.sigma, tau1 = 9.0, tau2 = 0.05, tau3 = 0.5;
+	const double f0 = s.f, fp0 = s.fp0;
+	const double eps = DBL_EPSILON * fmax(fabs(f0), 1.0);
+	double alpha = alpha1, alpha_prev = 0.0, f_prev = f0, fp_prev = fp0;
+	double a = 0.0, fa = 0.0, fpa = 0.0, b = 0.0, fb = 0.0, fpb = NAN;
+	double xa[2], ga[2], fal, fpal;
+	bool bracketed = false;
+	for(int it = 0; it < 100; it++) {
+		bfgs2_probe(s, fdf, alpha, xa, fal, ga, fpal);
+		if(fal > f0 + alpha * rho * fp0 || fal >= f_prev) {
+			a = alpha_prev, fa = f_prev, fpa = fp_prev;
+			b = alpha, fb = fal, fpb = NAN;
+			bracketed = true;
+			break;
+		}
+		if(fabs(fpal) <= -sigma * fp0) {
+			xo[0] = xa[0], xo[1] = xa[1], go[0] = ga[0], go[1] = ga[1], fo = fal;
+			alpha_out = alpha;
+			return true;
+		}
+		if(fpal >= 0.0) {
+			a = alpha, fa = fal, fpa = fpal;
+			b = alpha_prev, fb = f_prev, fpb = fp_prev;
+			bracketed = true;
+			break;
+		}
+		const double delta = alpha - alpha_prev;
+		const double next = bfgs2_interp(alpha_prev, f_prev, fp_prev, alpha, fal, fpal, alpha + delta, alpha + tau1 * delta);
+		alpha_prev = alpha, f_prev = fal, fp_prev = fpal;
+		alpha = next;
+	}
+	if(!bracketed)
+		return false;
+	for(int it = 0; it < 100; it++) {
+		const double delta = b - a;
+		alpha = bfgs2_interp(a, fa, fpa, b, fb, fpb, a + tau2 * delta, b - tau3 * delta);
+		if((a - alpha) * fpa <= eps)
+			return false;  // round-off prevents further progress
+		bfgs2_probe(s, fdf, alpha, xa, fal, ga, fpal);
+		if(fal > f0 + rho * alpha * fp0 || fal >= fa) {
+			b = alpha, fb = fal, fpb = NAN;
+		} else {
+			if(fabs(fpal) <= -sigma * fp0) {
+				xo[0] = xa[0], xo[1] = xa[1], go[0] = ga[0], go[1] = ga[1], fo = fal;
+				alpha_out = alpha;
+				return true;
+			}
+			if(delta * fpal >= 0.0)
+				b = a, fb = fa, fpb = fpa;
+			a = alpha, fa = fal, fpa = fpal;
+		}
+	}
+	return false;
+}
+
+// one iteration: false when no progress is possible (state unchanged)
+template <class Fdf>
+__device__ bool bfgs2_iterate(Bfgs2 &s, const Fdf &fdf)
+{
+	if(s.pnorm == 0.0 || s.gnorm == 0.0 || s.fp0 == 0.0)
+		return false;
+	double alpha1;
+	if(s.delta_f < 0.0) {
+		const double del = fmax(-s.delta_f, 10.0 * DBL_EPSILON * fabs(s.f));
+		alpha1 = fmin(1.0, 2.0 * del / (-s.fp0));
+	} else
+		alpha1 = fabs(s.step);
+	double x1[2], g1[2], f1, alpha;
+	if(!bfgs2_line(s, fdf, alpha1, alpha, x1, f1, g1))
+		return false;
+	double sv[2] = {alpha * s.p[0], alpha * s.p[1]};
+	double yv[2] = {g1[0] - s.g[0], g1[1] - s.g[1]};
+	s.delta_f = f1 - s.f;
+	s.x[0] = x1[0], s.x[1] = x1[1], s.g[0] = g1[0], s.g[1] = g1[1], s.f = f1;
+	const double sg = dot2(sv, g1), yg = dot2(yv, g1), sy = dot2(sv, yv), yy = dot2(yv, yv);
+	double A = 0.0, B = 0.0;
+	if(sy != 0.0) {
+		B = sg / sy;
+		A = -(1.0 + yy / sy) * B + yg / sy;
+	}
+	s.p[0] = -(g1[0] - A * sv[0] - B * yv[0]);
+	s.p[1] = -(g1[1] - A * sv[1] - B * yv[1]);
+	s.gnorm = sqrt(dot2(g1, g1));
+	s.pnorm = sqrt(dot2(s.p, s.p));
+	s.fp0 = dot2(s.p, g1);
+	if(!(s.fp0 < 0.0))
+		bfgs2_steepest(s);
+	return true;
+}
+
+// method 0: trust-region Newton (tol: smallest step); 1: BFGS2 with the
+// gradient in the co-ordinates; 2: BFGS2 as the reference's extremizer
+// runs it (unit-vector gradient components, co-ordinates returned
+// unconditioned).  The BFGS2 methods stop at |gradient| < 1e-3 as the
+// reference does.
 __global__ void k_peak_refine(int S, int L, int polar, const double2 *coeff, long long cstride, const double *theta0, const double *phi0, double sign,
-			      int max_iter, double tol, double *out /* [S][4] */, int *status, const RecCoef *rc_g, const double *lnpre_g, int n_rc)
+			      int max_iter, double tol, double *out /* [S][4] */, int *status, const RecCoef *rc_g, const double *lnpre_g, int n_rc,
+			      int method)
 {
 	// the tables in shared memory when they fit (n_rc > 0), else read
 	// from global memory
@@ -559,10 +788,50 @@ __global__ void k_peak_refine(int S, int L, int polar, const double2 *coeff, lon
 		}
 		return;
 	}
+	if(method != 0) {
+		const PeakFdf fdf{L, polar, c, rc, lnpre, sign, method == 2};
+		double tc = t, pc = p;
+		condition_tp(tc, pc);
+		Bfgs2 bs;
+		bs.x[0] = t;
+		bs.x[1] = p;
+		fdf(bs.x, bs.f, bs.g);
+		bfgs2_steepest(bs);
+		bs.delta_f = 0.0;
+		bs.step = M_PI / 24;
+		bs.sigma = 1e-3;
+		int it = 0, converged = 0;
+		// converged: stopped by the gradient test, or where no step makes
+		// progress any more (the line search's round-off stop), as the
+		// reference's loop ends; not at the iteration limit
+		while(it < max_iter) {
+			if(!bfgs2_iterate(bs, fdf)) {
+				converged = 1;
+				break;
+			}
+			it++;
+			if(sqrt(dot2(bs.g, bs.g)) < 1e-3) {
+				converged = 1;
+				break;
+			}
+		}
+		double tf = bs.x[0], pf = bs.x[1], tcf = tf, pcf = pf;
+		condition_tp(tcf, pcf);
+		if(method == 1)
+			tf = tcf, pf = pcf;
+		if((threadIdx.x & 31) == 0) {
+			out[4 * s + 0] = tf;
+			out[4 * s + 1] = pf;
+			out[4 * s + 2] = -sign * bs.f;
+			out[4 * s + 3] = ang_dist(tc, pc, tcf, pcf);
+			status[s] = converged | (it << 1);
+		}
+		return;
+	}
 	condition_tp(t, p);
 	const double ts = t, ps = p;
 	double radius = M_PI / 24;
-	PeakEval e = peak_eval(L, polar, c, t, p, rc, lnpre);
+	PeakEval e = peak_eval<true>(L, polar, c, t, p, rc, lnpre);
 	double g = sign * e.f;
 	int it = 0, converged = 0;
 	for(; it < max_iter; it++) {
@@ -594,7 +863,7 @@ __global__ void k_peak_refine(int S, int L, int polar, const double2 *coeff, lon
 		}
 		double tn = t + du, pn = p + dv / st;
 		condition_tp(tn, pn);
-		const PeakEval en = peak_eval(L, polar, c, tn, pn, rc, lnpre);
+		const PeakEval en = peak_eval<true>(L, polar, c, tn, pn, rc, lnpre);
 		const double gn = sign * en.f;
 		if(gn >= g) {
 			// a short step that no longer raises the value is at the
@@ -673,10 +942,66 @@ struct DevBuf {
 	template <class T> T *as() const { return (T *) p; }
 };
 
+// ---------------------------------------------------------------------------
+// azimuthal synthesis on a HEALPix ring grid, one block per (ring, series):
+// Re sum_m F_m e^{i m phi_j} at the ring's own pixel longitudes (see
+// ring_npix / ring_first_pixel), by Horner's rule in e^{i phi_j}; e^{i phi_j}
+// and e^{-i M phi_j} from FP64 sincospi of the exact phase fractions.  Out:
+// float [S][12 nside^2] in RING order.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_ring_pix(int N, int nt, int M, const typename V2<T>::t *F, float *out)
+{
+	typedef typename V2<T>::t T2;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int W = 2 * M + 1;
+	T2 *Fs = (T2 *) smem_raw;
+	const long long row = blockIdx.x;  // series * nt + ring - 1
+	const int s = (int) (row / nt);
+	const int i = (int) (row % nt) + 1;
+	for(int k = threadIdx.x; k < W; k += blockDim.x)
+		Fs[k] = F[row * W + k];
+	__syncthreads();
+	int np, den;
+	double off;
+	if(i < N || i > 3 * N) {
+		const int k = i < N ? i : 4 * N - i;
+		np = 4 * k;
+		den = 2 * k;
+		off = 0.5;
+	} else {
+		np = 4 * N;
+		den = 2 * N;
+		off = ((i + N) & 1) ? 0.0 : 0.5;
+	}
+	const long long first = i <= N ? 2LL * i * (i - 1)
+				       : (i <= 3 * N ? 2LL * N * (N - 1) + 4LL * N * (i - N) : 12LL * N * N - 2LL * (4 * N - i + 1) * (4 * N - i));
+	float *o = out + (long long) s * 12 * N * N + first;
+	for(int j = threadIdx.x; j < np; j += blockDim.x) {
+		// phi_j / pi = (j + off) / den
+		const double fr = (j + off) / den;
+		double sn, cs;
+		sincospi(fr, &sn, &cs);
+		const T zr = (T) cs, zi = (T) sn;
+		T vr = Fs[W - 1].x, vi = Fs[W - 1].y;
+		for(int k = W - 2; k >= 0; k--) {
+			const T2 f = Fs[k];
+			const T nr = vr * zr - vi * zi + f.x;
+			const T ni = vr * zi + vi * zr + f.y;
+			vr = nr;
+			vi = ni;
+		}
+		// times e^{-i M phi_j}
+		sincospi(fmod(M * fr, 2.0), &sn, &cs);
+		o[j] = (float) ((double) vr * cs + (double) vi * sn);
+	}
+}
+
 struct ShtPlan {
 	unsigned L = 0;       // table l_max
-	int kind = 0;         // kGridGL or kGridEquiangular
+	int kind = 0;         // kGridGL, kGridEquiangular or kGridRing
 	int nt = 0, nphi = 0;
+	int nside = 0;        // kGridRing: HEALPix nside (nt = 4 nside - 1 rings)
 	int fp32 = 0;
 	std::vector<double> theta;  // row co-latitudes (increasing)
 	double *d_x = nullptr;      // cos theta_i
@@ -700,11 +1025,23 @@ void *sht_plan_create(unsigned L, int kind, int nt, int nphi, int fp32)
 {
 	if(ensure_device())
 		return nullptr;
+	int nside_of_ring_plan = 0;
+	if(kind == kGridRing) {
+		// nt carries nside: 4 nside - 1 rings, at most 4 nside pixels each
+		if(nt < 1 || nt > 2048) {
+			set_error("sht plan: HEALPix nside %d outside 1 .. 2048", nt);
+			return nullptr;
+		}
+		nside_of_ring_plan = nt;
+		nphi = 4 * nt;
+		nt = 4 * nt - 1;
+	}
 	if(nt < 1 || nphi < 1 || nt > 8192 || nphi > 8192 || L > 2048) {
 		set_error("sht plan: bad grid %d x %d or l_max %u", nt, nphi, L);
 		return nullptr;
 	}
 	ShtPlan *p = new ShtPlan;
+	p->nside = nside_of_ring_plan;
 	p->L = L;
 	p->kind = kind;
 	p->nt = nt;
@@ -716,6 +1053,22 @@ void *sht_plan_create(unsigned L, int kind, int nt, int nphi, int fp32)
 		gl_nodes(nt, x.data(), w.data());  // decreasing x = increasing theta
 		for(int i = 0; i < nt; i++)
 			p->theta[i] = acos(x[i]);
+	} else if(kind == kGridRing) {
+		const int N = p->nside;
+		for(int r = 0; r < nt; r++) {
+			const int i = r + 1;
+			double z;
+			if(i < N)
+				z = 1.0 - (double) i * i / (3.0 * N * N);
+			else if(i <= 3 * N)
+				z = (4.0 * N - 2.0 * i) / (3.0 * N);
+			else {
+				const int k = 4 * N - i;
+				z = -(1.0 - (double) k * k / (3.0 * N * N));
+			}
+			x[r] = z;
+			p->theta[r] = acos(z);
+		}
 	} else {
 		for(int i = 0; i < nt; i++) {
 			p->theta[i] = M_PI * (i + 0.5) / nt;
@@ -798,6 +1151,27 @@ int sht_synthesis(void *plan, const void *coeff, int S, long long cstride, unsig
 	const int W = 2 * M + 1;
 	const int thr = pix_threads(p->nphi);
 	const unsigned grid = (unsigned) p->nt * (unsigned) S;
+	if(p->kind == kGridRing) {
+		if(out_kind != kPixReal) {
+			set_error("sht synthesis: HEALPix ring grids give real maps only");
+			return -1;
+		}
+		if((size_t) W * (p->fp32 ? sizeof(float2) : sizeof(double2)) > kMaxDynSmem) {
+			set_error("sht synthesis: l_max %u too large for a ring grid", Luse);
+			return -1;
+		}
+		if(p->fp32) {
+			if(launch_F<float>(p, (const double2 *) coeff, cstride, L_in, polar, Luse, M, S, scratch, st))
+				return -1;
+			k_ring_pix<float><<<grid, thr, (size_t) W * sizeof(float2), st>>>(p->nside, p->nt, M, (const float2 *) scratch, (float *) out);
+		} else {
+			if(launch_F<double>(p, (const double2 *) coeff, cstride, L_in, polar, Luse, M, S, scratch, st))
+				return -1;
+			k_ring_pix<double><<<grid, thr, (size_t) W * sizeof(double2), st>>>(p->nside, p->nt, M, (const double2 *) scratch, (float *) out);
+		}
+		CK(cudaGetLastError());
+		return 0;
+	}
 	if((size_t) (p->nphi + W) * (p->fp32 ? sizeof(float2) : sizeof(double2)) > kMaxDynSmem) {
 		set_error("sht synthesis: grid of %d columns too wide", p->nphi);
 		return -1;
@@ -1019,9 +1393,25 @@ static int rec_table(unsigned L, RecTable *out)
 	return 0;
 }
 
-int peak_refine(int S, unsigned L, int polar, const void *coeff, long long cstride, const double *theta0, const double *phi0, double sign, int max_iter,
-		double tol, double *out, int *status, void *stream)
+static int g_refine_method = 1;
+
+int peak_refine_method() { return g_refine_method; }
+
+int set_peak_refine_method(int method)
 {
+	if(method < 0 || method > 1) {
+		set_error("refinement method %d: 0 (trust-region Newton) or 1 (BFGS2)", method);
+		return -1;
+	}
+	g_refine_method = method;
+	return 0;
+}
+
+int peak_refine(int S, unsigned L, int polar, const void *coeff, long long cstride, const double *theta0, const double *phi0, double sign, int max_iter,
+		double tol, double *out, int *status, void *stream, int method)
+{
+	if(method < 0)
+		method = g_refine_method;
 	cudaStream_t st = stream ? (cudaStream_t) stream : lstream();
 	if(S <= 0)
 		return 0;
@@ -1034,7 +1424,7 @@ int peak_refine(int S, unsigned L, int polar, const void *coeff, long long cstri
 		sm = 0;
 	const int wpb = 4;
 	k_peak_refine<<<(S + wpb - 1) / wpb, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out,
-								  status, t.rc, t.lnpre, staged ? t.n : 0);
+								  status, t.rc, t.lnpre, staged ? t.n : 0, method);
 	CK(cudaGetLastError());
 	return 0;
 }

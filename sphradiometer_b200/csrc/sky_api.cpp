@@ -4,6 +4,8 @@
 
 #include <cuda_runtime_api.h>
 
+#include <cmath>
+
 #include "abi_common.h"
 
 using namespace sphrad;
@@ -16,15 +18,17 @@ struct sphrad_sky_grid {
 	void *plan;
 	unsigned l_max;
 	int nt, nphi, fp32;
+	int nside;  // HEALPix ring grids, else 0
 };
 
 extern "C" sphrad_sky_grid *sphrad_sky_grid_new(unsigned l_max, int kind, int ntheta, int nphi, int fp32)
 {
-	if(kind != SPHRAD_GRID_GL && kind != SPHRAD_GRID_CELL) {
+	if(kind != SPHRAD_GRID_GL && kind != SPHRAD_GRID_CELL && kind != SPHRAD_GRID_HEALPIX) {
 		set_error("sphrad_sky_grid_new: unknown grid kind %d", kind);
 		return NULL;
 	}
-	void *p = sht_plan_create(l_max, kind == SPHRAD_GRID_GL ? kGridGL : kGridEquiangular, ntheta, nphi, fp32);
+	const int gk = kind == SPHRAD_GRID_GL ? kGridGL : (kind == SPHRAD_GRID_CELL ? kGridEquiangular : kGridRing);
+	void *p = sht_plan_create(l_max, gk, ntheta, kind == SPHRAD_GRID_HEALPIX ? 1 : nphi, fp32);
 	if(!p)
 		return NULL;
 	sphrad_sky_grid *g = (sphrad_sky_grid *) malloc(sizeof(*g));
@@ -32,8 +36,28 @@ extern "C" sphrad_sky_grid *sphrad_sky_grid_new(unsigned l_max, int kind, int nt
 		sht_plan_destroy(p);
 		return NULL;
 	}
-	*g = {p, l_max, ntheta, nphi, fp32 ? 1 : 0};
+	if(kind == SPHRAD_GRID_HEALPIX)
+		*g = {p, l_max, 4 * ntheta - 1, 4 * ntheta, fp32 ? 1 : 0, ntheta};
+	else
+		*g = {p, l_max, ntheta, nphi, fp32 ? 1 : 0, 0};
 	return g;
+}
+
+extern "C" long long sphrad_sky_grid_pixels(const sphrad_sky_grid *g)
+{
+	return g->nside ? 12LL * g->nside * g->nside : (long long) g->nt * g->nphi;
+}
+
+// sh_series_healpix.cc:220-238 (lmax2nside): the smallest power of two not
+// below ceil(l_max / 2 + 0.75), so that the map has at least the 2 (l_max +
+// 1) rings of the harmonic transform
+extern "C" int sphrad_healpix_nside(unsigned l_max)
+{
+	const double want = ceil(l_max / 2.0 + 0.75);
+	for(int n = 1; n > 0; n <<= 1)
+		if(n >= want)
+			return n;
+	return -1;
 }
 
 extern "C" void sphrad_sky_grid_free(sphrad_sky_grid *g)
@@ -83,6 +107,10 @@ extern "C" int sphrad_sky_grid_argmax(sphrad_sky_grid *g, const void *sky, int n
 		return 0;
 	if(check_scratch(g, n_sky, scratch_bytes))
 		return -1;
+	if(g->nside) {
+		set_error("sphrad_sky_grid_argmax: not available on HEALPix ring grids");
+		return -1;
+	}
 	unsigned Luse = l_use < sky_l_max ? l_use : sky_l_max;
 	if(Luse > g->l_max)
 		Luse = g->l_max;
@@ -92,6 +120,10 @@ extern "C" int sphrad_sky_grid_argmax(sphrad_sky_grid *g, const void *sky, int n
 		return -1;
 	return sht_rows_argmax(g->plan, n_sky, rb, theta, phi, nullptr, caller_stream(stream));
 }
+
+extern "C" int sphrad_sky_set_refinement(int method) { return set_peak_refine_method(method); }
+
+extern "C" int sphrad_sky_refinement(void) { return peak_refine_method(); }
 
 extern "C" int sphrad_sky_refine_peaks(const void *sky, int n_sky, unsigned sky_l_max, const double *theta0, const double *phi0, double *out, int *status,
 				       void *stream)

@@ -44,9 +44,10 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity)
 	return ok != 0;
 }
 
-// bounded wait: false on timeout (sets the abort flag and the error word)
-// or when another role has aborted
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag, unsigned *err, unsigned code)
+// bounded wait: false on timeout after limit clock cycles (sets the abort
+// flag and the error word) or when another role has aborted
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag, unsigned *err, unsigned code,
+					  unsigned long long limit = kWaitCycles)
 {
 	const unsigned long long t0 = clock64();
 	while(true) {
@@ -54,7 +55,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
 			return true;
 		if(*abort_flag)
 			return false;
-		if(clock64() - t0 > kWaitCycles) {
+		if(clock64() - t0 > limit) {
 			*abort_flag = 1;
 			atomicExch(err, code);
 			return false;
@@ -63,10 +64,10 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
 }
 
 // bounded wait that ignores the abort flag (draining copies in flight)
-__device__ __forceinline__ void mbar_drain(uint32_t bar, uint32_t parity)
+__device__ __forceinline__ void mbar_drain(uint32_t bar, uint32_t parity, unsigned long long limit = kWaitCycles)
 {
 	const unsigned long long t0 = clock64();
-	while(!mbar_try(bar, parity) && clock64() - t0 < kWaitCycles) {
+	while(!mbar_try(bar, parity) && clock64() - t0 < limit) {
 	}
 }
 

@@ -141,3 +141,17 @@ def test_library_wigner_3j_against_exact_values(S):
         assert abs(got - O.wigner_3j(*args)) <= 1e-13 * max(abs(ref), 1e-3)
     for args in [(80, 60, 50, 3, -7, 4), (96, 48, 48, 0, 12, -12), (59, 59, 30, 20, -25, 5)]:
         assert abs(L.sh_series_wigner_3j(*args) - O.wigner_3j(*args)) <= 1e-12 * max(abs(O.wigner_3j(*args)), 1e-6)
+
+
+def test_healpix_nside_follows_the_reference_rule():
+    """sphrad_healpix_nside: lmax2nside of sh_series_healpix.cc:220-238, the
+    smallest power of two not below ceil(l_max / 2 + 0.75)."""
+    import math
+    import sphradiometer_b200 as S
+    lib = S.load()
+    for L in range(0, 300):
+        want = 1
+        while want < math.ceil(L / 2.0 + 0.75):
+            want *= 2
+        assert lib.sphrad_healpix_nside(L) == want, L
+    assert lib.sphrad_healpix_nside(32) == 32 and lib.sphrad_healpix_nside(25) == 16
