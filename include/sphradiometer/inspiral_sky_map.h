@@ -7,10 +7,11 @@
  * library load without recomputing delay tables.
  *
  * Provided: the directory tree, the time-series length, the network
- * baselines and the positive- / negative-frequency correlator plans.  The
- * FITS parts of the cache (log prior, autocorrelator projections) and the
- * rest of the inspiral module (LAL frame I/O, projection operators, sky
- * generation) are not part of this library.
+ * baselines and the positive- / negative-frequency correlator plans, and
+ * the projection operator correlator_network_plan_mult_by_projection.  The
+ * FITS parts of the cache (log prior, autocorrelator projections) and LAL
+ * frame I/O are not part of this library; sky generation over plain arrays
+ * is sphrad_generate_alm_skys (sphradiometer_b200.h).
  *
  * Differences from the reference: a baseline whose cached direction does
  * not match the instruments fails the whole read (the reference leaves a
@@ -40,6 +41,16 @@ struct correlator_network_baselines *read_precalc_correlator_network_baselines(c
  * plans' cross-spectrum scratch */
 int read_precalc_correlator_network_plan_fd(struct correlator_network_plan_fd *fdplansp, struct correlator_network_plan_fd *fdplansn,
 					    const struct correlator_network_baselines *baselines, int tseries_length, char *parent_dir);
+
+/* reference inspiral_sky_map.h:52, inspiral_sky_map.c:423-549: multiply
+ * every frequency bin j of every baseline's delay kernel by the projection
+ * operator of the network's detectors for polarisation ratio beta and angle
+ * psi, weighted by psd[j][k] (bin j, detector k); the instruments must
+ * carry their LALDetector as data (instrument_new_from_LALDetector).  The
+ * antenna patterns follow LAL's XLALComputeDetAMResponse at gmst 0; the
+ * work runs on the GPU as in sphrad_network_plan_mult_by_projection.
+ * 0 on success, -1 on failure. */
+int correlator_network_plan_mult_by_projection(struct correlator_network_plan_fd *plan, double beta, double psi, double **psd);
 
 #ifdef __cplusplus
 }

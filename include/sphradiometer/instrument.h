@@ -8,9 +8,9 @@
  * gsl_block / gsl_vector is provided so the structs below keep the
  * reference's memory layout.  Vectors this library allocates use
  * malloc() for the gsl_vector, its gsl_block and the data, with
- * owner = 1, so GSL's gsl_vector_free() can release them.  The LAL
- * constructors (instrument_new_from_LALDetector, instrument_new_from_name)
- * are not provided: LAL is outside this library.
+ * owner = 1, so GSL's gsl_vector_free() can release them.
+ * instrument_new_from_name is not provided: it needs LAL's table of named
+ * detectors, which is outside this library.
  */
 #ifndef SPHRADIOMETER_B200_INSTRUMENT_H
 #define SPHRADIOMETER_B200_INSTRUMENT_H
@@ -41,6 +41,24 @@ typedef struct {
 #endif
 #endif
 
+/* LAL's detector description (lal/LALDetectors.h), which the reference's
+ * instruments carry in their data pointer (instrument.c:175-181): LAL's own
+ * header when it is available, otherwise a declaration of its leading
+ * members with LAL's layout (vertex location in metres, response tensor),
+ * the only ones this library reads. */
+#if defined(__has_include)
+#if __has_include(<lal/LALDetectors.h>)
+#include <lal/LALDetectors.h>
+#define SPHRAD_B200_HAVE_LAL 1
+#endif
+#endif
+#ifndef SPHRAD_B200_HAVE_LAL
+typedef struct tagLALDetector {
+	double location[3];
+	float response[3][3];
+} LALDetector;
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -65,6 +83,9 @@ struct instrument *instrument_new(double, double, double, void *);
 void instrument_free(struct instrument *);
 struct instrument *instrument_copy(const struct instrument *);
 struct instrument *instrument_new_from_r_theta_phi(double, double, double, void *);
+/* reference instrument.h:101, instrument.c:175-181: phase centre = the
+ * detector's vertex / c; the instrument borrows det as its data */
+struct instrument *instrument_new_from_LALDetector(LALDetector *);
 
 struct instrument_array *instrument_array_new(int);
 int instrument_array_len(const struct instrument_array *);

@@ -76,15 +76,20 @@ int sphrad_batch_integrate(sphrad_batch_plan *plan, const void *fseries, int n_s
  *
  * Its split-K scratch is a static 8 MiB array inside the library, held by
  * every GPU that loads the library until the process exits; a call needing
- * more (n_seg above 8 MiB / (n_baselines * round_up(l_max + 1, 4) * 4 B),
- * about 19,000 segments for 3 baselines at l_max = 32, half that for
- * SPHRAD_PREC_FP64) is refused with -1 and a message.  Each call zero-fills
- * the part it uses before launching.  All calls share the array, so calls
- * that overlap on the GPU (other streams, other threads) race and must be
- * serialised by the caller.  The first call on each device looks up the
- * array's device address (cudaGetSymbolAddress); make that first call
- * before any stream capture.  Arguments are those of
- * sphrad_batch_integrate. */
+ * more is refused with -1 and a message that gives this plan's limit.  The
+ * scratch of n_seg segments is n_seg * n_baselines * round_up(l_max + 1, 4)
+ * elements (4 bytes, 8 for SPHRAD_PREC_FP64), times up to 16 copies for the
+ * tcgen05 precisions when n_seg is below 16 * 128 (fewer segments spread
+ * their partial sums over copies); that stays within the array, and the
+ * limit is about 19,000 segments for 3 baselines at l_max = 32.  Each call
+ * zero-fills the part it uses before launching.  All calls share the
+ * array, so calls that overlap on the GPU (other streams, other threads)
+ * race and must be serialised by the caller.  The first call on each
+ * device looks up the array's device address (cudaGetSymbolAddress), and
+ * so does the first call after the device's context changed (a reset);
+ * make those calls before any stream capture.  Arguments are those of
+ * sphrad_batch_integrate, for plans of polar (non-rotating) baselines only:
+ * plans of projected, non-polar kernels are refused. */
 int sphrad_batch_integrate_noalloc(sphrad_batch_plan *plan, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky, void *cuda_stream);
 
 /* sphrad_batch_integrate with a split-K factor (0: the tuned or default
@@ -224,6 +229,13 @@ int sphrad_batch_integrate_tseries(sphrad_batch_plan *plan, sphrad_fseries_plan 
  * detector k.  All baselines must share L and n.  0 on success, -1 on
  * failure (the plan is unchanged up to the failing baseline). */
 int sphrad_network_plan_mult_by_projection(struct correlator_network_plan_fd *plan, double beta, const double *fplus, const double *fcross, double **psd);
+/* F+ and Fx of a detector with response tensor D (LALDetector.response) for
+ * a wave from right ascension ra, declination dec at polarisation angle psi
+ * and Greenwich sidereal time gmst -- LAL's XLALComputeDetAMResponse, the
+ * formulas of Anderson et al., Phys. Rev. D 63, 042003 (2001), app. B, which
+ * correlator_network_plan_mult_by_projection (inspiral_sky_map.h) evaluates
+ * on the mesh.  Host arithmetic; returns 0. */
+int sphrad_antenna_response(double *fplus, double *fcross, const float D[3][3], double ra, double dec, double psi, double gmst);
 
 /* Sky maps of the inspiral path, generate_alm_skys (inspiral_sky_map.c:
  * 942-1101) with generate_alm_sky (:869-939), over plain arrays instead of

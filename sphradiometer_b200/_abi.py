@@ -168,6 +168,9 @@ SIGNATURES = {
     "projection_matrix_delay": (_P(sh_series_array), [_u, _u, _P(gsl_vector), _d]),
     "projection_delay_element": (_d, [_d, _d, _vp]),
     "sphrad_network_plan_mult_by_projection": (_i, [_P(correlator_network_plan_fd), _d, _vp, _vp, _vp]),
+    "correlator_network_plan_mult_by_projection": (_i, [_P(correlator_network_plan_fd), _d, _d, _vp]),
+    "sphrad_antenna_response": (_i, [_vp, _vp, _vp, _d, _d, _d, _d]),
+    "instrument_new_from_LALDetector": (_P(instrument), [_vp]),
     # precalculated plans on disk
     "make_precalc_directories": (_i, [C.c_char_p, _i]),
     "write_precalc_time_series_length": (_i, [_u, C.c_char_p]),
@@ -267,7 +270,11 @@ def load():
             raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m sphradiometer_b200.build`")
         L = C.CDLL(LIB_PATH)
         for name, (res, args) in SIGNATURES.items():
-            f = getattr(L, name)
+            # a symbol this build lacks fails where it is called, not here
+            # (tests/test_abi_cpu.py checks that every declared one exists)
+            f = getattr(L, name, None)
+            if f is None:
+                continue
             f.restype = res
             f.argtypes = args
         _lib = L

@@ -71,6 +71,15 @@ constexpr int CC_KC = 16;                // bins per CUDA-core stage
 constexpr int kMaxChain = 64;            // most pipeline stages one tcgen05 CTA accumulates
 }  // namespace
 
+// Programmatic dependent launch: a contraction lets the grid launched after
+// it (its epilogue) be scheduled once its own set-up is done, and waits for
+// the grid before it (which may write its inputs or read its workspace)
+// only after that set-up; the epilogue loads its tables, then waits for the
+// contraction before it reads the partial sums.  Without the launch
+// attribute both instructions return at once.
+__device__ __forceinline__ void pdl_allow_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait_prior() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ------------------------------------------------------------------------
 // tcgen05 contraction
 // ------------------------------------------------------------------------
@@ -83,8 +92,31 @@ struct EpArgs {
 	const void *W;          // [B][nq] complex T: weight / n * D_b^l_{0 m}
 	const double *gmst;     // [S] or NULL
 	const float *segw;      // [S][B] extra per-segment baseline factors, or NULL
-	double2 *sky;           // [S][nq]
+	double2 *sky;           // [S][nq], or see out_row
+	// packed outputs: segment s's sky at sky + out_row[s] in the layout of
+	// l_max seg_L[s] <= L (coefficients above it dropped); NULL: [S][nq]
+	const long long *out_row;
+	const unsigned *seg_L;
+	int accumulate;         // add into the outputs (FP64 atomics) instead of storing
 };
+
+__device__ __forceinline__ long long d_lmoff(int L, int l, int m)
+{
+	const long long LL = (long long) L + 1;
+	const long long x = (long long) m * (m - 1);
+	const long long mo = (m >= 0) ? LL * m - x / 2 : LL * (LL + m) + x / 2;
+	return mo + l - (m < 0 ? -m : m);
+}
+
+// one output coefficient: stored, or added by FP64 atomics
+__device__ __forceinline__ void ep_put(double2 *p, double re, double im, int accumulate)
+{
+	if(accumulate) {
+		atomicAdd(&p->x, re);
+		atomicAdd(&p->y, im);
+	} else
+		*p = make_double2(re, im);
+}
 
 struct TcArgs {
 	int S, n_det, B, Kst, tiles, npad, tmem_cols, accstride;
@@ -100,7 +132,16 @@ struct TcArgs {
 	unsigned *err;
 	unsigned long long wait;  // bound of every wait, clock cycles
 	int hold;              // failure-detection tests: stage of CTA 0's range whose spectra are never loaded (-1: none)
+	// indexed spectra (IDX): row s of the batch, detector d, bin k is
+	// rows[row_off[s] + det_off[d] + k], k < Ku -- segments anywhere in a
+	// packed array, no tensor map
+	const double2 *rows;
+	const long long *row_off;
+	int det_off[3];
+	int Ku;
 };
+
+constexpr int IDX_RP = 144;  // bytes per segment row in the indexed spectra ring (8 bins + 16 B pad: conflict-free)
 
 // Split the complex value (re, im) into NPART packed bf16x2 words (re in the
 // low half): part q is the round-to-nearest bf16 of what parts 0..q-1 left,
@@ -166,7 +207,7 @@ struct PieceCursor {
 	}
 };
 
-template <int NPART, int NFS, int NABS, int NBS, bool ATM>
+template <int NPART, int NFS, int NABS, int NBS, bool ATM, bool IDX = false>
 __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_constant__ CUtensorMap tmF, const __grid_constant__ TcArgs a)
 {
 	extern __shared__ uint8_t smem_raw[];
@@ -174,7 +215,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	// through it stay shared-memory accesses (an integer round trip would
 	// make them generic)
 	uint8_t *smem = smem_raw + ((1024 - ((uintptr_t) smem_raw & 1023)) & 1023);
-	const int f_slab = TM * 128;
+	const int f_slab = TM * (IDX ? IDX_RP : 128);
 	const int f_stage = a.n_det * f_slab;
 	const int btile = a.npad * KE * 2;
 	const int ab_bytes = a.B * NPART * btile;
@@ -227,8 +268,43 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	__syncthreads();
 	tc_fence_after();
 	const uint32_t tmem = *tslot;
+	pdl_allow_dependents();
+	pdl_wait_prior();
 
-	if(warp == 0) {
+	if(warp == 0 && IDX) {
+		// ---------------- producer: indexed spectra ----------------
+		// one bulk copy per (detector, segment row) of the stage's bins
+		// present in the row, the whole warp issuing them after lane 0
+		// has declared the stage's bytes
+		int issued = 0;
+		for(int it = 0; it < nst; it++) {
+			const int u = u0 + it;
+			const int fs = it % NFS;
+			const bool ok = mbar_wait(smem_u32(&f_empty[fs]), ((it / NFS) & 1) ^ 1, abort_flag, a.err, 1, a.wait);
+			if(!__all_sync(0xffffffffu, ok))
+				break;
+			const int t = u / a.Kst, k0 = (u % a.Kst) * KB;
+			const int nb = a.Ku - k0 < KB ? a.Ku - k0 : KB;
+			const int nrow = a.S - t * TM < TM ? a.S - t * TM : TM;
+			const uint32_t bytes = (uint32_t) nb * 16u;
+			if(it == a.hold && blockIdx.x == 0) {
+				issued = it + 1;
+				continue;
+			}
+			if(lane == 0)
+				mbar_arrive_tx(smem_u32(&f_full[fs]), (uint32_t) (nrow * a.n_det) * bytes);
+			__syncwarp();
+			for(int q = lane; q < nrow * a.n_det; q += 32) {
+				const int d = q / nrow, r = q - d * nrow;
+				const double2 *src = a.rows + a.row_off[t * TM + r] + a.det_off[d] + k0;
+				bulk_g2s(smem_u32(sF + fs * f_stage + d * f_slab + r * IDX_RP), src, bytes, smem_u32(&f_full[fs]));
+			}
+			issued = it + 1;
+		}
+		if(lane == 0)
+			for(int it = (issued > NFS ? issued - NFS : 0); it < issued; it++)
+				mbar_drain(smem_u32(&f_full[it % NFS]), (it / NFS) & 1, a.wait);
+	} else if(warp == 0) {
 		// ---------------- producer: spectra only ----------------
 		// Runs NFS stages ahead of the converters, gated only by their
 		// release of the ring slot, across piece boundaries.
@@ -348,15 +424,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			// this thread's bins of every detector, rounded to FP32
 			float2 f[TC_MAXDET][BPT];
 			{
-				const uint8_t *base = sF + fs * f_stage + r * 128;
+				const uint8_t *base = sF + fs * f_stage + r * (IDX ? IDX_RP : 128);
+				// indexed rows carry only the bins present and only rows of
+				// the batch: the rest of the slot is stale, masked here
+				const int uu = u0 + it;
+				const bool row_in = !IDX || (uu / a.Kst) * TM + r < a.S;
+				const int k0 = (uu % a.Kst) * KB;
 #pragma unroll
 				for(int d = 0; d < TC_MAXDET; d++)
 #pragma unroll
 					for(int c = 0; c < BPT; c++) {
 						const int cc = g * BPT + c;
 						double2 v = make_double2(0, 0);
-						if(d < a.n_det)
-							v = *(const double2 *) (base + d * f_slab + ((cc ^ (r & 7)) << 4));
+						if(d < a.n_det && row_in && (!IDX || k0 + cc < a.Ku))
+							v = *(const double2 *) (base + d * f_slab + (IDX ? cc << 4 : ((cc ^ (r & 7)) << 4)));
 						f[d][c] = make_float2((float) v.x, (float) v.y);
 					}
 			}
@@ -647,6 +728,8 @@ __global__ void __launch_bounds__(32 * (2 + NWMAX), 1) k_cc_stream(const __grid_
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
 	__syncthreads();
+	pdl_allow_dependents();
+	pdl_wait_prior();
 
 	if(warp == 0) {
 		if(lane == 0) {
@@ -828,6 +911,7 @@ __global__ void k_epilogue(const __grid_constant__ EpArgs e, T *acc)
 	T *sP = (T *) (sPh + 2 * e.L + 1);                              // [B][Lp1]
 	const int s = blockIdx.x;
 	T *row = acc + (size_t) s * e.B * e.accstride;
+	pdl_wait_prior();
 	for(int i = threadIdx.x; i < e.B * e.Lp1; i += blockDim.x) {
 		const int b = i / e.Lp1;
 		T v = row[b * e.accstride + i % e.Lp1];
@@ -857,7 +941,13 @@ __global__ void k_epilogue(const __grid_constant__ EpArgs e, T *acc)
 			im += w.y * pv;
 		}
 		const double2 ph = sPh[e.mq[q] + e.L];
-		e.sky[(size_t) s * e.nq + q] = make_double2((double) re * ph.x - (double) im * ph.y, (double) re * ph.y + (double) im * ph.x);
+		const double vr = (double) re * ph.x - (double) im * ph.y, vi = (double) re * ph.y + (double) im * ph.x;
+		if(e.out_row) {
+			const int Ls = (int) e.seg_L[s];
+			if(l <= Ls)
+				ep_put(e.sky + e.out_row[s] + d_lmoff(Ls, l, e.mq[q]), vr, vi, e.accumulate);
+		} else
+			ep_put(e.sky + (size_t) s * e.nq + q, vr, vi, e.accumulate);
 	}
 }
 
@@ -941,6 +1031,7 @@ __global__ void __launch_bounds__(EPI2_THREADS, QMAX <= 5 ? 3 : 2) k_epilogue_f3
 		}
 	};
 	int it = 0;
+	pdl_wait_prior();
 	if((int) blockIdx.x < nb)
 		fetch(blockIdx.x, 0);
 	for(int j = blockIdx.x; j < nb; j += gridDim.x, it++) {
@@ -959,11 +1050,12 @@ __global__ void __launch_bounds__(EPI2_THREADS, QMAX <= 5 ? 3 : 2) k_epilogue_f3
 		for(int g = 0; g < ns; g++) {
 			const float4 *cP = sP + (buf * EPG + g) * nph;
 			const double2 *cPh = sPh + (buf * EPG + g) * nph;
-			double2 *out = e.sky + (size_t) (s0 + g) * e.nq;
+			double2 *out = e.out_row ? e.sky + e.out_row[s0 + g] : e.sky + (size_t) (s0 + g) * e.nq;
+			const int Ls = e.out_row ? (int) e.seg_L[s0 + g] : e.L;
 #pragma unroll
 			for(int k = 0; k < QMAX; k++) {
 				const int q = threadIdx.x + k * EPI2_THREADS;
-				if(q < e.nq) {
+				if(q < e.nq && ql[k] <= Ls) {
 					const float4 pv = cP[ql[k]];
 					float re = w[k][0].x * pv.x, im = w[k][0].y * pv.x;
 					if(EB > 1) {
@@ -978,7 +1070,8 @@ __global__ void __launch_bounds__(EPI2_THREADS, QMAX <= 5 ? 3 : 2) k_epilogue_f3
 					double2 ph = cPh[qm[k] < 0 ? -qm[k] : qm[k]];
 					if(qm[k] < 0)
 						ph.y = -ph.y;
-					out[q] = make_double2((double) re * ph.x - (double) im * ph.y, (double) re * ph.y + (double) im * ph.x);
+					ep_put(out + (e.out_row ? d_lmoff(Ls, ql[k], qm[k]) : q), (double) re * ph.x - (double) im * ph.y,
+					       (double) re * ph.y + (double) im * ph.x, e.accumulate);
 				}
 			}
 		}
@@ -1067,9 +1160,9 @@ static size_t ccs_smem_bytes(const BatchPlan &P)
 	return 1024 + f + aa + dd + 8 + bars;
 }
 
-static size_t tc_smem_bytes(const BatchPlan &P, bool x_in_tmem = false)
+static size_t tc_smem_bytes(const BatchPlan &P, bool x_in_tmem = false, bool indexed = false)
 {
-	const size_t f = (size_t) P.nf * P.n_det * TM * 128;
+	const size_t f = (size_t) P.nf * P.n_det * TM * (indexed ? IDX_RP : 128);
 	const size_t aa = x_in_tmem ? 0 : (size_t) P.nab * P.B * P.npart * A_TILE;
 	const size_t bb = (size_t) P.nb * P.B * P.npart * P.npad * KE * 2;
 	const size_t bars = 8 * (2 * P.nf + 2 * P.nab + 2 * P.nb + 3) + 16;
@@ -1099,6 +1192,7 @@ void batch_plan_destroy(void *pp)
 }
 
 unsigned batch_plan_l_max(const void *p) { return ((const BatchPlan *) p)->L; }
+int batch_precision(const void *p) { return ((const BatchPlan *) p)->precision; }
 int batch_plan_n_det(const void *p) { return ((const BatchPlan *) p)->n_det; }
 int batch_plan_n(const void *p) { return ((const BatchPlan *) p)->n; }
 int batch_plan_bins(const void *p) { return ((const BatchPlan *) p)->Ku; }
@@ -1264,7 +1358,9 @@ void *batch_plan_create(const BatchPlanDesc &d, int precision)
 				     cudaFuncSetAttribute(k_tc_contract<2, 3, 2, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
 				     cudaFuncSetAttribute(k_tc_contract<2, NF, 3, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
 				     cudaFuncSetAttribute(k_tc_contract<3, NF, 2, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
-				     cudaFuncSetAttribute(k_tc_contract<2, 4, 4, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess)) {
+				     cudaFuncSetAttribute(k_tc_contract<2, 4, 4, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
+				     cudaFuncSetAttribute(k_tc_contract<2, NF, 3, 3, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
+				     cudaFuncSetAttribute(k_tc_contract<3, NF, 2, 3, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess)) {
 				set_error("batch plan: cannot reserve %zu bytes of shared memory", tc_smem_bytes(*P));
 				fail = true;
 			}
@@ -1407,6 +1503,25 @@ int batch_set_ctas(void *pp, int S, int ctas)
 	return 0;
 }
 
+// launch with programmatic stream serialisation (see pdl_allow_dependents):
+// the kernel may be scheduled while the one before it in the stream is
+// finishing, and waits for it where it reads what that one writes
+template <typename... KArgs, typename... Args>
+static cudaError_t launch_pdl(void (*kernel)(KArgs...), unsigned grid, unsigned block, size_t smem, cudaStream_t st, Args... args)
+{
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = dim3(grid);
+	cfg.blockDim = dim3(block);
+	cfg.dynamicSmemBytes = smem;
+	cfg.stream = st;
+	cudaLaunchAttribute at[1];
+	at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	at[0].val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = at;
+	cfg.numAttrs = 1;
+	return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // tensor map of the spectra [n_det][S][ld] (FP64 pairs): boxes of 8 bins x
 // 128 segments x every detector, 128B swizzle, zero fill past the edges
 static int ensure_tmap(BatchPlan *P, const void *F, int S, long long ld)
@@ -1433,7 +1548,18 @@ static int ensure_tmap(BatchPlan *P, const void *F, int S, long long ld)
 int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream_v, int split,
 	      const float *segw, int pipe_variant)
 {
+	return batch_run_ex(pp, F, S, ld, gmst, sky, ws, ws_bytes, stream_v, split, segw, pipe_variant, nullptr);
+}
+
+int batch_run_ex(void *pp, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream_v, int split,
+		 const float *segw, int pipe_variant, const BatchIdx *ix)
+{
 	BatchPlan *P = (BatchPlan *) pp;
+	const bool indexed = ix && ix->row_off;
+	if(indexed && !is_tc(P->precision)) {
+		set_error("batch_run: indexed spectra need a tcgen05 precision");
+		return -1;
+	}
 	cudaStream_t st = (cudaStream_t) stream_v;
 	if(S <= 0)
 		return 0;
@@ -1460,6 +1586,9 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 	e.gmst = gmst;
 	e.segw = segw;
 	e.sky = (double2 *) sky;
+	e.out_row = ix ? ix->out_row : nullptr;
+	e.seg_L = ix ? ix->seg_L : nullptr;
+	e.accumulate = ix ? ix->accumulate : 0;
 	e.reps = ws_reps(P, S);
 	e.rep_stride = (size_t) S * P->B * P->accstride;
 
@@ -1472,7 +1601,7 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 			set_error("batch_run: split %d above %d stages", split, P->Kst);
 			return -1;
 		}
-		if(ensure_tmap(P, F, S, ld))
+		if(!indexed && ensure_tmap(P, F, S, ld))
 			return -1;
 		TcArgs a;
 		memset(&a, 0, sizeof(a));
@@ -1491,6 +1620,13 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 		a.acc = (float *) ws;
 		a.wait = P->wait_limit ? P->wait_limit : kWaitCycles;
 		a.hold = P->hold_stage;
+		if(indexed) {
+			a.rows = (const double2 *) F;
+			a.row_off = ix->row_off;
+			for(int d = 0; d < P->n_det && d < 3; d++)
+				a.det_off[d] = ix->det_off[d];
+			a.Ku = P->Ku;
+		}
 		a.reps = e.reps;
 		a.rep_stride = e.rep_stride;
 		a.err = P->err;
@@ -1527,18 +1663,37 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 				P->nab = P->nab0;
 			}
 		}
+		if(indexed) {
+			// the indexed ring is 12 % wider: the shallower X-operand ring,
+			// X in shared memory
+			x_tmem = false;
+			a.acol = 0;
+			a.tmem_cols = P->tmem_cols;
+			P->nf = NF;
+			P->nab = P->npart == 3 ? 2 : 3;
+			if(tc_smem_bytes(*P, false, true) > 227 * 1024) {
+				P->nf = P->nf0;
+				P->nab = P->nab0;
+				set_error("batch_run: indexed spectra exceed the shared-memory budget at l_max %u", P->L);
+				return -1;
+			}
+		}
 		if(P->ev_begin)
 			cudaEventRecord(P->ev_begin, st);
-		if(x_tmem)
-			k_tc_contract<2, 4, 4, 3, true><<<ctas, TC_THREADS, tc_smem_bytes(*P, true), st>>>(P->tm, a);
+		if(indexed && P->npart == 3)
+			CKB(launch_pdl(k_tc_contract<3, NF, 2, 3, false, true>, ctas, TC_THREADS, tc_smem_bytes(*P, false, true), st, P->tm, a));
+		else if(indexed)
+			CKB(launch_pdl(k_tc_contract<2, NF, 3, 3, false, true>, ctas, TC_THREADS, tc_smem_bytes(*P, false, true), st, P->tm, a));
+		else if(x_tmem)
+			CKB(launch_pdl(k_tc_contract<2, 4, 4, 3, true>, ctas, TC_THREADS, tc_smem_bytes(*P, true), st, P->tm, a));
 		else if(P->npart == 3)
-			k_tc_contract<3, NF, 2, 3, false><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			CKB(launch_pdl(k_tc_contract<3, NF, 2, 3, false>, ctas, TC_THREADS, tc_smem_bytes(*P), st, P->tm, a));
 		else if(P->nf == 3)
-			k_tc_contract<2, 3, 2, 3, false><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			CKB(launch_pdl(k_tc_contract<2, 3, 2, 3, false>, ctas, TC_THREADS, tc_smem_bytes(*P), st, P->tm, a));
 		else if(P->nab == 4)
-			k_tc_contract<2, NF, 4, 3, false><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			CKB(launch_pdl(k_tc_contract<2, NF, 4, 3, false>, ctas, TC_THREADS, tc_smem_bytes(*P), st, P->tm, a));
 		else
-			k_tc_contract<2, NF, 3, 3, false><<<ctas, TC_THREADS, tc_smem_bytes(*P), st>>>(P->tm, a);
+			CKB(launch_pdl(k_tc_contract<2, NF, 3, 3, false>, ctas, TC_THREADS, tc_smem_bytes(*P), st, P->tm, a));
 		if(P->ev_end)
 			cudaEventRecord(P->ev_end, st);
 		launches++;
@@ -1572,9 +1727,9 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 		if(P->ev_begin)
 			cudaEventRecord(P->ev_begin, st);
 		if(P->precision == kPrecFP64)
-			k_cc_stream<double, CCS_NFS_F64, CCS_NWMAX_F64><<<ctas, threads, ccs_smem_bytes(*P), st>>>(P->tm, c);
+			CKB(launch_pdl(k_cc_stream<double, CCS_NFS_F64, CCS_NWMAX_F64>, ctas, threads, ccs_smem_bytes(*P), st, P->tm, c));
 		else
-			k_cc_stream<float, CCS_NFS_F32, CCS_NWMAX_F32><<<ctas, threads, ccs_smem_bytes(*P), st>>>(P->tm, c);
+			CKB(launch_pdl(k_cc_stream<float, CCS_NFS_F32, CCS_NWMAX_F32>, ctas, threads, ccs_smem_bytes(*P), st, P->tm, c));
 		if(P->ev_end)
 			cudaEventRecord(P->ev_end, st);
 		launches++;
@@ -1633,13 +1788,13 @@ int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, 
 		const int grid = nbatch < per_sm * sms ? nbatch : per_sm * sms;
 		const size_t esm2 = (size_t) 2 * EPG * (P->L + 1) * (sizeof(double2) + sizeof(float4));
 		if(qmax <= 5)
-			k_epilogue_f32<5><<<grid, EPI2_THREADS, esm2, st>>>(e, (float *) ws);
+			CKB(launch_pdl(k_epilogue_f32<5>, grid, EPI2_THREADS, esm2, st, e, (float *) ws));
 		else
-			k_epilogue_f32<10><<<grid, EPI2_THREADS, esm2, st>>>(e, (float *) ws);
+			CKB(launch_pdl(k_epilogue_f32<10>, grid, EPI2_THREADS, esm2, st, e, (float *) ws));
 	} else if(P->precision == kPrecFP64)
-		k_epilogue<double><<<S, 128, esmem, st>>>(e, (double *) ws);
+		CKB(launch_pdl(k_epilogue<double>, S, 128, esmem, st, e, (double *) ws));
 	else
-		k_epilogue<float><<<S, 128, esmem, st>>>(e, (float *) ws);
+		CKB(launch_pdl(k_epilogue<float>, S, 128, esmem, st, e, (float *) ws));
 	launches++;
 	P->last_kernels = launches;
 	CKB(cudaGetLastError());
@@ -1754,10 +1909,28 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 constexpr int kMaxDevices = 64;
 static std::mutex g_noalloc_mu;
 static void *g_noalloc_ptr[kMaxDevices];
+static CUcontext g_noalloc_ctx[kMaxDevices];
+
+static CUresult current_context(CUcontext *ctx)
+{
+	static PFN_cuCtxGetCurrent_v4000 fn = nullptr;
+	static std::once_flag once;
+	std::call_once(once, [] {
+		void *p = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if(cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+			fn = (PFN_cuCtxGetCurrent_v4000) p;
+	});
+	if(!fn)
+		return CUDA_ERROR_NOT_FOUND;
+	return fn(ctx);
+}
 
 // Device address of the scratch array on the current device.  Host code
-// cannot name the array's device address directly; it is looked up once per
-// device with that device current.
+// cannot name the array's device address directly; it is looked up with the
+// device current on the first call on a device, and again whenever the
+// device's context has changed since (a device reset unloads the module, and
+// the array then lives at a new address).
 static int noalloc_scratch(void **out)
 {
 	int dev = 0;
@@ -1766,8 +1939,11 @@ static int noalloc_scratch(void **out)
 		set_error("allocation-free integrate: device ordinal %d above %d", dev, kMaxDevices - 1);
 		return -1;
 	}
+	CUcontext ctx = nullptr;
+	if(current_context(&ctx) != CUDA_SUCCESS)
+		ctx = nullptr;
 	std::lock_guard<std::mutex> lk(g_noalloc_mu);
-	if(!g_noalloc_ptr[dev]) {
+	if(!g_noalloc_ptr[dev] || !ctx || ctx != g_noalloc_ctx[dev]) {
 		void *p = nullptr;
 		const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
 		if(e != cudaSuccess || !p) {
@@ -1775,9 +1951,24 @@ static int noalloc_scratch(void **out)
 			return -1;
 		}
 		g_noalloc_ptr[dev] = p;
+		g_noalloc_ctx[dev] = ctx;
 	}
 	*out = g_noalloc_ptr[dev];
 	return 0;
+}
+
+// the most segments whose split-K scratch fits the array: the workspace holds
+// ws_reps(S) copies (up to 16 for batches under 16 tiles), so the bound is
+// found by search, not by one division
+static size_t noalloc_max_segments(const BatchPlan *P)
+{
+	const size_t one = batch_workspace_bytes(P, 1) / (size_t) ws_reps(P, 1);
+	if(!one)
+		return 0;
+	size_t S = kNoAllocScratchBytes / one;
+	while(S > 0 && batch_workspace_bytes(P, (int) S) > kNoAllocScratchBytes)
+		S--;
+	return S;
 }
 
 size_t batch_noalloc_capacity() { return kNoAllocScratchBytes; }
@@ -1787,15 +1978,16 @@ int batch_run_noalloc(void *pp, const void *F, int S, long long ld, const double
 	BatchPlan *P = (BatchPlan *) pp;
 	const size_t need = batch_workspace_bytes(P, S);
 	if(need > kNoAllocScratchBytes) {
-		const size_t per_seg = batch_workspace_bytes(P, 1);
 		set_error("allocation-free integrate: %d segments need %zu bytes of scratch, above the %zu-byte static array (at most %zu segments for this plan)", S,
-			  need, kNoAllocScratchBytes, per_seg ? kNoAllocScratchBytes / per_seg : (size_t) 0);
+			  need, kNoAllocScratchBytes, noalloc_max_segments(P));
 		return -1;
 	}
 	void *ws = nullptr;
 	if(noalloc_scratch(&ws))
 		return -1;
-	// the array keeps whatever the previous call left: zero the part used
+	// The kernels leave the part they used zeroed, but a previous call that
+	// gave up part-way (a device-side wait that timed out) or a call of
+	// another plan with a longer workspace may leave it dirty: zero it.
 	CKB(cudaMemsetAsync(ws, 0, need ? need : 16, (cudaStream_t) stream_v));
 	return batch_run(P, F, S, ld, gmst, sky, ws, kNoAllocScratchBytes, stream_v, 0);
 }

@@ -130,6 +130,18 @@ extern "C" struct instrument *instrument_new_from_r_theta_phi(double r, double t
 	return instrument_new(r * sin(theta) * cos(phi), r * sin(theta) * sin(phi), r * cos(theta), data);
 }
 
+// instrument.c:175-181: the vertex in light-seconds, the detector borrowed
+// as the instrument's data
+extern "C" struct instrument *instrument_new_from_LALDetector(LALDetector *det)
+{
+	if(!det) {
+		set_error("instrument_new_from_LALDetector: NULL detector");
+		return NULL;
+	}
+	const double c = 299792458.0;  // m/s, exact (SI)
+	return instrument_new(det->location[0] / c, det->location[1] / c, det->location[2] / c, det);
+}
+
 extern "C" double instrument_r(const struct instrument *i) { return vector_magnitude(i->phase_centre); }
 
 // a - b (instrument.c:210-218)
@@ -1072,6 +1084,21 @@ extern "C" int sphrad_batch_integrate_weighted(sphrad_batch_plan *p, const void 
 	return batch_run(p->impl, fseries_dev, n_seg, ld, gmst_dev, sky_dev, workspace, workspace_bytes, stream, split > 0 ? split : 0, baseline_factor);
 }
 
+// uneven batches (uneven_api.cpp): spectra read in place through row
+// offsets (tcgen05 precisions) and skies added into packed outputs
+int sphrad::batch_integrate_packed(sphrad_batch_plan *p, const void *fseries_dev, int n_seg, long long ld, const BatchIdx *ix, void *sky_dev, void *workspace,
+				   size_t workspace_bytes, void *stream, int split, const float *baseline_factor)
+{
+	NEED_POLAR(p, "batch_integrate_packed");
+	return batch_run_ex(p->impl, fseries_dev, n_seg, ld, nullptr, sky_dev, workspace, workspace_bytes, stream, split > 0 ? split : 0, baseline_factor, -1,
+			    ix);
+}
+
+int sphrad::batch_is_tc(const sphrad_batch_plan *p)
+{
+	return p->impl && (batch_precision(p->impl) == SPHRAD_PREC_BF16X3 || batch_precision(p->impl) == SPHRAD_PREC_BF16X6);
+}
+
 extern "C" int sphrad_batch_integrate_host(sphrad_batch_plan *p, const void *fseries, int n_seg, long long ld, const double *gmst, void *sky)
 {
 	NEED_POLAR(p, "sphrad_batch_integrate_host");
@@ -1688,6 +1715,77 @@ extern "C" int sphrad_batch_generate_alm_skys(sphrad_batch_plan *plan_p, sphrad_
 // ------------------------------------------------------------------------
 // projection operator (inspiral_sky_map.c:387-549)
 // ------------------------------------------------------------------------
+// Antenna response of a detector with response tensor D to a wave from right
+// ascension ra, declination dec, polarisation angle psi at Greenwich mean
+// sidereal time gmst (LAL's XLALComputeDetAMResponse, which the reference
+// calls at inspiral_sky_map.c:357; the published formulas of Anderson,
+// Brady, Creighton & Flanagan, Phys. Rev. D 63, 042003 (2001), appendix B):
+// with the hour angle h = gmst - ra, the wave-frame axes
+//   X = (-cos psi sin h - sin psi cos h sin dec, -cos psi cos h + sin psi sin h sin dec, sin psi cos dec)
+//   Y = ( sin psi sin h - cos psi cos h sin dec,  sin psi cos h + cos psi sin h sin dec, cos psi cos dec)
+// give F+ = X.D.X - Y.D.Y and Fx = X.D.Y + Y.D.X.
+static void det_am_response(double *fplus, double *fcross, const float D[3][3], double ra, double dec, double psi, double gmst)
+{
+	const double h = gmst - ra;
+	const double ch = cos(h), sh = sin(h), cd = cos(dec), sd = sin(dec), cp = cos(psi), sp = sin(psi);
+	const double X[3] = {-cp * sh - sp * ch * sd, -cp * ch + sp * sh * sd, sp * cd};
+	const double Y[3] = {sp * sh - cp * ch * sd, sp * ch + cp * sh * sd, cp * cd};
+	double fp = 0.0, fc = 0.0;
+	for(int i = 0; i < 3; i++) {
+		double DX = 0.0, DY = 0.0;
+		for(int j = 0; j < 3; j++) {
+			DX += D[i][j] * X[j];
+			DY += D[i][j] * Y[j];
+		}
+		fp += X[i] * DX - Y[i] * DY;
+		fc += X[i] * DY + Y[i] * DX;
+	}
+	*fplus = fp;
+	*fcross = fc;
+}
+
+extern "C" int sphrad_antenna_response(double *fplus, double *fcross, const float D[3][3], double ra, double dec, double psi, double gmst)
+{
+	det_am_response(fplus, fcross, D, ra, dec, psi, gmst);
+	return 0;
+}
+
+// inspiral_sky_map.c:423-549 under its own name: the detectors are the
+// LALDetectors the instruments carry (instrument_new_from_LALDetector), their
+// antenna patterns at polarisation angle psi sampled on the reference's mesh
+// of the delay kernels' l_max (sh_series_from_func's layout: Gauss-Legendre
+// rows by increasing theta, 2(L+1) columns; CBCProjectionMatrix's call at
+// :357, phi as right ascension, pi/2 - theta as declination, gmst 0), then
+// the projected plans built as sphrad_network_plan_mult_by_projection does.
+extern "C" int correlator_network_plan_mult_by_projection(struct correlator_network_plan_fd *plan, double beta, double psi, double **psd)
+{
+	if(!plan || !psd) {
+		set_error("correlator_network_plan_mult_by_projection: NULL argument");
+		return -1;
+	}
+	const struct instrument_array *inst = plan->baselines->baselines[0]->instruments;
+	const int n_det = instrument_array_len(inst);
+	const unsigned L = plan->plans[0]->delay_product->l_max;
+	const int nt = 2 * ((int) L + 1), np = nt;
+	std::vector<double> x(nt), w(nt), fp((size_t) n_det * nt * np), fc((size_t) n_det * nt * np);
+	gl_nodes(nt, x.data(), w.data());  // decreasing x: increasing theta
+	for(int k = 0; k < n_det; k++) {
+		const LALDetector *det = (const LALDetector *) instrument_array_get(inst, k)->data;
+		if(!det) {
+			set_error("correlator_network_plan_mult_by_projection: instrument %d carries no detector (use instrument_new_from_LALDetector)", k);
+			return -1;
+		}
+		for(int i = 0; i < nt; i++) {
+			const double theta = acos(x[i]);
+			for(int j = 0; j < np; j++) {
+				const size_t e = ((size_t) k * nt + i) * np + j;
+				det_am_response(&fp[e], &fc[e], det->response, 2.0 * M_PI * j / np, M_PI_2 - theta, psi, 0.0);
+			}
+		}
+	}
+	return sphrad_network_plan_mult_by_projection(plan, beta, fp.data(), fc.data(), psd);
+}
+
 extern "C" int sphrad_network_plan_mult_by_projection(struct correlator_network_plan_fd *plan, double beta, const double *fplus, const double *fcross,
 						      double **psd)
 {

@@ -6,6 +6,8 @@
 #include <cstddef>
 #include <cstdint>
 
+struct sphrad_batch_plan;
+
 namespace sphrad {
 
 // ---- errors (thread-local message, NULL/negative returns at the ABI) ----
@@ -101,6 +103,21 @@ size_t batch_workspace_bytes(const void *plan, int S);
 // batch.cu: ring depths of the tcgen05 pipeline)
 int batch_run(void *plan, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream, int split,
 	      const float *segw = nullptr, int pipe_variant = -1);
+// segments read in place and skies written into packed outputs (uneven
+// batches): row s's spectrum of detector d at F + row_off[s] + det_off[d]
+// (double complex elements; tcgen05 precisions only, row_off NULL = the
+// [n_det][S][ld] layout), sky of row s at sky + out_row[s] in the layout of
+// l_max seg_L[s], stored or added (accumulate) -- out_row NULL = [S][nq]
+struct BatchIdx {
+	const long long *row_off = nullptr;
+	long long det_off[3] = {0, 0, 0};
+	const long long *out_row = nullptr;
+	const unsigned *seg_L = nullptr;
+	int accumulate = 0;
+};
+int batch_run_ex(void *plan, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream, int split,
+		 const float *segw, int pipe_variant, const BatchIdx *ix);
+int batch_precision(const void *plan);
 int batch_pipe_variant(const void *plan, int S);
 int batch_run_host(void *plan, const void *F_host, int S, long long ld, const double *gmst_host, void *sky_host);
 int batch_pick_split(const void *plan, int S);
@@ -190,11 +207,7 @@ int np_alm_finish(void *plan, int S, double factor, const void *prior, const dou
 // F[d][i][k] = in[in_off[seg[i]] + det[d] Ku + k] for a job of S segments
 // of n_sub detectors (device pointers; stream a cudaStream_t)
 int uneven_gather(int S, int n_sub, int Ku, long long ld, const int *seg, const long long *in_off, const int *det, const void *in, void *F, void *stream);
-// out[out_off[seg[i]] ...] += sky[i] truncated to l_max seg_L[seg[i]]
-// out[segment s] = sum over entries e in [ptr[s], ptr[s+1]) of the sky at
-// sky_all + rows[e] (layout L), truncated to seg_L[s]; every output written
-int uneven_combine(int n_seg, unsigned L, const int *ptr, const long long *rows, const long long *out_off, const unsigned *seg_L, const void *sky_all, void *out,
-		   void *stream);
+
 int batch_autotune(void *plan, const void *F, int S, long long ld, void *sky, void *ws, size_t ws_bytes, void *stream);
 int batch_set_split(void *plan, int S, int split);
 
@@ -290,5 +303,10 @@ int peak_refine(int S, unsigned L, int polar, const void *coeff, long long cstri
 		double tol, double *out, int *status, void *stream, int method = -1);
 int peak_refine_method();
 int set_peak_refine_method(int method);
+
+// the same through a public batch plan (correlator.cpp)
+int batch_integrate_packed(::sphrad_batch_plan *plan, const void *fseries_dev, int n_seg, long long ld, const BatchIdx *ix, void *sky_dev, void *workspace,
+			   size_t workspace_bytes, void *stream, int split, const float *baseline_factor);
+int batch_is_tc(const ::sphrad_batch_plan *plan);
 
 }  // namespace sphrad

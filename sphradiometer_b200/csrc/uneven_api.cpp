@@ -13,13 +13,15 @@
 // list and per-segment baseline factors (n_sub_baselines / B_s for the
 // segment's baselines assigned to the job, 0 otherwise, so each sky is the
 // mean over its own B_s baselines, correlator.c:1004).  A call zeroes the
-// packed outputs and runs every job: gather of its spectra, contraction,
-// epilogue into the job's own sky rows; the jobs are spread over a few
-// streams (longest first, each to the least loaded stream) so that small
-// jobs overlap, and one final kernel sums every segment's rows, in job
-// order, into the packed outputs truncated to each segment's l_max.  The
-// whole sequence can be captured once into a CUDA graph (forked over the
-// streams) and replayed.
+// packed outputs and runs every job: the contraction reads the job's
+// segments where they lie in the caller's packed spectra (one bulk copy per
+// segment row and stage; the FP32 / FP64 precisions gather them first) and
+// the epilogue adds each segment's sky into its packed output, truncated to
+// the segment's own l_max (FP64 atomics: a segment covered by two jobs gets
+// the same sum in either order).  The jobs are spread over a few streams
+// (longest first, each to the least loaded stream) so that small jobs
+// overlap.  The whole sequence can be captured once into a CUDA graph
+// (forked over the streams) and replayed.
 #include <sphradiometer_b200.h>
 #include <sphradiometer/correlator.h>
 #include <sphradiometer/instrument.h>
@@ -47,8 +49,11 @@ struct Job {
 	std::vector<float> w;        // [S][nb_sub]
 	int *d_seg = nullptr;
 	float *d_w = nullptr;
+	long long *d_rowoff = nullptr;  // [S] the segments' rows in the packed spectra
+	long long *d_outrow = nullptr;  // [S] their skies in the packed outputs
+	unsigned *d_segL = nullptr;     // [S] their l_max
+	bool indexed = false;           // tcgen05 precision: spectra read in place
 	int split = 0;               // tuned split (0 = heuristic)
-	size_t sky_off = 0;          // first row of its skies in the plan's sky_all (complex elements)
 	int slot = 0;                // stream and scratch slot
 };
 
@@ -77,14 +82,12 @@ struct sphrad_uneven_plan {
 	long long *d_in_off = nullptr, *d_out_off = nullptr;
 	unsigned *d_segL = nullptr;
 	std::vector<Job> jobs;
-	// job buffers: spectra and split-K scratch per slot (the jobs of a slot
-	// run in sequence), every job's skies in sky_all
+	// job buffers: gathered spectra (FP32 / FP64 jobs and the autotuner)
+	// and split-K scratch per slot (the jobs of a slot run in sequence);
+	// the autotuner's skies of one job
 	void *F = nullptr, *sky = nullptr, *ws = nullptr;
 	size_t F_bytes = 0, sky_bytes = 0, ws_bytes = 0;
 	int n_slots = 1;
-	// per segment, the rows of its skies in sky_all (CSR, job order)
-	int *d_cmb_ptr = nullptr;
-	long long *d_cmb_rows = nullptr;
 	cudaStream_t side[kSlots] = {};
 	cudaEvent_t ev[kSlots + 1] = {};
 	int fixed_split = 0;
@@ -116,6 +119,9 @@ static void drop_jobs(sphrad_uneven_plan *p)
 	for(Job &j : p->jobs) {
 		dfree(j.d_seg);
 		dfree(j.d_w);
+		dfree(j.d_rowoff);
+		dfree(j.d_outrow);
+		dfree(j.d_segL);
 	}
 	p->jobs.clear();
 	dfree(p->d_in_off);
@@ -126,10 +132,6 @@ static void drop_jobs(sphrad_uneven_plan *p)
 	dfree(p->F);
 	dfree(p->sky);
 	dfree(p->ws);
-	dfree(p->d_cmb_ptr);
-	dfree(p->d_cmb_rows);
-	p->d_cmb_ptr = nullptr;
-	p->d_cmb_rows = nullptr;
 	p->F = p->sky = p->ws = nullptr;
 	p->F_bytes = p->sky_bytes = p->ws_bytes = 0;
 	drop_graph(p);
@@ -319,15 +321,27 @@ extern "C" int sphrad_uneven_set_segments(sphrad_uneven_plan *p, int n_seg, cons
 	size_t Fb = 0, skb = 0, wsb = 0;
 	const size_t nq = (size_t) (p->L + 1) * (p->L + 1);
 	for(Job &j : p->jobs) {
-		j.sky_off = skb / 16;
-		skb += (size_t) j.seg.size() * nq * 16;
+		skb = std::max(skb, (size_t) j.seg.size() * nq * 16);
 		j.S = (int) j.seg.size();
 		j.bp = plan_for(p, j.bucket, (int) (std::find(p->subs.begin(), p->subs.end(), j.det) - p->subs.begin()));
 		if(!j.bp)
 			return -1;
+		j.indexed = batch_is_tc(j.bp) != 0;
+		std::vector<long long> ro(j.S), oro(j.S);
+		std::vector<unsigned> sl(j.S);
+		for(int i = 0; i < j.S; i++) {
+			ro[i] = p->in_off[j.seg[i]];
+			oro[i] = p->out_off[j.seg[i]];
+			sl[i] = p->segL[j.seg[i]];
+		}
 		j.d_seg = (int *) dmalloc(j.S * sizeof(int));
 		j.d_w = (float *) dmalloc(j.w.size() * sizeof(float));
-		if(!j.d_seg || !j.d_w || h2d(j.d_seg, j.seg.data(), j.S * sizeof(int)) || h2d(j.d_w, j.w.data(), j.w.size() * sizeof(float)))
+		j.d_rowoff = (long long *) dmalloc(j.S * sizeof(long long));
+		j.d_outrow = (long long *) dmalloc(j.S * sizeof(long long));
+		j.d_segL = (unsigned *) dmalloc(j.S * sizeof(unsigned));
+		if(!j.d_seg || !j.d_w || !j.d_rowoff || !j.d_outrow || !j.d_segL || h2d(j.d_seg, j.seg.data(), j.S * sizeof(int)) ||
+		   h2d(j.d_w, j.w.data(), j.w.size() * sizeof(float)) || h2d(j.d_rowoff, ro.data(), j.S * sizeof(long long)) ||
+		   h2d(j.d_outrow, oro.data(), j.S * sizeof(long long)) || h2d(j.d_segL, sl.data(), j.S * sizeof(unsigned)))
 			return -1;
 		Fb = std::max(Fb, (size_t) (j.det.size() * j.S * j.ld * 16));
 		wsb = std::max(wsb, sphrad_batch_workspace_size(j.bp, j.S));
@@ -349,20 +363,6 @@ extern "C" int sphrad_uneven_set_segments(sphrad_uneven_plan *p, int n_seg, cons
 	}
 	Fb = (Fb + 255) / 256 * 256;
 	wsb = (wsb + 255) / 256 * 256;
-	// per segment: its rows in sky_all, in job order
-	std::vector<int> cptr(n_seg + 1, 0);
-	for(const Job &j : p->jobs)
-		for(int s : j.seg)
-			cptr[s + 1]++;
-	for(int s = 0; s < n_seg; s++)
-		cptr[s + 1] += cptr[s];
-	std::vector<long long> crow(cptr[n_seg]);
-	{
-		std::vector<int> fill(cptr.begin(), cptr.end() - 1);
-		for(const Job &j : p->jobs)
-			for(size_t i = 0; i < j.seg.size(); i++)
-				crow[fill[j.seg[i]]++] = (long long) (j.sky_off + i * nq);
-	}
 	p->d_in_off = (long long *) dmalloc((n_seg > 0 ? n_seg : 1) * sizeof(long long));
 	p->d_out_off = (long long *) dmalloc((n_seg > 0 ? n_seg : 1) * sizeof(long long));
 	p->d_segL = (unsigned *) dmalloc((n_seg > 0 ? n_seg : 1) * sizeof(unsigned));
@@ -372,11 +372,7 @@ extern "C" int sphrad_uneven_set_segments(sphrad_uneven_plan *p, int n_seg, cons
 	p->F_bytes = Fb;
 	p->sky_bytes = skb;
 	p->ws_bytes = wsb;
-	p->d_cmb_ptr = (int *) dmalloc((n_seg + 1) * sizeof(int));
-	p->d_cmb_rows = (long long *) dmalloc((crow.empty() ? 1 : crow.size()) * sizeof(long long));
-	if(!p->d_in_off || !p->d_out_off || !p->d_segL || !p->F || !p->sky || !p->ws || !p->d_cmb_ptr || !p->d_cmb_rows)
-		return -1;
-	if(h2d(p->d_cmb_ptr, cptr.data(), (n_seg + 1) * sizeof(int)) || (!crow.empty() && h2d(p->d_cmb_rows, crow.data(), crow.size() * sizeof(long long))))
+	if(!p->d_in_off || !p->d_out_off || !p->d_segL || !p->F || !p->sky || !p->ws)
 		return -1;
 	if(n_seg > 0 && (h2d(p->d_in_off, p->in_off.data(), n_seg * sizeof(long long)) || h2d(p->d_out_off, p->out_off.data(), n_seg * sizeof(long long)) ||
 			 h2d(p->d_segL, p->segL.data(), n_seg * sizeof(unsigned))))
@@ -411,7 +407,7 @@ static int split_of(const sphrad_uneven_plan *p, const Job &j)
 // spectra, scratch and skies of job j
 static void *job_F(sphrad_uneven_plan *p, const Job &j) { return (char *) p->F + (size_t) j.slot * p->F_bytes; }
 static void *job_ws(sphrad_uneven_plan *p, const Job &j) { return (char *) p->ws + (size_t) j.slot * p->ws_bytes; }
-static void *job_sky(sphrad_uneven_plan *p, const Job &j) { return (double *) p->sky + 2 * j.sky_off; }
+static void *job_sky(sphrad_uneven_plan *p, const Job &) { return p->sky; }
 
 // the jobs forked over the slots' streams from st, joined back, then the
 // combine into the outputs on st
@@ -422,8 +418,9 @@ static int run_jobs(sphrad_uneven_plan *p, const void *in, void *out, cudaStream
 	ss[0] = st;
 	for(int s = 1; s < p->n_slots; s++)
 		ss[s] = p->side[s];
-	if(cudaEventRecord(p->ev[0], st) != cudaSuccess) {
-		set_error("uneven: event record failed");
+	// the jobs add into the packed outputs
+	if(cudaMemsetAsync(out, 0, (size_t) p->out_total * 16, st) != cudaSuccess || cudaEventRecord(p->ev[0], st) != cudaSuccess) {
+		set_error("uneven: output zeroing or event record failed");
 		return -1;
 	}
 	for(int s = 1; s < p->n_slots; s++)
@@ -433,20 +430,31 @@ static int run_jobs(sphrad_uneven_plan *p, const void *in, void *out, cudaStream
 		}
 	for(Job &j : p->jobs) {
 		cudaStream_t js = ss[j.slot];
-		if(uneven_gather(j.S, (int) j.det.size(), j.Ku, j.ld, j.d_seg, p->d_in_off, j.det.data(), in, job_F(p, j), js))
+		BatchIdx ix;
+		ix.out_row = j.d_outrow;
+		ix.seg_L = j.d_segL;
+		ix.accumulate = 1;
+		const void *F = in;
+		if(j.indexed) {
+			ix.row_off = j.d_rowoff;
+			for(size_t d = 0; d < j.det.size() && d < 3; d++)
+				ix.det_off[d] = (long long) j.det[d] * j.Ku;
+		} else {
+			if(uneven_gather(j.S, (int) j.det.size(), j.Ku, j.ld, j.d_seg, p->d_in_off, j.det.data(), in, job_F(p, j), js))
+				return -1;
+			F = job_F(p, j);
+			k++;
+		}
+		if(batch_integrate_packed(j.bp, F, j.S, j.ld, &ix, out, job_ws(p, j), p->ws_bytes, js, split_of(p, j), j.d_w))
 			return -1;
-		if(sphrad_batch_integrate_weighted(j.bp, job_F(p, j), j.S, j.ld, NULL, job_sky(p, j), job_ws(p, j), p->ws_bytes, js, split_of(p, j), j.d_w))
-			return -1;
-		k += 1 + sphrad_batch_kernels_per_call(j.bp);
+		k += sphrad_batch_kernels_per_call(j.bp);
 	}
 	for(int s = 1; s < p->n_slots; s++)
 		if(cudaEventRecord(p->ev[s], ss[s]) != cudaSuccess || cudaStreamWaitEvent(st, p->ev[s], 0) != cudaSuccess) {
 			set_error("uneven: stream join failed");
 			return -1;
 		}
-	if(uneven_combine(p->n_seg, p->L, p->d_cmb_ptr, p->d_cmb_rows, p->d_out_off, p->d_segL, p->sky, out, st))
-		return -1;
-	p->kernels = k + 1;
+	p->kernels = k;
 	return 0;
 }
 

@@ -155,3 +155,26 @@ def test_healpix_nside_follows_the_reference_rule():
             want *= 2
         assert lib.sphrad_healpix_nside(L) == want, L
     assert lib.sphrad_healpix_nside(32) == 32 and lib.sphrad_healpix_nside(25) == 16
+
+
+def test_antenna_response_known_answers():
+    """sphrad_antenna_response (LAL's XLALComputeDetAMResponse, Anderson et
+    al. 2001 app. B): an L-shaped detector with arms along x and y sees a
+    wave from overhead (declination 90 deg) with F+ = -cos 2a, Fx = sin 2a,
+    a = psi + gmst - ra; any wave has F+^2 + Fx^2 independent of psi."""
+    import ctypes as C
+    import math
+    import sphradiometer_b200 as S
+    lib = S.load()
+    D = ((C.c_float * 3) * 3)()
+    D[0][0], D[1][1] = 0.5, -0.5
+    fp, fc = C.c_double(), C.c_double()
+    for psi, gmst, ra in ((0.0, 0.0, 0.0), (0.3, 1.0, 0.4), (1.2, -0.7, 2.2)):
+        lib.sphrad_antenna_response(C.byref(fp), C.byref(fc), D, ra, math.pi / 2, psi, gmst)
+        a = psi + gmst - ra
+        assert abs(fp.value + math.cos(2 * a)) < 1e-7 and abs(fc.value - math.sin(2 * a)) < 1e-7
+    norms = []
+    for psi in (0.0, 0.5, 1.3):
+        lib.sphrad_antenna_response(C.byref(fp), C.byref(fc), D, 0.7, 0.4, psi, 0.2)
+        norms.append(fp.value ** 2 + fc.value ** 2)
+    assert max(norms) - min(norms) < 1e-7

@@ -144,3 +144,87 @@ def test_nonpolar_tensor_core_path_across_tiles():
     bp.close()
     ref.close()
     net.close()
+
+
+class LALDetector(C.Structure):
+    # the leading members of LAL's LALDetector (vertex in metres, response tensor)
+    _fields_ = [("location", C.c_double * 3), ("response", (C.c_float * 3) * 3)]
+
+
+def lal_like_detector(theta, phi, azimuth):
+    """A detector on the Earth's surface at co-latitude theta, longitude
+    phi: perpendicular arms along azimuth and azimuth + 90 deg in the local
+    horizontal plane, response tensor (x x^T - y y^T) / 2."""
+    R = 6.371e6
+    r = np.array([np.sin(theta) * np.cos(phi), np.sin(theta) * np.sin(phi), np.cos(theta)])
+    e_t = np.array([np.cos(theta) * np.cos(phi), np.cos(theta) * np.sin(phi), -np.sin(theta)])
+    e_p = np.array([-np.sin(phi), np.cos(phi), 0.0])
+    x = np.cos(azimuth) * e_t + np.sin(azimuth) * e_p
+    y = -np.sin(azimuth) * e_t + np.cos(azimuth) * e_p
+    d = LALDetector()
+    for i in range(3):
+        d.location[i] = R * r[i]
+    D = 0.5 * (np.outer(x, x) - np.outer(y, y))
+    for i in range(3):
+        for j in range(3):
+            d.response[i][j] = float(D[i, j])
+    return d
+
+
+def am_response(D, ra, dec, psi, gmst):
+    """The published detector response (Anderson et al. 2001, PRD 63 042003,
+    app. B), in numpy."""
+    h = gmst - ra
+    X = np.array([-np.cos(psi) * np.sin(h) - np.sin(psi) * np.cos(h) * np.sin(dec),
+                  -np.cos(psi) * np.cos(h) + np.sin(psi) * np.sin(h) * np.sin(dec), np.sin(psi) * np.cos(dec)])
+    Y = np.array([np.sin(psi) * np.sin(h) - np.cos(psi) * np.cos(h) * np.sin(dec),
+                  np.sin(psi) * np.cos(h) + np.cos(psi) * np.sin(h) * np.sin(dec), np.cos(psi) * np.cos(dec)])
+    return X @ D @ X - Y @ D @ Y, X @ D @ Y + Y @ D @ X
+
+
+def test_reference_named_projection_uses_detector_responses():
+    """correlator_network_plan_mult_by_projection (inspiral_sky_map.c:423-549)
+    with instruments made by instrument_new_from_LALDetector equals the
+    mesh-taking variant fed the same antenna patterns computed in numpy from
+    the response tensors at the reference's call (:357: phi as right
+    ascension, pi/2 - theta as declination, gmst 0)."""
+    import sphradiometer_b200 as S
+    L_ = S.load()
+    dets = [lal_like_detector(0.9, 0.3, 0.2), lal_like_detector(1.4, 2.1, 1.1), lal_like_detector(2.0, -1.2, 2.5)]
+    n, dt, L, beta, psi = 256, 1.0 / 2048, 6, 0.6, 0.35
+    rng = np.random.default_rng(5)
+    psd = rng.uniform(0.5, 2.0, size=(n, 3))
+    rows = (C.POINTER(C.c_double) * n)(*[np.ctypeslib.as_ctypes(psd[j]) for j in range(n)])
+
+    def network():
+        arr = L_.instrument_array_new(0)
+        for d in dets:
+            assert L_.instrument_array_append(arr, L_.instrument_new_from_LALDetector(C.byref(d)))
+        bl = L_.correlator_network_baselines_new(arr)
+        plan = L_.correlator_network_plan_fd_new_l(bl, n, dt, L)
+        assert plan, S.last_error()
+        return arr, bl, plan
+
+    a_arr, a_bl, a_plan = network()
+    assert L_.correlator_network_plan_mult_by_projection(a_plan, beta, psi, C.cast(rows, C.c_void_p)) == 0, S.last_error()
+    # the same patterns from numpy
+    nt = 2 * (L + 1)
+    x, _ = O.gl_nodes(nt)
+    fp = np.zeros((3, nt, nt))
+    fc = np.zeros((3, nt, nt))
+    for k, d in enumerate(dets):
+        D = np.array([[d.response[i][j] for j in range(3)] for i in range(3)], dtype=np.float64)
+        for i in range(nt):
+            for j in range(nt):
+                fp[k, i, j], fc[k, i, j] = am_response(D, 2 * np.pi * j / nt, np.pi / 2 - np.arccos(x[i]), psi, 0.0)
+    b_arr, b_bl, b_plan = network()
+    assert L_.sphrad_network_plan_mult_by_projection(b_plan, beta, np.ascontiguousarray(fp).ctypes.data, np.ascontiguousarray(fc).ctypes.data,
+                                                     C.cast(rows, C.c_void_p)) == 0, S.last_error()
+    for k in range(3):
+        da = S.array_to_numpy(a_plan.contents.plans[k].contents.delay_product)
+        db = S.array_to_numpy(b_plan.contents.plans[k].contents.delay_product)
+        assert np.max(np.abs(da - db)) <= 1e-12 * np.max(np.abs(db)), k
+    for plan, bl, arr in ((a_plan, a_bl, a_arr), (b_plan, b_bl, b_arr)):
+        L_.correlator_network_plan_fd_free(plan)
+        L_.correlator_network_baselines_free(bl)
+        L_.instrument_array_free(arr)

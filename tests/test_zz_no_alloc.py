@@ -8,8 +8,11 @@ array instead of a caller workspace.  The test calls it twice in a row
 through the C ABI and checks each result against the workspace entry point
 (sphrad_batch_integrate) on the same inputs, with the tolerance the bf16x3
 parity tests use; it also checks that a batch too large for the array is
-refused with an error before any device work.  This file is collected last
-so a stop-at-first-failure run has already run every other test.
+refused with an error before any device work, and that the second call
+leaves the device's free memory and torch's allocations unchanged (the
+first call on a device may load the library's module, which places the
+static array).  This file is collected last so a stop-at-first-failure run
+has already run every other test.
 """
 import numpy as np
 import pytest
@@ -40,11 +43,18 @@ def test_noalloc_matches_workspace_entry_point_on_two_calls():
     ref = bp.integrate(F, g).cpu().numpy()
     stream = torch.cuda.current_stream()
     nq = (l_max + 1) ** 2
-    for _ in range(2):
-        out = torch.full((n_seg, nq), float("nan"), dtype=torch.complex128, device="cuda")
+    outs = [torch.full((n_seg, nq), float("nan"), dtype=torch.complex128, device="cuda") for _ in range(2)]
+    torch.cuda.synchronize()
+    for k, out in enumerate(outs):
+        if k == 1:
+            free0, alloc0 = torch.cuda.mem_get_info()[0], torch.cuda.memory_allocated()
         rc = L.sphrad_batch_integrate_noalloc(bp._p, F.data_ptr(), n_seg, F.shape[2], g.data_ptr(), out.data_ptr(), stream.cuda_stream)
         assert rc == 0, S.last_error()
         torch.cuda.synchronize()
+        if k == 1:
+            # the second call allocated no device memory
+            assert torch.cuda.mem_get_info()[0] == free0
+            assert torch.cuda.memory_allocated() == alloc0
         got = out.cpu().numpy()
         assert np.all(np.isfinite(got))
         assert rel_l2(got, ref) < TOL
@@ -52,8 +62,11 @@ def test_noalloc_matches_workspace_entry_point_on_two_calls():
     assert bp.status() == 0
 
     # a batch beyond the static array is refused up front
-    rc = L.sphrad_batch_integrate_noalloc(bp._p, F.data_ptr(), 1_000_000, F.shape[2], g.data_ptr(), out.data_ptr(), stream.cuda_stream)
+    rc = L.sphrad_batch_integrate_noalloc(bp._p, F.data_ptr(), 1_000_000, F.shape[2], g.data_ptr(), outs[0].data_ptr(), stream.cuda_stream)
     assert rc == -1
-    assert "scratch" in S.last_error()
+    msg = S.last_error()
+    assert "scratch" in msg
+    # the message names this plan's limit: 8 MiB over 3 x 36 FP32 partial sums per segment
+    assert "at most 19418 segments" in msg, msg
     bp.close()
     net.close()
