@@ -523,6 +523,9 @@ def projection_report(S, n_seg: int = 4096, reps: int = 3):
         out[f"{prec}_maps_per_s"] = n_seg / t
         out[f"{prec}_tflops"] = flops / t / 1e12
         bp.close()
+    if "bf16x3_maps_per_s" in out and "fp64_maps_per_s" in out:
+        # the tensor-bound shape: bf16x3 tcgen05 against the FP64 CUDA-core GEMM
+        out["split_vs_fp64"] = out["bf16x3_maps_per_s"] / out["fp64_maps_per_s"]
     # generate_alm_skys for n_seg events at once: complex SNR series of
     # every detector -> spectra -> the skies of both projection signs
     # (x 8 B, + log prior, GMST rotation), bf16x3
@@ -701,7 +704,9 @@ def c4_report(S, n_train: int = 1000000, epochs: int = 16, n_eval: int = 32768):
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     del feats, targets
-    ev = P.evaluate(S, gen, prop, n_eval, seed=77, reps=2)
+    untrained = S.Proposal(max_batch=4096, seed=12)
+    ev = P.evaluate(S, gen, prop, n_eval, seed=77, reps=2, untrained=untrained)
+    untrained.close()
     ev.update({"training_maps": n_train, "epochs": epochs, "final_loss": losses[-1], "dataset_s": t_data, "train_s": t_train})
     prop.close()
     gen.close()
@@ -922,6 +927,11 @@ def run(args):
             torch.cuda.synchronize()
             extra[f"{other}_batched_maps_per_s"] = n_seg * reps / (a.elapsed_time(b) / 1e3)
             op.close()
+        # the split precision against FP64 on the same batched path: the
+        # polar contraction is HBM-bound in both, so this ratio is small;
+        # the drop-in ratio above also carries the per-call host work
+        if "fp64_batched_maps_per_s" in extra:
+            extra["split_vs_fp64_batched"] = value / world / extra["fp64_batched_maps_per_s"]
         # exactly the c1 batch size (64 segments per launch)
         if n_seg != 64:
             bp64 = S.BatchPlan(net, prec)

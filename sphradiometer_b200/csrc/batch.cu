@@ -71,12 +71,17 @@ constexpr int CC_KC = 16;                // bins per CUDA-core stage
 constexpr int kMaxChain = 64;            // most pipeline stages one tcgen05 CTA accumulates
 }  // namespace
 
-// Programmatic dependent launch: a contraction lets the grid launched after
-// it (its epilogue) be scheduled once its own set-up is done, and waits for
-// the grid before it (which may write its inputs or read its workspace)
-// only after that set-up; the epilogue loads its tables, then waits for the
-// contraction before it reads the partial sums.  Without the launch
-// attribute both instructions return at once.
+// Programmatic dependent launch.  A contraction lets the grid launched after
+// it (its epilogue) be scheduled once its own set-up is done; the epilogue
+// loads its tables, then waits for the contraction before it reads the
+// partial sums.  An epilogue lets the next grid start at once: only our
+// epilogues release a dependent early, so a contraction that starts early
+// follows an epilogue, which writes no input of it -- the contraction
+// streams and multiplies its spectra meanwhile and waits for that epilogue
+// (which re-zeroes the workspace) only before its first partial sums leave.
+// A kernel that follows any other work starts when that work has completed,
+// as without the attribute.  Without the launch attribute both
+// instructions return at once.
 __device__ __forceinline__ void pdl_allow_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait_prior() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
@@ -269,7 +274,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	tc_fence_after();
 	const uint32_t tmem = *tslot;
 	pdl_allow_dependents();
-	pdl_wait_prior();
+	bool prior_done = false;  // converter warps: waited for the grid before (before the first flush)
 
 	if(warp == 0 && IDX) {
 		// ---------------- producer: indexed spectra ----------------
@@ -495,6 +500,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 				break;
 			const int q = warp & 3;
 			const int s = ((u0 + it) / a.Kst) * TM + q * 32 + lane;
+			if(!prior_done) {
+				pdl_wait_prior();
+				prior_done = true;
+			}
 			for(int b = (warp - 2) >> 2; b < a.B; b += CONV_WARPS / 4) {
 				for(int c0 = 0; c0 < a.accstride; c0 += 16) {
 					uint32_t v[16], w[16];
@@ -729,7 +738,6 @@ __global__ void __launch_bounds__(32 * (2 + NWMAX), 1) k_cc_stream(const __grid_
 	}
 	__syncthreads();
 	pdl_allow_dependents();
-	pdl_wait_prior();
 
 	if(warp == 0) {
 		if(lane == 0) {
@@ -778,6 +786,7 @@ __global__ void __launch_bounds__(32 * (2 + NWMAX), 1) k_cc_stream(const __grid_
 		for(int j = 0; j < CCS_LG; j++)
 			acc[r][j] = 0;
 	int cur_tile = u0 / a.Kst;
+	bool prior_done = false;
 	for(int it = 0; it < nst; it++) {
 		const int u = u0 + it;
 		const int fs = it % NFS;
@@ -852,6 +861,10 @@ __global__ void __launch_bounds__(32 * (2 + NWMAX), 1) k_cc_stream(const __grid_
 		if(last) {
 			const int tile = cur_tile;
 			cur_tile = (u + 1) / a.Kst;
+			if(!prior_done) {
+				pdl_wait_prior();
+				prior_done = true;
+			}
 #pragma unroll
 			for(int r = 0; r < 4; r++) {
 				const int s = tile * TM + 4 * lane + r;
@@ -911,6 +924,7 @@ __global__ void k_epilogue(const __grid_constant__ EpArgs e, T *acc)
 	T *sP = (T *) (sPh + 2 * e.L + 1);                              // [B][Lp1]
 	const int s = blockIdx.x;
 	T *row = acc + (size_t) s * e.B * e.accstride;
+	pdl_allow_dependents();
 	pdl_wait_prior();
 	for(int i = threadIdx.x; i < e.B * e.Lp1; i += blockDim.x) {
 		const int b = i / e.Lp1;
@@ -1031,6 +1045,7 @@ __global__ void __launch_bounds__(EPI2_THREADS, QMAX <= 5 ? 3 : 2) k_epilogue_f3
 		}
 	};
 	int it = 0;
+	pdl_allow_dependents();
 	pdl_wait_prior();
 	if((int) blockIdx.x < nb)
 		fetch(blockIdx.x, 0);

@@ -3,7 +3,8 @@
 Skies come from the library itself: seeded 3-detector injections
 (workload.make_batch_torch) integrated by the batched tcgen05 path in the
 Earth frame.  Each sky's label is the plain extremizer's answer: the best
-pixel of a 64 x 128 grid of the full sky, refined by FP64 Newton steps.
+pixel of a 64 x 128 grid of the full sky, refined in FP64 by the library's
+refinement (BFGS2 by default, sphrad_sky_set_refinement).
 A 3-detector sky is exactly symmetric under reflection through the plane of
 its baselines (the delays depend on the source only through r_ij . s), so
 its maximum is defined up to that mirror image; labels and comparisons use
@@ -118,12 +119,17 @@ def train(prop, feats, targets, epochs: int = 4, batch: int = 4096, lr: float = 
     return losses
 
 
-def evaluate(S, gen: Generator, prop, n: int, seed: int, max_move_deg: float = 30.0, basin_deg: float = 6.0, dominance: float = 0.1, reps: int = 3):
+def evaluate(S, gen: Generator, prop, n: int, seed: int, max_move_deg: float = 30.0, basin_deg: float = 6.0, dominance: float = 0.1, reps: int = 3,
+             untrained=None):
     """Learned-proposal localisation against the plain extremizer on fresh
     skies: proposal error, fallback rate, agreement within 0.5 degrees
-    (modulo the mirror image) and localisations per second of both."""
+    (modulo the mirror image) and localisations per second of both; and
+    every direction's error against the injected source (modulo the mirror
+    image), for the trained network's raw proposals, an untrained network's
+    (``untrained``, same architecture, when given), the plain extremizer
+    and the proposal localisation."""
     import torch
-    sky, _ = gen.skies(n, seed)
+    sky, inj = gen.skies(n, seed)
     torch.cuda.synchronize()
     ref, _ = gen.grid_search(sky)
     feats = prop.sky_features(sky)
@@ -150,7 +156,25 @@ def evaluate(S, gen: Generator, prop, n: int, seed: int, max_move_deg: float = 3
     torch.cuda.synchronize()
     t_prop = (time.perf_counter() - t0) / reps
     q = torch.quantile(perr.float(), torch.tensor([0.5, 0.9, 0.99], device=perr.device)).cpu().numpy()
+    # against the injected source: the sky peaks at the source or opposite
+    # to it depending on the delay convention; take the sign the plain
+    # extremizer's answers agree with
+    src = unit(inj["theta"], inj["phi"])
+    qs = torch.tensor([0.5, 0.9], device=perr.device)
+    e_plus = torch.rad2deg(angle(vr, canonical(src, gen.nrm)))
+    e_minus = torch.rad2deg(angle(vr, canonical(-src, gen.nrm)))
+    truth = canonical(src if e_plus.median() <= e_minus.median() else -src, gen.nrm)
+
+    def terr(v):
+        e = torch.rad2deg(angle(v, truth)).float()
+        return [float(x) for x in torch.quantile(e, qs).cpu().numpy()]
+
+    vs_truth = {"grid_search": terr(vr), "proposal_localisation": terr(vo), "trained_proposal_raw": terr(vp)}
+    if untrained is not None:
+        du = torch.cat([untrained.forward(feats[c0:c0 + untrained.max_batch]) for c0 in range(0, n, untrained.max_batch)])
+        vs_truth["untrained_proposal_raw"] = terr(canonical(du.double(), gen.nrm))
     return {
+        "err_vs_injection_deg_p50_p90": vs_truth,
         "skies": n,
         "proposal_err_deg_p50_p90_p99": [float(x) for x in q],
         "fallback_rate": nfb / n,
