@@ -139,14 +139,18 @@ struct TcArgs {
 	int hold;              // failure-detection tests: stage of CTA 0's range whose spectra are never loaded (-1: none)
 	// indexed spectra (IDX): row s of the batch, detector d, bin k is
 	// rows[row_off[s] + det_off[d] + k], k < Ku -- segments anywhere in a
-	// packed array, no tensor map
+	// packed array, no tensor map; the converter threads stage their own
+	// bins (16-byte asynchronous copies, zero-filled past a row's end or
+	// the batch), NFS - 1 stages ahead
 	const double2 *rows;
 	const long long *row_off;
 	int det_off[3];
 	int Ku;
 };
 
-constexpr int IDX_RP = 144;  // bytes per segment row in the indexed spectra ring (8 bins + 16 B pad: conflict-free)
+// indexed spectra ring: slot [detector][bin of the thread][converter
+// thread] of 16-byte elements, so a warp's loads are consecutive
+constexpr int IDX_PLANE = CONV_WARPS * 32 * 16;
 
 // Split the complex value (re, im) into NPART packed bf16x2 words (re in the
 // low half): part q is the round-to-nearest bf16 of what parts 0..q-1 left,
@@ -220,7 +224,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	// through it stay shared-memory accesses (an integer round trip would
 	// make them generic)
 	uint8_t *smem = smem_raw + ((1024 - ((uintptr_t) smem_raw & 1023)) & 1023);
-	const int f_slab = TM * (IDX ? IDX_RP : 128);
+	const int f_slab = TM * 128;  // = (KB / (CONV_WARPS / 4)) * IDX_PLANE
 	const int f_stage = a.n_det * f_slab;
 	const int btile = a.npad * KE * 2;
 	const int ab_bytes = a.B * NPART * btile;
@@ -276,44 +280,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	pdl_allow_dependents();
 	bool prior_done = false;  // converter warps: waited for the grid before (before the first flush)
 
-	if(warp == 0 && IDX) {
-		// ---------------- producer: indexed spectra ----------------
-		// one bulk copy per (detector, segment row) of the stage's bins
-		// present in the row, the whole warp issuing them after lane 0
-		// has declared the stage's bytes
-		int issued = 0;
-		for(int it = 0; it < nst; it++) {
-			const int u = u0 + it;
-			const int fs = it % NFS;
-			const bool ok = mbar_wait(smem_u32(&f_empty[fs]), ((it / NFS) & 1) ^ 1, abort_flag, a.err, 1, a.wait);
-			if(!__all_sync(0xffffffffu, ok))
-				break;
-			const int t = u / a.Kst, k0 = (u % a.Kst) * KB;
-			const int nb = a.Ku - k0 < KB ? a.Ku - k0 : KB;
-			const int nrow = a.S - t * TM < TM ? a.S - t * TM : TM;
-			const uint32_t bytes = (uint32_t) nb * 16u;
-			if(it == a.hold && blockIdx.x == 0) {
-				issued = it + 1;
-				continue;
-			}
-			if(lane == 0)
-				mbar_arrive_tx(smem_u32(&f_full[fs]), (uint32_t) (nrow * a.n_det) * bytes);
-			__syncwarp();
-			for(int q = lane; q < nrow * a.n_det; q += 32) {
-				const int d = q / nrow, r = q - d * nrow;
-				const double2 *src = a.rows + a.row_off[t * TM + r] + a.det_off[d] + k0;
-				bulk_g2s(smem_u32(sF + fs * f_stage + d * f_slab + r * IDX_RP), src, bytes, smem_u32(&f_full[fs]));
-			}
-			issued = it + 1;
-		}
-		if(lane == 0)
-			for(int it = (issued > NFS ? issued - NFS : 0); it < issued; it++)
-				mbar_drain(smem_u32(&f_full[it % NFS]), (it / NFS) & 1, a.wait);
-	} else if(warp == 0) {
+	if(warp == 0) {
 		// ---------------- producer: spectra only ----------------
 		// Runs NFS stages ahead of the converters, gated only by their
-		// release of the ring slot, across piece boundaries.
-		if(lane == 0) {
+		// release of the ring slot, across piece boundaries.  (Indexed
+		// spectra: the converters stage their own.)
+		if(lane == 0 && !IDX) {
 			int issued = 0;
 			for(int it = 0; it < nst; it++) {
 				const int u = u0 + it;
@@ -418,37 +390,72 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 		const int roff = (r >> 3) * 256 + (r & 7) * 16 + (g >> 1) * 128 + (g & 1) * 8;
 		PieceCursor pc{u0, u1, a.Kst};
 		int piece = 0;
+		// indexed spectra: this thread's bins of stage j of its range
+		// (row r, bins g BPT .. g BPT + BPT - 1 of every detector) into
+		// slot j % NFS, one copy group per stage (empty past the range)
+		const int ct = (warp - 2) * 32 + lane;
+		int cur_tile = -1;
+		const double2 *rowp = nullptr;
+		auto stage_in = [&](int j) {
+			if(j < nst) {
+				const int u = u0 + j, t = u / a.Kst, k0 = (u % a.Kst) * KB + g * BPT;
+				if(t != cur_tile) {
+					cur_tile = t;
+					const int s = t * TM + r;
+					rowp = s < a.S ? a.rows + a.row_off[s] : nullptr;
+				}
+				const uint32_t dst = smem_u32(sF + (j % NFS) * f_stage + ct * 16);
+#pragma unroll
+				for(int d = 0; d < TC_MAXDET; d++)
+#pragma unroll
+					for(int c = 0; c < BPT; c++)
+						if(d < a.n_det) {
+							const bool ok = rowp != nullptr && k0 + c < a.Ku;
+							cp_async16(dst + (uint32_t) ((d * BPT + c) * IDX_PLANE), ok ? (const void *) (rowp + a.det_off[d] + k0 + c) : (const void *) a.rows,
+								   ok ? 16u : 0u);
+						}
+			}
+			cp_async_commit();
+		};
+		if constexpr(IDX)
+			for(int j = 0; j < NFS - 1; j++)
+				stage_in(j);
 		for(int it = 0; it < nst; it++) {
 			bool first, last;
 			pc.step(u0 + it, first, last);
 			const int fs = it % NFS;
 			const uint32_t fph = (it / NFS) & 1;
-			const bool okf = mbar_wait(smem_u32(&f_full[fs]), fph, abort_flag, a.err, 5, a.wait);
-			if(!__all_sync(0xffffffffu, okf))
-				break;
+			if constexpr(IDX) {
+				// slot (it - 1) % NFS, read by this thread in the previous
+				// iteration, takes stage it + NFS - 1; stage it has landed
+				// once at most NFS - 1 groups are in flight
+				stage_in(it + NFS - 1);
+				cp_async_wait<NFS - 1>();
+			} else {
+				const bool okf = mbar_wait(smem_u32(&f_full[fs]), fph, abort_flag, a.err, 5, a.wait);
+				if(!__all_sync(0xffffffffu, okf))
+					break;
+			}
 			// this thread's bins of every detector, rounded to FP32
 			float2 f[TC_MAXDET][BPT];
 			{
-				const uint8_t *base = sF + fs * f_stage + r * (IDX ? IDX_RP : 128);
-				// indexed rows carry only the bins present and only rows of
-				// the batch: the rest of the slot is stale, masked here
-				const int uu = u0 + it;
-				const bool row_in = !IDX || (uu / a.Kst) * TM + r < a.S;
-				const int k0 = (uu % a.Kst) * KB;
+				const uint8_t *base = sF + fs * f_stage;
 #pragma unroll
 				for(int d = 0; d < TC_MAXDET; d++)
 #pragma unroll
 					for(int c = 0; c < BPT; c++) {
 						const int cc = g * BPT + c;
 						double2 v = make_double2(0, 0);
-						if(d < a.n_det && row_in && (!IDX || k0 + cc < a.Ku))
-							v = *(const double2 *) (base + d * f_slab + (IDX ? cc << 4 : ((cc ^ (r & 7)) << 4)));
+						if(d < a.n_det)
+							v = *(const double2 *) (base + (IDX ? (d * BPT + c) * IDX_PLANE + ct * 16 : d * f_slab + r * 128 + ((cc ^ (r & 7)) << 4)));
 						f[d][c] = make_float2((float) v.x, (float) v.y);
 					}
 			}
-			__syncwarp();
-			if(lane == 0)
-				mbar_arrive(smem_u32(&f_empty[fs]));
+			if constexpr(!IDX) {
+				__syncwarp();
+				if(lane == 0)
+					mbar_arrive(smem_u32(&f_empty[fs]));
+			}
 			const int as = it % NABS;
 			const uint32_t aph = (it / NABS) & 1;
 			const bool oke = mbar_wait(smem_u32(&ab_empty[as]), aph ^ 1, abort_flag, a.err, 6, a.wait);
@@ -533,6 +540,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 				mbar_arrive(smem_u32(acc_empty));
 			piece++;
 		}
+		// no copy of this thread may still land after an early exit
+		if constexpr(IDX)
+			cp_async_wait<0>();
 	}
 	tc_fence_before();
 	__syncthreads();
@@ -979,6 +989,7 @@ constexpr int EPI2_THREADS = 256;
 constexpr int EB = 3;
 constexpr int EPG = 4;
 constexpr int EPF = 4;  // partial sums fetched per thread per batch (EPG B (L+1) <= 1024)
+constexpr int EP_MAXREPS = 16;  // most workspace copies (ws_reps)
 
 template <int QMAX>
 __global__ void __launch_bounds__(EPI2_THREADS, QMAX <= 5 ? 3 : 2) k_epilogue_f32(const __grid_constant__ EpArgs e, float *acc)
@@ -1032,9 +1043,17 @@ __global__ void __launch_bounds__(EPI2_THREADS, QMAX <= 5 ? 3 : 2) k_epilogue_f3
 #pragma unroll
 		for(int k = 0; k < EPF; k++)
 			if(f_g[k] >= 0 && s0 + f_g[k] < e.S) {
-				float v = __ldcg(rows + f_src[k]);
-				for(int r = 1; r < e.reps; r++)
-					v += __ldcg(rows + (size_t) r * e.rep_stride + f_src[k]);
+				// the copies' loads are independent: issued eight at a
+				// time, summed as a tree
+				const float *src = rows + f_src[k];
+				float v = 0.f;
+				for(int r0 = 0; r0 < e.reps; r0 += 8) {
+					float p[8];
+#pragma unroll
+					for(int r = 0; r < 8; r++)
+						p[r] = r0 + r < e.reps ? __ldcg(src + (size_t) (r0 + r) * e.rep_stride) : 0.f;
+					v += ((p[0] + p[1]) + (p[2] + p[3])) + ((p[4] + p[5]) + (p[6] + p[7]));
+				}
 				dP[f_dst[k]] = v * (e.segw ? e.segw[(size_t) (s0 + f_g[k]) * e.B + f_b[k]] : 1.f);
 			}
 		if(ph_on) {
@@ -1044,6 +1063,11 @@ __global__ void __launch_bounds__(EPI2_THREADS, QMAX <= 5 ? 3 : 2) k_epilogue_f3
 			sPh[(buf * EPG + ph_g) * nph + ph_m] = make_double2(cs, sn);
 		}
 	};
+	// lanes of baselines b >= B are never fetched: zero them once (their
+	// weights are zero, but zero times stale shared memory can be NaN)
+	for(int i = threadIdx.x; i < 2 * EPG * nph; i += EPI2_THREADS)
+		sP[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+	__syncthreads();
 	int it = 0;
 	pdl_allow_dependents();
 	pdl_wait_prior();
@@ -1175,9 +1199,9 @@ static size_t ccs_smem_bytes(const BatchPlan &P)
 	return 1024 + f + aa + dd + 8 + bars;
 }
 
-static size_t tc_smem_bytes(const BatchPlan &P, bool x_in_tmem = false, bool indexed = false)
+static size_t tc_smem_bytes(const BatchPlan &P, bool x_in_tmem = false)
 {
-	const size_t f = (size_t) P.nf * P.n_det * TM * (indexed ? IDX_RP : 128);
+	const size_t f = (size_t) P.nf * P.n_det * TM * 128;
 	const size_t aa = x_in_tmem ? 0 : (size_t) P.nab * P.B * P.npart * A_TILE;
 	const size_t bb = (size_t) P.nb * P.B * P.npart * P.npad * KE * 2;
 	const size_t bars = 8 * (2 * P.nf + 2 * P.nab + 2 * P.nb + 3) + 16;
@@ -1375,6 +1399,7 @@ void *batch_plan_create(const BatchPlanDesc &d, int precision)
 				     cudaFuncSetAttribute(k_tc_contract<3, NF, 2, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
 				     cudaFuncSetAttribute(k_tc_contract<2, 4, 4, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
 				     cudaFuncSetAttribute(k_tc_contract<2, NF, 3, 3, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
+				     cudaFuncSetAttribute(k_tc_contract<2, 3, 2, 2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess ||
 				     cudaFuncSetAttribute(k_tc_contract<3, NF, 2, 3, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024) != cudaSuccess)) {
 				set_error("batch plan: cannot reserve %zu bytes of shared memory", tc_smem_bytes(*P));
 				fail = true;
@@ -1431,7 +1456,7 @@ static int ws_reps(const BatchPlan *P, int S)
 	if(!is_tc(P->precision) || S <= 0)
 		return 1;
 	const int tiles = (S + TM - 1) / TM;
-	return std::max(1, std::min(16, 16 / tiles));
+	return std::max(1, std::min(EP_MAXREPS, 16 / tiles));
 }
 
 size_t batch_workspace_bytes(const void *pp, int S)
@@ -1654,6 +1679,7 @@ int batch_run_ex(void *pp, const void *F, int S, long long ld, const double *gms
 		// shared-memory budget
 		P->nf = P->nf0;
 		P->nab = P->nab0;
+		P->nb = 3;
 		const int variant = pipe_variant >= 0 ? pipe_variant : (P->pipe.count(S) ? P->pipe[S] : 0);
 		bool x_tmem = false;
 		a.acol = 0;
@@ -1679,16 +1705,24 @@ int batch_run_ex(void *pp, const void *F, int S, long long ld, const double *gms
 			}
 		}
 		if(indexed) {
-			// the indexed ring is 12 % wider: the shallower X-operand ring,
-			// X in shared memory
+			// X in shared memory; the deepest spectra ring that fits (the
+			// converters' copies run NFS - 1 stages ahead): three stages
+			// with two-deep operand rings, else two
 			x_tmem = false;
 			a.acol = 0;
 			a.tmem_cols = P->tmem_cols;
-			P->nf = NF;
-			P->nab = P->npart == 3 ? 2 : 3;
-			if(tc_smem_bytes(*P, false, true) > 227 * 1024) {
+			P->nf = 3;
+			P->nab = 2;
+			P->nb = 2;
+			if(P->npart != 2 || tc_smem_bytes(*P) > 227 * 1024) {
+				P->nf = NF;
+				P->nab = P->npart == 3 ? 2 : 3;
+				P->nb = 3;
+			}
+			if(tc_smem_bytes(*P) > 227 * 1024) {
 				P->nf = P->nf0;
 				P->nab = P->nab0;
+				P->nb = 3;
 				set_error("batch_run: indexed spectra exceed the shared-memory budget at l_max %u", P->L);
 				return -1;
 			}
@@ -1696,9 +1730,11 @@ int batch_run_ex(void *pp, const void *F, int S, long long ld, const double *gms
 		if(P->ev_begin)
 			cudaEventRecord(P->ev_begin, st);
 		if(indexed && P->npart == 3)
-			CKB(launch_pdl(k_tc_contract<3, NF, 2, 3, false, true>, ctas, TC_THREADS, tc_smem_bytes(*P, false, true), st, P->tm, a));
+			CKB(launch_pdl(k_tc_contract<3, NF, 2, 3, false, true>, ctas, TC_THREADS, tc_smem_bytes(*P), st, P->tm, a));
+		else if(indexed && P->nf == 3)
+			CKB(launch_pdl(k_tc_contract<2, 3, 2, 2, false, true>, ctas, TC_THREADS, tc_smem_bytes(*P), st, P->tm, a));
 		else if(indexed)
-			CKB(launch_pdl(k_tc_contract<2, NF, 3, 3, false, true>, ctas, TC_THREADS, tc_smem_bytes(*P, false, true), st, P->tm, a));
+			CKB(launch_pdl(k_tc_contract<2, NF, 3, 3, false, true>, ctas, TC_THREADS, tc_smem_bytes(*P), st, P->tm, a));
 		else if(x_tmem)
 			CKB(launch_pdl(k_tc_contract<2, 4, 4, 3, true>, ctas, TC_THREADS, tc_smem_bytes(*P, true), st, P->tm, a));
 		else if(P->npart == 3)

@@ -9,8 +9,10 @@ is held to them directly:
   c1's native plan l_max ~547): every 64th bin row and two projections
   over all bins, relative L2 <= 1e-10; rotation plans <= 1e-12;
 * the drop-in correlator_network_integrate_power_fd: <= 1e-10;
-* the batched path with the GMST rotation fused: FP64 <= 1e-10, bf16x3
-  <= 1e-5 over the batch and 3e-5 per sky (the split-precision bound).
+* the batched path with the GMST rotation fused: FP64 <= 1e-10, FP32
+  <= 1e-5, bf16x3 <= 1e-5 over the batch and 3e-5 per sky (the
+  split-precision bound); c0 has a single baseline, so the epilogues' lanes
+  of absent baselines are exercised.
 
 And the reference's own test programs test/product_validate.c and
 test/rotation_validate.c, compiled unmodified against this repository's
@@ -86,7 +88,7 @@ def test_gpu_skies_match_reference(S, name):
     Fd = torch.from_numpy(np.ascontiguousarray(batch["F"])).cuda()
     gd = torch.from_numpy(np.ascontiguousarray(batch["gmst"])).cuda()
     ref = g["skies_gmst"]
-    for prec, tb, ts in (("fp64", 1e-10, 1e-10), ("bf16x3", 1e-5, 3e-5)):
+    for prec, tb, ts in (("fp64", 1e-10, 1e-10), ("fp32", 1e-5, 1e-5), ("bf16x3", 1e-5, 3e-5)):
         bp = S.BatchPlan(net, prec)
         sky = bp.integrate(Fd, gd).cpu().numpy()
         assert bp.status() == 0
