@@ -295,9 +295,18 @@ int sphrad_uneven_set_segments(sphrad_uneven_plan *plan, int n_seg, const int *b
  * at out_offset[s], (l_max_s + 1)^2 coefficients.  Returns n_seg. */
 int sphrad_uneven_layout(const sphrad_uneven_plan *plan, long long *in_offset, long long *out_offset, long long *in_total, long long *out_total);
 int sphrad_uneven_jobs(const sphrad_uneven_plan *plan);
-/* split-K of every job: > 0 fixed, 0 = each job's tuned (or default) value */
+/* tcgen05 precisions: every job's contraction in one persistent launch (the
+ * units of all jobs cut into equal ranges over the SMs), then the jobs'
+ * epilogues (1, the default); 0: one contraction and epilogue per job on a
+ * few streams, with per-job split-K.  sphrad_uneven_persistent reports
+ * whether the persistent launch is in use. */
+int sphrad_uneven_set_persistent(sphrad_uneven_plan *plan, int on);
+int sphrad_uneven_persistent(const sphrad_uneven_plan *plan);
+/* split-K of every job (per-job launches): > 0 fixed, 0 = each job's tuned
+ * (or default) value */
 int sphrad_uneven_set_split(sphrad_uneven_plan *plan, int split);
-/* tunes every job's split-K on these device spectra (CUDA events) */
+/* tunes every job's split-K (per-job launches) on these device spectra
+ * (CUDA events) */
 int sphrad_uneven_autotune(sphrad_uneven_plan *plan, const void *spectra, void *skies, void *cuda_stream);
 int sphrad_uneven_use_graph(sphrad_uneven_plan *plan, int on);
 /* spectra, skies: device arrays in the packed layouts */

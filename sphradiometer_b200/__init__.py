@@ -873,6 +873,14 @@ class UnevenPlan:
     def use_graph(self, on: bool):
         load().sphrad_uneven_use_graph(self._p, int(bool(on)))
 
+    def set_persistent(self, on: bool):
+        """One persistent contraction over every job (tcgen05 precisions,
+        the default) or one contraction per job."""
+        load().sphrad_uneven_set_persistent(self._p, int(bool(on)))
+
+    def persistent(self) -> bool:
+        return bool(load().sphrad_uneven_persistent(self._p))
+
     def autotune(self, spectra, out=None):
         import torch
         out = self._out(spectra, out)

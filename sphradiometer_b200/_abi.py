@@ -222,6 +222,8 @@ SIGNATURES = {
     "sphrad_uneven_set_split": (_i, [_vp, _i]),
     "sphrad_uneven_autotune": (_i, [_vp, _vp, _vp, _vp]),
     "sphrad_uneven_use_graph": (_i, [_vp, _i]),
+    "sphrad_uneven_set_persistent": (_i, [_vp, _i]),
+    "sphrad_uneven_persistent": (_i, [_vp]),
     "sphrad_uneven_integrate": (_i, [_vp, _vp, _vp, _vp]),
     "sphrad_uneven_kernels_per_call": (_i, [_vp]),
     "sphrad_sky_grid_new": (_vp, [_u, _i, _i, _i, _i]),

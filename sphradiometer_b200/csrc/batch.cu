@@ -35,6 +35,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -69,19 +70,23 @@ constexpr int A_TILE = TM * KE * 2;      // bytes of one bf16 A tile (4096)
 constexpr int CC_TS = 16;                // segments per CUDA-core block
 constexpr int CC_KC = 16;                // bins per CUDA-core stage
 constexpr int kMaxChain = 64;            // most pipeline stages one tcgen05 CTA accumulates
+constexpr int kEarlySegments = 512;      // batches whose epilogue releases the next grid early
 }  // namespace
 
 // Programmatic dependent launch.  A contraction lets the grid launched after
 // it (its epilogue) be scheduled once its own set-up is done; the epilogue
 // loads its tables, then waits for the contraction before it reads the
-// partial sums.  An epilogue lets the next grid start at once: only our
-// epilogues release a dependent early, so a contraction that starts early
-// follows an epilogue, which writes no input of it -- the contraction
-// streams and multiplies its spectra meanwhile and waits for that epilogue
-// (which re-zeroes the workspace) only before its first partial sums leave.
-// A kernel that follows any other work starts when that work has completed,
-// as without the attribute.  Without the launch attribute both
-// instructions return at once.
+// partial sums.  The epilogue of a small batch (at most kEarlySegments)
+// lets the next grid start at once: only our epilogues release a dependent
+// early, so a contraction that starts early follows an epilogue, which
+// writes no input of it -- the contraction streams and multiplies its
+// spectra meanwhile and waits for that epilogue (which re-zeroes the
+// workspace) only before its first partial sums leave.  (For large batches
+// the early start costs more than it hides: the next contraction's CTAs
+// and loads compete with the epilogue's stores.)  A kernel that follows any
+// other work starts when that work has completed, as without the
+// attribute.  Without the launch attribute both instructions return at
+// once.
 __device__ __forceinline__ void pdl_allow_dependents() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
 __device__ __forceinline__ void pdl_wait_prior() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
@@ -103,6 +108,7 @@ struct EpArgs {
 	const long long *out_row;
 	const unsigned *seg_L;
 	int accumulate;         // add into the outputs (FP64 atomics) instead of storing
+	int early;              // let the next grid start at once (small batches)
 };
 
 __device__ __forceinline__ long long d_lmoff(int L, int l, int m)
@@ -123,8 +129,24 @@ __device__ __forceinline__ void ep_put(double2 *p, double re, double im, int acc
 		*p = make_double2(re, im);
 }
 
+constexpr int kMaxJobs = 24;  // jobs of one indexed launch (carried in the kernel parameters)
+
+// One job of an indexed launch: segments of one sub-network at one DFT
+// length, read where they lie in a packed array: row s, detector d, bin k
+// is rows[row_off[s] + det_off[d] + k], k < Ku.
+struct TcJob {
+	int u_begin;            // its first (tile, stage) unit in the launch
+	int Kst, Ku, S, B, nd;  // stages, bins, segments, baselines, detectors
+	int bi[3], bj[3];       // baselines as detector indices 0 .. nd - 1
+	int det_off[3];
+	const long long *row_off;
+	const uint8_t *bops;    // its delay-table operand [Kst][B][NPART][npad KE bf16]
+	float *acc;             // its workspace [S][B][accstride] (one copy)
+};
+
 struct TcArgs {
 	int S, n_det, B, Kst, tiles, npad, tmem_cols, accstride;
+	int units;             // (tile, stage) units of the launch
 	int acol;              // first TMEM column of the X-operand ring (X in tensor memory)
 	int bi[TC_MAXB], bj[TC_MAXB];
 	const uint8_t *bops;   // [Kst][B][NPART][npad * KE bf16], UMMA layout
@@ -137,16 +159,23 @@ struct TcArgs {
 	unsigned *err;
 	unsigned long long wait;  // bound of every wait, clock cycles
 	int hold;              // failure-detection tests: stage of CTA 0's range whose spectra are never loaded (-1: none)
-	// indexed spectra (IDX): row s of the batch, detector d, bin k is
-	// rows[row_off[s] + det_off[d] + k], k < Ku -- segments anywhere in a
-	// packed array, no tensor map; the converter threads stage their own
-	// bins (16-byte asynchronous copies, zero-filled past a row's end or
-	// the batch), NFS - 1 stages ahead
+	// indexed spectra (IDX): jobs of segments anywhere in a packed array,
+	// no tensor map; the units of job i follow those of job i - 1, and B,
+	// n_det above are the largest of the jobs'.  The converter threads
+	// stage their own bins (16-byte asynchronous copies, zero-filled past a
+	// row's end or the batch), NFS - 1 stages ahead
 	const double2 *rows;
-	const long long *row_off;
-	int det_off[3];
-	int Ku;
+	int njobs;
+	TcJob job[kMaxJobs];
 };
+
+// the job of unit u, for units visited in increasing order from a cursor
+__device__ __forceinline__ const TcJob &job_seek(const TcArgs &a, int &jb, int u)
+{
+	while(jb + 1 < a.njobs && u >= a.job[jb + 1].u_begin)
+		jb++;
+	return a.job[jb];
+}
 
 // indexed spectra ring: slot [detector][bin of the thread][converter
 // thread] of 16-byte elements, so a warp's loads are consecutive
@@ -193,14 +222,15 @@ __device__ __forceinline__ void split_pair(float re, float im, uint32_t *w)
 // Launching tiles x ks CTAs reproduces the classic split-K cut (ks equal
 // stage ranges per tile).
 struct PieceCursor {
-	int u0, u1, Kst;
+	int u0, u1;
 	int pstart = 0, plen = 1, send = 0;  // current piece start and length, end of the run in this tile
-	// stage u of the range (called for u0, u0 + 1, ...): is it the first /
-	// last stage of its piece?
-	__device__ __forceinline__ void step(int u, bool &first, bool &last)
+	// stage u of the range (called for u0, u0 + 1, ...), in a job whose
+	// units start at ub, Kst stages per tile: is it the first / last stage
+	// of its piece?
+	__device__ __forceinline__ void step(int u, int ub, int Kst, bool &first, bool &last)
 	{
-		if(u == u0 || u % Kst == 0) {
-			const int tend = (u / Kst + 1) * Kst;
+		if(u == u0 || (u - ub) % Kst == 0) {
+			const int tend = ub + ((u - ub) / Kst + 1) * Kst;
 			send = u1 < tend ? u1 : tend;
 			const int len = send - u;
 			const int np = (len + kMaxChain - 1) / kMaxChain;
@@ -245,7 +275,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	volatile int *abort_flag = (volatile int *) (tslot + 1);
 
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-	const long long units = (long long) a.tiles * a.Kst;
+	const long long units = a.units;
 	const int u0 = (int) (units * blockIdx.x / gridDim.x);
 	const int u1 = (int) (units * (blockIdx.x + 1) / gridDim.x);
 	const int nst = u1 - u0;
@@ -316,11 +346,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 #pragma unroll
 			for(int i = 0; i < NPART; i++)
 				idesc[i] = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (((NPART - i) * a.npad) >> 3) << 17) | ((uint32_t) (TM >> 4) << 24);
-			PieceCursor pc{u0, u1, a.Kst};
-			int piece = 0;
+			PieceCursor pc{u0, u1};
+			int piece = 0, jb = 0;
 			for(int it = 0; it < nst; it++) {
 				bool first, last;
-				pc.step(u0 + it, first, last);
+				int nb = a.B;
+				if constexpr(IDX) {
+					const TcJob &J = job_seek(a, jb, u0 + it);
+					pc.step(u0 + it, J.u_begin, J.Kst, first, last);
+					nb = J.B;
+				} else
+					pc.step(u0 + it, 0, a.Kst, first, last);
 				const int as = it % NABS;
 				const uint32_t aph = (it / NABS) & 1;
 				const int bs = it % NBS;
@@ -334,7 +370,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 				if(!mbar_wait(smem_u32(&b_full[bs]), bph, abort_flag, a.err, 4, a.wait))
 					break;
 				tc_fence_after();
-				for(int b = 0; b < a.B; b++) {
+				for(int b = 0; b < nb; b++) {
 					const uint32_t d0 = tmem + (uint32_t) (b * NPART * a.npad);
 					const uint32_t b0 = smem_u32(sB + bs * ab_bytes + b * NPART * btile);
 #pragma unroll
@@ -365,13 +401,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 		// ---------------- producer: delay-table operand ----------------
 		// L2-resident; prefetched NBS stages ahead of the MMAs
 		if(lane == 0) {
-			int issued = 0;
+			int issued = 0, jb = 0;
 			for(int it = 0; it < nst; it++) {
 				const int bs = it % NBS;
 				if(!mbar_wait(smem_u32(&b_empty[bs]), ((it / NBS) & 1) ^ 1, abort_flag, a.err, 2, a.wait))
 					break;
-				mbar_arrive_tx(smem_u32(&b_full[bs]), ab_bytes);
-				bulk_g2s(smem_u32(sB + bs * ab_bytes), a.bops + (size_t) ((u0 + it) % a.Kst) * ab_bytes, ab_bytes, smem_u32(&b_full[bs]));
+				// (an indexed job's operand holds its own baselines)
+				const uint8_t *src = a.bops + (size_t) ((u0 + it) % a.Kst) * ab_bytes;
+				uint32_t bytes = (uint32_t) ab_bytes;
+				if constexpr(IDX) {
+					const TcJob &J = job_seek(a, jb, u0 + it);
+					bytes = (uint32_t) (J.B * NPART * btile);
+					src = J.bops + (size_t) ((u0 + it - J.u_begin) % J.Kst) * bytes;
+				}
+				mbar_arrive_tx(smem_u32(&b_full[bs]), bytes);
+				bulk_g2s(smem_u32(sB + bs * ab_bytes), src, bytes, smem_u32(&b_full[bs]));
 				issued = it + 1;
 			}
 			for(int it = (issued > NBS ? issued - NBS : 0); it < issued; it++)
@@ -388,30 +432,33 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 		const int r = (warp & 3) * 32 + lane;
 		const int g = (warp - 2) >> 2;
 		const int roff = (r >> 3) * 256 + (r & 7) * 16 + (g >> 1) * 128 + (g & 1) * 8;
-		PieceCursor pc{u0, u1, a.Kst};
-		int piece = 0;
+		PieceCursor pc{u0, u1};
+		int piece = 0, jb = 0;
 		// indexed spectra: this thread's bins of stage j of its range
-		// (row r, bins g BPT .. g BPT + BPT - 1 of every detector) into
-		// slot j % NFS, one copy group per stage (empty past the range)
+		// (row r, bins g BPT .. g BPT + BPT - 1 of every detector of the
+		// stage's job) into slot j % NFS, one copy group per stage (empty
+		// past the range)
 		const int ct = (warp - 2) * 32 + lane;
-		int cur_tile = -1;
+		int in_jb = 0, cur_jb = -1, cur_tile = -1;
 		const double2 *rowp = nullptr;
 		auto stage_in = [&](int j) {
 			if(j < nst) {
-				const int u = u0 + j, t = u / a.Kst, k0 = (u % a.Kst) * KB + g * BPT;
-				if(t != cur_tile) {
+				const TcJob &J = job_seek(a, in_jb, u0 + j);
+				const int lu = u0 + j - J.u_begin, t = lu / J.Kst, k0 = (lu % J.Kst) * KB + g * BPT;
+				if(t != cur_tile || in_jb != cur_jb) {
 					cur_tile = t;
+					cur_jb = in_jb;
 					const int s = t * TM + r;
-					rowp = s < a.S ? a.rows + a.row_off[s] : nullptr;
+					rowp = s < J.S ? a.rows + J.row_off[s] : nullptr;
 				}
 				const uint32_t dst = smem_u32(sF + (j % NFS) * f_stage + ct * 16);
 #pragma unroll
 				for(int d = 0; d < TC_MAXDET; d++)
 #pragma unroll
 					for(int c = 0; c < BPT; c++)
-						if(d < a.n_det) {
-							const bool ok = rowp != nullptr && k0 + c < a.Ku;
-							cp_async16(dst + (uint32_t) ((d * BPT + c) * IDX_PLANE), ok ? (const void *) (rowp + a.det_off[d] + k0 + c) : (const void *) a.rows,
+						if(d < J.nd) {
+							const bool ok = rowp != nullptr && k0 + c < J.Ku;
+							cp_async16(dst + (uint32_t) ((d * BPT + c) * IDX_PLANE), ok ? (const void *) (rowp + J.det_off[d] + k0 + c) : (const void *) a.rows,
 								   ok ? 16u : 0u);
 						}
 			}
@@ -422,7 +469,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 				stage_in(j);
 		for(int it = 0; it < nst; it++) {
 			bool first, last;
-			pc.step(u0 + it, first, last);
+			// this stage's job: detectors, baselines, segments, tile
+			int nd = a.n_det, nb = a.B, nS = a.S, tile = (u0 + it) / a.Kst;
+			const int *bi = a.bi, *bj = a.bj;
+			float *accp = a.acc;
+			if constexpr(IDX) {
+				const TcJob &J = job_seek(a, jb, u0 + it);
+				pc.step(u0 + it, J.u_begin, J.Kst, first, last);
+				nd = J.nd;
+				nb = J.B;
+				nS = J.S;
+				tile = (u0 + it - J.u_begin) / J.Kst;
+				bi = J.bi;
+				bj = J.bj;
+				accp = J.acc;
+			} else
+				pc.step(u0 + it, 0, a.Kst, first, last);
 			const int fs = it % NFS;
 			const uint32_t fph = (it / NFS) & 1;
 			if constexpr(IDX) {
@@ -446,7 +508,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 					for(int c = 0; c < BPT; c++) {
 						const int cc = g * BPT + c;
 						double2 v = make_double2(0, 0);
-						if(d < a.n_det)
+						if(d < nd)
 							v = *(const double2 *) (base + (IDX ? (d * BPT + c) * IDX_PLANE + ct * 16 : d * f_slab + r * 128 + ((cc ^ (r & 7)) << 4)));
 						f[d][c] = make_float2((float) v.x, (float) v.y);
 					}
@@ -465,9 +527,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 				tc_fence_after();  // the MMAs that read the slot have retired
 #pragma unroll
 			for(int b = 0; b < TC_MAXB3; b++) {
-				if(b >= a.B)
+				if(b >= nb)
 					break;
-				const int da = a.bi[b], db = a.bj[b];
+				const int da = bi[b], db = bj[b];
 				uint32_t part[BPT][NPART];
 #pragma unroll
 				for(int c = 0; c < BPT; c++) {
@@ -506,12 +568,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			if(!__all_sync(0xffffffffu, got))
 				break;
 			const int q = warp & 3;
-			const int s = ((u0 + it) / a.Kst) * TM + q * 32 + lane;
+			const int s = tile * TM + q * 32 + lane;
 			if(!prior_done) {
 				pdl_wait_prior();
 				prior_done = true;
 			}
-			for(int b = (warp - 2) >> 2; b < a.B; b += CONV_WARPS / 4) {
+			for(int b = (warp - 2) >> 2; b < nb; b += CONV_WARPS / 4) {
 				for(int c0 = 0; c0 < a.accstride; c0 += 16) {
 					uint32_t v[16], w[16];
 					const uint32_t ta = tmem + ((uint32_t) (q * 32) << 16) + (uint32_t) (b * NPART * a.npad + c0);
@@ -523,8 +585,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 						for(int j = 0; j < 16; j++)
 							v[j] = __float_as_uint(__uint_as_float(v[j]) + __uint_as_float(w[j]));
 					}
-					if(s < a.S) {
-						float *dst = a.acc + (size_t) (blockIdx.x % a.reps) * a.rep_stride + ((size_t) s * a.B + b) * a.accstride + c0;
+					if(s < nS) {
+						float *dst = accp + (size_t) (blockIdx.x % a.reps) * a.rep_stride + ((size_t) s * nb + b) * a.accstride + c0;
 #pragma unroll
 						for(int j = 0; j < 4; j++)
 							if(c0 + 4 * j < a.accstride)
@@ -678,15 +740,17 @@ __global__ void k_cc_contract(const __grid_constant__ CcArgs c)
 //   warp 1          bulk-copy producer of the delay-table ring: per stage
 //                   a [KE][B][NPL] block of T (row 2k: w_k Re D, row 2k+1:
 //                   -w_k Im D, l zero-padded to NPL = 12 G), L2-resident;
-//   warps 2 ..      compute warps, one per (baseline b, l-group g of 12):
-//                   each stage they first form together X_b = F_j conj(F_i)
+//   warps 2 ..      compute warps, 4 / RPT per (baseline b, l-group g
+//                   of 12), each taking 32 RPT of the tile's rows: each
+//                   stage they first form together X_b = F_j conj(F_i)
 //                   in FP64 for all 128 rows x 8 bins of every baseline
 //                   into a double-buffered operand sA[b][k][row] of T, meet
-//                   at a bounded mbarrier, then thread (lane) accumulates
-//                   rows 4 lane .. 4 lane + 3 x l 12 g .. 12 g + 11 of
-//                   baseline b: per k one vector load of 4 X values and
-//                   three (FP64: six) broadcast vector loads of 12 D values
-//                   for 48 FMAs.
+//                   at a bounded mbarrier, then a thread accumulates RPT
+//                   consecutive rows x l 12 g .. 12 g + 11 of baseline b:
+//                   per k one vector load of RPT X values and three (FP64:
+//                   six) broadcast vector loads of 12 D values for 12 RPT
+//                   FMAs.  FP32 runs RPT = 2 where the warps fit (twice
+//                   the warps of RPT = 4 to hide shared-memory latency).
 // Partial sums leave at the end of each piece (the part of the CTA's range
 // inside one tile) by atomics into the split-K workspace [S][B][accstride].
 constexpr int CCS_LG = 12;  // l per compute warp
@@ -700,16 +764,17 @@ struct CcsArgs {
 	unsigned long long wait;  // bound of every wait, clock cycles
 };
 
-template <class T, int NFS, int NWMAX>
+template <class T, int NFS, int NWMAX, int RPT>
 __global__ void __launch_bounds__(32 * (2 + NWMAX), 1) k_cc_stream(const __grid_constant__ CUtensorMap tmF, const __grid_constant__ CcsArgs a)
 {
+	constexpr int RS = 4 / RPT;  // compute warps per (baseline, l-group): row quarters of 32 RPT rows
 	extern __shared__ uint8_t smem_raw[];
 	// aligned by an offset on the shared array itself, so that accesses
 	// through it stay shared-memory accesses (an integer round trip would
 	// make them generic)
 	uint8_t *smem = smem_raw + ((1024 - ((uintptr_t) smem_raw & 1023)) & 1023);
 	constexpr int NDS = 2;  // delay-table ring depth
-	const int NW = a.B * a.G;
+	const int NW = a.B * a.G * RS;
 	const int NPL = a.G * CCS_LG;
 	const int f_slab = TM * 128;
 	const int f_stage = a.n_det * f_slab;
@@ -787,11 +852,12 @@ __global__ void __launch_bounds__(32 * (2 + NWMAX), 1) k_cc_stream(const __grid_
 	if(cw >= NW)
 		return;
 	const int ctid = cw * 32 + lane, nct = NW * 32;
-	const int b = cw / a.G, g = cw % a.G;
+	const int b = cw / (a.G * RS), g = (cw / RS) % a.G, h = cw % RS;
 	const int l0 = g * CCS_LG;
-	T acc[4][CCS_LG];
+	const int row0 = h * 32 * RPT + RPT * lane;  // this thread's first tile row
+	T acc[RPT][CCS_LG];
 #pragma unroll
-	for(int r = 0; r < 4; r++)
+	for(int r = 0; r < RPT; r++)
 #pragma unroll
 		for(int j = 0; j < CCS_LG; j++)
 			acc[r][j] = 0;
@@ -835,12 +901,20 @@ __global__ void __launch_bounds__(32 * (2 + NWMAX), 1) k_cc_stream(const __grid_
 		if(!__all_sync(0xffffffffu, okd))
 			break;
 		// ---- accumulate ----
-		const T *ap = xa + (size_t) b * KE * TM + 4 * lane;
+		const T *ap = xa + (size_t) b * KE * TM + row0;
 		const T *dp = sD + ds * d_stage + b * NPL + l0;
 #pragma unroll 2
 		for(int k = 0; k < KE; k++) {
-			T x[4], dv[CCS_LG];
-			if constexpr(sizeof(T) == 4) {
+			T x[RPT], dv[CCS_LG];
+			if constexpr(sizeof(T) == 4 && RPT == 2) {
+				const float2 v = *(const float2 *) (ap + k * TM);
+				x[0] = v.x, x[1] = v.y;
+#pragma unroll
+				for(int q = 0; q < CCS_LG / 4; q++) {
+					const float4 w = *(const float4 *) (dp + k * a.B * NPL + 4 * q);
+					dv[4 * q] = w.x, dv[4 * q + 1] = w.y, dv[4 * q + 2] = w.z, dv[4 * q + 3] = w.w;
+				}
+			} else if constexpr(sizeof(T) == 4) {
 				const float4 v = *(const float4 *) (ap + k * TM);
 				x[0] = v.x, x[1] = v.y, x[2] = v.z, x[3] = v.w;
 #pragma unroll
@@ -849,6 +923,7 @@ __global__ void __launch_bounds__(32 * (2 + NWMAX), 1) k_cc_stream(const __grid_
 					dv[4 * q] = w.x, dv[4 * q + 1] = w.y, dv[4 * q + 2] = w.z, dv[4 * q + 3] = w.w;
 				}
 			} else {
+				static_assert(RPT == 4, "FP64 runs four rows per thread");
 				const double2 v0 = *(const double2 *) (ap + k * TM), v1 = *(const double2 *) (ap + k * TM + 2);
 				x[0] = v0.x, x[1] = v0.y, x[2] = v1.x, x[3] = v1.y;
 #pragma unroll
@@ -858,7 +933,7 @@ __global__ void __launch_bounds__(32 * (2 + NWMAX), 1) k_cc_stream(const __grid_
 				}
 			}
 #pragma unroll
-			for(int r = 0; r < 4; r++)
+			for(int r = 0; r < RPT; r++)
 #pragma unroll
 				for(int j = 0; j < CCS_LG; j++)
 					acc[r][j] = fma(x[r], dv[j], acc[r][j]);
@@ -876,8 +951,8 @@ __global__ void __launch_bounds__(32 * (2 + NWMAX), 1) k_cc_stream(const __grid_
 				prior_done = true;
 			}
 #pragma unroll
-			for(int r = 0; r < 4; r++) {
-				const int s = tile * TM + 4 * lane + r;
+			for(int r = 0; r < RPT; r++) {
+				const int s = tile * TM + row0 + r;
 				if(s < a.S) {
 					T *dst = (T *) a.acc + ((size_t) s * a.B + b) * a.accstride + l0;
 #pragma unroll
@@ -934,7 +1009,8 @@ __global__ void k_epilogue(const __grid_constant__ EpArgs e, T *acc)
 	T *sP = (T *) (sPh + 2 * e.L + 1);                              // [B][Lp1]
 	const int s = blockIdx.x;
 	T *row = acc + (size_t) s * e.B * e.accstride;
-	pdl_allow_dependents();
+	if(e.early)
+		pdl_allow_dependents();
 	pdl_wait_prior();
 	for(int i = threadIdx.x; i < e.B * e.Lp1; i += blockDim.x) {
 		const int b = i / e.Lp1;
@@ -1069,7 +1145,8 @@ __global__ void __launch_bounds__(EPI2_THREADS, QMAX <= 5 ? 3 : 2) k_epilogue_f3
 		sP[i] = make_float4(0.f, 0.f, 0.f, 0.f);
 	__syncthreads();
 	int it = 0;
-	pdl_allow_dependents();
+	if(e.early)
+		pdl_allow_dependents();
 	pdl_wait_prior();
 	if((int) blockIdx.x < nb)
 		fetch(blockIdx.x, 0);
@@ -1130,6 +1207,7 @@ struct BatchPlan {
 	uint8_t *bops = nullptr;   // tcgen05 operand table
 	void *dops = nullptr;      // streamed CUDA-core operand table [Kst][KE][B][12 ccG] (T), or null
 	int ccG = 0;               // l-groups of 12 of the streamed CUDA-core path
+	int ccR = 4;               // its rows per thread: 2 (twice the compute warps) where they fit, else 4
 	int Kst = 0, npad = 0, tmem_cols = 0;
 	int npart = 2, nf = NF, nab = 3, nb = 5;  // bf16 parts per operand; spectrum, X-operand and D-operand ring depths
 	void *W = nullptr;         // [B][nq] complex T
@@ -1184,7 +1262,8 @@ static bool is_tc(int precision) { return precision == kPrecBF16x3 || precision 
 // detectors)
 static bool is_stream(const BatchPlan *P) { return is_tc(P->precision) || P->dops != nullptr; }
 
-constexpr int CCS_NWMAX_F32 = 15;  // compute warps: l_max <= 59 with 3 baselines
+constexpr int CCS_NWMAX_F32 = 15;  // compute warps at 4 rows per thread: l_max <= 59 with 3 baselines
+constexpr int CCS_NWMAX_F32_R2 = 18;  // at 2 rows per thread (two warps per baseline and l-group): l_max <= 35
 constexpr int CCS_NWMAX_F64 = 9;   // l_max <= 35 with 3 baselines
 constexpr int CCS_NFS_F32 = 3, CCS_NFS_F64 = 2;
 
@@ -1199,14 +1278,19 @@ static size_t ccs_smem_bytes(const BatchPlan &P)
 	return 1024 + f + aa + dd + 8 + bars;
 }
 
-static size_t tc_smem_bytes(const BatchPlan &P, bool x_in_tmem = false)
+static size_t tc_smem_for(int nf, int nab, int nb, int n_det, int B, int npart, int npad, bool x_in_tmem)
 {
-	const size_t f = (size_t) P.nf * P.n_det * TM * 128;
-	const size_t aa = x_in_tmem ? 0 : (size_t) P.nab * P.B * P.npart * A_TILE;
-	const size_t bb = (size_t) P.nb * P.B * P.npart * P.npad * KE * 2;
-	const size_t bars = 8 * (2 * P.nf + 2 * P.nab + 2 * P.nb + 3) + 16;
+	const size_t f = (size_t) nf * n_det * TM * 128;
+	const size_t aa = x_in_tmem ? 0 : (size_t) nab * B * npart * A_TILE;
+	const size_t bb = (size_t) nb * B * npart * npad * KE * 2;
+	const size_t bars = 8 * (2 * nf + 2 * nab + 2 * nb + 3) + 16;
 	// 1 KB for aligning the base, 4 KB of slack past the last tile
 	return 1024 + f + aa + bb + bars + 4096;
+}
+
+static size_t tc_smem_bytes(const BatchPlan &P, bool x_in_tmem = false)
+{
+	return tc_smem_for(P.nf, P.nab, P.nb, P.n_det, P.B, P.npart, P.npad, x_in_tmem);
 }
 
 void batch_plan_destroy(void *pp)
@@ -1429,8 +1513,13 @@ void *batch_plan_create(const BatchPlanDesc &d, int precision)
 			if(stream_sync())
 				fail = true;
 			dfree(Dt64);
-			cudaError_t ra = dbl ? cudaFuncSetAttribute(k_cc_stream<double, CCS_NFS_F64, CCS_NWMAX_F64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024)
-					     : cudaFuncSetAttribute(k_cc_stream<float, CCS_NFS_F32, CCS_NWMAX_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+			// FP32: two rows per thread and twice the compute warps where
+			// they fit (more warps to hide the shared-memory latency)
+			P->ccR = (!dbl && 2 * B * G <= CCS_NWMAX_F32_R2) ? 2 : 4;
+			cudaError_t ra = dbl ? cudaFuncSetAttribute(k_cc_stream<double, CCS_NFS_F64, CCS_NWMAX_F64, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024)
+					     : P->ccR == 2
+						       ? cudaFuncSetAttribute(k_cc_stream<float, CCS_NFS_F32, CCS_NWMAX_F32_R2, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024)
+						       : cudaFuncSetAttribute(k_cc_stream<float, CCS_NFS_F32, CCS_NWMAX_F32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
 			if(!fail && (ccs_smem_bytes(*P) > 227 * 1024 || ra != cudaSuccess)) {
 				// the tiled CUDA-core kernel serves this plan instead
 				dfree(P->dops);
@@ -1585,6 +1674,31 @@ static int ensure_tmap(BatchPlan *P, const void *F, int S, long long ld)
 	return 0;
 }
 
+// the epilogue of e.S segments whose partial sums are in ws
+static int launch_epilogue(const BatchPlan *P, const EpArgs &e, void *ws, cudaStream_t st)
+{
+	const int S = e.S;
+	const size_t el = P->precision == kPrecFP64 ? sizeof(double) : sizeof(float);
+	const size_t esmem = (size_t) P->B * P->Lp1 * el + (2 * P->L + 1) * sizeof(double2);
+	const int qmax = (P->nq + EPI2_THREADS - 1) / EPI2_THREADS;
+	if(P->precision != kPrecFP64 && P->B <= EB && qmax <= 10 && EPG * P->B * P->Lp1 <= EPF * EPI2_THREADS && EPG * (P->L + 1) <= EPI2_THREADS) {
+		// resident blocks only (3 per SM by registers at QMAX 5, 2 at 10)
+		const int sms = sm_count();
+		const int per_sm = qmax <= 5 ? 3 : 2;
+		const int nbatch = (S + EPG - 1) / EPG;
+		const int grid = nbatch < per_sm * sms ? nbatch : per_sm * sms;
+		const size_t esm2 = (size_t) 2 * EPG * (P->L + 1) * (sizeof(double2) + sizeof(float4));
+		if(qmax <= 5)
+			CKB(launch_pdl(k_epilogue_f32<5>, grid, EPI2_THREADS, esm2, st, e, (float *) ws));
+		else
+			CKB(launch_pdl(k_epilogue_f32<10>, grid, EPI2_THREADS, esm2, st, e, (float *) ws));
+	} else if(P->precision == kPrecFP64)
+		CKB(launch_pdl(k_epilogue<double>, S, 128, esmem, st, e, (double *) ws));
+	else
+		CKB(launch_pdl(k_epilogue<float>, S, 128, esmem, st, e, (float *) ws));
+	return 0;
+}
+
 int batch_run(void *pp, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream_v, int split,
 	      const float *segw, int pipe_variant)
 {
@@ -1631,6 +1745,7 @@ int batch_run_ex(void *pp, const void *F, int S, long long ld, const double *gms
 	e.accumulate = ix ? ix->accumulate : 0;
 	e.reps = ws_reps(P, S);
 	e.rep_stride = (size_t) S * P->B * P->accstride;
+	e.early = S <= kEarlySegments;
 
 	if(is_tc(P->precision)) {
 		if(((uintptr_t) F & 15) || ((ld * 16) & 15)) {
@@ -1660,18 +1775,32 @@ int batch_run_ex(void *pp, const void *F, int S, long long ld, const double *gms
 		a.acc = (float *) ws;
 		a.wait = P->wait_limit ? P->wait_limit : kWaitCycles;
 		a.hold = P->hold_stage;
-		if(indexed) {
-			a.rows = (const double2 *) F;
-			a.row_off = ix->row_off;
-			for(int d = 0; d < P->n_det && d < 3; d++)
-				a.det_off[d] = ix->det_off[d];
-			a.Ku = P->Ku;
-		}
 		a.reps = e.reps;
 		a.rep_stride = e.rep_stride;
 		a.err = P->err;
 		const int tiles = (S + TM - 1) / TM;
 		a.tiles = tiles;
+		a.units = tiles * P->Kst;
+		if(indexed) {
+			a.rows = (const double2 *) F;
+			a.njobs = 1;
+			TcJob &J = a.job[0];
+			J.u_begin = 0;
+			J.Kst = P->Kst;
+			J.Ku = P->Ku;
+			J.S = S;
+			J.B = P->B;
+			J.nd = P->n_det;
+			for(int b = 0; b < P->B && b < 3; b++) {
+				J.bi[b] = P->bi[b];
+				J.bj[b] = P->bj[b];
+			}
+			for(int d = 0; d < P->n_det && d < 3; d++)
+				J.det_off[d] = (int) ix->det_off[d];
+			J.row_off = ix->row_off;
+			J.bops = P->bops;
+			J.acc = (float *) ws;
+		}
 		// CTAs: an explicit split-K factor ks cuts every tile's stages into
 		// ks ranges; otherwise the tuned or default count
 		const int ctas = split > 0 ? tiles * split : batch_pick_ctas(P, S);
@@ -1774,13 +1903,15 @@ int batch_run_ex(void *pp, const void *F, int S, long long ld, const double *gms
 		const int tiles = (S + TM - 1) / TM;
 		c.tiles = tiles;
 		const int ctas = split > 0 ? tiles * split : batch_pick_ctas(P, S);
-		const int threads = 32 * (2 + P->B * P->ccG);
+		const int threads = 32 * (2 + P->B * P->ccG * (4 / P->ccR));
 		if(P->ev_begin)
 			cudaEventRecord(P->ev_begin, st);
 		if(P->precision == kPrecFP64)
-			CKB(launch_pdl(k_cc_stream<double, CCS_NFS_F64, CCS_NWMAX_F64>, ctas, threads, ccs_smem_bytes(*P), st, P->tm, c));
+			CKB(launch_pdl(k_cc_stream<double, CCS_NFS_F64, CCS_NWMAX_F64, 4>, ctas, threads, ccs_smem_bytes(*P), st, P->tm, c));
+		else if(P->ccR == 2)
+			CKB(launch_pdl(k_cc_stream<float, CCS_NFS_F32, CCS_NWMAX_F32_R2, 2>, ctas, threads, ccs_smem_bytes(*P), st, P->tm, c));
 		else
-			CKB(launch_pdl(k_cc_stream<float, CCS_NFS_F32, CCS_NWMAX_F32>, ctas, threads, ccs_smem_bytes(*P), st, P->tm, c));
+			CKB(launch_pdl(k_cc_stream<float, CCS_NFS_F32, CCS_NWMAX_F32, 4>, ctas, threads, ccs_smem_bytes(*P), st, P->tm, c));
 		if(P->ev_end)
 			cudaEventRecord(P->ev_end, st);
 		launches++;
@@ -1826,28 +1957,154 @@ int batch_run_ex(void *pp, const void *F, int S, long long ld, const double *gms
 			cudaEventRecord(P->ev_end, st);
 		launches++;
 	}
-	const size_t el = P->precision == kPrecFP64 ? sizeof(double) : sizeof(float);
-	const size_t esmem = (size_t) P->B * P->Lp1 * el + (2 * P->L + 1) * sizeof(double2);
-	const int qmax = (P->nq + EPI2_THREADS - 1) / EPI2_THREADS;
-	if(P->precision != kPrecFP64 && P->B <= EB && qmax <= 10 && EPG * P->B * P->Lp1 <= EPF * EPI2_THREADS && EPG * (P->L + 1) <= EPI2_THREADS) {
-		int sms = 148, dev = 0;
-		cudaGetDevice(&dev);
-		cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-		// resident blocks only (3 per SM by registers at QMAX 5, 2 at 10)
-		const int per_sm = qmax <= 5 ? 3 : 2;
-		const int nbatch = (S + EPG - 1) / EPG;
-		const int grid = nbatch < per_sm * sms ? nbatch : per_sm * sms;
-		const size_t esm2 = (size_t) 2 * EPG * (P->L + 1) * (sizeof(double2) + sizeof(float4));
-		if(qmax <= 5)
-			CKB(launch_pdl(k_epilogue_f32<5>, grid, EPI2_THREADS, esm2, st, e, (float *) ws));
-		else
-			CKB(launch_pdl(k_epilogue_f32<10>, grid, EPI2_THREADS, esm2, st, e, (float *) ws));
-	} else if(P->precision == kPrecFP64)
-		CKB(launch_pdl(k_epilogue<double>, S, 128, esmem, st, e, (double *) ws));
-	else
-		CKB(launch_pdl(k_epilogue<float>, S, 128, esmem, st, e, (float *) ws));
+	if(launch_epilogue(P, e, ws, st))
+		return -1;
 	launches++;
 	P->last_kernels = launches;
+	CKB(cudaGetLastError());
+	return 0;
+}
+
+// ------------------------------------------------------------------------
+// several indexed jobs in one persistent contraction
+// ------------------------------------------------------------------------
+size_t batch_job_ws_bytes(const void *pp, int S)
+{
+	const BatchPlan *P = (const BatchPlan *) pp;
+	return (size_t) (S > 0 ? S : 0) * P->B * P->accstride * sizeof(float);
+}
+
+// The units of every job, one after the other, cut into equal contiguous
+// ranges over the CTAs (stream-K across the jobs): one launch per kMaxJobs
+// jobs instead of one per job, every SM streaming until the whole batch is
+// done.  Jobs: tcgen05 plans of one precision and l_max, each with its
+// segments' rows (ix.row_off, ix.det_off) in the packed array F and its
+// own zeroed workspace (batch_job_ws_bytes).  Returns the launches made,
+// -1 on failure.
+int batch_contract_multi(const MultiJob *jobs, int njobs, const void *F, void *stream_v, int ctas)
+{
+	cudaStream_t st = (cudaStream_t) stream_v;
+	if(njobs <= 0)
+		return 0;
+	const BatchPlan *P0 = (const BatchPlan *) jobs[0].plan;
+	if((uintptr_t) F & 15) {
+		set_error("batch_contract_multi: spectra must be 16-byte aligned");
+		return -1;
+	}
+	int Bmax = 0, ndmax = 0;
+	for(int i = 0; i < njobs; i++) {
+		const BatchPlan *P = (const BatchPlan *) jobs[i].plan;
+		if(!is_tc(P->precision) || P->precision != P0->precision || P->npad != P0->npad || P->accstride != P0->accstride || !jobs[i].ix.row_off ||
+		   !jobs[i].ws || jobs[i].S < 0) {
+			set_error("batch_contract_multi: job %d is not an indexed tcgen05 job of the first job's precision and l_max", i);
+			return -1;
+		}
+		Bmax = std::max(Bmax, P->B);
+		ndmax = std::max(ndmax, P->n_det);
+	}
+	const int npart = P0->npart, npad = P0->npad;
+	int cols = 32;
+	while(cols < npart * Bmax * npad)
+		cols <<= 1;
+	// the deepest spectra ring that fits the largest job: three stages
+	// with two-deep operand rings, else two
+	int nf = 3, nab = 2, nb = 2;
+	size_t smem = tc_smem_for(nf, nab, nb, ndmax, Bmax, npart, npad, false);
+	if(npart != 2 || smem > 227 * 1024) {
+		nf = NF;
+		nab = npart == 3 ? 2 : 3;
+		nb = 3;
+		smem = tc_smem_for(nf, nab, nb, ndmax, Bmax, npart, npad, false);
+	}
+	if(cols > 512 || smem > 227 * 1024) {
+		set_error("batch_contract_multi: %d baselines at l_max %u exceed the tensor or shared memory", Bmax, P0->L);
+		return -1;
+	}
+	int launches = 0;
+	for(int j0 = 0; j0 < njobs; j0 += kMaxJobs) {
+		const int nj = std::min(kMaxJobs, njobs - j0);
+		TcArgs a;
+		memset(&a, 0, sizeof(a));
+		a.n_det = ndmax;
+		a.B = Bmax;
+		a.Kst = 1;
+		a.npad = npad;
+		a.tmem_cols = cols;
+		a.accstride = P0->accstride;
+		a.reps = 1;
+		a.err = P0->err;
+		a.wait = P0->wait_limit ? P0->wait_limit : kWaitCycles;
+		a.hold = -1;
+		a.rows = (const double2 *) F;
+		a.njobs = nj;
+		long long units = 0;
+		for(int k = 0; k < nj; k++) {
+			const MultiJob &m = jobs[j0 + k];
+			const BatchPlan *P = (const BatchPlan *) m.plan;
+			TcJob &J = a.job[k];
+			J.u_begin = (int) units;
+			J.Kst = P->Kst;
+			J.Ku = P->Ku;
+			J.S = m.S;
+			J.B = P->B;
+			J.nd = P->n_det;
+			for(int b = 0; b < P->B && b < 3; b++) {
+				J.bi[b] = P->bi[b];
+				J.bj[b] = P->bj[b];
+			}
+			for(int d = 0; d < P->n_det && d < 3; d++)
+				J.det_off[d] = (int) m.ix.det_off[d];
+			J.row_off = m.ix.row_off;
+			J.bops = P->bops;
+			J.acc = (float *) m.ws;
+			units += (long long) ((m.S + TM - 1) / TM) * P->Kst;
+		}
+		if(units == 0)
+			continue;
+		if(units > INT_MAX / 2) {
+			set_error("batch_contract_multi: %lld units in one launch", units);
+			return -1;
+		}
+		a.units = (int) units;
+		const int nct = (int) std::min<long long>(ctas > 0 ? ctas : sm_count(), units);
+		if(npart == 3)
+			CKB(launch_pdl(k_tc_contract<3, NF, 2, 3, false, true>, nct, TC_THREADS, smem, st, P0->tm, a));
+		else if(nf == 3)
+			CKB(launch_pdl(k_tc_contract<2, 3, 2, 2, false, true>, nct, TC_THREADS, smem, st, P0->tm, a));
+		else
+			CKB(launch_pdl(k_tc_contract<2, NF, 3, 3, false, true>, nct, TC_THREADS, smem, st, P0->tm, a));
+		launches++;
+	}
+	return launches;
+}
+
+// The epilogue of one job of batch_contract_multi, after it
+int batch_epilogue_job(const MultiJob &m, void *sky, void *stream_v)
+{
+	const BatchPlan *P = (const BatchPlan *) m.plan;
+	if(m.S <= 0)
+		return 0;
+	EpArgs e;
+	e.S = m.S;
+	e.B = P->B;
+	e.Lp1 = P->Lp1;
+	e.L = P->L;
+	e.accstride = P->accstride;
+	e.nq = P->nq;
+	e.lq = P->lq;
+	e.mq = P->mq;
+	e.W = P->W;
+	e.gmst = nullptr;
+	e.segw = m.segw;
+	e.sky = (double2 *) sky;
+	e.out_row = m.ix.out_row;
+	e.seg_L = m.ix.seg_L;
+	e.accumulate = m.ix.accumulate;
+	e.reps = 1;
+	e.rep_stride = (size_t) m.S * P->B * P->accstride;
+	e.early = 0;
+	if(launch_epilogue(P, e, m.ws, (cudaStream_t) stream_v))
+		return -1;
 	CKB(cudaGetLastError());
 	return 0;
 }

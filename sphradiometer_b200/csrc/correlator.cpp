@@ -1094,6 +1094,8 @@ int sphrad::batch_integrate_packed(sphrad_batch_plan *p, const void *fseries_dev
 			    ix);
 }
 
+void *sphrad::batch_impl(sphrad_batch_plan *p) { return p ? p->impl : nullptr; }
+
 int sphrad::batch_is_tc(const sphrad_batch_plan *p)
 {
 	return p->impl && (batch_precision(p->impl) == SPHRAD_PREC_BF16X3 || batch_precision(p->impl) == SPHRAD_PREC_BF16X6);

@@ -59,6 +59,11 @@ const char *last_error() { return g_err.c_str(); }
 // ------------------------------------------------------------------------
 static std::mutex g_ctx_mu;
 static std::unordered_map<int, cudaStream_t> g_streams;
+// per device, a stream-ordered memory pool for the scratch of the
+// synchronous drop-in calls, which keeps what it has allocated: a call
+// takes and returns its scratch without cudaMalloc / cudaFree (whose free
+// synchronises the whole device)
+static std::unordered_map<int, cudaMemPool_t> g_pools;
 
 int ensure_device()
 {
@@ -75,6 +80,19 @@ int ensure_device()
 		cudaStream_t s;
 		CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
 		g_streams[dev] = s;
+	}
+	if(!g_pools.count(dev)) {
+		cudaMemPoolProps props;
+		memset(&props, 0, sizeof(props));
+		props.allocType = cudaMemAllocationTypePinned;
+		props.handleTypes = cudaMemHandleTypeNone;
+		props.location.type = cudaMemLocationTypeDevice;
+		props.location.id = dev;
+		cudaMemPool_t pool;
+		CK(cudaMemPoolCreate(&pool, &props));
+		uint64_t keep = ~0ull;
+		CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+		g_pools[dev] = pool;
 	}
 	return 0;
 }
@@ -150,6 +168,35 @@ void dfree(void *p)
 		cudaFree(p);
 }
 
+void *dscratch(size_t bytes)
+{
+	if(alloc_fault_due()) {
+		set_error("scratch of %zu bytes: injected allocation failure", bytes);
+		return nullptr;
+	}
+	if(ensure_device())
+		return nullptr;
+	const int dev = current_device();
+	cudaMemPool_t pool;
+	{
+		std::lock_guard<std::mutex> lk(g_ctx_mu);
+		pool = g_pools[dev];
+	}
+	void *p = nullptr;
+	cudaError_t e = cudaMallocFromPoolAsync(&p, bytes ? bytes : 16, pool, S());
+	if(e != cudaSuccess) {
+		set_error("scratch of %zu bytes: %s", bytes, cudaGetErrorString(e));
+		return nullptr;
+	}
+	return p;
+}
+
+void dscratch_free(void *p)
+{
+	if(p)
+		cudaFreeAsync(p, S());
+}
+
 int h2d(void *dst, const void *src, size_t bytes)
 {
 	CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, S()));
@@ -178,8 +225,8 @@ int dmemset(void *dst, int value, size_t bytes)
 struct DBuf {
 	void *p = nullptr;
 	DBuf() = default;
-	explicit DBuf(size_t bytes) { p = dmalloc(bytes); }
-	~DBuf() { dfree(p); }
+	explicit DBuf(size_t bytes) { p = dscratch(bytes); }
+	~DBuf() { dscratch_free(p); }
 	DBuf(const DBuf &) = delete;
 	DBuf &operator=(const DBuf &) = delete;
 	template <class T> T *as() const { return (T *) p; }
@@ -602,7 +649,7 @@ void forget_rot_mirror(const void *key)
 	std::lock_guard<std::mutex> lk(g_rot_mu);
 	auto it = g_rot_cache.find(key);
 	if(it != g_rot_cache.end()) {
-		dfree(it->second.D);
+		dscratch_free(it->second.D);
 		g_rot_cache.erase(it);
 	}
 }
@@ -617,8 +664,8 @@ int rotate_series(unsigned l_max, int polar, const double *series, const double 
 		std::lock_guard<std::mutex> lk(g_rot_mu);
 		RotMirror &m = g_rot_cache[cache_key];
 		if(!m.D || m.gen != gen || m.l_max != l_max) {
-			dfree(m.D);
-			m.D = (double2 *) dmalloc((len ? len : 1) * sizeof(double2));
+			dscratch_free(m.D);
+			m.D = (double2 *) dscratch((len ? len : 1) * sizeof(double2));
 			if(!m.D)
 				return -1;
 			if(len && h2d(m.D, Dflat, len * sizeof(double2)))

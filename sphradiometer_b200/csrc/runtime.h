@@ -30,6 +30,11 @@ void *dmalloc(size_t bytes);  // NULL + error on failure
 int set_alloc_fault(long n);
 bool alloc_fault_due();
 void dfree(void *p);
+// scratch ordered on the library stream, from a per-device pool that keeps
+// its memory: for buffers whose every use is on that stream (the drop-in
+// calls, which synchronise before they return)
+void *dscratch(size_t bytes);  // NULL + error on failure
+void dscratch_free(void *p);
 int h2d(void *dst, const void *src, size_t bytes);       // async on lib stream
 int d2h(void *dst, const void *src, size_t bytes);       // async on lib stream
 int dmemset(void *dst, int value, size_t bytes);         // async on lib stream
@@ -118,6 +123,18 @@ struct BatchIdx {
 int batch_run_ex(void *plan, const void *F, int S, long long ld, const double *gmst, void *sky, void *ws, size_t ws_bytes, void *stream, int split,
 		 const float *segw, int pipe_variant, const BatchIdx *ix);
 int batch_precision(const void *plan);
+// several indexed jobs (plans of one tcgen05 precision and l_max) in one
+// persistent contraction, then each job's epilogue
+struct MultiJob {
+	void *plan;             // batch.cu plan (sphrad_batch_plan's impl)
+	int S;
+	BatchIdx ix;            // rows in the packed spectra, packed outputs
+	const float *segw;      // [S][B] baseline factors, or NULL
+	void *ws;               // its own workspace, zeroed (batch_job_ws_bytes)
+};
+size_t batch_job_ws_bytes(const void *plan, int S);
+int batch_contract_multi(const MultiJob *jobs, int njobs, const void *F, void *stream, int ctas);
+int batch_epilogue_job(const MultiJob &job, void *sky, void *stream);
 int batch_pipe_variant(const void *plan, int S);
 int batch_run_host(void *plan, const void *F_host, int S, long long ld, const double *gmst_host, void *sky_host);
 int batch_pick_split(const void *plan, int S);
@@ -308,5 +325,6 @@ int set_peak_refine_method(int method);
 int batch_integrate_packed(::sphrad_batch_plan *plan, const void *fseries_dev, int n_seg, long long ld, const BatchIdx *ix, void *sky_dev, void *workspace,
 			   size_t workspace_bytes, void *stream, int split, const float *baseline_factor);
 int batch_is_tc(const ::sphrad_batch_plan *plan);
+void *batch_impl(::sphrad_batch_plan *plan);  // its batch.cu plan
 
 }  // namespace sphrad

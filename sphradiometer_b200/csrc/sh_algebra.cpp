@@ -70,8 +70,8 @@ void *ext_buffer(std::vector<std::pair<void *, size_t>> &v, size_t i, size_t nee
 // RAII device buffer over the runtime allocator
 struct Dev {
 	void *p = nullptr;
-	explicit Dev(size_t bytes) { p = dmalloc(bytes); }
-	~Dev() { dfree(p); }
+	explicit Dev(size_t bytes) { p = dscratch(bytes); }
+	~Dev() { dscratch_free(p); }
 	Dev(const Dev &) = delete;
 	Dev &operator=(const Dev &) = delete;
 };

@@ -91,6 +91,11 @@ struct sphrad_uneven_plan {
 	cudaStream_t side[kSlots] = {};
 	cudaEvent_t ev[kSlots + 1] = {};
 	int fixed_split = 0;
+	// persistent launch (tcgen05 precisions): every job's contraction in
+	// one launch, each job with its own zeroed workspace at ws_off
+	int persistent = 1;
+	void *ws_multi = nullptr;
+	std::vector<size_t> ws_off;
 	// graph
 	int use_graph = 1;
 	cudaStream_t cap = nullptr;
@@ -132,7 +137,9 @@ static void drop_jobs(sphrad_uneven_plan *p)
 	dfree(p->F);
 	dfree(p->sky);
 	dfree(p->ws);
-	p->F = p->sky = p->ws = nullptr;
+	dfree(p->ws_multi);
+	p->F = p->sky = p->ws = p->ws_multi = nullptr;
+	p->ws_off.clear();
 	p->F_bytes = p->sky_bytes = p->ws_bytes = 0;
 	drop_graph(p);
 }
@@ -379,6 +386,20 @@ extern "C" int sphrad_uneven_set_segments(sphrad_uneven_plan *p, int n_seg, cons
 		return -1;
 	if(dmemset(p->ws, 0, wsb * p->n_slots) || stream_sync())
 		return -1;
+	// the persistent launch's workspaces: one per job, side by side
+	bool all_indexed = !p->jobs.empty();
+	for(const Job &j : p->jobs)
+		all_indexed = all_indexed && j.indexed;
+	if(all_indexed) {
+		size_t tot = 0;
+		for(const Job &j : p->jobs) {
+			p->ws_off.push_back(tot);
+			tot += (batch_job_ws_bytes(batch_impl(j.bp), j.S) + 255) / 256 * 256;
+		}
+		p->ws_multi = dmalloc(tot ? tot : 256);
+		if(!p->ws_multi || dmemset(p->ws_multi, 0, tot ? tot : 256) || stream_sync())
+			return -1;
+	}
 	return 0;
 }
 
@@ -409,10 +430,64 @@ static void *job_F(sphrad_uneven_plan *p, const Job &j) { return (char *) p->F +
 static void *job_ws(sphrad_uneven_plan *p, const Job &j) { return (char *) p->ws + (size_t) j.slot * p->ws_bytes; }
 static void *job_sky(sphrad_uneven_plan *p, const Job &) { return p->sky; }
 
-// the jobs forked over the slots' streams from st, joined back, then the
-// combine into the outputs on st
+// the outputs zeroed, every job's contraction in one persistent launch on
+// st, then the jobs' epilogues forked over the slots' streams and joined
+// back
+static int run_persistent(sphrad_uneven_plan *p, const void *in, void *out, cudaStream_t st)
+{
+	cudaStream_t ss[kSlots];
+	ss[0] = st;
+	for(int s = 1; s < p->n_slots; s++)
+		ss[s] = p->side[s];
+	if(cudaMemsetAsync(out, 0, (size_t) p->out_total * 16, st) != cudaSuccess) {
+		set_error("uneven: output zeroing failed");
+		return -1;
+	}
+	std::vector<MultiJob> mj(p->jobs.size());
+	for(size_t i = 0; i < p->jobs.size(); i++) {
+		const Job &j = p->jobs[i];
+		MultiJob &m = mj[i];
+		m.plan = batch_impl(j.bp);
+		m.S = j.S;
+		m.ix.row_off = j.d_rowoff;
+		for(size_t d = 0; d < j.det.size() && d < 3; d++)
+			m.ix.det_off[d] = (long long) j.det[d] * j.Ku;
+		m.ix.out_row = j.d_outrow;
+		m.ix.seg_L = j.d_segL;
+		m.ix.accumulate = 1;
+		m.segw = j.d_w;
+		m.ws = (char *) p->ws_multi + p->ws_off[i];
+	}
+	const int nl = batch_contract_multi(mj.data(), (int) mj.size(), in, st, 0);
+	if(nl < 0)
+		return -1;
+	if(cudaEventRecord(p->ev[0], st) != cudaSuccess) {
+		set_error("uneven: event record failed");
+		return -1;
+	}
+	for(int s = 1; s < p->n_slots; s++)
+		if(cudaStreamWaitEvent(ss[s], p->ev[0], 0) != cudaSuccess) {
+			set_error("uneven: stream fork failed");
+			return -1;
+		}
+	for(size_t i = 0; i < mj.size(); i++)
+		if(batch_epilogue_job(mj[i], out, ss[i % p->n_slots]))
+			return -1;
+	for(int s = 1; s < p->n_slots; s++)
+		if(cudaEventRecord(p->ev[s], ss[s]) != cudaSuccess || cudaStreamWaitEvent(st, p->ev[s], 0) != cudaSuccess) {
+			set_error("uneven: stream join failed");
+			return -1;
+		}
+	p->kernels = nl + (int) mj.size();
+	return 0;
+}
+
+// the jobs forked over the slots' streams from st, each its own
+// contraction and epilogue, joined back
 static int run_jobs(sphrad_uneven_plan *p, const void *in, void *out, cudaStream_t st)
 {
+	if(p->persistent && p->ws_multi)
+		return run_persistent(p, in, out, st);
 	int k = 0;
 	cudaStream_t ss[kSlots];
 	ss[0] = st;
@@ -464,6 +539,15 @@ extern "C" int sphrad_uneven_set_split(sphrad_uneven_plan *p, int split)
 	drop_graph(p);
 	return 0;
 }
+
+extern "C" int sphrad_uneven_set_persistent(sphrad_uneven_plan *p, int on)
+{
+	p->persistent = on ? 1 : 0;
+	drop_graph(p);
+	return 0;
+}
+
+extern "C" int sphrad_uneven_persistent(const sphrad_uneven_plan *p) { return p->persistent && p->ws_multi ? 1 : 0; }
 
 extern "C" int sphrad_uneven_use_graph(sphrad_uneven_plan *p, int on)
 {

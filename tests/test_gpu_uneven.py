@@ -8,8 +8,8 @@ truncated to the segment's l_max.
 Tolerances: bf16x3 contraction, relative L2 <= 1e-5 over the batch and
 3e-5 per sky; FP64 contraction 1e-10.  Graph replay and direct launches
 differ only in the order of the FP32 atomic split-K sums (<= 1e-6 of the
-largest coefficient), other split-K factors also in how the FP32 sums are
-grouped (<= 4e-6).
+largest coefficient), other split-K factors, and the persistent launch
+against per-job launches, also in how the FP32 sums are grouped (<= 4e-6).
 """
 import numpy as np
 import pytest
@@ -91,6 +91,7 @@ def test_uneven_graph_split_and_three_detectors(S):
     plan = S.UnevenPlan(pos, DT, batch["buckets"], 32)
     plan.set_segments(batch["bucket"], batch["mask"], batch["l_max"])
     assert plan.jobs() <= 4  # one sub-network: one job per bucket
+    plan.set_persistent(False)
     plan.use_graph(False)
     direct = plan.integrate(batch["spectra"]).clone()
     plan.use_graph(True)
@@ -106,6 +107,35 @@ def test_uneven_graph_split_and_three_detectors(S):
     assert float((tuned - fixed).abs().max() / fixed.abs().max()) < 4e-6
     ref = oracle_skies(S, pos, batch, plan, 32)
     got = plan.unpack(tuned)
+    assert max(rel(g, r) for g, r in zip(got, ref)) < 3e-5
+    plan.close()
+
+
+def test_uneven_persistent_launch(S):
+    """Every job's contraction in one persistent launch (the default for
+    tcgen05 precisions): one contraction plus one epilogue per job per
+    call; the same skies as one launch per job up to the grouping of the
+    FP32 sums, and the oracle's within the bf16x3 bounds."""
+    pos = W.random_positions(4, W.R_EARTH_S, W.rng_for(9))
+    batch = W.make_uneven_batch(pos, 96, seed=21, t_range=(0.25, 2.0), l_choices=(16, 32, 48), buckets=(1024, 2048, 4096, 8192))
+    plan = S.UnevenPlan(pos, DT, batch["buckets"], 48)
+    plan.set_segments(batch["bucket"], batch["mask"], batch["l_max"])
+    assert plan.persistent() and 2 <= plan.jobs() <= 24
+    pers = plan.integrate(batch["spectra"]).clone()
+    assert plan.kernels_per_call() == 1 + plan.jobs()
+    plan.set_persistent(False)
+    per_job = plan.integrate(batch["spectra"]).clone()
+    assert not plan.persistent()
+    plan.set_persistent(True)
+    again = plan.integrate(batch["spectra"]).clone()
+    scale = float(per_job.abs().max())
+    assert float((pers - per_job).abs().max()) < 4e-6 * scale
+    assert float((pers - again).abs().max()) < 1e-6 * scale
+    got = plan.unpack(pers)
+    ref = oracle_skies(S, pos, batch, plan, 48)
+    num = np.sqrt(sum(np.linalg.norm(g - r) ** 2 for g, r in zip(got, ref)))
+    den = np.sqrt(sum(np.linalg.norm(r) ** 2 for r in ref))
+    assert num / den < 1e-5, num / den
     assert max(rel(g, r) for g, r in zip(got, ref)) < 3e-5
     plan.close()
 
