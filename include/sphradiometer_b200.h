@@ -153,9 +153,7 @@ int sphrad_batch_status(sphrad_batch_plan *plan);
 /* Bound of every device-side wait of the contraction kernels, in SM clock
  * cycles (0: the default, about 2 s at the B200's clock).  Polar plans. */
 int sphrad_batch_set_wait_limit(sphrad_batch_plan *plan, unsigned long long cycles);
-/* Failure-detection hook for tests (tcgen05 plans, spectra by tensor map:
- * not the indexed spectra of uneven batches, which the converter threads
- * copy themselves): the spectrum producer
+/* Failure-detection hook for tests (tcgen05 plans): the spectrum producer
  * of the contraction's first CTA skips loading stage `stage` of its range
  * (-1: off), so the wait on that stage runs out; with a short wait limit
  * the call returns, sphrad_batch_status reports the code, and later calls

@@ -14,14 +14,16 @@
 // segment's baselines assigned to the job, 0 otherwise, so each sky is the
 // mean over its own B_s baselines, correlator.c:1004).  A call zeroes the
 // packed outputs and runs every job: the contraction reads the job's
-// segments where they lie in the caller's packed spectra (one bulk copy per
-// segment row and stage; the FP32 / FP64 precisions gather them first) and
-// the epilogue adds each segment's sky into its packed output, truncated to
-// the segment's own l_max (FP64 atomics: a segment covered by two jobs gets
-// the same sum in either order).  The jobs are spread over a few streams
-// (longest first, each to the least loaded stream) so that small jobs
-// overlap.  The whole sequence can be captured once into a CUDA graph
-// (forked over the streams) and replayed.
+// segments where they lie in the caller's packed spectra (the FP32 / FP64
+// precisions gather them first) and the epilogue adds each segment's sky
+// into its packed output, truncated to the segment's own l_max (FP64
+// atomics: a segment covered by two jobs gets the same sum in either
+// order).  With a tcgen05 precision all jobs' contractions run in one
+// persistent launch (batch_contract_multi) and the jobs' epilogues are
+// forked over a few streams; otherwise, or on request, each job runs its
+// own contraction and epilogue, the jobs spread over the streams (longest
+// first, each to the least loaded stream).  The whole sequence can be
+// captured once into a CUDA graph and replayed.
 #include <sphradiometer_b200.h>
 #include <sphradiometer/correlator.h>
 #include <sphradiometer/instrument.h>
