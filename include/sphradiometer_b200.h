@@ -153,7 +153,9 @@ int sphrad_batch_status(sphrad_batch_plan *plan);
 /* Bound of every device-side wait of the contraction kernels, in SM clock
  * cycles (0: the default, about 2 s at the B200's clock).  Polar plans. */
 int sphrad_batch_set_wait_limit(sphrad_batch_plan *plan, unsigned long long cycles);
-/* Failure-detection hook for tests (tcgen05 plans): the spectrum producer
+/* Failure-detection hook for tests (tcgen05 plans, spectra by tensor map:
+ * not the indexed spectra of uneven batches, which the converter threads
+ * copy themselves): the spectrum producer
  * of the contraction's first CTA skips loading stage `stage` of its range
  * (-1: off), so the wait on that stage runs out; with a short wait limit
  * the call returns, sphrad_batch_status reports the code, and later calls
@@ -293,10 +295,10 @@ int sphrad_uneven_set_segments(sphrad_uneven_plan *plan, int n_seg, const int *b
  * at out_offset[s], (l_max_s + 1)^2 coefficients.  Returns n_seg. */
 int sphrad_uneven_layout(const sphrad_uneven_plan *plan, long long *in_offset, long long *out_offset, long long *in_total, long long *out_total);
 int sphrad_uneven_jobs(const sphrad_uneven_plan *plan);
-/* tcgen05 precisions: every job's contraction in one persistent launch (the
- * units of all jobs cut into equal ranges over the SMs), then the jobs'
- * epilogues (1, the default); 0: one contraction and epilogue per job on a
- * few streams, with per-job split-K.  sphrad_uneven_persistent reports
+/* 0 (the default): one contraction and epilogue per job on a few streams,
+ * with per-job split-K; 1 (tcgen05 precisions): every job's contraction in
+ * one persistent launch (the units of all jobs cut into equal ranges over
+ * the SMs), then the jobs' epilogues.  sphrad_uneven_persistent reports
  * whether the persistent launch is in use. */
 int sphrad_uneven_set_persistent(sphrad_uneven_plan *plan, int on);
 int sphrad_uneven_persistent(const sphrad_uneven_plan *plan);

@@ -874,8 +874,8 @@ class UnevenPlan:
         load().sphrad_uneven_use_graph(self._p, int(bool(on)))
 
     def set_persistent(self, on: bool):
-        """One persistent contraction over every job (tcgen05 precisions,
-        the default) or one contraction per job."""
+        """One persistent contraction over every job (tcgen05 precisions)
+        or one contraction per job (the default)."""
         load().sphrad_uneven_set_persistent(self._p, int(bool(on)))
 
     def persistent(self) -> bool:

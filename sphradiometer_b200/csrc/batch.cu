@@ -161,9 +161,9 @@ struct TcArgs {
 	int hold;              // failure-detection tests: stage of CTA 0's range whose spectra are never loaded (-1: none)
 	// indexed spectra (IDX): jobs of segments anywhere in a packed array,
 	// no tensor map; the units of job i follow those of job i - 1, and B,
-	// n_det above are the largest of the jobs'.  The producer warp copies
-	// them with coalesced 16-byte asynchronous copies (zero-filled past a
-	// row's end or the job) into the tensor map's slot layout
+	// n_det above are the largest of the jobs'.  The converter threads
+	// stage their own bins (16-byte asynchronous copies, zero-filled past a
+	// row's end or the batch), NFS - 1 stages ahead
 	const double2 *rows;
 	int njobs;
 	TcJob job[kMaxJobs];
@@ -177,6 +177,9 @@ __device__ __forceinline__ const TcJob &job_seek(const TcArgs &a, int &jb, int u
 	return a.job[jb];
 }
 
+// indexed spectra ring: slot [detector][bin of the thread][converter
+// thread] of 16-byte elements, so a warp's loads are consecutive
+constexpr int IDX_PLANE = CONV_WARPS * 32 * 16;
 
 // Split the complex value (re, im) into NPART packed bf16x2 words (re in the
 // low half): part q is the round-to-nearest bf16 of what parts 0..q-1 left,
@@ -251,7 +254,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	// through it stay shared-memory accesses (an integer round trip would
 	// make them generic)
 	uint8_t *smem = smem_raw + ((1024 - ((uintptr_t) smem_raw & 1023)) & 1023);
-	const int f_slab = TM * 128;
+	const int f_slab = TM * 128;  // = (KB / (CONV_WARPS / 4)) * IDX_PLANE
 	const int f_stage = a.n_det * f_slab;
 	const int btile = a.npad * KE * 2;
 	const int ab_bytes = a.B * NPART * btile;
@@ -270,7 +273,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	uint64_t *mma_done = acc_empty + 1;     // every MMA of the CTA retired
 	uint32_t *tslot = (uint32_t *) (mma_done + 1);
 	volatile int *abort_flag = (volatile int *) (tslot + 1);
-	long long *sRow = (long long *) (mma_done + 2);  // IDX: the current tile's row offsets [TM] (-1: past the job)
 
 	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 	const long long units = a.units;
@@ -280,7 +282,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 
 	if(threadIdx.x == 0) {
 		for(int i = 0; i < NFS; i++) {
-			mbar_init(smem_u32(&f_full[i]), IDX ? 32 : 1);
+			mbar_init(smem_u32(&f_full[i]), 1);
 			mbar_init(smem_u32(&f_empty[i]), CONV_WARPS);
 		}
 		for(int i = 0; i < NABS; i++) {
@@ -308,54 +310,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	pdl_allow_dependents();
 	bool prior_done = false;  // converter warps: waited for the grid before (before the first flush)
 
-	if(warp == 0 && IDX) {
-		// ---------------- producer: indexed spectra ----------------
-		// The whole warp copies each stage into the same swizzled slot
-		// layout the tensor map writes: eight lanes per (detector, row)
-		// take its stage's 8 bins (16 bytes each, coalesced 128 bytes),
-		// four rows per instruction; rows past the job's segments and bins
-		// past a row's end are zero-filled by the copy.  Every lane then
-		// arrives on the stage's barrier once its copies have landed.
-		const int c = lane & 7, sub = lane >> 3;
-		int jb = 0, cur_jb = -1, cur_tile = -1;
-		for(int it = 0; it < nst; it++) {
-			const int u = u0 + it;
-			const int fs = it % NFS;
-			const bool ok = mbar_wait(smem_u32(&f_empty[fs]), ((it / NFS) & 1) ^ 1, abort_flag, a.err, 1, a.wait);
-			if(!__all_sync(0xffffffffu, ok))
-				break;
-			const TcJob &J = job_seek(a, jb, u);
-			const int lu = u - J.u_begin, t = lu / J.Kst, k = (lu % J.Kst) * KB + c;
-			if(t != cur_tile || jb != cur_jb) {
-				cur_tile = t;
-				cur_jb = jb;
-				__syncwarp();
-				for(int r = lane; r < TM; r += 32)
-					sRow[r] = t * TM + r < J.S ? J.row_off[t * TM + r] : -1;
-				__syncwarp();
-			}
-			if(it == a.hold && blockIdx.x == 0)
-				continue;  // withheld on request: the stage's barrier never completes
-			const uint32_t slot = smem_u32(sF + fs * f_stage);
-			for(int r0 = 0; r0 < TM; r0 += 4) {
-				const int r = r0 + sub;
-				const long long ro = sRow[r];
-				const bool in = ro >= 0 && k < J.Ku;
-				const uint32_t dst = slot + (uint32_t) (r * 128 + ((c ^ (r & 7)) << 4));
-#pragma unroll
-				for(int d = 0; d < TC_MAXDET; d++)
-					if(d < J.nd)
-						cp_async16(dst + (uint32_t) (d * f_slab), in ? (const void *) (a.rows + ro + J.det_off[d] + k) : (const void *) a.rows, in ? 16u : 0u);
-			}
-			cp_async_mbar_arrive(smem_u32(&f_full[fs]));
-		}
-		// no copy of this warp may still land after it exits
-		cp_async_wait<0>();
-	} else if(warp == 0) {
+	if(warp == 0) {
 		// ---------------- producer: spectra only ----------------
 		// Runs NFS stages ahead of the converters, gated only by their
-		// release of the ring slot, across piece boundaries.
-		if(lane == 0) {
+		// release of the ring slot, across piece boundaries.  (Indexed
+		// spectra: the converters stage their own.)
+		if(lane == 0 && !IDX) {
 			int issued = 0;
 			for(int it = 0; it < nst; it++) {
 				const int u = u0 + it;
@@ -474,6 +434,39 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 		const int roff = (r >> 3) * 256 + (r & 7) * 16 + (g >> 1) * 128 + (g & 1) * 8;
 		PieceCursor pc{u0, u1};
 		int piece = 0, jb = 0;
+		// indexed spectra: this thread's bins of stage j of its range
+		// (row r, bins g BPT .. g BPT + BPT - 1 of every detector of the
+		// stage's job) into slot j % NFS, one copy group per stage (empty
+		// past the range)
+		const int ct = (warp - 2) * 32 + lane;
+		int in_jb = 0, cur_jb = -1, cur_tile = -1;
+		const double2 *rowp = nullptr;
+		auto stage_in = [&](int j) {
+			if(j < nst) {
+				const TcJob &J = job_seek(a, in_jb, u0 + j);
+				const int lu = u0 + j - J.u_begin, t = lu / J.Kst, k0 = (lu % J.Kst) * KB + g * BPT;
+				if(t != cur_tile || in_jb != cur_jb) {
+					cur_tile = t;
+					cur_jb = in_jb;
+					const int s = t * TM + r;
+					rowp = s < J.S ? a.rows + J.row_off[s] : nullptr;
+				}
+				const uint32_t dst = smem_u32(sF + (j % NFS) * f_stage + ct * 16);
+#pragma unroll
+				for(int d = 0; d < TC_MAXDET; d++)
+#pragma unroll
+					for(int c = 0; c < BPT; c++)
+						if(d < J.nd) {
+							const bool ok = rowp != nullptr && k0 + c < J.Ku;
+							cp_async16(dst + (uint32_t) ((d * BPT + c) * IDX_PLANE), ok ? (const void *) (rowp + J.det_off[d] + k0 + c) : (const void *) a.rows,
+								   ok ? 16u : 0u);
+						}
+			}
+			cp_async_commit();
+		};
+		if constexpr(IDX)
+			for(int j = 0; j < NFS - 1; j++)
+				stage_in(j);
 		for(int it = 0; it < nst; it++) {
 			bool first, last;
 			// this stage's job: detectors, baselines, segments, tile
@@ -494,9 +487,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 				pc.step(u0 + it, 0, a.Kst, first, last);
 			const int fs = it % NFS;
 			const uint32_t fph = (it / NFS) & 1;
-			const bool okf = mbar_wait(smem_u32(&f_full[fs]), fph, abort_flag, a.err, 5, a.wait);
-			if(!__all_sync(0xffffffffu, okf))
-				break;
+			if constexpr(IDX) {
+				// slot (it - 1) % NFS, read by this thread in the previous
+				// iteration, takes stage it + NFS - 1; stage it has landed
+				// once at most NFS - 1 groups are in flight
+				stage_in(it + NFS - 1);
+				cp_async_wait<NFS - 1>();
+			} else {
+				const bool okf = mbar_wait(smem_u32(&f_full[fs]), fph, abort_flag, a.err, 5, a.wait);
+				if(!__all_sync(0xffffffffu, okf))
+					break;
+			}
 			// this thread's bins of every detector, rounded to FP32
 			float2 f[TC_MAXDET][BPT];
 			{
@@ -508,13 +509,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 						const int cc = g * BPT + c;
 						double2 v = make_double2(0, 0);
 						if(d < nd)
-							v = *(const double2 *) (base + d * f_slab + r * 128 + ((cc ^ (r & 7)) << 4));
+							v = *(const double2 *) (base + (IDX ? (d * BPT + c) * IDX_PLANE + ct * 16 : d * f_slab + r * 128 + ((cc ^ (r & 7)) << 4)));
 						f[d][c] = make_float2((float) v.x, (float) v.y);
 					}
 			}
-			__syncwarp();
-			if(lane == 0)
-				mbar_arrive(smem_u32(&f_empty[fs]));
+			if constexpr(!IDX) {
+				__syncwarp();
+				if(lane == 0)
+					mbar_arrive(smem_u32(&f_empty[fs]));
+			}
 			const int as = it % NABS;
 			const uint32_t aph = (it / NABS) & 1;
 			const bool oke = mbar_wait(smem_u32(&ab_empty[as]), aph ^ 1, abort_flag, a.err, 6, a.wait);
@@ -599,6 +602,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 				mbar_arrive(smem_u32(acc_empty));
 			piece++;
 		}
+		// no copy of this thread may still land after an early exit
+		if constexpr(IDX)
+			cp_async_wait<0>();
 	}
 	tc_fence_before();
 	__syncthreads();
@@ -1272,20 +1278,19 @@ static size_t ccs_smem_bytes(const BatchPlan &P)
 	return 1024 + f + aa + dd + 8 + bars;
 }
 
-static size_t tc_smem_for(int nf, int nab, int nb, int n_det, int B, int npart, int npad, bool x_in_tmem, bool indexed)
+static size_t tc_smem_for(int nf, int nab, int nb, int n_det, int B, int npart, int npad, bool x_in_tmem)
 {
 	const size_t f = (size_t) nf * n_det * TM * 128;
 	const size_t aa = x_in_tmem ? 0 : (size_t) nab * B * npart * A_TILE;
 	const size_t bb = (size_t) nb * B * npart * npad * KE * 2;
 	const size_t bars = 8 * (2 * nf + 2 * nab + 2 * nb + 3) + 16;
-	const size_t rows = indexed ? TM * sizeof(long long) : 0;  // the indexed producer's row table
 	// 1 KB for aligning the base, 4 KB of slack past the last tile
-	return 1024 + f + aa + bb + bars + rows + 4096;
+	return 1024 + f + aa + bb + bars + 4096;
 }
 
-static size_t tc_smem_bytes(const BatchPlan &P, bool x_in_tmem = false, bool indexed = false)
+static size_t tc_smem_bytes(const BatchPlan &P, bool x_in_tmem = false)
 {
-	return tc_smem_for(P.nf, P.nab, P.nb, P.n_det, P.B, P.npart, P.npad, x_in_tmem, indexed);
+	return tc_smem_for(P.nf, P.nab, P.nb, P.n_det, P.B, P.npart, P.npad, x_in_tmem);
 }
 
 void batch_plan_destroy(void *pp)
@@ -1829,20 +1834,21 @@ int batch_run_ex(void *pp, const void *F, int S, long long ld, const double *gms
 			}
 		}
 		if(indexed) {
-			// X in shared memory; the deepest spectra ring that fits:
-			// three stages with two-deep operand rings, else two
+			// X in shared memory; the deepest spectra ring that fits (the
+			// converters' copies run NFS - 1 stages ahead): three stages
+			// with two-deep operand rings, else two
 			x_tmem = false;
 			a.acol = 0;
 			a.tmem_cols = P->tmem_cols;
 			P->nf = 3;
 			P->nab = 2;
 			P->nb = 2;
-			if(P->npart != 2 || tc_smem_bytes(*P, false, true) > 227 * 1024) {
+			if(P->npart != 2 || tc_smem_bytes(*P) > 227 * 1024) {
 				P->nf = NF;
 				P->nab = P->npart == 3 ? 2 : 3;
 				P->nb = 3;
 			}
-			if(tc_smem_bytes(*P, false, true) > 227 * 1024) {
+			if(tc_smem_bytes(*P) > 227 * 1024) {
 				P->nf = P->nf0;
 				P->nab = P->nab0;
 				P->nb = 3;
@@ -1853,11 +1859,11 @@ int batch_run_ex(void *pp, const void *F, int S, long long ld, const double *gms
 		if(P->ev_begin)
 			cudaEventRecord(P->ev_begin, st);
 		if(indexed && P->npart == 3)
-			CKB(launch_pdl(k_tc_contract<3, NF, 2, 3, false, true>, ctas, TC_THREADS, tc_smem_bytes(*P, false, true), st, P->tm, a));
+			CKB(launch_pdl(k_tc_contract<3, NF, 2, 3, false, true>, ctas, TC_THREADS, tc_smem_bytes(*P), st, P->tm, a));
 		else if(indexed && P->nf == 3)
-			CKB(launch_pdl(k_tc_contract<2, 3, 2, 2, false, true>, ctas, TC_THREADS, tc_smem_bytes(*P, false, true), st, P->tm, a));
+			CKB(launch_pdl(k_tc_contract<2, 3, 2, 2, false, true>, ctas, TC_THREADS, tc_smem_bytes(*P), st, P->tm, a));
 		else if(indexed)
-			CKB(launch_pdl(k_tc_contract<2, NF, 3, 3, false, true>, ctas, TC_THREADS, tc_smem_bytes(*P, false, true), st, P->tm, a));
+			CKB(launch_pdl(k_tc_contract<2, NF, 3, 3, false, true>, ctas, TC_THREADS, tc_smem_bytes(*P), st, P->tm, a));
 		else if(x_tmem)
 			CKB(launch_pdl(k_tc_contract<2, 4, 4, 3, true>, ctas, TC_THREADS, tc_smem_bytes(*P, true), st, P->tm, a));
 		else if(P->npart == 3)
@@ -2003,12 +2009,12 @@ int batch_contract_multi(const MultiJob *jobs, int njobs, const void *F, void *s
 	// the deepest spectra ring that fits the largest job: three stages
 	// with two-deep operand rings, else two
 	int nf = 3, nab = 2, nb = 2;
-	size_t smem = tc_smem_for(nf, nab, nb, ndmax, Bmax, npart, npad, false, true);
+	size_t smem = tc_smem_for(nf, nab, nb, ndmax, Bmax, npart, npad, false);
 	if(npart != 2 || smem > 227 * 1024) {
 		nf = NF;
 		nab = npart == 3 ? 2 : 3;
 		nb = 3;
-		smem = tc_smem_for(nf, nab, nb, ndmax, Bmax, npart, npad, false, true);
+		smem = tc_smem_for(nf, nab, nb, ndmax, Bmax, npart, npad, false);
 	}
 	if(cols > 512 || smem > 227 * 1024) {
 		set_error("batch_contract_multi: %d baselines at l_max %u exceed the tensor or shared memory", Bmax, P0->L);

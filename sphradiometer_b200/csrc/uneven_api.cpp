@@ -18,12 +18,12 @@
 // precisions gather them first) and the epilogue adds each segment's sky
 // into its packed output, truncated to the segment's own l_max (FP64
 // atomics: a segment covered by two jobs gets the same sum in either
-// order).  With a tcgen05 precision all jobs' contractions run in one
-// persistent launch (batch_contract_multi) and the jobs' epilogues are
-// forked over a few streams; otherwise, or on request, each job runs its
-// own contraction and epilogue, the jobs spread over the streams (longest
-// first, each to the least loaded stream).  The whole sequence can be
-// captured once into a CUDA graph and replayed.
+// order).  Each job runs its own contraction and epilogue, the jobs spread
+// over a few streams (longest first, each to the least loaded stream); on
+// request (tcgen05 precisions) all jobs' contractions run in one persistent
+// launch (batch_contract_multi) and the jobs' epilogues are forked over the
+// streams.  The whole sequence can be captured once into a CUDA graph and
+// replayed.
 #include <sphradiometer_b200.h>
 #include <sphradiometer/correlator.h>
 #include <sphradiometer/instrument.h>
@@ -93,9 +93,10 @@ struct sphrad_uneven_plan {
 	cudaStream_t side[kSlots] = {};
 	cudaEvent_t ev[kSlots + 1] = {};
 	int fixed_split = 0;
-	// persistent launch (tcgen05 precisions): every job's contraction in
-	// one launch, each job with its own zeroed workspace at ws_off
-	int persistent = 1;
+	// persistent launch (tcgen05 precisions, on request): every job's
+	// contraction in one launch, each job with its own zeroed workspace at
+	// ws_off
+	int persistent = 0;
 	void *ws_multi = nullptr;
 	std::vector<size_t> ws_off;
 	// graph

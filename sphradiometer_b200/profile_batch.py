@@ -3,8 +3,9 @@
 ``python -m sphradiometer_b200.profile_batch --segments 2048 --calls 5``
 builds the 3-detector, 4096 Hz, l_max = 32 plan, uploads one seeded batch
 and calls the batched integrator ``--calls`` times (after the split-K
-choice), printing the mean device time per call.  Used to drive ncu
-captures of one kernel on a bounded case.
+choice), printing the mean device time per call; ``--graph N`` captures N
+calls into a CUDA graph once and replays it ``--calls`` times.  Used to
+drive ncu captures of one kernel on a bounded case.
 """
 from __future__ import annotations
 
@@ -22,6 +23,7 @@ def main():
     ap.add_argument("--autotune", action="store_true", help="use the autotuned split-K and pipeline variant")
     ap.add_argument("--ctas", type=int, default=0, help="pin the tcgen05 contraction's CTA count")
     ap.add_argument("--pipeline", type=int, default=-1, help="pin the tcgen05 pipeline variant (0, 1, 2)")
+    ap.add_argument("--graph", type=int, default=0, help="capture this many calls into a CUDA graph and time --calls replays of it")
     args = ap.parse_args()
     import torch
 
@@ -46,13 +48,24 @@ def main():
         bp.set_pipeline(args.segments, args.pipeline)
     out = bp.integrate(F, g)
     torch.cuda.synchronize()
+    run = lambda: bp.integrate(F, g, out=out)  # noqa: E731
+    per = 1
+    if args.graph > 0:
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            for _ in range(args.graph):
+                bp.integrate(F, g, out=out)
+        run = graph.replay
+        per = args.graph
+        run()
+        torch.cuda.synchronize()
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record()
     for _ in range(args.calls):
-        bp.integrate(F, g, out=out)
+        run()
     b.record()
     torch.cuda.synchronize()
-    ms = a.elapsed_time(b) / args.calls
+    ms = a.elapsed_time(b) / (args.calls * per)
     print(f"segments {args.segments} split {bp.split(args.segments)} ctas {bp.ctas(args.segments) if args.precision.startswith('bf16') else '-'} "
           f"variant {bp.pipeline(args.segments)} "
           f"precision {args.precision}: {ms:.4f} ms/call, "
