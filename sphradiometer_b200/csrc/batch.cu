@@ -1014,9 +1014,16 @@ __global__ void k_epilogue(const __grid_constant__ EpArgs e, T *acc)
 	pdl_wait_prior();
 	for(int i = threadIdx.x; i < e.B * e.Lp1; i += blockDim.x) {
 		const int b = i / e.Lp1;
-		T v = row[b * e.accstride + i % e.Lp1];
-		for(int r = 1; r < e.reps; r++)
-			v += row[(size_t) r * e.rep_stride + b * e.accstride + i % e.Lp1];
+		// the copies' loads are independent: issued eight at a time
+		const T *src = row + b * e.accstride + i % e.Lp1;
+		T v = 0;
+		for(int r0 = 0; r0 < e.reps; r0 += 8) {
+			T p[8];
+#pragma unroll
+			for(int r = 0; r < 8; r++)
+				p[r] = r0 + r < e.reps ? __ldcg(src + (size_t) (r0 + r) * e.rep_stride) : (T) 0;
+			v += ((p[0] + p[1]) + (p[2] + p[3])) + ((p[4] + p[5]) + (p[6] + p[7]));
+		}
 		sP[i] = v * (e.segw ? (T) e.segw[(size_t) s * e.B + b] : (T) 1);
 	}
 	for(int m = (int) threadIdx.x - e.L; m <= e.L; m += blockDim.x) {
@@ -1119,17 +1126,9 @@ __global__ void __launch_bounds__(EPI2_THREADS, QMAX <= 5 ? 3 : 2) k_epilogue_f3
 #pragma unroll
 		for(int k = 0; k < EPF; k++)
 			if(f_g[k] >= 0 && s0 + f_g[k] < e.S) {
-				// the copies' loads are independent: issued eight at a
-				// time, summed as a tree
-				const float *src = rows + f_src[k];
-				float v = 0.f;
-				for(int r0 = 0; r0 < e.reps; r0 += 8) {
-					float p[8];
-#pragma unroll
-					for(int r = 0; r < 8; r++)
-						p[r] = r0 + r < e.reps ? __ldcg(src + (size_t) (r0 + r) * e.rep_stride) : 0.f;
-					v += ((p[0] + p[1]) + (p[2] + p[3])) + ((p[4] + p[5]) + (p[6] + p[7]));
-				}
+				float v = __ldcg(rows + f_src[k]);
+				for(int r = 1; r < e.reps; r++)
+					v += __ldcg(rows + (size_t) r * e.rep_stride + f_src[k]);
 				dP[f_dst[k]] = v * (e.segw ? e.segw[(size_t) (s0 + f_g[k]) * e.B + f_b[k]] : 1.f);
 			}
 		if(ph_on) {
@@ -1141,9 +1140,11 @@ __global__ void __launch_bounds__(EPI2_THREADS, QMAX <= 5 ? 3 : 2) k_epilogue_f3
 	};
 	// lanes of baselines b >= B are never fetched: zero them once (their
 	// weights are zero, but zero times stale shared memory can be NaN)
-	for(int i = threadIdx.x; i < 2 * EPG * nph; i += EPI2_THREADS)
-		sP[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-	__syncthreads();
+	if(e.B < EB) {
+		for(int i = threadIdx.x; i < 2 * EPG * nph; i += EPI2_THREADS)
+			sP[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+		__syncthreads();
+	}
 	int it = 0;
 	if(e.early)
 		pdl_allow_dependents();
@@ -1681,7 +1682,12 @@ static int launch_epilogue(const BatchPlan *P, const EpArgs &e, void *ws, cudaSt
 	const size_t el = P->precision == kPrecFP64 ? sizeof(double) : sizeof(float);
 	const size_t esmem = (size_t) P->B * P->Lp1 * el + (2 * P->L + 1) * sizeof(double2);
 	const int qmax = (P->nq + EPI2_THREADS - 1) / EPI2_THREADS;
-	if(P->precision != kPrecFP64 && P->B <= EB && qmax <= 10 && EPG * P->B * P->Lp1 <= EPF * EPI2_THREADS && EPG * (P->L + 1) <= EPI2_THREADS) {
+	// small batches: one block per segment (more blocks than batches of
+	// EPG segments; the copies of a small batch's workspace summed with
+	// independent loads)
+	const bool small = S <= kEarlySegments;
+	if(!small && P->precision != kPrecFP64 && P->B <= EB && qmax <= 10 && EPG * P->B * P->Lp1 <= EPF * EPI2_THREADS &&
+	   EPG * (P->L + 1) <= EPI2_THREADS) {
 		// resident blocks only (3 per SM by registers at QMAX 5, 2 at 10)
 		const int sms = sm_count();
 		const int per_sm = qmax <= 5 ? 3 : 2;
@@ -1695,7 +1701,7 @@ static int launch_epilogue(const BatchPlan *P, const EpArgs &e, void *ws, cudaSt
 	} else if(P->precision == kPrecFP64)
 		CKB(launch_pdl(k_epilogue<double>, S, 128, esmem, st, e, (double *) ws));
 	else
-		CKB(launch_pdl(k_epilogue<float>, S, 128, esmem, st, e, (float *) ws));
+		CKB(launch_pdl(k_epilogue<float>, S, small ? 256 : 128, esmem, st, e, (float *) ws));
 	return 0;
 }
 
