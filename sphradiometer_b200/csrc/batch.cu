@@ -1037,24 +1037,56 @@ __global__ void k_epilogue(const __grid_constant__ EpArgs e, T *acc)
 	for(int r = 0; r < e.reps; r++)
 		for(int i = threadIdx.x; i < e.B * e.accstride; i += blockDim.x)
 			row[(size_t) r * e.rep_stride + i] = 0;
+	// EPQ outputs per thread at a time: their tables (l, m, the first
+	// three baselines' weights) loaded together through the read-only
+	// path, so a thread waits for one round of loads per EPQ outputs
+	constexpr int EPQ = 4;
 	const T2 *W = (const T2 *) e.W;
-	for(int q = threadIdx.x; q < e.nq; q += blockDim.x) {
-		const int l = e.lq[q];
-		T re = 0, im = 0;
-		for(int b = 0; b < e.B; b++) {
-			const T2 w = W[(size_t) b * e.nq + q];
-			const T pv = sP[b * e.Lp1 + l];
-			re += w.x * pv;
-			im += w.y * pv;
+	const int Ls = e.out_row ? (int) e.seg_L[s] : e.L;
+	for(int q0 = threadIdx.x; q0 < e.nq; q0 += EPQ * blockDim.x) {
+		int lk[EPQ], mk[EPQ];
+		T2 wk[EPQ][3];
+#pragma unroll
+		for(int k = 0; k < EPQ; k++) {
+			const int q = q0 + k * blockDim.x;
+			const bool in = q < e.nq;
+			lk[k] = in ? __ldg(e.lq + q) : 0;
+			mk[k] = in ? __ldg(e.mq + q) : 0;
+#pragma unroll
+			for(int b = 0; b < 3; b++) {
+				T2 z;
+				z.x = z.y = 0;
+				wk[k][b] = (in && b < e.B) ? __ldg(W + (size_t) b * e.nq + q) : z;
+			}
 		}
-		const double2 ph = sPh[e.mq[q] + e.L];
-		const double vr = (double) re * ph.x - (double) im * ph.y, vi = (double) re * ph.y + (double) im * ph.x;
-		if(e.out_row) {
-			const int Ls = (int) e.seg_L[s];
-			if(l <= Ls)
-				ep_put(e.sky + e.out_row[s] + d_lmoff(Ls, l, e.mq[q]), vr, vi, e.accumulate);
-		} else
-			ep_put(e.sky + (size_t) s * e.nq + q, vr, vi, e.accumulate);
+#pragma unroll
+		for(int k = 0; k < EPQ; k++) {
+			const int q = q0 + k * blockDim.x;
+			if(q >= e.nq)
+				continue;
+			const int l = lk[k];
+			T re = 0, im = 0;
+#pragma unroll
+			for(int b = 0; b < 3; b++)
+				if(b < e.B) {
+					const T pv = sP[b * e.Lp1 + l];
+					re += wk[k][b].x * pv;
+					im += wk[k][b].y * pv;
+				}
+			for(int b = 3; b < e.B; b++) {
+				const T2 w = W[(size_t) b * e.nq + q];
+				const T pv = sP[b * e.Lp1 + l];
+				re += w.x * pv;
+				im += w.y * pv;
+			}
+			const double2 ph = sPh[mk[k] + e.L];
+			const double vr = (double) re * ph.x - (double) im * ph.y, vi = (double) re * ph.y + (double) im * ph.x;
+			if(e.out_row) {
+				if(l <= Ls)
+					ep_put(e.sky + e.out_row[s] + d_lmoff(Ls, l, mk[k]), vr, vi, e.accumulate);
+			} else
+				ep_put(e.sky + (size_t) s * e.nq + q, vr, vi, e.accumulate);
+		}
 	}
 }
 
@@ -1072,7 +1104,7 @@ constexpr int EPI2_THREADS = 256;
 constexpr int EB = 3;
 constexpr int EPG = 4;
 constexpr int EPF = 4;  // partial sums fetched per thread per batch (EPG B (L+1) <= 1024)
-constexpr int EP_MAXREPS = 16;  // most workspace copies (ws_reps)
+constexpr int EP_MAXREPS = 4;  // most workspace copies (ws_reps)
 
 template <int QMAX>
 __global__ void __launch_bounds__(EPI2_THREADS, QMAX <= 5 ? 3 : 2) k_epilogue_f32(const __grid_constant__ EpArgs e, float *acc)
@@ -1539,8 +1571,11 @@ void *batch_plan_create(const BatchPlanDesc &d, int precision)
 }
 
 // copies of the tcgen05 path's split-K workspace for S segments: one for 16
-// tiles or more, up to 16 for a single tile (the CTAs of a launch spread
-// over few tiles' rows, and each copy takes a share of their atomics)
+// tiles or more, up to EP_MAXREPS for few tiles (the CTAs of a launch
+// spread over few tiles' rows, and each copy takes a share of their
+// atomics; measured at 64 segments: 4 copies 10.0 us per call, 16 copies
+// 11.0, 1 copy 10.2 -- more copies cost the epilogue more loads than they
+// save in atomic contention)
 static int ws_reps(const BatchPlan *P, int S)
 {
 	if(!is_tc(P->precision) || S <= 0)
