@@ -932,11 +932,25 @@ __global__ void __launch_bounds__(32 * (2 + NWMAX), 1) k_cc_stream(const __grid_
 					dv[2 * q] = w.x, dv[2 * q + 1] = w.y;
 				}
 			}
+			if constexpr(sizeof(T) == 4 && RPT == 2) {
+				// packed FP32 FMAs (sm_100): two degrees per instruction
 #pragma unroll
-			for(int r = 0; r < RPT; r++)
+				for(int r = 0; r < RPT; r++) {
+					const float2 xr = make_float2(x[r], x[r]);
 #pragma unroll
-				for(int j = 0; j < CCS_LG; j++)
-					acc[r][j] = fma(x[r], dv[j], acc[r][j]);
+					for(int j = 0; j < CCS_LG; j += 2) {
+						const float2 c = __ffma2_rn(xr, make_float2(dv[j], dv[j + 1]), make_float2(acc[r][j], acc[r][j + 1]));
+						acc[r][j] = c.x;
+						acc[r][j + 1] = c.y;
+					}
+				}
+			} else {
+#pragma unroll
+				for(int r = 0; r < RPT; r++)
+#pragma unroll
+					for(int j = 0; j < CCS_LG; j++)
+						acc[r][j] = fma(x[r], dv[j], acc[r][j]);
+			}
 		}
 		__syncwarp();
 		if(lane == 0)
