@@ -420,10 +420,10 @@ struct RecCoef {
 };
 
 template <bool H>
-__device__ void peak_eval_order(int L, int polar, const double2 *c, int m, double x, double st, double phi, const RecCoef *rc, const double *lnpre,
-				PeakEval &acc)
+__device__ void peak_eval_order(int L, int polar, const double2 *c, int m, double x, double st, double lst, double phi, const RecCoef *rc,
+				const double *lnpre, PeakEval &acc)
 {
-	double lam = exp(lnpre[m] + m * log(st));
+	double lam = exp(lnpre[m] + m * lst);
 	if(m & 1)
 		lam = -lam;
 	double lam_prev = 0;
@@ -431,6 +431,9 @@ __device__ void peak_eval_order(int L, int polar, const double2 *c, int m, doubl
 	double Br = 0, Bi = 0, B1r = 0, B1i = 0, B2r = 0, B2i = 0;
 	const double inv_s = 1.0 / st, cot = x / st, m2s = (double) m * m * inv_s * inv_s;
 	const RecCoef *r = rc + tab_off(L, 1, m) - m;
+	// order m and -m rows of the coefficients: consecutive in l (m-major)
+	const double2 *cpm = polar ? c : c + lmoff(L, m, m) - m;
+	const double2 *cnm = c + (m > 0 ? lmoff(L, m, -m) - m : 0);
 	for(int l = m; l <= L; l++) {
 		const RecCoef k = r[l];
 		if(l > m) {
@@ -440,7 +443,7 @@ __device__ void peak_eval_order(int L, int polar, const double2 *c, int m, doubl
 		}
 		const double d1 = (l * x * lam - k.c * lam_prev) * inv_s;
 		const double d2 = H ? -cot * d1 - ((double) l * (l + 1) - m2s) * lam : 0.0;
-		const double2 cp = c[polar ? l : lmoff(L, l, m)];
+		const double2 cp = cpm[l];
 		Ar += cp.x * lam;
 		Ai += cp.y * lam;
 		A1r += cp.x * d1;
@@ -450,7 +453,7 @@ __device__ void peak_eval_order(int L, int polar, const double2 *c, int m, doubl
 			A2i += cp.y * d2;
 		}
 		if(m > 0) {
-			const double2 cn = c[lmoff(L, l, -m)];
+			const double2 cn = cnm[l];
 			Br += cn.x * lam;
 			Bi += cn.y * lam;
 			B1r += cn.x * d1;
@@ -494,14 +497,15 @@ __device__ PeakEval peak_eval(int L, int polar, const double2 *c, double theta, 
 	sincos(theta, &st, &x);
 	if(st < 1e-9)
 		st = 1e-9;
+	const double lst = log(st);
 	const int lane = threadIdx.x & 31;
 	const int M = polar ? 0 : L;
-	// pair order k with M - k so lanes carry equal recurrence lengths
-	for(int k = lane; k <= M / 2; k += 32) {
-		peak_eval_order<H>(L, polar, c, k, x, st, phi, rc, lnpre, e);
-		if(M - k != k)
-			peak_eval_order<H>(L, polar, c, M - k, x, st, phi, rc, lnpre, e);
-	}
+	// one order per lane: a warp pass runs its longest recurrence (its
+	// lowest order) once.  (Pairing orders k and M - k in a lane evens the
+	// lanes' work, but the warp then runs both loops' longest, L + 1 and
+	// M / 2 + 1 steps: 50 against 34 at L = 32.)
+	for(int m = lane; m <= M; m += 32)
+		peak_eval_order<H>(L, polar, c, m, x, st, lst, phi, rc, lnpre, e);
 	for(int o = 16; o; o >>= 1) {
 		e.f += __shfl_xor_sync(0xffffffffu, e.f, o);
 		e.ft += __shfl_xor_sync(0xffffffffu, e.ft, o);
@@ -751,15 +755,17 @@ __device__ bool bfgs2_iterate(Bfgs2 &s, const Fdf &fdf)
 	return true;
 }
 
-// method 0: trust-region Newton (tol: smallest step); 1: BFGS2 with the
+// METHOD 0: trust-region Newton (tol: smallest step); 1: BFGS2 with the
 // gradient in the co-ordinates; 2: BFGS2 as the reference's extremizer
 // runs it (unit-vector gradient components, co-ordinates returned
 // unconditioned).  The BFGS2 methods stop at |gradient| < 1e-3 as the
-// reference does.
-__global__ void k_peak_refine(int S, int L, int polar, const double2 *coeff, long long cstride, const double *theta0, const double *phi0, double sign,
-			      int max_iter, double tol, double *out /* [S][4] */, int *status, const RecCoef *rc_g, const double *lnpre_g, int n_rc,
-			      int method)
+// reference does.  One kernel per method: each carries only its own
+// state (registers, and instruction-cache footprint).
+template <int METHOD>
+__global__ void __launch_bounds__(128, 4) k_peak_refine(int S, int L, int polar, const double2 *coeff, long long cstride, const double *theta0, const double *phi0, double sign,
+			      int max_iter, double tol, double *out /* [S][4] */, int *status, const RecCoef *rc_g, const double *lnpre_g, int n_rc)
 {
+	constexpr int method = METHOD;
 	// the tables in shared memory when they fit (n_rc > 0), else read
 	// from global memory
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -788,8 +794,8 @@ __global__ void k_peak_refine(int S, int L, int polar, const double2 *coeff, lon
 		}
 		return;
 	}
-	if(method != 0) {
-		const PeakFdf fdf{L, polar, c, rc, lnpre, sign, method == 2};
+	if constexpr(METHOD != 0) {
+		const PeakFdf fdf{L, polar, c, rc, lnpre, sign, METHOD == 2};
 		double tc = t, pc = p;
 		condition_tp(tc, pc);
 		Bfgs2 bs;
@@ -1423,8 +1429,17 @@ int peak_refine(int S, unsigned L, int polar, const void *coeff, long long cstri
 	if(!staged)
 		sm = 0;
 	const int wpb = 4;
-	k_peak_refine<<<(S + wpb - 1) / wpb, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out,
-								  status, t.rc, t.lnpre, staged ? t.n : 0, method);
+	const unsigned grid = (S + wpb - 1) / wpb;
+	const int nrc = staged ? t.n : 0;
+	if(method == 0)
+		k_peak_refine<0><<<grid, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out, status,
+							       t.rc, t.lnpre, nrc);
+	else if(method == 1)
+		k_peak_refine<1><<<grid, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out, status,
+							       t.rc, t.lnpre, nrc);
+	else
+		k_peak_refine<2><<<grid, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out, status,
+							       t.rc, t.lnpre, nrc);
 	CK(cudaGetLastError());
 	return 0;
 }
