@@ -763,11 +763,14 @@ __device__ bool bfgs2_iterate(Bfgs2 &s, const Fdf &fdf)
 // state (registers, and instruction-cache footprint).
 template <int METHOD>
 __global__ void __launch_bounds__(128, 4) k_peak_refine(int S, int L, int polar, const double2 *coeff, long long cstride, const double *theta0, const double *phi0, double sign,
-			      int max_iter, double tol, double *out /* [S][4] */, int *status, const RecCoef *rc_g, const double *lnpre_g, int n_rc)
+			      int max_iter, double tol, double *out /* [S][4] */, int *status, const RecCoef *rc_g, const double *lnpre_g, int n_rc,
+			      int n_sky, int sky_off)
 {
 	constexpr int method = METHOD;
 	// the tables in shared memory when they fit (n_rc > 0), else read
-	// from global memory
+	// from global memory; with n_sky > 0 each warp also copies its
+	// series' n_sky coefficients to shared memory (at byte sky_off), so
+	// that every evaluation reads them there
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	const RecCoef *rc = rc_g;
 	const double *lnpre = lnpre_g;
@@ -786,6 +789,13 @@ __global__ void __launch_bounds__(128, 4) k_peak_refine(int S, int L, int polar,
 	if(s >= S)
 		return;
 	const double2 *c = coeff + (long long) s * cstride;
+	if(n_sky > 0) {
+		double2 *cs = (double2 *) (smem_raw + sky_off) + (size_t) (threadIdx.x >> 5) * n_sky;
+		for(int i = threadIdx.x & 31; i < n_sky; i += 32)
+			cs[i] = c[i];
+		__syncwarp();
+		c = cs;
+	}
 	double t = theta0[s], p = phi0[s];
 	if(!(t == t) || !(p == p)) {
 		if((threadIdx.x & 31) == 0) {
@@ -1136,6 +1146,7 @@ static int launch_F(const ShtPlan *p, const double2 *coeff, long long cstride, u
 }
 
 constexpr size_t kMaxDynSmem = 48 * 1024;
+constexpr size_t kRefineSmem = 100 * 1024;  // peak refinement: tables + four warps' series
 static size_t align_up(size_t b) { return (b + 255) & ~(size_t) 255; }
 
 static int pix_threads(int nphi) { return nphi >= 256 ? 256 : ((nphi + 31) / 32) * 32; }
@@ -1431,15 +1442,28 @@ int peak_refine(int S, unsigned L, int polar, const void *coeff, long long cstri
 	const int wpb = 4;
 	const unsigned grid = (S + wpb - 1) / wpb;
 	const int nrc = staged ? t.n : 0;
+	// each warp's series in shared memory too, when the block's share
+	// stays within kRefineSmem (evaluations then read no global memory)
+	const size_t clen = polar ? (size_t) L + 1 : (size_t) (L + 1) * (L + 1);
+	const size_t sky_off = (sm + 15) & ~(size_t) 15;
+	const bool stage_sky = staged && sky_off + (size_t) wpb * clen * sizeof(double2) <= kRefineSmem;
+	if(stage_sky)
+		sm = sky_off + (size_t) wpb * clen * sizeof(double2);
+	const int nsky = stage_sky ? (int) clen : 0;
+	// (the attribute is per device: set on every call that needs it)
+	if(sm > kMaxDynSmem)
+		CK(method == 0 ? cudaFuncSetAttribute(k_peak_refine<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kRefineSmem)
+		   : method == 1 ? cudaFuncSetAttribute(k_peak_refine<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kRefineSmem)
+				 : cudaFuncSetAttribute(k_peak_refine<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kRefineSmem));
 	if(method == 0)
 		k_peak_refine<0><<<grid, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out, status,
-							       t.rc, t.lnpre, nrc);
+							       t.rc, t.lnpre, nrc, nsky, (int) sky_off);
 	else if(method == 1)
 		k_peak_refine<1><<<grid, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out, status,
-							       t.rc, t.lnpre, nrc);
+							       t.rc, t.lnpre, nrc, nsky, (int) sky_off);
 	else
 		k_peak_refine<2><<<grid, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out, status,
-							       t.rc, t.lnpre, nrc);
+							       t.rc, t.lnpre, nrc, nsky, (int) sky_off);
 	CK(cudaGetLastError());
 	return 0;
 }
