@@ -414,18 +414,16 @@ struct PeakEval {
 // recurrence coefficients of order m, degree l (table [tab_off(L, 1, m) + l - m]):
 // a, b of lambda_l = a x lambda_{l-1} - b lambda_{l-2} (l = m+1: a =
 // sqrt(2m+3), b = 0) and c_l = sqrt((2l+1)(l^2 - m^2)/(2l-1)) of the
-// derivative; lnpre[m] is the log normalisation of lambda_m^m
+// derivative; pre[m] is the normalisation of lambda_m^m (= pre[m] sin^m)
 struct RecCoef {
 	double a, b, c;
 };
 
 template <bool H>
-__device__ void peak_eval_order(int L, int polar, const double2 *c, int m, double x, double st, double lst, double phi, const RecCoef *rc,
-				const double *lnpre, PeakEval &acc)
+__device__ void peak_eval_order(int L, int polar, const double2 *c, int m, double x, double st, double lam, double cs, double sn, const RecCoef *rc,
+				PeakEval &acc)
 {
-	double lam = exp(lnpre[m] + m * lst);
-	if(m & 1)
-		lam = -lam;
+	// lam: lambda_m^m with its sign; (cs, sn): e^{i m phi}
 	double lam_prev = 0;
 	double Ar = 0, Ai = 0, A1r = 0, A1i = 0, A2r = 0, A2i = 0;
 	double Br = 0, Bi = 0, B1r = 0, B1i = 0, B2r = 0, B2i = 0;
@@ -472,8 +470,6 @@ __device__ void peak_eval_order(int L, int polar, const double2 *c, int m, doubl
 		B2r = -B2r;
 		B2i = -B2i;
 	}
-	double sn, cs;
-	sincos(m * phi, &sn, &cs);
 	// A e^{i m phi} + B e^{-i m phi}
 	const double Re0 = Ar * cs - Ai * sn + Br * cs + Bi * sn;
 	const double ImA = Ar * sn + Ai * cs, ImB = Bi * cs - Br * sn;
@@ -490,22 +486,55 @@ __device__ void peak_eval_order(int L, int polar, const double2 *c, int m, doubl
 }
 
 template <bool H>
-__device__ PeakEval peak_eval(int L, int polar, const double2 *c, double theta, double phi, const RecCoef *rc, const double *lnpre)
+__device__ PeakEval peak_eval(int L, int polar, const double2 *c, double theta, double phi, const RecCoef *rc, const double *pre)
 {
 	PeakEval e = {0, 0, 0, 0, 0, 0};
 	double st, x;
 	sincos(theta, &st, &x);
 	if(st < 1e-9)
 		st = 1e-9;
-	const double lst = log(st);
+	double s1, c1;
+	sincos(phi, &s1, &c1);
 	const int lane = threadIdx.x & 31;
 	const int M = polar ? 0 : L;
+	// sin^lane theta and e^{i lane phi}: prefix products over the lanes
+	// (five multiplications each, in place of an exp and a sincos per
+	// order)
+	double pw = lane ? st : 1.0, zr = lane ? c1 : 1.0, zi = lane ? s1 : 0.0;
+#pragma unroll
+	for(int o = 1; o < 32; o <<= 1) {
+		const double qw = __shfl_up_sync(0xffffffffu, pw, o);
+		const double qr = __shfl_up_sync(0xffffffffu, zr, o);
+		const double qi = __shfl_up_sync(0xffffffffu, zi, o);
+		if(lane >= o) {
+			pw *= qw;
+			const double r = zr * qr - zi * qi;
+			zi = zr * qi + zi * qr;
+			zr = r;
+		}
+	}
+	// sin^32 theta and e^{32 i phi}, the step between warp passes
+	const double pw32 = __shfl_sync(0xffffffffu, pw, 31) * st;
+	const double w31r = __shfl_sync(0xffffffffu, zr, 31), w31i = __shfl_sync(0xffffffffu, zi, 31);
+	const double z32r = w31r * c1 - w31i * s1, z32i = w31r * s1 + w31i * c1;
+	double gw = 1.0, gr = 1.0, gi = 0.0;
 	// one order per lane: a warp pass runs its longest recurrence (its
 	// lowest order) once.  (Pairing orders k and M - k in a lane evens the
 	// lanes' work, but the warp then runs both loops' longest, L + 1 and
 	// M / 2 + 1 steps: 50 against 34 at L = 32.)
-	for(int m = lane; m <= M; m += 32)
-		peak_eval_order<H>(L, polar, c, m, x, st, lst, phi, rc, lnpre, e);
+	for(int m0 = 0; m0 <= M; m0 += 32) {
+		const int m = m0 + lane;
+		if(m <= M) {
+			double lam = pre[m] * pw * gw;
+			if(m & 1)
+				lam = -lam;
+			peak_eval_order<H>(L, polar, c, m, x, st, lam, zr * gr - zi * gi, zr * gi + zi * gr, rc, e);
+		}
+		gw *= pw32;
+		const double r = gr * z32r - gi * z32i;
+		gi = gr * z32i + gi * z32r;
+		gr = r;
+	}
 	for(int o = 16; o; o >>= 1) {
 		e.f += __shfl_xor_sync(0xffffffffu, e.f, o);
 		e.ft += __shfl_xor_sync(0xffffffffu, e.ft, o);
@@ -565,14 +594,14 @@ struct PeakFdf {
 	int L, polar;
 	const double2 *c;
 	const RecCoef *rc;
-	const double *lnpre;
+	const double *pre;
 	double sign;
 	bool unit_grad;
 	__device__ void operator()(const double *x, double &h, double *g) const
 	{
 		double t = x[0], p = x[1];
 		condition_tp(t, p);
-		const PeakEval e = peak_eval<false>(L, polar, c, t, p, rc, lnpre);
+		const PeakEval e = peak_eval<false>(L, polar, c, t, p, rc, pre);
 		h = -sign * e.f;
 		g[0] = -sign * e.ft;
 		g[1] = -sign * (unit_grad ? e.fp / sin(t) : e.fp);
@@ -755,6 +784,9 @@ __device__ bool bfgs2_iterate(Bfgs2 &s, const Fdf &fdf)
 	return true;
 }
 
+constexpr size_t kRefineSmem = 227 * 1024;  // peak refinement: tables + the block's series
+constexpr int kRefineWarps = 12;             // most warps (series) per refinement block
+
 // METHOD 0: trust-region Newton (tol: smallest step); 1: BFGS2 with the
 // gradient in the co-ordinates; 2: BFGS2 as the reference's extremizer
 // runs it (unit-vector gradient components, co-ordinates returned
@@ -762,8 +794,8 @@ __device__ bool bfgs2_iterate(Bfgs2 &s, const Fdf &fdf)
 // reference does.  One kernel per method: each carries only its own
 // state (registers, and instruction-cache footprint).
 template <int METHOD>
-__global__ void __launch_bounds__(128, 4) k_peak_refine(int S, int L, int polar, const double2 *coeff, long long cstride, const double *theta0, const double *phi0, double sign,
-			      int max_iter, double tol, double *out /* [S][4] */, int *status, const RecCoef *rc_g, const double *lnpre_g, int n_rc,
+__global__ void __launch_bounds__(32 * kRefineWarps, 1) k_peak_refine(int S, int L, int polar, const double2 *coeff, long long cstride, const double *theta0, const double *phi0, double sign,
+			      int max_iter, double tol, double *out /* [S][4] */, int *status, const RecCoef *rc_g, const double *pre_g, int n_rc,
 			      int n_sky, int sky_off)
 {
 	constexpr int method = METHOD;
@@ -773,17 +805,17 @@ __global__ void __launch_bounds__(128, 4) k_peak_refine(int S, int L, int polar,
 	// that every evaluation reads them there
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	const RecCoef *rc = rc_g;
-	const double *lnpre = lnpre_g;
+	const double *pre = pre_g;
 	if(n_rc > 0) {
 		RecCoef *rcs = (RecCoef *) smem_raw;
-		double *lps = (double *) (rcs + n_rc);
+		double *ps = (double *) (rcs + n_rc);
 		for(int i = threadIdx.x; i < n_rc; i += blockDim.x)
 			rcs[i] = rc_g[i];
 		for(int i = threadIdx.x; i <= L; i += blockDim.x)
-			lps[i] = lnpre_g[i];
+			ps[i] = pre_g[i];
 		__syncthreads();
 		rc = rcs;
-		lnpre = lps;
+		pre = ps;
 	}
 	const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
 	if(s >= S)
@@ -805,7 +837,7 @@ __global__ void __launch_bounds__(128, 4) k_peak_refine(int S, int L, int polar,
 		return;
 	}
 	if constexpr(METHOD != 0) {
-		const PeakFdf fdf{L, polar, c, rc, lnpre, sign, METHOD == 2};
+		const PeakFdf fdf{L, polar, c, rc, pre, sign, METHOD == 2};
 		double tc = t, pc = p;
 		condition_tp(tc, pc);
 		Bfgs2 bs;
@@ -847,7 +879,7 @@ __global__ void __launch_bounds__(128, 4) k_peak_refine(int S, int L, int polar,
 	condition_tp(t, p);
 	const double ts = t, ps = p;
 	double radius = M_PI / 24;
-	PeakEval e = peak_eval<true>(L, polar, c, t, p, rc, lnpre);
+	PeakEval e = peak_eval<true>(L, polar, c, t, p, rc, pre);
 	double g = sign * e.f;
 	int it = 0, converged = 0;
 	for(; it < max_iter; it++) {
@@ -879,7 +911,7 @@ __global__ void __launch_bounds__(128, 4) k_peak_refine(int S, int L, int polar,
 		}
 		double tn = t + du, pn = p + dv / st;
 		condition_tp(tn, pn);
-		const PeakEval en = peak_eval<true>(L, polar, c, tn, pn, rc, lnpre);
+		const PeakEval en = peak_eval<true>(L, polar, c, tn, pn, rc, pre);
 		const double gn = sign * en.f;
 		if(gn >= g) {
 			// a short step that no longer raises the value is at the
@@ -1146,7 +1178,6 @@ static int launch_F(const ShtPlan *p, const double2 *coeff, long long cstride, u
 }
 
 constexpr size_t kMaxDynSmem = 48 * 1024;
-constexpr size_t kRefineSmem = 100 * 1024;  // peak refinement: tables + four warps' series
 static size_t align_up(size_t b) { return (b + 255) & ~(size_t) 255; }
 
 static int pix_threads(int nphi) { return nphi >= 256 ? 256 : ((nphi + 31) / 32) * 32; }
@@ -1359,7 +1390,7 @@ int sht_product(void *plan, int S, const void *a, long long astride, unsigned La
 // host in FP64 and kept for the process
 struct RecTable {
 	RecCoef *rc = nullptr;
-	double *lnpre = nullptr;
+	double *pre = nullptr;  // normalisation of lambda_m^m
 	int n = 0;
 };
 static std::mutex g_rec_mu;
@@ -1377,12 +1408,12 @@ static int rec_table(unsigned L, RecTable *out)
 	}
 	const int n = (int) tab_off((int) L, 1, (int) L + 1);
 	std::vector<RecCoef> rc(n);
-	std::vector<double> lp(L + 1);
+	std::vector<double> pre(L + 1);
 	for(int m = 0; m <= (int) L; m++) {
 		double v = 0.5 * log((2.0 * m + 1.0) / (4.0 * M_PI));
 		for(int k = 1; k <= m; k++)
 			v += 0.5 * log((2.0 * k - 1.0) / (2.0 * k));
-		lp[m] = v;
+		pre[m] = exp(v);
 		for(int l = m; l <= (int) L; l++) {
 			RecCoef c = {0, 0, 0};
 			if(l == m + 1)
@@ -1399,10 +1430,10 @@ static int rec_table(unsigned L, RecTable *out)
 	RecTable t;
 	t.n = n;
 	t.rc = (RecCoef *) dmalloc(n * sizeof(RecCoef));
-	t.lnpre = (double *) dmalloc((L + 1) * sizeof(double));
-	if(!t.rc || !t.lnpre || h2d(t.rc, rc.data(), n * sizeof(RecCoef)) || h2d(t.lnpre, lp.data(), (L + 1) * sizeof(double)) || stream_sync()) {
+	t.pre = (double *) dmalloc((L + 1) * sizeof(double));
+	if(!t.rc || !t.pre || h2d(t.rc, rc.data(), n * sizeof(RecCoef)) || h2d(t.pre, pre.data(), (L + 1) * sizeof(double)) || stream_sync()) {
 		dfree(t.rc);
-		dfree(t.lnpre);
+		dfree(t.pre);
 		return -1;
 	}
 	g_rec[key] = t;
@@ -1439,17 +1470,20 @@ int peak_refine(int S, unsigned L, int polar, const void *coeff, long long cstri
 	const bool staged = sm <= kMaxDynSmem;
 	if(!staged)
 		sm = 0;
-	const int wpb = 4;
-	const unsigned grid = (S + wpb - 1) / wpb;
-	const int nrc = staged ? t.n : 0;
-	// each warp's series in shared memory too, when the block's share
-	// stays within kRefineSmem (evaluations then read no global memory)
+	// each warp's series in shared memory too (evaluations then read no
+	// global memory), as many warps per block as the tables and their
+	// series fit in kRefineSmem -- one block per SM, up to kRefineWarps
+	// warps; otherwise four warps reading their series from global memory
 	const size_t clen = polar ? (size_t) L + 1 : (size_t) (L + 1) * (L + 1);
 	const size_t sky_off = (sm + 15) & ~(size_t) 15;
-	const bool stage_sky = staged && sky_off + (size_t) wpb * clen * sizeof(double2) <= kRefineSmem;
+	const size_t fit = staged && sky_off < kRefineSmem ? (kRefineSmem - sky_off) / (clen * sizeof(double2)) : 0;
+	const bool stage_sky = fit >= 4;
+	const int wpb = stage_sky ? (int) std::min<size_t>(fit, kRefineWarps) : 4;
 	if(stage_sky)
 		sm = sky_off + (size_t) wpb * clen * sizeof(double2);
 	const int nsky = stage_sky ? (int) clen : 0;
+	const unsigned grid = (S + wpb - 1) / wpb;
+	const int nrc = staged ? t.n : 0;
 	// (the attribute is per device: set on every call that needs it)
 	if(sm > kMaxDynSmem)
 		CK(method == 0 ? cudaFuncSetAttribute(k_peak_refine<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kRefineSmem)
@@ -1457,13 +1491,13 @@ int peak_refine(int S, unsigned L, int polar, const void *coeff, long long cstri
 				 : cudaFuncSetAttribute(k_peak_refine<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kRefineSmem));
 	if(method == 0)
 		k_peak_refine<0><<<grid, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out, status,
-							       t.rc, t.lnpre, nrc, nsky, (int) sky_off);
+							       t.rc, t.pre, nrc, nsky, (int) sky_off);
 	else if(method == 1)
 		k_peak_refine<1><<<grid, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out, status,
-							       t.rc, t.lnpre, nrc, nsky, (int) sky_off);
+							       t.rc, t.pre, nrc, nsky, (int) sky_off);
 	else
 		k_peak_refine<2><<<grid, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out, status,
-							       t.rc, t.lnpre, nrc, nsky, (int) sky_off);
+							       t.rc, t.pre, nrc, nsky, (int) sky_off);
 	CK(cudaGetLastError());
 	return 0;
 }
