@@ -1026,7 +1026,10 @@ def run(args):
                                  f"clocks sampled across them",
                        "parallelism": f"replicas x{world} (segments sharded, no collective)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": profiled_traffic(n_seg), "kernel": "k_tc_contract" if prec == "bf16x3" else "k_cc_stream",
+                         "traffic": profiled_traffic(n_seg),
+                         "traffic_source": "ncu capture of the same kernel and workload (dram__bytes_read.sum + dram__bytes_write.sum per launch), "
+                                           "recorded in profiles/k_tc_contract_c1.md and scaled by the segments per launch",
+                         "kernel": "k_tc_contract" if prec == "bf16x3" else "k_cc_stream",
                          "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback",
                          "algorithmic_bytes_per_launch": alg_bytes, "partial_sum_bytes_per_launch": partial_sum_bytes,
                          "mean_launch_ms": mean_k * 1e3},

@@ -178,3 +178,26 @@ def test_antenna_response_known_answers():
         lib.sphrad_antenna_response(C.byref(fp), C.byref(fc), D, 0.7, 0.4, psi, 0.2)
         norms.append(fp.value ** 2 + fc.value ** 2)
     assert max(norms) - min(norms) < 1e-7
+
+
+def c_caller(out_path):
+    """Compile tests/c/fd_caller.c (a C program of the reference's kind)
+    against include/sphradiometer and link it with the library."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lib_dir = os.path.join(ROOT, "sphradiometer_b200")
+    cmd = [cc, "-O2", "-Wall", "-Wextra", "-Werror", "-std=c11", "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "c", "fd_caller.c"),
+           "-L", lib_dir, "-lsphradiometer_b200", "-Wl,-rpath," + lib_dir, "-lm", "-o", str(out_path)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return str(out_path)
+
+
+def test_c_caller_compiles_against_headers_and_links(tmp_path):
+    """The headers compile as C (no warnings) and every function the
+    drop-in FD path needs resolves in the library at link time."""
+    exe = c_caller(tmp_path / "fd_caller")
+    assert os.path.exists(exe)
