@@ -78,10 +78,11 @@ int sphrad_batch_integrate(sphrad_batch_plan *plan, const void *fseries, int n_s
  * every GPU that loads the library until the process exits; a call needing
  * more is refused with -1 and a message that gives this plan's limit.  The
  * scratch of n_seg segments is n_seg * n_baselines * round_up(l_max + 1, 4)
- * elements (4 bytes, 8 for SPHRAD_PREC_FP64), times up to 16 copies for the
- * tcgen05 precisions when n_seg is below 16 * 128 (fewer segments spread
- * their partial sums over copies); that stays within the array, and the
- * limit is about 19,000 segments for 3 baselines at l_max = 32.  Each call
+ * elements (4 bytes, 8 for SPHRAD_PREC_FP64), times min(4, 16 / tiles)
+ * copies for the tcgen05 precisions (tiles = ceil(n_seg / 128): batches of
+ * fewer than 9 tiles spread their partial sums over copies); that stays
+ * within the array, and the limit is about 19,000 segments for 3
+ * baselines at l_max = 32.  Each call
  * zero-fills the part it uses before launching.  All calls share the
  * array, so calls that overlap on the GPU (other streams, other threads)
  * race and must be serialised by the caller.  The first call on each
