@@ -311,39 +311,144 @@ __global__ void k_rows_argmax(int S, int nt, int nphi, const RowBest *rb, const 
 // azimuthal analysis, one block per (row i, series s), thread per order:
 //   H_m(theta_i) = (2 pi / nphi) w_i sum_j mesh_j e^{-2 pi i (m j mod nphi)/nphi}
 // ---------------------------------------------------------------------------
-template <class Tin2, class T>
-__global__ void k_sht_H(int nt, int nphi, int M, const Tin2 *mesh, const double *w, const typename V2<T>::t *tw, typename V2<T>::t *H)
+constexpr int SP_ROWS = 4;  // most rows per block of the product synthesis (one warp each)
+constexpr int SP_PB = 5;    // pixels per lane and pass
+
+// Synthesis of two series' rows at the grid's pixels and their product
+// (the pixel-domain product's first half): blockDim / 32 rows per block,
+// one warp per row; a lane takes SP_PB pixels j = j0 + lane + 32 q, so
+// each broadcast read of the two rows' coefficients serves SP_PB Horner
+// steps of each series.  Same arithmetic per pixel as k_sht_pix's product
+// mode.
+template <class T>
+__global__ void k_sht_pix_prod(long long nrows, int nphi, int M, const typename V2<T>::t *F, const typename V2<T>::t *F2, const typename V2<T>::t *tw,
+			       double2 *out)
 {
 	typedef typename V2<T>::t T2;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
-	T2 *tws = (T2 *) smem_raw;
-	T2 *row_s = tws + nphi;
-	const long long row = blockIdx.x;  // series * nt + theta row
-	const int i = (int) (row % nt);
 	const int W = 2 * M + 1;
-	for(int k = threadIdx.x; k < nphi; k += blockDim.x) {
+	const int rpb = blockDim.x >> 5;
+	T2 *tws = (T2 *) smem_raw;
+	T2 *Fs = tws + nphi;    // [rpb][W]
+	T2 *F2s = Fs + rpb * W;  // [rpb][W]
+	const long long row0 = (long long) blockIdx.x * rpb;
+	for(int k = threadIdx.x; k < nphi; k += blockDim.x)
 		tws[k] = tw[k];
-		const Tin2 v = mesh[row * nphi + k];
-		row_s[k] = mk2((T) v.x, (T) v.y);
+	for(int k = threadIdx.x; k < rpb * W; k += blockDim.x) {
+		const int r = k / W;
+		const bool in = row0 + r < nrows;
+		const long long src = (row0 + r) * W + (k - r * W);
+		Fs[k] = in ? F[src] : mk2((T) 0, (T) 0);
+		F2s[k] = in ? F2[src] : mk2((T) 0, (T) 0);
 	}
 	__syncthreads();
+	const int r = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const long long row = row0 + r;
+	if(row >= nrows)
+		return;
+	const T2 *fa = Fs + r * W, *fb = F2s + r * W;
+	for(int j0 = 0; j0 < nphi; j0 += 32 * SP_PB) {
+		T2 z[SP_PB];
+		T vr[SP_PB], vi[SP_PB], wr[SP_PB], wi[SP_PB];
+#pragma unroll
+		for(int q = 0; q < SP_PB; q++) {
+			const int j = j0 + lane + 32 * q;
+			z[q] = j < nphi ? tws[j] : mk2((T) 0, (T) 0);
+			vr[q] = fa[W - 1].x;
+			vi[q] = fa[W - 1].y;
+			wr[q] = fb[W - 1].x;
+			wi[q] = fb[W - 1].y;
+		}
+		for(int k = W - 2; k >= 0; k--) {
+			const T2 f = fa[k], g = fb[k];
+#pragma unroll
+			for(int q = 0; q < SP_PB; q++) {
+				const T nr = vr[q] * z[q].x - vi[q] * z[q].y + f.x;
+				const T ni = vr[q] * z[q].y + vi[q] * z[q].x + f.y;
+				vr[q] = nr;
+				vi[q] = ni;
+				const T qr = wr[q] * z[q].x - wi[q] * z[q].y + g.x;
+				const T qi = wr[q] * z[q].y + wi[q] * z[q].x + g.y;
+				wr[q] = qr;
+				wi[q] = qi;
+			}
+		}
+#pragma unroll
+		for(int q = 0; q < SP_PB; q++) {
+			const int j = j0 + lane + 32 * q;
+			if(j >= nphi)
+				continue;
+			const T2 e = tws[(int) (((long long) M * j) % nphi)];  // e^{+i M phi_j}; multiply by its conjugate
+			const T ar = vr[q] * e.x + vi[q] * e.y, ai = vi[q] * e.x - vr[q] * e.y;
+			const T br = wr[q] * e.x + wi[q] * e.y, bi = wi[q] * e.x - wr[q] * e.y;
+			out[row * nphi + j] = double2{ar * br - ai * bi, ar * bi + ai * br};
+		}
+	}
+}
+
+constexpr int SH_ROWS = 4;  // most rows per block of the azimuthal analysis (one warp each)
+constexpr int SH_QB = 4;    // consecutive orders per lane
+
+template <class Tin2, class T>
+__global__ void k_sht_H(long long nrows, int nt, int nphi, int M, const Tin2 *mesh, const double *w, const typename V2<T>::t *tw, typename V2<T>::t *H)
+{
+	// blockDim / 32 (<= SH_ROWS) rows per block, one warp per row; a lane takes SH_QB
+	// consecutive orders: one scattered twiddle read per pixel for the
+	// first, the others by multiplying with the pixel's e^{i phi_j} (a
+	// broadcast read), so each pixel value read serves SH_QB sums
+	typedef typename V2<T>::t T2;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	T2 *tws = (T2 *) smem_raw;
+	T2 *rows_s = tws + nphi;
+	const int W = 2 * M + 1;
+	const int rpb = blockDim.x >> 5;
+	const long long row0 = (long long) blockIdx.x * rpb;
+	for(int k = threadIdx.x; k < nphi; k += blockDim.x)
+		tws[k] = tw[k];
+	for(int k = threadIdx.x; k < rpb * nphi; k += blockDim.x) {
+		const int r = k / nphi;
+		T2 v = mk2((T) 0, (T) 0);
+		if(row0 + r < nrows) {
+			const Tin2 x = mesh[(row0 + r) * nphi + (k - r * nphi)];
+			v = mk2((T) x.x, (T) x.y);
+		}
+		rows_s[k] = v;
+	}
+	__syncthreads();
+	const int r = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	const long long row = row0 + r;
+	if(row >= nrows)
+		return;
+	const int i = (int) (row % nt);
+	const T2 *rv = rows_s + r * nphi;
 	const T scale = (T) (2.0 * M_PI / nphi * w[i]);
-	for(int mi = threadIdx.x; mi < W; mi += blockDim.x) {
-		const int m = mi - M;
-		const int step = ((m % nphi) + nphi) % nphi;
+	for(int mi0 = lane * SH_QB; mi0 < W; mi0 += 32 * SH_QB) {
+		const int m0 = mi0 - M;
+		const int step = ((m0 % nphi) + nphi) % nphi;
 		int idx = 0;
-		T hr = 0, hi = 0;
+		T hr[SH_QB], hi[SH_QB];
+#pragma unroll
+		for(int q = 0; q < SH_QB; q++)
+			hr[q] = hi[q] = 0;
 		for(int j = 0; j < nphi; j++) {
-			const T2 e = tws[idx];
-			const T2 v = row_s[j];
-			// v * conj(e)
-			hr += v.x * e.x + v.y * e.y;
-			hi += v.y * e.x - v.x * e.y;
+			const T2 v = rv[j];
+			const T2 z = tws[j];  // e^{i phi_j}
+			T2 e = tws[idx];      // e^{i m0 phi_j}
+#pragma unroll
+			for(int q = 0; q < SH_QB; q++) {
+				// v * conj(e), e = e^{i (m0 + q) phi_j}
+				hr[q] += v.x * e.x + v.y * e.y;
+				hi[q] += v.y * e.x - v.x * e.y;
+				e = cmul2(e, z);
+			}
 			idx += step;
 			if(idx >= nphi)
 				idx -= nphi;
 		}
-		H[row * W + mi] = mk2(hr * scale, hi * scale);
+#pragma unroll
+		for(int q = 0; q < SH_QB; q++)
+			if(mi0 + q < W)
+				H[row * W + mi0 + q] = mk2(hr[q] * scale, hi[q] * scale);
 	}
 }
 
@@ -1285,20 +1390,26 @@ int sht_analysis(void *plan, const void *mesh, int S, unsigned L_out, int polar_
 		return 0;
 	const int M = polar_out ? 0 : (int) L_out;
 	const int W = 2 * M + 1;
-	const int thr = pix_threads(p->nphi < W ? W : p->nphi);
-	if((size_t) 2 * p->nphi * (p->fp32 ? sizeof(float2) : sizeof(double2)) > kMaxDynSmem) {
+	// rows per block of the azimuthal analysis: as many as fit beside the
+	// twiddles in the shared-memory budget, up to SH_ROWS
+	const size_t esz = p->fp32 ? sizeof(float2) : sizeof(double2);
+	const size_t fit = kMaxDynSmem / ((size_t) p->nphi * esz);  // rows of the grid, twiddles included
+	const int rpb = fit >= 2 ? (int) std::min<size_t>(SH_ROWS, fit - 1) : 0;
+	if(rpb < 1) {
 		set_error("sht analysis: grid of %d columns too wide", p->nphi);
 		return -1;
 	}
-	const unsigned grid = (unsigned) p->nt * (unsigned) S, agrid = (unsigned) W * (unsigned) S;
+	const long long nrows = (long long) p->nt * S;
+	const unsigned grid = (unsigned) ((nrows + rpb - 1) / rpb), agrid = (unsigned) W * (unsigned) S;
+	const size_t hsm = (size_t) (1 + rpb) * p->nphi * esz;
 	if(p->fp32) {
-		k_sht_H<double2, float><<<grid, thr, (size_t) 2 * p->nphi * sizeof(float2), st>>>(p->nt, p->nphi, M, (const double2 *) mesh, p->d_w,
-												    (const float2 *) p->d_tw, (float2 *) scratch);
+		k_sht_H<double2, float><<<grid, 32 * rpb, hsm, st>>>(nrows, p->nt, p->nphi, M, (const double2 *) mesh, p->d_w, (const float2 *) p->d_tw,
+								     (float2 *) scratch);
 		k_sht_A<float><<<agrid, 256, 0, st>>>((int) L_out, (int) L_layout, polar_out, M, (int) p->L, p->nt, (const float2 *) scratch, (const float *) p->d_tab,
 								(double2 *) out, ostride);
 	} else {
-		k_sht_H<double2, double><<<grid, thr, (size_t) 2 * p->nphi * sizeof(double2), st>>>(p->nt, p->nphi, M, (const double2 *) mesh, p->d_w,
-												      (const double2 *) p->d_tw, (double2 *) scratch);
+		k_sht_H<double2, double><<<grid, 32 * rpb, hsm, st>>>(nrows, p->nt, p->nphi, M, (const double2 *) mesh, p->d_w, (const double2 *) p->d_tw,
+								      (double2 *) scratch);
 		k_sht_A<double><<<agrid, 256, 0, st>>>((int) L_out, (int) L_layout, polar_out, M, (int) p->L, p->nt, (const double2 *) scratch,
 								 (const double *) p->d_tab, (double2 *) out, ostride);
 	}
@@ -1345,16 +1456,18 @@ int sht_product(void *plan, int S, const void *a, long long astride, unsigned La
 	const int M = (pa && pb) ? 0 : (int) (La > Lb ? La : Lb);
 	const int W = 2 * M + 1;
 	const size_t esz = p->fp32 ? sizeof(float2) : sizeof(double2);
-	const size_t sm = (size_t) (p->nphi + 2 * W) * esz;
-	if(sm > kMaxDynSmem) {
+	// rows per block of the product synthesis: as many as fit, up to SP_ROWS
+	int rpb = SP_ROWS;
+	while(rpb > 0 && (size_t) (p->nphi + 2 * rpb * W) * esz > kMaxDynSmem)
+		rpb--;
+	if(rpb < 1) {
 		set_error("sht product: grid of %d columns too wide", p->nphi);
 		return -1;
 	}
+	const size_t sm = (size_t) (p->nphi + 2 * rpb * W) * esz;
 	size_t fb, mb, hb;
 	product_layout(p, S, La, pa, Lb, pb, Ld, pd, &fb, &mb, &hb);
 	char *Fa = (char *) scratch, *Fb = Fa + fb, *mesh = Fb + fb, *H = mesh + mb;
-	const int thr = pix_threads(p->nphi);
-	const unsigned grid = (unsigned) p->nt * (unsigned) S;
 	// F arrays at the common order limit M (a factor with fewer orders
 	// contributes zeros there)
 	auto fill = [&](const void *c, long long cs, unsigned Lc, int pc, char *F) -> int {
@@ -1370,12 +1483,14 @@ int sht_product(void *plan, int S, const void *a, long long astride, unsigned La
 	};
 	if(fill(a, astride, La, pa, Fa) || fill(b, bstride, Lb, pb, Fb))
 		return -1;
+	const long long nrows = (long long) p->nt * S;
+	const unsigned pgrid = (unsigned) ((nrows + rpb - 1) / rpb);
 	if(p->fp32)
-		k_sht_pix<float, 3, double2><<<grid, thr, sm, st>>>(p->nt, p->nphi, M, (const float2 *) Fa, (const float2 *) Fb, (const float2 *) p->d_tw,
-								    (double2 *) mesh, 1.0);
+		k_sht_pix_prod<float><<<pgrid, 32 * rpb, sm, st>>>(nrows, p->nphi, M, (const float2 *) Fa, (const float2 *) Fb, (const float2 *) p->d_tw,
+								   (double2 *) mesh);
 	else
-		k_sht_pix<double, 3, double2><<<grid, thr, sm, st>>>(p->nt, p->nphi, M, (const double2 *) Fa, (const double2 *) Fb, (const double2 *) p->d_tw,
-								     (double2 *) mesh, 1.0);
+		k_sht_pix_prod<double><<<pgrid, 32 * rpb, sm, st>>>(nrows, p->nphi, M, (const double2 *) Fa, (const double2 *) Fb, (const double2 *) p->d_tw,
+								    (double2 *) mesh);
 	CK(cudaGetLastError());
 	const int pd_eff = pd || (pa && pb);
 	if(pd_eff != pd) {
