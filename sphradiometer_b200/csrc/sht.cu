@@ -159,6 +159,64 @@ __global__ void k_sht_F(int L_in, int polar, const Tin2 *coeff, long long cstrid
 	F[((long long) s * nt + i) * W + mi] = mk2(ar, ai);
 }
 
+// The same Legendre synthesis for SF_SER series per block and one order:
+// the order's table column block (degrees x rows) and the series'
+// coefficients of that order in shared memory, a thread per row keeping
+// SF_SER sums, so each table value read serves SF_SER series (the
+// per-(series, order, row) kernel above reads it once per series).  Same
+// sums in the same order, so the results are those of k_sht_F.
+constexpr int SF_SER = 16;
+
+template <class Tin2, class T>
+__global__ void k_sht_F_tile(int S, int L_in, int polar, const Tin2 *coeff, long long cstride, int Luse, int M, int Ltab, int nt, const T *tab,
+			     typename V2<T>::t *F)
+{
+	typedef typename V2<T>::t T2;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int W = 2 * M + 1;
+	const int mi = blockIdx.x % W;
+	const int s0 = (blockIdx.x / W) * SF_SER;
+	const int m = mi - M;
+	const int am = m < 0 ? -m : m;
+	const int K = ((polar && m != 0) || am > Luse) ? 0 : Luse - am + 1;  // degrees am .. Luse
+	T *ts = (T *) smem_raw;                               // [K][nt]
+	T2 *cs = (T2 *) (smem_raw + (((size_t) K * nt * sizeof(T) + 15) & ~(size_t) 15));  // [SF_SER][K]
+	const T *t0 = tab + tab_off(Ltab, nt, am);
+	for(int k = threadIdx.x; k < K * nt; k += blockDim.x)
+		ts[k] = t0[k];
+	for(int k = threadIdx.x; k < SF_SER * K; k += blockDim.x) {
+		const int ss = k / K, l = am + (k - ss * K);
+		const int sr = s0 + ss;
+		T2 v = mk2((T) 0, (T) 0);
+		if(sr < S) {
+			const Tin2 c = coeff[(long long) sr * cstride + (polar ? l : lmoff(L_in, l, m))];
+			v = mk2((T) c.x, (T) c.y);
+		}
+		cs[k] = v;
+	}
+	__syncthreads();
+	const bool neg = m < 0 && (am & 1);
+	for(int i = threadIdx.x; i < nt; i += blockDim.x) {
+		T ar[SF_SER], ai[SF_SER];
+#pragma unroll
+		for(int ss = 0; ss < SF_SER; ss++)
+			ar[ss] = ai[ss] = 0;
+		for(int k = 0; k < K; k++) {
+			const T p = ts[k * nt + i];
+#pragma unroll
+			for(int ss = 0; ss < SF_SER; ss++) {
+				const T2 c = cs[ss * K + k];
+				ar[ss] += c.x * p;
+				ai[ss] += c.y * p;
+			}
+		}
+#pragma unroll
+		for(int ss = 0; ss < SF_SER; ss++)
+			if(s0 + ss < S)
+				F[((long long) (s0 + ss) * nt + i) * W + mi] = neg ? mk2(-ar[ss], -ai[ss]) : mk2(ar[ss], ai[ss]);
+	}
+}
+
 // ---------------------------------------------------------------------------
 // azimuthal synthesis, one block per (row i, series s):
 //   v_j = sum_m F_m e^{i m phi_j}, phi_j = 2 pi j / nphi, by Horner's rule in
@@ -486,6 +544,77 @@ __global__ void k_sht_A(int L_out, int L_lay, int polar_out, int M, int Ltab, in
 		}
 		if(lane == 0)
 			out[(long long) s * ostride + (polar_out ? l : lmoff(L_lay, l, m))] = make_double2(sg * (double) ar, sg * (double) ai);
+	}
+}
+
+// The same Legendre analysis for SA_SER series per block and one order:
+// their H columns of the order and the order's table block in shared
+// memory; a thread keeps SA_LS series x SA_LL degrees of sums over the
+// rows, so each shared read serves several sums.  (Rows summed in order,
+// not by the warp tree of k_sht_A: the results agree to rounding.)
+constexpr int SA_SER = 16, SA_LS = 4, SA_LL = 2;
+
+template <class T>
+__global__ void k_sht_A_tile(int S, int L_out, int L_lay, int polar_out, int M, int Ltab, int nt, const typename V2<T>::t *H, const T *tab,
+			     double2 *out, long long ostride)
+{
+	typedef typename V2<T>::t T2;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int W = 2 * M + 1;
+	const int mi = blockIdx.x % W;
+	const int s0 = (blockIdx.x / W) * SA_SER;
+	const int m = mi - M;
+	const int am = m < 0 ? -m : m;
+	if(am > L_out || (polar_out && m != 0))
+		return;
+	const int K = L_out - am + 1;
+	T2 *hs = (T2 *) smem_raw;           // [SA_SER][nt]
+	T *ts = (T *) (hs + SA_SER * nt);   // [K][nt]
+	for(int k = threadIdx.x; k < SA_SER * nt; k += blockDim.x) {
+		const int ss = k / nt, i = k - ss * nt;
+		hs[k] = s0 + ss < S ? H[((long long) (s0 + ss) * nt + i) * W + mi] : mk2((T) 0, (T) 0);
+	}
+	const T *t0 = tab + tab_off(Ltab, nt, am);
+	for(int k = threadIdx.x; k < K * nt; k += blockDim.x)
+		ts[k] = t0[k];
+	__syncthreads();
+	const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
+	constexpr int NSG = SA_SER / SA_LS;
+	const int sgp = threadIdx.x % NSG;  // series group
+	for(int lg = threadIdx.x / NSG; lg * SA_LL < K; lg += blockDim.x / NSG) {
+		T ar[SA_LS][SA_LL], ai[SA_LS][SA_LL];
+#pragma unroll
+		for(int a = 0; a < SA_LS; a++)
+#pragma unroll
+			for(int b = 0; b < SA_LL; b++)
+				ar[a][b] = ai[a][b] = 0;
+		for(int i = 0; i < nt; i++) {
+			T p[SA_LL];
+#pragma unroll
+			for(int b = 0; b < SA_LL; b++)
+				p[b] = lg * SA_LL + b < K ? ts[(lg * SA_LL + b) * nt + i] : (T) 0;
+#pragma unroll
+			for(int a = 0; a < SA_LS; a++) {
+				const T2 v = hs[(sgp * SA_LS + a) * nt + i];
+#pragma unroll
+				for(int b = 0; b < SA_LL; b++) {
+					ar[a][b] += v.x * p[b];
+					ai[a][b] += v.y * p[b];
+				}
+			}
+		}
+#pragma unroll
+		for(int a = 0; a < SA_LS; a++) {
+			const int sr = s0 + sgp * SA_LS + a;
+			if(sr >= S)
+				continue;
+#pragma unroll
+			for(int b = 0; b < SA_LL; b++) {
+				const int l = am + lg * SA_LL + b;
+				if(l <= L_out)
+					out[(long long) sr * ostride + (polar_out ? l : lmoff(L_lay, l, m))] = make_double2(sg * (double) ar[a][b], sg * (double) ai[a][b]);
+			}
+		}
 	}
 }
 
@@ -1275,9 +1404,21 @@ static int launch_F(const ShtPlan *p, const double2 *coeff, long long cstride, u
 		    cudaStream_t st)
 {
 	const int W = 2 * M + 1;
-	const unsigned grid = (unsigned) ((W * p->nt + 127) / 128) * (unsigned) S;
-	k_sht_F<double2, T><<<grid, 128, 0, st>>>((int) L_in, polar, coeff, cstride, (int) Luse, M, (int) p->L, p->nt, (const T *) p->d_tab,
-						  (typename V2<T>::t *) F);
+	// tiled over series when an order's table block and the tile's
+	// coefficients fit in shared memory (48 KB), else one thread per
+	// (series, order, row)
+	const int Kmax = (int) Luse + 1;
+	const size_t tsm = (((size_t) Kmax * p->nt * sizeof(T) + 15) & ~(size_t) 15) + (size_t) SF_SER * Kmax * sizeof(typename V2<T>::t);
+	if(tsm <= 48 * 1024) {
+		const int thr = p->nt >= 256 ? 256 : ((p->nt + 31) / 32) * 32;
+		const unsigned grid = (unsigned) W * (unsigned) ((S + SF_SER - 1) / SF_SER);
+		k_sht_F_tile<double2, T><<<grid, thr, tsm, st>>>(S, (int) L_in, polar, coeff, cstride, (int) Luse, M, (int) p->L, p->nt, (const T *) p->d_tab,
+								  (typename V2<T>::t *) F);
+	} else {
+		const unsigned grid = (unsigned) ((W * p->nt + 127) / 128) * (unsigned) S;
+		k_sht_F<double2, T><<<grid, 128, 0, st>>>((int) L_in, polar, coeff, cstride, (int) Luse, M, (int) p->L, p->nt, (const T *) p->d_tab,
+							  (typename V2<T>::t *) F);
+	}
 	CK(cudaGetLastError());
 	return 0;
 }
@@ -1402,15 +1543,28 @@ int sht_analysis(void *plan, const void *mesh, int S, unsigned L_out, int polar_
 	const long long nrows = (long long) p->nt * S;
 	const unsigned grid = (unsigned) ((nrows + rpb - 1) / rpb), agrid = (unsigned) W * (unsigned) S;
 	const size_t hsm = (size_t) (1 + rpb) * p->nphi * esz;
+	// the tiled Legendre analysis: SA_SER series' H columns and one order's
+	// table block in shared memory
+	const unsigned tgrid = (unsigned) W * (unsigned) ((S + SA_SER - 1) / SA_SER);
+	const size_t asm_f = (size_t) SA_SER * p->nt * sizeof(float2) + (size_t) (L_out + 1) * p->nt * sizeof(float);
+	const size_t asm_d = (size_t) SA_SER * p->nt * sizeof(double2) + (size_t) (L_out + 1) * p->nt * sizeof(double);
 	if(p->fp32) {
 		k_sht_H<double2, float><<<grid, 32 * rpb, hsm, st>>>(nrows, p->nt, p->nphi, M, (const double2 *) mesh, p->d_w, (const float2 *) p->d_tw,
 								     (float2 *) scratch);
-		k_sht_A<float><<<agrid, 256, 0, st>>>((int) L_out, (int) L_layout, polar_out, M, (int) p->L, p->nt, (const float2 *) scratch, (const float *) p->d_tab,
-								(double2 *) out, ostride);
+		if(asm_f <= kMaxDynSmem)
+			k_sht_A_tile<float><<<tgrid, 128, asm_f, st>>>(S, (int) L_out, (int) L_layout, polar_out, M, (int) p->L, p->nt, (const float2 *) scratch,
+								       (const float *) p->d_tab, (double2 *) out, ostride);
+		else
+			k_sht_A<float><<<agrid, 256, 0, st>>>((int) L_out, (int) L_layout, polar_out, M, (int) p->L, p->nt, (const float2 *) scratch,
+								(const float *) p->d_tab, (double2 *) out, ostride);
 	} else {
 		k_sht_H<double2, double><<<grid, 32 * rpb, hsm, st>>>(nrows, p->nt, p->nphi, M, (const double2 *) mesh, p->d_w, (const double2 *) p->d_tw,
 								      (double2 *) scratch);
-		k_sht_A<double><<<agrid, 256, 0, st>>>((int) L_out, (int) L_layout, polar_out, M, (int) p->L, p->nt, (const double2 *) scratch,
+		if(asm_d <= kMaxDynSmem)
+			k_sht_A_tile<double><<<tgrid, 128, asm_d, st>>>(S, (int) L_out, (int) L_layout, polar_out, M, (int) p->L, p->nt, (const double2 *) scratch,
+									(const double *) p->d_tab, (double2 *) out, ostride);
+		else
+			k_sht_A<double><<<agrid, 256, 0, st>>>((int) L_out, (int) L_layout, polar_out, M, (int) p->L, p->nt, (const double2 *) scratch,
 								 (const double *) p->d_tab, (double2 *) out, ostride);
 	}
 	CK(cudaGetLastError());
@@ -1471,15 +1625,8 @@ int sht_product(void *plan, int S, const void *a, long long astride, unsigned La
 	// F arrays at the common order limit M (a factor with fewer orders
 	// contributes zeros there)
 	auto fill = [&](const void *c, long long cs, unsigned Lc, int pc, char *F) -> int {
-		const unsigned g = (unsigned) ((W * p->nt + 127) / 128) * (unsigned) S;
-		if(p->fp32)
-			k_sht_F<double2, float><<<g, 128, 0, st>>>((int) Lc, pc, (const double2 *) c, cs, (int) Lc, M, (int) p->L, p->nt, (const float *) p->d_tab,
-								    (float2 *) F);
-		else
-			k_sht_F<double2, double><<<g, 128, 0, st>>>((int) Lc, pc, (const double2 *) c, cs, (int) Lc, M, (int) p->L, p->nt,
-								     (const double *) p->d_tab, (double2 *) F);
-		CK(cudaGetLastError());
-		return 0;
+		return p->fp32 ? launch_F<float>(p, (const double2 *) c, cs, Lc, pc, Lc, M, S, F, st)
+			       : launch_F<double>(p, (const double2 *) c, cs, Lc, pc, Lc, M, S, F, st);
 	};
 	if(fill(a, astride, La, pa, Fa) || fill(b, bstride, Lb, pb, Fb))
 		return -1;
