@@ -444,13 +444,90 @@ __global__ void k_sht_pix_prod(long long nrows, int nphi, int M, const typename 
 	}
 }
 
-constexpr int SH_ROWS = 4;  // most rows per block of the azimuthal analysis (one warp each)
-constexpr int SH_QB = 4;    // consecutive orders per lane
+constexpr int SH_ROWS = 16;  // most rows per block of the azimuthal analysis
+constexpr int SH_RT = 4;     // rows per thread
+constexpr int SH_QB = 4;     // consecutive orders per thread
 
 template <class Tin2, class T>
-__global__ void k_sht_H(long long nrows, int nt, int nphi, int M, const Tin2 *mesh, const double *w, const typename V2<T>::t *tw, typename V2<T>::t *H)
+__global__ void k_sht_H(long long nrows, int nt, int nphi, int M, const Tin2 *mesh, const double *w, const typename V2<T>::t *tw, typename V2<T>::t *H,
+			int rpb)
 {
-	// blockDim / 32 (<= SH_ROWS) rows per block, one warp per row; a lane takes SH_QB
+	// rpb (<= SH_ROWS, a multiple of SH_RT) rows per block; a thread takes
+	// SH_RT rows x SH_QB consecutive orders: per pixel one scattered
+	// twiddle read for its first order (the others by multiplying with
+	// the pixel's e^{i phi_j}, a broadcast read) and SH_RT row values, for
+	// SH_RT x SH_QB sums
+	typedef typename V2<T>::t T2;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	T2 *tws = (T2 *) smem_raw;
+	T2 *rows_s = tws + nphi;  // [rpb][nphi]
+	const int W = 2 * M + 1;
+	const long long row0 = (long long) blockIdx.x * rpb;
+	for(int k = threadIdx.x; k < nphi; k += blockDim.x)
+		tws[k] = tw[k];
+	for(int k = threadIdx.x; k < rpb * nphi; k += blockDim.x) {
+		const int r = k / nphi;
+		T2 v = mk2((T) 0, (T) 0);
+		if(row0 + r < nrows) {
+			const Tin2 x = mesh[(row0 + r) * nphi + (k - r * nphi)];
+			v = mk2((T) x.x, (T) x.y);
+		}
+		rows_s[k] = v;
+	}
+	__syncthreads();
+	const int ngroups = (W + SH_QB - 1) / SH_QB;   // order groups
+	const int nrg = rpb / SH_RT;                   // row groups
+	for(int task = threadIdx.x; task < ngroups * nrg; task += blockDim.x) {
+		const int og = task % ngroups, rg = task / ngroups;
+		const int mi0 = og * SH_QB, m0 = mi0 - M;
+		const int step = ((m0 % nphi) + nphi) % nphi;
+		const T2 *rv = rows_s + rg * SH_RT * nphi;
+		int idx = 0;
+		T hr[SH_RT][SH_QB], hi[SH_RT][SH_QB];
+#pragma unroll
+		for(int a = 0; a < SH_RT; a++)
+#pragma unroll
+			for(int q = 0; q < SH_QB; q++)
+				hr[a][q] = hi[a][q] = 0;
+		for(int j = 0; j < nphi; j++) {
+			const T2 z = tws[j];  // e^{i phi_j}
+			T2 e = tws[idx];      // e^{i m0 phi_j}
+			T2 v[SH_RT];
+#pragma unroll
+			for(int a = 0; a < SH_RT; a++)
+				v[a] = rv[a * nphi + j];
+#pragma unroll
+			for(int q = 0; q < SH_QB; q++) {
+#pragma unroll
+				for(int a = 0; a < SH_RT; a++) {
+					// v * conj(e), e = e^{i (m0 + q) phi_j}
+					hr[a][q] += v[a].x * e.x + v[a].y * e.y;
+					hi[a][q] += v[a].y * e.x - v[a].x * e.y;
+				}
+				e = cmul2(e, z);
+			}
+			idx += step;
+			if(idx >= nphi)
+				idx -= nphi;
+		}
+#pragma unroll
+		for(int a = 0; a < SH_RT; a++) {
+			const long long row = row0 + rg * SH_RT + a;
+			if(row >= nrows)
+				continue;
+			const T scale = (T) (2.0 * M_PI / nphi * w[(int) (row % nt)]);
+#pragma unroll
+			for(int q = 0; q < SH_QB; q++)
+				if(mi0 + q < W)
+					H[row * W + mi0 + q] = mk2(hr[a][q] * scale, hi[a][q] * scale);
+		}
+	}
+}
+
+template <class Tin2, class T>
+__global__ void k_sht_H1(long long nrows, int nt, int nphi, int M, const Tin2 *mesh, const double *w, const typename V2<T>::t *tw, typename V2<T>::t *H)
+{
+	// wide grids: blockDim / 32 rows per block, one warp per row; a lane takes SH_QB
 	// consecutive orders: one scattered twiddle read per pixel for the
 	// first, the others by multiplying with the pixel's e^{i phi_j} (a
 	// broadcast read), so each pixel value read serves SH_QB sums
@@ -1532,10 +1609,13 @@ int sht_analysis(void *plan, const void *mesh, int S, unsigned L_out, int polar_
 	const int M = polar_out ? 0 : (int) L_out;
 	const int W = 2 * M + 1;
 	// rows per block of the azimuthal analysis: as many as fit beside the
-	// twiddles in the shared-memory budget, up to SH_ROWS
+	// twiddles in the shared-memory budget, up to SH_ROWS, a multiple of
+	// SH_RT
 	const size_t esz = p->fp32 ? sizeof(float2) : sizeof(double2);
 	const size_t fit = kMaxDynSmem / ((size_t) p->nphi * esz);  // rows of the grid, twiddles included
-	const int rpb = fit >= 2 ? (int) std::min<size_t>(SH_ROWS, fit - 1) : 0;
+	// (wide grids, fewer than 1 + SH_RT rows: one row per warp, k_sht_H1)
+	const bool wide = fit < 1 + SH_RT;
+	const int rpb = !wide ? (int) std::min<size_t>(SH_ROWS, (fit - 1) / SH_RT * SH_RT) : (fit >= 2 ? (int) std::min<size_t>(SH_RT, fit - 1) : 0);
 	if(rpb < 1) {
 		set_error("sht analysis: grid of %d columns too wide", p->nphi);
 		return -1;
@@ -1549,8 +1629,12 @@ int sht_analysis(void *plan, const void *mesh, int S, unsigned L_out, int polar_
 	const size_t asm_f = (size_t) SA_SER * p->nt * sizeof(float2) + (size_t) (L_out + 1) * p->nt * sizeof(float);
 	const size_t asm_d = (size_t) SA_SER * p->nt * sizeof(double2) + (size_t) (L_out + 1) * p->nt * sizeof(double);
 	if(p->fp32) {
-		k_sht_H<double2, float><<<grid, 32 * rpb, hsm, st>>>(nrows, p->nt, p->nphi, M, (const double2 *) mesh, p->d_w, (const float2 *) p->d_tw,
-								     (float2 *) scratch);
+		if(wide)
+			k_sht_H1<double2, float><<<grid, 32 * rpb, hsm, st>>>(nrows, p->nt, p->nphi, M, (const double2 *) mesh, p->d_w, (const float2 *) p->d_tw,
+									      (float2 *) scratch);
+		else
+			k_sht_H<double2, float><<<grid, 128, hsm, st>>>(nrows, p->nt, p->nphi, M, (const double2 *) mesh, p->d_w, (const float2 *) p->d_tw,
+									(float2 *) scratch, rpb);
 		if(asm_f <= kMaxDynSmem)
 			k_sht_A_tile<float><<<tgrid, 128, asm_f, st>>>(S, (int) L_out, (int) L_layout, polar_out, M, (int) p->L, p->nt, (const float2 *) scratch,
 								       (const float *) p->d_tab, (double2 *) out, ostride);
@@ -1558,8 +1642,12 @@ int sht_analysis(void *plan, const void *mesh, int S, unsigned L_out, int polar_
 			k_sht_A<float><<<agrid, 256, 0, st>>>((int) L_out, (int) L_layout, polar_out, M, (int) p->L, p->nt, (const float2 *) scratch,
 								(const float *) p->d_tab, (double2 *) out, ostride);
 	} else {
-		k_sht_H<double2, double><<<grid, 32 * rpb, hsm, st>>>(nrows, p->nt, p->nphi, M, (const double2 *) mesh, p->d_w, (const double2 *) p->d_tw,
-								      (double2 *) scratch);
+		if(wide)
+			k_sht_H1<double2, double><<<grid, 32 * rpb, hsm, st>>>(nrows, p->nt, p->nphi, M, (const double2 *) mesh, p->d_w, (const double2 *) p->d_tw,
+									       (double2 *) scratch);
+		else
+			k_sht_H<double2, double><<<grid, 128, hsm, st>>>(nrows, p->nt, p->nphi, M, (const double2 *) mesh, p->d_w, (const double2 *) p->d_tw,
+									 (double2 *) scratch, rpb);
 		if(asm_d <= kMaxDynSmem)
 			k_sht_A_tile<double><<<tgrid, 128, asm_d, st>>>(S, (int) L_out, (int) L_layout, polar_out, M, (int) p->L, p->nt, (const double2 *) scratch,
 									(const double *) p->d_tab, (double2 *) out, ostride);
