@@ -168,7 +168,11 @@ void dfree(void *p)
 		cudaFree(p);
 }
 
-void *dscratch(size_t bytes)
+void *dscratch(size_t bytes) { return dscratch_on(bytes, nullptr); }
+
+void dscratch_free(void *p) { dscratch_free_on(p, nullptr); }
+
+void *dscratch_on(size_t bytes, void *stream)
 {
 	if(alloc_fault_due()) {
 		set_error("scratch of %zu bytes: injected allocation failure", bytes);
@@ -183,7 +187,7 @@ void *dscratch(size_t bytes)
 		pool = g_pools[dev];
 	}
 	void *p = nullptr;
-	cudaError_t e = cudaMallocFromPoolAsync(&p, bytes ? bytes : 16, pool, S());
+	cudaError_t e = cudaMallocFromPoolAsync(&p, bytes ? bytes : 16, pool, stream ? (cudaStream_t) stream : S());
 	if(e != cudaSuccess) {
 		set_error("scratch of %zu bytes: %s", bytes, cudaGetErrorString(e));
 		return nullptr;
@@ -191,10 +195,10 @@ void *dscratch(size_t bytes)
 	return p;
 }
 
-void dscratch_free(void *p)
+void dscratch_free_on(void *p, void *stream)
 {
 	if(p)
-		cudaFreeAsync(p, S());
+		cudaFreeAsync(p, stream ? (cudaStream_t) stream : S());
 }
 
 int h2d(void *dst, const void *src, size_t bytes)

@@ -35,6 +35,9 @@ void dfree(void *p);
 // calls, which synchronise before they return)
 void *dscratch(size_t bytes);  // NULL + error on failure
 void dscratch_free(void *p);
+// the same, ordered on a given stream (NULL: the library stream)
+void *dscratch_on(size_t bytes, void *stream);
+void dscratch_free_on(void *p, void *stream);
 int h2d(void *dst, const void *src, size_t bytes);       // async on lib stream
 int d2h(void *dst, const void *src, size_t bytes);       // async on lib stream
 int dmemset(void *dst, int value, size_t bytes);         // async on lib stream

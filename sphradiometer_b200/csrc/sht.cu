@@ -707,7 +707,9 @@ __global__ void k_zero2(long long n, Tout2 *p, long long stride, int S)
 }
 
 // ---------------------------------------------------------------------------
-// peak refinement: one warp per series, FP64.  Maximises g = sign * Re f on
+// peak refinement: one warp per series at a time, FP64, on the series
+// folded to the orders m >= 0 of Re f where it is staged in shared
+// memory.  Maximises g = sign * Re f on
 // the sphere by trust-region Newton steps in the local orthonormal frame
 // (d theta, sin theta d phi) with the covariant Hessian; value, gradient and
 // Hessian come from one pass of the Legendre recurrences per step:
@@ -730,7 +732,12 @@ struct RecCoef {
 	double a, b, c;
 };
 
-template <bool H>
+// FOLD: c holds the folded series of Re f, orders m >= 0 only, laid out
+// as the m >= 0 part of a full series ([m][l - m]):
+//   c_lm = a_lm + (-1)^m conj(a_{l,-m})  (m > 0),  c_l0 = a_l0,
+// since Re(a_{l,-m} Y_{l,-m}) = Re((-1)^m conj(a_{l,-m}) Y_lm) with
+// Y_{l,-m} = (-1)^m conj(Y_lm); the -m rows are then not read
+template <bool H, bool FOLD>
 __device__ void peak_eval_order(int L, int polar, const double2 *c, int m, double x, double st, double lam, double cs, double sn, const RecCoef *rc,
 				PeakEval &acc)
 {
@@ -761,7 +768,7 @@ __device__ void peak_eval_order(int L, int polar, const double2 *c, int m, doubl
 			A2r += cp.x * d2;
 			A2i += cp.y * d2;
 		}
-		if(m > 0) {
+		if(!FOLD && m > 0) {
 			const double2 cn = cnm[l];
 			Br += cn.x * lam;
 			Bi += cn.y * lam;
@@ -796,7 +803,7 @@ __device__ void peak_eval_order(int L, int polar, const double2 *c, int m, doubl
 	acc.ftp += -m * ImA1 + m * ImB1;
 }
 
-template <bool H>
+template <bool H, bool FOLD>
 __device__ PeakEval peak_eval(int L, int polar, const double2 *c, double theta, double phi, const RecCoef *rc, const double *pre)
 {
 	PeakEval e = {0, 0, 0, 0, 0, 0};
@@ -839,7 +846,7 @@ __device__ PeakEval peak_eval(int L, int polar, const double2 *c, double theta, 
 			double lam = pre[m] * pw * gw;
 			if(m & 1)
 				lam = -lam;
-			peak_eval_order<H>(L, polar, c, m, x, st, lam, zr * gr - zi * gi, zr * gi + zi * gr, rc, e);
+			peak_eval_order<H, FOLD>(L, polar, c, m, x, st, lam, zr * gr - zi * gi, zr * gi + zi * gr, rc, e);
 		}
 		gw *= pw32;
 		const double r = gr * z32r - gi * z32i;
@@ -901,6 +908,7 @@ __device__ double ang_dist(double t1, double p1, double t2, double p2)
 // the unit vectors (d/dtheta, (1/sin theta) d/dphi), which makes the line
 // search's slope differ from the true one away from the equator.
 // ---------------------------------------------------------------------------
+template <bool FOLD>
 struct PeakFdf {
 	int L, polar;
 	const double2 *c;
@@ -912,7 +920,7 @@ struct PeakFdf {
 	{
 		double t = x[0], p = x[1];
 		condition_tp(t, p);
-		const PeakEval e = peak_eval<false>(L, polar, c, t, p, rc, pre);
+		const PeakEval e = peak_eval<false, FOLD>(L, polar, c, t, p, rc, pre);
 		h = -sign * e.f;
 		g[0] = -sign * e.ft;
 		g[1] = -sign * (unit_grad ? e.fp / sin(t) : e.fp);
@@ -1096,49 +1104,18 @@ __device__ bool bfgs2_iterate(Bfgs2 &s, const Fdf &fdf)
 }
 
 constexpr size_t kRefineSmem = 227 * 1024;  // peak refinement: tables + the block's series
-constexpr int kRefineWarps = 12;             // most warps (series) per refinement block
+// most warps (series) per refinement block: the Newton kernel's state
+// (value, gradient and Hessian) fits 168 registers a thread, 12 warps;
+// the BFGS2 kernels' 128, 16 warps
+__host__ __device__ constexpr int refine_warps(int method) { return method == 0 ? 12 : 16; }
 
-// METHOD 0: trust-region Newton (tol: smallest step); 1: BFGS2 with the
-// gradient in the co-ordinates; 2: BFGS2 as the reference's extremizer
-// runs it (unit-vector gradient components, co-ordinates returned
-// unconditioned).  The BFGS2 methods stop at |gradient| < 1e-3 as the
-// reference does.  One kernel per method: each carries only its own
-// state (registers, and instruction-cache footprint).
-template <int METHOD>
-__global__ void __launch_bounds__(32 * kRefineWarps, 1) k_peak_refine(int S, int L, int polar, const double2 *coeff, long long cstride, const double *theta0, const double *phi0, double sign,
-			      int max_iter, double tol, double *out /* [S][4] */, int *status, const RecCoef *rc_g, const double *pre_g, int n_rc,
-			      int n_sky, int sky_off)
+// refinement of series s (coefficients c) by METHOD (the methods are
+// listed at k_peak_refine); warp-collective
+template <int METHOD, bool FOLD>
+__device__ __forceinline__ void refine_series(int s, const double2 *c, int L, int polar, const double *theta0, const double *phi0, double sign, int max_iter,
+					      double tol, double *out, int *status, const RecCoef *rc, const double *pre)
 {
 	constexpr int method = METHOD;
-	// the tables in shared memory when they fit (n_rc > 0), else read
-	// from global memory; with n_sky > 0 each warp also copies its
-	// series' n_sky coefficients to shared memory (at byte sky_off), so
-	// that every evaluation reads them there
-	extern __shared__ __align__(16) unsigned char smem_raw[];
-	const RecCoef *rc = rc_g;
-	const double *pre = pre_g;
-	if(n_rc > 0) {
-		RecCoef *rcs = (RecCoef *) smem_raw;
-		double *ps = (double *) (rcs + n_rc);
-		for(int i = threadIdx.x; i < n_rc; i += blockDim.x)
-			rcs[i] = rc_g[i];
-		for(int i = threadIdx.x; i <= L; i += blockDim.x)
-			ps[i] = pre_g[i];
-		__syncthreads();
-		rc = rcs;
-		pre = ps;
-	}
-	const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-	if(s >= S)
-		return;
-	const double2 *c = coeff + (long long) s * cstride;
-	if(n_sky > 0) {
-		double2 *cs = (double2 *) (smem_raw + sky_off) + (size_t) (threadIdx.x >> 5) * n_sky;
-		for(int i = threadIdx.x & 31; i < n_sky; i += 32)
-			cs[i] = c[i];
-		__syncwarp();
-		c = cs;
-	}
 	double t = theta0[s], p = phi0[s];
 	if(!(t == t) || !(p == p)) {
 		if((threadIdx.x & 31) == 0) {
@@ -1148,7 +1125,7 @@ __global__ void __launch_bounds__(32 * kRefineWarps, 1) k_peak_refine(int S, int
 		return;
 	}
 	if constexpr(METHOD != 0) {
-		const PeakFdf fdf{L, polar, c, rc, pre, sign, METHOD == 2};
+		const PeakFdf<FOLD> fdf{L, polar, c, rc, pre, sign, METHOD == 2};
 		double tc = t, pc = p;
 		condition_tp(tc, pc);
 		Bfgs2 bs;
@@ -1190,7 +1167,7 @@ __global__ void __launch_bounds__(32 * kRefineWarps, 1) k_peak_refine(int S, int
 	condition_tp(t, p);
 	const double ts = t, ps = p;
 	double radius = M_PI / 24;
-	PeakEval e = peak_eval<true>(L, polar, c, t, p, rc, pre);
+	PeakEval e = peak_eval<true, FOLD>(L, polar, c, t, p, rc, pre);
 	double g = sign * e.f;
 	int it = 0, converged = 0;
 	for(; it < max_iter; it++) {
@@ -1222,7 +1199,7 @@ __global__ void __launch_bounds__(32 * kRefineWarps, 1) k_peak_refine(int S, int
 		}
 		double tn = t + du, pn = p + dv / st;
 		condition_tp(tn, pn);
-		const PeakEval en = peak_eval<true>(L, polar, c, tn, pn, rc, pre);
+		const PeakEval en = peak_eval<true, FOLD>(L, polar, c, tn, pn, rc, pre);
 		const double gn = sign * en.f;
 		if(gn >= g) {
 			// a short step that no longer raises the value is at the
@@ -1256,6 +1233,83 @@ __global__ void __launch_bounds__(32 * kRefineWarps, 1) k_peak_refine(int S, int
 		out[4 * s + 2] = e.f;
 		out[4 * s + 3] = ang_dist(ts, ps, t, p);
 		status[s] = converged | (it << 1);
+	}
+}
+
+// METHOD 0: trust-region Newton (tol: smallest step); 1: BFGS2 with the
+// gradient in the co-ordinates; 2: BFGS2 as the reference's extremizer
+// runs it (unit-vector gradient components, co-ordinates returned
+// unconditioned).  The BFGS2 methods stop at |gradient| < 1e-3 as the
+// reference does.  One kernel per method: each carries only its own
+// state (registers, and instruction-cache footprint).
+//
+// With a work counter (next, zero at launch) the grid is persistent: each
+// warp takes its next series from the counter until none is left, so that
+// series that need many iterations do not hold a whole wave of blocks
+// behind them; without one, a warp per series.  The staged (FOLD) kernel
+// runs up to refine_warps(METHOD) warps per block; the unstaged one four.
+template <int METHOD, bool FOLD>
+__global__ void __launch_bounds__(FOLD ? 32 * refine_warps(METHOD) : 128, 1)
+    k_peak_refine(int S, int L, int polar, const double2 *coeff, long long cstride, const double *theta0, const double *phi0, double sign, int max_iter,
+		  double tol, double *out /* [S][4] */, int *status, const RecCoef *rc_g, const double *pre_g, int n_rc, int n_sky, int sky_off, int *next)
+{
+	// the tables in shared memory when they fit (n_rc > 0), else read
+	// from global memory; with n_sky > 0 each warp also copies its
+	// series' n_sky coefficients to shared memory (at byte sky_off), so
+	// that every evaluation reads them there -- with FOLD (always staged)
+	// the folded series of Re f, orders m >= 0 (n_sky of them)
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const RecCoef *rc = rc_g;
+	const double *pre = pre_g;
+	if(n_rc > 0) {
+		RecCoef *rcs = (RecCoef *) smem_raw;
+		double *ps = (double *) (rcs + n_rc);
+		for(int i = threadIdx.x; i < n_rc; i += blockDim.x)
+			rcs[i] = rc_g[i];
+		for(int i = threadIdx.x; i <= L; i += blockDim.x)
+			ps[i] = pre_g[i];
+		__syncthreads();
+		rc = rcs;
+		pre = ps;
+	}
+	const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+	double2 *cs = (double2 *) (smem_raw + sky_off) + (size_t) warp * n_sky;
+	int s = blockIdx.x * (blockDim.x >> 5) + warp;
+	for(;;) {
+		if(next) {
+			int v = 0;
+			if(lane == 0)
+				v = atomicAdd(next, 1);
+			s = __shfl_sync(0xffffffffu, v, 0);
+		}
+		if(s >= S)
+			return;
+		const double2 *c = coeff + (long long) s * cstride;
+		if(n_sky > 0) {
+			__syncwarp();  // the previous series is no longer read
+			if(FOLD && !polar) {
+				for(int m = 0; m <= L; m++) {
+					const long long o = lmoff(L, m, m) - m, on = m > 0 ? lmoff(L, m, -m) - m : 0;
+					for(int l = m + lane; l <= L; l += 32) {
+						double2 v = c[o + l];
+						if(m > 0) {
+							const double2 w = c[on + l];
+							v.x += (m & 1) ? -w.x : w.x;
+							v.y -= (m & 1) ? -w.y : w.y;
+						}
+						cs[o + l] = v;
+					}
+				}
+			} else {
+				for(int i = lane; i < n_sky; i += 32)
+					cs[i] = c[i];
+			}
+			__syncwarp();
+			c = cs;
+		}
+		refine_series<METHOD, FOLD>(s, c, L, polar, theta0, phi0, sign, max_iter, tol, out, status, rc, pre);
+		if(!next)
+			return;
 	}
 }
 
@@ -1822,32 +1876,51 @@ int peak_refine(int S, unsigned L, int polar, const void *coeff, long long cstri
 		sm = 0;
 	// each warp's series in shared memory too (evaluations then read no
 	// global memory), as many warps per block as the tables and their
-	// series fit in kRefineSmem -- one block per SM, up to kRefineWarps
-	// warps; otherwise four warps reading their series from global memory
-	const size_t clen = polar ? (size_t) L + 1 : (size_t) (L + 1) * (L + 1);
+	// series fit in kRefineSmem -- one block per SM, up to
+	// refine_warps(method) warps; otherwise four warps reading their series from global memory.
+	// A staged series is folded to the orders m >= 0 of Re f (half the
+	// bytes and half the products of the evaluation)
+	const size_t clen_fold = polar ? (size_t) L + 1 : (size_t) tab_off((int) L, 1, (int) L + 1);
 	const size_t sky_off = (sm + 15) & ~(size_t) 15;
-	const size_t fit = staged && sky_off < kRefineSmem ? (kRefineSmem - sky_off) / (clen * sizeof(double2)) : 0;
+	const size_t fit = staged && sky_off < kRefineSmem ? (kRefineSmem - sky_off) / (clen_fold * sizeof(double2)) : 0;
 	const bool stage_sky = fit >= 4;
-	const int wpb = stage_sky ? (int) std::min<size_t>(fit, kRefineWarps) : 4;
+	const int wpb = stage_sky ? (int) std::min<size_t>(fit, refine_warps(method)) : 4;
 	if(stage_sky)
-		sm = sky_off + (size_t) wpb * clen * sizeof(double2);
-	const int nsky = stage_sky ? (int) clen : 0;
-	const unsigned grid = (S + wpb - 1) / wpb;
+		sm = sky_off + (size_t) wpb * clen_fold * sizeof(double2);
+	const int nsky = stage_sky ? (int) clen_fold : 0;
 	const int nrc = staged ? t.n : 0;
-	// (the attribute is per device: set on every call that needs it)
-	if(sm > kMaxDynSmem)
-		CK(method == 0 ? cudaFuncSetAttribute(k_peak_refine<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kRefineSmem)
-		   : method == 1 ? cudaFuncSetAttribute(k_peak_refine<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kRefineSmem)
-				 : cudaFuncSetAttribute(k_peak_refine<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kRefineSmem));
-	if(method == 0)
-		k_peak_refine<0><<<grid, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out, status,
-							       t.rc, t.pre, nrc, nsky, (int) sky_off);
-	else if(method == 1)
-		k_peak_refine<1><<<grid, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out, status,
-							       t.rc, t.pre, nrc, nsky, (int) sky_off);
+	auto launch = [&](auto kern) -> int {
+		// (the attribute is per device: set on every call that needs it)
+		if(sm > kMaxDynSmem)
+			CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) kRefineSmem));
+		// a persistent grid of the resident blocks, the series handed
+		// out by a counter, when there are more series than resident
+		// warps; else a warp per series
+		int dev = 0, sms = 0, per_sm = 0;
+		CK(cudaGetDevice(&dev));
+		CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+		CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * wpb, sm));
+		const long long blocks = (S + wpb - 1) / wpb, resident = (long long) sms * (per_sm > 0 ? per_sm : 1);
+		int *next = nullptr;
+		if(blocks > resident) {
+			next = (int *) dscratch_on(sizeof(int), st);
+			if(!next)
+				return -1;
+			CK(cudaMemsetAsync(next, 0, sizeof(int), st));
+		}
+		const unsigned grid = (unsigned) (next ? resident : blocks);
+		kern<<<grid, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out, status, t.rc, t.pre,
+						nrc, nsky, (int) sky_off, next);
+		dscratch_free_on(next, st);
+		return 0;
+	};
+	int bad;
+	if(stage_sky)
+		bad = method == 0 ? launch(k_peak_refine<0, true>) : method == 1 ? launch(k_peak_refine<1, true>) : launch(k_peak_refine<2, true>);
 	else
-		k_peak_refine<2><<<grid, 32 * wpb, sm, st>>>(S, (int) L, polar, (const double2 *) coeff, cstride, theta0, phi0, sign, max_iter, tol, out, status,
-							       t.rc, t.pre, nrc, nsky, (int) sky_off);
+		bad = method == 0 ? launch(k_peak_refine<0, false>) : method == 1 ? launch(k_peak_refine<1, false>) : launch(k_peak_refine<2, false>);
+	if(bad)
+		return -1;
 	CK(cudaGetLastError());
 	return 0;
 }

@@ -1,6 +1,6 @@
 """Drive one family of kernels on a bounded case, for profiling.
 
-``python -m sphradiometer_b200.profile_kernels <stage> [--n N] [--calls C]``
+``python -m sphradiometer_b200.profile_kernels <stage> [--n N] [--calls C] [--method M]``
 
 stages:
   render    64 x 128 FP32 sky grids of N c1 skies (k_sht_F, k_sht_pix)
@@ -50,6 +50,7 @@ def main():
     ap.add_argument("stage", choices=["render", "peaks", "rotate", "product", "mlp", "uneven", "uneven_tuned", "fseries", "nonpolar", "td"])
     ap.add_argument("--n", type=int, default=4096)
     ap.add_argument("--calls", type=int, default=3)
+    ap.add_argument("--method", type=int, default=-1, help="peaks: refinement method (0 trust-region Newton, 1 BFGS2; default: the library's)")
     args = ap.parse_args()
     import torch
 
@@ -65,6 +66,8 @@ def main():
         run = lambda: g.render(sky, out=out)  # noqa: E731
     elif args.stage == "peaks":
         sky, keep = c1_skies(S, W, n)
+        if args.method >= 0 and S.load().sphrad_sky_set_refinement(args.method):
+            raise SystemExit(f"refinement method {args.method}: not accepted")
         run = lambda: S.sky_peaks(sky)  # noqa: E731
     elif args.stage in ("rotate", "product"):
         L = 48
