@@ -45,7 +45,7 @@ namespace {
 
 constexpr int GM = 128;         // rows per tile (MMA M)
 constexpr int GK = 64;          // K per pipeline stage (4 MMAs of K = 16)
-constexpr int G_THREADS = 128;  // 4 warps: loaders, one MMA issuer, epilogue
+constexpr int G_THREADS = 256;  // 8 warps: loaders, one MMA issuer, epilogue
 
 // network dimensions (padded)
 constexpr int F_IN = 338;       // real inputs: l <= 12 a_lm
@@ -196,72 +196,109 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ Gemm
 	tc_fence_after();
 	ok = __syncthreads_and(ok && !abort_flag);
 	if(ok && nk > 0) {
-		const int r = warp * 32 + lane;
-		const int m = m0 + r;
-		for(int c0 = 0; c0 < NT; c0 += 16) {
-			uint32_t v[16];
-			tmem_ld16(tmem + ((uint32_t) (warp * 32) << 16) + (uint32_t) c0, v);
-			const int nb = n0 + c0;
-			if(EPI == kEpiStoreF32) {
-				float *dst = g.C + (long long) m * g.ldc + nb;
-				if(ks > 1) {
+		// Epilogue through shared memory (the operand ring is idle once the
+		// last MMA has retired): the accumulators go TMEM -> registers ->
+		// sZ by rows, then every global access is a whole-row one -- four
+		// consecutive columns a thread, 16 B of FP32 or 8 B of bf16, so a
+		// warp covers whole row segments -- and the transposed bf16 output
+		// and the column sums read sH column-wise.
+		constexpr int ZS = NT + 4;  // row stride of sZ (floats): rows 4 banks apart
+		constexpr int HS = NT + 4;  // row stride of sH (bf16)
+		static_assert((size_t) GM * ZS * 4 + (size_t) GM * HS * 2 <= (size_t) GSTAGES * (A_BYTES + B_BYTES), "epilogue tiles exceed the ring");
+		float *sZ = (float *) smem;
+		__nv_bfloat16 *sH = (__nv_bfloat16 *) (sZ + GM * ZS);
+		{
+			// warps w and w + 4 reach TMEM lanes 32 (w % 4) ..; they take
+			// alternate 16-column groups
+			const int q4 = warp & 3, r = q4 * 32 + lane;
+			for(int c0 = 16 * (warp >> 2); c0 < NT; c0 += 16 * (G_THREADS / 128)) {
+				uint32_t v[16];
+				tmem_ld16(tmem + ((uint32_t) (q4 * 32) << 16) + (uint32_t) c0, v);
 #pragma unroll
-					for(int j = 0; j < 16; j += 4)
-						atomicAdd((float4 *) (dst + j), make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]), __uint_as_float(v[j + 2]),
-											    __uint_as_float(v[j + 3])));
-				} else {
+				for(int j = 0; j < 16; j += 4)
+					*(float4 *) (sZ + r * ZS + c0 + j) =
+						make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]), __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
+			}
+		}
+		__syncthreads();
+		constexpr int NQ = NT / 4;  // column quads of a row
+		// QB quads a thread per round: their global loads (pre-activations,
+		// biases) issued before the first is used
+		constexpr int QB = 4;
+		for(int i0 = tid; i0 < GM * NQ; i0 += QB * G_THREADS) {
+			float4 extra[QB];
 #pragma unroll
-					for(int j = 0; j < 16; j += 4)
-						*(float4 *) (dst + j) =
-							make_float4(__uint_as_float(v[j]), __uint_as_float(v[j + 1]), __uint_as_float(v[j + 2]), __uint_as_float(v[j + 3]));
-				}
-			} else if(EPI == kEpiBias) {
-				float *dst = g.C + (long long) m * g.ldc + nb;
-#pragma unroll
-				for(int j = 0; j < 16; j++)
-					dst[j] = __uint_as_float(v[j]) + g.bias[nb + j];
-			} else if(EPI == kEpiBiasGelu) {
-				__align__(16) __nv_bfloat16 h[16];
-#pragma unroll
-				for(int j = 0; j < 16; j++) {
-					const float z = __uint_as_float(v[j]) + g.bias[nb + j];
-					if(g.C)
-						g.C[(long long) m * g.ldc + nb + j] = z;
-					h[j] = __float2bfloat16_rn(gelu(z));
-				}
-				*(uint4 *) (g.H + (long long) m * g.ldh + nb) = *(const uint4 *) &h[0];
-				*(uint4 *) (g.H + (long long) m * g.ldh + nb + 8) = *(const uint4 *) &h[8];
-				if(g.HT)
-#pragma unroll
-					for(int j = 0; j < 16; j++)
-						g.HT[(long long) (nb + j) * g.ldht + m] = h[j];
-			} else {  // kEpiGeluBwd
-				__align__(16) __nv_bfloat16 h[16];
-				float d[16];
-#pragma unroll
-				for(int j = 0; j < 16; j++) {
-					const float z = g.Zin[(long long) m * g.ldz + nb + j];
-					d[j] = __uint_as_float(v[j]) * gelu_grad(z);
-					h[j] = __float2bfloat16_rn(d[j]);
-				}
-				*(uint4 *) (g.H + (long long) m * g.ldh + nb) = *(const uint4 *) &h[0];
-				*(uint4 *) (g.H + (long long) m * g.ldh + nb + 8) = *(const uint4 *) &h[8];
-				if(g.HT)
-#pragma unroll
-					for(int j = 0; j < 16; j++)
-						g.HT[(long long) (nb + j) * g.ldht + m] = h[j];
-				if(g.colsum) {
-					// bias gradient of the bf16 dZ the weight gradients see
-#pragma unroll
-					for(int j = 0; j < 16; j++) {
-						float s = __bfloat162float(h[j]);
-						for(int o = 16; o; o >>= 1)
-							s += __shfl_xor_sync(0xffffffffu, s, o);
-						if(lane == 0)
-							atomicAdd(&g.colsum[nb + j], s);
-					}
+			for(int k = 0; k < QB; k++) {
+				const int idx = i0 + k * G_THREADS;
+				extra[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+				if(idx < GM * NQ) {
+					const int r = idx / NQ, q = idx - r * NQ;
+					if(EPI == kEpiGeluBwd)
+						extra[k] = *(const float4 *) (g.Zin + (long long) (m0 + r) * g.ldz + n0 + 4 * q);
+					else if(EPI == kEpiBias || EPI == kEpiBiasGelu)
+						extra[k] = __ldg((const float4 *) (g.bias + n0 + 4 * q));
 				}
 			}
+#pragma unroll
+			for(int k = 0; k < QB; k++) {
+				const int idx = i0 + k * G_THREADS;
+				if(idx >= GM * NQ)
+					break;
+				const int r = idx / NQ, q = idx - r * NQ;
+				const int m = m0 + r, n = n0 + 4 * q;
+				const float4 acc = *(const float4 *) (sZ + r * ZS + 4 * q);
+				const float4 x = extra[k];
+				if(EPI == kEpiStoreF32) {
+					float4 *dst = (float4 *) (g.C + (long long) m * g.ldc + n);
+					if(ks > 1)
+						atomicAdd(dst, acc);
+					else
+						*dst = acc;
+				} else if(EPI == kEpiBias) {
+					*(float4 *) (g.C + (long long) m * g.ldc + n) = make_float4(acc.x + x.x, acc.y + x.y, acc.z + x.z, acc.w + x.w);
+				} else {
+					float e[4];
+					if(EPI == kEpiBiasGelu) {
+						const float4 z = make_float4(acc.x + x.x, acc.y + x.y, acc.z + x.z, acc.w + x.w);
+						if(g.C)
+							*(float4 *) (g.C + (long long) m * g.ldc + n) = z;
+						e[0] = gelu(z.x), e[1] = gelu(z.y), e[2] = gelu(z.z), e[3] = gelu(z.w);
+					} else {  // kEpiGeluBwd: x = the pre-activation
+						e[0] = acc.x * gelu_grad(x.x), e[1] = acc.y * gelu_grad(x.y), e[2] = acc.z * gelu_grad(x.z), e[3] = acc.w * gelu_grad(x.w);
+					}
+					__align__(8) __nv_bfloat16 h[4];
+#pragma unroll
+					for(int j = 0; j < 4; j++)
+						h[j] = __float2bfloat16_rn(e[j]);
+					*(uint2 *) (g.H + (long long) m * g.ldh + n) = *(const uint2 *) h;
+					*(uint2 *) (sH + r * HS + 4 * q) = *(const uint2 *) h;
+				}
+			}
+		}
+		if(EPI == kEpiBiasGelu || EPI == kEpiGeluBwd) {
+			__syncthreads();
+			// transposed output: column n's 128 rows are 256 contiguous
+			// bytes of HT; a thread takes 16 rows (one 32-byte sector) of
+			// one column, consecutive lanes consecutive columns
+			if(g.HT)
+				for(int idx = tid; idx < NT * (GM / 16); idx += G_THREADS) {
+					const int cn = idx % NT, rc = idx / NT;
+					__align__(16) __nv_bfloat16 t[16];
+#pragma unroll
+					for(int i = 0; i < 16; i++)
+						t[i] = sH[(16 * rc + i) * HS + cn];
+					uint4 *dst = (uint4 *) (g.HT + (long long) (n0 + cn) * g.ldht + m0 + 16 * rc);
+					dst[0] = *(const uint4 *) &t[0];
+					dst[1] = *(const uint4 *) &t[8];
+				}
+			if(EPI == kEpiGeluBwd && g.colsum)
+				// bias gradient of the bf16 dZ the weight gradients see
+				for(int cn = tid; cn < NT; cn += G_THREADS) {
+					float sum = 0.f;
+					for(int i = 0; i < GM; i++)
+						sum += __bfloat162float(sH[i * HS + cn]);
+					atomicAdd(&g.colsum[n0 + cn], sum);
+				}
 		}
 	} else if(tid == 0 && nk > 0) {
 		atomicExch(g.err, 3u);
