@@ -7,9 +7,9 @@
 // Network: 338 -> 512 -> 512 -> 512 -> 3, GELU (erf form) after each hidden
 // layer, bf16 weights and activations, FP32 accumulation.  Every matrix
 // product runs on the tcgen05 tensor cores (k_gemm): C[M][N] = A[M][K]
-// B[N][K]^T with both operands K-major bf16 in global memory, staged
-// through shared memory in the UMMA core-matrix layout (no swizzle),
-// accumulated in TMEM and finished by a fused epilogue:
+// B[N][K]^T with both operands K-major bf16 in global memory, brought into
+// a 4-deep shared-memory ring by TMA (128-byte swizzle), accumulated in
+// TMEM and finished by a fused epilogue:
 //   forward   Z = A W^T + b, H = GELU(Z) (bf16, also written transposed for
 //             the weight gradients)
 //   backward  dZ = (dZ_next W_next) * GELU'(Z) (bf16, both layouts) and the
@@ -19,12 +19,17 @@
 // -> 384 columns, outputs 3 -> 16).  Training uses Adam on FP32 master
 // weights and refreshes the bf16 copies (and their transposes) after each
 // step.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
-#include <cmath>
 #include <algorithm>
+#include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "runtime.h"
@@ -84,25 +89,11 @@ __device__ __forceinline__ float gelu_grad(float z)
 	return 0.5f * (1.0f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
 }
 
-// byte offset of the 16-byte chunk c (8 bf16 along K) of row r in a tile of
-// R rows x 64 K: four K-slices of 16 (R x 32 B each), core matrices of 8
-// rows x 16 B, LBO 128 (K direction), SBO 256 (8-row groups)
-__device__ __forceinline__ uint32_t tile_off(int R, int r, int c) { return (uint32_t) ((c >> 1) * (R * 32) + (r >> 3) * 256 + (c & 1) * 128 + (r & 7) * 16); }
-
-// 16-byte asynchronous copies global -> shared (cp.async): the operand
-// tiles of later K chunks load while the tensor core works on earlier ones
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src)
-{
-	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N> __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
 constexpr int GSTAGES = 4;  // operand ring depth (K chunks in shared memory)
 
 template <int NT, int EPI>
-__global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ GemmArgs g)
+__global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+						    const __grid_constant__ GemmArgs g)
 {
 	constexpr int A_BYTES = GM * GK * 2;
 	constexpr int B_BYTES = NT * GK * 2;
@@ -110,20 +101,24 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ Gemm
 	extern __shared__ uint8_t smem_raw[];
 	// aligned by an offset on the shared array itself, so that accesses
 	// through it stay shared-memory accesses (an integer round trip would
-	// make them generic)
+	// make them generic); every tile starts on a 1024-byte boundary, as the
+	// 128-byte swizzle needs
 	uint8_t *smem = smem_raw + ((1024 - ((uintptr_t) smem_raw & 1023)) & 1023);
 	uint8_t *sA = smem, *sB = smem + GSTAGES * A_BYTES;
-	__shared__ __align__(8) uint64_t bars[GSTAGES];
+	__shared__ __align__(8) uint64_t full[GSTAGES], done[GSTAGES];
 	__shared__ uint32_t tslot;
-	__shared__ int abort_flag;
+	__shared__ int abort_flag, ok_all;
 
 	const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 	const int tiles_n = g.N / NT;
 	const int m0 = (blockIdx.x / tiles_n) * GM, n0 = (blockIdx.x % tiles_n) * NT;
 	if(tid == 0) {
-		for(int i = 0; i < GSTAGES; i++)
-			mbar_init(smem_u32(&bars[i]), 1);
+		for(int i = 0; i < GSTAGES; i++) {
+			mbar_init(smem_u32(&full[i]), 1);
+			mbar_init(smem_u32(&done[i]), 1);
+		}
 		abort_flag = 0;
+		ok_all = 0;
 		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 	}
 	if(warp == 0)
@@ -139,62 +134,57 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ Gemm
 	const int per = (nk_all + ks - 1) / ks;
 	const int kbeg = blockIdx.y * per;
 	const int nk = kbeg >= nk_all ? 0 : (nk_all - kbeg < per ? nk_all - kbeg : per);
-	// every thread issues its share of chunk kc's 16-byte copies
-	auto load = [&](int kc_local) {
-		const int kc = kbeg + kc_local;
-		const int b = kc_local % GSTAGES;
-		const uint32_t a_s = smem_u32(sA + b * A_BYTES), b_s = smem_u32(sB + b * B_BYTES);
-		const __nv_bfloat16 *Ag = g.A + (long long) m0 * g.lda + (long long) kc * GK;
-		for(int i = tid; i < GM * 8; i += G_THREADS) {
-			const int r = i >> 3, c = i & 7;
-			cp_async16(a_s + tile_off(GM, r, c), Ag + (long long) r * g.lda + c * 8);
-		}
-		const __nv_bfloat16 *Bg = g.B + (long long) n0 * g.ldb + (long long) kc * GK;
-		for(int i = tid; i < NT * 8; i += G_THREADS) {
-			const int r = i >> 3, c = i & 7;
-			cp_async16(b_s + tile_off(NT, r, c), Bg + (long long) r * g.ldb + c * 8);
-		}
-	};
-	for(int s = 0; s < GSTAGES - 1; s++) {
-		if(s < nk)
-			load(s);
-		cp_async_commit();
-	}
-	bool ok = true;
-	int issued = -1;  // last chunk whose MMAs were issued
-	for(int kc = 0; kc < nk; kc++) {
-		const int b = kc % GSTAGES;
-		// chunk kc is complete for this thread; hand it to the async proxy
-		cp_async_wait<GSTAGES - 2>();
-		fence_proxy_async();
-		__syncthreads();
-		if(tid == 0) {
+	if(tid == 0) {
+		// One thread streams the operands and issues the MMAs: chunk c's
+		// A and B tiles land by TMA on full[c % GSTAGES]; its MMAs commit
+		// to done[c % GSTAGES], which frees the slot for chunk
+		// c + GSTAGES.  Loads run GSTAGES - 1 chunks ahead.
+		auto issue = [&](int c) {
+			const int b = c % GSTAGES;
+			mbar_arrive_tx(smem_u32(&full[b]), A_BYTES + B_BYTES);
+			tma_load_2d(smem_u32(sA + b * A_BYTES), &tmA, smem_u32(&full[b]), (kbeg + c) * GK, m0);
+			tma_load_2d(smem_u32(sB + b * B_BYTES), &tmB, smem_u32(&full[b]), (kbeg + c) * GK, n0);
+		};
+		int loaded = 0, issued = -1;
+		bool ok = true;
+		for(; loaded < GSTAGES - 1 && loaded < nk; loaded++)
+			issue(loaded);
+		for(int kc = 0; kc < nk; kc++) {
+			const int b = kc % GSTAGES;
+			if(!mbar_wait(smem_u32(&full[b]), (kc / GSTAGES) & 1, &abort_flag, g.err, 1)) {
+				ok = false;
+				break;
+			}
 			tc_fence_after();
 			const uint32_t a0 = smem_u32(sA + b * A_BYTES), b0 = smem_u32(sB + b * B_BYTES);
 #pragma unroll
 			for(int s = 0; s < GK / 16; s++)
-				umma_bf16(tmem, umma_desc(a0 + s * GM * 32, 128, 256), umma_desc(b0 + s * NT * 32, 128, 256), idesc, (kc > 0 || s > 0) ? 1u : 0u);
-			umma_commit(smem_u32(&bars[b]));
+				umma_bf16(tmem, umma_desc_sw128(a0 + s * 32), umma_desc_sw128(b0 + s * 32), idesc, (kc > 0 || s > 0) ? 1u : 0u);
+			umma_commit(smem_u32(&done[b]));
+			issued = kc;
+			if(loaded < nk) {
+				// the slot of chunk `loaded` held chunk kc - 1
+				if(kc >= 1 && !mbar_wait(smem_u32(&done[(kc - 1) % GSTAGES]), ((kc - 1) / GSTAGES) & 1, &abort_flag, g.err, 2)) {
+					ok = false;
+					break;
+				}
+				issue(loaded++);
+			}
 		}
-		issued = kc;
-		// refill the slot chunk kc - 1 used, once its MMAs are done
-		const int nx = kc + GSTAGES - 1;
-		if(nx < nk) {
-			if(kc >= 1)
-				ok = mbar_wait(smem_u32(&bars[(kc - 1) % GSTAGES]), ((kc - 1) / GSTAGES) & 1, &abort_flag, g.err, 1);
-			ok = __syncthreads_and(ok);
-			if(!ok)
-				break;
-			load(nx);
-		}
-		cp_async_commit();
+		// the last commit covers every MMA of the tile
+		if(ok && nk > 0)
+			ok = mbar_wait(smem_u32(&done[(nk - 1) % GSTAGES]), ((nk - 1) / GSTAGES) & 1, &abort_flag, g.err, 2);
+		else if(issued >= 0)
+			mbar_drain(smem_u32(&done[issued % GSTAGES]), (issued / GSTAGES) & 1);
+		// no copy may still land in the ring after a failed wait
+		if(!ok)
+			for(int c = issued + 1; c < loaded; c++)
+				mbar_drain(smem_u32(&full[c % GSTAGES]), (c / GSTAGES) & 1);
+		ok_all = ok;
 	}
-	cp_async_wait_all();
-	// the last commit covers every MMA of the tile
-	if(ok && nk > 0)
-		ok = mbar_wait(smem_u32(&bars[(nk - 1) % GSTAGES]), ((nk - 1) / GSTAGES) & 1, &abort_flag, g.err, 2);
+	__syncthreads();
 	tc_fence_after();
-	ok = __syncthreads_and(ok && !abort_flag);
+	const bool ok = ok_all != 0;
 	if(ok && nk > 0) {
 		// Epilogue through shared memory (the operand ring is idle once the
 		// last MMA has retired): the accumulators go TMEM -> registers ->
@@ -300,12 +290,8 @@ __global__ void __launch_bounds__(G_THREADS) k_gemm(const __grid_constant__ Gemm
 					atomicAdd(&g.colsum[n0 + cn], sum);
 				}
 		}
-	} else if(tid == 0 && nk > 0) {
-		atomicExch(g.err, 3u);
-		// let the MMAs in flight finish before the accumulator is freed
-		if(issued >= 0)
-			mbar_drain(smem_u32(&bars[issued % GSTAGES]), (issued / GSTAGES) & 1);
-	}
+	} else if(tid == 0 && nk > 0)
+		atomicExch(g.err, 3u);  // (the MMAs and copies in flight were drained above)
 	tc_fence_before();
 	__syncthreads();
 	if(warp == 0)
@@ -629,6 +615,56 @@ int mlp_refresh(void *plan, void *stream);
 
 static size_t smem_bytes(int NT) { return 1024 + (size_t) GSTAGES * (GM * GK * 2 + NT * GK * 2); }
 
+// TMA descriptors of the operands: a bf16 matrix [rows][ld] read as
+// [rows][cols] in boxes of 64 K x box_rows rows, 128-byte swizzle (the
+// layout umma_desc_sw128 reads).  Encoded once per (device, matrix, box):
+// the network's buffers are fixed for the life of a plan.
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+	static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+	static std::once_flag once;
+	std::call_once(once, [] {
+		void *p = nullptr;
+		cudaDriverEntryPointQueryResult q;
+		if(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess && q == cudaDriverEntryPointSuccess)
+			fn = (PFN_cuTensorMapEncodeTiled_v12000) p;
+	});
+	return fn;
+}
+
+static int operand_map(const __nv_bfloat16 *p, long long rows, long long cols, long long ld, int box_rows, CUtensorMap *out)
+{
+	static std::mutex mu;
+	static std::map<std::tuple<int, const void *, long long, long long, long long, int>, CUtensorMap> cache;
+	int dev = 0;
+	CKM(cudaGetDevice(&dev));
+	const auto key = std::make_tuple(dev, (const void *) p, rows, cols, ld, box_rows);
+	std::lock_guard<std::mutex> lk(mu);
+	auto it = cache.find(key);
+	if(it != cache.end()) {
+		*out = it->second;
+		return 0;
+	}
+	if(!encode_fn()) {
+		set_error("gemm: cuTensorMapEncodeTiled unavailable");
+		return -1;
+	}
+	cuuint64_t gdim[2] = {(cuuint64_t) cols, (cuuint64_t) rows};
+	cuuint64_t gstr[1] = {(cuuint64_t) ld * 2};
+	cuuint32_t box[2] = {(cuuint32_t) GK, (cuuint32_t) box_rows};
+	cuuint32_t estr[2] = {1, 1};
+	CUtensorMap m;
+	const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<__nv_bfloat16 *>(p), gdim, gstr, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+				       CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+	if(r != CUDA_SUCCESS) {
+		set_error("gemm: cuTensorMapEncodeTiled failed (%d)", (int) r);
+		return -1;
+	}
+	cache[key] = m;
+	*out = m;
+	return 0;
+}
+
 template <int NT, int EPI>
 static int launch_gemm(const GemmArgs &g, cudaStream_t st)
 {
@@ -636,6 +672,9 @@ static int launch_gemm(const GemmArgs &g, cudaStream_t st)
 		set_error("gemm: shape %d x %d x %d not padded", g.M, g.N, g.K);
 		return -1;
 	}
+	CUtensorMap tmA, tmB;
+	if(operand_map(g.A, g.M, g.K, g.lda, GM, &tmA) || operand_map(g.B, g.N, g.K, g.ldb, NT, &tmB))
+		return -1;
 	const size_t sm = smem_bytes(NT);
 	CKM(cudaFuncSetAttribute(k_gemm<NT, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm));
 	const unsigned tiles = (unsigned) (g.M / GM) * (unsigned) (g.N / NT);
@@ -654,7 +693,7 @@ static int launch_gemm(const GemmArgs &g, cudaStream_t st)
 		}
 	}
 	dim3 grid(tiles, h.ksplit);
-	k_gemm<NT, EPI><<<grid, G_THREADS, sm, st>>>(h);
+	k_gemm<NT, EPI><<<grid, G_THREADS, sm, st>>>(tmA, tmB, h);
 	CKM(cudaGetLastError());
 	return 0;
 }

@@ -79,6 +79,13 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap *map
 		: "memory");
 }
 
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int x, int y)
+{
+	asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(dst), "l"((uint64_t) map),
+		     "r"(bar), "r"(x), "r"(y)
+		     : "memory");
+}
+
 __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
 {
 	asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst), "l"(src), "r"(bytes), "r"(bar)
@@ -110,6 +117,22 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
 	d |= (uint64_t) ((lbo >> 4) & 0x3FFF) << 16;
 	d |= (uint64_t) ((sbo >> 4) & 0x3FFF) << 32;
 	d |= (uint64_t) 1 << 46;
+	return d;
+}
+
+// the same for a K-major operand in the 128-byte swizzled layout a TMA
+// copy with CU_TENSOR_MAP_SWIZZLE_128B writes (rows of 64 bf16 = 128 B, 8-row
+// groups 1024 B apart, the tile 1024-byte aligned): SBO 1024, LBO unused,
+// swizzle mode 2; the K steps of 16 elements inside the 128-byte row advance
+// the start address by 32 B
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr)
+{
+	uint64_t d = 0;
+	d |= (uint64_t) ((saddr >> 4) & 0x3FFF);
+	d |= (uint64_t) 1 << 16;
+	d |= (uint64_t) (1024 >> 4) << 32;
+	d |= (uint64_t) 1 << 46;
+	d |= (uint64_t) 2 << 61;
 	return d;
 }
 
