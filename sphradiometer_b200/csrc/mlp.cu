@@ -362,17 +362,24 @@ __global__ void k_sky_features(int n, int L, const double2 *sky, float *feat)
 
 // FP32 features [n][338] -> bf16 X [rows][D0] (zero padded) and, when XT is
 // given, X^T [D0][rows]
+// (32 x 32 tiles, 32 x 8 threads: X written along its rows, XT along its
+// rows through the tile in shared memory)
 __global__ void k_load_features(int n, int rows, const float *feat, __nv_bfloat16 *X, __nv_bfloat16 *XT)
 {
-	const long long total = (long long) rows * D0;
-	for(long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < total; e += (long long) gridDim.x * blockDim.x) {
-		const int r = (int) (e / D0), k = (int) (e % D0);
+	__shared__ __nv_bfloat16 t[32][34];
+	const int r0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+	for(int i = threadIdx.y; i < 32; i += blockDim.y) {
+		const int r = r0 + i, k = k0 + threadIdx.x;
 		const float f = (r < n && k < F_IN) ? feat[(long long) r * F_IN + k] : 0.f;
 		const __nv_bfloat16 b = __float2bfloat16_rn(f);
-		X[e] = b;
-		if(XT)
-			XT[(long long) k * rows + r] = b;
+		X[(long long) r * D0 + k] = b;
+		t[i][threadIdx.x] = b;
 	}
+	if(!XT)
+		return;
+	__syncthreads();
+	for(int i = threadIdx.y; i < 32; i += blockDim.y)
+		XT[(long long) (k0 + i) * rows + r0 + threadIdx.x] = t[threadIdx.x][i];
 }
 
 // cosine loss against unit targets: L = mean_r (1 - y_r . t_r / |y_r|);
@@ -396,13 +403,13 @@ __global__ void k_loss_grad(int n, int rows, const float *Y, const float *target
 		g[1] = sc * (t1 - c * y1 / ny);
 		g[2] = sc * (t2 - c * y2 / ny);
 	}
-	for(int j = 0; j < D4K; j++) {
-		const float v = j < 3 ? g[j] : 0.f;
-		const __nv_bfloat16 b = __float2bfloat16_rn(v);
+	// the three live columns of dY and rows of dYT (their padding is zero
+	// from the plan's creation on)
+	for(int j = 0; j < 3; j++) {
+		const __nv_bfloat16 b = __float2bfloat16_rn(g[j]);
 		dY[(long long) r * D4K + j] = b;
+		dYT[(long long) j * rows + r] = b;
 	}
-	for(int j = 0; j < GM; j++)
-		dYT[(long long) j * rows + r] = __float2bfloat16_rn(j < 3 ? g[j] : 0.f);
 	// head bias gradient from the same bf16-rounded dY the GEMMs use
 	for(int j = 0; j < 3; j++) {
 		float s = __bfloat162float(__float2bfloat16_rn(g[j]));
@@ -433,28 +440,58 @@ __global__ void k_directions(int n, const float *Y, float *dir)
 // Adam on FP32 master parameters w[rows][cols] (valid block vr x vc; the
 // padding stays zero) and refresh of the bf16 copy [rows][cols] and, when
 // given, the transposed copy [tcols... ] laid out as [cols][ldt]
+__device__ __forceinline__ float adam_step(int e, int r, int k, int vr, int vc, float *w, const float *grad, long long ldg, float *m, float *v, float lr,
+					   float b1, float b2, float eps, float c1, float c2)
+{
+	float x = w[e];
+	if(r < vr && k < vc) {
+		const float gr = grad[(long long) r * ldg + k];
+		const float mm = b1 * m[e] + (1 - b1) * gr;
+		const float vv = b2 * v[e] + (1 - b2) * gr * gr;
+		m[e] = mm;
+		v[e] = vv;
+		x -= lr * (mm / c1) / (sqrtf(vv / c2) + eps);
+		w[e] = x;
+	}
+	return x;
+}
+
+// (a grid-stride loop: the biases, and weights without a transposed copy)
 __global__ void k_adam(int rows, int cols, int vr, int vc, float *w, const float *grad, long long ldg, float *m, float *v, float lr, float b1, float b2,
-		       float eps, float c1, float c2, __nv_bfloat16 *wb, __nv_bfloat16 *wbT, int ldt)
+		       float eps, float c1, float c2, __nv_bfloat16 *wb)
 {
 	const long long total = (long long) rows * cols;
 	for(long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < total; e += (long long) gridDim.x * blockDim.x) {
 		const int r = (int) (e / cols), k = (int) (e % cols);
-		float x = w[e];
-		if(r < vr && k < vc) {
-			const float gr = grad[(long long) r * ldg + k];
-			const float mm = b1 * m[e] + (1 - b1) * gr;
-			const float vv = b2 * v[e] + (1 - b2) * gr * gr;
-			m[e] = mm;
-			v[e] = vv;
-			x -= lr * (mm / c1) / (sqrtf(vv / c2) + eps);
-			w[e] = x;
-		}
-		if(wb) {
-			const __nv_bfloat16 b = __float2bfloat16_rn(x);
+		const float x = adam_step((int) e, r, k, vr, vc, w, grad, ldg, m, v, lr, b1, b2, eps, c1, c2);
+		if(wb)
+			wb[e] = __float2bfloat16_rn(x);
+	}
+}
+
+// the same on 32 x 32 tiles of a weight matrix (32 x 8 threads) that also
+// has a transposed bf16 copy [cols][ldt]: both copies written along their
+// rows, the transposed one through the tile in shared memory
+__global__ void k_adam_t(int rows, int cols, int vr, int vc, float *w, const float *grad, long long ldg, float *m, float *v, float lr, float b1, float b2,
+			 float eps, float c1, float c2, __nv_bfloat16 *wb, __nv_bfloat16 *wbT, int ldt)
+{
+	__shared__ __nv_bfloat16 t[32][34];
+	const int r0 = blockIdx.y * 32, k0 = blockIdx.x * 32;
+	for(int i = threadIdx.y; i < 32; i += blockDim.y) {
+		const int r = r0 + i, k = k0 + threadIdx.x;
+		__nv_bfloat16 b = __float2bfloat16_rn(0.f);
+		if(r < rows && k < cols) {
+			const int e = r * cols + k;
+			b = __float2bfloat16_rn(adam_step(e, r, k, vr, vc, w, grad, ldg, m, v, lr, b1, b2, eps, c1, c2));
 			wb[e] = b;
-			if(wbT)
-				wbT[(long long) k * ldt + r] = b;
 		}
+		t[i][threadIdx.x] = b;
+	}
+	__syncthreads();
+	for(int i = threadIdx.y; i < 32; i += blockDim.y) {
+		const int k = k0 + i, r = r0 + threadIdx.x;
+		if(k < cols && r < rows)
+			wbT[(long long) k * ldt + r] = t[threadIdx.x][i];
 	}
 }
 
@@ -764,7 +801,8 @@ void *mlp_create(int max_batch, unsigned long long seed)
 			return nullptr;
 		}
 	}
-	if(dmemset(p->WbT[3], 0, (size_t) HID * D4K * 2) || dmemset(p->gW[3], 0, (size_t) GM * HID * 4) || dmemset(p->err, 0, 4) || stream_sync()) {
+	if(dmemset(p->WbT[3], 0, (size_t) HID * D4K * 2) || dmemset(p->gW[3], 0, (size_t) GM * HID * 4) || dmemset(p->err, 0, 4) ||
+	   dmemset(p->dY, 0, (size_t) R * D4K * 2) || dmemset(p->dYT, 0, (size_t) GM * R * 2) || stream_sync()) {
 		delete p;
 		return nullptr;
 	}
@@ -785,9 +823,12 @@ static void adam_launch(Mlp *p, int i, float lr, float b1, float b2, float eps, 
 	const int ldt = (i == 3) ? D4K : rows;
 	const long long ldg = cols;
 	const int vr = update ? p->vout[i] : 0;
-	k_adam<<<256, 256, 0, st>>>(rows, cols, vr, p->vin[i], p->W[i], p->gW[i], ldg, p->mW[i], p->vW[i], lr, b1, b2, eps, c1, c2, p->Wb[i], wT, ldt);
-	k_adam<<<1, 256, 0, st>>>(1, rows, update ? 1 : 0, p->vout[i], p->bvec[i], p->gb[i], rows, p->mb[i], p->vb[i], lr, b1, b2, eps, c1, c2, nullptr,
-				   nullptr, 0);
+	if(wT)
+		k_adam_t<<<dim3((cols + 31) / 32, (rows + 31) / 32), dim3(32, 8), 0, st>>>(rows, cols, vr, p->vin[i], p->W[i], p->gW[i], ldg, p->mW[i], p->vW[i], lr,
+											  b1, b2, eps, c1, c2, p->Wb[i], wT, ldt);
+	else
+		k_adam<<<256, 256, 0, st>>>(rows, cols, vr, p->vin[i], p->W[i], p->gW[i], ldg, p->mW[i], p->vW[i], lr, b1, b2, eps, c1, c2, p->Wb[i]);
+	k_adam<<<1, 256, 0, st>>>(1, rows, update ? 1 : 0, p->vout[i], p->bvec[i], p->gb[i], rows, p->mb[i], p->vb[i], lr, b1, b2, eps, c1, c2, nullptr);
 }
 
 int mlp_refresh(void *plan, void *stream)
@@ -833,7 +874,7 @@ int mlp_load(void *plan, const float *feat, int n, int with_transpose, void *str
 		return -1;
 	}
 	const int R = rows_for(n > 0 ? n : 1);
-	k_load_features<<<512, 256, 0, st>>>(n, R, feat ? feat : p->feat, p->X, with_transpose ? p->XT : nullptr);
+	k_load_features<<<dim3(D0 / 32, R / 32), dim3(32, 8), 0, st>>>(n, R, feat ? feat : p->feat, p->X, with_transpose ? p->XT : nullptr);
 	CKM(cudaGetLastError());
 	return 0;
 }
