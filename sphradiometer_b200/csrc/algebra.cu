@@ -24,6 +24,7 @@
 #include <algorithm>
 
 #include "runtime.h"
+#include "tc_common.cuh"
 #include "wigner.cuh"
 
 namespace sphrad {
@@ -48,7 +49,18 @@ __device__ __forceinline__ long long lm_off(int L, int l, int m)
 }
 
 // first element of degree l's (2l+1)^2 block: sum_{j<l} (2j+1)^2 for l >= 1
-__device__ __forceinline__ long long blk_off(int l) { return l <= 1 ? 0 : (4LL * l * l * l - l - 3) / 3; }
+// offset of degree l's block in the Delta table: blocks of degrees 1, 2, ...
+// each [wp][wp] with wp = 2l+1 rounded up to 4, zero-padded (16-byte
+// aligned blocks and rows)
+__host__ __device__ __forceinline__ long long delta_off(int l)
+{
+	long long o = 0;
+	for(int j = 1; j < l; j++) {
+		const long long wp = (2 * j + 4) & ~3;
+		o += wp * wp;
+	}
+	return o;
+}
 
 template <class T> struct Cx;
 template <> struct Cx<float> {
@@ -99,6 +111,18 @@ __device__ __forceinline__ double2 phase_mul(double2 c, double phi, int q)
 	}
 }
 
+// four consecutive values (16-byte aligned for float, 32 for double)
+__device__ __forceinline__ void load4(const float *p, float *d)
+{
+	const float4 v = *(const float4 *) p;
+	d[0] = v.x, d[1] = v.y, d[2] = v.z, d[3] = v.w;
+}
+__device__ __forceinline__ void load4(const double *p, double *d)
+{
+	const double2 a = *(const double2 *) p, b = *(const double2 *) (p + 2);
+	d[0] = a.x, d[1] = a.y, d[2] = b.x, d[3] = b.y;
+}
+
 // Rotation of G series at degree l (blockIdx.y) through the factorisation of
 // the reference's Wigner-D matrices (sh_series_rotation.c:287-422) by the
 // fixed real matrix Delta = D(R_y(pi/2)):
@@ -123,46 +147,106 @@ __global__ void __launch_bounds__(128) k_rotate_fac(int n, int L, int polar, con
 	}
 	T2 *sU = (T2 *) rot_smem;        // [G][w]: P Z(-gamma) c
 	T2 *sV = sU + G * w;             // [G][w]: E Delta^T (...)
-	const T *Dl = delta + blk_off(l);
-	// Delta in shared memory, or read from the (L2-resident) table when a
-	// degree's block does not fit
-	T *sD = (T *) (sV + G * w);      // [w][w]
-	if(!dglobal)
-		for(int i = threadIdx.x; i < w * w; i += blockDim.x)
-			sD[i] = Dl[i];
-	const T *D = dglobal ? Dl : sD;
-	for(int i = threadIdx.x; i < G * w; i += blockDim.x) {
-		const int g = i / w, mi = i - g * w, m = mi - l, s = s0 + g;
-		double2 c = make_double2(0.0, 0.0);
-		if(s < n) {
-			const double2 *cs = in + (long long) s * istride;
-			if(!polar)
-				c = cs[lm_off(L, l, m)];
-			else if(m == 0)
-				c = cs[l];
-			c = phase_mul(c, -(double) m * abg[3 * (size_t) s + 2], m);
-		}
-		sU[i] = T2{(T) c.x, (T) c.y};
+	// Delta (padded [wp][wp], wp = w rounded up to 4) in shared memory by
+	// 16-byte asynchronous copies, all in flight while the coefficients
+	// are gathered; or read from the (L2-resident) table when a degree's
+	// block does not fit
+	const int wp = (w + 3) & ~3, nq4 = wp / 4;
+	const T *Dl = delta + delta_off(l);
+	T *sD = (T *) (sV + G * w);
+	if(!dglobal) {
+		const int nchunk = wp * wp * (int) sizeof(T) / 16;
+		for(int i = threadIdx.x; i < nchunk; i += blockDim.x)
+			cp_async16(smem_u32(sD) + 16u * i, (const char *) Dl + 16 * (size_t) i, 16);
+		cp_async_commit();
 	}
-	__syncthreads();
-	for(int k = threadIdx.x; k < w; k += blockDim.x) {
-		T2 acc[G];
+	const T *D = dglobal ? Dl : sD;
+	// the degree's coefficients lie scattered over the m-major layout: a
+	// thread issues PF of its loads before it uses the first
+	constexpr int PF = 8;
+	for(int i0 = threadIdx.x; i0 < G * w; i0 += PF * blockDim.x) {
+		double2 c[PF];
 #pragma unroll
-		for(int g = 0; g < G; g++)
-			acc[g] = T2{(T) 0, (T) 0};
-		for(int m = 0; m < w; m++) {
-			const T d = D[m * w + k];
-#pragma unroll
-			for(int g = 0; g < G; g++) {
-				const T2 u = sU[g * w + m];
-				acc[g].x += d * u.x;
-				acc[g].y += d * u.y;
+		for(int k = 0; k < PF; k++) {
+			const int i = i0 + k * blockDim.x;
+			c[k] = make_double2(0.0, 0.0);
+			if(i < G * w) {
+				const int g = i / w, m = i - g * w - l, s = s0 + g;
+				if(s < n) {
+					const double2 *cs = in + (long long) s * istride;
+					if(!polar)
+						c[k] = __ldg(cs + lm_off(L, l, m));
+					else if(m == 0)
+						c[k] = __ldg(cs + l);
+				}
 			}
 		}
 #pragma unroll
-		for(int g = 0; g < G; g++)
-			sV[g * w + k] = acc[g];
+		for(int k = 0; k < PF; k++) {
+			const int i = i0 + k * blockDim.x;
+			if(i < G * w) {
+				const int g = i / w, m = i - g * w - l, s = s0 + g;
+				double2 cc = c[k];
+				if(s < n)
+					cc = phase_mul(cc, -(double) m * abg[3 * (size_t) s + 2], m);
+				sU[i] = T2{(T) cc.x, (T) cc.y};
+			}
+		}
 	}
+	if(!dglobal)
+		cp_async_wait<0>();
+	__syncthreads();
+	if(!dglobal) {
+		// sV = Delta^T sU, register-blocked: a thread takes four series
+		// (gq) and four output orders (kq); per m one vector load of Delta's
+		// row and four of the series feed 32 FMAs (same summation order)
+		for(int t = threadIdx.x; t < (G / 4) * nq4; t += blockDim.x) {
+			const int gq = t / nq4, kq = t - gq * nq4;
+			T2 acc[4][4];
+#pragma unroll
+			for(int i = 0; i < 4; i++)
+#pragma unroll
+				for(int j = 0; j < 4; j++)
+					acc[i][j] = T2{(T) 0, (T) 0};
+			for(int m = 0; m < w; m++) {
+				T d[4];
+				load4(sD + m * wp + 4 * kq, d);
+#pragma unroll
+				for(int i = 0; i < 4; i++) {
+					const T2 u = sU[(4 * gq + i) * w + m];
+#pragma unroll
+					for(int j = 0; j < 4; j++) {
+						acc[i][j].x += d[j] * u.x;
+						acc[i][j].y += d[j] * u.y;
+					}
+				}
+			}
+#pragma unroll
+			for(int i = 0; i < 4; i++)
+#pragma unroll
+				for(int j = 0; j < 4; j++)
+					if(4 * kq + j < w)
+						sV[(4 * gq + i) * w + 4 * kq + j] = acc[i][j];
+		}
+	} else
+		for(int k = threadIdx.x; k < w; k += blockDim.x) {
+			T2 acc[G];
+#pragma unroll
+			for(int g = 0; g < G; g++)
+				acc[g] = T2{(T) 0, (T) 0};
+			for(int m = 0; m < w; m++) {
+				const T d = D[m * wp + k];
+#pragma unroll
+				for(int g = 0; g < G; g++) {
+					const T2 u = sU[g * w + m];
+					acc[g].x += d * u.x;
+					acc[g].y += d * u.y;
+				}
+			}
+#pragma unroll
+			for(int g = 0; g < G; g++)
+				sV[g * w + k] = acc[g];
+		}
 	__syncthreads();
 	// E(beta): e^{i k beta} (FP64 phases), in place
 	for(int i = threadIdx.x; i < G * w; i += blockDim.x) {
@@ -174,24 +258,58 @@ __global__ void __launch_bounds__(128) k_rotate_fac(int n, int L, int polar, con
 		}
 	}
 	__syncthreads();
-	for(int mi = threadIdx.x; mi < w; mi += blockDim.x) {
-		T2 acc[G];
+	if(!dglobal) {
+		// sU = Delta sV: four series (gq) and four output orders (mq), the
+		// orders' rows of Delta read per k
+		for(int t = threadIdx.x; t < (G / 4) * nq4; t += blockDim.x) {
+			const int gq = t / nq4, mq = t - gq * nq4;
+			T2 acc[4][4];
 #pragma unroll
-		for(int g = 0; g < G; g++)
-			acc[g] = T2{(T) 0, (T) 0};
-		for(int k = 0; k < w; k++) {
-			const T d = D[mi * w + k];
+			for(int i = 0; i < 4; i++)
 #pragma unroll
-			for(int g = 0; g < G; g++) {
-				const T2 v = sV[g * w + k];
-				acc[g].x += d * v.x;
-				acc[g].y += d * v.y;
+				for(int j = 0; j < 4; j++)
+					acc[i][j] = T2{(T) 0, (T) 0};
+			for(int k = 0; k < w; k++) {
+				T d[4];
+#pragma unroll
+				for(int j = 0; j < 4; j++)
+					d[j] = sD[(4 * mq + j) * wp + k];
+#pragma unroll
+				for(int i = 0; i < 4; i++) {
+					const T2 v = sV[(4 * gq + i) * w + k];
+#pragma unroll
+					for(int j = 0; j < 4; j++) {
+						acc[i][j].x += d[j] * v.x;
+						acc[i][j].y += d[j] * v.y;
+					}
+				}
 			}
-		}
 #pragma unroll
-		for(int g = 0; g < G; g++)
-			sU[g * w + mi] = acc[g];
-	}
+			for(int i = 0; i < 4; i++)
+#pragma unroll
+				for(int j = 0; j < 4; j++)
+					if(4 * mq + j < w)
+						sU[(4 * gq + i) * w + 4 * mq + j] = acc[i][j];
+		}
+	} else
+		for(int mi = threadIdx.x; mi < w; mi += blockDim.x) {
+			T2 acc[G];
+#pragma unroll
+			for(int g = 0; g < G; g++)
+				acc[g] = T2{(T) 0, (T) 0};
+			for(int k = 0; k < w; k++) {
+				const T d = D[mi * wp + k];
+#pragma unroll
+				for(int g = 0; g < G; g++) {
+					const T2 v = sV[g * w + k];
+					acc[g].x += d * v.x;
+					acc[g].y += d * v.y;
+				}
+			}
+#pragma unroll
+			for(int g = 0; g < G; g++)
+				sU[g * w + mi] = acc[g];
+		}
 	__syncthreads();
 	// (-i)^m e^{-i m alpha} (FP64 phases) and the output
 	for(int i = threadIdx.x; i < G * w; i += blockDim.x) {
@@ -229,23 +347,23 @@ static int delta_table(int L, const double **d64, const float **d32)
 		t.d64 = nullptr;
 		t.d32 = nullptr;
 		t.L = -1;
-		const size_t len = rot_offset((unsigned) L + 1);
+		const size_t len = (size_t) delta_off(L + 1);
 		// R_y(pi/2) as euler_rotation_matrix(0, pi/2, 0) builds it
 		const double R[9] = {0.0, 0.0, 1.0, 0.0, 1.0, 0.0, -1.0, 0.0, 0.0};
 		std::vector<double> flat(2 * (len ? len : 1));
 		if(L >= 1 && build_rotation_plan((unsigned) L, R, flat.data()))
 			return -1;
 		// flat: element (m, k) of degree l at rot_offset(l) + (2l+1)(k+l) + (m+l);
-		// table: [m][k] row-major
+		// table: [m][k] row-major in padded blocks (delta_off)
 		std::vector<double> h64(len ? len : 1, 0.0);
 		std::vector<float> h32(len ? len : 1, 0.f);
 		for(int l = 1; l <= L; l++) {
-			const size_t o = rot_offset((unsigned) l), w = 2 * (size_t) l + 1;
+			const size_t o = rot_offset((unsigned) l), w = 2 * (size_t) l + 1, wp = (w + 3) & ~(size_t) 3, po = (size_t) delta_off(l);
 			for(size_t m = 0; m < w; m++)
 				for(size_t k = 0; k < w; k++) {
 					const double v = flat[2 * (o + w * k + m)];
-					h64[o + m * w + k] = v;
-					h32[o + m * w + k] = (float) v;
+					h64[po + m * wp + k] = v;
+					h32[po + m * wp + k] = (float) v;
 				}
 		}
 		t.d64 = (double *) dmalloc(h64.size() * sizeof(double));
@@ -287,7 +405,8 @@ int rotate_batch(const void *in, int n, unsigned L, int polar, const double *R, 
 	const int w = 2 * (int) L + 1;
 	const size_t kMaxSmem = 200 * 1024;
 	if(fp32_apply) {
-		size_t smem = (size_t) 2 * kRotG32 * w * sizeof(float2) + (size_t) w * w * sizeof(float);
+		const size_t wp = (size_t) (w + 3) & ~(size_t) 3;
+		size_t smem = (size_t) 2 * kRotG32 * w * sizeof(float2) + wp * wp * sizeof(float);
 		const int dglobal = smem > kMaxSmem;
 		if(dglobal)
 			smem = (size_t) 2 * kRotG32 * w * sizeof(float2);
@@ -295,7 +414,8 @@ int rotate_batch(const void *in, int n, unsigned L, int polar, const double *R, 
 		k_rotate_fac<float, kRotG32><<<dim3((n + kRotG32 - 1) / kRotG32, L + 1), 128, smem, st>>>(n, (int) L, polar, (const double2 *) in, istride, abg,
 													   d32, dglobal, (double2 *) out);
 	} else {
-		size_t smem = (size_t) 2 * kRotG64 * w * sizeof(double2) + (size_t) w * w * sizeof(double);
+		const size_t wp = (size_t) (w + 3) & ~(size_t) 3;
+		size_t smem = (size_t) 2 * kRotG64 * w * sizeof(double2) + wp * wp * sizeof(double);
 		const int dglobal = smem > kMaxSmem;
 		if(dglobal)
 			smem = (size_t) 2 * kRotG64 * w * sizeof(double2);
