@@ -97,11 +97,28 @@ __global__ void k_euler(int n, const double *__restrict__ R_all, double *__restr
 	abg[3 * (size_t) s + 2] = g;
 }
 
-// c * e^{i phi} * i^q (q taken mod 4) in FP64
-__device__ __forceinline__ double2 phase_mul(double2 c, double phi, int q)
+// The phase factors a rotation applies, per series s and j = -L..L:
+// ph[s][0][j + L] = e^{-i j gamma}, ph[s][1][..] = e^{i j beta},
+// ph[s][2][..] = e^{-i j alpha} (FP64 sincos of the same arguments the
+// degree blocks used to form), so that the blocks of every degree read
+// them instead of evaluating (2l+1) sincos per series each
+__global__ void k_rot_phases(int n, int L, const double *__restrict__ abg, double2 *__restrict__ ph)
 {
-	double sn, cs;
-	sincos(phi, &sn, &cs);
+	const int W2 = 2 * L + 1;
+	const long long total = (long long) n * 3 * W2;
+	for(long long e = blockIdx.x * (long long) blockDim.x + threadIdx.x; e < total; e += (long long) gridDim.x * blockDim.x) {
+		const int s = (int) (e / (3 * W2)), r = (int) (e - (long long) s * 3 * W2), a = r / W2, j = r - a * W2 - L;
+		const double x = a == 0 ? -(double) j * abg[3 * (size_t) s + 2] : a == 1 ? (double) j * abg[3 * (size_t) s + 1] : -(double) j * abg[3 * (size_t) s];
+		double sn, cs;
+		sincos(x, &sn, &cs);
+		ph[e] = make_double2(cs, sn);
+	}
+}
+
+// c * e^{i phi} * i^q (q taken mod 4) in FP64, e^{i phi} given as (cos, sin)
+__device__ __forceinline__ double2 phase_mul(double2 c, double2 e, int q)
+{
+	const double cs = e.x, sn = e.y;
 	double2 v = make_double2(c.x * cs - c.y * sn, c.x * sn + c.y * cs);
 	switch(q & 3) {
 	case 1: return make_double2(-v.y, v.x);
@@ -133,7 +150,7 @@ __device__ __forceinline__ void load4(const double *p, double *d)
 // run in T with Delta in shared memory (Delta[m][k] at m (2l+1) + k).
 template <class T, int G>
 __global__ void __launch_bounds__(128) k_rotate_fac(int n, int L, int polar, const double2 *__restrict__ in, long long istride,
-						    const double *__restrict__ abg, const T *__restrict__ delta, int dglobal, double2 *__restrict__ out)
+						    const double2 *__restrict__ ph, const T *__restrict__ delta, int dglobal, double2 *__restrict__ out)
 {
 	using T2 = typename Cx<T>::type;
 	extern __shared__ __align__(16) unsigned char rot_smem[];
@@ -163,13 +180,14 @@ __global__ void __launch_bounds__(128) k_rotate_fac(int n, int L, int polar, con
 	const T *D = dglobal ? Dl : sD;
 	// the degree's coefficients lie scattered over the m-major layout: a
 	// thread issues PF of its loads before it uses the first
+	const int W2 = 2 * L + 1;
 	constexpr int PF = 8;
 	for(int i0 = threadIdx.x; i0 < G * w; i0 += PF * blockDim.x) {
-		double2 c[PF];
+		double2 c[PF], e[PF];
 #pragma unroll
 		for(int k = 0; k < PF; k++) {
 			const int i = i0 + k * blockDim.x;
-			c[k] = make_double2(0.0, 0.0);
+			c[k] = e[k] = make_double2(0.0, 0.0);
 			if(i < G * w) {
 				const int g = i / w, m = i - g * w - l, s = s0 + g;
 				if(s < n) {
@@ -178,6 +196,7 @@ __global__ void __launch_bounds__(128) k_rotate_fac(int n, int L, int polar, con
 						c[k] = __ldg(cs + lm_off(L, l, m));
 					else if(m == 0)
 						c[k] = __ldg(cs + l);
+					e[k] = __ldg(ph + (size_t) s * 3 * W2 + m + L);
 				}
 			}
 		}
@@ -188,7 +207,7 @@ __global__ void __launch_bounds__(128) k_rotate_fac(int n, int L, int polar, con
 				const int g = i / w, m = i - g * w - l, s = s0 + g;
 				double2 cc = c[k];
 				if(s < n)
-					cc = phase_mul(cc, -(double) m * abg[3 * (size_t) s + 2], m);
+					cc = phase_mul(cc, e[k], m);
 				sU[i] = T2{(T) cc.x, (T) cc.y};
 			}
 		}
@@ -248,13 +267,23 @@ __global__ void __launch_bounds__(128) k_rotate_fac(int n, int L, int polar, con
 				sV[g * w + k] = acc[g];
 		}
 	__syncthreads();
-	// E(beta): e^{i k beta} (FP64 phases), in place
-	for(int i = threadIdx.x; i < G * w; i += blockDim.x) {
-		const int g = i / w, k = i - g * w, s = s0 + g;
-		if(s < n) {
-			const T2 v = sV[i];
-			const double2 r = phase_mul(make_double2((double) v.x, (double) v.y), (double) (k - l) * abg[3 * (size_t) s + 1], 0);
-			sV[i] = T2{(T) r.x, (T) r.y};
+	// E(beta): e^{i k beta} (FP64 phases), in place; the table loads of
+	// PF elements issued together
+	for(int i0 = threadIdx.x; i0 < G * w; i0 += PF * blockDim.x) {
+		double2 e[PF];
+#pragma unroll
+		for(int q = 0; q < PF; q++) {
+			const int i = i0 + q * blockDim.x, g = i / w, k = i - g * w, s = s0 + g;
+			e[q] = i < G * w && s < n ? __ldg(ph + ((size_t) s * 3 + 1) * W2 + k - l + L) : make_double2(1.0, 0.0);
+		}
+#pragma unroll
+		for(int q = 0; q < PF; q++) {
+			const int i = i0 + q * blockDim.x, g = i / w, s = s0 + g;
+			if(i < G * w && s < n) {
+				const T2 v = sV[i];
+				const double2 r = phase_mul(make_double2((double) v.x, (double) v.y), e[q], 0);
+				sV[i] = T2{(T) r.x, (T) r.y};
+			}
 		}
 	}
 	__syncthreads();
@@ -312,11 +341,20 @@ __global__ void __launch_bounds__(128) k_rotate_fac(int n, int L, int polar, con
 		}
 	__syncthreads();
 	// (-i)^m e^{-i m alpha} (FP64 phases) and the output
-	for(int i = threadIdx.x; i < G * w; i += blockDim.x) {
-		const int g = i / w, mi = i - g * w, m = mi - l, s = s0 + g;
-		if(s < n) {
-			const T2 v = sU[i];
-			out[(long long) s * ostride + lm_off(L, l, m)] = phase_mul(make_double2((double) v.x, (double) v.y), -(double) m * abg[3 * (size_t) s], -m);
+	for(int i0 = threadIdx.x; i0 < G * w; i0 += PF * blockDim.x) {
+		double2 e[PF];
+#pragma unroll
+		for(int q = 0; q < PF; q++) {
+			const int i = i0 + q * blockDim.x, g = i / w, mi = i - g * w, s = s0 + g;
+			e[q] = i < G * w && s < n ? __ldg(ph + ((size_t) s * 3 + 2) * W2 + mi - l + L) : make_double2(1.0, 0.0);
+		}
+#pragma unroll
+		for(int q = 0; q < PF; q++) {
+			const int i = i0 + q * blockDim.x, g = i / w, mi = i - g * w, m = mi - l, s = s0 + g;
+			if(i < G * w && s < n) {
+				const T2 v = sU[i];
+				out[(long long) s * ostride + lm_off(L, l, m)] = phase_mul(make_double2((double) v.x, (double) v.y), e[q], -m);
+			}
 		}
 	}
 }
@@ -377,11 +415,10 @@ static int delta_table(int L, const double **d64, const float **d32)
 	return 0;
 }
 
-size_t rotate_batch_scratch_bytes(unsigned L, int n)
-{
-	(void) L;
-	return ((size_t) (n > 0 ? n : 1) * 3 * sizeof(double) + 255) / 256 * 256;
-}
+// scratch: the Euler angles [n][3], then the phase table [n][3][2L+1]
+static size_t rot_abg_bytes(int n) { return ((size_t) (n > 0 ? n : 1) * 3 * sizeof(double) + 255) / 256 * 256; }
+
+size_t rotate_batch_scratch_bytes(unsigned L, int n) { return rot_abg_bytes(n) + (size_t) (n > 0 ? n : 1) * 3 * (2 * (size_t) L + 1) * sizeof(double2); }
 
 int rotate_batch(const void *in, int n, unsigned L, int polar, const double *R, void *out, int fp32_apply, void *scratch, size_t scratch_bytes,
 		 void *stream)
@@ -401,7 +438,9 @@ int rotate_batch(const void *in, int n, unsigned L, int polar, const double *R, 
 		return -1;
 	const long long istride = polar ? (long long) L + 1 : (long long) (L + 1) * (L + 1);
 	double *abg = (double *) scratch;
+	double2 *ph = (double2 *) ((char *) scratch + rot_abg_bytes(n));
 	k_euler<<<(n + 127) / 128, 128, 0, st>>>(n, R, abg);
+	k_rot_phases<<<(int) std::min<long long>(((long long) n * 3 * (2 * L + 1) + 255) / 256, 4096), 256, 0, st>>>(n, (int) L, abg, ph);
 	const int w = 2 * (int) L + 1;
 	const size_t kMaxSmem = 200 * 1024;
 	if(fp32_apply) {
@@ -411,7 +450,7 @@ int rotate_batch(const void *in, int n, unsigned L, int polar, const double *R, 
 		if(dglobal)
 			smem = (size_t) 2 * kRotG32 * w * sizeof(float2);
 		CK(cudaFuncSetAttribute(k_rotate_fac<float, kRotG32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) std::max(smem, (size_t) 48 * 1024)));
-		k_rotate_fac<float, kRotG32><<<dim3((n + kRotG32 - 1) / kRotG32, L + 1), 128, smem, st>>>(n, (int) L, polar, (const double2 *) in, istride, abg,
+		k_rotate_fac<float, kRotG32><<<dim3((n + kRotG32 - 1) / kRotG32, L + 1), 128, smem, st>>>(n, (int) L, polar, (const double2 *) in, istride, ph,
 													   d32, dglobal, (double2 *) out);
 	} else {
 		const size_t wp = (size_t) (w + 3) & ~(size_t) 3;
@@ -420,7 +459,7 @@ int rotate_batch(const void *in, int n, unsigned L, int polar, const double *R, 
 		if(dglobal)
 			smem = (size_t) 2 * kRotG64 * w * sizeof(double2);
 		CK(cudaFuncSetAttribute(k_rotate_fac<double, kRotG64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) std::max(smem, (size_t) 48 * 1024)));
-		k_rotate_fac<double, kRotG64><<<dim3((n + kRotG64 - 1) / kRotG64, L + 1), 128, smem, st>>>(n, (int) L, polar, (const double2 *) in, istride, abg,
+		k_rotate_fac<double, kRotG64><<<dim3((n + kRotG64 - 1) / kRotG64, L + 1), 128, smem, st>>>(n, (int) L, polar, (const double2 *) in, istride, ph,
 													     d64, dglobal, (double2 *) out);
 	}
 	CK(cudaGetLastError());
