@@ -168,13 +168,19 @@ __global__ void __launch_bounds__(128) k_rotate_fac(int n, int L, int polar, con
 	// 16-byte asynchronous copies, all in flight while the coefficients
 	// are gathered; or read from the (L2-resident) table when a degree's
 	// block does not fit
-	const int wp = (w + 3) & ~3, nq4 = wp / 4;
+	// In shared memory its rows are wps apart, wps / 4 odd: a warp's
+	// 16-byte loads from 32 different rows then meet 8 distinct bank groups
+	// (4 wavefronts, no replays).
+	const int wp = (w + 3) & ~3, nq4 = wp / 4, wps = (nq4 & 1) ? wp : wp + 4;
 	const T *Dl = delta + delta_off(l);
 	T *sD = (T *) (sV + G * w);
 	if(!dglobal) {
-		const int nchunk = wp * wp * (int) sizeof(T) / 16;
-		for(int i = threadIdx.x; i < nchunk; i += blockDim.x)
-			cp_async16(smem_u32(sD) + 16u * i, (const char *) Dl + 16 * (size_t) i, 16);
+		constexpr int CPR = 16 / (int) sizeof(T);  // elements of a 16-byte chunk
+		const int rowc = wp / CPR;                 // chunks of a row
+		for(int i = threadIdx.x; i < wp * rowc; i += blockDim.x) {
+			const int r = i / rowc, c = i - r * rowc;
+			cp_async16(smem_u32(sD + r * wps + c * CPR), (const char *) (Dl + (size_t) r * wp + c * CPR), 16);
+		}
 		cp_async_commit();
 	}
 	const T *D = dglobal ? Dl : sD;
@@ -229,7 +235,7 @@ __global__ void __launch_bounds__(128) k_rotate_fac(int n, int L, int polar, con
 					acc[i][j] = T2{(T) 0, (T) 0};
 			for(int m = 0; m < w; m++) {
 				T d[4];
-				load4(sD + m * wp + 4 * kq, d);
+				load4(sD + m * wps + 4 * kq, d);
 #pragma unroll
 				for(int i = 0; i < 4; i++) {
 					const T2 u = sU[(4 * gq + i) * w + m];
@@ -288,8 +294,9 @@ __global__ void __launch_bounds__(128) k_rotate_fac(int n, int L, int polar, con
 	}
 	__syncthreads();
 	if(!dglobal) {
-		// sU = Delta sV: four series (gq) and four output orders (mq), the
-		// orders' rows of Delta read per k
+		// sU = Delta sV: four series (gq) and the output orders mq + j nq4
+		// (j < 4), their rows of Delta read four k at a time (16-byte loads,
+		// the k order of every sum kept)
 		for(int t = threadIdx.x; t < (G / 4) * nq4; t += blockDim.x) {
 			const int gq = t / nq4, mq = t - gq * nq4;
 			T2 acc[4][4];
@@ -298,27 +305,41 @@ __global__ void __launch_bounds__(128) k_rotate_fac(int n, int L, int polar, con
 #pragma unroll
 				for(int j = 0; j < 4; j++)
 					acc[i][j] = T2{(T) 0, (T) 0};
-			for(int k = 0; k < w; k++) {
-				T d[4];
+			int k0 = 0;
+			for(; k0 + 4 <= w; k0 += 4) {
+				T d[4][4];
 #pragma unroll
 				for(int j = 0; j < 4; j++)
-					d[j] = sD[(4 * mq + j) * wp + k];
+					load4(sD + (mq + j * nq4) * wps + k0, d[j]);
+#pragma unroll
+				for(int kk = 0; kk < 4; kk++)
+#pragma unroll
+					for(int i = 0; i < 4; i++) {
+						const T2 v = sV[(4 * gq + i) * w + k0 + kk];
+#pragma unroll
+						for(int j = 0; j < 4; j++) {
+							acc[i][j].x += d[j][kk] * v.x;
+							acc[i][j].y += d[j][kk] * v.y;
+						}
+					}
+			}
+			for(int k = k0; k < w; k++)
 #pragma unroll
 				for(int i = 0; i < 4; i++) {
 					const T2 v = sV[(4 * gq + i) * w + k];
 #pragma unroll
 					for(int j = 0; j < 4; j++) {
-						acc[i][j].x += d[j] * v.x;
-						acc[i][j].y += d[j] * v.y;
+						const T d = sD[(mq + j * nq4) * wps + k];
+						acc[i][j].x += d * v.x;
+						acc[i][j].y += d * v.y;
 					}
 				}
-			}
 #pragma unroll
 			for(int i = 0; i < 4; i++)
 #pragma unroll
 				for(int j = 0; j < 4; j++)
-					if(4 * mq + j < w)
-						sU[(4 * gq + i) * w + 4 * mq + j] = acc[i][j];
+					if(mq + j * nq4 < w)
+						sU[(4 * gq + i) * w + mq + j * nq4] = acc[i][j];
 		}
 	} else
 		for(int mi = threadIdx.x; mi < w; mi += blockDim.x) {
@@ -445,7 +466,7 @@ int rotate_batch(const void *in, int n, unsigned L, int polar, const double *R, 
 	const size_t kMaxSmem = 200 * 1024;
 	if(fp32_apply) {
 		const size_t wp = (size_t) (w + 3) & ~(size_t) 3;
-		size_t smem = (size_t) 2 * kRotG32 * w * sizeof(float2) + wp * wp * sizeof(float);
+		size_t smem = (size_t) 2 * kRotG32 * w * sizeof(float2) + wp * (wp + 4) * sizeof(float);
 		const int dglobal = smem > kMaxSmem;
 		if(dglobal)
 			smem = (size_t) 2 * kRotG32 * w * sizeof(float2);
@@ -454,7 +475,7 @@ int rotate_batch(const void *in, int n, unsigned L, int polar, const double *R, 
 													   d32, dglobal, (double2 *) out);
 	} else {
 		const size_t wp = (size_t) (w + 3) & ~(size_t) 3;
-		size_t smem = (size_t) 2 * kRotG64 * w * sizeof(double2) + wp * wp * sizeof(double);
+		size_t smem = (size_t) 2 * kRotG64 * w * sizeof(double2) + wp * (wp + 4) * sizeof(double);
 		const int dglobal = smem > kMaxSmem;
 		if(dglobal)
 			smem = (size_t) 2 * kRotG64 * w * sizeof(double2);
