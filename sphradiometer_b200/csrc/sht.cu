@@ -167,6 +167,30 @@ __global__ void k_sht_F(int L_in, int polar, const Tin2 *coeff, long long cstrid
 // sums in the same order, so the results are those of k_sht_F.
 constexpr int SF_SER = 16;
 
+// block-wide staging of n values into shared memory, dst[k] = f(k): every
+// thread issues PF of its loads before it stores the first (a plain loop
+// would wait out one L2 round trip per element)
+constexpr int kStagePF = 8;
+template <class V, class F>
+__device__ __forceinline__ void stage_ahead(V *dst, int n, F f)
+{
+	for(int k0 = threadIdx.x; k0 < n; k0 += kStagePF * blockDim.x) {
+		V v[kStagePF];
+#pragma unroll
+		for(int q = 0; q < kStagePF; q++) {
+			const int k = k0 + q * blockDim.x;
+			if(k < n)
+				v[q] = f(k);
+		}
+#pragma unroll
+		for(int q = 0; q < kStagePF; q++) {
+			const int k = k0 + q * blockDim.x;
+			if(k < n)
+				dst[k] = v[q];
+		}
+	}
+}
+
 template <class Tin2, class T>
 __global__ void k_sht_F_tile(int S, int L_in, int polar, const Tin2 *coeff, long long cstride, int Luse, int M, int Ltab, int nt, const T *tab,
 			     typename V2<T>::t *F)
@@ -182,18 +206,17 @@ __global__ void k_sht_F_tile(int S, int L_in, int polar, const Tin2 *coeff, long
 	T *ts = (T *) smem_raw;                               // [K][nt]
 	T2 *cs = (T2 *) (smem_raw + (((size_t) K * nt * sizeof(T) + 15) & ~(size_t) 15));  // [SF_SER][K]
 	const T *t0 = tab + tab_off(Ltab, nt, am);
-	for(int k = threadIdx.x; k < K * nt; k += blockDim.x)
-		ts[k] = t0[k];
-	for(int k = threadIdx.x; k < SF_SER * K; k += blockDim.x) {
+	stage_ahead(ts, K * nt, [&](int k) { return __ldg(t0 + k); });
+	stage_ahead(cs, SF_SER * K, [&](int k) {
 		const int ss = k / K, l = am + (k - ss * K);
 		const int sr = s0 + ss;
 		T2 v = mk2((T) 0, (T) 0);
 		if(sr < S) {
-			const Tin2 c = coeff[(long long) sr * cstride + (polar ? l : lmoff(L_in, l, m))];
+			const Tin2 c = __ldg(coeff + (long long) sr * cstride + (polar ? l : lmoff(L_in, l, m)));
 			v = mk2((T) c.x, (T) c.y);
 		}
-		cs[k] = v;
-	}
+		return v;
+	});
 	__syncthreads();
 	const bool neg = m < 0 && (am & 1);
 	for(int i = threadIdx.x; i < nt; i += blockDim.x) {
@@ -647,13 +670,12 @@ __global__ void k_sht_A_tile(int S, int L_out, int L_lay, int polar_out, int M, 
 	const int K = L_out - am + 1;
 	T2 *hs = (T2 *) smem_raw;           // [SA_SER][nt]
 	T *ts = (T *) (hs + SA_SER * nt);   // [K][nt]
-	for(int k = threadIdx.x; k < SA_SER * nt; k += blockDim.x) {
+	stage_ahead(hs, SA_SER * nt, [&](int k) {
 		const int ss = k / nt, i = k - ss * nt;
-		hs[k] = s0 + ss < S ? H[((long long) (s0 + ss) * nt + i) * W + mi] : mk2((T) 0, (T) 0);
-	}
+		return s0 + ss < S ? __ldg(H + ((long long) (s0 + ss) * nt + i) * W + mi) : mk2((T) 0, (T) 0);
+	});
 	const T *t0 = tab + tab_off(Ltab, nt, am);
-	for(int k = threadIdx.x; k < K * nt; k += blockDim.x)
-		ts[k] = t0[k];
+	stage_ahead(ts, K * nt, [&](int k) { return __ldg(t0 + k); });
 	__syncthreads();
 	const double sg = (m < 0 && (am & 1)) ? -1.0 : 1.0;
 	constexpr int NSG = SA_SER / SA_LS;
