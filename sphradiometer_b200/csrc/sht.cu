@@ -486,17 +486,16 @@ __global__ void k_sht_H(long long nrows, int nt, int nphi, int M, const Tin2 *me
 	T2 *rows_s = tws + nphi;  // [rpb][nphi]
 	const int W = 2 * M + 1;
 	const long long row0 = (long long) blockIdx.x * rpb;
-	for(int k = threadIdx.x; k < nphi; k += blockDim.x)
-		tws[k] = tw[k];
-	for(int k = threadIdx.x; k < rpb * nphi; k += blockDim.x) {
+	stage_ahead(tws, nphi, [&](int k) { return __ldg(tw + k); });
+	stage_ahead(rows_s, rpb * nphi, [&](int k) {
 		const int r = k / nphi;
 		T2 v = mk2((T) 0, (T) 0);
 		if(row0 + r < nrows) {
-			const Tin2 x = mesh[(row0 + r) * nphi + (k - r * nphi)];
+			const Tin2 x = __ldg(mesh + (row0 + r) * nphi + (k - r * nphi));
 			v = mk2((T) x.x, (T) x.y);
 		}
-		rows_s[k] = v;
-	}
+		return v;
+	});
 	__syncthreads();
 	const int ngroups = (W + SH_QB - 1) / SH_QB;   // order groups
 	const int nrg = rpb / SH_RT;                   // row groups
