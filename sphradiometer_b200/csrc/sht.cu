@@ -1309,16 +1309,43 @@ __global__ void __launch_bounds__(FOLD ? 32 * refine_warps(METHOD) : 128, 1)
 		if(n_sky > 0) {
 			__syncwarp();  // the previous series is no longer read
 			if(FOLD && !polar) {
-				for(int m = 0; m <= L; m++) {
-					const long long o = lmoff(L, m, m) - m, on = m > 0 ? lmoff(L, m, -m) - m : 0;
-					for(int l = m + lane; l <= L; l += 32) {
-						double2 v = c[o + l];
-						if(m > 0) {
-							const double2 w = c[on + l];
-							v.x += (m & 1) ? -w.x : w.x;
-							v.y -= (m & 1) ? -w.y : w.y;
+				// the folded index i is the series' own index of (l, m >= 0):
+				// lanes walk it in steps of 32 (m decoded incrementally) and
+				// issue four elements' loads per round
+				int mcur = 0;
+				int ocur = 0, onext = L + 1;  // first index of order mcur, mcur + 1
+				for(int i0 = lane; i0 < n_sky; i0 += 32 * 4) {
+					double2 a[4], b[4];
+					int mm[4];
+#pragma unroll
+					for(int q = 0; q < 4; q++) {
+						const int i = i0 + 32 * q;
+						a[q] = b[q] = make_double2(0.0, 0.0);
+						mm[q] = 0;
+						if(i < n_sky) {
+							while(i >= onext) {
+								mcur++;
+								ocur = onext;
+								onext += L + 1 - mcur;
+							}
+							const int m = mcur, l = m + (i - ocur);
+							mm[q] = m;
+							a[q] = c[i];
+							if(m > 0)
+								b[q] = c[lmoff(L, l, -m)];
 						}
-						cs[o + l] = v;
+					}
+#pragma unroll
+					for(int q = 0; q < 4; q++) {
+						const int i = i0 + 32 * q;
+						if(i < n_sky) {
+							double2 v = a[q];
+							if(mm[q] > 0) {
+								v.x += (mm[q] & 1) ? -b[q].x : b[q].x;
+								v.y -= (mm[q] & 1) ? -b[q].y : b[q].y;
+							}
+							cs[i] = v;
+						}
 					}
 				}
 			} else {
