@@ -60,6 +60,26 @@ def test_rotate_batch_matches_oracle(S, l_max, polar, fp32):
         assert rel(got[s], ref) < tol, (s, rel(got[s], ref))
 
 
+@pytest.mark.parametrize("fp32", [False, True])
+def test_rotate_batch_large_lmax(S, fp32):
+    """l_max 80: in FP64 a degree's Delta block and the block's series no
+    longer fit shared memory together, so the products read Delta from the
+    (L2-resident) table in its padded layout; in FP32 the shared-memory
+    tile is about 150 KB.  Bound: the FP32 application's 2e-6, and in FP64
+    the accuracy of the reference recursion's Delta at this degree (its
+    orthogonality error grows from 5e-13 at l = 48 to 1e-11 at 64)."""
+    import torch
+    l_max, n = 80, 5
+    rng = np.random.default_rng(80)
+    series = np.array([random_series(rng, l_max, False) for _ in range(n)])
+    R = np.array([r for _, r in random_rotations(rng, n)])
+    got = S.rotate_batch(torch.from_numpy(series).cuda(), torch.from_numpy(R).cuda(), l_max, polar=False, fp32=fp32).cpu().numpy()
+    tol = 2e-6 if fp32 else 1e-9
+    for s in range(n):
+        ref = O.rotate(series[s], l_max, False, O.rotation_plan(l_max, R[s]))
+        assert rel(got[s], ref) < tol, (s, rel(got[s], ref))
+
+
 @pytest.mark.parametrize("la,lb,ld", [(0, 0, 0), (3, 5, 8), (12, 12, 12), (20, 16, 40), (48, 48, 48), (10, 6, 30)])
 @pytest.mark.parametrize("fp32", [False, True])
 def test_product_batch_matches_oracle(S, la, lb, ld, fp32):
