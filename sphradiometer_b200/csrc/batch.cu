@@ -177,9 +177,6 @@ __device__ __forceinline__ const TcJob &job_seek(const TcArgs &a, int &jb, int u
 	return a.job[jb];
 }
 
-// indexed spectra ring: slot [detector][bin of the thread][converter
-// thread] of 16-byte elements, so a warp's loads are consecutive
-constexpr int IDX_PLANE = CONV_WARPS * 32 * 16;
 
 // Split the complex value (re, im) into NPART packed bf16x2 words (re in the
 // low half): part q is the round-to-nearest bf16 of what parts 0..q-1 left,
@@ -254,7 +251,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 	// through it stay shared-memory accesses (an integer round trip would
 	// make them generic)
 	uint8_t *smem = smem_raw + ((1024 - ((uintptr_t) smem_raw & 1023)) & 1023);
-	const int f_slab = TM * 128;  // = (KB / (CONV_WARPS / 4)) * IDX_PLANE
+	const int f_slab = TM * 128;
 	const int f_stage = a.n_det * f_slab;
 	const int btile = a.npad * KE * 2;
 	const int ab_bytes = a.B * NPART * btile;
@@ -282,7 +279,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 
 	if(threadIdx.x == 0) {
 		for(int i = 0; i < NFS; i++) {
-			mbar_init(smem_u32(&f_full[i]), 1);
+			// (indexed spectra: one arrival per converter thread, when its
+			// copies of the stage have landed)
+			mbar_init(smem_u32(&f_full[i]), IDX ? CONV_WARPS * 32 : 1);
 			mbar_init(smem_u32(&f_empty[i]), CONV_WARPS);
 		}
 		for(int i = 0; i < NABS; i++) {
@@ -434,35 +433,45 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 		const int roff = (r >> 3) * 256 + (r & 7) * 16 + (g >> 1) * 128 + (g & 1) * 8;
 		PieceCursor pc{u0, u1};
 		int piece = 0, jb = 0;
-		// indexed spectra: this thread's bins of stage j of its range
-		// (row r, bins g BPT .. g BPT + BPT - 1 of every detector of the
-		// stage's job) into slot j % NFS, one copy group per stage (empty
-		// past the range)
+		// indexed spectra: the converter threads stage the ring themselves,
+		// in the tensor-map path's layout ([detector][row][128 B], the
+		// 16-byte chunks of row r permuted by r & 7).  Thread ct copies the
+		// elements ct + 512 q, bin fastest, so that a warp's copies cover 4
+		// rows x 128 contiguous bytes (and 4 whole rows of the slot); its
+		// copies arrive on f_full[slot] when they land, and a slot is
+		// refilled once every converter warp has released it (f_empty).
 		const int ct = (warp - 2) * 32 + lane;
 		int in_jb = 0, cur_jb = -1, cur_tile = -1;
-		const double2 *rowp = nullptr;
-		auto stage_in = [&](int j) {
-			if(j < nst) {
-				const TcJob &J = job_seek(a, in_jb, u0 + j);
-				const int lu = u0 + j - J.u_begin, t = lu / J.Kst, k0 = (lu % J.Kst) * KB + g * BPT;
-				if(t != cur_tile || in_jb != cur_jb) {
-					cur_tile = t;
-					cur_jb = in_jb;
-					const int s = t * TM + r;
-					rowp = s < J.S ? a.rows + J.row_off[s] : nullptr;
-				}
-				const uint32_t dst = smem_u32(sF + (j % NFS) * f_stage + ct * 16);
-#pragma unroll
-				for(int d = 0; d < TC_MAXDET; d++)
-#pragma unroll
-					for(int c = 0; c < BPT; c++)
-						if(d < J.nd) {
-							const bool ok = rowp != nullptr && k0 + c < J.Ku;
-							cp_async16(dst + (uint32_t) ((d * BPT + c) * IDX_PLANE), ok ? (const void *) (rowp + J.det_off[d] + k0 + c) : (const void *) a.rows,
-								   ok ? 16u : 0u);
-						}
+		const double2 *rowA = nullptr, *rowB = nullptr;  // rows ct >> 3 and 64 + (ct >> 3) of the tile
+		auto stage_in = [&](int j) -> bool {
+			if(j >= nst)
+				return true;
+			const int js = j % NFS;
+			if(!mbar_wait(smem_u32(&f_empty[js]), ((j / NFS) & 1) ^ 1, abort_flag, a.err, 1, a.wait))
+				return false;
+			const TcJob &J = job_seek(a, in_jb, u0 + j);
+			const int lu = u0 + j - J.u_begin, t = lu / J.Kst, k0 = (lu % J.Kst) * KB;
+			if(t != cur_tile || in_jb != cur_jb) {
+				cur_tile = t;
+				cur_jb = in_jb;
+				const int sa = t * TM + (ct >> 3), sb = sa + 64;
+				rowA = sa < J.S ? a.rows + J.row_off[sa] : nullptr;
+				rowB = sb < J.S ? a.rows + J.row_off[sb] : nullptr;
 			}
-			cp_async_commit();
+			const uint32_t slot = smem_u32(sF + js * f_stage);
+			const int c = ct & 7;
+#pragma unroll
+			for(int q = 0; q < 2 * TC_MAXDET; q++) {
+				const int d = q >> 1, rr = (ct >> 3) + 64 * (q & 1);
+				if(d < J.nd) {
+					const double2 *rp = (q & 1) ? rowB : rowA;
+					const bool ok = rp != nullptr && k0 + c < J.Ku;
+					cp_async16(slot + (uint32_t) (d * f_slab + rr * 128 + ((c ^ (rr & 7)) << 4)), ok ? (const void *) (rp + J.det_off[d] + k0 + c) : (const void *) a.rows,
+						   ok ? 16u : 0u);
+				}
+			}
+			cp_async_arrive_noinc(smem_u32(&f_full[js]));
+			return true;
 		};
 		if constexpr(IDX)
 			for(int j = 0; j < NFS - 1; j++)
@@ -488,11 +497,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			const int fs = it % NFS;
 			const uint32_t fph = (it / NFS) & 1;
 			if constexpr(IDX) {
-				// slot (it - 1) % NFS, read by this thread in the previous
-				// iteration, takes stage it + NFS - 1; stage it has landed
-				// once at most NFS - 1 groups are in flight
-				stage_in(it + NFS - 1);
-				cp_async_wait<NFS - 1>();
+				// stage it + NFS - 1 into the slot stage it - 1 used, then
+				// wait for stage it
+				const bool okf = stage_in(it + NFS - 1) && mbar_wait(smem_u32(&f_full[fs]), fph, abort_flag, a.err, 5, a.wait);
+				if(!__all_sync(0xffffffffu, okf))
+					break;
 			} else {
 				const bool okf = mbar_wait(smem_u32(&f_full[fs]), fph, abort_flag, a.err, 5, a.wait);
 				if(!__all_sync(0xffffffffu, okf))
@@ -509,15 +518,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 						const int cc = g * BPT + c;
 						double2 v = make_double2(0, 0);
 						if(d < nd)
-							v = *(const double2 *) (base + (IDX ? (d * BPT + c) * IDX_PLANE + ct * 16 : d * f_slab + r * 128 + ((cc ^ (r & 7)) << 4)));
+							v = *(const double2 *) (base + d * f_slab + r * 128 + ((cc ^ (r & 7)) << 4));
 						f[d][c] = make_float2((float) v.x, (float) v.y);
 					}
 			}
-			if constexpr(!IDX) {
-				__syncwarp();
-				if(lane == 0)
-					mbar_arrive(smem_u32(&f_empty[fs]));
-			}
+			__syncwarp();
+			if(lane == 0)
+				mbar_arrive(smem_u32(&f_empty[fs]));
 			const int as = it % NABS;
 			const uint32_t aph = (it / NABS) & 1;
 			const bool oke = mbar_wait(smem_u32(&ab_empty[as]), aph ^ 1, abort_flag, a.err, 6, a.wait);
@@ -604,7 +611,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 		}
 		// no copy of this thread may still land after an early exit
 		if constexpr(IDX)
-			cp_async_wait<0>();
+			cp_async_wait_all();
 	}
 	tc_fence_before();
 	__syncthreads();
