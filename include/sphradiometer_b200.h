@@ -296,11 +296,12 @@ int sphrad_uneven_set_segments(sphrad_uneven_plan *plan, int n_seg, const int *b
  * at out_offset[s], (l_max_s + 1)^2 coefficients.  Returns n_seg. */
 int sphrad_uneven_layout(const sphrad_uneven_plan *plan, long long *in_offset, long long *out_offset, long long *in_total, long long *out_total);
 int sphrad_uneven_jobs(const sphrad_uneven_plan *plan);
-/* 0 (the default): one contraction and epilogue per job on a few streams,
- * with per-job split-K; 1 (tcgen05 precisions): every job's contraction in
- * one persistent launch (the units of all jobs cut into equal ranges over
- * the SMs), then the jobs' epilogues.  sphrad_uneven_persistent reports
- * whether the persistent launch is in use. */
+/* 1 (the default; tcgen05 precisions): every job's contraction in one
+ * persistent launch (the units of all jobs cut into equal ranges over the
+ * SMs), then the jobs' epilogues; 0: one contraction and epilogue per job
+ * on a few streams, with per-job split-K (the FP32 and FP64 precisions
+ * always run so).  sphrad_uneven_persistent reports whether the persistent
+ * launch is in use. */
 int sphrad_uneven_set_persistent(sphrad_uneven_plan *plan, int on);
 int sphrad_uneven_persistent(const sphrad_uneven_plan *plan);
 /* split-K of every job (per-job launches): > 0 fixed, 0 = each job's tuned

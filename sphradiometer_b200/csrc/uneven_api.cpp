@@ -19,10 +19,10 @@
 // into its packed output, truncated to the segment's own l_max (FP64
 // atomics: a segment covered by two jobs gets the same sum in either
 // order).  Each job runs its own contraction and epilogue, the jobs spread
-// over a few streams (longest first, each to the least loaded stream); on
-// request (tcgen05 precisions) all jobs' contractions run in one persistent
-// launch (batch_contract_multi) and the jobs' epilogues are forked over the
-// streams.  The whole sequence can be captured once into a CUDA graph and
+// over a few streams (longest first, each to the least loaded stream); for
+// the tcgen05 precisions (by default; per-job launches on request) all
+// jobs' contractions run in one persistent launch (batch_contract_multi)
+// and the jobs' epilogues are forked over the streams.  The whole sequence can be captured once into a CUDA graph and
 // replayed.
 #include <sphradiometer_b200.h>
 #include <sphradiometer/correlator.h>
@@ -93,10 +93,10 @@ struct sphrad_uneven_plan {
 	cudaStream_t side[kSlots] = {};
 	cudaEvent_t ev[kSlots + 1] = {};
 	int fixed_split = 0;
-	// persistent launch (tcgen05 precisions, on request): every job's
+	// persistent launch (tcgen05 precisions, the default): every job's
 	// contraction in one launch, each job with its own zeroed workspace at
 	// ws_off
-	int persistent = 0;
+	int persistent = 1;
 	void *ws_multi = nullptr;
 	std::vector<size_t> ws_off;
 	// graph

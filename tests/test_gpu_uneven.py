@@ -113,16 +113,14 @@ def test_uneven_graph_split_and_three_detectors(S):
 
 def test_uneven_persistent_launch(S):
     """Every job's contraction in one persistent launch (tcgen05
-    precisions, on request): one contraction plus one epilogue per job per
+    precisions, the default): one contraction plus one epilogue per job per
     call; the same skies as one launch per job up to the grouping of the
     FP32 sums, and the oracle's within the bf16x3 bounds."""
     pos = W.random_positions(4, W.R_EARTH_S, W.rng_for(9))
     batch = W.make_uneven_batch(pos, 96, seed=21, t_range=(0.25, 2.0), l_choices=(16, 32, 48), buckets=(1024, 2048, 4096, 8192))
     plan = S.UnevenPlan(pos, DT, batch["buckets"], 48)
     plan.set_segments(batch["bucket"], batch["mask"], batch["l_max"])
-    assert not plan.persistent() and 2 <= plan.jobs() <= 24
-    plan.set_persistent(True)
-    assert plan.persistent()
+    assert plan.persistent() and 2 <= plan.jobs() <= 24
     pers = plan.integrate(batch["spectra"]).clone()
     assert plan.kernels_per_call() == 1 + plan.jobs()
     plan.set_persistent(False)
