@@ -882,19 +882,25 @@ __global__ void __launch_bounds__(32 * (2 + NWMAX), 1) k_cc_stream(const __grid_
 		for(int p = ctid; p < TM * KB; p += nct) {
 			const int r = p & (TM - 1), c = p >> 7;
 			const uint8_t *base = sF + fs * f_stage + r * 128 + ((c ^ (r & 7)) << 4);
-			double2 f[3];
+			// X in the contraction's own precision: FP32 products of the
+			// FP32-rounded spectra (FP64 runs at half the FP32 rate), or FP64
+			using TX2 = typename V2<T>::type;
+			TX2 f[3];
 #pragma unroll
-			for(int d = 0; d < 3; d++)
-				f[d] = d < a.n_det ? *(const double2 *) (base + d * f_slab) : make_double2(0, 0);
+			for(int d = 0; d < 3; d++) {
+				const double2 v = d < a.n_det ? *(const double2 *) (base + d * f_slab) : make_double2(0, 0);
+				f[d].x = (T) v.x;
+				f[d].y = (T) v.y;
+			}
 #pragma unroll
 			for(int bb = 0; bb < 3; bb++) {
 				if(bb >= a.B)
 					break;
 				const int ia = a.bi[bb], ib = a.bj[bb];
-				const double2 fa = ia == 0 ? f[0] : (ia == 1 ? f[1] : f[2]);
-				const double2 fb = ib == 0 ? f[0] : (ib == 1 ? f[1] : f[2]);
-				xa[(bb * KE + 2 * c) * TM + r] = (T) fma(fb.x, fa.x, fb.y * fa.y);
-				xa[(bb * KE + 2 * c + 1) * TM + r] = (T) fma(fb.y, fa.x, -fb.x * fa.y);
+				const TX2 fa = ia == 0 ? f[0] : (ia == 1 ? f[1] : f[2]);
+				const TX2 fb = ib == 0 ? f[0] : (ib == 1 ? f[1] : f[2]);
+				xa[(bb * KE + 2 * c) * TM + r] = fma(fb.x, fa.x, fb.y * fa.y);
+				xa[(bb * KE + 2 * c + 1) * TM + r] = fma(fb.y, fa.x, -fb.x * fa.y);
 			}
 		}
 		__syncwarp();
