@@ -223,10 +223,11 @@ struct PieceCursor {
 	int pstart = 0, plen = 1, send = 0;  // current piece start and length, end of the run in this tile
 	// stage u of the range (called for u0, u0 + 1, ...), in a job whose
 	// units start at ub, Kst stages per tile: is it the first / last stage
-	// of its piece?
+	// of its piece?  (Tiles, and jobs, are contiguous in u, so a tile
+	// starts where the previous tile's run ended.)
 	__device__ __forceinline__ void step(int u, int ub, int Kst, bool &first, bool &last)
 	{
-		if(u == u0 || (u - ub) % Kst == 0) {
+		if(u == u0 || u == send) {
 			const int tend = ub + ((u - ub) / Kst + 1) * Kst;
 			send = u1 < tend ? u1 : tend;
 			const int len = send - u;
@@ -441,7 +442,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 		// copies arrive on f_full[slot] when they land, and a slot is
 		// refilled once every converter warp has released it (f_empty).
 		const int ct = (warp - 2) * 32 + lane;
+		// (Stages are staged in increasing order, so the tile and the stage
+		// within it advance by counting; the job's constants are reloaded
+		// only when the job changes.)
 		int in_jb = 0, cur_jb = -1, cur_tile = -1;
+		int s_k = 0, s_Kst = 1, s_Ku = 0, s_nd = 0, s_off[TC_MAXDET] = {};
 		const double2 *rowA = nullptr, *rowB = nullptr;  // rows ct >> 3 and 64 + (ct >> 3) of the tile
 		auto stage_in = [&](int j) -> bool {
 			if(j >= nst)
@@ -450,7 +455,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			if(!mbar_wait(smem_u32(&f_empty[js]), ((j / NFS) & 1) ^ 1, abort_flag, a.err, 1, a.wait))
 				return false;
 			const TcJob &J = job_seek(a, in_jb, u0 + j);
-			const int lu = u0 + j - J.u_begin, t = lu / J.Kst, k0 = (lu % J.Kst) * KB;
+			int t = cur_tile;
+			if(in_jb != cur_jb) {
+				const int lu = u0 + j - J.u_begin;
+				s_Kst = J.Kst;
+				s_Ku = J.Ku;
+				s_nd = J.nd;
+#pragma unroll
+				for(int d = 0; d < TC_MAXDET; d++)
+					s_off[d] = J.det_off[d];
+				t = lu / s_Kst;
+				s_k = lu % s_Kst;
+			} else if(++s_k == s_Kst) {
+				s_k = 0;
+				t++;
+			}
+			const int k0 = s_k * KB;
 			if(t != cur_tile || in_jb != cur_jb) {
 				cur_tile = t;
 				cur_jb = in_jb;
@@ -463,10 +483,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 #pragma unroll
 			for(int q = 0; q < 2 * TC_MAXDET; q++) {
 				const int d = q >> 1, rr = (ct >> 3) + 64 * (q & 1);
-				if(d < J.nd) {
+				if(d < s_nd) {
 					const double2 *rp = (q & 1) ? rowB : rowA;
-					const bool ok = rp != nullptr && k0 + c < J.Ku;
-					cp_async16(slot + (uint32_t) (d * f_slab + rr * 128 + ((c ^ (rr & 7)) << 4)), ok ? (const void *) (rp + J.det_off[d] + k0 + c) : (const void *) a.rows,
+					const bool ok = rp != nullptr && k0 + c < s_Ku;
+					cp_async16(slot + (uint32_t) (d * f_slab + rr * 128 + ((c ^ (rr & 7)) << 4)), ok ? (const void *) (rp + s_off[d] + k0 + c) : (const void *) a.rows,
 						   ok ? 16u : 0u);
 				}
 			}
@@ -476,6 +496,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 		if constexpr(IDX)
 			for(int j = 0; j < NFS - 1; j++)
 				stage_in(j);
+		int m_jb = -1, m_t = 0, m_k = 0, m_Kst = 1;  // indexed: tile and stage, counted
 		for(int it = 0; it < nst; it++) {
 			bool first, last;
 			// this stage's job: detectors, baselines, segments, tile
@@ -488,7 +509,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 				nd = J.nd;
 				nb = J.B;
 				nS = J.S;
-				tile = (u0 + it - J.u_begin) / J.Kst;
+				if(jb != m_jb) {
+					const int lu = u0 + it - J.u_begin;
+					m_jb = jb;
+					m_Kst = J.Kst;
+					m_t = lu / m_Kst;
+					m_k = lu % m_Kst;
+				} else if(++m_k == m_Kst) {
+					m_k = 0;
+					m_t++;
+				}
+				tile = m_t;
 				bi = J.bi;
 				bj = J.bj;
 				accp = J.acc;
