@@ -496,7 +496,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 		if constexpr(IDX)
 			for(int j = 0; j < NFS - 1; j++)
 				stage_in(j);
-		int m_jb = -1, m_t = 0, m_k = 0, m_Kst = 1;  // indexed: tile and stage, counted
+		// indexed: tile and stage, counted; the job's constants, reloaded
+		// on a job change
+		int m_jb = -1, m_t = 0, m_k = 0, m_Kst = 1, m_ub = 0, m_nd = 0, m_nb = 0, m_nS = 0;
+		int m_bi[TC_MAXB3] = {}, m_bj[TC_MAXB3] = {};
+		float *m_acc = nullptr;
 		for(int it = 0; it < nst; it++) {
 			bool first, last;
 			// this stage's job: detectors, baselines, segments, tile
@@ -505,24 +509,32 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			float *accp = a.acc;
 			if constexpr(IDX) {
 				const TcJob &J = job_seek(a, jb, u0 + it);
-				pc.step(u0 + it, J.u_begin, J.Kst, first, last);
-				nd = J.nd;
-				nb = J.B;
-				nS = J.S;
 				if(jb != m_jb) {
-					const int lu = u0 + it - J.u_begin;
 					m_jb = jb;
+					m_ub = J.u_begin;
 					m_Kst = J.Kst;
+					m_nd = J.nd;
+					m_nb = J.B;
+					m_nS = J.S;
+#pragma unroll
+					for(int b = 0; b < TC_MAXB3; b++) {
+						m_bi[b] = J.bi[b];
+						m_bj[b] = J.bj[b];
+					}
+					m_acc = J.acc;
+					const int lu = u0 + it - m_ub;
 					m_t = lu / m_Kst;
 					m_k = lu % m_Kst;
 				} else if(++m_k == m_Kst) {
 					m_k = 0;
 					m_t++;
 				}
+				pc.step(u0 + it, m_ub, m_Kst, first, last);
+				nd = m_nd;
+				nb = m_nb;
+				nS = m_nS;
 				tile = m_t;
-				bi = J.bi;
-				bj = J.bj;
-				accp = J.acc;
+				accp = m_acc;
 			} else
 				pc.step(u0 + it, 0, a.Kst, first, last);
 			const int fs = it % NFS;
@@ -567,7 +579,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_tc_contract(const __grid_cons
 			for(int b = 0; b < TC_MAXB3; b++) {
 				if(b >= nb)
 					break;
-				const int da = bi[b], db = bj[b];
+				const int da = IDX ? m_bi[b] : bi[b], db = IDX ? m_bj[b] : bj[b];
 				uint32_t part[BPT][NPART];
 #pragma unroll
 				for(int c = 0; c < BPT; c++) {
